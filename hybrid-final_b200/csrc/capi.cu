@@ -1,0 +1,758 @@
+// capi.cu -- C ABI of libhpic: case lifecycle, operators, interchange, batches.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "capi_internal.hpp"
+
+using namespace hp;
+
+namespace hpi {
+
+thread_local std::string g_err;
+
+void set_error(const std::string &m) { g_err = m; }
+
+hp_status cuda_fail(cudaError_t e, const char *what) {
+    set_error(std::string(what) + ": " + cudaGetErrorString(e));
+    return HP_ERR_CUDA;
+}
+
+} // namespace hpi
+
+using hpi::cuda_fail;
+using hpi::set_error;
+
+#define CK(call)                                                                                                       \
+    do {                                                                                                               \
+        cudaError_t e_ = (call);                                                                                       \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);                                                           \
+    } while (0)
+
+namespace {
+
+hp_status from_exception(const std::exception &e) {
+    std::string m = e.what();
+    set_error(m);
+    if (m.rfind("deck:", 0) == 0) return HP_ERR_DECK;
+    if (m.rfind("unsupported:", 0) == 0) return HP_ERR_UNSUPPORTED;
+    return HP_ERR_ARG;
+}
+
+BuildOpts build_opts(const hp_case_opts *o) {
+    BuildOpts b;
+    if (o) {
+        b.seed = o->seed;
+        b.cap_per_cell = o->cap_per_cell;
+    }
+    return b;
+}
+
+void fill_info(const Setup &s, hp_case_info *out) {
+    std::memset(out, 0, sizeof(*out));
+    out->ngx = s.ngx; out->ngy = s.ngy; out->ncx = s.ncx; out->ncy = s.ncy;
+    out->Gsize = s.Gsize; out->Csize = s.Csize;
+    out->nsp = s.nsp; out->main_gas = s.main_gas; out->cond_numr = s.cond_numr; out->n_unknowns = s.n_unknowns;
+    for (int i = 0; i < s.nsp && i < 8; i++) out->cap[i] = s.cap[i];
+    out->mcc_subcycles = s.mcc_n;
+    out->dt = s.dt; out->dx = s.dx; out->dy = s.dy;
+}
+
+// Collision probability per cell from its lower-left node
+// (src/cuda_mccAr.cu:57-58 for electrons with dt_mcc, :189 for ions with dt).
+std::vector<float> cell_probabilities(const Setup &s) {
+    std::vector<float> p((size_t)3 * s.Csize, 0.0f);
+    if (s.main_gas != GAS_AR) return p;
+    for (int c = 0; c < s.Csize; c++) {
+        int i = c / s.ncy, j = c % s.ncy, node = i * s.ngy + j;
+        float P1 = 1.0f - std::exp(-1 * s.dt_mcc * s.sigv[0] * s.back_den1[node]);
+        float P2 = P1 + 1.0f - std::exp(-1 * s.dt_mcc * s.sigv[1] * s.fluid_den[node]);
+        float Pi = 1.0f - std::exp(-1 * s.dt * s.sigv[2] * s.back_den1[node]);
+        p[c] = P1;
+        p[(size_t)s.Csize + c] = P2;
+        p[(size_t)2 * s.Csize + c] = Pi;
+    }
+    return p;
+}
+
+// Node-layout operator (W,S,C,N,E per node, 0 off the unknowns) and its
+// row-scaled symmetric form D^-1 A, with D = 2 per Neumann edge doubling
+// (the NBC factors of src/load.c:161-164).
+void node_stencils(const Setup &s, std::vector<float> &st, std::vector<float> &sym, std::vector<float> &scale) {
+    const int G = s.Gsize;
+    st.assign((size_t)5 * G, 0.0f);
+    sym.assign((size_t)5 * G, 0.0f);
+    scale.assign(G, 1.0f);
+    for (int u = 0; u < s.n_unknowns; u++) {
+        int n = s.unk_node[u];
+        int i = n / s.ngy, j = n % s.ngy;
+        float dscale = (float)(((i == 0 || i == s.ncx) ? 2 : 1) * ((j == 0 || j == s.ncy) ? 2 : 1));
+        for (int k = 0; k < 5; k++) {
+            float a = s.stencil[(size_t)5 * u + k];
+            st[(size_t)k * G + n] = a;
+            sym[(size_t)k * G + n] = a / dscale;
+        }
+        scale[n] = 1.0f / dscale;
+    }
+}
+
+template <class T> hp_status dalloc(hp_case *c, T **p, size_t count) {
+    size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    cudaError_t e = cudaMalloc((void **)p, bytes);
+    if (e != cudaSuccess) {
+        set_error(std::string("cudaMalloc of ") + std::to_string(bytes) + " bytes: " + cudaGetErrorString(e));
+        return HP_ERR_OOM;
+    }
+    c->allocs.push_back(*p);
+    c->alloc_bytes.push_back(bytes);
+    c->bytes += bytes;
+    e = cudaMemset(*p, 0, bytes);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMemset");
+    return HP_OK;
+}
+
+template <class T> hp_status dupload(hp_case *c, T **p, const std::vector<T> &v) {
+    hp_status st = dalloc(c, p, v.size());
+    if (st != HP_OK) return st;
+    if (!v.empty()) CK(cudaMemcpy(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    return HP_OK;
+}
+
+#define TRY(x)                                                                                                         \
+    do {                                                                                                               \
+        hp_status s_ = (x);                                                                                            \
+        if (s_ != HP_OK) return s_;                                                                                    \
+    } while (0)
+
+hp_status upload_particles(hp_case *c, int isp, const int *counts, const float *x, const float *y, const float *vx,
+                           const float *vy, const float *vz) {
+    const Setup &s = c->s;
+    const int C = s.Csize, cap = c->h.sp[isp].cap;
+    std::vector<float> bx((size_t)C * cap, 0.0f), by(bx.size(), 0.0f), bvx(bx.size(), 0.0f), bvy(bx.size(), 0.0f),
+        bvz(bx.size(), 0.0f);
+    std::vector<int> cnt(C, 0);
+    size_t q = 0;
+    for (int cell = 0; cell < C; cell++) {
+        int n = counts[cell];
+        if (n < 0 || n > cap) {
+            set_error("cell " + std::to_string(cell) + " holds " + std::to_string(n) + " particles, slot pool is " +
+                      std::to_string(cap));
+            return HP_ERR_CAPACITY;
+        }
+        cnt[cell] = n;
+        for (int k = 0; k < n; k++, q++) {
+            size_t d = (size_t)cell * cap + k;
+            bx[d] = x[q]; by[d] = y[q]; bvx[d] = vx[q]; bvy[d] = vy[q]; bvz[d] = vz[q];
+        }
+    }
+    DevSpecies &sp = c->h.sp[isp];
+    CK(cudaMemcpy(sp.x, bx.data(), bx.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(sp.y, by.data(), by.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(sp.vx, bvx.data(), bvx.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(sp.vy, bvy.data(), bvy.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(sp.vz, bvz.data(), bvz.size() * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(sp.cnt, cnt.data(), (size_t)C * 4, cudaMemcpyHostToDevice));
+    CK(cudaMemset(sp.nmov, 0, (size_t)C * 4));
+    return HP_OK;
+}
+
+hp_status build_device(hp_case *c) {
+    const Setup &s = c->s;
+    DevCase &h = c->h;
+    std::memset(&h, 0, sizeof(h));
+    const int G = s.Gsize, C = s.Csize;
+    if (s.nsp > DMAXSP || s.cond_numr > DMAXCOND || s.src_num > DMAXSRC) {
+        set_error("case exceeds the library's species/conductor/source limits");
+        return HP_ERR_UNSUPPORTED;
+    }
+    h.ngx = s.ngx; h.ngy = s.ngy; h.ncx = s.ncx; h.ncy = s.ncy; h.G = G; h.C = C; h.nsp = s.nsp;
+    h.gas = s.main_gas; h.cond_numr = s.cond_numr; h.n_unknowns = s.n_unknowns;
+    h.dt_dx = s.dt_dx; h.dt_dy = s.dt_dy; h.dt = s.dt;
+    h.dx = s.dx; h.dy = s.dy; h.idx = s.idx; h.idy = s.idy; h.hdx = s.hdx; h.hdy = s.hdy; h.idxy = s.idxy;
+    TRY(dupload(c, (int **)&h.sidx, s.sidx));
+    TRY(dupload(c, (int **)&h.boundary, s.boundary));
+    TRY(dupload(c, (int **)&h.face, s.face));
+    TRY(dupload(c, (int **)&h.cond_id, s.cond_id));
+    {
+        std::vector<float> eps(C);
+        for (int k = 0; k < C; k++) eps[k] = (float)(EPS0 * s.eps_r[k]); // src/cuda_Field.cu:289-291
+        TRY(dupload(c, (float **)&h.eps, eps));
+    }
+    TRY(dupload(c, (float **)&h.dep_factor, s.dep_factor));
+    for (int isp = 0; isp < s.nsp; isp++) {
+        DevSpecies &sp = h.sp[isp];
+        sp.cap = s.cap[isp];
+        sp.Ascale = s.sp[isp].Ascale;
+        sp.q_density = s.sp[isp].q_density;
+        sp.Escale = s.sp[isp].Escale;
+        size_t nslot = (size_t)C * sp.cap;
+        TRY(dalloc(c, &sp.x, nslot));
+        TRY(dalloc(c, &sp.y, nslot));
+        TRY(dalloc(c, &sp.vx, nslot));
+        TRY(dalloc(c, &sp.vy, nslot));
+        TRY(dalloc(c, &sp.vz, nslot));
+        TRY(dalloc(c, &sp.code, nslot));
+        TRY(dalloc(c, &sp.cnt, C));
+        TRY(dalloc(c, &sp.nmov, C));
+        TRY(dalloc(c, &h.cw[isp], C));
+    }
+    TRY(dalloc(c, &h.Ex, G));
+    TRY(dalloc(c, &h.Ey, G));
+    TRY(dalloc(c, &h.phi, G));
+    TRY(dalloc(c, &h.phi_p, G));
+    TRY(dupload(c, (float **)&h.lap, s.lap_basis));
+    {
+        std::vector<float> st, sym, scale;
+        node_stencils(s, st, sym, scale);
+        TRY(dupload(c, (float **)&h.st, st));
+        TRY(dupload(c, (float **)&h.st_sym, sym));
+        TRY(dupload(c, (float **)&h.row_scale, scale));
+    }
+    TRY(dalloc(c, &h.pf_x, G));
+    TRY(dalloc(c, &h.pf_r, G));
+    TRY(dalloc(c, &h.pf_p, G));
+    TRY(dalloc(c, &h.pf_ap, G));
+    TRY(dalloc(c, &h.x64, G));
+    TRY(dalloc(c, &h.b64, G));
+    TRY(dalloc(c, &h.dots, 64));
+    TRY(dalloc(c, &h.den, (size_t)s.nsp * G));
+    TRY(dalloc(c, &h.source, G));
+    TRY(dalloc(c, &h.ave_den, (size_t)s.nsp * G));
+    TRY(dalloc(c, &h.ave_phi, G));
+    h.src_num = s.src_num;
+    for (int k = 0; k < s.src_num; k++) {
+        h.src_mid[k] = s.src_mid[k];
+        h.src_dc[k] = s.src_dc[k];
+        h.src_ac[k] = s.src_ac[k];
+        h.src_2pif[k] = s.src_2pifreq[k];
+        h.src_rphase[k] = s.src_rphase[k];
+    }
+    for (int k = 0; k < s.cond_numr; k++) h.efield_flag[k] = s.efield_flag[k];
+    TRY(dupload(c, (float **)&h.xsec, s.xsec));
+    h.n_logx = s.n_logx;
+    h.xw = 2 + s.n_cx;
+    h.idlogx = s.idlogx;
+    for (size_t k = 0; k < s.sigv.size() && k < 8; k++) h.sigv[k] = s.sigv[k];
+    for (int k = 0; k < s.TnRct && k < 16; k++) {
+        h.th[k] = s.collf[k].Th_e;
+        h.mofm[k] = s.collf[k].mofM;
+    }
+    c->prob = cell_probabilities(s);
+    TRY(dupload(c, (float **)&h.prob, c->prob));
+    TRY(dupload(c, (float **)&h.back_vel1, s.back_vel1));
+    TRY(dupload(c, (float **)&h.vsave, s.vsave));
+    h.nvel = s.nvel;
+    h.mcc_n = s.mcc_n;
+    h.seed = c->opts.seed;
+    TRY(dalloc(c, &h.tstep, 1));
+    TRY(dalloc(c, &h.status, 1));
+    TRY(dalloc(c, &h.cond_charge, (size_t)s.nsp * s.cond_numr));
+    TRY(dalloc(c, &h.mcc_count, (size_t)8 * C));
+    TRY(dalloc(c, &h.pcg_iters, 2));
+    TRY(dalloc(c, &h.ave_count, 1));
+    h.field_mode = c->opts.field_mode;
+    h.pcg_max_iter = c->opts.pcg_max_iter > 0 ? c->opts.pcg_max_iter : 100000;
+    h.pcg_tol2 = s.PCGtol2;
+    h.pcg_rtol = c->opts.pcg_rtol > 0 ? c->opts.pcg_rtol : 1e-8;
+    TRY(dalloc(c, &c->d_list0, 1));
+    TRY(dalloc(c, &c->d_case, 1));
+    CK(cudaMemcpy(c->d_case, &h, sizeof(h), cudaMemcpyHostToDevice));
+    {
+        std::vector<int> items = {0, s.nsp * C, 0, C, 0, G};
+        TRY(dupload(c, &c->d_items, items));
+    }
+    for (int isp = 0; isp < s.nsp; isp++)
+        TRY(upload_particles(c, isp, s.p_count[isp].data(), s.p_x[isp].data(), s.p_y[isp].data(), s.p_vx[isp].data(),
+                             s.p_vy[isp].data(), s.p_vz[isp].data()));
+    c->pcg_cluster = pcg_cluster_for_nodes(G);
+    return HP_OK;
+}
+
+cudaStream_t as_stream(void *s) { return (cudaStream_t)s; }
+
+
+hp_status op_field(hp_case *c, cudaStream_t st) {
+    PcgGroup g{c->pcg_cluster, c->lc.pcg_block, c->d_list0, 1};
+    cudaError_t e = launch_field(c->d_case, c->d_items + 4, 1, c->s.Gsize, &g, 1, st);
+    return e == cudaSuccess ? HP_OK : cuda_fail(e, "field");
+}
+hp_status op_move(hp_case *c, cudaStream_t st) {
+    cudaError_t e = launch_move(c->d_case, c->d_items, 1, c->s.nsp * c->s.Csize, c->lc, st);
+    return e == cudaSuccess ? HP_OK : cuda_fail(e, "move");
+}
+hp_status op_sort(hp_case *c, cudaStream_t st) {
+    cudaError_t e = launch_sort(c->d_case, c->d_items, 1, c->s.nsp * c->s.Csize, c->lc, st);
+    return e == cudaSuccess ? HP_OK : cuda_fail(e, "sort");
+}
+hp_status op_mcc(hp_case *c, cudaStream_t st) {
+    if (c->s.main_gas != GAS_AR) {
+        set_error("MCC for this gas is not built");
+        return HP_ERR_UNSUPPORTED;
+    }
+    cudaError_t e = launch_mcc_ar(c->d_case, c->d_items + 2, 1, c->s.Csize, c->lc, st);
+    return e == cudaSuccess ? HP_OK : cuda_fail(e, "mcc");
+}
+hp_status op_deposit(hp_case *c, cudaStream_t st) {
+    cudaError_t e = launch_deposit(c->d_case, c->d_items, c->d_items + 4, 1, c->s.nsp * c->s.Csize, c->s.Gsize,
+                                   c->lc, st);
+    return e == cudaSuccess ? HP_OK : cuda_fail(e, "deposit");
+}
+
+hp_status one_step(hp_case *c, cudaStream_t st) {
+    cudaError_t e = launch_advance(c->d_case, 1, st);
+    if (e != cudaSuccess) return cuda_fail(e, "advance");
+    TRY(op_field(c, st));
+    TRY(op_move(c, st));
+    TRY(op_sort(c, st));
+    TRY(op_mcc(c, st));
+    TRY(op_deposit(c, st));
+    e = launch_accumulate(c->d_case, c->d_items + 4, 1, c->s.Gsize, st);
+    return e == cudaSuccess ? HP_OK : cuda_fail(e, "accumulate");
+}
+
+int check_cuda_device(int dev) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return -1;
+    if (dev < 0 || dev >= n) return -2;
+    return 0;
+}
+
+} // namespace
+
+// ======================================================================== C ABI
+extern "C" {
+
+const char *hp_last_error(void) { return hpi::g_err.c_str(); }
+
+void hp_case_opts_default(hp_case_opts *o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->seed = 1;
+    o->field_mode = 0;
+    o->pcg_rtol = 1e-8;
+    o->pcg_max_iter = 0;
+    o->o2_all_species = 0;
+    o->device = 0;
+}
+
+hp_status hp_setup_build(const char *deck, size_t len, const hp_case_opts *opts, hp_setup **out) {
+    if (!deck || !out) return set_error("null argument"), HP_ERR_ARG;
+    hp_setup *s = new hp_setup();
+    hp_case_opts_default(&s->opts);
+    if (opts) s->opts = *opts;
+    try {
+        build_setup(deck, len, build_opts(&s->opts), s->s);
+    } catch (const std::exception &e) {
+        delete s;
+        return from_exception(e);
+    }
+    *out = s;
+    return HP_OK;
+}
+
+void hp_setup_destroy(hp_setup *s) { delete s; }
+
+hp_status hp_setup_get_info(const hp_setup *s, hp_case_info *out) {
+    if (!s || !out) return HP_ERR_ARG;
+    fill_info(s->s, out);
+    return HP_OK;
+}
+
+hp_status hp_setup_get_particles(const hp_setup *su, int isp, int layout, int *cells, float *x, float *y, float *vx,
+                                 float *vy, float *vz, size_t cap, size_t *n_out) {
+    if (!su || isp < 0 || isp >= su->s.nsp) return set_error("bad species"), HP_ERR_ARG;
+    const Setup &s = su->s;
+    size_t n = (size_t)s.sp[isp].np;
+    if (n_out) *n_out = n;
+    if (cap < n) return set_error("output arrays too small"), HP_ERR_ARG;
+    if (layout == 0) {
+        if (cells) std::memcpy(cells, s.p_count[isp].data(), (size_t)s.Csize * sizeof(int));
+        std::memcpy(x, s.p_x[isp].data(), n * 4); std::memcpy(y, s.p_y[isp].data(), n * 4);
+        std::memcpy(vx, s.p_vx[isp].data(), n * 4); std::memcpy(vy, s.p_vy[isp].data(), n * 4);
+        std::memcpy(vz, s.p_vz[isp].data(), n * 4);
+    } else {
+        if (cells) std::memcpy(cells, s.h_cell[isp].data(), n * sizeof(int));
+        std::memcpy(x, s.h_x[isp].data(), n * 4); std::memcpy(y, s.h_y[isp].data(), n * 4);
+        std::memcpy(vx, s.h_vx[isp].data(), n * 4); std::memcpy(vy, s.h_vy[isp].data(), n * 4);
+        std::memcpy(vz, s.h_vz[isp].data(), n * 4);
+    }
+    return HP_OK;
+}
+
+static hp_status table_of(const Setup &s, const std::vector<float> *prob, int what, void *out, size_t bytes,
+                          size_t *needed) {
+    const void *src = nullptr;
+    size_t nb = 0;
+    std::vector<float> tmpf;
+    std::vector<int> tmpi;
+    switch (what) {
+    case 0: src = s.sidx.data(); nb = s.sidx.size() * 4; break;
+    case 1: src = s.a_idx.data(); nb = s.a_idx.size() * 4; break;
+    case 2: src = s.boundary.data(); nb = s.boundary.size() * 4; break;
+    case 3: src = s.face.data(); nb = s.face.size() * 4; break;
+    case 4: src = s.cond_id.data(); nb = s.cond_id.size() * 4; break;
+    case 5: src = s.area.data(); nb = s.area.size() * 4; break;
+    case 6: src = s.back_den1.data(); nb = s.back_den1.size() * 4; break;
+    case 7: src = s.back_vel1.data(); nb = s.back_vel1.size() * 4; break;
+    case 8: src = s.lap_basis.data(); nb = s.lap_basis.size() * 4; break;
+    case 9: src = s.stencil.data(); nb = s.stencil.size() * 4; break;
+    case 10: src = s.vsave.data(); nb = s.vsave.size() * 4; break;
+    case 11: src = s.xsec.data(); nb = s.xsec.size() * 4; break;
+    case 12:
+        for (auto &cf : s.collf) { tmpf.push_back(cf.Flag); tmpf.push_back(cf.mofM); tmpf.push_back(cf.Th_e); tmpf.push_back(cf.RR); }
+        src = tmpf.data(); nb = tmpf.size() * 4; break;
+    case 13: src = s.sigv.data(); nb = s.sigv.size() * 4; break;
+    case 14: src = s.dens_region.data(); nb = s.dens_region.size() * 4; break;
+    case 15:
+        if (prob) { src = prob->data(); nb = prob->size() * 4; }
+        else { tmpf = cell_probabilities(s); src = tmpf.data(); nb = tmpf.size() * 4; }
+        break;
+    case 16: src = s.eps_r.data(); nb = s.eps_r.size() * 4; break;
+    case 17: src = s.back_den2.data(); nb = s.back_den2.size() * 4; break;
+    case 18: src = s.back_vel2.data(); nb = s.back_vel2.size() * 4; break;
+    // reference-layout matrix and set-up vectors (src/load.c:121-246)
+    case 19: src = s.a_val.data(); nb = s.a_val.size() * 4; break;
+    case 20: src = s.ai.data(); nb = s.ai.size() * 4; break;
+    case 21: src = s.aj.data(); nb = s.aj.size() * 4; break;
+    case 22: src = s.matm.data(); nb = s.matm.size() * 4; break;
+    case 23: src = s.cond_b.data(); nb = s.cond_b.size() * 4; break;
+    case 24: src = s.temp_b.data(); nb = s.temp_b.size() * 4; break;
+    case 25: src = s.ta_val.data(); nb = s.ta_val.size() * 4; break;
+    case 26: // species scalars: 16 floats per species
+        for (int i = 0; i < s.nsp; i++) {
+            const SpeciesP &p = s.sp[i];
+            float v[16] = {p.np2c, p.mass, p.q, p.q_density, p.vti, p.qm, p.Escale, p.Ascale, p.Denscale, p.MCCscale,
+                           (float)p.MAXNP, p.Temp, p.InitDens, (float)p.np, (float)s.cap[i], 0.0f};
+            tmpf.insert(tmpf.end(), v, v + 16);
+        }
+        src = tmpf.data(); nb = tmpf.size() * 4; break;
+    case 27: src = s.node_temp.data(); nb = s.node_temp.size() * 4; break;
+    case 28: src = s.dep_factor.data(); nb = s.dep_factor.size() * 4; break;
+    case 29: src = s.fluid_den.data(); nb = s.fluid_den.size() * 4; break;
+    case 30: // scalars: dt, dt_mcc, PCGtol, dx, dy, idx, idy, hdx, hdy, idxy, zlength, mcc_n, nvel, TnRct, n_logx, idlogx
+    {
+        float v[16] = {s.dt, s.dt_mcc, s.PCGtol, s.dx, s.dy, s.idx, s.idy, s.hdx, s.hdy, s.idxy, s.zlength,
+                       (float)s.mcc_n, (float)s.nvel, (float)s.TnRct, (float)s.n_logx, s.idlogx};
+        tmpf.assign(v, v + 16);
+        src = tmpf.data(); nb = tmpf.size() * 4; break;
+    }
+    case 31: // sources: per source mid, dc, ac, 2pif, rphase; then efield flags
+        for (int k = 0; k < s.src_num; k++) {
+            tmpf.push_back((float)s.src_mid[k]); tmpf.push_back(s.src_dc[k]); tmpf.push_back(s.src_ac[k]);
+            tmpf.push_back(s.src_2pifreq[k]); tmpf.push_back(s.src_rphase[k]);
+        }
+        for (int k = 0; k < s.cond_numr; k++) tmpf.push_back((float)s.efield_flag[k]);
+        src = tmpf.data(); nb = tmpf.size() * 4; break;
+    case 32: src = s.unk_node.data(); nb = s.unk_node.size() * 4; break;
+    default: set_error("unknown table id"); return HP_ERR_ARG;
+    }
+    if (needed) *needed = nb;
+    if (!out) return HP_OK;
+    if (bytes < nb) return set_error("output buffer too small"), HP_ERR_ARG;
+    if (nb) std::memcpy(out, src, nb);
+    return HP_OK;
+}
+
+hp_status hp_setup_get_table(const hp_setup *s, int what, void *out, size_t bytes, size_t *needed) {
+    if (!s) return HP_ERR_ARG;
+    return table_of(s->s, nullptr, what, out, bytes, needed);
+}
+
+hp_status hp_get_table(hp_case *c, int what, void *out, size_t bytes, size_t *needed) {
+    if (!c) return HP_ERR_ARG;
+    return table_of(c->s, &c->prob, what, out, bytes, needed);
+}
+
+static hp_status case_from(const Setup &s, const hp_case_opts *opts, hp_case **out) {
+    hp_case_opts o;
+    hp_case_opts_default(&o);
+    if (opts) o = *opts;
+    int chk = check_cuda_device(o.device);
+    if (chk == -1) return set_error("no CUDA device: libhpic has no CPU path"), HP_ERR_NO_CUDA;
+    if (chk == -2) return set_error("device ordinal out of range"), HP_ERR_ARG;
+    CK(cudaSetDevice(o.device));
+    hp_case *c = new hp_case();
+    c->s = s;
+    c->opts = o;
+    c->device = o.device;
+    hp_status st = build_device(c);
+    if (st == HP_OK) {
+        cudaError_t e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) st = cuda_fail(e, "cudaStreamCreate");
+    }
+    if (st == HP_OK) st = op_deposit(c, c->own_stream); // Deposit_Basic before the loop (src/cuda_main.cu:28)
+    if (st == HP_OK) {
+        cudaError_t e = cudaStreamSynchronize(c->own_stream);
+        if (e != cudaSuccess) st = cuda_fail(e, "initial deposit");
+    }
+    if (st != HP_OK) {
+        hp_case_destroy(c);
+        return st;
+    }
+    c->last_stream = c->own_stream;
+    *out = c;
+    return HP_OK;
+}
+
+hp_status hp_case_create(const char *deck, size_t len, const hp_case_opts *opts, hp_case **out) {
+    if (!deck || !out) return set_error("null argument"), HP_ERR_ARG;
+    hp_case_opts o;
+    hp_case_opts_default(&o);
+    if (opts) o = *opts;
+    int chk = check_cuda_device(o.device);
+    if (chk == -1) return set_error("no CUDA device: libhpic has no CPU path"), HP_ERR_NO_CUDA;
+    Setup s;
+    try {
+        build_setup(deck, len, build_opts(&o), s);
+    } catch (const std::exception &e) {
+        return from_exception(e);
+    }
+    if (s.main_gas != GAS_AR) return set_error("MCC for this gas is not built"), HP_ERR_UNSUPPORTED;
+    return case_from(s, &o, out);
+}
+
+hp_status hp_case_create_from_setup(const hp_setup *su, const hp_case_opts *opts, hp_case **out) {
+    if (!su || !out) return HP_ERR_ARG;
+    hp_case_opts o = su->opts;
+    if (opts) o = *opts;
+    return case_from(su->s, &o, out);
+}
+
+hp_status hp_case_destroy(hp_case *c) {
+    if (!c) return HP_OK;
+    cudaSetDevice(c->device);
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    if (c->own_stream) {
+        cudaStreamSynchronize(c->own_stream);
+        cudaStreamDestroy(c->own_stream);
+    }
+    cudaDeviceSynchronize();
+    for (void *p : c->allocs) cudaFree(p);
+    delete c;
+    return HP_OK;
+}
+
+hp_status hp_case_get_info(const hp_case *c, hp_case_info *out) {
+    if (!c || !out) return HP_ERR_ARG;
+    fill_info(c->s, out);
+    out->device_bytes = c->bytes;
+    out->pcg_cluster = c->pcg_cluster;
+    out->pcg_block = c->lc.pcg_block;
+    int64_t t = 0;
+    cudaMemcpy(&t, c->h.tstep, 8, cudaMemcpyDeviceToHost);
+    out->tstep = t;
+    return HP_OK;
+}
+
+hp_status hp_case_status(hp_case *c, uint32_t *status) {
+    if (!c || !status) return HP_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->last_stream));
+    CK(cudaMemcpy(status, c->h.status, 4, cudaMemcpyDeviceToHost));
+    return HP_OK;
+}
+
+hp_status hp_case_set_tstep(hp_case *c, int64_t t) {
+    if (!c) return HP_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->last_stream));
+    CK(cudaMemcpy(c->h.tstep, &t, 8, cudaMemcpyHostToDevice));
+    return HP_OK;
+}
+
+#define OP_BODY(fn)                                                                                                    \
+    if (!c) return HP_ERR_ARG;                                                                                         \
+    if (c->batch) return set_error("case belongs to a batch"), HP_ERR_ARG;                                             \
+    CK(cudaSetDevice(c->device));                                                                                      \
+    hp_status st_ = fn(c, as_stream(stream));                                                                          \
+    c->last_stream = as_stream(stream);                                                                                \
+    return st_;
+
+hp_status hp_Field(hp_case *c, void *stream) { OP_BODY(op_field) }
+hp_status hp_Move(hp_case *c, void *stream) { OP_BODY(op_move) }
+hp_status hp_SortBoundary(hp_case *c, void *stream) { OP_BODY(op_sort) }
+hp_status hp_MCC(hp_case *c, void *stream) { OP_BODY(op_mcc) }
+hp_status hp_Deposit(hp_case *c, void *stream) { OP_BODY(op_deposit) }
+
+hp_status hp_step(hp_case *c, int nsteps, void *stream) {
+    if (!c || nsteps < 0) return HP_ERR_ARG;
+    if (c->batch) return set_error("case belongs to a batch"), HP_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = as_stream(stream);
+    if (!c->graph) {
+        // capture one step on the case's own stream, after the caller's work
+        cudaEvent_t ev;
+        CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        CK(cudaEventRecord(ev, st));
+        CK(cudaStreamWaitEvent(c->own_stream, ev, 0));
+        CK(cudaEventDestroy(ev));
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(c->own_stream, cudaStreamCaptureModeThreadLocal));
+        hp_status s1 = one_step(c, c->own_stream);
+        cudaError_t e = cudaStreamEndCapture(c->own_stream, &g);
+        if (s1 != HP_OK) return s1;
+        if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        e = cudaGraphInstantiate(&c->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+        CK(cudaStreamSynchronize(c->own_stream));
+    }
+    for (int k = 0; k < nsteps; k++) CK(cudaGraphLaunch(c->graph, st));
+    c->last_stream = st;
+    return HP_OK;
+}
+
+hp_status hp_get_particles(hp_case *c, int isp, int *counts, float *x, float *y, float *vx, float *vy, float *vz,
+                           size_t cap, size_t *n_out) {
+    if (!c || isp < 0 || isp >= c->s.nsp) return HP_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->last_stream));
+    const int C = c->s.Csize;
+    const DevSpecies &sp = c->h.sp[isp];
+    std::vector<int> cnt(C);
+    CK(cudaMemcpy(cnt.data(), sp.cnt, (size_t)C * 4, cudaMemcpyDeviceToHost));
+    size_t total = 0;
+    for (int v : cnt) total += (size_t)v;
+    if (n_out) *n_out = total;
+    if (counts) std::memcpy(counts, cnt.data(), (size_t)C * 4);
+    if (!x) return HP_OK;
+    if (cap < total) return set_error("output arrays too small"), HP_ERR_ARG;
+    const size_t ns = (size_t)C * sp.cap;
+    std::vector<float> b(ns);
+    float *outs[5] = {x, y, vx, vy, vz};
+    float *srcs[5] = {sp.x, sp.y, sp.vx, sp.vy, sp.vz};
+    for (int a = 0; a < 5; a++) {
+        if (!outs[a]) continue;
+        CK(cudaMemcpy(b.data(), srcs[a], ns * 4, cudaMemcpyDeviceToHost));
+        size_t q = 0;
+        for (int cell = 0; cell < C; cell++)
+            for (int k = 0; k < cnt[cell]; k++) outs[a][q++] = b[(size_t)cell * sp.cap + k];
+    }
+    return HP_OK;
+}
+
+hp_status hp_get_movers(hp_case *c, int isp, int *counts, float *x, float *y, float *vx, float *vy, float *vz,
+                        int8_t *codes, size_t cap, size_t *n_out) {
+    if (!c || isp < 0 || isp >= c->s.nsp) return HP_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->last_stream));
+    const int C = c->s.Csize;
+    const DevSpecies &sp = c->h.sp[isp];
+    std::vector<int> m(C);
+    CK(cudaMemcpy(m.data(), sp.nmov, (size_t)C * 4, cudaMemcpyDeviceToHost));
+    size_t total = 0;
+    for (int v : m) total += (size_t)v;
+    if (n_out) *n_out = total;
+    if (counts) std::memcpy(counts, m.data(), (size_t)C * 4);
+    if (!x) return HP_OK;
+    if (cap < total) return set_error("output arrays too small"), HP_ERR_ARG;
+    const size_t ns = (size_t)C * sp.cap;
+    std::vector<float> b(ns);
+    float *outs[5] = {x, y, vx, vy, vz};
+    float *srcs[5] = {sp.x, sp.y, sp.vx, sp.vy, sp.vz};
+    for (int a = 0; a < 5; a++) {
+        CK(cudaMemcpy(b.data(), srcs[a], ns * 4, cudaMemcpyDeviceToHost));
+        size_t q = 0;
+        for (int cell = 0; cell < C; cell++)
+            for (int r = 0; r < m[cell]; r++) outs[a][q++] = b[(size_t)cell * sp.cap + sp.cap - 1 - r];
+    }
+    if (codes) {
+        std::vector<int8_t> cb(ns);
+        CK(cudaMemcpy(cb.data(), sp.code, ns, cudaMemcpyDeviceToHost));
+        size_t q = 0;
+        for (int cell = 0; cell < C; cell++)
+            for (int r = 0; r < m[cell]; r++) codes[q++] = cb[(size_t)cell * sp.cap + sp.cap - 1 - r];
+    }
+    return HP_OK;
+}
+
+hp_status hp_set_particles(hp_case *c, int isp, const int *counts, const float *x, const float *y, const float *vx,
+                           const float *vy, const float *vz) {
+    if (!c || isp < 0 || isp >= c->s.nsp || !counts) return HP_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->last_stream));
+    return upload_particles(c, isp, counts, x, y, vx, vy, vz);
+}
+
+static hp_status grid_ptr(hp_case *c, hp_grid_field f, void **p, size_t *nb) {
+    const int G = c->s.Gsize, nsp = c->s.nsp;
+    switch (f) {
+    case HP_GRID_EX: *p = c->h.Ex; *nb = (size_t)G * 4; break;
+    case HP_GRID_EY: *p = c->h.Ey; *nb = (size_t)G * 4; break;
+    case HP_GRID_PHI: *p = c->h.phi; *nb = (size_t)G * 4; break;
+    case HP_GRID_PHI_POIS: *p = c->h.phi_p; *nb = (size_t)G * 4; break;
+    case HP_GRID_DEN: *p = c->h.den; *nb = (size_t)nsp * G * 8; break;
+    case HP_GRID_SOURCE: *p = c->h.source; *nb = (size_t)G * 8; break;
+    case HP_GRID_PCG_X:
+        if (c->opts.field_mode == 0) { *p = c->h.pf_x; *nb = (size_t)G * 4; }
+        else { *p = c->h.x64; *nb = (size_t)G * 8; }
+        break;
+    case HP_GRID_PCG_B: *p = c->h.b64; *nb = (size_t)G * 8; break;
+    case HP_GRID_AVE_DEN: *p = c->h.ave_den; *nb = (size_t)nsp * G * 8; break;
+    case HP_GRID_AVE_PHI: *p = c->h.ave_phi; *nb = (size_t)G * 8; break;
+    case HP_GRID_COND_CHARGE: *p = c->h.cond_charge; *nb = (size_t)nsp * c->s.cond_numr * 4; break;
+    case HP_GRID_MCC_COUNT: *p = c->h.mcc_count; *nb = (size_t)8 * c->s.Csize * 4; break;
+    default: return set_error("unknown grid field"), HP_ERR_ARG;
+    }
+    return HP_OK;
+}
+
+hp_status hp_get_grid(hp_case *c, hp_grid_field f, void *out, size_t bytes) {
+    if (!c || !out) return HP_ERR_ARG;
+    void *p;
+    size_t nb;
+    TRY(grid_ptr(c, f, &p, &nb));
+    if (bytes < nb) return set_error("output buffer too small (" + std::to_string(nb) + " needed)"), HP_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->last_stream));
+    CK(cudaMemcpy(out, p, nb, cudaMemcpyDeviceToHost));
+    return HP_OK;
+}
+
+hp_status hp_set_grid(hp_case *c, hp_grid_field f, const void *in, size_t bytes) {
+    if (!c || !in) return HP_ERR_ARG;
+    void *p;
+    size_t nb;
+    TRY(grid_ptr(c, f, &p, &nb));
+    if (bytes != nb) return set_error("input size mismatch (" + std::to_string(nb) + " expected)"), HP_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->last_stream));
+    CK(cudaMemcpy(p, in, nb, cudaMemcpyHostToDevice));
+    return HP_OK;
+}
+
+hp_status hp_reset_averages(hp_case *c) {
+    if (!c) return HP_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->last_stream));
+    CK(cudaMemset(c->h.ave_den, 0, (size_t)c->s.nsp * c->s.Gsize * 8));
+    CK(cudaMemset(c->h.ave_phi, 0, (size_t)c->s.Gsize * 8));
+    CK(cudaMemset(c->h.ave_count, 0, 8));
+    return HP_OK;
+}
+
+hp_status hp_get_average_count(hp_case *c, int64_t *n) {
+    if (!c || !n) return HP_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->last_stream));
+    CK(cudaMemcpy(n, c->h.ave_count, 8, cudaMemcpyDeviceToHost));
+    return HP_OK;
+}
+
+hp_status hp_last_pcg_iters(hp_case *c, int *inner, int *outer) {
+    if (!c) return HP_ERR_ARG;
+    int v[2];
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->last_stream));
+    CK(cudaMemcpy(v, c->h.pcg_iters, 8, cudaMemcpyDeviceToHost));
+    if (inner) *inner = v[0];
+    if (outer) *outer = v[1];
+    return HP_OK;
+}
+
+} // extern "C"

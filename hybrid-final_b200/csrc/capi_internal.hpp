@@ -1,0 +1,56 @@
+// capi_internal.hpp -- host-side objects behind the opaque C handles.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "../../include/hpic.h"
+#include "dev.cuh"
+#include "kernels.cuh"
+#include "setup.hpp"
+
+struct hp_setup {
+    hp::Setup s;
+    hp_case_opts opts;
+};
+
+struct hp_case {
+    hp::Setup s;
+    hp_case_opts opts;
+    int device = 0;
+    hp::DevCase h{};               // host image of the device descriptor
+    hp::DevCase *d_case = nullptr; // device descriptor
+    int *d_items = nullptr;        // item_start arrays: [0..1] particles, [2..3] cells, [4..5] nodes
+    std::vector<void *> allocs;
+    std::vector<size_t> alloc_bytes;
+    size_t bytes = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t last_stream = nullptr;
+    hp::LaunchCfg lc;
+    int pcg_cluster = 1;           // CTAs of this case's field-solve cluster
+    int *d_list0 = nullptr;        // device {0}: the case's index in its own one-case list
+    cudaGraphExec_t graph = nullptr;
+    hp_batch *batch = nullptr;
+    std::vector<float> prob; // [3*C]
+};
+
+namespace hpi {
+void set_error(const std::string &m);
+hp_status cuda_fail(cudaError_t e, const char *what);
+// Build the per-case prefix arrays and device descriptor array of a batch.
+struct BatchDev {
+    hp::DevCase *d_cases = nullptr;
+    int *d_part = nullptr, *d_cell = nullptr, *d_node = nullptr;
+    int n = 0, n_part = 0, n_cell = 0, n_node = 0;
+    int max_g = 0;
+    // PCG groups for every cluster cap 1,2,4,8,16: lists of case indices per
+    // cluster size, concatenated in d_lists
+    int *d_lists = nullptr;
+    int list_off[5][5] = {}, list_n[5][5] = {};
+    std::vector<hp::PcgGroup> groups(int cluster_max, int block) const;
+};
+hp_status batch_dev_build(hp_case *const *cases, int n, BatchDev &b);
+void batch_dev_free(BatchDev &b);
+hp_status run_step(const BatchDev &b, const hp::LaunchCfg &lc, int gas, cudaStream_t st);
+} // namespace hpi

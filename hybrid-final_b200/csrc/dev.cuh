@@ -1,0 +1,88 @@
+// dev.cuh -- device-side case descriptors shared by the kernels and the host API.
+//
+// HBM layout of one case (all arrays owned by the library):
+//   particles, per species s, structure of arrays over a cell-blocked slot pool:
+//     x[s][c*cap + k], y, vx, vy, vz    float   (x, y = offset inside cell c in [0,1))
+//     code[s][c*cap + k]                int8    (mover direction after Move)
+//     cnt[s][c]                         int32   particles resident in cell c
+//     nmov[s][c]                        int32   movers parked at the top of cell c
+//   cell c = i*ncy + j for the cell whose lower-left node is (i, j); the
+//   reference indexes the same cell by its node i*ngy + j and strides its
+//   slots by Gsize (src/cuda_Particle.cu:44-52).  Slots of one cell are
+//   contiguous here, so a warp that owns a cell reads 32 consecutive floats
+//   per access.
+//   grid: Ex, Ey, phi (float, node layout), den (double, nsp*Gsize),
+//   source (double), PCG vectors in node layout (Gsize entries, non-unknown
+//   nodes held at zero).
+#pragma once
+#include <cstdint>
+
+namespace hp {
+
+constexpr int DMAXSP = 5;
+constexpr int DMAXCOND = 8;
+constexpr int DMAXSRC = 8;
+
+struct DevSpecies {
+    float *x, *y, *vx, *vy, *vz;
+    int8_t *code;
+    int *cnt;
+    int *nmov;
+    int cap;
+    float Ascale, q_density, Escale;
+};
+
+struct DevCase {
+    // geometry
+    int ngx, ngy, ncx, ncy, G, C, nsp, gas, cond_numr, n_unknowns;
+    float dt_dx, dt_dy, dt;
+    float dx, dy, idx, idy, hdx, hdy, idxy;
+    const int *sidx;        // StructureIndex [(ncx+2)*(ncy+2)]
+    const int *boundary, *face, *cond_id; // [G]
+    const float *eps;       // [C] EPS0 * eps_r
+    const float *dep_factor;// [G]
+    DevSpecies sp[DMAXSP];
+    // field
+    float *Ex, *Ey, *phi, *phi_p;   // [G]
+    const float *lap;               // [cond_numr*G]
+    const float *st;                // [5*G] stencil per node: W,S,C,N,E (0 off the unknowns)
+    const float *st_sym;            // [5*G] row-scaled symmetric stencil (refinement mode)
+    const float *row_scale;         // [G] 1/d_i used to symmetrise (refinement mode)
+    float *pf_x, *pf_r, *pf_p, *pf_ap; // [G] FP32 PCG vectors
+    double *x64, *b64;              // [G] FP64 solution and right-hand side
+    double *dots;                   // scratch for cluster reductions [64]
+    double *den;                    // [nsp*G]
+    double *source;                 // [G]
+    double4 *cw[DMAXSP];            // [C] per-cell corner weight sums
+    double *ave_den, *ave_phi;      // [nsp*G], [G]
+    // sources (src/cuda_Field.cu:10-20)
+    int src_num;
+    int src_mid[DMAXSRC];
+    float src_dc[DMAXSRC], src_ac[DMAXSRC], src_2pif[DMAXSRC], src_rphase[DMAXSRC];
+    int efield_flag[DMAXCOND];
+    // collisions
+    const float *xsec;              // [n_logx * xw]
+    int n_logx, xw;
+    float idlogx;
+    float sigv[8];
+    float th[16];                   // CollF.Th_e
+    float mofm[16];
+    const float *prob;              // [3*C]: electron P1, P2; ion P
+    const float *back_vel1;         // [G]
+    const float *vsave;
+    int nvel, mcc_n;
+    uint64_t seed;
+    // bookkeeping
+    int64_t *tstep;                 // device step counter
+    uint32_t *status;
+    float *cond_charge;             // [nsp*cond_numr]
+    unsigned int *mcc_count;        // [16*nsp]
+    int *pcg_iters;                 // [2]: inner, outer of the last solve
+    int64_t *ave_count;
+    // solver controls
+    int field_mode, pcg_max_iter;
+    float pcg_tol2;
+    double pcg_rtol;
+};
+
+} // namespace hp

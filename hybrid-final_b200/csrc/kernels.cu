@@ -1,0 +1,1104 @@
+// kernels.cu -- sm_100a kernels of one PIC/MCC step, batched over cases.
+//
+// Work mapping: the particle kernels give one warp to one (case, species,
+// cell); the slots of a cell are contiguous, so each warp access is one or
+// more full 128-byte lines.  The grid kernels give one thread to one node.
+// The Poisson solve runs one thread-block cluster per case and keeps the
+// whole CG iteration inside one launch, with cluster barriers between the
+// phases and cluster-wide (DSMEM) reductions of the dot products.
+//
+// Floating-point contract: this file is compiled with --fmad=false so that
+// every a*b+c is two roundings, exactly as the CPU checker evaluates it; the
+// elementary functions come from hp_math.h, identical on host and device.
+#include <cooperative_groups.h>
+#include <cstdint>
+
+#include "hp_math.h"
+#include "hp_rng.h"
+#include "kernels.cuh"
+
+namespace cg = cooperative_groups;
+
+namespace hp {
+namespace {
+
+constexpr unsigned FULL = 0xffffffffu;
+constexpr uint32_t ST_OVERFLOW = 0x1u, ST_NONFINITE = 0x2u, ST_NOCONV = 0x4u;
+
+__device__ __forceinline__ int find_case(const int *start, int n, int w) {
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+        int mid = (lo + hi) >> 1;
+        if (start[mid] <= w) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ unsigned lanemask_lt() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// ------------------------------------------------------------------ Move
+// MoveE_Basic (src/cuda_Move.cu:181-270): bilinear gather of the node field,
+// v += Ascale E, x += v dt/dx in cell units, single-cell exit with one wrap.
+// Stayers are compacted in place (order kept); movers are parked at the top
+// of the cell's slots, r-th mover at slot cap-1-r, with a direction code
+// (di+1)*3 + (dj+1) in place of the reference's relative CellID.
+__global__ void __launch_bounds__(256) k_move(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
+                                              int ncases, int items) {
+    const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (warp >= items) return;
+    const int ci = find_case(item_start, ncases, warp);
+    const DevCase &d = cases[ci];
+    const int w = warp - item_start[ci];
+    const int s = w / d.C, c = w - s * d.C;
+    const DevSpecies &sp = d.sp[s];
+    const int n = sp.cnt[c];
+    if (n == 0) {
+        if (lane == 0) sp.nmov[c] = 0;
+        return;
+    }
+    const int cap = sp.cap;
+    if (2 * n > cap) { // the reference's ReArg condition (src/cuda_Sortboundary.cu:63-65)
+        if (lane == 0) {
+            sp.nmov[c] = 0;
+            atomicOr(d.status, ST_OVERFLOW);
+        }
+        return;
+    }
+    const int i = c / d.ncy, j = c - i * d.ncy;
+    const int node = i * d.ngy + j;
+    const float ex_ws = d.Ex[node], ex_wn = d.Ex[node + 1], ex_es = d.Ex[node + d.ngy], ex_en = d.Ex[node + d.ngy + 1];
+    const float ey_ws = d.Ey[node], ey_wn = d.Ey[node + 1], ey_es = d.Ey[node + d.ngy], ey_en = d.Ey[node + d.ngy + 1];
+    const float As = sp.Ascale, dtdx = d.dt_dx, dtdy = d.dt_dy;
+    const size_t base = (size_t)c * cap;
+    const unsigned lt = lanemask_lt();
+    int m = 0;
+    for (int k0 = 0; k0 < n; k0 += 32) {
+        const int k = k0 + lane;
+        const bool act = k < n;
+        float lx = 0.f, ly = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
+        if (act) {
+            lx = sp.x[base + k];
+            ly = sp.y[base + k];
+            vx = sp.vx[base + k];
+            vy = sp.vy[base + k];
+            vz = sp.vz[base + k];
+        }
+        const float del_vx = ex_ws * (1 - lx) * (1 - ly) + ex_wn * (1 - lx) * ly + ex_es * lx * (1 - ly) + ex_en * lx * ly;
+        const float del_vy = ey_ws * (1 - lx) * (1 - ly) + ey_wn * (1 - lx) * ly + ey_es * lx * (1 - ly) + ey_en * lx * ly;
+        const float mvX = vx + del_vx * As;
+        const float mvY = vy + del_vy * As;
+        lx += mvX * dtdx;
+        ly += mvY * dtdy;
+        const bool out = act && (ly >= 1 || ly < 0 || lx >= 1 || lx < 0);
+        int di = 0, dj = 0;
+        if (out) {
+            if (ly >= 1) { dj = 1; ly = (float)((double)ly - 1.0); }
+            else if (ly < 0) { dj = -1; ly = (float)((double)ly + 1.0); }
+            if (lx >= 1) { di = 1; lx = (float)((double)lx - 1.0); }
+            else if (lx < 0) { di = -1; lx = (float)((double)lx + 1.0); }
+        }
+        const unsigned bout = __ballot_sync(FULL, out);
+        const int before = m + __popc(bout & lt);
+        __syncwarp();
+        if (act) {
+            const size_t dst = out ? base + (size_t)(cap - 1 - before) : base + (size_t)(k - before);
+            sp.x[dst] = lx;
+            sp.y[dst] = ly;
+            sp.vx[dst] = mvX;
+            sp.vy[dst] = mvY;
+            sp.vz[dst] = vz;
+            if (out) sp.code[dst] = (int8_t)((di + 1) * 3 + (dj + 1));
+        }
+        m += __popc(bout);
+    }
+    if (lane == 0) {
+        sp.cnt[c] = n - m;
+        sp.nmov[c] = m;
+    }
+}
+
+// ------------------------------------------------------------------ Sort
+// Outcome of one mover, from the ghost-grid code of the cell it moved into
+// (src/cuda_Sortboundary.cu:70-256): 0 plasma; >=100 conductor (absorbed and
+// counted); -1 Dirichlet (absorbed); -2/-6 Neumann x walls, -4/-8 Neumann y
+// walls and -12/-16/-20/-24 Neumann corners (specular reflection back into
+// the domain).  The reference leaves any other code undefined (its
+// uninitialised Sum_CID/Flag_* are used); here such a mover is absorbed.
+struct MoverFate {
+    int fi, fj;
+    bool absorbed, flipx, flipy;
+    int cond; // conductor index or -1
+};
+
+__device__ __forceinline__ MoverFate mover_fate(const DevCase &d, int si, int sj, int di, int dj) {
+    MoverFate f;
+    f.fi = si + di;
+    f.fj = sj + dj;
+    f.absorbed = false;
+    f.flipx = f.flipy = false;
+    f.cond = -1;
+    const int S = d.sidx[(si + 1 + di) * (d.ncy + 2) + (sj + 1 + dj)];
+    switch (S) {
+    case 0: break;
+    case -2: f.fi += 1; f.flipx = true; break;
+    case -6: f.fi -= 1; f.flipx = true; break;
+    case -4: f.fj += 1; f.flipy = true; break;
+    case -8: f.fj -= 1; f.flipy = true; break;
+    case -12: f.fi += 1; f.fj += 1; f.flipx = f.flipy = true; break;
+    case -16: f.fi -= 1; f.fj += 1; f.flipx = f.flipy = true; break;
+    case -20: f.fi += 1; f.fj -= 1; f.flipx = f.flipy = true; break;
+    case -24: f.fi -= 1; f.fj -= 1; f.flipx = f.flipy = true; break;
+    default:
+        f.absorbed = true;
+        if (S >= 100) f.cond = S - 101;
+        break;
+    }
+    if (!f.absorbed && (f.fi < 0 || f.fi >= d.ncx || f.fj < 0 || f.fj >= d.ncy)) f.absorbed = true;
+    return f;
+}
+
+// SortBoundary_Basic re-bins movers by destination with an atomicAdd on the
+// destination count, so the order inside a cell depends on arrival order.
+// Here the warp that owns destination cell (i,j) pulls: it scans the mover
+// lists of the 3x3 source cells in increasing cell index, keeps the movers
+// whose fate lands in (i,j), and appends them after its stayers in list
+// order.  The resulting order is a fixed function of the input.
+__global__ void __launch_bounds__(256) k_sort(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
+                                              int ncases, int items) {
+    const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (warp >= items) return;
+    const int ci = find_case(item_start, ncases, warp);
+    const DevCase &d = cases[ci];
+    const int w = warp - item_start[ci];
+    const int s = w / d.C, c = w - s * d.C;
+    const DevSpecies &sp = d.sp[s];
+    const int cap = sp.cap;
+    const int i = c / d.ncy, j = c - i * d.ncy;
+    const int n0 = sp.cnt[c];
+    const int mown = sp.nmov[c];
+    const int limit = cap - mown;
+    const size_t base = (size_t)c * cap;
+    const unsigned lt = lanemask_lt();
+    // conductor tallies of this cell's own absorbed movers (src/cuda_Sortboundary.cu:254-256)
+    for (int r0 = 0; r0 < mown; r0 += 32) {
+        const int r = r0 + lane;
+        if (r < mown) {
+            const int code = sp.code[base + cap - 1 - r];
+            const MoverFate f = mover_fate(d, i, j, code / 3 - 1, code % 3 - 1);
+            if (f.absorbed && f.cond >= 0 && f.cond < d.cond_numr)
+                atomicAdd(&d.cond_charge[s * d.cond_numr + f.cond], 1.0f);
+        }
+    }
+    int out = n0;
+    bool overflow = false;
+    for (int si = i - 1; si <= i + 1; si++) {
+        if (si < 0 || si >= d.ncx) continue;
+        for (int sj = j - 1; sj <= j + 1; sj++) {
+            if (sj < 0 || sj >= d.ncy) continue;
+            const int src = si * d.ncy + sj;
+            const int m = sp.nmov[src];
+            const size_t sbase = (size_t)src * cap;
+            for (int r0 = 0; r0 < m; r0 += 32) {
+                const int r = r0 + lane;
+                bool match = false;
+                MoverFate f;
+                if (r < m) {
+                    const int code = sp.code[sbase + cap - 1 - r];
+                    f = mover_fate(d, si, sj, code / 3 - 1, code % 3 - 1);
+                    match = !f.absorbed && f.fi == i && f.fj == j;
+                }
+                const unsigned bm = __ballot_sync(FULL, match);
+                if (match) {
+                    const int slot = out + __popc(bm & lt);
+                    if (slot < limit) {
+                        const size_t q = sbase + (size_t)(cap - 1 - r);
+                        const float x = sp.x[q], y = sp.y[q];
+                        const float vx = sp.vx[q], vy = sp.vy[q], vz = sp.vz[q];
+                        const size_t dst = base + (size_t)slot;
+                        sp.x[dst] = f.flipx ? 1 - x : x;
+                        sp.y[dst] = f.flipy ? 1 - y : y;
+                        sp.vx[dst] = f.flipx ? -1 * vx : vx;
+                        sp.vy[dst] = f.flipy ? -1 * vy : vy;
+                        sp.vz[dst] = vz;
+                    } else {
+                        overflow = true;
+                    }
+                }
+                out += __popc(bm);
+            }
+        }
+    }
+    if (__any_sync(FULL, overflow) && lane == 0) atomicOr(d.status, ST_OVERFLOW);
+    if (lane == 0) sp.cnt[c] = out < limit ? out : limit;
+}
+
+// ------------------------------------------------------------------ MCC (Ar)
+// Argon_CrossSection (src/cuda_mccAr.cu:707-776): linear interpolation on the
+// 81-point log10 grid, constant below it, 0.1*exp decay above it.  The
+// reference reads one row past the table when log10(E) equals the last grid
+// point exactly; the index is clamped here.
+__device__ __forceinline__ float xsec_lookup(const DevCase &d, int ch, float engy) {
+    if (engy == 0) return 0.0f;
+    const float lengy = hp_log10f(engy);
+    const float *t = d.xsec;
+    const int W = d.xw;
+    const float xe0 = t[0], xeN = t[(d.n_logx - 1) * W];
+    if (lengy < xe0) return t[2 + ch];
+    if (lengy > xeN) return t[(d.n_logx - 1) * W + 2 + ch] * 0.1f * hp_expf(-1 * (lengy - xeN));
+    const float ee1 = d.idlogx * (lengy - xe0);
+    int ee2 = (int)ee1;
+    if (ee2 > d.n_logx - 2) ee2 = d.n_logx - 2;
+    const float a1 = ee1 - ee2;
+    const float a2 = 1 - a1;
+    return a2 * t[ee2 * W + 2 + ch] + a1 * t[(ee2 + 1) * W + 2 + ch];
+}
+
+// dev_maxwellv (src/cuda_mcc.cu:139-147); cos/sin of 2*pi*Rphi in turns
+__device__ __forceinline__ void maxwellv_dev(float &vx, float &vy, float &vz, float vsaven, float vti, float Rphi,
+                                             float Rthe) {
+    float sn, cs;
+    hp_sincos_turns(Rphi, &sn, &cs);
+    const float costheta = 1 - 2 * Rthe;
+    const float sintheta = sqrtf(1 - costheta * costheta);
+    vx = vti * vsaven * sintheta * cs;
+    vy = vti * vsaven * sintheta * sn;
+    vz = vti * vsaven * costheta;
+}
+
+// dev_anewvel (src/cuda_mcc.cu:148-173): electron scattering with the
+// Surendra angle; massrate term only when e_flag (never set on this path)
+__device__ __forceinline__ void anewvel_dev(float energy, float vel, float &nvx, float &nvy, float &nvz, float rand1,
+                                            float rand2) {
+    float coschi;
+    if (energy < 1e-30f) coschi = 1;
+    else coschi = (float)(((double)energy + 2.0 - 2.0 * (double)hp_powf((float)(energy + 1.0), rand1)) / energy);
+    const float sinchi = (float)sqrt(fabs(1.0 - (double)(coschi * coschi)));
+    float sinphi, cosphi;
+    hp_sincos_turns(rand2, &sinphi, &cosphi);
+    const float r13 = nvx, r23 = nvy, r33 = nvz;
+    float up1, up2, up3;
+    if (r33 == 1.0f) { up1 = 0; up2 = 1; up3 = 0; }
+    else { up1 = 0; up2 = 0; up3 = 1; }
+    float r12 = r23 * up3 - r33 * up2;
+    float r22 = r33 * up1 - r13 * up3;
+    float r32 = r13 * up2 - r23 * up1;
+    const float mag = sqrtf(r12 * r12 + r22 * r22 + r32 * r32);
+    r12 /= mag; r22 /= mag; r32 /= mag;
+    const float r11 = r22 * r33 - r32 * r23;
+    const float r21 = r32 * r13 - r12 * r33;
+    const float r31 = r12 * r23 - r22 * r13;
+    nvx = vel * (r11 * sinchi * cosphi + r12 * sinchi * sinphi + r13 * coschi);
+    nvy = vel * (r21 * sinchi * cosphi + r22 * sinchi * sinphi + r23 * coschi);
+    nvz = vel * (r31 * sinchi * cosphi + r32 * sinchi * sinphi + r33 * coschi);
+}
+
+// dev_newvel_IONSC (src/cuda_mcc.cu:174-201): isotropic ion scattering in the CM frame
+__device__ __forceinline__ void newvel_ionsc_dev(float &vxs, float &vys, float &vzs, float vel, float rand1,
+                                                 float rand2) {
+    const float coschi = sqrtf(rand1);
+    const float sinchi = (float)sqrt(fabs(1.0 - (double)(coschi * coschi)));
+    float sinphi, cosphi;
+    hp_sincos_turns(rand2, &sinphi, &cosphi);
+    const float r13 = vxs / vel, r23 = vys / vel, r33 = vzs / vel;
+    float up1, up2, up3;
+    if (r33 == 1.0f) { up1 = 0; up2 = 1; up3 = 0; }
+    else { up1 = 0; up2 = 0; up3 = 1; }
+    float r12 = r23 * up3 - r33 * up2;
+    float r22 = r33 * up1 - r13 * up3;
+    float r32 = r13 * up2 - r23 * up1;
+    const float mag = sqrtf(r12 * r12 + r22 * r22 + r32 * r32);
+    r12 /= mag; r22 /= mag; r32 /= mag;
+    const float r11 = r22 * r33 - r32 * r23;
+    const float r21 = r32 * r13 - r12 * r33;
+    const float r31 = r12 * r23 - r22 * r13;
+    vxs = vel * coschi * (r11 * sinchi * cosphi + r12 * sinchi * sinphi + r13 * coschi);
+    vys = vel * coschi * (r21 * sinchi * cosphi + r22 * sinchi * sinphi + r23 * coschi);
+    vzs = vel * coschi * (r31 * sinchi * cosphi + r32 * sinchi * sinphi + r33 * coschi);
+}
+
+// MCC_Ar_Basic (src/cuda_mcc.cu:97-106): in every cell the ions collide first
+// (Direct_Argon_ArIon, src/cuda_mccAr.cu:175-232), then the electrons
+// (Direct_Argon_Electron, src/cuda_mccAr.cu:41-174).  Each particle draws from
+// its own Philox stream (slot, cell, step, species) in the same order as the
+// reference draws from its per-cell curand state; where the reference passes
+// two curand_uniform() calls as arguments, the left one is drawn first.
+// Channel tallies go to the cell's own counters (the reference's MCCR).
+__global__ void __launch_bounds__(256) k_mcc_ar(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
+                                                int ncases, int items) {
+    const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (warp >= items) return;
+    const int ci = find_case(item_start, ncases, warp);
+    const DevCase &d = cases[ci];
+    const int c = warp - item_start[ci];
+    const int i = c / d.ncy, j = c - i * d.ncy;
+    const int node = i * d.ngy + j;
+    const float P1 = d.prob[c], P2 = d.prob[d.C + c], Pion = d.prob[2 * d.C + c];
+    const uint32_t step = (uint32_t)(*d.tstep);
+    const float bvel = d.back_vel1[node];
+    const unsigned lt = lanemask_lt();
+    unsigned cnt_ch[7] = {0, 0, 0, 0, 0, 0, 0};
+    // ---- ions
+    const DevSpecies &ion = d.sp[1];
+    const int ni = ion.cnt[c];
+    const size_t ibase = (size_t)c * ion.cap;
+    for (int k0 = 0; k0 < ni; k0 += 32) {
+        const int k = k0 + lane;
+        if (k >= ni) break;
+        hp_stream rs;
+        hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, 1u);
+        float R1 = hp_stream_next(&rs);
+        if (R1 > Pion) continue;
+        const int nn = (int)((d.nvel - 1) * hp_stream_next(&rs));
+        float vnx, vny, vnz;
+        {
+            const float a = hp_stream_next(&rs);
+            const float b = hp_stream_next(&rs);
+            maxwellv_dev(vnx, vny, vnz, d.vsave[nn], bvel, a, b);
+        }
+        const size_t q = ibase + k;
+        const float vx = ion.vx[q], vy = ion.vy[q], vz = ion.vz[q];
+        float VX = vx - vnx, VY = vy - vnz, VZ = vz - vny; // y/z of the neutral swapped as in src/cuda_mccAr.cu:200-202
+        const float dum = VX * VX + VY * VY + VZ * VZ;
+        const float engy = ion.Escale * dum;
+        const float vel = sqrtf(dum);
+        R1 = hp_stream_next(&rs) * d.sigv[2] / vel;
+        float SumSigma = xsec_lookup(d, 5, engy);
+        float ox, oy, oz;
+        if (R1 <= SumSigma) {
+            ox = vnx; oy = vny; oz = vnz;
+            cnt_ch[5]++;
+        } else if (R1 <= (SumSigma += xsec_lookup(d, 6, engy))) {
+            const float a = hp_stream_next(&rs);
+            const float b = hp_stream_next(&rs);
+            newvel_ionsc_dev(VX, VY, VZ, vel, a, b);
+            ox = VX + vnx; oy = VY + vny; oz = VZ + vnz;
+            cnt_ch[6]++;
+        } else {
+            ox = vx; oy = vy; oz = vz;
+        }
+        ion.vx[q] = ox;
+        ion.vy[q] = oy;
+        ion.vz[q] = oz;
+    }
+    // ---- electrons
+    const DevSpecies &el = d.sp[0];
+    const int ne = el.cnt[c];
+    const size_t ebase = (size_t)c * el.cap;
+    int add = 0;
+    bool overflow = false;
+    for (int k0 = 0; k0 < ne; k0 += 32) {
+        const int k = k0 + lane;
+        bool create = false;
+        float nx = 0, ny = 0, nevx = 0, nevy = 0, nevz = 0, nivx = 0, nivy = 0, nivz = 0;
+        if (k < ne) {
+            hp_stream rs;
+            hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, 0u);
+            int colltype = 0;
+            float R1 = 0.f;
+            for (int jj = 0; jj < d.mcc_n; jj++) {
+                R1 = hp_stream_next(&rs);
+                if (R1 < P2) { colltype = 1; break; }
+            }
+            if (colltype) {
+                const int target = (R1 <= P1) ? 0 : 1;
+                const size_t q = ebase + k;
+                float VX = el.vx[q], VY = el.vy[q], VZ = el.vz[q];
+                const float dum = VX * VX + VY * VY + VZ * VZ;
+                float vel = sqrtf(dum);
+                VX /= vel; VY /= vel; VZ /= vel;
+                float engy = el.Escale * dum;
+                float rengy = 0.f, vel2 = 0.f;
+                if (target == 0) {
+                    const float R2 = hp_stream_next(&rs) * d.sigv[0] / vel;
+                    float SumSigma = xsec_lookup(d, 0, engy);
+                    if (R2 <= SumSigma) {
+                        colltype = 0;
+                        cnt_ch[0]++;
+                    } else if (engy > d.th[1] && R2 <= (SumSigma += xsec_lookup(d, 1, engy))) {
+                        colltype = 0;
+                        engy -= d.th[1];
+                        vel = sqrtf(fabsf(engy) / el.Escale);
+                        cnt_ch[1]++;
+                    } else if (engy > d.th[2] && R2 <= (SumSigma += xsec_lookup(d, 2, engy))) {
+                        colltype = 0;
+                        engy -= d.th[2];
+                        vel = sqrtf(fabsf(engy) / el.Escale);
+                        cnt_ch[2]++;
+                    } else if (engy > d.th[3] && R2 <= (SumSigma += xsec_lookup(d, 3, engy))) {
+                        colltype = 2;
+                        engy -= d.th[3];
+                        const float u = hp_stream_next(&rs);
+                        rengy = (float)(10.0 * (double)hp_tanf_q1(u * hp_atanf((float)(engy / 20.0))));
+                        engy -= rengy;
+                        vel = sqrtf(fabsf(rengy) / el.Escale);
+                        vel2 = sqrtf(fabsf(engy) / el.Escale);
+                        cnt_ch[3]++;
+                    }
+                } else {
+                    const float R2 = hp_stream_next(&rs) * d.sigv[1] / vel;
+                    const float SumSigma = xsec_lookup(d, 4, engy);
+                    if (engy > d.th[4] && R2 <= SumSigma) {
+                        colltype = 2;
+                        engy -= d.th[4];
+                        const float u = hp_stream_next(&rs);
+                        rengy = (float)(10.0 * (double)hp_tanf_q1(u * hp_atanf((float)(engy / 20.0))));
+                        engy -= rengy;
+                        vel = sqrtf(fabsf(rengy) / el.Escale);
+                        vel2 = sqrtf(fabsf(engy) / el.Escale);
+                        cnt_ch[4]++;
+                    }
+                }
+                if (colltype == 0) {
+                    const float a = hp_stream_next(&rs);
+                    const float b = hp_stream_next(&rs);
+                    anewvel_dev(engy, vel, VX, VY, VZ, a, b);
+                    el.vx[q] = VX;
+                    el.vy[q] = VY;
+                    el.vz[q] = VZ;
+                } else if (colltype == 2) {
+                    nx = el.x[q];
+                    ny = el.y[q];
+                    nevx = VX; nevy = VY; nevz = VZ;
+                    {
+                        const float a = hp_stream_next(&rs);
+                        const float b = hp_stream_next(&rs);
+                        anewvel_dev(rengy, vel, nevx, nevy, nevz, a, b);
+                    }
+                    nivx = VX; nivy = VY; nivz = VZ;
+                    {
+                        const int nn = (int)((d.nvel - 1) * hp_stream_next(&rs));
+                        const float a = hp_stream_next(&rs);
+                        const float b = hp_stream_next(&rs);
+                        maxwellv_dev(nivx, nivy, nivz, d.vsave[nn], bvel, a, b);
+                    }
+                    {
+                        const float a = hp_stream_next(&rs);
+                        const float b = hp_stream_next(&rs);
+                        anewvel_dev(engy, vel2, VX, VY, VZ, a, b);
+                    }
+                    el.vx[q] = VX;
+                    el.vy[q] = VY;
+                    el.vz[q] = VZ;
+                    create = true;
+                }
+            }
+        }
+        const unsigned bc = __ballot_sync(FULL, create);
+        if (create) {
+            const int off = add + __popc(bc & lt);
+            const int se = ne + off, sn = ni + off;
+            if (se < el.cap && sn < ion.cap) {
+                const size_t qe = ebase + se, qi = ibase + sn;
+                el.x[qe] = nx; el.y[qe] = ny;
+                el.vx[qe] = nevx; el.vy[qe] = nevy; el.vz[qe] = nevz;
+                ion.x[qi] = nx; ion.y[qi] = ny;
+                ion.vx[qi] = nivx; ion.vy[qi] = nivy; ion.vz[qi] = nivz;
+            } else {
+                overflow = true;
+            }
+        }
+        add += __popc(bc);
+    }
+    if (__any_sync(FULL, overflow)) {
+        if (lane == 0) atomicOr(d.status, ST_OVERFLOW);
+        const int room = min(el.cap - ne, ion.cap - ni);
+        add = min(add, room);
+    }
+    if (lane == 0) {
+        el.cnt[c] = ne + add;
+        ion.cnt[c] = ni + add;
+    }
+    // per-cell channel tallies (the reference's MCCR per node)
+#pragma unroll
+    for (int ch = 0; ch < 7; ch++) {
+        const unsigned tot = __reduce_add_sync(FULL, cnt_ch[ch]);
+        if (lane == ch && tot) d.mcc_count[(size_t)c * 8 + ch] += tot;
+    }
+}
+
+// ------------------------------------------------------------------ Deposit
+// DepositAtom (src/cuda_Deposit.cu:289-317): per-cell sums of the four CIC
+// weights; lanes accumulate in FP32, the warp reduces in FP64 and writes one
+// double4 per cell, which the node pass gathers in a fixed order.
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(FULL, v, o);
+    return v;
+}
+
+__global__ void __launch_bounds__(256) k_deposit_cells(const DevCase *__restrict__ cases,
+                                                       const int *__restrict__ item_start, int ncases, int items) {
+    const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (warp >= items) return;
+    const int ci = find_case(item_start, ncases, warp);
+    const DevCase &d = cases[ci];
+    const int w = warp - item_start[ci];
+    const int s = w / d.C, c = w - s * d.C;
+    const DevSpecies &sp = d.sp[s];
+    const int n = sp.cnt[c];
+    const size_t base = (size_t)c * sp.cap;
+    float WS = 0.f, WN = 0.f, ES = 0.f, EN = 0.f;
+    for (int k = lane; k < n; k += 32) {
+        const float lx = sp.x[base + k], ly = sp.y[base + k];
+        WS += (1 - lx) * (1 - ly);
+        WN += (1 - lx) * ly;
+        ES += lx * (1 - ly);
+        EN += lx * ly;
+    }
+    const double a = warp_sum_d(WS), b = warp_sum_d(WN), e = warp_sum_d(ES), f = warp_sum_d(EN);
+    if (lane == 0) d.cw[s][c] = make_double4(a, b, e, f);
+}
+
+// DepositBoundary + SumSource + PCG_Set (src/cuda_Deposit.cu:277-288,35-104,30-34)
+__global__ void __launch_bounds__(256) k_deposit_nodes(const DevCase *__restrict__ cases,
+                                                       const int *__restrict__ item_start, int ncases, int items) {
+    const int t = (int)(blockIdx.x * (unsigned)blockDim.x + threadIdx.x);
+    if (t >= items) return;
+    const int ci = find_case(item_start, ncases, t);
+    const DevCase &d = cases[ci];
+    const int n = t - item_start[ci];
+    const int i = n / d.ngy, j = n - i * d.ngy;
+    const int ncy = d.ncy;
+    double sum = 0.0;
+    for (int s = 0; s < d.nsp; s++) {
+        const double4 *cw = d.cw[s];
+        double den = 0.0;
+        if (i < d.ncx && j < ncy) den += cw[i * ncy + j].x;
+        if (i < d.ncx && j > 0) den += cw[i * ncy + j - 1].y;
+        if (i > 0 && j < ncy) den += cw[(i - 1) * ncy + j].z;
+        if (i > 0 && j > 0) den += cw[(i - 1) * ncy + j - 1].w;
+        den *= (double)d.dep_factor[n];
+        d.den[(size_t)s * d.G + n] = den;
+        sum += den * (double)d.sp[s].q_density;
+    }
+    const double source = sum / 8.8542e-12;
+    d.source[n] = source;
+    d.b64[n] = d.st[2 * d.G + n] != 0.0f ? source : 0.0;
+}
+
+// ------------------------------------------------------------------ Field
+__device__ __forceinline__ float spmv_f(const float *__restrict__ st, int G, int ngy, int n, int i, int j, int ngx,
+                                        const float *__restrict__ v) {
+    // CSR order of the reference rows: W, S, C, N, E (src/load.c:170-240)
+    float out = 0.0f;
+    const float cw = st[n], cs = st[G + n], cc = st[2 * G + n], cn = st[3 * G + n], ce = st[4 * G + n];
+    if (cw != 0.0f) out += cw * v[n - ngy];
+    if (cs != 0.0f) out += cs * v[n - 1];
+    out += cc * v[n];
+    if (cn != 0.0f) out += cn * v[n + 1];
+    if (ce != 0.0f) out += ce * v[n + ngy];
+    (void)i; (void)j; (void)ngx;
+    return out;
+}
+
+__device__ __forceinline__ double spmv_d(const float *__restrict__ st, int G, int ngy, int n,
+                                         const double *__restrict__ v) {
+    double out = 0.0;
+    const float cw = st[n], cs = st[G + n], cc = st[2 * G + n], cn = st[3 * G + n], ce = st[4 * G + n];
+    if (cw != 0.0f) out += (double)cw * v[n - ngy];
+    if (cs != 0.0f) out += (double)cs * v[n - 1];
+    out += (double)cc * v[n];
+    if (cn != 0.0f) out += (double)cn * v[n + 1];
+    if (ce != 0.0f) out += (double)ce * v[n + ngy];
+    return out;
+}
+
+struct ClusterRed {
+    double *warp_part; // [32] in shared memory
+    double *slot;      // [4]  in shared memory, read by the whole cluster
+    double *bcast;     // [4]
+};
+
+// Sum of v over the cluster.  Deterministic for a fixed launch shape: warp
+// shuffle tree, warps in order, CTAs in rank order.  One cluster barrier.
+__device__ double cluster_sum2(cg::cluster_group &cl, double v0, double v1, const ClusterRed &sh, int parity,
+                               double *out1) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    v0 = warp_sum_d(v0);
+    v1 = warp_sum_d(v1);
+    if (lane == 0) {
+        sh.warp_part[wid] = v0;
+        sh.warp_part[16 + wid] = v1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < nw; k++) { a += sh.warp_part[k]; b += sh.warp_part[16 + k]; }
+        sh.slot[2 * parity] = a;
+        sh.slot[2 * parity + 1] = b;
+    }
+    cl.sync();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        const unsigned ncta = cl.num_blocks();
+        for (unsigned r = 0; r < ncta; r++) {
+            const double *rem = cl.map_shared_rank(sh.slot, r);
+            a += rem[2 * parity];
+            b += rem[2 * parity + 1];
+        }
+        sh.bcast[0] = a;
+        sh.bcast[1] = b;
+    }
+    __syncthreads();
+    if (out1) *out1 = sh.bcast[1];
+    const double r = sh.bcast[0];
+    __syncthreads();
+    return r;
+}
+
+// PCG_float (src/cuda_Field.cu:942-1072) as one launch per case cluster.
+// field_mode 0 keeps the reference's rule: FP32 Jacobi-PCG on the assembled
+// operator from the previous solution, until r'z <= PCGtol^2 (absolute).
+// field_mode 1: FP64 residual b - A x on the FP64 solution, an FP32 PCG
+// inner solve of the symmetrised system D^-1 A e = D^-1 r (D = 2 on each
+// Neumann edge the reference doubles), x += e, until ||r|| <= rtol ||b||.
+// Dot products are accumulated in FP64 in both modes.
+__global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, const int *__restrict__ list,
+                                             int nlist) {
+    cg::cluster_group cl = cg::this_cluster();
+    const int CS = (int)cl.num_blocks();
+    const int rank = (int)cl.block_rank();
+    const int li = (int)blockIdx.x / CS;
+    if (li >= nlist) return;
+    const DevCase &d = cases[list[li]];
+    const int G = d.G, ngy = d.ngy, ngx = d.ngx;
+    const int per = (G + CS - 1) / CS;
+    const int lo = rank * per, hi = min(G, lo + per);
+    const int T = blockDim.x;
+    __shared__ double s_warp[32];
+    __shared__ double s_slot[4];
+    __shared__ double s_bcast[4];
+    const ClusterRed sh{s_warp, s_slot, s_bcast};
+    int parity = 0;
+    float *__restrict__ x = d.pf_x;
+    float *__restrict__ r = d.pf_r;
+    float *__restrict__ p = d.pf_p;
+    float *__restrict__ ap = d.pf_ap;
+    const int maxit = d.pcg_max_iter;
+    int iters = 0, outer = 0;
+    bool bad = false;
+    if (d.field_mode == 0) {
+        const float *st = d.st;
+        double part = 0.0;
+        for (int n = lo + threadIdx.x; n < hi; n += T) {
+            const float cc = st[2 * G + n];
+            if (cc == 0.0f) continue;
+            const float ax = spmv_f(st, G, ngy, n, 0, 0, ngx, x);
+            const float rr = -1.0f * ax + (float)d.b64[n];
+            r[n] = rr;
+            const float z = (1 / cc) * rr;
+            p[n] = z;
+            part += (double)(rr * z);
+        }
+        double rz = cluster_sum2(cl, part, 0.0, sh, parity, nullptr);
+        parity ^= 1;
+        int iter = 1;
+        while (rz > (double)d.pcg_tol2 && iter <= maxit) {
+            part = 0.0;
+            for (int n = lo + threadIdx.x; n < hi; n += T) {
+                const float cc = st[2 * G + n];
+                if (cc == 0.0f) continue;
+                const float a = spmv_f(st, G, ngy, n, 0, 0, ngx, p);
+                ap[n] = a;
+                part += (double)(p[n] * a);
+            }
+            const double pap = cluster_sum2(cl, part, 0.0, sh, parity, nullptr);
+            parity ^= 1;
+            const float alpha = (pap != 0.0) ? (float)rz / (float)pap : 0.0f;
+            part = 0.0;
+            for (int n = lo + threadIdx.x; n < hi; n += T) {
+                const float cc = st[2 * G + n];
+                if (cc == 0.0f) continue;
+                x[n] = alpha * p[n] + x[n];
+                const float rr = -alpha * ap[n] + r[n];
+                r[n] = rr;
+                part += (double)(rr * ((1 / cc) * rr));
+            }
+            const double rznew = cluster_sum2(cl, part, 0.0, sh, parity, nullptr);
+            parity ^= 1;
+            if (!(rznew == rznew) || isinf(rznew)) { bad = true; break; }
+            const float beta = (rz != 0.0) ? (float)rznew / (float)rz : 0.0f;
+            for (int n = lo + threadIdx.x; n < hi; n += T) {
+                const float cc = st[2 * G + n];
+                if (cc == 0.0f) continue;
+                p[n] = beta * p[n] + (1 / cc) * r[n];
+            }
+            rz = rznew;
+            iter++;
+            cl.sync();
+        }
+        iters = iter;
+        for (int n = lo + threadIdx.x; n < hi; n += T) d.phi_p[n] = d.st[2 * G + n] != 0.0f ? x[n] : 0.0f;
+        if (iter > maxit && rank == 0 && threadIdx.x == 0) atomicOr(d.status, ST_NOCONV);
+    } else {
+        const float *st = d.st;
+        const float *ss = d.st_sym;
+        double *x64 = d.x64;
+        const double *b64 = d.b64;
+        double bb = 0.0;
+        for (int n = lo + threadIdx.x; n < hi; n += T) bb += b64[n] * b64[n];
+        bb = cluster_sum2(cl, bb, 0.0, sh, parity, nullptr);
+        parity ^= 1;
+        const double target = d.pcg_rtol * d.pcg_rtol * bb;
+        const double inner_rel2 = 1e-10; // inner solve: 1e-5 reduction of the preconditioned residual norm
+        for (outer = 0; outer < 12; outer++) {
+            double rr = 0.0, rz = 0.0;
+            for (int n = lo + threadIdx.x; n < hi; n += T) {
+                const float cc = st[2 * G + n];
+                if (cc == 0.0f) continue;
+                const double r64 = b64[n] - spmv_d(st, G, ngy, n, x64);
+                rr += r64 * r64;
+                const float rs = (float)(r64 * (double)d.row_scale[n]);
+                r[n] = rs;
+                x[n] = 0.0f;
+                const float z = (1 / ss[2 * G + n]) * rs;
+                p[n] = z;
+                rz += (double)(rs * z);
+            }
+            rr = cluster_sum2(cl, rr, rz, sh, parity, &rz);
+            parity ^= 1;
+            if (!(rr == rr) || isinf(rr)) { bad = true; break; }
+            if (rr <= target || bb == 0.0) break;
+            const double rz0 = rz;
+            int iter = 0;
+            while (rz > inner_rel2 * rz0 && iter < maxit) {
+                double part = 0.0;
+                for (int n = lo + threadIdx.x; n < hi; n += T) {
+                    const float cc = ss[2 * G + n];
+                    if (cc == 0.0f) continue;
+                    const float a = spmv_f(ss, G, ngy, n, 0, 0, ngx, p);
+                    ap[n] = a;
+                    part += (double)(p[n] * a);
+                }
+                const double pap = cluster_sum2(cl, part, 0.0, sh, parity, nullptr);
+                parity ^= 1;
+                const float alpha = (pap != 0.0) ? (float)(rz / pap) : 0.0f;
+                part = 0.0;
+                for (int n = lo + threadIdx.x; n < hi; n += T) {
+                    const float cc = ss[2 * G + n];
+                    if (cc == 0.0f) continue;
+                    x[n] = alpha * p[n] + x[n];
+                    const float rs = -alpha * ap[n] + r[n];
+                    r[n] = rs;
+                    part += (double)(rs * ((1 / cc) * rs));
+                }
+                const double rznew = cluster_sum2(cl, part, 0.0, sh, parity, nullptr);
+                parity ^= 1;
+                if (!(rznew == rznew) || isinf(rznew)) { bad = true; break; }
+                const float beta = (rz != 0.0) ? (float)(rznew / rz) : 0.0f;
+                for (int n = lo + threadIdx.x; n < hi; n += T) {
+                    const float cc = ss[2 * G + n];
+                    if (cc == 0.0f) continue;
+                    p[n] = beta * p[n] + (1 / cc) * r[n];
+                }
+                rz = rznew;
+                iter++;
+                cl.sync();
+            }
+            iters += iter;
+            if (bad) break;
+            for (int n = lo + threadIdx.x; n < hi; n += T)
+                if (st[2 * G + n] != 0.0f) x64[n] += (double)x[n];
+            cl.sync();
+        }
+        if (outer >= 12 && rank == 0 && threadIdx.x == 0) atomicOr(d.status, ST_NOCONV);
+        for (int n = lo + threadIdx.x; n < hi; n += T) d.phi_p[n] = st[2 * G + n] != 0.0f ? (float)x64[n] : 0.0f;
+    }
+    if (rank == 0 && threadIdx.x == 0) {
+        d.pcg_iters[0] = iters;
+        d.pcg_iters[1] = outer;
+        if (bad) atomicOr(d.status, ST_NONFINITE);
+    }
+}
+
+// Efield_cuda_Basic potential assembly (src/cuda_Field.cu:9-34):
+// TotPotential = sum_k V_k(t) * phi_Lap,k + phi_Pois, in the reference's
+// order and precision (float accumulation, V_k(t) from a double sine).
+__global__ void __launch_bounds__(256) k_potential(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
+                                                   int ncases, int items) {
+    const int t = (int)(blockIdx.x * (unsigned)blockDim.x + threadIdx.x);
+    if (t >= items) return;
+    const int ci = find_case(item_start, ncases, t);
+    const DevCase &d = cases[ci];
+    const int n = t - item_start[ci];
+    const double time = (double)(*d.tstep) * (double)d.dt;
+    float tot = 0.0f;
+    for (int k = 0; k < d.cond_numr; k++) {
+        float vk = 0.0f;
+        if (d.efield_flag[k]) {
+            for (int q = 0; q < d.src_num; q++)
+                if (d.src_mid[q] == k + 1)
+                    vk = (float)((double)vk + ((double)d.src_dc[q] +
+                                               (double)d.src_ac[q] * sin((double)d.src_2pif[q] * time + (double)d.src_rphase[q])));
+        }
+        tot += vk * d.lap[(size_t)k * d.G + n];
+    }
+    tot += 1 * d.phi_p[n];
+    d.phi[n] = tot;
+}
+
+// Cond_Sigma at one face node (src/cuda_Field.cu:500-558), on the Poisson part
+__device__ float cond_sigma(const DevCase &d, int n, int x, int y, int eT, int eL, int eD, int eX, int pL, int pR,
+                            int pD, int pU) {
+    const int b = d.boundary[n], f = d.face[n];
+    if (!((b == 3 || b == 1) && f != 8)) return 0.0f;
+    float SumSig = 0.0f;
+    for (int s = 0; s < d.nsp; s++) SumSig += (float)d.den[(size_t)s * d.G + n] * d.sp[s].q_density;
+    const float *P = d.phi_p;
+    const float *E = d.eps;
+    const float hdx = d.hdx, hdy = d.hdy, idxy = d.idxy;
+    switch (f) {
+    case 2: return hdy * (E[eT] + E[eL]) * (P[n] - P[pU]) - hdx * SumSig;
+    case 3: return hdy * (E[eD] + E[eX]) * (P[n] - P[pD]) - hdx * SumSig;
+    case 0: return hdx * (E[eL] + E[eX]) * (P[n] - P[pL]) - hdy * SumSig;
+    case 1: return hdx * (E[eT] + E[eD]) * (P[n] - P[pR]) - hdy * SumSig;
+    case 4: return hdy * (E[eT] + E[eL]) * (P[n] - P[pU]) + hdx * (E[eL] + E[eX]) * (P[n] - P[pL]) - idxy * SumSig;
+    case 5: return hdy * (E[eT] + E[eL]) * (P[n] - P[pU]) + hdx * (E[eT] + E[eD]) * (P[n] - P[pR]) - idxy * SumSig;
+    case 6: return hdy * (E[eD] + E[eX]) * (P[n] - P[pD]) + hdx * (E[eL] + E[eX]) * (P[n] - P[pL]) - idxy * SumSig;
+    case 7: return hdy * (E[eD] + E[eX]) * (P[n] - P[pD]) + hdx * (E[eT] + E[eD]) * (P[n] - P[pR]) - idxy * SumSig;
+    default: return 0.0f;
+    }
+    (void)x; (void)y;
+}
+
+// VtoEfield (src/cuda_Field.cu:698-846): E = -grad phi at nodes with the
+// reference's face, corner and boundary special cases.
+__global__ void __launch_bounds__(256) k_efield(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
+                                                int ncases, int items) {
+    const int t = (int)(blockIdx.x * (unsigned)blockDim.x + threadIdx.x);
+    if (t >= items) return;
+    const int ci = find_case(item_start, ncases, t);
+    const DevCase &d = cases[ci];
+    const int n = t - item_start[ci];
+    const int ngx = d.ngx, ngy = d.ngy;
+    const int x = n / ngy, y = n - x * ngy;
+    const int pL = x ? n - ngy : n, pR = (x == ngx - 1) ? n : n + ngy;
+    const int pD = y ? n - 1 : n, pU = (y == ngy - 1) ? n : n + 1;
+    int eT = x * (ngy - 1) + y;
+    int eL = x ? eT - ngy + 1 : eT;
+    int eD = y ? eT - 1 : eT;
+    const int eX = eL + eD - eT;
+    const int xo = (x == ngx - 1) ? ngy - 1 : 0, yo = (y == ngy - 1) ? 1 : 0;
+    eT -= (xo + yo);
+    eL -= yo;
+    eD -= xo;
+    const float *P = d.phi;
+    const float *E = d.eps;
+    const int f = d.face[n], b = d.boundary[n];
+    const float idx = d.idx, idy = d.idy, hdx = d.hdx, hdy = d.hdy, dx = d.dx, dy = d.dy;
+    float Ex, Ey;
+    bool write = true;
+    if (f == 0) { // LEFT
+        if (b == 3 || b == 2 || b == 1) {
+            Ex = -2.0f * cond_sigma(d, n, x, y, eT, eL, eD, eX, pL, pR, pD, pU) / (E[eL] + E[eX]);
+            Ey = 0.0f;
+        } else if (b == 4 || b >= 100) {
+            Ex = idx * (P[pL] - P[n]);
+            Ey = hdy * (P[pD] - P[pU]);
+        } else {
+            Ex = 0.5f * (E[eT] + E[eD]) * (P[pR] - P[n]) * idx;
+            Ex -= (0.5f * dx / dy) * E[eT] * (P[n] - P[pU]) * idy;
+            Ex -= (0.5f * dx / dy) * E[eD] * (P[n] - P[pD]) * idy;
+            Ex /= -0.5f * (E[eL] + E[eX]);
+            Ey = hdy * (P[pD] - P[pU]);
+        }
+    } else if (f == 1) { // RIGHT
+        if (b == 3 || b == 2 || b == 1) {
+            Ex = 2.0f * cond_sigma(d, n, x, y, eT, eL, eD, eX, pL, pR, pD, pU) / (E[eT] + E[eD]);
+            Ey = 0.0f;
+        } else if (b == 4 || b >= 100) {
+            Ex = idx * (P[n] - P[pR]);
+            Ey = hdy * (P[pD] - P[pU]);
+        } else {
+            Ex = 0.5f * (E[eL] + E[eX]) * (P[pL] - P[n]) * idx;
+            Ex -= (0.5f * dx / dy) * E[eL] * (P[n] - P[pU]) * idy;
+            Ex -= (0.5f * dx / dy) * E[eX] * (P[n] - P[pD]) * idy;
+            Ex /= 0.5f * (E[eT] + E[eD]);
+            Ey = hdy * (P[pD] - P[pU]);
+        }
+    } else if (f == 2) { // UP
+        if (b == 3 || b == 2 || b == 1) {
+            Ex = 0.0f;
+            Ey = 2.0f * cond_sigma(d, n, x, y, eT, eL, eD, eX, pL, pR, pD, pU) / (E[eT] + E[eL]);
+        } else if (b == 4 || b >= 100) {
+            Ex = hdx * (P[pL] - P[pR]);
+            Ey = idy * (P[n] - P[pU]);
+        } else {
+            Ex = hdx * (P[pL] - P[pR]);
+            Ey = 0.5f * (E[eD] + E[eX]) * (P[pD] - P[n]) * idy;
+            Ey -= (0.5f * dy / dx) * E[eD] * (P[n] - P[pR]) * idx;
+            Ey -= (0.5f * dy / dx) * E[eX] * (P[n] - P[pL]) * idx;
+            Ey /= 0.5f * (E[eT] + E[eL]);
+        }
+    } else if (f == 3) { // DOWN
+        if (b == 3 || b == 2 || b == 1) {
+            Ex = 0.0f;
+            Ey = -2.0f * cond_sigma(d, n, x, y, eT, eL, eD, eX, pL, pR, pD, pU) / (E[eD] + E[eX]);
+        } else if (b == 4 || b >= 100) {
+            Ex = hdx * (P[pL] - P[pR]);
+            Ey = idy * (P[pD] - P[n]);
+        } else {
+            Ex = hdx * (P[pL] - P[pR]);
+            Ey = 0.5f * (E[eT] + E[eL]) * (P[pU] - P[n]) * idy;
+            Ey -= (0.5f * dy / dx) * E[eT] * (P[n] - P[pR]) * idx;
+            Ey -= (0.5f * dy / dx) * E[eL] * (P[n] - P[pL]) * idx;
+            Ey /= -0.5f * (E[eD] + E[eX]);
+        }
+    } else if (f >= 4 && f <= 7) { // corners
+        const bool solid = (b == 3 || b == 1 || b == 4);
+        if (!solid) {
+            Ex = hdx * (P[pL] - P[pR]);
+            Ey = hdy * (P[pD] - P[pU]);
+        } else if (f == 4) { // UL
+            Ex = idx * (P[pL] - P[n]);
+            Ey = idy * (P[n] - P[pU]);
+        } else if (f == 5) { // UR
+            Ex = idx * (P[n] - P[pR]);
+            Ey = idy * (P[n] - P[pU]);
+        } else if (f == 6) { // LL
+            Ex = idx * (P[pL] - P[n]);
+            Ey = idy * (P[pD] - P[n]);
+        } else { // LR
+            Ex = idx * (P[n] - P[pR]);
+            Ey = idy * (P[pD] - P[n]);
+        }
+    } else if (b == 2) { // Neumann node without a face
+        if (x == 0 || x == ngx - 1) {
+            Ex = 0.0f;
+            Ey = hdy * (P[pD] - P[pU]);
+        } else if (y == 0 || y == ngy - 1) {
+            Ex = hdx * (P[pL] - P[pR]);
+            Ey = 0.0f;
+        } else {
+            write = false; // the reference leaves E unchanged here
+            Ex = Ey = 0.0f;
+        }
+    } else {
+        Ex = hdx * (P[pL] - P[pR]);
+        Ey = hdy * (P[pD] - P[pU]);
+    }
+    if (write) {
+        d.Ex[n] = Ex;
+        d.Ey[n] = Ey;
+    }
+}
+
+__global__ void k_advance(const DevCase *__restrict__ cases, int ncases) {
+    const int t = (int)(blockIdx.x * (unsigned)blockDim.x + threadIdx.x);
+    if (t < ncases) *cases[t].tstep += 1;
+}
+
+__global__ void __launch_bounds__(256) k_accumulate(const DevCase *__restrict__ cases,
+                                                    const int *__restrict__ item_start, int ncases, int items) {
+    const int t = (int)(blockIdx.x * (unsigned)blockDim.x + threadIdx.x);
+    if (t >= items) return;
+    const int ci = find_case(item_start, ncases, t);
+    const DevCase &d = cases[ci];
+    const int n = t - item_start[ci];
+    for (int s = 0; s < d.nsp; s++) d.ave_den[(size_t)s * d.G + n] += d.den[(size_t)s * d.G + n];
+    d.ave_phi[n] += (double)d.phi[n];
+    if (n == 0) *d.ave_count += 1;
+}
+
+inline unsigned blocks_for(long long threads, int per_block) { return (unsigned)((threads + per_block - 1) / per_block); }
+
+} // namespace
+
+cudaError_t launch_move(const DevCase *cases, const int *item_start, int ncases, int items, const LaunchCfg &lc,
+                        cudaStream_t st) {
+    if (items <= 0) return cudaSuccess;
+    const int tpb = 32 * lc.warps_per_block;
+    k_move<<<blocks_for((long long)items * 32, tpb), tpb, 0, st>>>(cases, item_start, ncases, items);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sort(const DevCase *cases, const int *item_start, int ncases, int items, const LaunchCfg &lc,
+                        cudaStream_t st) {
+    if (items <= 0) return cudaSuccess;
+    const int tpb = 32 * lc.warps_per_block;
+    k_sort<<<blocks_for((long long)items * 32, tpb), tpb, 0, st>>>(cases, item_start, ncases, items);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_mcc_ar(const DevCase *cases, const int *item_start, int ncases, int items, const LaunchCfg &lc,
+                          cudaStream_t st) {
+    if (items <= 0) return cudaSuccess;
+    const int tpb = 32 * lc.warps_per_block;
+    k_mcc_ar<<<blocks_for((long long)items * 32, tpb), tpb, 0, st>>>(cases, item_start, ncases, items);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_deposit(const DevCase *cases, const int *cell_items, const int *node_items, int ncases,
+                           int n_cell_items, int n_node_items, const LaunchCfg &lc, cudaStream_t st) {
+    const int tpb = 32 * lc.warps_per_block;
+    if (n_cell_items > 0)
+        k_deposit_cells<<<blocks_for((long long)n_cell_items * 32, tpb), tpb, 0, st>>>(cases, cell_items, ncases,
+                                                                                        n_cell_items);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (n_node_items > 0)
+        k_deposit_nodes<<<blocks_for(n_node_items, 256), 256, 0, st>>>(cases, node_items, ncases, n_node_items);
+    return cudaGetLastError();
+}
+
+int pcg_cluster_for_nodes(int G) {
+    // about 8 nodes per thread at 512 threads per CTA, up to a 16-CTA cluster
+    int cs = 1;
+    while (cs < 16 && (long long)G > (long long)cs * 512 * 8) cs *= 2;
+    return cs;
+}
+
+cudaError_t launch_field(const DevCase *cases, const int *node_items, int ncases, int n_node_items,
+                         const PcgGroup *groups, int ngroups, cudaStream_t st) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_pcg, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        attr_set = true;
+    }
+    for (int g = 0; g < ngroups; g++) {
+        const PcgGroup &pg = groups[g];
+        if (pg.n <= 0) continue;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(pg.n * pg.cluster), 1, 1);
+        cfg.blockDim = dim3((unsigned)pg.block, 1, 1);
+        cfg.dynamicSmemBytes = 0;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = (unsigned)pg.cluster;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        cudaError_t e = cudaLaunchKernelEx(&cfg, k_pcg, cases, pg.list, pg.n);
+        if (e != cudaSuccess) return e;
+    }
+    k_potential<<<blocks_for(n_node_items, 256), 256, 0, st>>>(cases, node_items, ncases, n_node_items);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_efield<<<blocks_for(n_node_items, 256), 256, 0, st>>>(cases, node_items, ncases, n_node_items);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_advance(const DevCase *cases, int ncases, cudaStream_t st) {
+    k_advance<<<blocks_for(ncases, 128), 128, 0, st>>>(cases, ncases);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_accumulate(const DevCase *cases, const int *node_items, int ncases, int n_node_items,
+                              cudaStream_t st) {
+    if (n_node_items <= 0) return cudaSuccess;
+    k_accumulate<<<blocks_for(n_node_items, 256), 256, 0, st>>>(cases, node_items, ncases, n_node_items);
+    return cudaGetLastError();
+}
+
+} // namespace hp

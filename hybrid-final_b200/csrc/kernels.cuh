@@ -1,0 +1,52 @@
+// kernels.cuh -- launch wrappers for the per-step kernels (kernels.cu).
+//
+// Every kernel takes the whole batch: an array of device case descriptors
+// and, for the warp-per-cell kernels, a prefix array item_start[ncases+1]
+// that maps a global work item to its case.  A single case is a batch of one.
+#pragma once
+#include <cuda_runtime.h>
+#include "dev.cuh"
+
+namespace hp {
+
+struct LaunchCfg {
+    int warps_per_block = 8;   // particle kernels: one warp per (species, cell)
+    int pcg_block = 512;       // PCG: threads per CTA
+    int pcg_cluster_max = 16;  // PCG: upper bound on CTAs per case
+};
+
+// Move: gather + push + single-cell exit test (src/cuda_Move.cu:181-270)
+cudaError_t launch_move(const DevCase *cases, const int *item_start, int ncases, int items, const LaunchCfg &lc,
+                        cudaStream_t st);
+// SortBoundary: boundary handling + deterministic re-bin (src/cuda_Sortboundary.cu:41-258)
+cudaError_t launch_sort(const DevCase *cases, const int *item_start, int ncases, int items, const LaunchCfg &lc,
+                        cudaStream_t st);
+// MCC, Ar set (src/cuda_mcc.cu:97-106, src/cuda_mccAr.cu:41-232)
+cudaError_t launch_mcc_ar(const DevCase *cases, const int *item_start, int ncases, int items, const LaunchCfg &lc,
+                          cudaStream_t st);
+// Deposit: per-cell CIC sums, then node gather + boundary scale + rho/eps0 + RHS
+// (src/cuda_Deposit.cu:3-20,30-104,277-325)
+cudaError_t launch_deposit(const DevCase *cases, const int *cell_items, const int *node_items, int ncases,
+                           int n_cell_items, int n_node_items, const LaunchCfg &lc, cudaStream_t st);
+// Field: PCG (src/cuda_Field.cu:133-181,942-1072), potential assembly and
+// E at nodes (src/cuda_Field.cu:2-42,500-558,698-846).  The PCG runs one
+// cluster per case; cases are grouped by cluster size (a launch has one
+// cluster shape), and each case's cluster size depends only on its own grid,
+// so a case gets the same reduction order alone and inside any batch.
+struct PcgGroup {
+    int cluster;      // CTAs per case
+    int block;        // threads per CTA
+    const int *list;  // device array of case indices
+    int n;
+};
+cudaError_t launch_field(const DevCase *cases, const int *node_items, int ncases, int n_node_items,
+                         const PcgGroup *groups, int ngroups, cudaStream_t st);
+// CTAs per case for a grid of G nodes
+int pcg_cluster_for_nodes(int G);
+// tstep += 1 for every case (device-side step counter, graph friendly)
+cudaError_t launch_advance(const DevCase *cases, int ncases, cudaStream_t st);
+// running sums of den and phi (N_ave accumulation, src/cuda_Diagnostic.cu:505-547)
+cudaError_t launch_accumulate(const DevCase *cases, const int *node_items, int ncases, int n_node_items,
+                              cudaStream_t st);
+
+} // namespace hp

@@ -1,0 +1,897 @@
+// setup.cpp -- case builder: deck -> every table the per-step operators read.
+//
+// This is a restatement of the reference's host setup, in the order its
+// main() runs it (src/main.c:45-49): InputRead, Geometry_setting,
+// Source_setting, FieldSolverSetting, GasSetting, followed by the parts of
+// main_cuda's set-up that produce step inputs (Set_NullCollisionTime_cuda,
+// PCG_SOLVER_Laplace with the gas-temperature solve and Calculate_*GasPara).
+// Arithmetic keeps the reference's float/double mix so that tables compare
+// bit-exactly with the reference's own set-up code (tests/test_setup.py).
+#include "setup.hpp"
+#include "json.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <sstream>
+#include <stdexcept>
+
+#include <dlfcn.h>
+
+namespace hp {
+
+namespace {
+
+[[noreturn]] void deck_fail(const std::string &m) { throw std::runtime_error("deck: " + m); }
+[[noreturn]] void unsupported(const std::string &m) { throw std::runtime_error("unsupported: " + m); }
+
+float fnum(const JVal &o, const char *k) { return (float)o.number(k); }
+int inum(const JVal &o, const char *k) { return (int)o.number(k); }
+int ivnzc(const JVal &o, const char *k) { // src/start.c IVnZC
+    int v = (int)o.number(k);
+    if (v == 0) deck_fail(std::string("\"") + k + "\" = 0");
+    return v;
+}
+float fvnzc(const JVal &o, const char *k) { // src/start.c FVnZC
+    float v = (float)o.number(k);
+    if (v == 0.0f) deck_fail(std::string("\"") + k + "\" = 0");
+    return v;
+}
+
+// Park-Miller minimal standard generator with Schrage's decomposition
+// (S. K. Park, K. W. Miller, CACM 31(10), 1988), as the reference's frand()
+// (src/Particle.c:211-226), including its division by 2^31-2.
+struct ParkMiller {
+    long seed;
+    float next() {
+        const long a = 16807, m = 2147483647, q = 127773, r = 2836;
+        long hi = seed / q;
+        long lo = seed - q * hi;
+        seed = a * lo - r * hi;
+        if (seed <= 0) seed = seed + m;
+        return (float)(seed / 2147483646.0);
+    }
+};
+
+// F(v) = -2 v e^{-v^2}/sqrt(pi) + erf(v): the Maxwellian speed CDF
+// (src/Particle.c:227-230), float argument, double evaluation.
+float maxwell_cdf(float v) {
+    // C semantics: exp and erf of the float promoted to double
+    return (float)(-2 * v * exp((double)(-v * v)) / sqrt(MPI) + erf((double)v));
+}
+
+void build_vsave(Setup &s) { // src/Particle.c:183-201
+    const float NVTS = 3.3f;
+    int nvel = (int)(1. / (1 - maxwell_cdf((float)NVTS)));
+    float dv = (float)(sqrt(MPI) / (4.0 * nvel));
+    s.vsave.assign((size_t)nvel, 0.0f);
+    int i = 0;
+    for (int n = 0; n < nvel; n++) {
+        float rr = (float)((1.0 * n) / nvel);
+        while (maxwell_cdf(i * dv) < rr) i++;
+        s.vsave[(size_t)n] = (float)(sqrt(2.0) * i * dv);
+    }
+    s.nvel = nvel;
+}
+
+void maxwellv(const Setup &s, ParkMiller &pm, float vti, float &vx, float &vy, float &vz) { // src/Particle.c:203-209
+    int n = (int)((s.nvel - 1) * pm.next());
+    float aphi = (float)(2 * MPI * pm.next());
+    float costheta = 1 - 2 * pm.next();
+    float sintheta = (float)sqrt((double)(1 - costheta * costheta));
+    vx = (float)(vti * s.vsave[(size_t)n] * sintheta * cos((double)aphi));
+    vy = (float)(vti * s.vsave[(size_t)n] * sintheta * sin((double)aphi));
+    vz = (float)(vti * s.vsave[(size_t)n] * costheta);
+}
+
+// ---------------------------------------------------------------- deck
+void read_geometry(const JVal &root, Setup &s, std::vector<int> &bx0, std::vector<int> &bx1, std::vector<int> &by0,
+                   std::vector<int> &by1, std::vector<int> &bbc, std::vector<float> &btemp) {
+    const JVal &geo = root.object("Geometry");
+    const JVal &spec = geo.object("SystemSpec");
+    s.xlength = fnum(spec, "X_length(m)");
+    s.ylength = fnum(spec, "Y_length(m)");
+    s.zlength = fnum(spec, "Z_length(m)");
+    s.ngx = inum(spec, "NumGridx");
+    s.ngy = inum(spec, "NumGridy");
+    if (s.ngx < 3 || s.ngy < 3) deck_fail("NumGridx/NumGridy must be at least 3");
+    const auto &bcs = geo.array("BoundaryCondition");
+    if (bcs.size() < 4) deck_fail("\"BoundaryCondition\" is too small!(BoundaryNum>=4)"); // src/start.c:53-56
+    for (size_t i = 0; i < bcs.size(); i++) {
+        const JVal &b = bcs[i];
+        int x0 = inum(b, "X0"), x1 = inum(b, "X1"), y0 = inum(b, "Y0"), y1 = inum(b, "Y1"), bc = inum(b, "B.C");
+        if (x0 > x1) deck_fail("BoundaryCondition line " + std::to_string(i + 1) + ": X0 > X1");
+        if (x1 >= s.ngx) deck_fail("BoundaryCondition line " + std::to_string(i + 1) + ": X1 >= NumGridx");
+        if (y0 > y1) deck_fail("BoundaryCondition line " + std::to_string(i + 1) + ": Y0 > Y1");
+        if (y1 >= s.ngy) deck_fail("BoundaryCondition line " + std::to_string(i + 1) + ": Y1 >= NumGridy");
+        if (bc > 4) deck_fail("BoundaryCondition line " + std::to_string(i + 1) + ": B.C > 4");
+        bx0.push_back(x0); bx1.push_back(x1); by0.push_back(y0); by1.push_back(y1); bbc.push_back(bc);
+        btemp.push_back(fnum(b, "Temp"));
+    }
+    const auto &cs = geo.array("ConductorSpec");
+    s.cond_num = (int)cs.size();
+    if (s.cond_num < 2) deck_fail("\"Conductor\" is too small!(CondNum>=2)");
+    if (s.cond_num > 100) deck_fail("\"Conductor\" is too large!(CondNum<100)");
+    std::vector<int> ids; // src/start.c:109-144 M_ID ordering rules
+    for (auto &c : cs) {
+        int id = inum(c, "M_ID");
+        if (id == 0) deck_fail("\"M_ID\" > 0");
+        if (ids.empty()) {
+            if (id != 1) deck_fail("First \"M_ID\" must be 1");
+            ids.push_back(id);
+        } else {
+            if (ids.back() > id) deck_fail("\"M_ID\" must be written in order.");
+            if (std::find(ids.begin(), ids.end(), id) == ids.end()) ids.push_back(id);
+        }
+    }
+    s.cond_numr = (int)ids.size();
+    int external = 0;
+    for (size_t i = 0; i < cs.size(); i++) {
+        const JVal &c = cs[i];
+        int x0 = inum(c, "X0"), x1 = inum(c, "X1"), y0 = inum(c, "Y0"), y1 = inum(c, "Y1");
+        if (x0 > x1 || x1 >= s.ngx || y0 > y1 || y1 >= s.ngy)
+            deck_fail("ConductorSpec line " + std::to_string(i + 1) + ": bad extent");
+        s.cond_mid.push_back(inum(c, "M_ID"));
+        s.cond_x0.push_back(x0); s.cond_x1.push_back(x1); s.cond_y0.push_back(y0); s.cond_y1.push_back(y1);
+        s.cond_temp.push_back(fnum(c, "Temp"));
+        float R = fnum(c, "R(Ohm)"), L = fnum(c, "L(H)"), C = fnum(c, "C(F)");
+        if (!(L < 1e-30f && R < 1e-30f && C >= 1)) external = 1; // src/start.c:173-177
+    }
+    if (external) unsupported("external circuit (R/L/C on a conductor) is outside this library's step path");
+    const auto &src = geo.array("Source");
+    s.src_num = (int)src.size();
+    s.max_freq = 0.0f;
+    for (size_t i = 0; i < src.size(); i++) {
+        const JVal &c = src[i];
+        int mid = inum(c, "M_ID");
+        if (std::find(s.cond_mid.begin(), s.cond_mid.end(), mid) == s.cond_mid.end())
+            deck_fail("Source line " + std::to_string(i + 1) + " is no matching Conductor");
+        float dc = fnum(c, "DC(V)"), pw = fnum(c, "Power(W)"), ac = fnum(c, "AC(V)"), fr = fnum(c, "Freq(1/s)");
+        float ph = fnum(c, "Phase(deg)");
+        if (dc == 0 && pw == 0 && ac == 0) deck_fail("Source line " + std::to_string(i + 1) + " is error");
+        if (pw != 0) unsupported("power-driven sources are outside this library's step path");
+        s.src_mid.push_back(mid);
+        s.src_dc.push_back(dc);
+        s.src_ac.push_back(ac);
+        s.src_freq.push_back(fr);
+        s.src_2pifreq.push_back((float)(2 * MPI * fr));
+        s.src_rphase.push_back((float)(MPI / 180 * ph));
+        if (fr != 0) s.max_freq = std::max(s.max_freq, fr);
+    }
+    const auto &diel = geo.array("DielectricSpec");
+    if (!diel.empty()) unsupported("dielectric blocks (DielectricSpec) are outside this library's step path");
+}
+
+void read_species_block(const JVal &cs, const char *key, SpeciesP &p, float mass, float q) {
+    const JVal &o = cs.object(key);
+    p.name = key;
+    p.S_ID = inum(o, "S_ID");
+    p.InitDens = fnum(o, "Density");
+    p.Temp = fnum(o, "Temp(eV)");
+    p.np2c = fnum(o, "np2c");
+    p.Ratio = inum(o, "Ratio");
+    p.MAXNP = inum(o, "Max_np");
+    p.mass = mass;
+    p.q = q;
+}
+
+void read_load(const JVal &o, int &type, float &x0, float &x1, float &y0, float &y1, bool charged) {
+    type = inum(o, "Loadtype");
+    const JVal &lp = o.object("LoadPosition(m)");
+    x0 = fnum(lp, "X0"); x1 = fnum(lp, "X1"); y0 = fnum(lp, "Y0"); y1 = fnum(lp, "Y1");
+    if (type == 4) { // SMARTLOAD: accepted by the reader, rejected by the loader
+    } else if (type == 0) {
+        if (x0 >= x1 || y0 >= y1) deck_fail("Load position error (UNIFORM)");
+    } else if (type == 1 || type == 2) {
+        if (x0 * x1 * y0 * y1 < 0) deck_fail("Load position error");
+    } else if (type == 3 && charged) {
+    } else {
+        deck_fail("\"Loadtype\" is error");
+    }
+}
+
+void read_fluid(const JVal &ns, const char *key, FluidP &f, float mass) {
+    const JVal &o = ns.object(key);
+    f.name = key;
+    f.InitDens = fnum(o, "Density");
+    f.Temp = fnum(o, "Temp(eV)");
+    f.mass = mass;
+    f.Vel = (float)sqrt(f.Temp * 1.38e-23 / f.mass);
+    f.Gamma1 = fnum(o, "Quenching");
+}
+
+void read_gas(const JVal &root, Setup &s) {
+    const JVal &g = root.object("GasSpecies");
+    s.main_gas = inum(g, "Type(0:Ar,1:O2,2:Ar/O2)");
+    switch (s.main_gas) {
+    case GAS_AR: s.nsp = 2; s.nfsp = 1; s.nBG = 1; break;
+    case GAS_O2: s.nsp = 4; s.nfsp = 4; s.nBG = 1; break;
+    case GAS_ARO2: s.nsp = 5; s.nfsp = 5; s.nBG = 2; break;
+    default: deck_fail("\"Type\" is error in GasSpecies.");
+    }
+    s.total_pressure = fnum(g, "TotalPres(Torr)");
+    const JVal &bgo = g.object("Background");
+    const JVal &ns = g.object("NeutralSpecies");
+    const JVal &cs = g.object("ChargeSpecies");
+    int ftype; float fx0, fx1, fy0, fy1;
+    const float me = (float)(5.485799486e-4 * AMU);
+    const float mAr = (float)(39.950 * AMU), mArIon = (float)(39.9500 * AMU);
+    const float mO2 = (float)(32.0000 * AMU), mO = (float)(16.0000 * AMU);
+    const float qe = (float)(-1.0 * CQ), qi = (float)(1.0 * CQ);
+    if (s.main_gas == GAS_AR) {
+        BackGP &b = s.bg[0];
+        b.name = "Argon"; b.Ratio = 1.0f; b.Pres = s.total_pressure;
+        b.Temp = fnum(bgo.object("Argon"), "Temp(eV)");
+        b.mass = mAr;
+        b.InitDens = (float)(NperTORR * b.Pres / (b.Temp + DBLMIN));
+        read_load(ns, ftype, fx0, fx1, fy0, fy1, false);
+        read_fluid(ns, "Ar*", s.fg[0], mAr);
+        read_load(cs, s.sp[0].loadtype, s.sp[0].x_center, s.sp[0].x_fall, s.sp[0].y_center, s.sp[0].y_fall, true);
+        read_species_block(cs, "Electron", s.sp[0], me, qe);
+        read_species_block(cs, "Ar+", s.sp[1], mArIon, qi);
+    } else if (s.main_gas == GAS_O2) {
+        BackGP &b = s.bg[0];
+        b.name = "Oxygen"; b.Ratio = 1.0f; b.Pres = s.total_pressure;
+        b.Temp = fnum(bgo.object("Oxygen"), "Temp(eV)");
+        b.mass = mO2;
+        b.InitDens = (float)(NperTORR * b.Pres / (b.Temp + DBLMIN));
+        read_load(ns, ftype, fx0, fx1, fy0, fy1, false);
+        read_fluid(ns, "O2A", s.fg[0], mO2);
+        read_fluid(ns, "O2B", s.fg[1], mO2);
+        read_fluid(ns, "OP", s.fg[2], mO);
+        read_fluid(ns, "OD", s.fg[3], mO);
+        read_load(cs, s.sp[0].loadtype, s.sp[0].x_center, s.sp[0].x_fall, s.sp[0].y_center, s.sp[0].y_fall, true);
+        read_species_block(cs, "Electron", s.sp[0], me, qe);
+        read_species_block(cs, "O2+", s.sp[1], mO2, qi);
+        read_species_block(cs, "O+", s.sp[2], mO, qi);
+        read_species_block(cs, "O-", s.sp[3], mO, qe);
+    } else {
+        float f1 = fnum(bgo.object("Argon"), "Ratio");
+        float f2 = fnum(bgo.object("Oxygen"), "Ratio");
+        f2 = f2 / (f1 + f2);
+        BackGP &a = s.bg[0], &o = s.bg[1];
+        a.name = "Argon"; a.Temp = fnum(bgo.object("Argon"), "Temp(eV)"); a.mass = mAr;
+        o.name = "Oxygen"; o.Temp = fnum(bgo.object("Oxygen"), "Temp(eV)"); o.mass = mO2;
+        a.Ratio = (float)(1.0 - f2);
+        a.Pres = s.total_pressure * a.Ratio;
+        o.Ratio = f2;
+        o.Pres = s.total_pressure * o.Ratio;
+        a.InitDens = (float)(NperTORR * a.Pres / (a.Temp + DBLMIN));
+        o.InitDens = (float)(NperTORR * o.Pres / (o.Temp + DBLMIN));
+        read_load(ns, ftype, fx0, fx1, fy0, fy1, false);
+        read_fluid(ns, "Ar*", s.fg[0], mAr);
+        read_fluid(ns, "O2A", s.fg[1], mO2);
+        read_fluid(ns, "O2B", s.fg[2], mO2);
+        read_fluid(ns, "OP", s.fg[3], mO);
+        read_fluid(ns, "OD", s.fg[4], mO);
+        read_load(cs, s.sp[0].loadtype, s.sp[0].x_center, s.sp[0].x_fall, s.sp[0].y_center, s.sp[0].y_fall, true);
+        read_species_block(cs, "Electron", s.sp[0], me, qe);
+        read_species_block(cs, "Ar+", s.sp[1], mArIon, qi);
+        read_species_block(cs, "O2+", s.sp[2], mO2, qi);
+        read_species_block(cs, "O+", s.sp[3], mO, qi);
+        read_species_block(cs, "O-", s.sp[4], mO, qe);
+    }
+}
+
+void read_method(const JVal &root, Setup &s) { // src/start.c:732-747
+    const JVal &m = root.object("SimulationMethod");
+    s.DT_PIC = ivnzc(m, "TimeStep_PIC");
+    ivnzc(m, "TimeStep_Conti");
+    s.PCGtol = fvnzc(m, "PCGMarginOfError");
+    s.PCGtol2 = s.PCGtol * s.PCGtol;
+    ivnzc(m, "HistoryMax");
+    ivnzc(m, "HistoryDivide");
+    s.N_ave = ivnzc(m, "AverageIter");
+    s.N_smt = inum(m, "DensitySmoothing");
+    if (s.N_smt > 0) unsupported("density smoothing (DensitySmoothing > 0)");
+    ivnzc(m, "ParticleLimit");
+    if (inum(m, "ConstB_Flag")) unsupported("constant magnetic field (ConstB_Flag)");
+}
+
+// ---------------------------------------------------------------- tables
+// Tables live in data/ beside lib/ of the package; HPIC_DATA_DIR overrides.
+std::string data_path(const char *file) {
+    const char *env = getenv("HPIC_DATA_DIR");
+    std::string dir;
+    if (env && *env) {
+        dir = env;
+    } else {
+        Dl_info info;
+        if (dladdr((void *)&data_path, &info) && info.dli_fname) {
+            std::string so = info.dli_fname;
+            size_t cut = so.find_last_of('/');
+            std::string libdir = cut == std::string::npos ? std::string(".") : so.substr(0, cut);
+            dir = libdir + "/../data";
+        }
+    }
+    if (!dir.empty() && dir.back() != '/') dir += '/';
+    return dir + file;
+}
+
+void load_xsec(Setup &s) {
+    const char *file = s.main_gas == GAS_AR ? "xsec_ar.txt" : s.main_gas == GAS_O2 ? "xsec_o2.txt" : "xsec_aro2.txt";
+    std::ifstream in(data_path(file));
+    if (!in) throw std::runtime_error(std::string("cannot open cross-section table ") + data_path(file));
+    std::vector<std::string> lines;
+    std::string line;
+    while (std::getline(in, line))
+        if (!line.empty() && line[0] != '#') lines.push_back(line);
+    if (lines.size() < 3) throw std::runtime_error("bad cross-section table");
+    int nlog, ncx, tn;
+    float idl;
+    {
+        std::istringstream h(lines[0]);
+        h >> nlog >> ncx >> tn >> idl;
+    }
+    if (tn != s.TnRct) throw std::runtime_error("cross-section table reaction count mismatch");
+    std::vector<float> th(tn), rr(tn);
+    {
+        std::istringstream a(lines[1]);
+        for (int i = 0; i < tn; i++) a >> th[i];
+        std::istringstream b(lines[2]);
+        for (int i = 0; i < tn; i++) b >> rr[i];
+    }
+    s.n_logx = nlog;
+    s.n_cx = ncx;
+    s.idlogx = idl;
+    s.xsec.assign((size_t)nlog * (2 + ncx), 0.0f);
+    for (int r = 0; r < nlog; r++) {
+        std::istringstream rs(lines[3 + r]);
+        for (int k = 0; k < 2 + ncx; k++) {
+            float v;
+            rs >> v;
+            // the reference multiplies each resampled channel by its deck flag
+            // (src/PhysicsData.c, e.g. :1615); flags are 0 or 1 in practice
+            s.xsec[(size_t)r * (2 + ncx) + k] = k < 2 ? v : s.collf[(size_t)(k - 2)].Flag * v;
+        }
+    }
+    for (int i = 0; i < tn; i++) {
+        s.collf[(size_t)i].Th_e = th[i];
+        s.collf[(size_t)i].RR = s.collf[(size_t)i].Flag != 0.0f && rr[i] != 0.0f ? s.collf[(size_t)i].Flag * rr[i] : 0.0f;
+    }
+}
+
+void read_collisions(const JVal &root, Setup &s) { // src/start.c:1003-1057
+    const JVal &co = root.object("Collision_On_Off");
+    if (s.main_gas == GAS_AR) {
+        s.TnRct = 10;
+        s.collf.assign(10, CollFP());
+        const JVal &a = co.object("ArgonCase");
+        const char *keys[10] = {"0.e+Ar>e+Ar", "1.e+Ar>e+Ar*", "2.e+Ar>e+Ar*m", "3.e+Ar>2e+Ar^", "4.e+Ar*m>2e+Ar^",
+                                "5.Ar+Ar^>Ar^+Ar", "6.Ar+Ar^>Ar+Ar^", "7.e+Ar*m>e+Ar", "8.Ar*m+Ar>e+Ar^+Ar",
+                                "9.Ar+Ar*m>Ar+Ar"};
+        for (int i = 0; i < 10; i++) s.collf[(size_t)i].Flag = fnum(a, keys[i]);
+        float me = s.sp[0].mass, mi = s.sp[1].mass, mb = s.bg[0].mass, mf = s.fg[0].mass;
+        float mofm[10] = {me / mb, me / mb, me / mb, me / mb, me / mf, mb / mi, mb / mi, me / mf, mf / mb, mb / mf};
+        for (int i = 0; i < 10; i++) s.collf[(size_t)i].mofM = mofm[i];
+    } else {
+        unsupported(s.main_gas == GAS_O2 ? "O2 reaction set" : "Ar/O2 reaction set");
+    }
+    for (auto &c : s.collf)
+        if (c.Flag < 0) c.Flag = 0.0f;
+    load_xsec(s);
+}
+
+// ---------------------------------------------------------------- geometry
+
+void geometry(Setup &s, const std::vector<int> &bx0, const std::vector<int> &bx1, const std::vector<int> &by0,
+              const std::vector<int> &by1, const std::vector<int> &bbc, const std::vector<float> &btemp) {
+    const int ngx = s.ngx, ngy = s.ngy;
+    s.Gsize = ngx * ngy;
+    s.ncx = ngx - 1;
+    s.ncy = ngy - 1;
+    s.Csize = s.ncx * s.ncy;
+    const int ncx = s.ncx, ncy = s.ncy, G = s.Gsize;
+    s.dx = s.xlength / ncx;
+    s.dy = s.ylength / ncy;
+    s.idx = 1 / s.dx;
+    s.idy = 1 / s.dy;
+    s.idxy = (float)(1.5 / (s.dx + s.dy));
+    s.hdx = (float)(0.5 / s.dx);
+    s.hdy = (float)(0.5 / s.dy);
+    s.boundary.assign(G, 0);
+    s.cond_id.assign(G, 0);
+    s.temp.assign(G, 0.0f);
+    s.face.assign(G, F_NONE);
+    s.area.assign(G, (float)(s.dy * s.zlength));
+    s.dens_region.assign(G, 0);
+    s.plasma_region.assign(s.Csize, 1);
+    s.eps_r.assign(s.Csize, 1.0f);
+    // boundary lines (src/start.c:1491-1506)
+    for (int j = 0; j < ngy; j++)
+        for (int i = 0; i < ngx; i++) {
+            int ID = i * ngy + j;
+            for (size_t k = 0; k < bx0.size(); k++) {
+                if (i >= bx0[k] && i <= bx1[k] && j >= by0[k] && j <= by1[k]) {
+                    if (bbc[k] == BC_DIRICHLET) {
+                        s.boundary[ID] = BC_DIRICHLET;
+                        s.temp[ID] = btemp[k];
+                    } else if (s.boundary[ID] != BC_DIRICHLET && bbc[k] == BC_NEUMANN) {
+                        s.boundary[ID] = BC_NEUMANN;
+                        s.temp[ID] = btemp[k];
+                    }
+                }
+            }
+        }
+    // conductors (src/start.c:1521-1537)
+    for (int k = 0; k < s.cond_num; k++)
+        for (int i = s.cond_x0[k]; i <= s.cond_x1[k]; i++)
+            for (int j = s.cond_y0[k]; j <= s.cond_y1[k]; j++) {
+                int ID = i * ngy + j;
+                s.cond_id[ID] = s.cond_mid[k];
+                if (s.boundary[ID] == 0 || s.boundary[ID] == BC_DIELECTRIC) {
+                    s.boundary[ID] = BC_CONDUCTOR;
+                    s.temp[ID] = s.cond_temp[k];
+                }
+                if (i < s.cond_x1[k] && j < s.cond_y1[k]) {
+                    int CID = i * ncy + j;
+                    s.plasma_region[CID] = 0;
+                    s.eps_r[CID] = 0.0f;
+                }
+            }
+    for (int i = 0; i < ncx; i++) // src/start.c:1539-1550
+        for (int j = 0; j < ncy; j++)
+            if (s.plasma_region[i * ncy + j] == 1) {
+                int ID = i * ngy + j;
+                s.dens_region[ID] = s.dens_region[ID + 1] = s.dens_region[ID + ngy] = s.dens_region[ID + ngy + 1] = 1;
+            }
+    // interior faces (src/start.c:1553-1626); eps_r is read into ints there
+    for (int i = 1; i < ngx - 1; i++)
+        for (int j = 1; j < ngy - 1; j++) {
+            int ID = i * ngy + j, CID = i * ncy + j;
+            int P1 = (int)s.eps_r[CID], P2 = (int)s.eps_r[CID - ncy], P3 = (int)s.eps_r[CID - 1],
+                P4 = (int)s.eps_r[CID - ncy - 1];
+            if (s.boundary[ID] != BC_CONDUCTOR) continue; // dielectric decks are rejected above
+            int f = -1;
+            if ((P2 == 1 && P1 == 1 && P4 == 1) || (P2 != 0 && P1 != 0 && P4 != 0 && P3 == 0)) f = F_UL;
+            else if ((P2 == 1 && P1 == 1 && P3 == 1) || (P2 != 0 && P1 != 0 && P3 != 0 && P4 == 0)) f = F_UR;
+            else if ((P2 == 1 && P1 == 1 && P4 != 1 && P3 != 1) || (P2 != 0 && P1 != 0 && P4 == 0 && P3 == 0)) f = F_UP;
+            else if ((P4 == 1 && P3 == 1 && P2 == 1) || (P2 != 0 && P4 != 0 && P3 != 0 && P1 == 0)) f = F_LL;
+            else if ((P4 == 1 && P3 == 1 && P1 == 1) || (P1 != 0 && P4 != 0 && P3 != 0 && P2 == 0)) f = F_LR;
+            else if ((P4 == 1 && P3 == 1 && P1 != 1 && P2 != 1) || (P4 != 0 && P3 != 0 && P1 == 0 && P2 == 0)) f = F_DOWN;
+            else if ((P4 == 1 && P2 == 1 && P1 != 1 && P3 != 1) || (P4 != 0 && P2 != 0 && P1 == 0 && P3 == 0)) f = F_LEFT;
+            else if ((P4 != 1 && P2 != 1 && P1 == 1 && P3 == 1) || (P4 == 0 && P2 == 0 && P1 != 0 && P3 != 0)) f = F_RIGHT;
+            if (f >= 0) {
+                s.face[ID] = f;
+                s.area[ID] = (f == F_UP || f == F_DOWN) ? s.dx * s.zlength
+                             : (f == F_LEFT || f == F_RIGHT) ? s.dy * s.zlength
+                                                             : (float)(0.5 * (s.dx + s.dy) * s.zlength);
+            }
+        }
+    auto set = [&](int ID, int f, bool xarea) {
+        s.face[ID] = f;
+        s.area[ID] = xarea ? s.dx * s.zlength : s.dy * s.zlength;
+    };
+    // the last domain corner (src/start.c:1770-1774) reads vec_G[Gsize], one
+    // past the array; that read is taken as CondID 0 here (what the
+    // reference's heap held in the golden runs)
+    auto cid = [&](int ID) { return ID >= 0 && ID < G ? s.cond_id[ID] : 0; };
+    // left/right domain edges (src/start.c:1628-1691)
+    for (int j = 1; j < ncy; j++) {
+        int ID = j;
+        if (s.boundary[ID] == BC_DIRICHLET) {
+            set(ID, F_RIGHT, false);
+            if (cid(ID + 1) == 0 && cid(ID - 1) != 0 && cid(ngy + ID) != 0) set(ID, F_UP, true);
+            else if (cid(ID + 1) != 0 && cid(ID - 1) == 0 && cid(ngy + ID) != 0) set(ID, F_DOWN, true);
+            else if (cid(ID + 1) != 0 && cid(ID - 1) != 0 && cid(ngy + ID) != 0) set(ID, F_NONE, false);
+            else if (cid(ID + 1) == 0 && cid(ID - 1) == 0 && cid(ngy + ID) != 0) set(ID, F_NONE, false);
+        } else if (s.boundary[ID] == BC_NEUMANN) {
+            set(ID, F_NONE, false);
+            if (cid(ID + 1) == 0 && cid(ID - 1) != 0 && cid(ngy + ID) != 0) set(ID, F_UP, true);
+            else if (cid(ID + 1) != 0 && cid(ID - 1) == 0 && cid(ngy + ID) != 0) set(ID, F_DOWN, true);
+            else if (cid(ID + 1) != 0 && cid(ID - 1) != 0 && cid(ngy + ID) == 0) set(ID, F_RIGHT, false);
+        }
+        ID = ncx * ngy + j;
+        if (s.boundary[ID] == BC_DIRICHLET) {
+            set(ID, F_LEFT, false);
+            if (cid(ID + 1) == 0 && cid(ID - 1) != 0 && cid(ID - ngy) != 0) set(ID, F_UP, true);
+            else if (cid(ID + 1) != 0 && cid(ID - 1) == 0 && cid(ID - ngy) != 0) set(ID, F_DOWN, true);
+            else if (cid(ID + 1) != 0 && cid(ID - 1) != 0 && cid(ID - ngy) != 0) set(ID, F_NONE, false);
+            else if (cid(ID + 1) == 0 && cid(ID - 1) == 0 && cid(ID - ngy) != 0) set(ID, F_NONE, false);
+        } else if (s.boundary[ID] == BC_NEUMANN) {
+            set(ID, F_NONE, false);
+            if (cid(ID + 1) == 0 && cid(ID - 1) != 0 && cid(ID - ngy) != 0) set(ID, F_UP, true);
+            else if (cid(ID + 1) != 0 && cid(ID - 1) == 0 && cid(ID - ngy) != 0) set(ID, F_DOWN, true);
+            else if (cid(ID + 1) != 0 && cid(ID - 1) != 0 && cid(ID - ngy) == 0) set(ID, F_LEFT, false);
+        }
+    }
+    // bottom/top domain edges (src/start.c:1692-1754)
+    for (int i = 1; i < ncx; i++) {
+        int ID = i * ngy;
+        if (s.boundary[ID] == BC_DIRICHLET) {
+            set(ID, F_UP, true);
+            if (cid(ID + ngy) == 0 && cid(ID - ngy) != 0 && cid(ID + 1) != 0) set(ID, F_RIGHT, false);
+            else if (cid(ID + ngy) != 0 && cid(ID - ngy) == 0 && cid(ID + 1) != 0) set(ID, F_LEFT, false);
+            else if (cid(ID + ngy) != 0 && cid(ID - ngy) != 0 && cid(ID + 1) != 0) set(ID, F_NONE, false);
+            else if (cid(ID + ngy) == 0 && cid(ID - ngy) == 0 && cid(ID + 1) != 0) set(ID, F_NONE, false);
+        } else if (s.boundary[ID] == BC_NEUMANN) {
+            set(ID, F_NONE, false);
+            if (cid(ID + ngy) == 0 && cid(ID - ngy) != 0 && cid(ID + 1) != 0) set(ID, F_RIGHT, false);
+            else if (cid(ID + ngy) != 0 && cid(ID - ngy) == 0 && cid(ID + 1) != 0) set(ID, F_LEFT, false);
+            else if (cid(ID + ngy) != 0 && cid(ID - ngy) != 0 && cid(ID + 1) == 0) set(ID, F_UP, true);
+        }
+        ID = i * ngy + ncy;
+        if (s.boundary[ID] == BC_DIRICHLET) {
+            set(ID, F_DOWN, true);
+            if (cid(ID + ngy) == 0 && cid(ID - ngy) != 0 && cid(ID - 1) != 0) set(ID, F_RIGHT, false);
+            else if (cid(ID + ngy) != 0 && cid(ID - ngy) == 0 && cid(ID - 1) != 0) set(ID, F_LEFT, false);
+            else if (cid(ID + ngy) != 0 && cid(ID - ngy) != 0 && cid(ID - 1) != 0) set(ID, F_NONE, false);
+            else if (cid(ID + ngy) == 0 && cid(ID - ngy) == 0 && cid(ID - 1) != 0) set(ID, F_NONE, false);
+        } else if (s.boundary[ID] == BC_NEUMANN) {
+            set(ID, F_NONE, false);
+            if (cid(ID + ngy) == 0 && cid(ID - ngy) != 0 && cid(ID - 1) != 0) set(ID, F_RIGHT, false);
+            else if (cid(ID + ngy) != 0 && cid(ID - ngy) == 0 && cid(ID - 1) != 0) set(ID, F_LEFT, false);
+            else if (cid(ID + ngy) != 0 && cid(ID - ngy) != 0 && cid(ID - 1) == 0) set(ID, F_DOWN, true);
+        }
+    }
+    // domain corners (src/start.c:1755-1774)
+    auto corner = [&](int ID, int f) {
+        if (s.boundary[ID] == BC_DIRICHLET && cid(ID + 1) == 0) {
+            s.face[ID] = f;
+            s.area[ID] = (float)(0.5 * (s.dx + s.dy) * s.zlength);
+        }
+    };
+    corner(0, F_UR);
+    corner(ncx * ngy, F_UL);
+    corner(ncy, F_LR);
+    corner(ncx * ngy + ncy, F_LL);
+    // StructureIndex on the (ncx+2) x (ncy+2) ghost grid (src/start.c:1776-1851)
+    const int SY = ncy + 2;
+    std::vector<int> SI((size_t)(ncx + 2) * SY, 0);
+    auto si = [&](int a, int b) -> int & { return SI[(size_t)a * SY + b]; };
+    for (int i = 0; i < ncx; i++)
+        for (int j = 0; j < ncy; j++) {
+            si(i + 1, j + 1) = 0;
+            for (int k = 0; k < s.cond_num; k++)
+                if (i >= s.cond_x0[k] && i < s.cond_x1[k] && j >= s.cond_y0[k] && j < s.cond_y1[k])
+                    si(i + 1, j + 1) = 100 + s.cond_mid[k];
+        }
+    for (int i = 1; i < ngx; i++) {
+        if ((s.boundary[(i - 1) * ngy] == BC_NEUMANN || s.boundary[i * ngy] == BC_NEUMANN) && si(i, 1) == 0)
+            si(i, 0) = -s.boundary[(i - 1) * ngy] - 2;
+        else
+            si(i, 0) = si(i, 1) ? si(i, 1) : -1;
+        if ((s.boundary[(i - 1) * ngy + ncy] == BC_NEUMANN || s.boundary[i * ngy + ncy] == BC_NEUMANN) && si(i, ngy - 1) == 0)
+            si(i, ngy) = -s.boundary[(i - 1) * ngy + ncy] - 6;
+        else
+            si(i, ngy) = si(i, ngy - 1) ? si(i, ngy - 1) : -1;
+    }
+    for (int j = 1; j < ngy; j++) {
+        if ((s.boundary[j - 1] == BC_NEUMANN || s.boundary[j] == BC_NEUMANN) && si(1, j) == 0)
+            si(0, j) = -s.boundary[j - 1];
+        else
+            si(0, j) = si(1, j) ? si(1, j) : -1;
+        if ((s.boundary[ncx * ngy + j - 1] == BC_NEUMANN || s.boundary[ncx * ngy + j] == BC_NEUMANN) && si(ngx - 1, j) == 0)
+            si(ngx, j) = -s.boundary[ncx * ngy + j] - 4;
+        else
+            si(ngx, j) = si(ngx - 1, j) ? si(ngx - 1, j) : -1;
+    }
+    si(0, 0) = -s.boundary[0];
+    si(ncx + 1, 0) = -s.boundary[(ncx - 1) * ngy];
+    si(0, ncy + 1) = -s.boundary[ngy + ncy];
+    si(ncx + 1, ncy + 1) = -s.boundary[(ncy - 1) * ngy + ncy]; // the reference's index, kept as written
+    s.sidx = SI;
+    // DepositBoundary scale per node (src/cuda_Deposit.cu:277-288)
+    s.dep_factor.assign(G, 1.0f);
+    for (int ID = 0; ID < G; ID++) {
+        float f = 1.0f;
+        int fc = s.face[ID];
+        if (fc == F_LEFT || fc == F_RIGHT || fc == F_UP || fc == F_DOWN) f *= 2;
+        else if (fc == F_UL || fc == F_LL || fc == F_UR || fc == F_LR) f *= 4;
+        if (s.boundary[ID] == BC_NEUMANN) f *= 2;
+        else if (s.boundary[ID] == BC_DIRICHLET && fc != F_NONE && s.cond_id[ID] != 0) f *= 2;
+        s.dep_factor[ID] = f;
+    }
+}
+
+// ---------------------------------------------------------------- field solver matrix
+void field_matrix(Setup &s) {
+    const int ngx = s.ngx, ngy = s.ngy, ncx = s.ncx, ncy = s.ncy;
+    s.a_idx.assign(s.Gsize, 0);
+    int n = 1;
+    for (int i = 0; i < ngx; i++) // src/start.c:1919-1928
+        for (int j = 0; j < ngy; j++) {
+            int G = i * ngy + j;
+            if (!s.cond_id[G] && s.boundary[G] != BC_DIRICHLET) s.a_idx[G] = n++;
+        }
+    const int N = n - 1;
+    s.n_unknowns = N;
+    s.a_val.assign(5 * (size_t)N, 0.0f);
+    s.ta_val.assign(5 * (size_t)N, 0.0f);
+    s.ai.assign(N + 1, 0);
+    s.aj.assign(5 * (size_t)N, 0);
+    s.matm.assign(N, 0.0f);
+    s.cond_b.assign((size_t)s.cond_numr * N, 0.0f);
+    s.temp_b.assign(N, 0.0f);
+    s.stencil.assign(5 * (size_t)N, 0.0f);
+    s.unk_node.assign(N, 0);
+    float dydx = (float)(0.5 * s.dy / s.dx);
+    float dxdy = (float)(0.5 * s.dx / s.dy);
+    auto epsr = [&](int a, int b) { return s.eps_r[(size_t)a * ncy + b]; };
+    int m = 0, l = 0;
+    s.ai[0] = 1;
+    for (int i = 0; i < ngx; i++)
+        for (int j = 0; j < ngy; j++) {
+            if (!s.a_idx[i * ngy + j]) continue;
+            int x1, y1, x2, y2;
+            x1 = (i == 0) ? i : i - 1; y1 = (j == ncy) ? j - 1 : j; y2 = (j == 0) ? j : j - 1;
+            float LEFT = dydx * (epsr(x1, y1) + epsr(x1, y2));
+            x1 = (i == ncx) ? i - 1 : i; y1 = (j == ncy) ? j - 1 : j; y2 = (j == 0) ? j : j - 1;
+            float RIGHT = dydx * (epsr(x1, y1) + epsr(x1, y2));
+            y1 = (j == ncy) ? j - 1 : j; x1 = (i == ncx) ? i - 1 : i; x2 = (i == 0) ? i : i - 1;
+            float UP = dxdy * (epsr(x1, y1) + epsr(x2, y1));
+            y1 = (j == 0) ? j : j - 1; x1 = (i == ncx) ? i - 1 : i; x2 = (i == 0) ? i : i - 1;
+            float DOWN = dxdy * (epsr(x1, y1) + epsr(x2, y1));
+            int LEFT_NBC = (i == 0) ? 2 : 1, RIGHT_NBC = (i == ncx) ? 2 : 1;
+            int UP_NBC = (j == ncy) ? 2 : 1, DOWN_NBC = (j == 0) ? 2 : 1;
+            float *st = &s.stencil[5 * (size_t)l];
+            s.unk_node[l] = i * ngy + j;
+            auto nb = [&](int G, float coef, float aval, float tval, int slot) {
+                if (s.cond_id[G]) {
+                    s.cond_b[(size_t)(s.cond_id[G] - 1) * N + l] += coef;
+                    s.temp_b[l] += coef * s.temp[G];
+                } else if (s.boundary[G] == BC_DIRICHLET) {
+                    s.temp_b[l] += coef * s.temp[G];
+                } else {
+                    s.a_val[m] = aval;
+                    s.aj[m] = s.a_idx[G];
+                    s.ta_val[m] = tval;
+                    st[slot] = aval;
+                    m++;
+                }
+            };
+            if (i) nb((i - 1) * ngy + j, LEFT, (-LEFT) * RIGHT_NBC, (-LEFT) * RIGHT_NBC, 0);
+            if (j) nb(i * ngy + j - 1, DOWN, (-DOWN) * UP_NBC, (-DOWN), 1);
+            float C = LEFT + DOWN + UP + RIGHT;
+            s.a_val[m] = C;
+            s.matm[l] = 1 / C;
+            s.aj[m] = s.a_idx[i * ngy + j];
+            s.ta_val[m] = LEFT + DOWN + UP + RIGHT;
+            st[2] = C;
+            m++;
+            if (j != ncy) nb(i * ngy + j + 1, UP, (-UP) * DOWN_NBC, (-UP), 3);
+            if (i != ncx) nb((i + 1) * ngy + j, RIGHT, (-RIGHT) * LEFT_NBC, (-RIGHT), 4);
+            l++;
+            s.ai[l] = m + 1;
+        }
+    s.a_val.resize(m);
+    s.ta_val.resize(m);
+    s.aj.resize(m);
+}
+
+// BiCGSTAB in double (H. A. van der Vorst, SIAM J. Sci. Stat. Comput. 13,
+// 1992) with Jacobi scaling, for the set-up solves.  The reference runs its
+// FP32 PCG to its loose absolute tolerance there (src/cuda_Field.cu:182-236);
+// solving to 1e-12 relative gives the limit that PCG approaches.
+std::vector<double> setup_solve(const Setup &s, const std::vector<float> &vals, const std::vector<double> &b) {
+    const int N = s.n_unknowns;
+    auto matvec = [&](const std::vector<double> &x, std::vector<double> &y) {
+        for (int r = 0; r < N; r++) {
+            double acc = 0;
+            for (int k = s.ai[r] - 1; k < s.ai[r + 1] - 1; k++) acc += (double)vals[k] * x[(size_t)s.aj[k] - 1];
+            y[r] = acc;
+        }
+    };
+    std::vector<double> dinv(N);
+    for (int r = 0; r < N; r++) {
+        double d = 0;
+        for (int k = s.ai[r] - 1; k < s.ai[r + 1] - 1; k++)
+            if (s.aj[k] - 1 == r) d = vals[k];
+        dinv[r] = d != 0 ? 1.0 / d : 1.0;
+    }
+    std::vector<double> x(N, 0.0), r(b), rh(b), p(N, 0.0), v(N, 0.0), sv(N), t(N), y(N), z(N);
+    double bn = 0;
+    for (double q : b) bn += q * q;
+    bn = sqrt(bn);
+    if (bn == 0) return x;
+    double rho = 1, alpha = 1, omega = 1;
+    for (int it = 0; it < 20000; it++) {
+        double rho1 = 0;
+        for (int i = 0; i < N; i++) rho1 += rh[i] * r[i];
+        if (rho1 == 0) break;
+        double beta = (rho1 / rho) * (alpha / omega);
+        for (int i = 0; i < N; i++) p[i] = r[i] + beta * (p[i] - omega * v[i]);
+        for (int i = 0; i < N; i++) y[i] = dinv[i] * p[i];
+        matvec(y, v);
+        double rv = 0;
+        for (int i = 0; i < N; i++) rv += rh[i] * v[i];
+        alpha = rho1 / rv;
+        for (int i = 0; i < N; i++) sv[i] = r[i] - alpha * v[i];
+        for (int i = 0; i < N; i++) z[i] = dinv[i] * sv[i];
+        matvec(z, t);
+        double tt = 0, ts = 0;
+        for (int i = 0; i < N; i++) { tt += t[i] * t[i]; ts += t[i] * sv[i]; }
+        omega = tt > 0 ? ts / tt : 0;
+        double rn = 0;
+        for (int i = 0; i < N; i++) {
+            x[i] += alpha * y[i] + omega * z[i];
+            r[i] = sv[i] - omega * t[i];
+            rn += r[i] * r[i];
+        }
+        rho = rho1;
+        if (sqrt(rn) <= 1e-12 * bn || omega == 0) break;
+    }
+    return x;
+}
+
+void laplace_and_gas(Setup &s) {
+    const int N = s.n_unknowns, G = s.Gsize;
+    // Laplace basis: conductor k at 1 V, the others at 0 V (src/cuda_Field.cu:192-219)
+    s.lap_basis.assign((size_t)s.cond_numr * G, 0.0f);
+    for (int k = 0; k < s.cond_numr; k++) {
+        std::vector<double> b(N);
+        for (int i = 0; i < N; i++) b[i] = s.cond_b[(size_t)k * N + i];
+        std::vector<double> x = setup_solve(s, s.a_val, b);
+        float *phi = &s.lap_basis[(size_t)k * G];
+        for (int g = 0; g < G; g++) {
+            if (s.a_idx[g]) phi[g] = (float)x[(size_t)s.a_idx[g] - 1];
+            else if (s.cond_id[g] == k + 1) phi[g] = 1.0f;
+        }
+    }
+    // gas temperature: TA x = temp_b (src/cuda_Field.cu:221-233)
+    {
+        std::vector<double> b(N);
+        for (int i = 0; i < N; i++) b[i] = s.temp_b[i];
+        std::vector<double> x = setup_solve(s, s.ta_val, b);
+        s.node_temp = s.temp;
+        for (int g = 0; g < G; g++)
+            if (s.a_idx[g]) s.node_temp[g] = (float)x[(size_t)s.a_idx[g] - 1];
+    }
+    s.back_den1.assign(G, 0.0f);
+    s.back_vel1.assign(G, 0.0f);
+    s.back_den2.assign(G, 0.0f);
+    s.back_vel2.assign(G, 0.0f);
+    for (int g = 0; g < G; g++) { // src/cuda_Field.cu:661-678
+        if (!s.dens_region[g]) continue;
+        float T = s.node_temp[g];
+        if (s.main_gas == GAS_AR || s.main_gas == GAS_O2) {
+            s.back_den1[g] = (float)(NperTORR * s.bg[0].Pres / (T * 8.6142e-5 + DBLMIN));
+            s.back_vel1[g] = (float)sqrt(T * 1.38e-23 / s.bg[0].mass);
+        } else {
+            s.back_den1[g] = (float)(NperTORR * s.bg[0].Pres / (T * 8.6142e-5 + DBLMIN));
+            s.back_vel1[g] = (float)sqrt(T * 1.38e-23 / s.bg[0].mass);
+            s.back_den2[g] = (float)(NperTORR * s.bg[1].Pres / (T * 8.6142e-5 + DBLMIN));
+            s.back_vel2[g] = (float)sqrt(T * 1.38e-23 / s.bg[1].mass);
+        }
+    }
+    // fluid (metastable) densities: held at the deck's value on the nodes of
+    // the plasma region; the continuity solver that evolves them is outside
+    // this library (src/cuda_Fluid.cu)
+    s.fluid_den.assign((size_t)s.nfsp * G, 0.0f);
+    for (int f = 0; f < s.nfsp; f++)
+        for (int g = 0; g < G; g++)
+            if (s.dens_region[g]) s.fluid_den[(size_t)f * G + g] = s.fg[f].InitDens;
+}
+
+// ---------------------------------------------------------------- species + load
+void gas_setting(Setup &s, const BuildOpts &o) { // src/start.c:1999-2051
+    // the reference seeds frand() with getpid() (src/main.c:43); any seed in
+    // [1, 2^31-2] is used as is, others are folded into that range
+    long pm_seed = (o.seed >= 1 && o.seed <= 2147483646ull) ? (long)o.seed : (long)(o.seed % 2147483646ull) + 1;
+    ParkMiller pm{pm_seed};
+    s.seed = o.seed;
+    build_vsave(s);
+    for (int isp = 0; isp < s.nsp; isp++) {
+        SpeciesP &p = s.sp[isp];
+        p.q_density = p.q * p.np2c;
+        p.vti = (float)sqrt(CQ * p.Temp / p.mass);
+        p.qm = p.q / p.mass;
+        p.Escale = (float)(0.5 * p.mass / CQ);
+        p.Ascale = p.qm * s.dt;
+        p.Denscale = p.np2c / s.dx / s.dy;
+        p.MCCscale = 1 / p.np2c * s.dx * s.dy * s.dt;
+        int cap = o.cap_per_cell > 0 ? o.cap_per_cell : p.MAXNP / s.Gsize;
+        cap = std::max(cap, 32);
+        s.cap[isp] = (cap + 31) / 32 * 32;
+        // SetParticleLoad (src/Particle.c:3-50) with SP[0]'s load type and window
+        const SpeciesP &l = s.sp[0];
+        if (l.loadtype != 0) unsupported("particle load types other than UNIFORM");
+        float Ninit = p.InitDens;
+        int n_per_cell = (int)(Ninit * s.dx * s.dy * s.zlength / p.np2c);
+        float y0 = l.y_center / s.dy, y1 = l.y_fall / s.dy - 1;
+        float x0 = l.x_center / s.dx, x1 = l.x_fall / s.dx - 1;
+        auto &hx = s.h_x[isp], &hy = s.h_y[isp], &hvx = s.h_vx[isp], &hvy = s.h_vy[isp], &hvz = s.h_vz[isp];
+        auto &hc = s.h_cell[isp];
+        for (int i = 0; i < s.ncx; i++)
+            for (int j = 0; j < s.ncy; j++) {
+                if (s.plasma_region[(size_t)i * s.ncy + j] != 1) continue;
+                int Num = (i >= x0 && i <= x1 && j >= y0 && j <= y1) ? n_per_cell : 0;
+                for (int n = 0; n < Num; n++) {
+                    float vx, vy, vz;
+                    maxwellv(s, pm, p.vti, vx, vy, vz);
+                    float x = (float)i + pm.next();
+                    float y = (float)j + pm.next();
+                    hx.push_back(x); hy.push_back(y); hvx.push_back(vx); hvy.push_back(vy); hvz.push_back(vz);
+                    hc.push_back(i * s.ngy + j);
+                }
+            }
+        p.np = (int)hx.size();
+        // Copy_HCPtoGCP (src/cuda_Particle.cu:28-58): cell from the integer part
+        std::vector<int> &cnt = s.p_count[isp];
+        cnt.assign(s.Csize, 0);
+        std::vector<int> cell_of(p.np);
+        for (int k = 0; k < p.np; k++) {
+            int XID = (int)hx[k], YID = (int)hy[k];
+            if (XID >= s.ncx || YID >= s.ncy) unsupported("initial particle on the far domain edge");
+            cell_of[k] = XID * s.ncy + YID;
+            cnt[cell_of[k]]++;
+        }
+        std::vector<int> start(s.Csize + 1, 0);
+        for (int c = 0; c < s.Csize; c++) start[c + 1] = start[c] + cnt[c];
+        std::vector<int> fill(start.begin(), start.end() - 1);
+        s.p_x[isp].assign(p.np, 0); s.p_y[isp].assign(p.np, 0);
+        s.p_vx[isp].assign(p.np, 0); s.p_vy[isp].assign(p.np, 0); s.p_vz[isp].assign(p.np, 0);
+        for (int k = 0; k < p.np; k++) {
+            int d = fill[cell_of[k]]++;
+            s.p_x[isp][d] = hx[k] - (int)hx[k];
+            s.p_y[isp][d] = hy[k] - (int)hy[k];
+            s.p_vx[isp][d] = hvx[k]; s.p_vy[isp][d] = hvy[k]; s.p_vz[isp][d] = hvz[k];
+        }
+    }
+}
+
+void null_collision(Setup &s) { // src/cuda_mcc.cu:202-276 (Ar)
+    const float prob_cut = 0.08f;
+    if (s.main_gas != GAS_AR) return;
+    s.sigv.assign(3, 0.0f);
+    const int W = 2 + s.n_cx;
+    for (int i = 0; i < s.n_logx; i++) {
+        const float *row = &s.xsec[(size_t)i * W];
+        float engy = row[1];
+        float sig0 = row[2] + row[3] + row[4] + row[5];
+        s.sigv[0] = (float)std::max((double)s.sigv[0], sqrt(2 * 1.602e-19 * engy / s.sp[0].mass) * sig0);
+        float sig1 = row[6];
+        s.sigv[1] = (float)std::max((double)s.sigv[1], sqrt(2 * 1.602e-19 * engy / s.sp[0].mass) * sig1);
+        float sig2 = row[7] + row[8];
+        s.sigv[2] = (float)std::max((double)s.sigv[2], sqrt(2 * 1.602e-19 * engy / s.sp[1].mass) * sig2);
+    }
+    float T0 = (float)(1.0 - exp((double)(-1 * s.dt * s.sigv[0] * s.bg[0].InitDens)));
+    float T1 = (float)(1.0 - exp((double)(-1 * s.dt * s.sigv[1] * s.fg[0].InitDens)));
+    float col0 = T0 + T1;
+    if (col0 > prob_cut) {
+        s.mcc_n = (int)ceil((double)(col0 / prob_cut));
+        float ratio = 1 / (float)s.mcc_n;
+        s.dt_mcc = s.dt * ratio;
+    } else {
+        s.mcc_n = 1;
+        s.dt_mcc = s.dt;
+    }
+}
+
+} // namespace
+
+void build_setup(const char *json, size_t len, const BuildOpts &o, Setup &s) {
+    JVal root;
+    try {
+        root = JParser(json, len).parse();
+    } catch (std::exception &e) {
+        deck_fail(e.what());
+    }
+    std::vector<int> bx0, bx1, by0, by1, bbc;
+    std::vector<float> btemp;
+    read_geometry(root, s, bx0, bx1, by0, by1, bbc, btemp);
+    read_gas(root, s);
+    read_method(root, s);
+    read_collisions(root, s);
+    geometry(s, bx0, bx1, by0, by1, bbc, btemp);
+    // Source_setting (src/Efield.c:3-66)
+    if (s.max_freq == 0.0f) deck_fail("no AC source: the time step is set from the highest source frequency");
+    s.dt = (float)(1.0 / s.max_freq / (float)s.DT_PIC);
+    s.dt_dx = s.dt / s.dx;
+    s.dt_dy = s.dt / s.dy;
+    s.efield_flag.assign(s.cond_numr, 0);
+    for (int i = 0; i < s.cond_numr; i++) {
+        int n = 0;
+        for (int j = 0; j < s.src_num; j++)
+            if (i + 1 == s.src_mid[j]) n++;
+        s.efield_flag[i] = (n > 0 && n < 4) ? 1 : 0;
+    }
+    field_matrix(s);
+    gas_setting(s, o);
+    null_collision(s);
+    laplace_and_gas(s);
+}
+
+} // namespace hp

@@ -1,0 +1,248 @@
+/*
+ * hpic.h -- C ABI of the B200 PIC/MCC step library (libhpic.so).
+ *
+ * The reference runs one discharge case per process through global
+ * `void (*op)(void)` operator pointers bound by start_cuda()
+ * (inc/main.h:25-32, src/cuda_start.cu:2-34) and called by main_cuda()
+ * (src/cuda_main.cu:112-183) in the order
+ *     PCG_SOLVER; EFIELD; MOVE; SORT_BOUNDARY; MCC; DEPOSIT.
+ * This header keeps those entry points, one per operator, but every call
+ * takes an explicit case handle and a CUDA stream instead of process
+ * globals, returns a status instead of calling exit(), and never
+ * synchronises the device implicitly.  No torch or CUDA types appear in the
+ * signatures; `stream` is a cudaStream_t passed as void* (NULL = legacy
+ * default stream).
+ *
+ * Ownership: the caller owns hp_case / hp_batch / hp_server handles; the
+ * library owns every device allocation behind them.  Calls on distinct
+ * handles may come from different host threads.
+ */
+#ifndef HPIC_H
+#define HPIC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+typedef enum hp_status {
+    HP_OK = 0,
+    HP_ERR_ARG = 1,         /* bad argument (NULL handle, index out of range) */
+    HP_ERR_DECK = 2,        /* deck failed the reference's validation rules (src/start.c:19-1430) */
+    HP_ERR_CUDA = 3,        /* a CUDA runtime call failed; hp_last_error() has the text */
+    HP_ERR_OOM = 4,         /* device or host allocation failed */
+    HP_ERR_UNSUPPORTED = 5, /* deck feature outside this library's path (see hp_last_error) */
+    HP_ERR_DEVICE = 6,      /* the case's device status word is non-zero (hp_case_status) */
+    HP_ERR_CAPACITY = 7,    /* batch/server admission refused: memory or slot budget */
+    HP_ERR_NO_CUDA = 8      /* no CUDA device: this library has no CPU fallback */
+} hp_status;
+
+/* Bits of the per-case device status word.  The reference has no error
+ * reporting (checkCudaErrors/gpuErrchk call exit(), src/cuda_main.cu:2-9) and
+ * silently halves an overfull cell (ReArgPtcls, src/cuda_Sortboundary.cu:23-40);
+ * here the kernels set a bit and the host decides. */
+#define HP_STATUS_CELL_OVERFLOW 0x1u /* a cell's slot pool is full (reference: ReArg condition) */
+#define HP_STATUS_NONFINITE 0x2u     /* NaN/Inf in the field solve (reference: src/cuda_main.cu:227) */
+#define HP_STATUS_PCG_NOCONV 0x4u    /* PCG hit its iteration cap */
+#define HP_STATUS_WAIT_TIMEOUT 0x8u  /* a bounded device-side wait gave up */
+
+/* Text of the last error raised on the calling host thread. */
+const char *hp_last_error(void);
+
+/* ---------------------------------------------------------------- set-up */
+/* Host-side case description: the deck read and every table the step
+ * consumes, built without touching a GPU.  It restates InputRead,
+ * Geometry_setting, Source_setting, FieldSolverSetting and GasSetting
+ * (src/main.c:45-49, src/start.c, src/load.c:121-246, src/Particle.c) plus
+ * the set-up parts of main_cuda (Set_NullCollisionTime_cuda,
+ * PCG_SOLVER_Laplace, Calculate_*GasPara). */
+typedef struct hp_setup hp_setup;
+struct hp_case_opts;
+hp_status hp_setup_build(const char *deck_json, size_t deck_len, const struct hp_case_opts *opts, hp_setup **out);
+void hp_setup_destroy(hp_setup *s);
+/* The initial particle load of species isp.  layout 0: cell-sorted, offsets
+ * in [0,1) and counts[Csize]; layout 1: the reference's load order with
+ * global cell coordinates x = i + offset (its HCP arrays, inc/def.h:109-117)
+ * and cells[] = i*ngy + j. */
+hp_status hp_setup_get_particles(const hp_setup *s, int isp, int layout, int *counts_or_cells, float *x, float *y,
+                                 float *vx, float *vy, float *vz, size_t cap, size_t *n_out);
+
+/* ---------------------------------------------------------------- cases */
+typedef struct hp_case hp_case;
+
+typedef struct hp_case_opts {
+    uint64_t seed;       /* loader seed (Park-Miller, src/Particle.c:211-226) and Philox key */
+    int cap_per_cell;    /* particle slots per cell per species; 0 = Max_np / Gsize of the deck */
+    int field_mode;      /* 0: reference rule, FP32 Jacobi-PCG to r'z < tol^2 (src/cuda_Field.cu:942-1072);
+                            1: FP32 PCG inner solve with FP64 residual refinement to pcg_rtol */
+    double pcg_rtol;     /* field_mode 1: ||b - A x||_2 / ||b||_2 target (default 1e-8) */
+    int pcg_max_iter;    /* 0 = 100000, the reference's cap */
+    int o2_all_species;  /* O2 gas: 0 = reference launch (electrons only, src/cuda_mcc.cu:76-77), 1 = all species */
+    int device;          /* CUDA device ordinal */
+} hp_case_opts;
+
+/* Default options. */
+void hp_case_opts_default(hp_case_opts *opts);
+
+/* Build a case from a JSON deck in the reference's format (the text, not a
+ * path).  Replaces InputRead + Geometry_setting + Source_setting +
+ * FieldSolverSetting + GasSetting (src/main.c:45-49) and main_cuda's
+ * Set_*_cuda uploads (src/cuda_main.cu:17-27), including the initial
+ * Deposit_Basic (src/cuda_main.cu:28). */
+hp_status hp_case_create(const char *deck_json, size_t deck_len, const hp_case_opts *opts, hp_case **out);
+hp_status hp_case_destroy(hp_case *c);
+
+typedef struct hp_case_info {
+    int ngx, ngy, ncx, ncy, Gsize, Csize;
+    int nsp, main_gas, cond_numr, n_unknowns;
+    int cap[8];            /* slots per cell, per species */
+    int mcc_subcycles;     /* DT_MCCn (src/cuda_mcc.cu:258-266) */
+    double dt, dx, dy;
+    int64_t tstep;         /* steps taken */
+    size_t device_bytes;   /* device memory held by the case */
+    int pcg_cluster;       /* CTAs per case in the field-solve cluster */
+    int pcg_block;         /* threads per CTA in the field solve */
+} hp_case_info;
+hp_status hp_case_get_info(const hp_case *c, hp_case_info *out);
+hp_status hp_setup_get_info(const hp_setup *s, hp_case_info *out);
+/* Build a case from an existing set-up (uploads its tables and particles). */
+hp_status hp_case_create_from_setup(const hp_setup *s, const hp_case_opts *opts, hp_case **out);
+
+/* Device status word (HP_STATUS_* bits); synchronises on the case's last stream. */
+hp_status hp_case_status(hp_case *c, uint32_t *status);
+
+/* Step counter used by hp_Field (V(t) at t = tstep*dt) and by the MCC
+ * random streams.  hp_step advances it by one before each step, like the
+ * reference's `t += dt; tstep++` (src/cuda_main.cu:114-115). */
+hp_status hp_case_set_tstep(hp_case *c, int64_t tstep);
+
+/* ------------------------------------------- per-step operators (drop-in) */
+/* PCG_SOLVER (src/cuda_Field.cu:133-181) followed by EFIELD =
+ * Efield_cuda_Basic (src/cuda_Field.cu:2-42): Poisson solve with warm start,
+ * potential assembly phi = sum_k V_k(t) phi_Lap,k + phi_Pois, E at nodes. */
+hp_status hp_Field(hp_case *c, void *stream);
+/* MOVE = Move_cuda -> MoveE_Basic (src/cuda_Move.cu:181-270). */
+hp_status hp_Move(hp_case *c, void *stream);
+/* SORT_BOUNDARY = SortBounndary_cuda -> SortBoundary_Basic
+ * (src/cuda_Sortboundary.cu:4-13,41-258). */
+hp_status hp_SortBoundary(hp_case *c, void *stream);
+/* MCC = MCC_Ar_cuda / MCC_O2_cuda / MCC_ArO2_cuda by the deck's gas
+ * (src/cuda_mcc.cu:2-20). */
+hp_status hp_MCC(hp_case *c, void *stream);
+/* DEPOSIT = Deposit_cuda (src/cuda_Deposit.cu:3-20): CIC density, boundary
+ * scaling, rho/eps0, PCG right-hand side. */
+hp_status hp_Deposit(hp_case *c, void *stream);
+/* n steps of the main loop body (src/cuda_main.cu:114-183 without the
+ * diagnostics and dump calls), fused where results allow; replayed from a
+ * CUDA graph after the first call on a stream. */
+hp_status hp_step(hp_case *c, int nsteps, void *stream);
+
+/* ------------------------------------------------- state interchange (host) */
+/* Particles of species isp in cell-sorted order.  counts[Csize] receives the
+ * particles per cell (cell = i*ncy + j); x, y are in-cell offsets in [0,1)
+ * as in GCP (inc/def.h:118-127).  Arrays must hold `cap` entries; n_out
+ * receives the total.  Synchronous. */
+hp_status hp_get_particles(hp_case *c, int isp, int *counts, float *x, float *y, float *vx, float *vy,
+                           float *vz, size_t cap, size_t *n_out);
+hp_status hp_set_particles(hp_case *c, int isp, const int *counts, const float *x, const float *y,
+                           const float *vx, const float *vy, const float *vz);
+/* Movers parked by hp_Move and not yet re-binned by hp_SortBoundary: per
+ * cell, in the order Move found them, with their wrapped offsets and the
+ * direction code (di+1)*3 + (dj+1) of the cell they left through
+ * (reference: the relative CellID of src/cuda_Move.cu:227-255). */
+hp_status hp_get_movers(hp_case *c, int isp, int *counts, float *x, float *y, float *vx, float *vy, float *vz,
+                        int8_t *codes, size_t cap, size_t *n_out);
+
+/* Per-node / per-unknown arrays.  Synchronous. */
+typedef enum hp_grid_field {
+    HP_GRID_EX = 0,      /* float[Gsize]  GGA.Ex */
+    HP_GRID_EY = 1,      /* float[Gsize]  GGA.Ey */
+    HP_GRID_PHI = 2,     /* float[Gsize]  TotPotential */
+    HP_GRID_PHI_POIS = 3,/* float[Gsize]  dev_phi (Poisson part) */
+    HP_GRID_DEN = 4,     /* double[nsp*Gsize] GPG.den (boundary-scaled weight count) */
+    HP_GRID_SOURCE = 5,  /* double[Gsize] dev_Source = rho/eps0 */
+    HP_GRID_PCG_X = 6,   /* double[N] unknown vector (warm start) */
+    HP_GRID_PCG_B = 7,   /* double[N] right-hand side */
+    HP_GRID_AVE_DEN = 8, /* double[nsp*Gsize] running sum of den since hp_reset_averages */
+    HP_GRID_AVE_PHI = 9, /* double[Gsize] running sum of TotPotential */
+    HP_GRID_COND_CHARGE = 10, /* float[nsp*CondNUMR] absorbed particles per conductor */
+    HP_GRID_MCC_COUNT = 11    /* uint32[nsp*16] collisions per channel since creation */
+} hp_grid_field;
+hp_status hp_get_grid(hp_case *c, hp_grid_field f, void *out, size_t bytes);
+hp_status hp_set_grid(hp_case *c, hp_grid_field f, const void *in, size_t bytes);
+/* Running averages (N_ave accumulation, src/cuda_Diagnostic.cu:505-547):
+ * the sums above and the number of accumulated steps. */
+hp_status hp_reset_averages(hp_case *c);
+hp_status hp_get_average_count(hp_case *c, int64_t *n);
+
+/* Field-solver iteration count of the last hp_Field (reference: *FIter). */
+hp_status hp_last_pcg_iters(hp_case *c, int *inner, int *outer);
+
+/* Case tables (constant over a run), for checkers and tools.  `what`:
+ * 0 StructureIndex int[(ncx+2)(ncy+2)], 1 A_idx int[Gsize], 2 node Boundary int[Gsize],
+ * 3 node Face int[Gsize], 4 node CondID int[Gsize], 5 node Area float[Gsize],
+ * 6 BackDen1 float[Gsize], 7 BackVel1 float[Gsize], 8 Laplace basis float[CondNUMR*Gsize],
+ * 9 stencil float[5*N] (W,S,C,N,E per unknown, 0 where absent), 10 vsave float[nvel],
+ * 11 cross-section table float[N_LOGX*(2+nch)], 12 CollF float[4*TnRct],
+ * 13 sigma-v max float[n], 14 node DensRegion int[Gsize], 15 MCC probabilities float[3*Gsize],
+ * 16 cell eps_r float[Csize], 17 BackDen2 float[Gsize], 18 BackVel2 float[Gsize]. */
+hp_status hp_get_table(hp_case *c, int what, void *out, size_t bytes, size_t *bytes_needed);
+hp_status hp_setup_get_table(const hp_setup *s, int what, void *out, size_t bytes, size_t *bytes_needed);
+
+/* ------------------------------------------------------------- batches */
+/* Many independent cases advanced together: one launch per phase over all
+ * cases, each step captured as a CUDA graph.  Cases keep their own handles;
+ * a case belongs to at most one batch at a time. */
+typedef struct hp_batch hp_batch;
+hp_status hp_batch_create(hp_case *const *cases, int n, hp_batch **out);
+hp_status hp_batch_destroy(hp_batch *b);
+hp_status hp_batch_step(hp_batch *b, int nsteps, void *stream);
+/* Per-phase launch shape chosen by the autotuner (hp_batch_autotune) or set here. */
+typedef struct hp_tune {
+    int warps_per_block_particles; /* Move/Sort/MCC/Deposit: warps per CTA (one warp per cell) */
+    int pcg_block;                 /* PCG: threads per CTA */
+    int pcg_cluster_max;           /* PCG: largest cluster per case */
+} hp_tune;
+hp_status hp_batch_set_tune(hp_batch *b, const hp_tune *t);
+hp_status hp_batch_get_tune(hp_batch *b, hp_tune *t);
+/* Time candidate launch shapes on the batch itself (state is saved and restored). */
+hp_status hp_batch_autotune(hp_batch *b, void *stream);
+
+/* ------------------------------------------------------------- serving */
+typedef struct hp_server hp_server;
+typedef struct hp_server_opts {
+    size_t mem_budget_bytes;   /* admission cap on the total device footprint */
+    int max_slots;             /* cases resident at once */
+    int steps_per_launch;      /* steps between admission points */
+    hp_case_opts case_opts;
+} hp_server_opts;
+hp_status hp_server_create(const hp_server_opts *o, hp_server **out);
+hp_status hp_server_destroy(hp_server *s);
+/* Queue a request: deck text and the number of steps to run.  Returns a
+ * request id.  Never blocks on the device. */
+hp_status hp_server_submit(hp_server *s, const char *deck_json, size_t len, int64_t nsteps, uint64_t seed,
+                           int64_t *request_id);
+/* Run one scheduling round: admit queued requests that fit, advance every
+ * resident case by steps_per_launch (or fewer, to finish exactly), retire
+ * finished cases.  Returns the number of requests still queued or running. */
+hp_status hp_server_poll(hp_server *s, void *stream, int *pending);
+typedef struct hp_result {
+    int64_t request_id;
+    uint32_t status;           /* device status word at retirement */
+    int64_t steps;
+    int64_t particle_pushes;   /* sum over steps of particles advanced */
+    double t_submit, t_admit, t_done; /* host clock, seconds */
+    int ngx, ngy, nsp;
+} hp_result;
+/* Pop one finished result; time-averaged n_s (nsp*Gsize) and phi (Gsize)
+ * are copied when the pointers are non-NULL.  *got = 0 when none is ready. */
+hp_status hp_server_take_result(hp_server *s, hp_result *r, double *ave_den, size_t den_cap,
+                                double *ave_phi, size_t phi_cap, int *got);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HPIC_H */

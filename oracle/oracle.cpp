@@ -1,0 +1,1027 @@
+// oracle.cpp -- CPU restatement of the PIC/MCC step (test infrastructure:
+// the checker the GPU results are compared with; never shipped).
+//
+// Follows, operator by operator:
+//   Move          src/cuda_Move.cu:181-270
+//   SortBoundary  src/cuda_Sortboundary.cu:41-258, codes from src/start.c:1776-1851
+//   MCC (Ar)      src/cuda_mcc.cu:97-106,139-201, src/cuda_mccAr.cu:41-232,707-776
+//   Deposit       src/cuda_Deposit.cu:3-104,277-325
+//   Field         src/cuda_Field.cu:2-42,133-181,500-558,639-660,698-846,942-1072
+// with the deterministic ordering this library defines where the reference
+// has none (per-particle Philox draws, pull-ordered re-binning).  See
+// oracle.h for the two precisions.
+#include "oracle.h"
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include <algorithm>
+#include <thread>
+
+#include "hp_math.h"
+#include "hp_rng.h"
+
+namespace {
+
+// cells are independent in the MCC and deposit passes: split them over host threads
+int g_threads = 0;
+int nthreads() {
+    if (g_threads <= 0) {
+        unsigned h = std::thread::hardware_concurrency();
+        g_threads = h ? (int)h : 1;
+    }
+    return g_threads;
+}
+template <class F> void par_for(int n, F f) {
+    const int T = std::min(nthreads(), std::max(1, n / 64));
+    if (T <= 1) {
+        for (int i = 0; i < n; i++) f(i);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; t++)
+        th.emplace_back([&, t] {
+            for (int i = t; i < n; i += T) f(i);
+        });
+    for (auto &x : th) x.join();
+}
+
+// ---------------------------------------------------------------- math by precision
+inline float m_log10(float x) { return hp_log10f(x); }
+inline double m_log10(double x) { return std::log10(x); }
+inline float m_exp(float x) { return hp_expf(x); }
+inline double m_exp(double x) { return std::exp(x); }
+inline float m_pow(float b, float e) { return hp_powf(b, e); }
+inline double m_pow(double b, double e) { return std::pow(b, e); }
+inline void m_sincos_turns(float t, float *s, float *c) { hp_sincos_turns(t, s, c); }
+inline void m_sincos_turns(double t, double *s, double *c) {
+    *s = std::sin(2.0 * M_PI * t);
+    *c = std::cos(2.0 * M_PI * t);
+}
+inline float m_tan(float y) { return hp_tanf_q1(y); }
+inline double m_tan(double y) { return std::tan(y); }
+inline float m_atan(float x) { return hp_atanf(x); }
+inline double m_atan(double x) { return std::atan(x); }
+
+// the kernels' warp tree: v[l] += v[l ^ o] for o = 16, 8, 4, 2, 1; lane 0
+inline double warp_tree(double *v) {
+    double t[32];
+    for (int o = 16; o > 0; o >>= 1) {
+        for (int l = 0; l < 32; l++) t[l] = v[l] + v[l ^ o];
+        std::memcpy(v, t, sizeof t);
+    }
+    return v[0];
+}
+
+struct Fate {
+    int fi, fj;
+    bool absorbed, flipx, flipy;
+    int cond;
+};
+
+struct SimBase {
+    or_case c;
+    int G = 0, C = 0, precision = 32;
+    std::vector<float> cond_charge;
+    std::vector<unsigned> mcc_count;
+    int pcg_iters[2] = {0, 0};
+    std::vector<double> ave_den, ave_phi;
+    int64_t ave_count = 0;
+    virtual ~SimBase() {}
+    virtual void set_particles(int, const int *, const float *, const float *, const float *, const float *,
+                               const float *) = 0;
+    virtual size_t num(int) = 0;
+    virtual void get_particles(int, int *, float *, float *, float *, float *, float *) = 0;
+    virtual void get_particles_d(int, int *, double *, double *, double *, double *, double *) = 0;
+    virtual size_t num_movers(int) = 0;
+    virtual void get_movers(int, int *, float *, float *, float *, float *, float *, int8_t *) = 0;
+    virtual void get_grid(int, void *) = 0;
+    virtual void set_grid(int, const void *) = 0;
+    virtual void field(int64_t) = 0;
+    virtual void move() = 0;
+    virtual void sort() = 0;
+    virtual void mcc(int64_t) = 0;
+    virtual void deposit() = 0;
+    virtual void accumulate() = 0;
+};
+
+template <class R> struct Sim : SimBase {
+    struct Sp {
+        std::vector<int> cnt, start;
+        std::vector<R> x, y, vx, vy, vz;
+        std::vector<int> mcnt, mstart;
+        std::vector<R> mx, my, mvx, mvy, mvz;
+        std::vector<int8_t> mcode;
+        void restart() {
+            start.assign(cnt.size() + 1, 0);
+            for (size_t k = 0; k < cnt.size(); k++) start[k + 1] = start[k] + cnt[k];
+        }
+    } sp[5];
+    std::vector<R> Ex, Ey, phi, phi_p;
+    std::vector<double> den, source, b64, x64;
+    std::vector<float> pf_x;
+    std::vector<double> cw[5][4];
+
+    explicit Sim(const or_case &cc, int prec) {
+        c = cc;
+        precision = prec;
+        G = c.ngx * c.ngy;
+        C = c.ncx * c.ncy;
+        for (int s = 0; s < c.nsp; s++) {
+            sp[s].cnt.assign(C, 0);
+            sp[s].mcnt.assign(C, 0);
+            sp[s].restart();
+            for (int q = 0; q < 4; q++) cw[s][q].assign(C, 0.0);
+        }
+        Ex.assign(G, 0); Ey.assign(G, 0); phi.assign(G, 0); phi_p.assign(G, 0);
+        den.assign((size_t)c.nsp * G, 0.0);
+        source.assign(G, 0.0); b64.assign(G, 0.0); x64.assign(G, 0.0);
+        pf_x.assign(G, 0.0f);
+        cond_charge.assign((size_t)c.nsp * c.cond_numr, 0.0f);
+        mcc_count.assign((size_t)8 * C, 0u);
+        ave_den.assign((size_t)c.nsp * G, 0.0);
+        ave_phi.assign(G, 0.0);
+    }
+
+    // ------------------------------------------------------------ state
+    void set_particles(int s, const int *counts, const float *x, const float *y, const float *vx, const float *vy,
+                       const float *vz) override {
+        Sp &p = sp[s];
+        p.cnt.assign(counts, counts + C);
+        p.restart();
+        size_t n = (size_t)p.start[C];
+        p.x.assign(x, x + n); p.y.assign(y, y + n);
+        p.vx.assign(vx, vx + n); p.vy.assign(vy, vy + n); p.vz.assign(vz, vz + n);
+    }
+    size_t num(int s) override { return sp[s].x.size(); }
+    void get_particles(int s, int *counts, float *x, float *y, float *vx, float *vy, float *vz) override {
+        Sp &p = sp[s];
+        if (counts) std::memcpy(counts, p.cnt.data(), (size_t)C * 4);
+        for (size_t k = 0; k < p.x.size(); k++) {
+            if (x) x[k] = (float)p.x[k];
+            if (y) y[k] = (float)p.y[k];
+            if (vx) vx[k] = (float)p.vx[k];
+            if (vy) vy[k] = (float)p.vy[k];
+            if (vz) vz[k] = (float)p.vz[k];
+        }
+    }
+    void get_particles_d(int s, int *counts, double *x, double *y, double *vx, double *vy, double *vz) override {
+        Sp &p = sp[s];
+        if (counts) std::memcpy(counts, p.cnt.data(), (size_t)C * 4);
+        for (size_t k = 0; k < p.x.size(); k++) {
+            x[k] = p.x[k]; y[k] = p.y[k]; vx[k] = p.vx[k]; vy[k] = p.vy[k]; vz[k] = p.vz[k];
+        }
+    }
+    size_t num_movers(int s) override { return sp[s].mx.size(); }
+    void get_movers(int s, int *counts, float *x, float *y, float *vx, float *vy, float *vz, int8_t *codes) override {
+        Sp &p = sp[s];
+        if (counts) std::memcpy(counts, p.mcnt.data(), (size_t)C * 4);
+        for (size_t k = 0; k < p.mx.size(); k++) {
+            x[k] = (float)p.mx[k]; y[k] = (float)p.my[k];
+            vx[k] = (float)p.mvx[k]; vy[k] = (float)p.mvy[k]; vz[k] = (float)p.mvz[k];
+            if (codes) codes[k] = p.mcode[k];
+        }
+    }
+    void get_grid(int which, void *out) override {
+        float *f = (float *)out;
+        double *d = (double *)out;
+        switch (which) {
+        case 0: for (int n = 0; n < G; n++) f[n] = (float)Ex[n]; break;
+        case 1: for (int n = 0; n < G; n++) f[n] = (float)Ey[n]; break;
+        case 2: for (int n = 0; n < G; n++) f[n] = (float)phi[n]; break;
+        case 3: for (int n = 0; n < G; n++) f[n] = (float)phi_p[n]; break;
+        case 4: std::memcpy(d, den.data(), den.size() * 8); break;
+        case 5: std::memcpy(d, source.data(), source.size() * 8); break;
+        case 6: std::memcpy(d, b64.data(), b64.size() * 8); break;
+        case 7:
+            if (precision == 32 && c.field_mode == 0) for (int n = 0; n < G; n++) d[n] = pf_x[n];
+            else std::memcpy(d, x64.data(), x64.size() * 8);
+            break;
+        }
+    }
+    void set_grid(int which, const void *in) override {
+        const float *f = (const float *)in;
+        const double *d = (const double *)in;
+        switch (which) {
+        case 0: for (int n = 0; n < G; n++) Ex[n] = f[n]; break;
+        case 1: for (int n = 0; n < G; n++) Ey[n] = f[n]; break;
+        case 2: for (int n = 0; n < G; n++) phi[n] = f[n]; break;
+        case 3: for (int n = 0; n < G; n++) phi_p[n] = f[n]; break;
+        case 4: std::memcpy(den.data(), d, den.size() * 8); break;
+        case 5: std::memcpy(source.data(), d, source.size() * 8); break;
+        case 6: std::memcpy(b64.data(), d, b64.size() * 8); break;
+        case 7:
+            if (precision == 32 && c.field_mode == 0) for (int n = 0; n < G; n++) pf_x[n] = (float)d[n];
+            else std::memcpy(x64.data(), d, x64.size() * 8);
+            break;
+        }
+    }
+
+    // ------------------------------------------------------------ Move
+    void move() override {
+        for (int s = 0; s < c.nsp; s++) {
+            Sp &p = sp[s];
+            std::vector<int> ncnt(C, 0);
+            std::vector<R> nx, ny, nvx, nvy, nvz;
+            nx.reserve(p.x.size()); ny.reserve(p.x.size()); nvx.reserve(p.x.size()); nvy.reserve(p.x.size());
+            nvz.reserve(p.x.size());
+            p.mcnt.assign(C, 0);
+            p.mx.clear(); p.my.clear(); p.mvx.clear(); p.mvy.clear(); p.mvz.clear(); p.mcode.clear();
+            const R As = (R)c.Ascale[s], dtdx = (R)c.dt_dx, dtdy = (R)c.dt_dy;
+            for (int cell = 0; cell < C; cell++) {
+                const int i = cell / c.ncy, j = cell - i * c.ncy, node = i * c.ngy + j;
+                const R ex_ws = Ex[node], ex_wn = Ex[node + 1], ex_es = Ex[node + c.ngy], ex_en = Ex[node + c.ngy + 1];
+                const R ey_ws = Ey[node], ey_wn = Ey[node + 1], ey_es = Ey[node + c.ngy], ey_en = Ey[node + c.ngy + 1];
+                for (int q = p.start[cell]; q < p.start[cell + 1]; q++) {
+                    R lx = p.x[q], ly = p.y[q];
+                    const R vx = p.vx[q], vy = p.vy[q], vz = p.vz[q];
+                    const R del_vx = ex_ws * (1 - lx) * (1 - ly) + ex_wn * (1 - lx) * ly + ex_es * lx * (1 - ly) + ex_en * lx * ly;
+                    const R del_vy = ey_ws * (1 - lx) * (1 - ly) + ey_wn * (1 - lx) * ly + ey_es * lx * (1 - ly) + ey_en * lx * ly;
+                    const R mvX = vx + del_vx * As;
+                    const R mvY = vy + del_vy * As;
+                    lx += mvX * dtdx;
+                    ly += mvY * dtdy;
+                    if (ly >= 1 || ly < 0 || lx >= 1 || lx < 0) {
+                        int di = 0, dj = 0;
+                        if (ly >= 1) { dj = 1; ly = (R)((double)ly - 1.0); }
+                        else if (ly < 0) { dj = -1; ly = (R)((double)ly + 1.0); }
+                        if (lx >= 1) { di = 1; lx = (R)((double)lx - 1.0); }
+                        else if (lx < 0) { di = -1; lx = (R)((double)lx + 1.0); }
+                        p.mcnt[cell]++;
+                        p.mx.push_back(lx); p.my.push_back(ly);
+                        p.mvx.push_back(mvX); p.mvy.push_back(mvY); p.mvz.push_back(vz);
+                        p.mcode.push_back((int8_t)((di + 1) * 3 + (dj + 1)));
+                    } else {
+                        ncnt[cell]++;
+                        nx.push_back(lx); ny.push_back(ly); nvx.push_back(mvX); nvy.push_back(mvY); nvz.push_back(vz);
+                    }
+                }
+            }
+            p.cnt.swap(ncnt);
+            p.x.swap(nx); p.y.swap(ny); p.vx.swap(nvx); p.vy.swap(nvy); p.vz.swap(nvz);
+            p.restart();
+            p.mstart.assign(C + 1, 0);
+            for (int k = 0; k < C; k++) p.mstart[k + 1] = p.mstart[k] + p.mcnt[k];
+        }
+    }
+
+    // ------------------------------------------------------------ SortBoundary
+    Fate fate(int si, int sj, int di, int dj) const {
+        Fate f{si + di, sj + dj, false, false, false, -1};
+        const int S = c.sidx[(si + 1 + di) * (c.ncy + 2) + (sj + 1 + dj)];
+        switch (S) {
+        case 0: break;
+        case -2: f.fi += 1; f.flipx = true; break;
+        case -6: f.fi -= 1; f.flipx = true; break;
+        case -4: f.fj += 1; f.flipy = true; break;
+        case -8: f.fj -= 1; f.flipy = true; break;
+        case -12: f.fi += 1; f.fj += 1; f.flipx = f.flipy = true; break;
+        case -16: f.fi -= 1; f.fj += 1; f.flipx = f.flipy = true; break;
+        case -20: f.fi += 1; f.fj -= 1; f.flipx = f.flipy = true; break;
+        case -24: f.fi -= 1; f.fj -= 1; f.flipx = f.flipy = true; break;
+        default:
+            f.absorbed = true;
+            if (S >= 100) f.cond = S - 101;
+            break;
+        }
+        if (!f.absorbed && (f.fi < 0 || f.fi >= c.ncx || f.fj < 0 || f.fj >= c.ncy)) f.absorbed = true;
+        return f;
+    }
+
+    void sort() override {
+        for (int s = 0; s < c.nsp; s++) {
+            Sp &p = sp[s];
+            // conductor tallies of absorbed movers
+            for (int cell = 0; cell < C; cell++) {
+                const int i = cell / c.ncy, j = cell - i * c.ncy;
+                for (int q = p.mstart[cell]; q < p.mstart[cell + 1]; q++) {
+                    const int code = p.mcode[q];
+                    const Fate f = fate(i, j, code / 3 - 1, code % 3 - 1);
+                    if (f.absorbed && f.cond >= 0 && f.cond < c.cond_numr) cond_charge[(size_t)s * c.cond_numr + f.cond] += 1.0f;
+                }
+            }
+            std::vector<int> ncnt(C, 0);
+            std::vector<R> nx, ny, nvx, nvy, nvz;
+            for (int cell = 0; cell < C; cell++) {
+                const int i = cell / c.ncy, j = cell - i * c.ncy;
+                for (int q = p.start[cell]; q < p.start[cell + 1]; q++) {
+                    nx.push_back(p.x[q]); ny.push_back(p.y[q]); nvx.push_back(p.vx[q]); nvy.push_back(p.vy[q]);
+                    nvz.push_back(p.vz[q]);
+                }
+                int out = p.cnt[cell];
+                for (int si = i - 1; si <= i + 1; si++) {
+                    if (si < 0 || si >= c.ncx) continue;
+                    for (int sj = j - 1; sj <= j + 1; sj++) {
+                        if (sj < 0 || sj >= c.ncy) continue;
+                        const int src = si * c.ncy + sj;
+                        for (int q = p.mstart[src]; q < p.mstart[src + 1]; q++) {
+                            const int code = p.mcode[q];
+                            const Fate f = fate(si, sj, code / 3 - 1, code % 3 - 1);
+                            if (f.absorbed || f.fi != i || f.fj != j) continue;
+                            const R x = p.mx[q], y = p.my[q], vx = p.mvx[q], vy = p.mvy[q], vz = p.mvz[q];
+                            nx.push_back(f.flipx ? 1 - x : x);
+                            ny.push_back(f.flipy ? 1 - y : y);
+                            nvx.push_back(f.flipx ? -1 * vx : vx);
+                            nvy.push_back(f.flipy ? -1 * vy : vy);
+                            nvz.push_back(vz);
+                            out++;
+                        }
+                    }
+                }
+                ncnt[cell] = out;
+            }
+            p.cnt.swap(ncnt);
+            p.x.swap(nx); p.y.swap(ny); p.vx.swap(nvx); p.vy.swap(nvy); p.vz.swap(nvz);
+            p.restart();
+            p.mcnt.assign(C, 0);
+            p.mstart.assign(C + 1, 0);
+            p.mx.clear(); p.my.clear(); p.mvx.clear(); p.mvy.clear(); p.mvz.clear(); p.mcode.clear();
+        }
+    }
+
+    // ------------------------------------------------------------ MCC (Ar)
+    R xsec(int ch, R engy) const {
+        if (engy == 0) return (R)0;
+        const R lengy = m_log10(engy);
+        const float *t = c.xsec;
+        const int W = c.xw;
+        const R xe0 = t[0], xeN = t[(c.n_logx - 1) * W];
+        if (lengy < xe0) return t[2 + ch];
+        if (lengy > xeN) return (R)t[(c.n_logx - 1) * W + 2 + ch] * (R)0.1f * m_exp((R)(-1 * (lengy - xeN)));
+        const R ee1 = (R)c.idlogx * (lengy - xe0);
+        int ee2 = (int)ee1;
+        if (ee2 > c.n_logx - 2) ee2 = c.n_logx - 2;
+        const R a1 = ee1 - ee2;
+        const R a2 = 1 - a1;
+        return a2 * (R)t[ee2 * W + 2 + ch] + a1 * (R)t[(ee2 + 1) * W + 2 + ch];
+    }
+    static void maxwellv(R &vx, R &vy, R &vz, R vsaven, R vti, R Rphi, R Rthe) {
+        R sn, cs;
+        m_sincos_turns(Rphi, &sn, &cs);
+        const R costheta = 1 - 2 * Rthe;
+        const R sintheta = std::sqrt(1 - costheta * costheta);
+        vx = vti * vsaven * sintheta * cs;
+        vy = vti * vsaven * sintheta * sn;
+        vz = vti * vsaven * costheta;
+    }
+    static void anewvel(R energy, R vel, R &nvx, R &nvy, R &nvz, R rand1, R rand2) {
+        R coschi;
+        if (energy < (R)1e-30f) coschi = 1;
+        else coschi = (R)(((double)energy + 2.0 - 2.0 * (double)m_pow((R)(energy + 1.0), rand1)) / energy);
+        const R sinchi = (R)std::sqrt(std::fabs(1.0 - (double)(coschi * coschi)));
+        R sinphi, cosphi;
+        m_sincos_turns(rand2, &sinphi, &cosphi);
+        const R r13 = nvx, r23 = nvy, r33 = nvz;
+        R up1, up2, up3;
+        if (r33 == (R)1.0f) { up1 = 0; up2 = 1; up3 = 0; }
+        else { up1 = 0; up2 = 0; up3 = 1; }
+        R r12 = r23 * up3 - r33 * up2;
+        R r22 = r33 * up1 - r13 * up3;
+        R r32 = r13 * up2 - r23 * up1;
+        const R mag = std::sqrt(r12 * r12 + r22 * r22 + r32 * r32);
+        r12 /= mag; r22 /= mag; r32 /= mag;
+        const R r11 = r22 * r33 - r32 * r23;
+        const R r21 = r32 * r13 - r12 * r33;
+        const R r31 = r12 * r23 - r22 * r13;
+        nvx = vel * (r11 * sinchi * cosphi + r12 * sinchi * sinphi + r13 * coschi);
+        nvy = vel * (r21 * sinchi * cosphi + r22 * sinchi * sinphi + r23 * coschi);
+        nvz = vel * (r31 * sinchi * cosphi + r32 * sinchi * sinphi + r33 * coschi);
+    }
+    static void newvel_ionsc(R &vxs, R &vys, R &vzs, R vel, R rand1, R rand2) {
+        const R coschi = std::sqrt(rand1);
+        const R sinchi = (R)std::sqrt(std::fabs(1.0 - (double)(coschi * coschi)));
+        R sinphi, cosphi;
+        m_sincos_turns(rand2, &sinphi, &cosphi);
+        const R r13 = vxs / vel, r23 = vys / vel, r33 = vzs / vel;
+        R up1, up2, up3;
+        if (r33 == (R)1.0f) { up1 = 0; up2 = 1; up3 = 0; }
+        else { up1 = 0; up2 = 0; up3 = 1; }
+        R r12 = r23 * up3 - r33 * up2;
+        R r22 = r33 * up1 - r13 * up3;
+        R r32 = r13 * up2 - r23 * up1;
+        const R mag = std::sqrt(r12 * r12 + r22 * r22 + r32 * r32);
+        r12 /= mag; r22 /= mag; r32 /= mag;
+        const R r11 = r22 * r33 - r32 * r23;
+        const R r21 = r32 * r13 - r12 * r33;
+        const R r31 = r12 * r23 - r22 * r13;
+        vxs = vel * coschi * (r11 * sinchi * cosphi + r12 * sinchi * sinphi + r13 * coschi);
+        vys = vel * coschi * (r21 * sinchi * cosphi + r22 * sinchi * sinphi + r23 * coschi);
+        vzs = vel * coschi * (r31 * sinchi * cosphi + r32 * sinchi * sinphi + r33 * coschi);
+    }
+
+    void mcc(int64_t tstep) override {
+        Sp &el = sp[0], &ion = sp[1];
+        const uint32_t step = (uint32_t)tstep;
+        std::vector<int> ecnt(C), icnt(C);
+        // per-cell outputs, then CSR rebuild
+        std::vector<std::vector<R>> enew(C), inew(C); // created particles: x,y,vx,vy,vz
+        par_for(C, [&](int cell) {
+            const int i = cell / c.ncy, j = cell - i * c.ncy, node = i * c.ngy + j;
+            const float P1 = c.prob[cell], P2 = c.prob[C + cell], Pion = c.prob[2 * C + cell];
+            const R bvel = c.back_vel1[node];
+            unsigned cnt_ch[7] = {0, 0, 0, 0, 0, 0, 0};
+            const int ni = ion.cnt[cell];
+            for (int k = 0; k < ni; k++) {
+                hp_stream rs;
+                hp_stream_init(&rs, c.seed, (uint32_t)k, (uint32_t)cell, step, 1u);
+                float R1 = hp_stream_next(&rs);
+                if (R1 > Pion) continue;
+                const int nn = (int)((c.nvel - 1) * hp_stream_next(&rs));
+                R vnx, vny, vnz;
+                {
+                    const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+                    maxwellv(vnx, vny, vnz, (R)c.vsave[nn], bvel, a, b);
+                }
+                const size_t q = (size_t)ion.start[cell] + k;
+                const R vx = ion.vx[q], vy = ion.vy[q], vz = ion.vz[q];
+                R VX = vx - vnx, VY = vy - vnz, VZ = vz - vny;
+                const R dum = VX * VX + VY * VY + VZ * VZ;
+                const R engy = (R)c.Escale[1] * dum;
+                const R vel = std::sqrt(dum);
+                const R Rr = (R)hp_stream_next(&rs) * (R)c.sigv[2] / vel;
+                R SumSigma = xsec(5, engy);
+                R ox, oy, oz;
+                if (Rr <= SumSigma) {
+                    ox = vnx; oy = vny; oz = vnz;
+                    cnt_ch[5]++;
+                } else if (Rr <= (SumSigma += xsec(6, engy))) {
+                    const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+                    newvel_ionsc(VX, VY, VZ, vel, a, b);
+                    ox = VX + vnx; oy = VY + vny; oz = VZ + vnz;
+                    cnt_ch[6]++;
+                } else {
+                    ox = vx; oy = vy; oz = vz;
+                }
+                ion.vx[q] = ox; ion.vy[q] = oy; ion.vz[q] = oz;
+            }
+            const int ne = el.cnt[cell];
+            for (int k = 0; k < ne; k++) {
+                hp_stream rs;
+                hp_stream_init(&rs, c.seed, (uint32_t)k, (uint32_t)cell, step, 0u);
+                int colltype = 0;
+                float R1 = 0.f;
+                for (int jj = 0; jj < c.mcc_n; jj++) {
+                    R1 = hp_stream_next(&rs);
+                    if (R1 < P2) { colltype = 1; break; }
+                }
+                if (!colltype) continue;
+                const int target = (R1 <= P1) ? 0 : 1;
+                const size_t q = (size_t)el.start[cell] + k;
+                R VX = el.vx[q], VY = el.vy[q], VZ = el.vz[q];
+                const R dum = VX * VX + VY * VY + VZ * VZ;
+                R vel = std::sqrt(dum);
+                VX /= vel; VY /= vel; VZ /= vel;
+                R engy = (R)c.Escale[0] * dum;
+                R rengy = 0, vel2 = 0;
+                const R Esc = (R)c.Escale[0];
+                auto ionize = [&](float th) {
+                    colltype = 2;
+                    engy -= (R)th;
+                    const R u = hp_stream_next(&rs);
+                    rengy = (R)(10.0 * (double)m_tan(u * m_atan((R)(engy / 20.0))));
+                    engy -= rengy;
+                    vel = std::sqrt(std::fabs(rengy) / Esc);
+                    vel2 = std::sqrt(std::fabs(engy) / Esc);
+                };
+                if (target == 0) {
+                    const R R2 = (R)hp_stream_next(&rs) * (R)c.sigv[0] / vel;
+                    R SumSigma = xsec(0, engy);
+                    if (R2 <= SumSigma) {
+                        colltype = 0;
+                        cnt_ch[0]++;
+                    } else if (engy > (R)c.th[1] && R2 <= (SumSigma += xsec(1, engy))) {
+                        colltype = 0;
+                        engy -= (R)c.th[1];
+                        vel = std::sqrt(std::fabs(engy) / Esc);
+                        cnt_ch[1]++;
+                    } else if (engy > (R)c.th[2] && R2 <= (SumSigma += xsec(2, engy))) {
+                        colltype = 0;
+                        engy -= (R)c.th[2];
+                        vel = std::sqrt(std::fabs(engy) / Esc);
+                        cnt_ch[2]++;
+                    } else if (engy > (R)c.th[3] && R2 <= (SumSigma += xsec(3, engy))) {
+                        ionize(c.th[3]);
+                        cnt_ch[3]++;
+                    }
+                } else {
+                    const R R2 = (R)hp_stream_next(&rs) * (R)c.sigv[1] / vel;
+                    const R SumSigma = xsec(4, engy);
+                    if (engy > (R)c.th[4] && R2 <= SumSigma) {
+                        ionize(c.th[4]);
+                        cnt_ch[4]++;
+                    }
+                }
+                if (colltype == 0) {
+                    const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+                    anewvel(engy, vel, VX, VY, VZ, a, b);
+                    el.vx[q] = VX; el.vy[q] = VY; el.vz[q] = VZ;
+                } else if (colltype == 2) {
+                    R nevx = VX, nevy = VY, nevz = VZ;
+                    {
+                        const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+                        anewvel(rengy, vel, nevx, nevy, nevz, a, b);
+                    }
+                    R nivx = VX, nivy = VY, nivz = VZ;
+                    {
+                        const int nn = (int)((c.nvel - 1) * hp_stream_next(&rs));
+                        const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+                        maxwellv(nivx, nivy, nivz, (R)c.vsave[nn], bvel, a, b);
+                    }
+                    {
+                        const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+                        anewvel(engy, vel2, VX, VY, VZ, a, b);
+                    }
+                    el.vx[q] = VX; el.vy[q] = VY; el.vz[q] = VZ;
+                    const R px = el.x[q], py = el.y[q];
+                    R e5[5] = {px, py, nevx, nevy, nevz};
+                    R i5[5] = {px, py, nivx, nivy, nivz};
+                    enew[cell].insert(enew[cell].end(), e5, e5 + 5);
+                    inew[cell].insert(inew[cell].end(), i5, i5 + 5);
+                }
+            }
+            for (int ch = 0; ch < 7; ch++) mcc_count[(size_t)cell * 8 + ch] += cnt_ch[ch];
+        });
+        auto append = [&](Sp &p, std::vector<std::vector<R>> &add) {
+            std::vector<R> nx, ny, nvx, nvy, nvz;
+            for (int cell = 0; cell < C; cell++) {
+                for (int q = p.start[cell]; q < p.start[cell + 1]; q++) {
+                    nx.push_back(p.x[q]); ny.push_back(p.y[q]); nvx.push_back(p.vx[q]); nvy.push_back(p.vy[q]);
+                    nvz.push_back(p.vz[q]);
+                }
+                const std::vector<R> &a = add[cell];
+                for (size_t k = 0; k < a.size(); k += 5) {
+                    nx.push_back(a[k]); ny.push_back(a[k + 1]); nvx.push_back(a[k + 2]); nvy.push_back(a[k + 3]);
+                    nvz.push_back(a[k + 4]);
+                }
+                p.cnt[cell] += (int)(a.size() / 5);
+            }
+            p.x.swap(nx); p.y.swap(ny); p.vx.swap(nvx); p.vy.swap(nvy); p.vz.swap(nvz);
+            p.restart();
+        };
+        append(el, enew);
+        append(ion, inew);
+    }
+
+    // ------------------------------------------------------------ Deposit
+    void deposit() override {
+        for (int s = 0; s < c.nsp; s++) {
+            Sp &p = sp[s];
+            par_for(C, [&](int cell) {
+                R lane[4][32];
+                for (int q = 0; q < 4; q++)
+                    for (int l = 0; l < 32; l++) lane[q][l] = 0;
+                const int n = p.cnt[cell];
+                for (int k = 0; k < n; k++) {
+                    const int l = k & 31;
+                    const R lx = p.x[(size_t)p.start[cell] + k], ly = p.y[(size_t)p.start[cell] + k];
+                    lane[0][l] += (1 - lx) * (1 - ly);
+                    lane[1][l] += (1 - lx) * ly;
+                    lane[2][l] += lx * (1 - ly);
+                    lane[3][l] += lx * ly;
+                }
+                for (int q = 0; q < 4; q++) {
+                    double v[32];
+                    for (int l = 0; l < 32; l++) v[l] = (double)lane[q][l];
+                    cw[s][q][cell] = warp_tree(v);
+                }
+            });
+        }
+        for (int n = 0; n < G; n++) {
+            const int i = n / c.ngy, j = n - i * c.ngy, ncy = c.ncy;
+            double sum = 0.0;
+            for (int s = 0; s < c.nsp; s++) {
+                double d = 0.0;
+                if (i < c.ncx && j < ncy) d += cw[s][0][i * ncy + j];
+                if (i < c.ncx && j > 0) d += cw[s][1][i * ncy + j - 1];
+                if (i > 0 && j < ncy) d += cw[s][2][(i - 1) * ncy + j];
+                if (i > 0 && j > 0) d += cw[s][3][(i - 1) * ncy + j - 1];
+                d *= (double)c.dep_factor[n];
+                den[(size_t)s * G + n] = d;
+                sum += d * (double)c.q_density[s];
+            }
+            const double src = sum / 8.8542e-12;
+            source[n] = src;
+            b64[n] = c.st[2 * G + n] != 0.0f ? src : 0.0;
+        }
+    }
+
+    // ------------------------------------------------------------ Field
+    float spmv_f(const float *st, int n, const std::vector<float> &v) const {
+        float out = 0.0f;
+        const float cw_ = st[n], cs = st[G + n], cc = st[2 * G + n], cn = st[3 * G + n], ce = st[4 * G + n];
+        if (cw_ != 0.0f) out += cw_ * v[n - c.ngy];
+        if (cs != 0.0f) out += cs * v[n - 1];
+        out += cc * v[n];
+        if (cn != 0.0f) out += cn * v[n + 1];
+        if (ce != 0.0f) out += ce * v[n + c.ngy];
+        return out;
+    }
+    double spmv_d(const float *st, int n, const std::vector<double> &v) const {
+        double out = 0.0;
+        const float cw_ = st[n], cs = st[G + n], cc = st[2 * G + n], cn = st[3 * G + n], ce = st[4 * G + n];
+        if (cw_ != 0.0f) out += (double)cw_ * v[n - c.ngy];
+        if (cs != 0.0f) out += (double)cs * v[n - 1];
+        out += (double)cc * v[n];
+        if (cn != 0.0f) out += (double)cn * v[n + 1];
+        if (ce != 0.0f) out += (double)ce * v[n + c.ngy];
+        return out;
+    }
+
+    // Cluster reduction of the GPU PCG: thread partials (nodes lo+t, lo+t+T, ...),
+    // warp trees, warps in order, CTAs in rank order.  f(n, acc) adds node n.
+    template <class F> double cluster_reduce(F f) const {
+        const int CS = c.pcg_cluster, T = c.pcg_block, nw = T / 32;
+        const int per = (G + CS - 1) / CS;
+        double total = 0.0;
+        for (int r = 0; r < CS; r++) {
+            const int lo = r * per, hi = std::min(G, lo + per);
+            double block = 0.0;
+            for (int w = 0; w < nw; w++) {
+                double v[32];
+                for (int l = 0; l < 32; l++) {
+                    double part = 0.0;
+                    for (int n = lo + w * 32 + l; n < hi; n += T) f(n, part);
+                    v[l] = part;
+                }
+                block += warp_tree(v);
+            }
+            total += block;
+        }
+        return total;
+    }
+
+    void field_f32() {
+        const float *st = c.st;
+        std::vector<float> x = pf_x, r(G, 0.0f), p(G, 0.0f), ap(G, 0.0f);
+        int iters = 0, outer = 0;
+        const int maxit = c.pcg_max_iter;
+        if (c.field_mode == 0) {
+            for (int n = 0; n < G; n++) {
+                const float cc = st[2 * G + n];
+                if (cc == 0.0f) continue;
+                const float ax = spmv_f(st, n, x);
+                const float rr = -1.0f * ax + (float)b64[n];
+                r[n] = rr;
+                p[n] = (1 / cc) * rr;
+            }
+            double rz = cluster_reduce([&](int n, double &a) {
+                const float cc = st[2 * G + n];
+                if (cc != 0.0f) a += (double)(r[n] * ((1 / cc) * r[n]));
+            });
+            int iter = 1;
+            while (rz > (double)c.pcg_tol2 && iter <= maxit) {
+                for (int n = 0; n < G; n++)
+                    if (st[2 * G + n] != 0.0f) ap[n] = spmv_f(st, n, p);
+                const double pap = cluster_reduce([&](int n, double &a) {
+                    if (st[2 * G + n] != 0.0f) a += (double)(p[n] * ap[n]);
+                });
+                const float alpha = (pap != 0.0) ? (float)rz / (float)pap : 0.0f;
+                for (int n = 0; n < G; n++) {
+                    const float cc = st[2 * G + n];
+                    if (cc == 0.0f) continue;
+                    x[n] = alpha * p[n] + x[n];
+                    r[n] = -alpha * ap[n] + r[n];
+                }
+                const double rznew = cluster_reduce([&](int n, double &a) {
+                    const float cc = st[2 * G + n];
+                    if (cc != 0.0f) a += (double)(r[n] * ((1 / cc) * r[n]));
+                });
+                if (!(rznew == rznew) || std::isinf(rznew)) break;
+                const float beta = (rz != 0.0) ? (float)rznew / (float)rz : 0.0f;
+                for (int n = 0; n < G; n++) {
+                    const float cc = st[2 * G + n];
+                    if (cc != 0.0f) p[n] = beta * p[n] + (1 / cc) * r[n];
+                }
+                rz = rznew;
+                iter++;
+            }
+            iters = iter;
+            pf_x = x;
+            for (int n = 0; n < G; n++) phi_p[n] = st[2 * G + n] != 0.0f ? x[n] : 0.0f;
+        } else {
+            const float *ss = c.st_sym;
+            double bb = cluster_reduce([&](int n, double &a) { a += b64[n] * b64[n]; });
+            const double target = c.pcg_rtol * c.pcg_rtol * bb;
+            for (outer = 0; outer < 12; outer++) {
+                std::vector<double> r64(G, 0.0);
+                for (int n = 0; n < G; n++) {
+                    const float cc = st[2 * G + n];
+                    if (cc == 0.0f) continue;
+                    r64[n] = b64[n] - spmv_d(st, n, x64);
+                    const float rs = (float)(r64[n] * (double)c.row_scale[n]);
+                    r[n] = rs;
+                    x[n] = 0.0f;
+                    p[n] = (1 / ss[2 * G + n]) * rs;
+                }
+                const double rr = cluster_reduce([&](int n, double &a) {
+                    if (st[2 * G + n] != 0.0f) a += r64[n] * r64[n];
+                });
+                double rz = cluster_reduce([&](int n, double &a) {
+                    if (st[2 * G + n] != 0.0f) a += (double)(r[n] * ((1 / ss[2 * G + n]) * r[n]));
+                });
+                if (!(rr == rr) || rr <= target || bb == 0.0) break;
+                const double rz0 = rz;
+                int iter = 0;
+                while (rz > 1e-10 * rz0 && iter < maxit) {
+                    for (int n = 0; n < G; n++)
+                        if (ss[2 * G + n] != 0.0f) ap[n] = spmv_f(ss, n, p);
+                    const double pap = cluster_reduce([&](int n, double &a) {
+                        if (ss[2 * G + n] != 0.0f) a += (double)(p[n] * ap[n]);
+                    });
+                    const float alpha = (pap != 0.0) ? (float)(rz / pap) : 0.0f;
+                    for (int n = 0; n < G; n++) {
+                        if (ss[2 * G + n] == 0.0f) continue;
+                        x[n] = alpha * p[n] + x[n];
+                        r[n] = -alpha * ap[n] + r[n];
+                    }
+                    const double rznew = cluster_reduce([&](int n, double &a) {
+                        const float cc = ss[2 * G + n];
+                        if (cc != 0.0f) a += (double)(r[n] * ((1 / cc) * r[n]));
+                    });
+                    const float beta = (rz != 0.0) ? (float)(rznew / rz) : 0.0f;
+                    for (int n = 0; n < G; n++) {
+                        const float cc = ss[2 * G + n];
+                        if (cc != 0.0f) p[n] = beta * p[n] + (1 / cc) * r[n];
+                    }
+                    rz = rznew;
+                    iter++;
+                }
+                iters += iter;
+                for (int n = 0; n < G; n++)
+                    if (st[2 * G + n] != 0.0f) x64[n] += (double)x[n];
+            }
+            for (int n = 0; n < G; n++) phi_p[n] = st[2 * G + n] != 0.0f ? (float)x64[n] : 0.0f;
+        }
+        pcg_iters[0] = iters;
+        pcg_iters[1] = outer;
+    }
+
+    // FP64 reference solve: Jacobi-PCG on the symmetric form D^-1 A, in double,
+    // warm-started, to ||r|| <= 1e-11 ||b||.
+    void field_f64() {
+        const float *st = c.st, *ss = c.st_sym;
+        std::vector<double> r(G, 0.0), p(G, 0.0), ap(G, 0.0), z(G, 0.0);
+        double bb = 0.0;
+        for (int n = 0; n < G; n++) bb += b64[n] * b64[n];
+        double rz = 0.0, rr = 0.0;
+        for (int n = 0; n < G; n++) {
+            if (st[2 * G + n] == 0.0f) continue;
+            const double res = b64[n] - spmv_d(st, n, x64);
+            rr += res * res;
+            r[n] = res * (double)c.row_scale[n];
+            z[n] = r[n] / (double)ss[2 * G + n];
+            p[n] = z[n];
+            rz += r[n] * z[n];
+        }
+        int it = 0;
+        const double tol2 = 1e-22 * bb;
+        while (rr > tol2 && bb > 0 && it < 200000) {
+            double pap = 0.0;
+            for (int n = 0; n < G; n++) {
+                if (ss[2 * G + n] == 0.0f) continue;
+                ap[n] = spmv_d(ss, n, p);
+                pap += p[n] * ap[n];
+            }
+            const double alpha = rz / pap;
+            double rznew = 0.0;
+            for (int n = 0; n < G; n++) {
+                if (ss[2 * G + n] == 0.0f) continue;
+                x64[n] += alpha * p[n];
+                r[n] -= alpha * ap[n];
+                z[n] = r[n] / (double)ss[2 * G + n];
+                rznew += r[n] * z[n];
+            }
+            const double beta = rznew / rz;
+            for (int n = 0; n < G; n++)
+                if (ss[2 * G + n] != 0.0f) p[n] = z[n] + beta * p[n];
+            rz = rznew;
+            it++;
+            if ((it & 31) == 0) { // true residual of the unscaled system
+                rr = 0.0;
+                for (int n = 0; n < G; n++) {
+                    if (st[2 * G + n] == 0.0f) continue;
+                    const double res = b64[n] - spmv_d(st, n, x64);
+                    rr += res * res;
+                }
+            }
+        }
+        pcg_iters[0] = it;
+        pcg_iters[1] = 1;
+        for (int n = 0; n < G; n++) phi_p[n] = st[2 * G + n] != 0.0f ? (R)x64[n] : (R)0;
+    }
+
+    R cond_sigma(int n, int eT, int eL, int eD, int eX, int pL, int pR, int pD, int pU) const {
+        const int b = c.boundary[n], f = c.face[n];
+        if (!((b == 3 || b == 1) && f != 8)) return 0;
+        R SumSig = 0;
+        for (int s = 0; s < c.nsp; s++) SumSig += (R)den[(size_t)s * G + n] * (R)c.q_density[s];
+        const R *P = phi_p.data();
+        auto E = [&](int k) { return (R)c.eps[k]; };
+        const R hdx = c.hdx, hdy = c.hdy, idxy = c.idxy;
+        switch (f) {
+        case 2: return hdy * (E(eT) + E(eL)) * (P[n] - P[pU]) - hdx * SumSig;
+        case 3: return hdy * (E(eD) + E(eX)) * (P[n] - P[pD]) - hdx * SumSig;
+        case 0: return hdx * (E(eL) + E(eX)) * (P[n] - P[pL]) - hdy * SumSig;
+        case 1: return hdx * (E(eT) + E(eD)) * (P[n] - P[pR]) - hdy * SumSig;
+        case 4: return hdy * (E(eT) + E(eL)) * (P[n] - P[pU]) + hdx * (E(eL) + E(eX)) * (P[n] - P[pL]) - idxy * SumSig;
+        case 5: return hdy * (E(eT) + E(eL)) * (P[n] - P[pU]) + hdx * (E(eT) + E(eD)) * (P[n] - P[pR]) - idxy * SumSig;
+        case 6: return hdy * (E(eD) + E(eX)) * (P[n] - P[pD]) + hdx * (E(eL) + E(eX)) * (P[n] - P[pL]) - idxy * SumSig;
+        case 7: return hdy * (E(eD) + E(eX)) * (P[n] - P[pD]) + hdx * (E(eT) + E(eD)) * (P[n] - P[pR]) - idxy * SumSig;
+        default: return 0;
+        }
+    }
+
+    void field(int64_t tstep) override {
+        if (precision == 32) field_f32();
+        else field_f64();
+        // potential assembly
+        const double time = (double)tstep * (double)c.dt;
+        std::vector<R> vk(c.cond_numr, 0);
+        for (int k = 0; k < c.cond_numr; k++) {
+            R v = 0;
+            if (c.efield_flag[k])
+                for (int q = 0; q < c.src_num; q++)
+                    if (c.src_mid[q] == k + 1)
+                        v = (R)((double)v + ((double)c.src_dc[q] +
+                                             (double)c.src_ac[q] * std::sin((double)c.src_2pif[q] * time + (double)c.src_rphase[q])));
+            vk[k] = v;
+        }
+        for (int n = 0; n < G; n++) {
+            R tot = 0;
+            for (int k = 0; k < c.cond_numr; k++) tot += vk[k] * (R)c.lap[(size_t)k * G + n];
+            tot += 1 * phi_p[n];
+            phi[n] = tot;
+        }
+        // E at nodes
+        const int ngx = c.ngx, ngy = c.ngy;
+        const R idx = c.idx, idy = c.idy, hdx = c.hdx, hdy = c.hdy, dx = c.dx, dy = c.dy;
+        const R half = (R)0.5f;
+        for (int n = 0; n < G; n++) {
+            const int x = n / ngy, y = n - x * ngy;
+            const int pL = x ? n - ngy : n, pR = (x == ngx - 1) ? n : n + ngy;
+            const int pD = y ? n - 1 : n, pU = (y == ngy - 1) ? n : n + 1;
+            int eT = x * (ngy - 1) + y;
+            int eL = x ? eT - ngy + 1 : eT;
+            int eD = y ? eT - 1 : eT;
+            const int eX = eL + eD - eT;
+            const int xo = (x == ngx - 1) ? ngy - 1 : 0, yo = (y == ngy - 1) ? 1 : 0;
+            eT -= (xo + yo);
+            eL -= yo;
+            eD -= xo;
+            const R *P = phi.data();
+            auto E = [&](int k) { return (R)c.eps[k]; };
+            const int f = c.face[n], b = c.boundary[n];
+            R ex, ey;
+            bool write = true;
+            if (f == 0) {
+                if (b == 3 || b == 2 || b == 1) {
+                    ex = (R)-2.0f * cond_sigma(n, eT, eL, eD, eX, pL, pR, pD, pU) / (E(eL) + E(eX));
+                    ey = 0;
+                } else if (b == 4 || b >= 100) {
+                    ex = idx * (P[pL] - P[n]);
+                    ey = hdy * (P[pD] - P[pU]);
+                } else {
+                    ex = half * (E(eT) + E(eD)) * (P[pR] - P[n]) * idx;
+                    ex -= (half * dx / dy) * E(eT) * (P[n] - P[pU]) * idy;
+                    ex -= (half * dx / dy) * E(eD) * (P[n] - P[pD]) * idy;
+                    ex /= -half * (E(eL) + E(eX));
+                    ey = hdy * (P[pD] - P[pU]);
+                }
+            } else if (f == 1) {
+                if (b == 3 || b == 2 || b == 1) {
+                    ex = (R)2.0f * cond_sigma(n, eT, eL, eD, eX, pL, pR, pD, pU) / (E(eT) + E(eD));
+                    ey = 0;
+                } else if (b == 4 || b >= 100) {
+                    ex = idx * (P[n] - P[pR]);
+                    ey = hdy * (P[pD] - P[pU]);
+                } else {
+                    ex = half * (E(eL) + E(eX)) * (P[pL] - P[n]) * idx;
+                    ex -= (half * dx / dy) * E(eL) * (P[n] - P[pU]) * idy;
+                    ex -= (half * dx / dy) * E(eX) * (P[n] - P[pD]) * idy;
+                    ex /= half * (E(eT) + E(eD));
+                    ey = hdy * (P[pD] - P[pU]);
+                }
+            } else if (f == 2) {
+                if (b == 3 || b == 2 || b == 1) {
+                    ex = 0;
+                    ey = (R)2.0f * cond_sigma(n, eT, eL, eD, eX, pL, pR, pD, pU) / (E(eT) + E(eL));
+                } else if (b == 4 || b >= 100) {
+                    ex = hdx * (P[pL] - P[pR]);
+                    ey = idy * (P[n] - P[pU]);
+                } else {
+                    ex = hdx * (P[pL] - P[pR]);
+                    ey = half * (E(eD) + E(eX)) * (P[pD] - P[n]) * idy;
+                    ey -= (half * dy / dx) * E(eD) * (P[n] - P[pR]) * idx;
+                    ey -= (half * dy / dx) * E(eX) * (P[n] - P[pL]) * idx;
+                    ey /= half * (E(eT) + E(eL));
+                }
+            } else if (f == 3) {
+                if (b == 3 || b == 2 || b == 1) {
+                    ex = 0;
+                    ey = (R)-2.0f * cond_sigma(n, eT, eL, eD, eX, pL, pR, pD, pU) / (E(eD) + E(eX));
+                } else if (b == 4 || b >= 100) {
+                    ex = hdx * (P[pL] - P[pR]);
+                    ey = idy * (P[pD] - P[n]);
+                } else {
+                    ex = hdx * (P[pL] - P[pR]);
+                    ey = half * (E(eT) + E(eL)) * (P[pU] - P[n]) * idy;
+                    ey -= (half * dy / dx) * E(eT) * (P[n] - P[pR]) * idx;
+                    ey -= (half * dy / dx) * E(eL) * (P[n] - P[pL]) * idx;
+                    ey /= -half * (E(eD) + E(eX));
+                }
+            } else if (f >= 4 && f <= 7) {
+                const bool solid = (b == 3 || b == 1 || b == 4);
+                if (!solid) { ex = hdx * (P[pL] - P[pR]); ey = hdy * (P[pD] - P[pU]); }
+                else if (f == 4) { ex = idx * (P[pL] - P[n]); ey = idy * (P[n] - P[pU]); }
+                else if (f == 5) { ex = idx * (P[n] - P[pR]); ey = idy * (P[n] - P[pU]); }
+                else if (f == 6) { ex = idx * (P[pL] - P[n]); ey = idy * (P[pD] - P[n]); }
+                else { ex = idx * (P[n] - P[pR]); ey = idy * (P[pD] - P[n]); }
+            } else if (b == 2) {
+                if (x == 0 || x == ngx - 1) { ex = 0; ey = hdy * (P[pD] - P[pU]); }
+                else if (y == 0 || y == ngy - 1) { ex = hdx * (P[pL] - P[pR]); ey = 0; }
+                else { write = false; ex = ey = 0; }
+            } else {
+                ex = hdx * (P[pL] - P[pR]);
+                ey = hdy * (P[pD] - P[pU]);
+            }
+            if (write) { Ex[n] = ex; Ey[n] = ey; }
+        }
+    }
+
+    void accumulate() override {
+        for (size_t k = 0; k < den.size(); k++) ave_den[k] += den[k];
+        for (int n = 0; n < G; n++) ave_phi[n] += (double)phi[n];
+        ave_count++;
+    }
+};
+
+} // namespace
+
+struct or_sim {
+    SimBase *impl;
+};
+
+extern "C" {
+
+or_sim *or_sim_new(const or_case *c, int precision) {
+    or_sim *s = new or_sim;
+    if (precision == 64) s->impl = new Sim<double>(*c, 64);
+    else s->impl = new Sim<float>(*c, 32);
+    return s;
+}
+void or_sim_free(or_sim *s) {
+    if (!s) return;
+    delete s->impl;
+    delete s;
+}
+void or_set_particles(or_sim *s, int isp, const int *counts, const float *x, const float *y, const float *vx,
+                      const float *vy, const float *vz) {
+    s->impl->set_particles(isp, counts, x, y, vx, vy, vz);
+}
+size_t or_num_particles(or_sim *s, int isp) { return s->impl->num(isp); }
+void or_get_particles(or_sim *s, int isp, int *counts, float *x, float *y, float *vx, float *vy, float *vz) {
+    s->impl->get_particles(isp, counts, x, y, vx, vy, vz);
+}
+void or_get_particles_d(or_sim *s, int isp, int *counts, double *x, double *y, double *vx, double *vy, double *vz) {
+    s->impl->get_particles_d(isp, counts, x, y, vx, vy, vz);
+}
+size_t or_num_movers(or_sim *s, int isp) { return s->impl->num_movers(isp); }
+void or_get_movers(or_sim *s, int isp, int *counts, float *x, float *y, float *vx, float *vy, float *vz,
+                   int8_t *codes) {
+    s->impl->get_movers(isp, counts, x, y, vx, vy, vz, codes);
+}
+void or_get_grid(or_sim *s, int which, void *out) { s->impl->get_grid(which, out); }
+void or_set_grid(or_sim *s, int which, const void *in) { s->impl->set_grid(which, in); }
+void or_get_counters(or_sim *s, float *cond_charge, unsigned *mcc_count, int *pcg_iters) {
+    SimBase *b = s->impl;
+    if (cond_charge) std::memcpy(cond_charge, b->cond_charge.data(), b->cond_charge.size() * 4);
+    if (mcc_count) std::memcpy(mcc_count, b->mcc_count.data(), b->mcc_count.size() * 4);
+    if (pcg_iters) { pcg_iters[0] = b->pcg_iters[0]; pcg_iters[1] = b->pcg_iters[1]; }
+}
+void or_field(or_sim *s, int64_t tstep) { s->impl->field(tstep); }
+void or_move(or_sim *s) { s->impl->move(); }
+void or_sort(or_sim *s) { s->impl->sort(); }
+void or_mcc(or_sim *s, int64_t tstep) { s->impl->mcc(tstep); }
+void or_deposit(or_sim *s) { s->impl->deposit(); }
+void or_run(or_sim *s, int64_t tstep0, int nsteps, int accumulate) {
+    for (int k = 1; k <= nsteps; k++) {
+        const int64_t t = tstep0 + k;
+        s->impl->field(t);
+        s->impl->move();
+        s->impl->sort();
+        s->impl->mcc(t);
+        s->impl->deposit();
+        if (accumulate) s->impl->accumulate();
+    }
+}
+void or_get_averages(or_sim *s, double *ave_den, double *ave_phi, int64_t *count) {
+    SimBase *b = s->impl;
+    if (ave_den) std::memcpy(ave_den, b->ave_den.data(), b->ave_den.size() * 8);
+    if (ave_phi) std::memcpy(ave_phi, b->ave_phi.data(), b->ave_phi.size() * 8);
+    if (count) *count = b->ave_count;
+}
+int or_num_threads(void) { return nthreads(); }
+void or_set_threads(int n) { g_threads = n; }
+
+} // extern "C"

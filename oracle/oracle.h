@@ -1,0 +1,92 @@
+/*
+ * oracle.h -- CPU checker for the PIC/MCC step (test infrastructure only).
+ *
+ * Nothing in the product links or calls this: tests/, the smoke check and
+ * bench.py's CPU baseline use it to compute the expected result of each
+ * operator on the same inputs the GPU sees.  It restates the reference's
+ * per-step algorithm (the files cited in oracle.cpp) on a plain host data
+ * layout: per species, particles in cell order with a count per cell (CSR).
+ *
+ * Two precisions:
+ *   or_sim_new(..., precision = 32): the single-precision form the GPU
+ *     kernels compute, operation for operation (same reduction trees, same
+ *     elementary functions from include/hp_math.h, no fused multiply-adds),
+ *     so results are expected to be bit-identical;
+ *   precision = 64: the same algorithm with every particle, field and
+ *     solver quantity in double and libm functions: the FP64 reference the
+ *     mixed-precision GPU runs are compared with over whole RF cycles.
+ */
+#ifndef HP_ORACLE_H
+#define HP_ORACLE_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct or_case {
+    int ngx, ngy, ncx, ncy, nsp, cond_numr, n_unknowns;
+    float dt_dx, dt_dy, dt, dx, dy, idx, idy, hdx, hdy, idxy;
+    const int *sidx, *boundary, *face, *cond_id;
+    const float *eps;        /* [C] EPS0 * eps_r */
+    const float *dep_factor; /* [G] */
+    float Ascale[5], q_density[5], Escale[5];
+    /* collisions (Ar set) */
+    const float *xsec;
+    int n_logx, xw;
+    float idlogx;
+    float sigv[8], th[16];
+    const float *prob; /* [3*C] */
+    const float *back_vel1;
+    const float *vsave;
+    int nvel, mcc_n;
+    uint64_t seed;
+    /* field */
+    const float *st, *st_sym, *row_scale; /* [5*G], [5*G], [G] node layout */
+    const float *lap;                     /* [cond_numr*G] */
+    int src_num, src_mid[8], efield_flag[8];
+    float src_dc[8], src_ac[8], src_2pif[8], src_rphase[8];
+    float pcg_tol2;
+    int pcg_max_iter, field_mode;
+    double pcg_rtol;
+    /* launch shape the GPU used for the PCG reductions */
+    int pcg_cluster, pcg_block;
+} or_case;
+
+typedef struct or_sim or_sim;
+
+or_sim *or_sim_new(const or_case *c, int precision);
+void or_sim_free(or_sim *s);
+/* particles of species isp in cell order: counts[C], arrays of sum(counts) */
+void or_set_particles(or_sim *s, int isp, const int *counts, const float *x, const float *y, const float *vx,
+                      const float *vy, const float *vz);
+size_t or_num_particles(or_sim *s, int isp);
+void or_get_particles(or_sim *s, int isp, int *counts, float *x, float *y, float *vx, float *vy, float *vz);
+/* double-precision copy of the particle state (precision 64) */
+void or_get_particles_d(or_sim *s, int isp, int *counts, double *x, double *y, double *vx, double *vy, double *vz);
+size_t or_num_movers(or_sim *s, int isp);
+void or_get_movers(or_sim *s, int isp, int *counts, float *x, float *y, float *vx, float *vy, float *vz,
+                   int8_t *codes);
+/* node fields: which 0 Ex, 1 Ey, 2 phi, 3 phi_pois (float[G]); 4 den (double[nsp*G]);
+ * 5 source (double[G]); 6 b (double[G]); 7 x (double[G]) */
+void or_get_grid(or_sim *s, int which, void *out);
+void or_set_grid(or_sim *s, int which, const void *in);
+void or_get_counters(or_sim *s, float *cond_charge, unsigned *mcc_count, int *pcg_iters);
+
+/* operators (reference order: Field, Move, SortBoundary, MCC, Deposit) */
+void or_field(or_sim *s, int64_t tstep);
+void or_move(or_sim *s);
+void or_sort(or_sim *s);
+void or_mcc(or_sim *s, int64_t tstep);
+void or_deposit(or_sim *s);
+/* n full steps from tstep+1; accumulates node averages when ave != 0 */
+void or_run(or_sim *s, int64_t tstep0, int nsteps, int accumulate);
+void or_get_averages(or_sim *s, double *ave_den, double *ave_phi, int64_t *count);
+int or_num_threads(void);
+void or_set_threads(int n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,275 @@
+"""ctypes binding of the CPU oracle (oracle/_build/liboracle.so).
+
+Test infrastructure only: tests/, the smoke check and bench.py's CPU
+baseline use this to compute the expected result of each step operator.
+The oracle reads the case tables the library built (through hpic's table
+export) and keeps its own particle and field state.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB = os.path.join(HERE, "_build", "liboracle.so")
+
+_F = C.POINTER(C.c_float)
+_I = C.POINTER(C.c_int)
+_D = C.POINTER(C.c_double)
+
+
+class OrCase(C.Structure):
+    _fields_ = [
+        ("ngx", C.c_int), ("ngy", C.c_int), ("ncx", C.c_int), ("ncy", C.c_int), ("nsp", C.c_int),
+        ("cond_numr", C.c_int), ("n_unknowns", C.c_int),
+        ("dt_dx", C.c_float), ("dt_dy", C.c_float), ("dt", C.c_float), ("dx", C.c_float), ("dy", C.c_float),
+        ("idx", C.c_float), ("idy", C.c_float), ("hdx", C.c_float), ("hdy", C.c_float), ("idxy", C.c_float),
+        ("sidx", _I), ("boundary", _I), ("face", _I), ("cond_id", _I), ("eps", _F), ("dep_factor", _F),
+        ("Ascale", C.c_float * 5), ("q_density", C.c_float * 5), ("Escale", C.c_float * 5),
+        ("xsec", _F), ("n_logx", C.c_int), ("xw", C.c_int), ("idlogx", C.c_float),
+        ("sigv", C.c_float * 8), ("th", C.c_float * 16), ("prob", _F), ("back_vel1", _F), ("vsave", _F),
+        ("nvel", C.c_int), ("mcc_n", C.c_int), ("seed", C.c_uint64),
+        ("st", _F), ("st_sym", _F), ("row_scale", _F), ("lap", _F),
+        ("src_num", C.c_int), ("src_mid", C.c_int * 8), ("efield_flag", C.c_int * 8),
+        ("src_dc", C.c_float * 8), ("src_ac", C.c_float * 8), ("src_2pif", C.c_float * 8),
+        ("src_rphase", C.c_float * 8),
+        ("pcg_tol2", C.c_float), ("pcg_max_iter", C.c_int), ("field_mode", C.c_int), ("pcg_rtol", C.c_double),
+        ("pcg_cluster", C.c_int), ("pcg_block", C.c_int),
+    ]
+
+
+_lib = None
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        P = C.c_void_p
+        sig = {
+            "or_sim_new": (P, [C.POINTER(OrCase), C.c_int]),
+            "or_sim_free": (None, [P]),
+            "or_set_particles": (None, [P, C.c_int, _I, _F, _F, _F, _F, _F]),
+            "or_num_particles": (C.c_size_t, [P, C.c_int]),
+            "or_get_particles": (None, [P, C.c_int, _I, _F, _F, _F, _F, _F]),
+            "or_get_particles_d": (None, [P, C.c_int, _I, _D, _D, _D, _D, _D]),
+            "or_num_movers": (C.c_size_t, [P, C.c_int]),
+            "or_get_movers": (None, [P, C.c_int, _I, _F, _F, _F, _F, _F, C.POINTER(C.c_int8)]),
+            "or_get_grid": (None, [P, C.c_int, P]),
+            "or_set_grid": (None, [P, C.c_int, P]),
+            "or_get_counters": (None, [P, _F, C.POINTER(C.c_uint), _I]),
+            "or_field": (None, [P, C.c_int64]),
+            "or_move": (None, [P]),
+            "or_sort": (None, [P]),
+            "or_mcc": (None, [P, C.c_int64]),
+            "or_deposit": (None, [P]),
+            "or_run": (None, [P, C.c_int64, C.c_int, C.c_int]),
+            "or_get_averages": (None, [P, _D, _D, C.POINTER(C.c_int64)]),
+            "or_num_threads": (C.c_int, []),
+            "or_set_threads": (None, [C.c_int]),
+        }
+        for k, (r, a) in sig.items():
+            f = getattr(L, k)
+            f.restype = r
+            f.argtypes = a
+        _lib = L
+    return _lib
+
+
+def _fp(a):
+    return a.ctypes.data_as(_F)
+
+
+def _ip(a):
+    return a.ctypes.data_as(_I)
+
+
+class Oracle:
+    """CPU restatement of one case.  `tables` is a callable name -> array
+    (hpic.Case.table or hpic.Setup.table); `info` the case info."""
+
+    GRID = dict(EX=0, EY=1, PHI=2, PHI_POIS=3, DEN=4, SOURCE=5, B=6, X=7)
+
+    def __init__(self, tables, info, opts, precision=32, pcg_cluster=1, pcg_block=512):
+        self.info = info
+        self.keep = {}
+        t = tables
+        sc = t("scalars")
+        spc = t("species").reshape(-1, 16)
+        src = t("sources")
+        c = OrCase()
+        c.ngx, c.ngy, c.ncx, c.ncy, c.nsp = info.ngx, info.ngy, info.ncx, info.ncy, info.nsp
+        c.cond_numr, c.n_unknowns = info.cond_numr, info.n_unknowns
+        dt, dx, dy = sc[0], sc[3], sc[4]
+        c.dt = dt
+        c.dt_dx = np.float32(dt) / np.float32(dx)
+        c.dt_dy = np.float32(dt) / np.float32(dy)
+        c.dx, c.dy, c.idx, c.idy, c.hdx, c.hdy, c.idxy = sc[3], sc[4], sc[5], sc[6], sc[7], sc[8], sc[9]
+
+        def keep(name, arr, dtype):
+            a = np.ascontiguousarray(arr, dtype=dtype)
+            self.keep[name] = a
+            return a.ctypes.data_as(_I if dtype == np.int32 else _F)
+
+        c.sidx = keep("sidx", t("sidx"), np.int32)
+        c.boundary = keep("boundary", t("boundary"), np.int32)
+        c.face = keep("face", t("face"), np.int32)
+        c.cond_id = keep("cond_id", t("cond_id"), np.int32)
+        c.eps = keep("eps", (8.8542e-12 * t("eps_r").astype(np.float64)).astype(np.float32), np.float32)
+        c.dep_factor = keep("dep", t("dep_factor"), np.float32)
+        for s in range(info.nsp):
+            c.Ascale[s] = spc[s, 7]
+            c.q_density[s] = spc[s, 3]
+            c.Escale[s] = spc[s, 6]
+        c.xsec = keep("xsec", t("xsec"), np.float32)
+        c.n_logx = int(sc[14])
+        c.xw = self.keep["xsec"].size // c.n_logx
+        c.idlogx = sc[15]
+        sigv = t("sigv")
+        for k in range(min(8, sigv.size)):
+            c.sigv[k] = sigv[k]
+        collf = t("collf").reshape(-1, 4)
+        for k in range(min(16, collf.shape[0])):
+            c.th[k] = collf[k, 2]
+        c.prob = keep("prob", t("prob"), np.float32)
+        c.back_vel1 = keep("bv1", t("back_vel1"), np.float32)
+        c.vsave = keep("vsave", t("vsave"), np.float32)
+        c.nvel = int(sc[12])
+        c.mcc_n = int(sc[11])
+        c.seed = opts.seed
+        G = info.Gsize
+        st_u = t("stencil").reshape(-1, 5)
+        unk = t("unk_node")
+        st = np.zeros((5, G), np.float32)
+        sym = np.zeros((5, G), np.float32)
+        scale = np.ones(G, np.float32)
+        ii, jj = unk // info.ngy, unk % info.ngy
+        d = (np.where((ii == 0) | (ii == info.ncx), 2, 1) * np.where((jj == 0) | (jj == info.ncy), 2, 1)).astype(
+            np.float32)
+        for k in range(5):
+            st[k, unk] = st_u[:, k]
+            sym[k, unk] = st_u[:, k] / d
+        scale[unk] = np.float32(1.0) / d
+        c.st = keep("st", st.ravel(), np.float32)
+        c.st_sym = keep("st_sym", sym.ravel(), np.float32)
+        c.row_scale = keep("scale", scale, np.float32)
+        c.lap = keep("lap", t("lap"), np.float32)
+        nsrc = (src.size - info.cond_numr) // 5
+        c.src_num = nsrc
+        for k in range(nsrc):
+            c.src_mid[k] = int(src[5 * k])
+            c.src_dc[k], c.src_ac[k], c.src_2pif[k], c.src_rphase[k] = src[5 * k + 1:5 * k + 5]
+        for k in range(info.cond_numr):
+            c.efield_flag[k] = int(src[5 * nsrc + k])
+        c.pcg_tol2 = np.float32(sc[2]) * np.float32(sc[2])
+        c.pcg_max_iter = opts.pcg_max_iter if opts.pcg_max_iter > 0 else 100000
+        c.field_mode = opts.field_mode
+        c.pcg_rtol = opts.pcg_rtol if opts.pcg_rtol > 0 else 1e-8
+        c.pcg_cluster = pcg_cluster
+        c.pcg_block = pcg_block
+        self.c = c
+        self.h = lib().or_sim_new(C.byref(c), precision)
+        self.precision = precision
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().or_sim_free(self.h)
+            self.h = None
+
+    def set_particles(self, isp, counts, x, y, vx, vy, vz):
+        arrs = [np.ascontiguousarray(a, np.float32) for a in (x, y, vx, vy, vz)]
+        counts = np.ascontiguousarray(counts, np.int32)
+        lib().or_set_particles(self.h, isp, _ip(counts), *[_fp(a) for a in arrs])
+
+    def particles(self, isp):
+        n = lib().or_num_particles(self.h, isp)
+        counts = np.zeros(self.info.Csize, np.int32)
+        arrs = [np.zeros(max(n, 1), np.float32) for _ in range(5)]
+        lib().or_get_particles(self.h, isp, _ip(counts), *[_fp(a) for a in arrs])
+        return counts, [a[:n] for a in arrs]
+
+    def particles_d(self, isp):
+        n = lib().or_num_particles(self.h, isp)
+        counts = np.zeros(self.info.Csize, np.int32)
+        arrs = [np.zeros(max(n, 1), np.float64) for _ in range(5)]
+        lib().or_get_particles_d(self.h, isp, _ip(counts), *[a.ctypes.data_as(_D) for a in arrs])
+        return counts, [a[:n] for a in arrs]
+
+    def movers(self, isp):
+        n = lib().or_num_movers(self.h, isp)
+        counts = np.zeros(self.info.Csize, np.int32)
+        arrs = [np.zeros(max(n, 1), np.float32) for _ in range(5)]
+        codes = np.zeros(max(n, 1), np.int8)
+        lib().or_get_movers(self.h, isp, _ip(counts), *[_fp(a) for a in arrs],
+                            codes.ctypes.data_as(C.POINTER(C.c_int8)))
+        return counts, [a[:n] for a in arrs], codes[:n]
+
+    def grid(self, name):
+        G, nsp = self.info.Gsize, self.info.nsp
+        w = self.GRID[name]
+        if w <= 3:
+            out = np.zeros(G, np.float32)
+        elif w == 4:
+            out = np.zeros(nsp * G, np.float64)
+        else:
+            out = np.zeros(G, np.float64)
+        lib().or_get_grid(self.h, w, out.ctypes.data_as(C.c_void_p))
+        return out
+
+    def set_grid(self, name, arr):
+        w = self.GRID[name]
+        dt = np.float32 if w <= 3 else np.float64
+        a = np.ascontiguousarray(arr, dtype=dt)
+        lib().or_set_grid(self.h, w, a.ctypes.data_as(C.c_void_p))
+
+    def counters(self):
+        cc = np.zeros(max(1, self.info.nsp * self.info.cond_numr), np.float32)
+        mc = np.zeros(8 * self.info.Csize, np.uint32)
+        it = np.zeros(2, np.int32)
+        lib().or_get_counters(self.h, _fp(cc), mc.ctypes.data_as(C.POINTER(C.c_uint)), _ip(it))
+        return cc, mc, it
+
+    def Field(self, tstep):
+        lib().or_field(self.h, tstep)
+
+    def Move(self):
+        lib().or_move(self.h)
+
+    def SortBoundary(self):
+        lib().or_sort(self.h)
+
+    def MCC(self, tstep):
+        lib().or_mcc(self.h, tstep)
+
+    def Deposit(self):
+        lib().or_deposit(self.h)
+
+    def run(self, tstep0, nsteps, accumulate=True):
+        lib().or_run(self.h, tstep0, nsteps, 1 if accumulate else 0)
+
+    def averages(self):
+        G, nsp = self.info.Gsize, self.info.nsp
+        d = np.zeros(nsp * G, np.float64)
+        p = np.zeros(G, np.float64)
+        n = C.c_int64(0)
+        lib().or_get_averages(self.h, d.ctypes.data_as(_D), p.ctypes.data_as(_D), C.byref(n))
+        return d, p, n.value
+
+
+def from_setup(setup, precision=32, field_mode=0, pcg_cluster=1, pcg_block=512):
+    """Oracle for a hpic.Setup, loaded with its initial particles."""
+    import hpic  # noqa: F401  (path set by the caller)
+    opts = setup.opts
+    opts.field_mode = field_mode
+    o = Oracle(setup.table, setup.info, opts, precision, pcg_cluster, pcg_block)
+    for s in range(setup.info.nsp):
+        counts, arrs = setup.particles(s, layout=0)
+        o.set_particles(s, counts, *arrs)
+    return o

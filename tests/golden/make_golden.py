@@ -1,0 +1,87 @@
+"""Generate the set-up golden fixtures from the reference's own code.
+
+Runs oracle/_ref/ref_dump (the reference's src/start.c, src/load.c,
+src/PhysicsData.c, src/Particle.c, src/Efield.c compiled in place by
+`make -C oracle ref`) on small decks and stores every table it produces in
+tests/golden/setup_<name>.npz together with the deck text and seed.  Needs
+the reference tree, so it runs only where that exists; the .npz files are
+committed and the tests read only them.
+
+usage: python tests/golden/make_golden.py
+"""
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, os.path.join(REPO, "hybrid-final_b200"))
+from hpic.decks import ccp_deck  # noqa: E402
+
+GGA = np.dtype([("Boundary", "i4"), ("CondID", "i4"), ("Face", "i4"), ("DensRegion", "i4"), ("Area", "f4"),
+                ("Temp", "f4"), ("BackDen1", "f4"), ("BackVel1", "f4"), ("BackDen2", "f4"), ("BackVel2", "f4"),
+                ("Lap_Pot", "f4"), ("Pois_Pot", "f4"), ("Ex", "f4"), ("Ey", "f4")])
+
+
+def block_deck():
+    """Thick block electrodes and a floating block inside: exercises the
+    conductor-face classification and the >=100 StructureIndex codes."""
+    d = ccp_deck(33, 21, 0.01, 0.00625, ppc=8)
+    geo = d["Geometry"]
+    geo["ConductorSpec"] = [
+        {"M_ID": 1, "X0": 0, "X1": 32, "Y0": 0, "Y1": 2, "Temp": 300.0, "R(Ohm)": 0.0, "L(H)": 0.0, "C(F)": 1.0},
+        {"M_ID": 2, "X0": 0, "X1": 32, "Y0": 18, "Y1": 20, "Temp": 300.0, "R(Ohm)": 0.0, "L(H)": 0.0, "C(F)": 1.0},
+        {"M_ID": 3, "X0": 12, "X1": 18, "Y0": 8, "Y1": 11, "Temp": 350.0, "R(Ohm)": 0.0, "L(H)": 0.0, "C(F)": 1.0},
+    ]
+    geo["BoundaryCondition"] = [
+        {"X0": 0, "X1": 0, "Y0": 0, "Y1": 20, "B.C": 2, "Temp": 300.0},
+        {"X0": 32, "X1": 32, "Y0": 0, "Y1": 20, "B.C": 2, "Temp": 300.0},
+        {"X0": 0, "X1": 32, "Y0": 0, "Y1": 0, "B.C": 1, "Temp": 300.0},
+        {"X0": 0, "X1": 32, "Y0": 20, "Y1": 20, "B.C": 1, "Temp": 300.0},
+    ]
+    return d
+
+
+DECKS = {
+    "ar_17x9": (ccp_deck(17, 9, 0.005, 0.0025, ppc=10), 12345),
+    "ar_33x17": (ccp_deck(33, 17, 0.01, 0.005, ppc=20, pressure_torr=0.1, voltage=200.0), 777),
+    "ar_block_33x21": (block_deck(), 4242),
+}
+
+
+def dump(name, deck, seed):
+    exe = os.path.join(REPO, "oracle", "_ref", "ref_dump")
+    if not os.path.exists(exe):
+        subprocess.run(["make", "-C", os.path.join(REPO, "oracle"), "ref"], check=True)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "deck.json")
+        with open(path, "w") as f:
+            json.dump(deck, f)
+        out = os.path.join(tmp, "out")
+        os.makedirs(out)
+        subprocess.run([exe, path, str(seed), out], check=True, stdout=subprocess.DEVNULL)
+        meta = dict(line.split() for line in open(os.path.join(out, "meta.txt")))
+        arrs = {}
+        for fn in os.listdir(out):
+            if not fn.endswith(".bin"):
+                continue
+            key = fn[:-4]
+            if key == "gga":
+                g = np.fromfile(os.path.join(out, fn), dtype=GGA)
+                for field in GGA.names:
+                    arrs["gga_" + field] = g[field]
+                continue
+            dt = np.int32 if key in ("sidx", "aidx", "ai", "aj") or key.endswith("_cell") else np.float32
+            arrs[key] = np.fromfile(os.path.join(out, fn), dtype=dt)
+        np.savez_compressed(os.path.join(HERE, f"setup_{name}.npz"), deck=json.dumps(deck), seed=seed,
+                            meta=json.dumps(meta), **arrs)
+
+
+if __name__ == "__main__":
+    for name, (deck, seed) in DECKS.items():
+        dump(name, deck, seed)
+        print("wrote", name)

@@ -1,0 +1,188 @@
+"""GPU operators vs. the CPU oracle, through the C ABI.
+
+The oracle evaluates the same single-precision arithmetic in the same order
+(including the warp and cluster reduction trees), so every operator is
+compared bit for bit: positions, velocities, cell counts, mover codes,
+collision channels, created particles, densities, potentials and fields.
+"""
+import numpy as np
+import pytest
+
+import hpic
+import oracle
+from hpic.decks import ccp_deck
+
+pytestmark = pytest.mark.gpu
+
+
+def bits(a):
+    a = np.ascontiguousarray(a)
+    return a.view(np.uint32 if a.dtype.itemsize == 4 else np.uint64)
+
+
+def same(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return a.shape == b.shape and np.array_equal(bits(a), bits(b))
+
+
+DECKS = {
+    "ar_17x9": (ccp_deck(17, 9, 0.005, 0.0025, ppc=10), 12345),
+    "ar_33x17_hv": (ccp_deck(33, 17, 0.01, 0.005, ppc=20, pressure_torr=0.1, voltage=300.0), 777),
+    "ar_65x33": (ccp_deck(65, 33, 0.02, 0.01, ppc=30), 99),
+}
+
+
+def pair(name, field_mode=0):
+    deck, seed = DECKS[name]
+    S = hpic.Setup(deck, seed=seed, field_mode=field_mode)
+    case = hpic.Case(setup=S, seed=seed, field_mode=field_mode)
+    info = case.info
+    o = oracle.Oracle(S.table, S.info, case.opts, 32, pcg_cluster=info.pcg_cluster, pcg_block=info.pcg_block)
+    for s in range(S.info.nsp):
+        counts, arrs = S.particles(s, layout=0)
+        o.set_particles(s, counts, *arrs)
+    o.Deposit()  # the library's initial Deposit_Basic
+    return case, o
+
+
+def check_particles(case, o, what=""):
+    for s in range(case.info.nsp):
+        gc, ga = case.particles(s)
+        oc, oa = o.particles(s)
+        assert np.array_equal(gc, oc), f"{what} species {s}: counts differ"
+        for k, (a, b) in enumerate(zip(ga, oa)):
+            assert same(a, b), f"{what} species {s}: component {k} differs"
+
+
+def check_grids(case, o, names=("DEN", "SOURCE"), what=""):
+    for n in names:
+        g = case.grid(n)
+        r = o.grid(n)
+        assert same(g, r), f"{what}: grid {n} differs (max |d| {np.abs(g.astype(np.float64) - r).max()})"
+
+
+@pytest.mark.parametrize("name", list(DECKS))
+def test_initial_deposit(name):
+    case, o = pair(name)
+    check_grids(case, o, ("DEN", "SOURCE"), "initial deposit")
+    g = case.grid("PCG_B")
+    assert same(g, o.grid("B"))
+
+
+@pytest.mark.parametrize("name", list(DECKS))
+@pytest.mark.parametrize("mode", [0, 1])
+def test_field(name, mode):
+    case, o = pair(name, field_mode=mode)
+    case.set_tstep(1)
+    case.Field()
+    o.Field(1)
+    for n in ("PHI_POIS", "PHI", "EX", "EY"):
+        assert same(case.grid(n), o.grid(n)), n
+    assert case.pcg_iters()[0] == o.counters()[2][0]
+    assert case.status() == 0
+
+
+@pytest.mark.parametrize("name", list(DECKS))
+def test_move_and_sort(name):
+    case, o = pair(name)
+    case.set_tstep(1)
+    case.Field()
+    o.Field(1)
+    case.Move()
+    o.Move()
+    check_particles(case, o, "after Move (stayers)")
+    for s in range(case.info.nsp):
+        gc, ga, gcode = case.movers(s)
+        oc, oa, ocode = o.movers(s)
+        assert np.array_equal(gc, oc)
+        assert np.array_equal(gcode, ocode)
+        for a, b in zip(ga, oa):
+            assert same(a, b)
+    case.SortBoundary()
+    o.SortBoundary()
+    check_particles(case, o, "after SortBoundary")
+    assert same(case.grid("COND_CHARGE"), o.counters()[0][: case.info.nsp * case.info.cond_numr])
+
+
+@pytest.mark.parametrize("name", list(DECKS))
+def test_mcc(name):
+    case, o = pair(name)
+    for t in (1, 2, 3):
+        case.set_tstep(t)
+        case.MCC()
+        o.MCC(t)
+        check_particles(case, o, f"after MCC step {t}")
+    assert np.array_equal(case.grid("MCC_COUNT"), o.counters()[1])
+    assert case.grid("MCC_COUNT").reshape(-1, 8).sum() > 0
+
+
+@pytest.mark.parametrize("name", list(DECKS))
+@pytest.mark.parametrize("mode", [0, 1])
+def test_steps_bit_exact(name, mode):
+    case, o = pair(name, field_mode=mode)
+    n = 25
+    case.step(n)
+    o.run(0, n, accumulate=True)
+    check_particles(case, o, f"after {n} steps")
+    check_grids(case, o, ("DEN", "SOURCE"), "after steps")
+    for g in ("PHI", "EX", "EY"):
+        assert same(case.grid(g), o.grid(g)), g
+    assert np.array_equal(case.grid("MCC_COUNT"), o.counters()[1])
+    d, p, cnt = o.averages()
+    assert case.average_count() == cnt == n
+    assert same(case.grid("AVE_DEN"), d)
+    assert same(case.grid("AVE_PHI"), p)
+    assert case.status() == 0
+    assert case.tstep() == n
+
+
+def test_graph_replay_matches_operator_calls():
+    deck, seed = DECKS["ar_33x17_hv"]
+    a = hpic.Case(deck, seed=seed)
+    b = hpic.Case(deck, seed=seed)
+    a.step(6)
+    for t in range(1, 7):
+        b.set_tstep(t)
+        b.Field(); b.Move(); b.SortBoundary(); b.MCC(); b.Deposit()
+    for s in range(2):
+        ca, pa = a.particles(s)
+        cb, pb = b.particles(s)
+        assert np.array_equal(ca, cb)
+        for x, y in zip(pa, pb):
+            assert same(x, y)
+
+
+def test_batch_equals_alone():
+    """A case advanced inside a batch gives the same bits as alone."""
+    decks = [DECKS["ar_17x9"], DECKS["ar_33x17_hv"], DECKS["ar_65x33"]]
+    alone = []
+    for deck, seed in decks:
+        c = hpic.Case(deck, seed=seed)
+        c.step(10)
+        alone.append(c)
+    mixed = [hpic.Case(deck, seed=seed) for deck, seed in decks]
+    b = hpic.Batch(mixed)
+    b.step(10)
+    b.close()
+    for a, m in zip(alone, mixed):
+        for s in range(2):
+            ca, pa = a.particles(s)
+            cm, pm = m.particles(s)
+            assert np.array_equal(ca, cm)
+            for x, y in zip(pa, pm):
+                assert same(x, y)
+        assert same(a.grid("PHI"), m.grid("PHI"))
+
+
+def test_rng_matches_curand_philox(tmp_path):
+    """hp_rng.h's Philox4x32-10 against curand's (device API) on the same key
+    and counter (tests/philox_check.cu)."""
+    import os
+    import subprocess
+    here = os.path.dirname(os.path.abspath(__file__))
+    exe = str(tmp_path / "philox_check")
+    subprocess.run(["nvcc", "-gencode", "arch=compute_100a,code=sm_100a", "-O2", "-I",
+                    os.path.join(here, "..", "include"), os.path.join(here, "philox_check.cu"), "-o", exe],
+                   check=True)
+    out = subprocess.run([exe], capture_output=True, text=True).stdout
+    assert "mismatches 0 host-vs-device 0" in out, out
