@@ -255,6 +255,7 @@ __device__ __forceinline__ float xsec_lookup(const DevCase &d, int ch, float eng
     const float ee1 = d.idlogx * (lengy - xe0);
     int ee2 = (int)ee1;
     if (ee2 > d.n_logx - 2) ee2 = d.n_logx - 2;
+    if (ee2 < 0) ee2 = 0; // NaN energy: keep the read inside the table
     const float a1 = ee1 - ee2;
     const float a2 = 1 - a1;
     return a2 * t[ee2 * W + 2 + ch] + a1 * t[(ee2 + 1) * W + 2 + ch];
@@ -818,6 +819,8 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
         d.pcg_iters[1] = outer;
         if (bad) atomicOr(d.status, ST_NONFINITE);
     }
+    // no CTA may leave while another can still read its shared memory
+    cl.sync();
 }
 
 // Efield_cuda_Basic potential assembly (src/cuda_Field.cu:9-34):

@@ -352,6 +352,7 @@ template <class R> struct Sim : SimBase {
         const R ee1 = (R)c.idlogx * (lengy - xe0);
         int ee2 = (int)ee1;
         if (ee2 > c.n_logx - 2) ee2 = c.n_logx - 2;
+        if (ee2 < 0) ee2 = 0;
         const R a1 = ee1 - ee2;
         const R a2 = 1 - a1;
         return a2 * (R)t[ee2 * W + 2 + ch] + a1 * (R)t[(ee2 + 1) * W + 2 + ch];
