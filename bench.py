@@ -1,0 +1,330 @@
+"""Benchmark: particle-pushes/s of the PIC/MCC step on B200.
+
+One step = Field (Poisson solve + E), Move, SortBoundary, MCC, Deposit for
+every particle of the case; one particle-push = one particle advanced through
+one step.  Default workload (N=1): the single large Ar case of the precision
+form, 513x257 nodes (16 cm x 8 cm), 200 macro-particles per cell per species
+(about 26M electrons + 26M Ar+), 100 V at 13.56 MHz, 50 mTorr, FP32
+particles, FP64 charge grid and FP64-refined field solve (field_mode 2).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank advances its own replica of the case (one case does
+not shard: replicas only); value = pushes of all ranks / max rank time.
+`--impl reference` times the CPU restatement of the step (the reference has
+no CPU step of its own) on this host's cores, on the same workload.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(REPO, "hybrid-final_b200")
+sys.path.insert(0, PKG)
+
+METRIC = "particle-pushes/s batched vs plain at ≤1% FP64 error; p50/p99 case latency"
+UNIT = "particle-pushes/s"
+MOVE_BYTES_PER_PARTICLE = 40  # Move: read x, y, vx, vy, vz (20 B) + write them back (20 B)
+
+WORKLOADS = {
+    "ar_513x257_200ppc": dict(ngx=513, ngy=257, xlen=0.16, ylen=0.08, ppc=200, voltage=100.0, pressure=0.05),
+    "ar_257x129_200ppc": dict(ngx=257, ngy=129, xlen=0.08, ylen=0.04, ppc=200, voltage=100.0, pressure=0.05),
+    "ar_129x65_50ppc": dict(ngx=129, ngy=65, xlen=0.04, ylen=0.02, ppc=50, voltage=100.0, pressure=0.05),
+}
+
+
+def make_deck(w):
+    from hpic.decks import ccp_deck
+    return ccp_deck(w["ngx"], w["ngy"], w["xlen"], w["ylen"], ppc=w["ppc"], voltage=w["voltage"],
+                    pressure_torr=w["pressure"])
+
+
+def launches_per_step(case):
+    """Kernels of one graph-captured step (counted from the launch sequence in
+    hybrid-final_b200/csrc/capi.cu one_step and kernels.cu launch_field)."""
+    mode = case.info.field_mode
+    field = (3 * 5 + 1) if mode == 2 else 1  # refinement passes (resid + 4 GEMMs) + final, or one PCG
+    return 1 + field + 2 + 1 + 1 + 1 + 2 + 1  # advance, field, potential+E, move, sort, mcc, deposit x2, accumulate
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.gpu), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for k, n in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(n)
+        med = float(np.median(sm)) if sm else None
+        return {"sm_mhz": med, "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_init(n_gpus):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as td
+        torch.cuda.set_device(local)
+        td.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+        dist = td
+    return rank, world, local, dist
+
+
+def allreduce(dist, v, op):
+    if dist is None:
+        return v
+    import torch
+    t = torch.tensor([float(v)], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def move_traffic(workload):
+    """dram bytes per k_move launch from the committed ncu summary, if any."""
+    path = os.path.join(REPO, "profiles", f"k_move_{workload}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch_full_case:"):
+            return float(line.split(":")[1].split()[0])
+    return None
+
+
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d["hbm_gbs"], "measured"
+    return 6650.0, "fallback"
+
+
+def cpu_baseline(setup, case_opts, budget_s=20.0):
+    """The CPU restatement (oracle, FP32 form) on this host: a bounded number
+    of full steps of the same case."""
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    o = oracle.Oracle(setup.table, setup.info, case_opts, 32, field_mode=case_opts.field_mode)
+    for s in range(setup.info.nsp):
+        counts, arrs = setup.particles(s, layout=0)
+        o.set_particles(s, counts, *arrs)
+    o.Deposit()
+    pushes, t_used, steps = 0, 0.0, 0
+    while steps < 1 or (t_used < budget_s and steps < 20):
+        n = sum(int(oracle.lib().or_num_particles(o.h, s)) for s in range(setup.info.nsp))
+        t0 = time.perf_counter()
+        o.run(steps, 1, accumulate=False)
+        t_used += time.perf_counter() - t0
+        pushes += n
+        steps += 1
+        if t_used > budget_s:
+            break
+    return dict(value=pushes / t_used, unit=UNIT, cores=int(oracle.lib().or_num_threads()), kind="port",
+                sample=f"{steps} full step(s) of the same case ({pushes} particle-pushes) on the host, "
+                       f"CPU restatement in FP32, {t_used:.1f} s")
+
+
+def run_ours(args, rank, world, local, dist):
+    import torch
+
+    import hpic
+    torch.cuda.set_device(local)
+    w = WORKLOADS[args.workload]
+    deck = make_deck(w)
+    seed = 1000 + rank
+    setup = hpic.Setup(deck, seed=seed, field_mode=args.field_mode)
+    case = hpic.Case(setup=setup, seed=seed, field_mode=args.field_mode, device=local)
+    stream = torch.cuda.current_stream().cuda_stream
+    # warm-up (graph capture happens on the first call)
+    case.step(args.warmup, stream)
+    torch.cuda.synchronize()
+    p0 = case.pushes()
+    clocks = ClockSampler(local)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    case.step(args.steps, stream)
+    e1.record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    pushes = case.pushes() - p0
+    ms_max = allreduce(dist, ms, "max")
+    pushes_all = allreduce(dist, pushes, "sum")
+    status = case.status()
+    resid = case.field_residual()
+
+    # per-operator breakdown (CUDA events on the launching stream), for the roofline
+    ops = {"Field": case.Field, "Move": case.Move, "SortBoundary": case.SortBoundary, "MCC": case.MCC,
+           "Deposit": case.Deposit}
+    reps = 3
+    op_ms = {k: 0.0 for k in ops}
+    move_particles = 0
+    t = case.tstep()
+    for r in range(reps):
+        case.set_tstep(t + r + 1)
+        for name, fn in ops.items():
+            if name == "Move":
+                move_particles += sum(case.particles_count(s) for s in range(case.info.nsp))
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            fn(stream)
+            b.record()
+            torch.cuda.synchronize()
+            op_ms[name] += a.elapsed_time(b) / reps
+    move_bytes = MOVE_BYTES_PER_PARTICLE * move_particles / reps
+    peak, peak_kind = peaks()
+    achieved = move_bytes / (op_ms["Move"] * 1e-3) / 1e9
+    traffic = move_traffic(args.workload)
+
+    # end to end through the C ABI with host buffers: the initial particle
+    # state comes from pinned host memory, K steps run, the time-averaged
+    # densities and potential come back to host memory
+    pinned = []
+    for s in range(setup.info.nsp):
+        counts, arrs = setup.particles(s, layout=0)
+        parr = [torch.from_numpy(a).pin_memory() for a in arrs]
+        pinned.append((counts, parr))
+    G, nsp = case.info.Gsize, case.info.nsp
+    out_den = torch.empty(nsp * G, dtype=torch.float64).pin_memory()
+    out_phi = torch.empty(G, dtype=torch.float64).pin_memory()
+    h2d = sum(sum(a.numel() * 4 for a in parr) + counts.nbytes for counts, parr in pinned)
+    d2h = out_den.numel() * 8 + out_phi.numel() * 8
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    pe0 = case.pushes()
+    for s, (counts, parr) in enumerate(pinned):
+        hpic._check(hpic.lib().hp_set_particles(case.h, s, counts.ctypes.data_as(hpic._I),
+                                                *[hpic.C.cast(a.data_ptr(), hpic._F) for a in parr]))
+    case.reset_averages()
+    case.step(args.steps, stream)
+    hpic.lib().hp_get_grid(case.h, hpic.GRID["AVE_DEN"], hpic.C.c_void_p(out_den.data_ptr()), d2h)
+    hpic.lib().hp_get_grid(case.h, hpic.GRID["AVE_PHI"], hpic.C.c_void_p(out_phi.data_ptr()), out_phi.numel() * 8)
+    f1.record()
+    torch.cuda.synchronize()
+    e2e_ms = allreduce(dist, f0.elapsed_time(f1), "max")
+    e2e_pushes = allreduce(dist, case.pushes() - pe0, "sum")
+
+    result = dict(
+        metric=METRIC, value=pushes_all / (ms_max * 1e-3), unit=UNIT, n_gpus=world, steps=args.steps,
+        warmup=args.warmup, ms_per_step=ms_max / args.steps, higher_is_better=True, scaling="weak",
+        vs_baseline=None, dtype="f32 particles / f64 charge and field refinement", data="synthetic",
+        config=dict(workload=args.workload, nodes=f"{w['ngx']}x{w['ngy']}", ppc_per_species=w["ppc"],
+                    particles=int(sum(case.particles_count(s) for s in range(nsp))),
+                    gas="Ar", pressure_torr=w["pressure"], rf_voltage=w["voltage"], field_mode=case.info.field_mode,
+                    parallelism=f"replicas x{world}", l2="state (>4 GB) larger than L2: no flush needed",
+                    field_relative_residual=resid, device_status=status),
+        e2e=dict(value=e2e_pushes / (e2e_ms * 1e-3), unit=UNIT, h2d_bytes_per_step=h2d / args.steps,
+                 d2h_bytes_per_step=d2h / args.steps),
+        roofline=dict(bound="hbm", kernel="k_move", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
+                      peak_source=peak_kind, traffic=traffic, algorithmic_bytes_per_launch=move_bytes),
+        op_ms=op_ms,
+        gpu_launches=launches_per_step(case) * args.steps,
+        clocks=clk,
+    )
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(setup, case.opts)
+    return result
+
+
+def run_reference(args):
+    """CPU restatement of the step on this host (all its cores), same workload."""
+    import hpic
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    w = WORKLOADS[args.workload]
+    setup = hpic.Setup(make_deck(w), seed=1000, field_mode=args.field_mode)
+    budget = float(os.environ.get("HPIC_REF_BUDGET_S", "90"))
+    cb = cpu_baseline(setup, setup.opts, budget_s=budget)
+    return dict(metric=METRIC, value=cb["value"], unit=UNIT, n_gpus=int(os.environ.get("WORLD_SIZE", "1")),
+                steps=args.steps, warmup=args.warmup, higher_is_better=True, scaling="weak", vs_baseline=None,
+                dtype="f32", data="synthetic", impl="reference",
+                config=dict(workload=args.workload, nodes=f"{w['ngx']}x{w['ngy']}", ppc_per_species=w["ppc"]),
+                cpu_baseline=dict(kind=cb["kind"], cores=cb["cores"], sample=cb["sample"], value=cb["value"],
+                                  unit=UNIT),
+                e2e=dict(value=cb["value"], unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="ar_513x257_200ppc", choices=list(WORKLOADS))
+    ap.add_argument("--field-mode", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    rank = int(os.environ.get("RANK", "0"))
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(run_reference(args)), flush=True)
+        return
+    rank, world, local, dist = dist_init(args.gpus)
+    res = run_ours(args, rank, world, local, dist)
+    if rank == 0:
+        print(json.dumps(res), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -65,11 +65,23 @@ hp_status batch_dev_build(hp_case *const *cases, int n, BatchDev &b) {
         for (int k = 0; k <= m; k++) {
             b.list_off[m][k] = (int)lists.size();
             for (int i = 0; i < n; i++) {
+                if (cases[i]->h.field_mode == 2) continue; // separable inner solve, not PCG
                 int cs = std::min(pcg_cluster_for_nodes(cases[i]->s.Gsize), 1 << m);
                 if (cs == (1 << k)) lists.push_back(i);
             }
             b.list_n[m][k] = (int)lists.size() - b.list_off[m][k];
         }
+    {
+        std::vector<int> fidx;
+        std::vector<hp_case *> fc;
+        for (int i = 0; i < n; i++)
+            if (cases[i]->h.field_mode == 2) {
+                fidx.push_back(i);
+                fc.push_back(cases[i]);
+            }
+        hp_status fs = fast_plan_build(fc.data(), fidx, b.fast);
+        if (fs != HP_OK) return fs;
+    }
     CK(cudaMalloc(&b.d_lists, sizeof(int) * std::max<size_t>(lists.size(), 1)));
     if (!lists.empty())
         CK(cudaMemcpy(b.d_lists, lists.data(), sizeof(int) * lists.size(), cudaMemcpyHostToDevice));
@@ -91,6 +103,7 @@ void batch_dev_free(BatchDev &b) {
     cudaFree(b.d_cell);
     cudaFree(b.d_node);
     cudaFree(b.d_lists);
+    fast_plan_free(b.fast);
     b = BatchDev();
 }
 
@@ -98,7 +111,7 @@ hp_status run_step(const BatchDev &b, const LaunchCfg &lc, int gas, cudaStream_t
     if (gas != GAS_AR) return set_error("MCC for this gas is not built"), HP_ERR_UNSUPPORTED;
     CK(launch_advance(b.d_cases, b.n, st));
     const std::vector<PcgGroup> g = b.groups(lc.pcg_cluster_max, lc.pcg_block);
-    CK(launch_field(b.d_cases, b.d_node, b.n, b.n_node, g.data(), (int)g.size(), st));
+    CK(launch_field(b.d_cases, b.d_node, b.n, b.n_node, g.data(), (int)g.size(), &b.fast.plan, st));
     CK(launch_move(b.d_cases, b.d_part, b.n, b.n_part, lc, st));
     CK(launch_sort(b.d_cases, b.d_part, b.n, b.n_part, lc, st));
     CK(launch_mcc_ar(b.d_cases, b.d_cell, b.n, b.n_cell, lc, st));

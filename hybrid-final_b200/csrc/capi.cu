@@ -23,6 +23,58 @@ hp_status cuda_fail(cudaError_t e, const char *what) {
     return HP_ERR_CUDA;
 }
 
+hp_status fast_plan_build(hp_case *const *cases, const std::vector<int> &idx, FastPlanDev &out) {
+    out = FastPlanDev();
+    const int n = (int)idx.size();
+    if (n == 0) return HP_OK;
+    std::vector<int> items(n + 1, 0);
+    std::vector<GemmProb> st[4];
+    int tiles[4] = {0, 0, 0, 0};
+    for (int q = 0; q < n; q++) {
+        const hp::DevCase &h = cases[q]->h;
+        const int nx = h.fs_nx, ny = h.fs_ny;
+        items[q + 1] = items[q] + nx * ny;
+        const int tn = (nx + 63) / 64, tm = (ny + 63) / 64;
+        GemmProb g[4];
+        std::memset(g, 0, sizeof g);
+        // A1 = X V ; Y = (W^T A1) .* inv ; A2 = Y V^T ; x64 += W A2
+        g[0] = GemmProb{ny, nx, nx, h.fs_x, h.fs_V, h.fs_a1, nullptr, nullptr, 0, 0, 0, 0, tn, 0};
+        g[1] = GemmProb{ny, nx, ny, h.fs_Wt, h.fs_a1, h.fs_y, h.fs_inv, nullptr, 0, 0, 0, 1, tn, 0};
+        g[2] = GemmProb{ny, nx, nx, h.fs_y, h.fs_Vt, h.fs_a1, nullptr, nullptr, 0, 0, 0, 0, tn, 0};
+        g[3] = GemmProb{ny, nx, ny, h.fs_W, h.fs_a1, nullptr, nullptr, h.x64, h.ngy, h.fs_i0, h.fs_j0, 2, tn, 0};
+        for (int k = 0; k < 4; k++) {
+            g[k].tile_start = tiles[k];
+            tiles[k] += tm * tn;
+            st[k].push_back(g[k]);
+        }
+    }
+    cudaError_t e;
+    if ((e = cudaMalloc(&out.d_list, sizeof(int) * n)) != cudaSuccess) return cuda_fail(e, "fast plan");
+    if ((e = cudaMalloc(&out.d_items, sizeof(int) * (n + 1))) != cudaSuccess) return cuda_fail(e, "fast plan");
+    if ((e = cudaMalloc(&out.d_probs, sizeof(GemmProb) * 4 * n)) != cudaSuccess) return cuda_fail(e, "fast plan");
+    cudaMemcpy(out.d_list, idx.data(), sizeof(int) * n, cudaMemcpyHostToDevice);
+    cudaMemcpy(out.d_items, items.data(), sizeof(int) * (n + 1), cudaMemcpyHostToDevice);
+    for (int k = 0; k < 4; k++) {
+        e = cudaMemcpy(out.d_probs + (size_t)k * n, st[k].data(), sizeof(GemmProb) * n, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return cuda_fail(e, "fast plan");
+        out.plan.probs[k] = out.d_probs + (size_t)k * n;
+        out.plan.ntiles[k] = tiles[k];
+    }
+    out.plan.list = out.d_list;
+    out.plan.item_start = out.d_items;
+    out.plan.n = n;
+    out.plan.items = items[n];
+    out.plan.passes = cases[0]->h.fs_passes > 0 ? cases[0]->h.fs_passes : 3;
+    return HP_OK;
+}
+
+void fast_plan_free(FastPlanDev &f) {
+    cudaFree(f.d_list);
+    cudaFree(f.d_items);
+    cudaFree(f.d_probs);
+    f = FastPlanDev();
+}
+
 } // namespace hpi
 
 using hpi::cuda_fail;
@@ -129,35 +181,40 @@ template <class T> hp_status dupload(hp_case *c, T **p, const std::vector<T> &v)
         if (s_ != HP_OK) return s_;                                                                                    \
     } while (0)
 
+// Counts per cell and CSR arrays from the host: the arrays go to the device
+// as they are (one copy each) and a kernel files them into the slot pool.
 hp_status upload_particles(hp_case *c, int isp, const int *counts, const float *x, const float *y, const float *vx,
                            const float *vy, const float *vz) {
     const Setup &s = c->s;
     const int C = s.Csize, cap = c->h.sp[isp].cap;
-    std::vector<float> bx((size_t)C * cap, 0.0f), by(bx.size(), 0.0f), bvx(bx.size(), 0.0f), bvy(bx.size(), 0.0f),
-        bvz(bx.size(), 0.0f);
-    std::vector<int> cnt(C, 0);
-    size_t q = 0;
+    std::vector<int> start(C + 1, 0);
     for (int cell = 0; cell < C; cell++) {
-        int n = counts[cell];
-        if (n < 0 || n > cap) {
-            set_error("cell " + std::to_string(cell) + " holds " + std::to_string(n) + " particles, slot pool is " +
-                      std::to_string(cap));
+        const int n = counts[cell];
+        if (n < 0 || 2 * n > cap) {
+            set_error("cell " + std::to_string(cell) + " holds " + std::to_string(n) +
+                      " particles; the slot pool takes at most " + std::to_string(cap / 2));
             return HP_ERR_CAPACITY;
         }
-        cnt[cell] = n;
-        for (int k = 0; k < n; k++, q++) {
-            size_t d = (size_t)cell * cap + k;
-            bx[d] = x[q]; by[d] = y[q]; bvx[d] = vx[q]; bvy[d] = vy[q]; bvz[d] = vz[q];
-        }
+        start[cell + 1] = start[cell] + n;
     }
-    DevSpecies &sp = c->h.sp[isp];
-    CK(cudaMemcpy(sp.x, bx.data(), bx.size() * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(sp.y, by.data(), by.size() * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(sp.vx, bvx.data(), bvx.size() * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(sp.vy, bvy.data(), bvy.size() * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(sp.vz, bvz.data(), bvz.size() * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(sp.cnt, cnt.data(), (size_t)C * 4, cudaMemcpyHostToDevice));
-    CK(cudaMemset(sp.nmov, 0, (size_t)C * 4));
+    const size_t total = (size_t)start[C];
+    int *d_start = nullptr;
+    float *d_src = nullptr;
+    CK(cudaMalloc(&d_start, sizeof(int) * (size_t)(C + 1)));
+    cudaError_t e = cudaMalloc(&d_src, sizeof(float) * std::max<size_t>(5 * total, 1));
+    if (e != cudaSuccess) {
+        cudaFree(d_start);
+        return cuda_fail(e, "cudaMalloc (particle upload)");
+    }
+    const float *arr[5] = {x, y, vx, vy, vz};
+    e = cudaMemcpy(d_start, start.data(), sizeof(int) * (size_t)(C + 1), cudaMemcpyHostToDevice);
+    for (int a = 0; a < 5 && e == cudaSuccess && total; a++)
+        e = cudaMemcpy(d_src + (size_t)a * total, arr[a], sizeof(float) * total, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = launch_scatter(c->h.sp[isp], C, d_start, d_src, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    cudaFree(d_start);
+    cudaFree(d_src);
+    if (e != cudaSuccess) return cuda_fail(e, "particle upload");
     return HP_OK;
 }
 
@@ -255,7 +312,27 @@ hp_status build_device(hp_case *c) {
     TRY(dalloc(c, &h.mcc_count, (size_t)8 * C));
     TRY(dalloc(c, &h.pcg_iters, 2));
     TRY(dalloc(c, &h.ave_count, 1));
+    TRY(dalloc(c, &h.pushes, 32));
     h.field_mode = c->opts.field_mode;
+    if (h.field_mode == 2) {
+        // separable inner solve when the operator allows it, else mode 1
+        if (build_fast_solver(s, c->fs)) {
+            const size_t nxy = (size_t)c->fs.nx * c->fs.ny;
+            h.fs_i0 = c->fs.i0; h.fs_j0 = c->fs.j0; h.fs_nx = c->fs.nx; h.fs_ny = c->fs.ny;
+            h.fs_passes = c->fs_passes;
+            TRY(dupload(c, (float **)&h.fs_V, c->fs.V));
+            TRY(dupload(c, (float **)&h.fs_Vt, c->fs.Vt));
+            TRY(dupload(c, (float **)&h.fs_W, c->fs.W));
+            TRY(dupload(c, (float **)&h.fs_Wt, c->fs.Wt));
+            TRY(dupload(c, (float **)&h.fs_inv, c->fs.inv_eig));
+            TRY(dalloc(c, &h.fs_x, nxy));
+            TRY(dalloc(c, &h.fs_a1, nxy));
+            TRY(dalloc(c, &h.fs_y, nxy));
+            TRY(dalloc(c, &h.fs_res, 2));
+        } else {
+            h.field_mode = 1;
+        }
+    }
     h.pcg_max_iter = c->opts.pcg_max_iter > 0 ? c->opts.pcg_max_iter : 100000;
     h.pcg_tol2 = s.PCGtol2;
     h.pcg_rtol = c->opts.pcg_rtol > 0 ? c->opts.pcg_rtol : 1e-8;
@@ -270,6 +347,10 @@ hp_status build_device(hp_case *c) {
         TRY(upload_particles(c, isp, s.p_count[isp].data(), s.p_x[isp].data(), s.p_y[isp].data(), s.p_vx[isp].data(),
                              s.p_vy[isp].data(), s.p_vz[isp].data()));
     c->pcg_cluster = pcg_cluster_for_nodes(G);
+    if (h.field_mode == 2) {
+        hp_case *one[1] = {c};
+        TRY(hpi::fast_plan_build(one, std::vector<int>{0}, c->fplan));
+    }
     return HP_OK;
 }
 
@@ -278,7 +359,9 @@ cudaStream_t as_stream(void *s) { return (cudaStream_t)s; }
 
 hp_status op_field(hp_case *c, cudaStream_t st) {
     PcgGroup g{c->pcg_cluster, c->lc.pcg_block, c->d_list0, 1};
-    cudaError_t e = launch_field(c->d_case, c->d_items + 4, 1, c->s.Gsize, &g, 1, st);
+    const bool fast = c->h.field_mode == 2;
+    cudaError_t e = launch_field(c->d_case, c->d_items + 4, 1, c->s.Gsize, &g, fast ? 0 : 1,
+                                 fast ? &c->fplan.plan : nullptr, st);
     return e == cudaSuccess ? HP_OK : cuda_fail(e, "field");
 }
 hp_status op_move(hp_case *c, cudaStream_t st) {
@@ -384,8 +467,8 @@ hp_status hp_setup_get_particles(const hp_setup *su, int isp, int layout, int *c
     return HP_OK;
 }
 
-static hp_status table_of(const Setup &s, const std::vector<float> *prob, int what, void *out, size_t bytes,
-                          size_t *needed) {
+static hp_status table_of(const Setup &s, const std::vector<float> *prob, const FastSolver *fs, int what, void *out,
+                          size_t bytes, size_t *needed) {
     const void *src = nullptr;
     size_t nb = 0;
     std::vector<float> tmpf;
@@ -449,6 +532,16 @@ static hp_status table_of(const Setup &s, const std::vector<float> *prob, int wh
         for (int k = 0; k < s.cond_numr; k++) tmpf.push_back((float)s.efield_flag[k]);
         src = tmpf.data(); nb = tmpf.size() * 4; break;
     case 32: src = s.unk_node.data(); nb = s.unk_node.size() * 4; break;
+    // separable inverse of field_mode 2: 33 int[6] {ok, i0, j0, nx, ny, 0};
+    // 34 V, 35 V^T (nx*nx); 36 W, 37 W^T (ny*ny); 38 1/(lambda_i+theta_j) (ny*nx)
+    case 33:
+        tmpi = {fs && fs->ok ? 1 : 0, fs ? fs->i0 : 0, fs ? fs->j0 : 0, fs ? fs->nx : 0, fs ? fs->ny : 0, 0};
+        src = tmpi.data(); nb = tmpi.size() * 4; break;
+    case 34: if (fs) { src = fs->V.data(); nb = fs->V.size() * 4; } break;
+    case 35: if (fs) { src = fs->Vt.data(); nb = fs->Vt.size() * 4; } break;
+    case 36: if (fs) { src = fs->W.data(); nb = fs->W.size() * 4; } break;
+    case 37: if (fs) { src = fs->Wt.data(); nb = fs->Wt.size() * 4; } break;
+    case 38: if (fs) { src = fs->inv_eig.data(); nb = fs->inv_eig.size() * 4; } break;
     default: set_error("unknown table id"); return HP_ERR_ARG;
     }
     if (needed) *needed = nb;
@@ -460,12 +553,21 @@ static hp_status table_of(const Setup &s, const std::vector<float> *prob, int wh
 
 hp_status hp_setup_get_table(const hp_setup *s, int what, void *out, size_t bytes, size_t *needed) {
     if (!s) return HP_ERR_ARG;
-    return table_of(s->s, nullptr, what, out, bytes, needed);
+    if (what >= 33 && what <= 38 && !s->fs_built) {
+        hp_setup *m = const_cast<hp_setup *>(s);
+        try {
+            build_fast_solver(m->s, m->fs);
+        } catch (const std::exception &e) {
+            return from_exception(e);
+        }
+        m->fs_built = true;
+    }
+    return table_of(s->s, nullptr, &s->fs, what, out, bytes, needed);
 }
 
 hp_status hp_get_table(hp_case *c, int what, void *out, size_t bytes, size_t *needed) {
     if (!c) return HP_ERR_ARG;
-    return table_of(c->s, &c->prob, what, out, bytes, needed);
+    return table_of(c->s, &c->prob, &c->fs, what, out, bytes, needed);
 }
 
 static hp_status case_from(const Setup &s, const hp_case_opts *opts, hp_case **out) {
@@ -533,6 +635,7 @@ hp_status hp_case_destroy(hp_case *c) {
     }
     cudaDeviceSynchronize();
     for (void *p : c->allocs) cudaFree(p);
+    hpi::fast_plan_free(c->fplan);
     delete c;
     return HP_OK;
 }
@@ -542,6 +645,7 @@ hp_status hp_case_get_info(const hp_case *c, hp_case_info *out) {
     fill_info(c->s, out);
     out->device_bytes = c->bytes;
     out->pcg_cluster = c->pcg_cluster;
+    out->field_mode = c->h.field_mode;
     out->pcg_block = c->lc.pcg_block;
     int64_t t = 0;
     cudaMemcpy(&t, c->h.tstep, 8, cudaMemcpyDeviceToHost);
@@ -741,6 +845,30 @@ hp_status hp_get_average_count(hp_case *c, int64_t *n) {
     CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(c->last_stream));
     CK(cudaMemcpy(n, c->h.ave_count, 8, cudaMemcpyDeviceToHost));
+    return HP_OK;
+}
+
+hp_status hp_case_pushes(hp_case *c, int64_t *pushes) {
+    if (!c || !pushes) return HP_ERR_ARG;
+    unsigned long long v[32];
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->last_stream));
+    CK(cudaMemcpy(v, c->h.pushes, sizeof v, cudaMemcpyDeviceToHost));
+    int64_t t = 0;
+    for (int k = 0; k < 32; k++) t += (int64_t)v[k];
+    *pushes = t;
+    return HP_OK;
+}
+
+hp_status hp_last_field_residual(hp_case *c, double *rel) {
+    if (!c || !rel) return HP_ERR_ARG;
+    *rel = -1.0;
+    if (c->h.field_mode != 2) return HP_OK;
+    double v[2];
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->last_stream));
+    CK(cudaMemcpy(v, c->h.fs_res, sizeof v, cudaMemcpyDeviceToHost));
+    *rel = v[1] > 0 ? v[0] / v[1] : 0.0;
     return HP_OK;
 }
 

@@ -7,12 +7,25 @@
 
 #include "../../include/hpic.h"
 #include "dev.cuh"
+#include "fastsolve.hpp"
 #include "kernels.cuh"
 #include "setup.hpp"
+
+namespace hpi {
+// Device lists for field_mode 2 over a set of cases (indices into the
+// descriptor array the kernels see).
+struct FastPlanDev {
+    hp::FastPlan plan;
+    int *d_list = nullptr, *d_items = nullptr;
+    hp::GemmProb *d_probs = nullptr;
+};
+} // namespace hpi
 
 struct hp_setup {
     hp::Setup s;
     hp_case_opts opts;
+    bool fs_built = false;
+    hp::FastSolver fs; // built on first request of its tables
 };
 
 struct hp_case {
@@ -30,12 +43,17 @@ struct hp_case {
     hp::LaunchCfg lc;
     int pcg_cluster = 1;           // CTAs of this case's field-solve cluster
     int *d_list0 = nullptr;        // device {0}: the case's index in its own one-case list
+    hp::FastSolver fs;             // field_mode 2: separable inverse (fs.ok false otherwise)
+    int fs_passes = 3;
+    hpi::FastPlanDev fplan;        // its device lists (one-case plan)
     cudaGraphExec_t graph = nullptr;
     hp_batch *batch = nullptr;
     std::vector<float> prob; // [3*C]
 };
 
 namespace hpi {
+hp_status fast_plan_build(hp_case *const *cases, const std::vector<int> &idx, FastPlanDev &out);
+void fast_plan_free(FastPlanDev &f);
 void set_error(const std::string &m);
 hp_status cuda_fail(cudaError_t e, const char *what);
 // Build the per-case prefix arrays and device descriptor array of a batch.
@@ -49,6 +67,7 @@ struct BatchDev {
     int *d_lists = nullptr;
     int list_off[5][5] = {}, list_n[5][5] = {};
     std::vector<hp::PcgGroup> groups(int cluster_max, int block) const;
+    FastPlanDev fast;
 };
 hp_status batch_dev_build(hp_case *const *cases, int n, BatchDev &b);
 void batch_dev_free(BatchDev &b);

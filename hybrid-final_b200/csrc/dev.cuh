@@ -79,6 +79,13 @@ struct DevCase {
     unsigned int *mcc_count;        // [16*nsp]
     int *pcg_iters;                 // [2]: inner, outer of the last solve
     int64_t *ave_count;
+    unsigned long long *pushes;     // [32] particles pushed by Move, spread over 32 counters
+    // separable inner solve (field_mode 2): rectangle of unknowns and scratch
+    int fs_i0, fs_j0, fs_nx, fs_ny, fs_passes;
+    float *fs_x;                    // [ny*nx] residual of the symmetrised system
+    float *fs_a1, *fs_y;            // [ny*nx] products
+    const float *fs_V, *fs_Vt, *fs_W, *fs_Wt, *fs_inv;
+    double *fs_res;                 // [2]: final ||r||, ||b||
     // solver controls
     int field_mode, pcg_max_iter;
     float pcg_tol2;

@@ -62,6 +62,7 @@ __global__ void __launch_bounds__(256) k_move(const DevCase *__restrict__ cases,
         if (lane == 0) sp.nmov[c] = 0;
         return;
     }
+    if (lane == 0) atomicAdd(&d.pushes[warp & 31], (unsigned long long)n);
     const int cap = sp.cap;
     if (2 * n > cap) { // the reference's ReArg condition (src/cuda_Sortboundary.cu:63-65)
         if (lane == 0) {
@@ -1012,6 +1013,29 @@ __global__ void __launch_bounds__(256) k_accumulate(const DevCase *__restrict__ 
     if (n == 0) *d.ave_count += 1;
 }
 
+// CSR particle arrays (cell order, start[c] = first particle of cell c) into
+// the cell-blocked slot pool of one species; one warp per cell.
+__global__ void __launch_bounds__(256) k_scatter(DevSpecies sp, int C, const int *__restrict__ start,
+                                                 const float *__restrict__ src) {
+    const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (warp >= C) return;
+    const int b = start[warp], n = start[warp + 1] - b;
+    const size_t total = (size_t)start[C];
+    const size_t base = (size_t)warp * sp.cap;
+    for (int k = lane; k < n; k += 32) {
+        sp.x[base + k] = src[b + k];
+        sp.y[base + k] = src[total + b + k];
+        sp.vx[base + k] = src[2 * total + b + k];
+        sp.vy[base + k] = src[3 * total + b + k];
+        sp.vz[base + k] = src[4 * total + b + k];
+    }
+    if (lane == 0) {
+        sp.cnt[warp] = n;
+        sp.nmov[warp] = 0;
+    }
+}
+
 inline unsigned blocks_for(long long threads, int per_block) { return (unsigned)((threads + per_block - 1) / per_block); }
 
 } // namespace
@@ -1061,7 +1085,7 @@ int pcg_cluster_for_nodes(int G) {
 }
 
 cudaError_t launch_field(const DevCase *cases, const int *node_items, int ncases, int n_node_items,
-                         const PcgGroup *groups, int ngroups, cudaStream_t st) {
+                         const PcgGroup *groups, int ngroups, const FastPlan *fast, cudaStream_t st) {
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(k_pcg, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
@@ -1085,10 +1109,19 @@ cudaError_t launch_field(const DevCase *cases, const int *node_items, int ncases
         cudaError_t e = cudaLaunchKernelEx(&cfg, k_pcg, cases, pg.list, pg.n);
         if (e != cudaSuccess) return e;
     }
+    if (fast && fast->n > 0) {
+        cudaError_t ef = launch_fast_field(cases, *fast, st);
+        if (ef != cudaSuccess) return ef;
+    }
     k_potential<<<blocks_for(n_node_items, 256), 256, 0, st>>>(cases, node_items, ncases, n_node_items);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_efield<<<blocks_for(n_node_items, 256), 256, 0, st>>>(cases, node_items, ncases, n_node_items);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_scatter(const DevSpecies &sp, int C, const int *start, const float *src, cudaStream_t st) {
+    k_scatter<<<blocks_for((long long)C * 32, 256), 256, 0, st>>>(sp, C, start, src);
     return cudaGetLastError();
 }
 

@@ -39,10 +39,32 @@ struct PcgGroup {
     const int *list;  // device array of case indices
     int n;
 };
+// field_mode 2 (fastsolve.cu): refinement passes with the separable inverse
+struct GemmProb {
+    int M, N, K;
+    const float *A, *B;
+    float *C;
+    const float *S;  // epi 1: elementwise scale of the product
+    double *x64;     // epi 2: x64[(i0 + n) * ngy + (j0 + m)] += product
+    int ngy, i0, j0, epi;
+    int tiles_n, tile_start;
+};
+struct FastPlan {
+    const int *list = nullptr;       // device: case indices
+    const int *item_start = nullptr; // device: prefix of rectangle sizes [n+1]
+    int n = 0, items = 0;
+    const GemmProb *probs[4] = {nullptr, nullptr, nullptr, nullptr}; // device, one list per product
+    int ntiles[4] = {0, 0, 0, 0};
+    int passes = 3;
+};
+cudaError_t launch_fast_field(const DevCase *cases, const FastPlan &fp, cudaStream_t st);
 cudaError_t launch_field(const DevCase *cases, const int *node_items, int ncases, int n_node_items,
-                         const PcgGroup *groups, int ngroups, cudaStream_t st);
+                         const PcgGroup *groups, int ngroups, const FastPlan *fast, cudaStream_t st);
 // CTAs per case for a grid of G nodes
 int pcg_cluster_for_nodes(int G);
+// CSR particles (5 arrays of start[C] floats back to back: x, y, vx, vy, vz)
+// into the cell-blocked slots of one species; sets cnt and clears nmov
+cudaError_t launch_scatter(const DevSpecies &sp, int C, const int *start, const float *src, cudaStream_t st);
 // tstep += 1 for every case (device-side step counter, graph friendly)
 cudaError_t launch_advance(const DevCase *cases, int ncases, cudaStream_t st);
 // running sums of den and phi (N_ave accumulation, src/cuda_Diagnostic.cu:505-547)

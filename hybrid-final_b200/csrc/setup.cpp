@@ -812,9 +812,19 @@ void gas_setting(Setup &s, const BuildOpts &o) { // src/start.c:1999-2051
         std::vector<int> &cnt = s.p_count[isp];
         cnt.assign(s.Csize, 0);
         std::vector<int> cell_of(p.np);
+        // frand() can return exactly 1.0 (seed 2^31-2), which puts a particle
+        // at x = i + 1: the reference then files it under cell i+1, and for
+        // the last column or row that "cell" does not exist (its kernels read
+        // past the grid).  Such a particle stays in the last cell here, with
+        // its offset just below 1.
+        std::vector<float> offx(p.np), offy(p.np);
         for (int k = 0; k < p.np; k++) {
             int XID = (int)hx[k], YID = (int)hy[k];
-            if (XID >= s.ncx || YID >= s.ncy) unsupported("initial particle on the far domain edge");
+            float ox = hx[k] - XID, oy = hy[k] - YID;
+            if (XID >= s.ncx) { XID = s.ncx - 1; ox = 0.99999994f; }
+            if (YID >= s.ncy) { YID = s.ncy - 1; oy = 0.99999994f; }
+            offx[k] = ox;
+            offy[k] = oy;
             cell_of[k] = XID * s.ncy + YID;
             cnt[cell_of[k]]++;
         }
@@ -825,8 +835,8 @@ void gas_setting(Setup &s, const BuildOpts &o) { // src/start.c:1999-2051
         s.p_vx[isp].assign(p.np, 0); s.p_vy[isp].assign(p.np, 0); s.p_vz[isp].assign(p.np, 0);
         for (int k = 0; k < p.np; k++) {
             int d = fill[cell_of[k]]++;
-            s.p_x[isp][d] = hx[k] - (int)hx[k];
-            s.p_y[isp][d] = hy[k] - (int)hy[k];
+            s.p_x[isp][d] = offx[k];
+            s.p_y[isp][d] = offy[k];
             s.p_vx[isp][d] = hvx[k]; s.p_vy[isp][d] = hvy[k]; s.p_vz[isp][d] = hvz[k];
         }
     }

@@ -26,9 +26,10 @@ GRID = dict(EX=0, EY=1, PHI=2, PHI_POIS=3, DEN=4, SOURCE=5, PCG_X=6, PCG_B=7, AV
 TABLE = dict(sidx=0, a_idx=1, boundary=2, face=3, cond_id=4, area=5, back_den1=6, back_vel1=7, lap=8,
              stencil=9, vsave=10, xsec=11, collf=12, sigv=13, dens_region=14, prob=15, eps_r=16,
              back_den2=17, back_vel2=18, a_val=19, ai=20, aj=21, matm=22, cond_b=23, temp_b=24, ta_val=25,
-             species=26, node_temp=27, dep_factor=28, fluid_den=29, scalars=30, sources=31, unk_node=32)
+             species=26, node_temp=27, dep_factor=28, fluid_den=29, scalars=30, sources=31, unk_node=32,
+             fs_info=33, fs_V=34, fs_Vt=35, fs_W=36, fs_Wt=37, fs_inv=38)
 TABLE_DTYPE = {0: np.int32, 1: np.int32, 2: np.int32, 3: np.int32, 4: np.int32, 14: np.int32, 20: np.int32,
-               21: np.int32, 32: np.int32}
+               21: np.int32, 32: np.int32, 33: np.int32}
 
 
 class HpicError(RuntimeError):
@@ -48,7 +49,7 @@ class CaseInfo(C.Structure):
                 ("Csize", C.c_int), ("nsp", C.c_int), ("main_gas", C.c_int), ("cond_numr", C.c_int),
                 ("n_unknowns", C.c_int), ("cap", C.c_int * 8), ("mcc_subcycles", C.c_int), ("dt", C.c_double),
                 ("dx", C.c_double), ("dy", C.c_double), ("tstep", C.c_int64), ("device_bytes", C.c_size_t),
-                ("pcg_cluster", C.c_int), ("pcg_block", C.c_int)]
+                ("pcg_cluster", C.c_int), ("pcg_block", C.c_int), ("field_mode", C.c_int)]
 
 
 class Tune(C.Structure):
@@ -102,6 +103,8 @@ _SIGS = {
     "hp_reset_averages": (C.c_int, [_P]),
     "hp_get_average_count": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "hp_last_pcg_iters": (C.c_int, [_P, _I, _I]),
+    "hp_last_field_residual": (C.c_int, [_P, C.POINTER(C.c_double)]),
+    "hp_case_pushes": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "hp_get_table": (C.c_int, [_P, C.c_int, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
     "hp_batch_create": (C.c_int, [C.POINTER(_P), C.c_int, C.POINTER(_P)]),
     "hp_batch_destroy": (C.c_int, [_P]),
@@ -264,6 +267,16 @@ class Case:
         a, b = C.c_int(0), C.c_int(0)
         _check(lib().hp_last_pcg_iters(self.h, C.byref(a), C.byref(b)))
         return a.value, b.value
+
+    def field_residual(self):
+        r = C.c_double(0)
+        _check(lib().hp_last_field_residual(self.h, C.byref(r)))
+        return r.value
+
+    def pushes(self):
+        n = C.c_int64(0)
+        _check(lib().hp_case_pushes(self.h, C.byref(n)))
+        return n.value
 
     def particles(self, isp):
         n = C.c_size_t(0)

@@ -44,7 +44,7 @@ def ccp_deck(ngx, ngy, xlen, ylen, *, gas="Ar", pressure_torr=0.05, voltage=100.
     dy = ylen / (ngy - 1)
     np2c = density * dx * dy / (ppc + 0.005)
     gsize = ngx * ngy
-    max_np = int(max_np_factor * ppc * gsize * 6)  # room for (O2/ArO2) density ratios
+    max_np = int(max_np_factor * ppc * gsize)
     max_np = max(max_np, 32 * gsize)
     gas_ev = gas_k * KB_EV
     bc = [

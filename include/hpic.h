@@ -77,7 +77,10 @@ typedef struct hp_case_opts {
     uint64_t seed;       /* loader seed (Park-Miller, src/Particle.c:211-226) and Philox key */
     int cap_per_cell;    /* particle slots per cell per species; 0 = Max_np / Gsize of the deck */
     int field_mode;      /* 0: reference rule, FP32 Jacobi-PCG to r'z < tol^2 (src/cuda_Field.cu:942-1072);
-                            1: FP32 PCG inner solve with FP64 residual refinement to pcg_rtol */
+                            1: FP32 Jacobi-PCG inner solve with FP64 residual refinement to pcg_rtol;
+                            2: FP64 refinement whose inner solve is the separable (tensor-product
+                               eigenbasis) inverse of the operator, run as FP32 GEMMs; falls back to
+                               1 when the operator is not separable */
     double pcg_rtol;     /* field_mode 1: ||b - A x||_2 / ||b||_2 target (default 1e-8) */
     int pcg_max_iter;    /* 0 = 100000, the reference's cap */
     int o2_all_species;  /* O2 gas: 0 = reference launch (electrons only, src/cuda_mcc.cu:76-77), 1 = all species */
@@ -105,6 +108,7 @@ typedef struct hp_case_info {
     size_t device_bytes;   /* device memory held by the case */
     int pcg_cluster;       /* CTAs per case in the field-solve cluster */
     int pcg_block;         /* threads per CTA in the field solve */
+    int field_mode;        /* solver in use: 2 falls back to 1 when the operator is not separable */
 } hp_case_info;
 hp_status hp_case_get_info(const hp_case *c, hp_case_info *out);
 hp_status hp_setup_get_info(const hp_setup *s, hp_case_info *out);
@@ -180,6 +184,11 @@ hp_status hp_get_average_count(hp_case *c, int64_t *n);
 
 /* Field-solver iteration count of the last hp_Field (reference: *FIter). */
 hp_status hp_last_pcg_iters(hp_case *c, int *inner, int *outer);
+/* field_mode 2: ||b - A x|| / ||b|| after the last solve (-1 in other modes). */
+hp_status hp_last_field_residual(hp_case *c, double *rel);
+/* Particles advanced by Move since the case was created (the unit of the
+ * particle-pushes/s metric). */
+hp_status hp_case_pushes(hp_case *c, int64_t *pushes);
 
 /* Case tables (constant over a run), for checkers and tools.  `what`:
  * 0 StructureIndex int[(ncx+2)(ncy+2)], 1 A_idx int[Gsize], 2 node Boundary int[Gsize],

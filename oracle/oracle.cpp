@@ -652,7 +652,51 @@ template <class R> struct Sim : SimBase {
         return total;
     }
 
+    // C[m][n] = sum_k A[m][k] B[k][n], accumulated in k order from zero with
+    // separate multiply and add roundings, as the GPU's grouped GEMM
+    static void gemm(const float *A, const float *B, float *Cm, int M, int N, int K) {
+        std::vector<float> acc((size_t)N);
+        for (int m = 0; m < M; m++) {
+            std::fill(acc.begin(), acc.end(), 0.0f);
+            for (int k = 0; k < K; k++) {
+                const float a = A[(size_t)m * K + k];
+                const float *b = B + (size_t)k * N;
+                for (int n = 0; n < N; n++) acc[n] = acc[n] + a * b[n];
+            }
+            std::copy(acc.begin(), acc.end(), Cm + (size_t)m * N);
+        }
+    }
+
+    void field_fast() {
+        const float *st = c.st;
+        const int nx = c.fs_nx, ny = c.fs_ny;
+        const size_t nxy = (size_t)nx * ny;
+        std::vector<float> X(nxy), A1(nxy), Y(nxy), E(nxy);
+        for (int pass = 0; pass < c.fs_passes; pass++) {
+            for (int j = 0; j < ny; j++)
+                for (int i = 0; i < nx; i++) {
+                    const int node = (c.fs_i0 + i) * c.ngy + (c.fs_j0 + j);
+                    const double r64 = b64[node] - spmv_d(st, node, x64);
+                    X[(size_t)j * nx + i] = (float)(r64 * (double)c.row_scale[node]);
+                }
+            gemm(X.data(), c.fs_V, A1.data(), ny, nx, nx);
+            gemm(c.fs_Wt, A1.data(), Y.data(), ny, nx, ny);
+            for (size_t k = 0; k < nxy; k++) Y[k] = Y[k] * c.fs_inv[k];
+            gemm(Y.data(), c.fs_Vt, A1.data(), ny, nx, nx);
+            gemm(c.fs_W, A1.data(), E.data(), ny, nx, ny);
+            for (int j = 0; j < ny; j++)
+                for (int i = 0; i < nx; i++) x64[(size_t)(c.fs_i0 + i) * c.ngy + (c.fs_j0 + j)] += (double)E[(size_t)j * nx + i];
+        }
+        for (int n = 0; n < G; n++) phi_p[n] = st[2 * G + n] != 0.0f ? (float)x64[n] : 0.0f;
+        pcg_iters[0] = c.fs_passes;
+        pcg_iters[1] = c.fs_passes;
+    }
+
     void field_f32() {
+        if (c.field_mode == 2) {
+            field_fast();
+            return;
+        }
         const float *st = c.st;
         std::vector<float> x = pf_x, r(G, 0.0f), p(G, 0.0f), ap(G, 0.0f);
         int iters = 0, outer = 0;

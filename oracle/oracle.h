@@ -52,6 +52,9 @@ typedef struct or_case {
     double pcg_rtol;
     /* launch shape the GPU used for the PCG reductions */
     int pcg_cluster, pcg_block;
+    /* field_mode 2: separable inverse on the rectangle of unknowns */
+    int fs_i0, fs_j0, fs_nx, fs_ny, fs_passes;
+    const float *fs_V, *fs_Vt, *fs_W, *fs_Wt, *fs_inv;
 } or_case;
 
 typedef struct or_sim or_sim;

@@ -36,6 +36,8 @@ class OrCase(C.Structure):
         ("src_rphase", C.c_float * 8),
         ("pcg_tol2", C.c_float), ("pcg_max_iter", C.c_int), ("field_mode", C.c_int), ("pcg_rtol", C.c_double),
         ("pcg_cluster", C.c_int), ("pcg_block", C.c_int),
+        ("fs_i0", C.c_int), ("fs_j0", C.c_int), ("fs_nx", C.c_int), ("fs_ny", C.c_int), ("fs_passes", C.c_int),
+        ("fs_V", _F), ("fs_Vt", _F), ("fs_W", _F), ("fs_Wt", _F), ("fs_inv", _F),
     ]
 
 
@@ -97,7 +99,8 @@ class Oracle:
 
     GRID = dict(EX=0, EY=1, PHI=2, PHI_POIS=3, DEN=4, SOURCE=5, B=6, X=7)
 
-    def __init__(self, tables, info, opts, precision=32, pcg_cluster=1, pcg_block=512):
+    def __init__(self, tables, info, opts, precision=32, pcg_cluster=1, pcg_block=512, field_mode=None,
+                 fs_passes=3):
         self.info = info
         self.keep = {}
         t = tables
@@ -170,7 +173,19 @@ class Oracle:
             c.efield_flag[k] = int(src[5 * nsrc + k])
         c.pcg_tol2 = np.float32(sc[2]) * np.float32(sc[2])
         c.pcg_max_iter = opts.pcg_max_iter if opts.pcg_max_iter > 0 else 100000
-        c.field_mode = opts.field_mode
+        c.field_mode = opts.field_mode if field_mode is None else field_mode
+        if c.field_mode == 2:
+            fi = t("fs_info")
+            if fi[0]:
+                c.fs_i0, c.fs_j0, c.fs_nx, c.fs_ny = (int(v) for v in fi[1:5])
+                c.fs_passes = fs_passes
+                c.fs_V = keep("fsV", t("fs_V"), np.float32)
+                c.fs_Vt = keep("fsVt", t("fs_Vt"), np.float32)
+                c.fs_W = keep("fsW", t("fs_W"), np.float32)
+                c.fs_Wt = keep("fsWt", t("fs_Wt"), np.float32)
+                c.fs_inv = keep("fsinv", t("fs_inv"), np.float32)
+            else:
+                c.field_mode = 1
         c.pcg_rtol = opts.pcg_rtol if opts.pcg_rtol > 0 else 1e-8
         c.pcg_cluster = pcg_cluster
         c.pcg_block = pcg_block
