@@ -181,7 +181,7 @@ def run_ours(args, rank, world, local, dist):
     w = WORKLOADS[args.workload]
     deck = make_deck(w)
     seed = 1000 + rank
-    setup = hpic.Setup(deck, seed=seed, field_mode=args.field_mode)
+    setup = hpic.Setup(deck, seed=seed, field_mode=args.field_mode, gas_temp_mode=1)
     case = hpic.Case(setup=setup, seed=seed, field_mode=args.field_mode, device=local)
     stream = torch.cuda.current_stream().cuda_stream
     # warm-up (graph capture happens on the first call)
@@ -289,7 +289,7 @@ def run_reference(args):
     import hpic
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     w = WORKLOADS[args.workload]
-    setup = hpic.Setup(make_deck(w), seed=1000, field_mode=args.field_mode)
+    setup = hpic.Setup(make_deck(w), seed=1000, field_mode=args.field_mode, gas_temp_mode=1)
     budget = float(os.environ.get("HPIC_REF_BUDGET_S", "90"))
     cb = cpu_baseline(setup, setup.opts, budget_s=budget)
     return dict(metric=METRIC, value=cb["value"], unit=UNIT, n_gpus=int(os.environ.get("WORLD_SIZE", "1")),

@@ -101,6 +101,7 @@ BuildOpts build_opts(const hp_case_opts *o) {
     if (o) {
         b.seed = o->seed;
         b.cap_per_cell = o->cap_per_cell;
+        b.gas_temp_mode = o->gas_temp_mode;
     }
     return b;
 }

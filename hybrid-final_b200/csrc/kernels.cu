@@ -286,7 +286,7 @@ __device__ __forceinline__ void anewvel_dev(float energy, float vel, float &nvx,
     hp_sincos_turns(rand2, &sinphi, &cosphi);
     const float r13 = nvx, r23 = nvy, r33 = nvz;
     float up1, up2, up3;
-    if (r33 == 1.0f) { up1 = 0; up2 = 1; up3 = 0; }
+    if (r33 == 1.0f || r33 == -1.0f) { up1 = 0; up2 = 1; up3 = 0; }
     else { up1 = 0; up2 = 0; up3 = 1; }
     float r12 = r23 * up3 - r33 * up2;
     float r22 = r33 * up1 - r13 * up3;
@@ -310,7 +310,7 @@ __device__ __forceinline__ void newvel_ionsc_dev(float &vxs, float &vys, float &
     hp_sincos_turns(rand2, &sinphi, &cosphi);
     const float r13 = vxs / vel, r23 = vys / vel, r33 = vzs / vel;
     float up1, up2, up3;
-    if (r33 == 1.0f) { up1 = 0; up2 = 1; up3 = 0; }
+    if (r33 == 1.0f || r33 == -1.0f) { up1 = 0; up2 = 1; up3 = 0; }
     else { up1 = 0; up2 = 0; up3 = 1; }
     float r12 = r23 * up3 - r33 * up2;
     float r22 = r33 * up1 - r13 * up3;

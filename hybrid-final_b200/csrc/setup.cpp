@@ -716,7 +716,7 @@ std::vector<double> setup_solve(const Setup &s, const std::vector<float> &vals, 
     return x;
 }
 
-void laplace_and_gas(Setup &s) {
+void laplace_and_gas(Setup &s, int gas_temp_mode) {
     const int N = s.n_unknowns, G = s.Gsize;
     // Laplace basis: conductor k at 1 V, the others at 0 V (src/cuda_Field.cu:192-219)
     s.lap_basis.assign((size_t)s.cond_numr * G, 0.0f);
@@ -734,7 +734,7 @@ void laplace_and_gas(Setup &s) {
     {
         std::vector<double> b(N);
         for (int i = 0; i < N; i++) b[i] = s.temp_b[i];
-        std::vector<double> x = setup_solve(s, s.ta_val, b);
+        std::vector<double> x = setup_solve(s, gas_temp_mode == 1 ? s.a_val : s.ta_val, b);
         s.node_temp = s.temp;
         for (int g = 0; g < G; g++)
             if (s.a_idx[g]) s.node_temp[g] = (float)x[(size_t)s.a_idx[g] - 1];
@@ -901,7 +901,7 @@ void build_setup(const char *json, size_t len, const BuildOpts &o, Setup &s) {
     field_matrix(s);
     gas_setting(s, o);
     null_collision(s);
-    laplace_and_gas(s);
+    laplace_and_gas(s, o.gas_temp_mode);
 }
 
 } // namespace hp

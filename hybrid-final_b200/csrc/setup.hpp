@@ -117,6 +117,7 @@ struct Setup {
 struct BuildOpts {
     uint64_t seed = 1;
     int cap_per_cell = 0;
+    int gas_temp_mode = 0; // 0 reference temperature operator, 1 potential operator (uniform for equal walls)
 };
 
 // Throws std::runtime_error with a message; the message starts with

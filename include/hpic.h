@@ -85,6 +85,10 @@ typedef struct hp_case_opts {
     int pcg_max_iter;    /* 0 = 100000, the reference's cap */
     int o2_all_species;  /* O2 gas: 0 = reference launch (electrons only, src/cuda_mcc.cu:76-77), 1 = all species */
     int device;          /* CUDA device ordinal */
+    int gas_temp_mode;   /* background-gas temperature field: 0 = the reference's solve, whose matrix
+                            leaves out the Neumann doubling on the x = 0 edge (src/load.c:171-237, Atemp)
+                            and so cools the gas toward that wall; 1 = the same solve on the potential
+                            operator, which keeps equal wall temperatures uniform */
 } hp_case_opts;
 
 /* Default options. */

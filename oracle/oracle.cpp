@@ -375,7 +375,7 @@ template <class R> struct Sim : SimBase {
         m_sincos_turns(rand2, &sinphi, &cosphi);
         const R r13 = nvx, r23 = nvy, r33 = nvz;
         R up1, up2, up3;
-        if (r33 == (R)1.0f) { up1 = 0; up2 = 1; up3 = 0; }
+        if (r33 == (R)1.0f || r33 == (R)-1.0f) { up1 = 0; up2 = 1; up3 = 0; }
         else { up1 = 0; up2 = 0; up3 = 1; }
         R r12 = r23 * up3 - r33 * up2;
         R r22 = r33 * up1 - r13 * up3;
@@ -396,7 +396,7 @@ template <class R> struct Sim : SimBase {
         m_sincos_turns(rand2, &sinphi, &cosphi);
         const R r13 = vxs / vel, r23 = vys / vel, r33 = vzs / vel;
         R up1, up2, up3;
-        if (r33 == (R)1.0f) { up1 = 0; up2 = 1; up3 = 0; }
+        if (r33 == (R)1.0f || r33 == (R)-1.0f) { up1 = 0; up2 = 1; up3 = 0; }
         else { up1 = 0; up2 = 0; up3 = 1; }
         R r12 = r23 * up3 - r33 * up2;
         R r22 = r33 * up1 - r13 * up3;

@@ -143,3 +143,16 @@ def test_no_gpu_is_a_loud_error():
     with pytest.raises(hpic.HpicError) as e:
         hpic.Case(deck)
     assert e.value.status == hpic.HP_ERR_NO_CUDA
+
+
+def test_gas_temperature_modes():
+    """Mode 0 keeps the reference's temperature operator, which has no
+    Neumann doubling on the x = 0 edge and cools the gas toward that wall;
+    mode 1 solves on the potential operator and keeps equal walls uniform."""
+    from hpic.decks import ccp_deck
+    deck = ccp_deck(33, 17, 0.01, 0.005, ppc=2, gas_k=300.0)
+    ref = hpic.Setup(deck, seed=1, gas_temp_mode=0).table("node_temp").reshape(33, 17)
+    fix = hpic.Setup(deck, seed=1, gas_temp_mode=1).table("node_temp").reshape(33, 17)
+    assert np.allclose(fix, 300.0, rtol=1e-5)
+    assert ref[0, 8] < 0.5 * ref[16, 8]       # cold x = 0 wall
+    assert abs(ref[-1, 8] - 300.0) < 10.0      # the x = ncx wall keeps its Neumann doubling
