@@ -94,6 +94,7 @@ _SIGS = {
     "hp_MCC": (C.c_int, [_P, _P]),
     "hp_Deposit": (C.c_int, [_P, _P]),
     "hp_step": (C.c_int, [_P, C.c_int, _P]),
+    "hp_Deposit_noalloc": (C.c_int, [_P, _P, _P]),
     "hp_get_particles": (C.c_int, [_P, C.c_int, _I, _F, _F, _F, _F, _F, C.c_size_t, C.POINTER(C.c_size_t)]),
     "hp_set_particles": (C.c_int, [_P, C.c_int, _I, _F, _F, _F, _F, _F]),
     "hp_get_movers": (C.c_int, [_P, C.c_int, _I, _F, _F, _F, _F, _F, C.POINTER(C.c_int8), C.c_size_t,

@@ -143,6 +143,21 @@ hp_status hp_MCC(hp_case *c, void *stream);
 /* DEPOSIT = Deposit_cuda (src/cuda_Deposit.cu:3-20): CIC density, boundary
  * scaling, rho/eps0, PCG right-hand side. */
 hp_status hp_Deposit(hp_case *c, void *stream);
+/* No counterpart in the reference.  The charge deposit of hp_Deposit for
+ * callers that cannot let a library allocate device memory (a host that
+ * budgets or pools every byte of the GPU itself, or a timed loop that must not
+ * hit cudaMalloc's implicit device synchronisation): it allocates nothing and
+ * writes the boundary-scaled node densities GPG.den of every species into
+ * den_out (device memory, nsp * Gsize doubles, species-major), leaving the
+ * case's own density, source and right-hand side untouched.  Its per-cell
+ * scratch is one fixed array inside the library, 2^19 (species x cells)
+ * entries (16 MiB), held on every GPU that loads the library until the
+ * process exits; larger cases get HP_ERR_CAPACITY.  The first call on a
+ * device looks up that array's device address, so make it before any stream
+ * capture.  All calls share the one array: calls whose work overlaps on the
+ * GPU (other streams, other host threads) race and must be ordered by the
+ * caller.  Every scratch entry a call reads it has written first. */
+hp_status hp_Deposit_noalloc(hp_case *c, double *den_out, void *stream);
 /* n steps of the main loop body (src/cuda_main.cu:114-183 without the
  * diagnostics and dump calls), fused where results allow; replayed from a
  * CUDA graph after the first call on a stream. */
