@@ -181,8 +181,8 @@ def run_ours(args, rank, world, local, dist):
     w = WORKLOADS[args.workload]
     deck = make_deck(w)
     seed = 1000 + rank
-    setup = hpic.Setup(deck, seed=seed, field_mode=args.field_mode, gas_temp_mode=1)
-    case = hpic.Case(setup=setup, seed=seed, field_mode=args.field_mode, device=local)
+    setup = hpic.Setup(deck, seed=seed, field_mode=args.field_mode, gas_temp_mode=1, move_mode=args.move_mode)
+    case = hpic.Case(setup=setup, seed=seed, field_mode=args.field_mode, move_mode=args.move_mode, device=local)
     stream = torch.cuda.current_stream().cuda_stream
     # warm-up (graph capture happens on the first call)
     case.step(args.warmup, stream)
@@ -289,7 +289,8 @@ def run_reference(args):
     import hpic
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     w = WORKLOADS[args.workload]
-    setup = hpic.Setup(make_deck(w), seed=1000, field_mode=args.field_mode, gas_temp_mode=1)
+    setup = hpic.Setup(make_deck(w), seed=1000, field_mode=args.field_mode, gas_temp_mode=1,
+                       move_mode=args.move_mode)
     budget = float(os.environ.get("HPIC_REF_BUDGET_S", "90"))
     cb = cpu_baseline(setup, setup.opts, budget_s=budget)
     return dict(metric=METRIC, value=cb["value"], unit=UNIT, n_gpus=int(os.environ.get("WORLD_SIZE", "1")),
@@ -309,6 +310,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="ar_513x257_200ppc", choices=list(WORKLOADS))
     ap.add_argument("--field-mode", type=int, default=2)
+    ap.add_argument("--move-mode", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

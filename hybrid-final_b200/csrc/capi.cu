@@ -242,6 +242,11 @@ hp_status build_device(hp_case *c) {
         TRY(dupload(c, (float **)&h.eps, eps));
     }
     TRY(dupload(c, (float **)&h.dep_factor, s.dep_factor));
+    if (c->opts.move_mode != 0 && c->opts.move_mode != 1) return set_error("move_mode must be 0 or 1"), HP_ERR_ARG;
+    for (int isp = 0; isp < s.nsp; isp++) {
+        // a far mover's key holds its rank r < cap/2 in 18 bits
+        if (s.cap[isp] > (1 << 19)) return set_error("cap_per_cell above 2^19"), HP_ERR_ARG;
+    }
     for (int isp = 0; isp < s.nsp; isp++) {
         DevSpecies &sp = h.sp[isp];
         sp.cap = s.cap[isp];
@@ -314,6 +319,9 @@ hp_status build_device(hp_case *c) {
     TRY(dalloc(c, &h.pcg_iters, 2));
     TRY(dalloc(c, &h.ave_count, 1));
     TRY(dalloc(c, &h.pushes, 32));
+    TRY(dalloc(c, &h.far_in, (size_t)s.nsp * C));
+    TRY(dalloc(c, &h.far_key, (size_t)s.nsp * C * HP_FAR_BUCKET));
+    h.move_mode = c->opts.move_mode;
     h.field_mode = c->opts.field_mode;
     if (h.field_mode == 2) {
         // separable inner solve when the operator allows it, else mode 1

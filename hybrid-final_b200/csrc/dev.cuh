@@ -3,7 +3,7 @@
 // HBM layout of one case (all arrays owned by the library):
 //   particles, per species s, structure of arrays over a cell-blocked slot pool:
 //     x[s][c*cap + k], y, vx, vy, vz    float   (x, y = offset inside cell c in [0,1))
-//     code[s][c*cap + k]                int8    (mover direction after Move)
+//     code[s][c*cap + k]                int8    (mover destination after Move)
 //     cnt[s][c]                         int32   particles resident in cell c
 //     nmov[s][c]                        int32   movers parked at the top of cell c
 //   cell c = i*ncy + j for the cell whose lower-left node is (i, j); the
@@ -16,6 +16,10 @@
 //   nodes held at zero).
 #pragma once
 #include <cstdint>
+
+// far movers (beyond the 3x3 neighbourhood) one destination cell accepts per
+// step and species; more sets the overflow status
+#define HP_FAR_BUCKET 32
 
 namespace hp {
 
@@ -80,6 +84,9 @@ struct DevCase {
     int *pcg_iters;                 // [2]: inner, outer of the last solve
     int64_t *ave_count;
     unsigned long long *pushes;     // [32] particles pushed by Move, spread over 32 counters
+    unsigned long long *far_key;    // [nsp*C*HP_FAR_BUCKET] movers arriving from beyond the 3x3 neighbourhood
+    int *far_in;                    // [nsp*C] entries in each bucket (cleared by Sort)
+    int move_mode;                  // 0 one cell crossing per step (reference), 1 cross until inside a cell
     // separable inner solve (field_mode 2): rectangle of unknowns and scratch
     int fs_i0, fs_j0, fs_nx, fs_ny, fs_passes;
     float *fs_x;                    // [ny*nx] residual of the symmetrised system

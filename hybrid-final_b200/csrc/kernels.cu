@@ -23,7 +23,7 @@ namespace hp {
 namespace {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr uint32_t ST_OVERFLOW = 0x1u, ST_NONFINITE = 0x2u, ST_NOCONV = 0x4u;
+constexpr uint32_t ST_OVERFLOW = 0x1u, ST_NONFINITE = 0x2u, ST_NOCONV = 0x4u, ST_WALK = 0x10u;
 
 __device__ __forceinline__ int find_case(const int *start, int n, int w) {
     int lo = 0, hi = n;
@@ -41,12 +41,103 @@ __device__ __forceinline__ unsigned lanemask_lt() {
     return m;
 }
 
+// ------------------------------------------------------------------ mover fate
+// Outcome of one cell crossing, from the ghost-grid code of the cell entered
+// (src/cuda_Sortboundary.cu:70-256): 0 plasma; >=100 conductor (absorbed and
+// counted); -1 Dirichlet (absorbed); -2/-6 Neumann x walls, -4/-8 Neumann y
+// walls and -12/-16/-20/-24 Neumann corners (specular reflection back into
+// the domain).  The reference leaves any other code undefined (its
+// uninitialised Sum_CID/Flag_* are used); here such a mover is absorbed.
+struct MoverFate {
+    int fi, fj;
+    bool absorbed, flipx, flipy;
+    int cond; // conductor index or -1
+};
+
+__device__ __forceinline__ MoverFate mover_fate(const DevCase &d, int si, int sj, int di, int dj) {
+    MoverFate f;
+    f.fi = si + di;
+    f.fj = sj + dj;
+    f.absorbed = false;
+    f.flipx = f.flipy = false;
+    f.cond = -1;
+    const int S = d.sidx[(si + 1 + di) * (d.ncy + 2) + (sj + 1 + dj)];
+    switch (S) {
+    case 0: break;
+    case -2: f.fi += 1; f.flipx = true; break;
+    case -6: f.fi -= 1; f.flipx = true; break;
+    case -4: f.fj += 1; f.flipy = true; break;
+    case -8: f.fj -= 1; f.flipy = true; break;
+    case -12: f.fi += 1; f.fj += 1; f.flipx = f.flipy = true; break;
+    case -16: f.fi -= 1; f.fj += 1; f.flipx = f.flipy = true; break;
+    case -20: f.fi += 1; f.fj -= 1; f.flipx = f.flipy = true; break;
+    case -24: f.fi -= 1; f.fj -= 1; f.flipx = f.flipy = true; break;
+    default:
+        f.absorbed = true;
+        if (S >= 100) f.cond = S - 101;
+        break;
+    }
+    if (!f.absorbed && (f.fi < 0 || f.fi >= d.ncx || f.fj < 0 || f.fj >= d.ncy)) f.absorbed = true;
+    return f;
+}
+
+constexpr int CODE_FAR = 14, CODE_ABSORBED = 15;
+// far movers a destination cell accepts per step (per species)
+constexpr int FAR_B = HP_FAR_BUCKET;
+
+// Where a particle that left cell (i, j) ends.  Each crossing wraps the
+// offset by one cell (src/cuda_Move.cu:227-255) and applies the rule of the
+// ghost code of the cell entered (mover_fate), flipping the offset and the
+// velocity on a Neumann wall.  move_mode 0 stops after the first crossing as
+// the reference does (its multi-cell loop, src/cuda_Move.cu:247-253, is
+// commented out, so a particle faster than one cell per step keeps an offset
+// outside [0,1)); move_mode 1 crosses until the offset is back in [0,1).
+// Returns 0 when the particle stays in the domain, 1 when absorbed, 2 when the
+// crossing bound was hit (absorbed and flagged).
+__device__ __forceinline__ int walk(const DevCase &d, int &i, int &j, float &lx, float &ly, float &vx, float &vy,
+                                    int &cond) {
+    const int maxs = d.move_mode ? 2 * (d.ncx + d.ncy) + 4 : 1;
+    for (int s = 0; s < maxs; s++) {
+        int di = 0, dj = 0;
+        if (ly >= 1) { dj = 1; ly = (float)((double)ly - 1.0); }
+        else if (ly < 0) { dj = -1; ly = (float)((double)ly + 1.0); }
+        if (lx >= 1) { di = 1; lx = (float)((double)lx - 1.0); }
+        else if (lx < 0) { di = -1; lx = (float)((double)lx + 1.0); }
+        const MoverFate f = mover_fate(d, i, j, di, dj);
+        if (f.absorbed) {
+            cond = f.cond;
+            return 1;
+        }
+        if (f.flipx) { lx = 1 - lx; vx = -1 * vx; }
+        if (f.flipy) { ly = 1 - ly; vy = -1 * vy; }
+        // a particle that reaches a wall exactly (offset 0 after the wrap) flips
+        // to offset 1, the wall itself, which no cell holds: keep it just inside
+        // (move_mode 0 keeps offset 1, as the reference does)
+        if (d.move_mode) {
+            if (f.flipx && lx == 1) lx = 0x1.fffffep-1f;
+            if (f.flipy && ly == 1) ly = 0x1.fffffep-1f;
+        }
+        i = f.fi;
+        j = f.fj;
+        if (!(ly >= 1 || ly < 0 || lx >= 1 || lx < 0)) return 0;
+    }
+    if (d.move_mode) {
+        cond = -1;
+        return 2;
+    }
+    return 0;
+}
+
 // ------------------------------------------------------------------ Move
 // MoveE_Basic (src/cuda_Move.cu:181-270): bilinear gather of the node field,
-// v += Ascale E, x += v dt/dx in cell units, single-cell exit with one wrap.
-// Stayers are compacted in place (order kept); movers are parked at the top
-// of the cell's slots, r-th mover at slot cap-1-r, with a direction code
-// (di+1)*3 + (dj+1) in place of the reference's relative CellID.
+// v += Ascale E, x += v dt/dx in cell units.  A particle that leaves its
+// cell is resolved here (walk), including the boundary rules the reference
+// applies in SortBoundary.  Stayers are compacted in place (order kept);
+// movers are parked at the top of the cell's slots, r-th mover at slot
+// cap-1-r, with a code: the destination (di+1)*3 + (dj+1) when it lies in the
+// 3x3 neighbourhood, CODE_FAR beyond it (also listed in the destination's
+// bucket as source<<18 | r), CODE_ABSORBED when it left
+// the domain.
 __global__ void __launch_bounds__(256) k_move(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
                                               int ncases, int items) {
     const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
@@ -92,17 +183,23 @@ __global__ void __launch_bounds__(256) k_move(const DevCase *__restrict__ cases,
         }
         const float del_vx = ex_ws * (1 - lx) * (1 - ly) + ex_wn * (1 - lx) * ly + ex_es * lx * (1 - ly) + ex_en * lx * ly;
         const float del_vy = ey_ws * (1 - lx) * (1 - ly) + ey_wn * (1 - lx) * ly + ey_es * lx * (1 - ly) + ey_en * lx * ly;
-        const float mvX = vx + del_vx * As;
-        const float mvY = vy + del_vy * As;
+        float mvX = vx + del_vx * As;
+        float mvY = vy + del_vy * As;
         lx += mvX * dtdx;
         ly += mvY * dtdy;
         const bool out = act && (ly >= 1 || ly < 0 || lx >= 1 || lx < 0);
-        int di = 0, dj = 0;
+        int code = 4, fi = i, fj = j;
         if (out) {
-            if (ly >= 1) { dj = 1; ly = (float)((double)ly - 1.0); }
-            else if (ly < 0) { dj = -1; ly = (float)((double)ly + 1.0); }
-            if (lx >= 1) { di = 1; lx = (float)((double)lx - 1.0); }
-            else if (lx < 0) { di = -1; lx = (float)((double)lx + 1.0); }
+            int cond = -1;
+            const int r = walk(d, fi, fj, lx, ly, mvX, mvY, cond);
+            if (r) {
+                code = CODE_ABSORBED;
+                if (cond >= 0 && cond < d.cond_numr) atomicAdd(&d.cond_charge[s * d.cond_numr + cond], 1.0f);
+                if (r == 2) atomicOr(d.status, ST_WALK);
+            } else {
+                const int ddi = fi - i, ddj = fj - j;
+                code = (ddi >= -1 && ddi <= 1 && ddj >= -1 && ddj <= 1) ? (ddi + 1) * 3 + (ddj + 1) : CODE_FAR;
+            }
         }
         const unsigned bout = __ballot_sync(FULL, out);
         const int before = m + __popc(bout & lt);
@@ -114,7 +211,15 @@ __global__ void __launch_bounds__(256) k_move(const DevCase *__restrict__ cases,
             sp.vx[dst] = mvX;
             sp.vy[dst] = mvY;
             sp.vz[dst] = vz;
-            if (out) sp.code[dst] = (int8_t)((di + 1) * 3 + (dj + 1));
+            if (out) sp.code[dst] = (int8_t)code;
+            if (code == CODE_FAR) {
+                const size_t b = (size_t)s * d.C + (size_t)(fi * d.ncy + fj);
+                const int q = atomicAdd(&d.far_in[b], 1);
+                if (q < FAR_B)
+                    d.far_key[b * FAR_B + q] = ((unsigned long long)c << 18) | (unsigned long long)before;
+                else
+                    atomicOr(d.status, ST_OVERFLOW);
+            }
         }
         m += __popc(bout);
     }
@@ -125,51 +230,13 @@ __global__ void __launch_bounds__(256) k_move(const DevCase *__restrict__ cases,
 }
 
 // ------------------------------------------------------------------ Sort
-// Outcome of one mover, from the ghost-grid code of the cell it moved into
-// (src/cuda_Sortboundary.cu:70-256): 0 plasma; >=100 conductor (absorbed and
-// counted); -1 Dirichlet (absorbed); -2/-6 Neumann x walls, -4/-8 Neumann y
-// walls and -12/-16/-20/-24 Neumann corners (specular reflection back into
-// the domain).  The reference leaves any other code undefined (its
-// uninitialised Sum_CID/Flag_* are used); here such a mover is absorbed.
-struct MoverFate {
-    int fi, fj;
-    bool absorbed, flipx, flipy;
-    int cond; // conductor index or -1
-};
-
-__device__ __forceinline__ MoverFate mover_fate(const DevCase &d, int si, int sj, int di, int dj) {
-    MoverFate f;
-    f.fi = si + di;
-    f.fj = sj + dj;
-    f.absorbed = false;
-    f.flipx = f.flipy = false;
-    f.cond = -1;
-    const int S = d.sidx[(si + 1 + di) * (d.ncy + 2) + (sj + 1 + dj)];
-    switch (S) {
-    case 0: break;
-    case -2: f.fi += 1; f.flipx = true; break;
-    case -6: f.fi -= 1; f.flipx = true; break;
-    case -4: f.fj += 1; f.flipy = true; break;
-    case -8: f.fj -= 1; f.flipy = true; break;
-    case -12: f.fi += 1; f.fj += 1; f.flipx = f.flipy = true; break;
-    case -16: f.fi -= 1; f.fj += 1; f.flipx = f.flipy = true; break;
-    case -20: f.fi += 1; f.fj -= 1; f.flipx = f.flipy = true; break;
-    case -24: f.fi -= 1; f.fj -= 1; f.flipx = f.flipy = true; break;
-    default:
-        f.absorbed = true;
-        if (S >= 100) f.cond = S - 101;
-        break;
-    }
-    if (!f.absorbed && (f.fi < 0 || f.fi >= d.ncx || f.fj < 0 || f.fj >= d.ncy)) f.absorbed = true;
-    return f;
-}
-
 // SortBoundary_Basic re-bins movers by destination with an atomicAdd on the
 // destination count, so the order inside a cell depends on arrival order.
 // Here the warp that owns destination cell (i,j) pulls: it scans the mover
-// lists of the 3x3 source cells in increasing cell index, keeps the movers
-// whose fate lands in (i,j), and appends them after its stayers in list
-// order.  The resulting order is a fixed function of the input.
+// lists of the 3x3 source cells in increasing cell index and appends, in list
+// order, the movers whose code names (i,j), then the movers that travelled
+// further (this cell's bucket) in (source cell, r) order.  The boundary rules
+// were applied by Move.  The resulting order is a fixed function of the input.
 __global__ void __launch_bounds__(256) k_sort(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
                                               int ncases, int items) {
     const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
@@ -187,16 +254,6 @@ __global__ void __launch_bounds__(256) k_sort(const DevCase *__restrict__ cases,
     const int limit = cap - mown;
     const size_t base = (size_t)c * cap;
     const unsigned lt = lanemask_lt();
-    // conductor tallies of this cell's own absorbed movers (src/cuda_Sortboundary.cu:254-256)
-    for (int r0 = 0; r0 < mown; r0 += 32) {
-        const int r = r0 + lane;
-        if (r < mown) {
-            const int code = sp.code[base + cap - 1 - r];
-            const MoverFate f = mover_fate(d, i, j, code / 3 - 1, code % 3 - 1);
-            if (f.absorbed && f.cond >= 0 && f.cond < d.cond_numr)
-                atomicAdd(&d.cond_charge[s * d.cond_numr + f.cond], 1.0f);
-        }
-    }
     int out = n0;
     bool overflow = false;
     for (int si = i - 1; si <= i + 1; si++) {
@@ -204,30 +261,23 @@ __global__ void __launch_bounds__(256) k_sort(const DevCase *__restrict__ cases,
         for (int sj = j - 1; sj <= j + 1; sj++) {
             if (sj < 0 || sj >= d.ncy) continue;
             const int src = si * d.ncy + sj;
+            const int want = (i - si + 1) * 3 + (j - sj + 1);
             const int m = sp.nmov[src];
             const size_t sbase = (size_t)src * cap;
             for (int r0 = 0; r0 < m; r0 += 32) {
                 const int r = r0 + lane;
-                bool match = false;
-                MoverFate f;
-                if (r < m) {
-                    const int code = sp.code[sbase + cap - 1 - r];
-                    f = mover_fate(d, si, sj, code / 3 - 1, code % 3 - 1);
-                    match = !f.absorbed && f.fi == i && f.fj == j;
-                }
+                const bool match = r < m && sp.code[sbase + cap - 1 - r] == want;
                 const unsigned bm = __ballot_sync(FULL, match);
                 if (match) {
                     const int slot = out + __popc(bm & lt);
                     if (slot < limit) {
                         const size_t q = sbase + (size_t)(cap - 1 - r);
-                        const float x = sp.x[q], y = sp.y[q];
-                        const float vx = sp.vx[q], vy = sp.vy[q], vz = sp.vz[q];
                         const size_t dst = base + (size_t)slot;
-                        sp.x[dst] = f.flipx ? 1 - x : x;
-                        sp.y[dst] = f.flipy ? 1 - y : y;
-                        sp.vx[dst] = f.flipx ? -1 * vx : vx;
-                        sp.vy[dst] = f.flipy ? -1 * vy : vy;
-                        sp.vz[dst] = vz;
+                        sp.x[dst] = sp.x[q];
+                        sp.y[dst] = sp.y[q];
+                        sp.vx[dst] = sp.vx[q];
+                        sp.vy[dst] = sp.vy[q];
+                        sp.vz[dst] = sp.vz[q];
                     } else {
                         overflow = true;
                     }
@@ -235,6 +285,40 @@ __global__ void __launch_bounds__(256) k_sort(const DevCase *__restrict__ cases,
                 out += __popc(bm);
             }
         }
+    }
+    // far movers: this cell's bucket, ordered by (source cell, r) with a
+    // bitonic network across the lanes (keys are distinct)
+    const size_t b = (size_t)s * d.C + c;
+    int nf = d.far_in[b];
+    if (nf) {
+        __syncwarp();
+        if (lane == 0) d.far_in[b] = 0;
+        if (nf > FAR_B) nf = FAR_B; // Move flagged the overflow
+        unsigned long long key = lane < nf ? d.far_key[b * FAR_B + lane] : ~0ull;
+#pragma unroll
+        for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+            for (int jj = k >> 1; jj > 0; jj >>= 1) {
+                const unsigned long long o = __shfl_xor_sync(FULL, key, jj);
+                const bool keep_min = ((lane & jj) == 0) == ((lane & k) == 0);
+                key = keep_min ? (o < key ? o : key) : (o > key ? o : key);
+            }
+        if (lane < nf) {
+            const int slot = out + lane;
+            if (slot < limit) {
+                const int src = (int)(key >> 18), r = (int)(key & 0x3FFFF);
+                const size_t q = (size_t)src * cap + (size_t)(cap - 1 - r);
+                const size_t dst = base + (size_t)slot;
+                sp.x[dst] = sp.x[q];
+                sp.y[dst] = sp.y[q];
+                sp.vx[dst] = sp.vx[q];
+                sp.vy[dst] = sp.vy[q];
+                sp.vz[dst] = sp.vz[q];
+            } else {
+                overflow = true;
+            }
+        }
+        out += nf;
     }
     if (__any_sync(FULL, overflow) && lane == 0) atomicOr(d.status, ST_OVERFLOW);
     if (lane == 0) sp.cnt[c] = out < limit ? out : limit;

@@ -127,6 +127,27 @@ def ccp_deck(ngx, ngy, xlen, ylen, *, gas="Ar", pressure_torr=0.05, voltage=100.
     return deck
 
 
+def block_deck():
+    """A 33 x 21 CCP with thick block electrodes (node rows 0-2 and 18-20)
+    and a floating block conductor inside (nodes 12-18 x 8-11): exercises the
+    conductor-face classification and the >= 100 StructureIndex codes, so
+    particles are absorbed on (and counted for) conductors."""
+    d = ccp_deck(33, 21, 0.01, 0.00625, ppc=8)
+    geo = d["Geometry"]
+    geo["ConductorSpec"] = [
+        {"M_ID": 1, "X0": 0, "X1": 32, "Y0": 0, "Y1": 2, "Temp": 300.0, "R(Ohm)": 0.0, "L(H)": 0.0, "C(F)": 1.0},
+        {"M_ID": 2, "X0": 0, "X1": 32, "Y0": 18, "Y1": 20, "Temp": 300.0, "R(Ohm)": 0.0, "L(H)": 0.0, "C(F)": 1.0},
+        {"M_ID": 3, "X0": 12, "X1": 18, "Y0": 8, "Y1": 11, "Temp": 350.0, "R(Ohm)": 0.0, "L(H)": 0.0, "C(F)": 1.0},
+    ]
+    geo["BoundaryCondition"] = [
+        {"X0": 0, "X1": 0, "Y0": 0, "Y1": 20, "B.C": 2, "Temp": 300.0},
+        {"X0": 32, "X1": 32, "Y0": 0, "Y1": 20, "B.C": 2, "Temp": 300.0},
+        {"X0": 0, "X1": 32, "Y0": 0, "Y1": 0, "B.C": 1, "Temp": 300.0},
+        {"X0": 0, "X1": 32, "Y0": 20, "Y1": 20, "B.C": 1, "Temp": 300.0},
+    ]
+    return d
+
+
 def write_deck(path, deck):
     with open(path, "w") as f:
         json.dump(deck, f, indent=1)

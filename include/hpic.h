@@ -89,6 +89,11 @@ typedef struct hp_case_opts {
                             leaves out the Neumann doubling on the x = 0 edge (src/load.c:171-237, Atemp)
                             and so cools the gas toward that wall; 1 = the same solve on the potential
                             operator, which keeps equal wall temperatures uniform */
+    int move_mode;       /* cell crossings per push: 0 = one (the reference's wrap, src/cuda_Move.cu:227-255,
+                            whose multi-cell loop is commented out, so a particle faster than a cell per
+                            step keeps an offset outside [0,1) and its later gathers read the wrong
+                            cell); 1 = cross cell by cell, with the boundary rule of every cell entered,
+                            until the offset is inside a cell */
 } hp_case_opts;
 
 /* Default options. */

@@ -88,6 +88,7 @@ struct SimBase {
     int pcg_iters[2] = {0, 0};
     std::vector<double> ave_den, ave_phi;
     int64_t ave_count = 0;
+    bool walk_bound_hit = false; // a walk that reached its crossing bound
     virtual ~SimBase() {}
     virtual void set_particles(int, const int *, const float *, const float *, const float *, const float *,
                                const float *) = 0;
@@ -219,54 +220,8 @@ template <class R> struct Sim : SimBase {
     }
 
     // ------------------------------------------------------------ Move
-    void move() override {
-        for (int s = 0; s < c.nsp; s++) {
-            Sp &p = sp[s];
-            std::vector<int> ncnt(C, 0);
-            std::vector<R> nx, ny, nvx, nvy, nvz;
-            nx.reserve(p.x.size()); ny.reserve(p.x.size()); nvx.reserve(p.x.size()); nvy.reserve(p.x.size());
-            nvz.reserve(p.x.size());
-            p.mcnt.assign(C, 0);
-            p.mx.clear(); p.my.clear(); p.mvx.clear(); p.mvy.clear(); p.mvz.clear(); p.mcode.clear();
-            const R As = (R)c.Ascale[s], dtdx = (R)c.dt_dx, dtdy = (R)c.dt_dy;
-            for (int cell = 0; cell < C; cell++) {
-                const int i = cell / c.ncy, j = cell - i * c.ncy, node = i * c.ngy + j;
-                const R ex_ws = Ex[node], ex_wn = Ex[node + 1], ex_es = Ex[node + c.ngy], ex_en = Ex[node + c.ngy + 1];
-                const R ey_ws = Ey[node], ey_wn = Ey[node + 1], ey_es = Ey[node + c.ngy], ey_en = Ey[node + c.ngy + 1];
-                for (int q = p.start[cell]; q < p.start[cell + 1]; q++) {
-                    R lx = p.x[q], ly = p.y[q];
-                    const R vx = p.vx[q], vy = p.vy[q], vz = p.vz[q];
-                    const R del_vx = ex_ws * (1 - lx) * (1 - ly) + ex_wn * (1 - lx) * ly + ex_es * lx * (1 - ly) + ex_en * lx * ly;
-                    const R del_vy = ey_ws * (1 - lx) * (1 - ly) + ey_wn * (1 - lx) * ly + ey_es * lx * (1 - ly) + ey_en * lx * ly;
-                    const R mvX = vx + del_vx * As;
-                    const R mvY = vy + del_vy * As;
-                    lx += mvX * dtdx;
-                    ly += mvY * dtdy;
-                    if (ly >= 1 || ly < 0 || lx >= 1 || lx < 0) {
-                        int di = 0, dj = 0;
-                        if (ly >= 1) { dj = 1; ly = (R)((double)ly - 1.0); }
-                        else if (ly < 0) { dj = -1; ly = (R)((double)ly + 1.0); }
-                        if (lx >= 1) { di = 1; lx = (R)((double)lx - 1.0); }
-                        else if (lx < 0) { di = -1; lx = (R)((double)lx + 1.0); }
-                        p.mcnt[cell]++;
-                        p.mx.push_back(lx); p.my.push_back(ly);
-                        p.mvx.push_back(mvX); p.mvy.push_back(mvY); p.mvz.push_back(vz);
-                        p.mcode.push_back((int8_t)((di + 1) * 3 + (dj + 1)));
-                    } else {
-                        ncnt[cell]++;
-                        nx.push_back(lx); ny.push_back(ly); nvx.push_back(mvX); nvy.push_back(mvY); nvz.push_back(vz);
-                    }
-                }
-            }
-            p.cnt.swap(ncnt);
-            p.x.swap(nx); p.y.swap(ny); p.vx.swap(nvx); p.vy.swap(nvy); p.vz.swap(nvz);
-            p.restart();
-            p.mstart.assign(C + 1, 0);
-            for (int k = 0; k < C; k++) p.mstart[k + 1] = p.mstart[k] + p.mcnt[k];
-        }
-    }
-
-    // ------------------------------------------------------------ SortBoundary
+    // Fate of one cell crossing from the ghost code of the cell entered
+    // (src/cuda_Sortboundary.cu:70-256; codes from src/start.c:1776-1851).
     Fate fate(int si, int sj, int di, int dj) const {
         Fate f{si + di, sj + dj, false, false, false, -1};
         const int S = c.sidx[(si + 1 + di) * (c.ncy + 2) + (sj + 1 + dj)];
@@ -289,20 +244,120 @@ template <class R> struct Sim : SimBase {
         return f;
     }
 
+    // One wrap per crossing (src/cuda_Move.cu:227-255) and the rule of the
+    // cell entered; move_mode 0 stops after one crossing as the reference
+    // does, move_mode 1 crosses until the offset is inside a cell (bounded).
+    // 0 inside the domain, 1 absorbed, 2 crossing bound hit.
+    static R one_below() { return std::nextafter((R)1, (R)0); }
+    int walk(int &i, int &j, R &lx, R &ly, R &vx, R &vy, int &cond) const {
+        const int maxs = c.move_mode ? 2 * (c.ncx + c.ncy) + 4 : 1;
+        for (int st = 0; st < maxs; st++) {
+            int di = 0, dj = 0;
+            if (ly >= 1) { dj = 1; ly = (R)((double)ly - 1.0); }
+            else if (ly < 0) { dj = -1; ly = (R)((double)ly + 1.0); }
+            if (lx >= 1) { di = 1; lx = (R)((double)lx - 1.0); }
+            else if (lx < 0) { di = -1; lx = (R)((double)lx + 1.0); }
+            const Fate f = fate(i, j, di, dj);
+            if (f.absorbed) {
+                cond = f.cond;
+                return 1;
+            }
+            if (f.flipx) { lx = 1 - lx; vx = -1 * vx; }
+            if (f.flipy) { ly = 1 - ly; vy = -1 * vy; }
+            // a particle that reaches a wall exactly (offset 0 after the wrap) flips
+            // to offset 1, the wall itself, which no cell holds: keep it just inside
+            // (move_mode 0 keeps offset 1, as the reference does)
+            if (c.move_mode) {
+                if (f.flipx && lx == 1) lx = one_below();
+                if (f.flipy && ly == 1) ly = one_below();
+            }
+            i = f.fi;
+            j = f.fj;
+            if (!(ly >= 1 || ly < 0 || lx >= 1 || lx < 0)) return 0;
+        }
+        if (c.move_mode) {
+            cond = -1;
+            return 2;
+        }
+        return 0;
+    }
+
+    // movers beyond the 3x3 neighbourhood: (species, dest) -> (source<<18 | r, mover index)
+    std::vector<std::vector<std::pair<uint64_t, size_t>>> far[5];
+
+    // MoveE_Basic (src/cuda_Move.cu:181-270) with the boundary rules applied
+    // per crossing; mover codes: destination (di+1)*3+(dj+1) within the 3x3
+    // neighbourhood, 14 beyond it, 15 absorbed.
+    void move() override {
+        for (int s = 0; s < c.nsp; s++) {
+            Sp &p = sp[s];
+            std::vector<int> ncnt(C, 0);
+            std::vector<R> nx, ny, nvx, nvy, nvz;
+            nx.reserve(p.x.size()); ny.reserve(p.x.size()); nvx.reserve(p.x.size()); nvy.reserve(p.x.size());
+            nvz.reserve(p.x.size());
+            p.mcnt.assign(C, 0);
+            p.mx.clear(); p.my.clear(); p.mvx.clear(); p.mvy.clear(); p.mvz.clear(); p.mcode.clear();
+            far[s].assign(C, {});
+            const R As = (R)c.Ascale[s], dtdx = (R)c.dt_dx, dtdy = (R)c.dt_dy;
+            for (int cell = 0; cell < C; cell++) {
+                const int i = cell / c.ncy, j = cell - i * c.ncy, node = i * c.ngy + j;
+                const R ex_ws = Ex[node], ex_wn = Ex[node + 1], ex_es = Ex[node + c.ngy], ex_en = Ex[node + c.ngy + 1];
+                const R ey_ws = Ey[node], ey_wn = Ey[node + 1], ey_es = Ey[node + c.ngy], ey_en = Ey[node + c.ngy + 1];
+                for (int q = p.start[cell]; q < p.start[cell + 1]; q++) {
+                    R lx = p.x[q], ly = p.y[q];
+                    const R vx = p.vx[q], vy = p.vy[q], vz = p.vz[q];
+                    const R del_vx = ex_ws * (1 - lx) * (1 - ly) + ex_wn * (1 - lx) * ly + ex_es * lx * (1 - ly) + ex_en * lx * ly;
+                    const R del_vy = ey_ws * (1 - lx) * (1 - ly) + ey_wn * (1 - lx) * ly + ey_es * lx * (1 - ly) + ey_en * lx * ly;
+                    R mvX = vx + del_vx * As;
+                    R mvY = vy + del_vy * As;
+                    lx += mvX * dtdx;
+                    ly += mvY * dtdy;
+                    if (ly >= 1 || ly < 0 || lx >= 1 || lx < 0) {
+                        int fi = i, fj = j, cond = -1, code;
+                        const int r = walk(fi, fj, lx, ly, mvX, mvY, cond);
+                        if (r) {
+                            code = 15;
+                            if (cond >= 0 && cond < c.cond_numr) cond_charge[(size_t)s * c.cond_numr + cond] += 1.0f;
+                            if (r == 2) walk_bound_hit = true;
+                        } else {
+                            const int ddi = fi - i, ddj = fj - j;
+                            code = (ddi >= -1 && ddi <= 1 && ddj >= -1 && ddj <= 1) ? (ddi + 1) * 3 + (ddj + 1) : 14;
+                        }
+                        if (code == 14)
+                            far[s][fi * c.ncy + fj].push_back(
+                                {((uint64_t)cell << 18) | (uint64_t)p.mcnt[cell], p.mx.size()});
+                        p.mcnt[cell]++;
+                        p.mx.push_back(lx); p.my.push_back(ly);
+                        p.mvx.push_back(mvX); p.mvy.push_back(mvY); p.mvz.push_back(vz);
+                        p.mcode.push_back((int8_t)code);
+                    } else {
+                        ncnt[cell]++;
+                        nx.push_back(lx); ny.push_back(ly); nvx.push_back(mvX); nvy.push_back(mvY); nvz.push_back(vz);
+                    }
+                }
+            }
+            p.cnt.swap(ncnt);
+            p.x.swap(nx); p.y.swap(ny); p.vx.swap(nvx); p.vy.swap(nvy); p.vz.swap(nvz);
+            p.restart();
+            p.mstart.assign(C + 1, 0);
+            for (int k = 0; k < C; k++) p.mstart[k + 1] = p.mstart[k] + p.mcnt[k];
+        }
+    }
+
+    // ------------------------------------------------------------ SortBoundary
+    // Pull order per destination cell: its stayers, the 3x3 source cells'
+    // movers addressed to it (sources in increasing cell index, movers in
+    // list order), then the far movers in (source, r) order.
     void sort() override {
         for (int s = 0; s < c.nsp; s++) {
             Sp &p = sp[s];
-            // conductor tallies of absorbed movers
-            for (int cell = 0; cell < C; cell++) {
-                const int i = cell / c.ncy, j = cell - i * c.ncy;
-                for (int q = p.mstart[cell]; q < p.mstart[cell + 1]; q++) {
-                    const int code = p.mcode[q];
-                    const Fate f = fate(i, j, code / 3 - 1, code % 3 - 1);
-                    if (f.absorbed && f.cond >= 0 && f.cond < c.cond_numr) cond_charge[(size_t)s * c.cond_numr + f.cond] += 1.0f;
-                }
-            }
             std::vector<int> ncnt(C, 0);
             std::vector<R> nx, ny, nvx, nvy, nvz;
+            auto take = [&](size_t q) {
+                nx.push_back(p.mx[q]); ny.push_back(p.my[q]); nvx.push_back(p.mvx[q]); nvy.push_back(p.mvy[q]);
+                nvz.push_back(p.mvz[q]);
+            };
+            if (far[s].size() != (size_t)C) far[s].assign(C, {});
             for (int cell = 0; cell < C; cell++) {
                 const int i = cell / c.ncy, j = cell - i * c.ncy;
                 for (int q = p.start[cell]; q < p.start[cell + 1]; q++) {
@@ -315,19 +370,19 @@ template <class R> struct Sim : SimBase {
                     for (int sj = j - 1; sj <= j + 1; sj++) {
                         if (sj < 0 || sj >= c.ncy) continue;
                         const int src = si * c.ncy + sj;
+                        const int want = (i - si + 1) * 3 + (j - sj + 1);
                         for (int q = p.mstart[src]; q < p.mstart[src + 1]; q++) {
-                            const int code = p.mcode[q];
-                            const Fate f = fate(si, sj, code / 3 - 1, code % 3 - 1);
-                            if (f.absorbed || f.fi != i || f.fj != j) continue;
-                            const R x = p.mx[q], y = p.my[q], vx = p.mvx[q], vy = p.mvy[q], vz = p.mvz[q];
-                            nx.push_back(f.flipx ? 1 - x : x);
-                            ny.push_back(f.flipy ? 1 - y : y);
-                            nvx.push_back(f.flipx ? -1 * vx : vx);
-                            nvy.push_back(f.flipy ? -1 * vy : vy);
-                            nvz.push_back(vz);
+                            if (p.mcode[q] != want) continue;
+                            take((size_t)q);
                             out++;
                         }
                     }
+                }
+                auto &fl = far[s][cell];
+                std::sort(fl.begin(), fl.end());
+                for (auto &e : fl) {
+                    take(e.second);
+                    out++;
                 }
                 ncnt[cell] = out;
             }
@@ -337,6 +392,7 @@ template <class R> struct Sim : SimBase {
             p.mcnt.assign(C, 0);
             p.mstart.assign(C + 1, 0);
             p.mx.clear(); p.my.clear(); p.mvx.clear(); p.mvy.clear(); p.mvz.clear(); p.mcode.clear();
+            far[s].assign(C, {});
         }
     }
 
@@ -1038,6 +1094,7 @@ void or_get_movers(or_sim *s, int isp, int *counts, float *x, float *y, float *v
 }
 void or_get_grid(or_sim *s, int which, void *out) { s->impl->get_grid(which, out); }
 void or_set_grid(or_sim *s, int which, const void *in) { s->impl->set_grid(which, in); }
+int or_walk_bound_hit(or_sim *s) { return s->impl->walk_bound_hit ? 1 : 0; }
 void or_get_counters(or_sim *s, float *cond_charge, unsigned *mcc_count, int *pcg_iters) {
     SimBase *b = s->impl;
     if (cond_charge) std::memcpy(cond_charge, b->cond_charge.data(), b->cond_charge.size() * 4);

@@ -55,6 +55,8 @@ typedef struct or_case {
     /* field_mode 2: separable inverse on the rectangle of unknowns */
     int fs_i0, fs_j0, fs_nx, fs_ny, fs_passes;
     const float *fs_V, *fs_Vt, *fs_W, *fs_Wt, *fs_inv;
+    /* cell crossings per push: 0 one (reference), 1 until inside a cell */
+    int move_mode;
 } or_case;
 
 typedef struct or_sim or_sim;
@@ -76,6 +78,8 @@ void or_get_movers(or_sim *s, int isp, int *counts, float *x, float *y, float *v
 void or_get_grid(or_sim *s, int which, void *out);
 void or_set_grid(or_sim *s, int which, const void *in);
 void or_get_counters(or_sim *s, float *cond_charge, unsigned *mcc_count, int *pcg_iters);
+/* 1 once a move_mode 1 walk reached its crossing bound (the particle was absorbed) */
+int or_walk_bound_hit(or_sim *s);
 
 /* operators (reference order: Field, Move, SortBoundary, MCC, Deposit) */
 void or_field(or_sim *s, int64_t tstep);

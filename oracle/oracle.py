@@ -38,6 +38,7 @@ class OrCase(C.Structure):
         ("pcg_cluster", C.c_int), ("pcg_block", C.c_int),
         ("fs_i0", C.c_int), ("fs_j0", C.c_int), ("fs_nx", C.c_int), ("fs_ny", C.c_int), ("fs_passes", C.c_int),
         ("fs_V", _F), ("fs_Vt", _F), ("fs_W", _F), ("fs_Wt", _F), ("fs_inv", _F),
+        ("move_mode", C.c_int),
     ]
 
 
@@ -67,6 +68,7 @@ def lib():
             "or_get_grid": (None, [P, C.c_int, P]),
             "or_set_grid": (None, [P, C.c_int, P]),
             "or_get_counters": (None, [P, _F, C.POINTER(C.c_uint), _I]),
+            "or_walk_bound_hit": (C.c_int, [P]),
             "or_field": (None, [P, C.c_int64]),
             "or_move": (None, [P]),
             "or_sort": (None, [P]),
@@ -187,6 +189,7 @@ class Oracle:
             else:
                 c.field_mode = 1
         c.pcg_rtol = opts.pcg_rtol if opts.pcg_rtol > 0 else 1e-8
+        c.move_mode = opts.move_mode
         c.pcg_cluster = pcg_cluster
         c.pcg_block = pcg_block
         self.c = c
@@ -250,6 +253,9 @@ class Oracle:
         it = np.zeros(2, np.int32)
         lib().or_get_counters(self.h, _fp(cc), mc.ctypes.data_as(C.POINTER(C.c_uint)), _ip(it))
         return cc, mc, it
+
+    def walk_bound_hit(self):
+        return bool(lib().or_walk_bound_hit(self.h))
 
     def Field(self, tstep):
         lib().or_field(self.h, tstep)

@@ -20,30 +20,11 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(REPO, "hybrid-final_b200"))
-from hpic.decks import ccp_deck  # noqa: E402
+from hpic.decks import block_deck, ccp_deck  # noqa: E402
 
 GGA = np.dtype([("Boundary", "i4"), ("CondID", "i4"), ("Face", "i4"), ("DensRegion", "i4"), ("Area", "f4"),
                 ("Temp", "f4"), ("BackDen1", "f4"), ("BackVel1", "f4"), ("BackDen2", "f4"), ("BackVel2", "f4"),
                 ("Lap_Pot", "f4"), ("Pois_Pot", "f4"), ("Ex", "f4"), ("Ey", "f4")])
-
-
-def block_deck():
-    """Thick block electrodes and a floating block inside: exercises the
-    conductor-face classification and the >=100 StructureIndex codes."""
-    d = ccp_deck(33, 21, 0.01, 0.00625, ppc=8)
-    geo = d["Geometry"]
-    geo["ConductorSpec"] = [
-        {"M_ID": 1, "X0": 0, "X1": 32, "Y0": 0, "Y1": 2, "Temp": 300.0, "R(Ohm)": 0.0, "L(H)": 0.0, "C(F)": 1.0},
-        {"M_ID": 2, "X0": 0, "X1": 32, "Y0": 18, "Y1": 20, "Temp": 300.0, "R(Ohm)": 0.0, "L(H)": 0.0, "C(F)": 1.0},
-        {"M_ID": 3, "X0": 12, "X1": 18, "Y0": 8, "Y1": 11, "Temp": 350.0, "R(Ohm)": 0.0, "L(H)": 0.0, "C(F)": 1.0},
-    ]
-    geo["BoundaryCondition"] = [
-        {"X0": 0, "X1": 0, "Y0": 0, "Y1": 20, "B.C": 2, "Temp": 300.0},
-        {"X0": 32, "X1": 32, "Y0": 0, "Y1": 20, "B.C": 2, "Temp": 300.0},
-        {"X0": 0, "X1": 32, "Y0": 0, "Y1": 0, "B.C": 1, "Temp": 300.0},
-        {"X0": 0, "X1": 32, "Y0": 20, "Y1": 20, "B.C": 1, "Temp": 300.0},
-    ]
-    return d
 
 
 DECKS = {

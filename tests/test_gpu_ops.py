@@ -10,7 +10,7 @@ import pytest
 
 import hpic
 import oracle
-from hpic.decks import ccp_deck
+from hpic.decks import block_deck, ccp_deck
 
 pytestmark = pytest.mark.gpu
 
@@ -29,13 +29,14 @@ DECKS = {
     "ar_17x9": (ccp_deck(17, 9, 0.005, 0.0025, ppc=10), 12345),
     "ar_33x17_hv": (ccp_deck(33, 17, 0.01, 0.005, ppc=20, pressure_torr=0.1, voltage=300.0), 777),
     "ar_65x33": (ccp_deck(65, 33, 0.02, 0.01, ppc=30), 99),
+    "ar_block_33x21": (block_deck(), 4242),
 }
 
 
-def pair(name, field_mode=0):
+def pair(name, field_mode=0, move_mode=0):
     deck, seed = DECKS[name]
-    S = hpic.Setup(deck, seed=seed, field_mode=field_mode)
-    case = hpic.Case(setup=S, seed=seed, field_mode=field_mode)
+    S = hpic.Setup(deck, seed=seed, field_mode=field_mode, move_mode=move_mode)
+    case = hpic.Case(setup=S, seed=seed, field_mode=field_mode, move_mode=move_mode)
     info = case.info
     o = oracle.Oracle(S.table, S.info, case.opts, 32, pcg_cluster=info.pcg_cluster, pcg_block=info.pcg_block)
     for s in range(S.info.nsp):
@@ -83,8 +84,9 @@ def test_field(name, mode):
 
 
 @pytest.mark.parametrize("name", list(DECKS))
-def test_move_and_sort(name):
-    case, o = pair(name)
+@pytest.mark.parametrize("move_mode", [0, 1])
+def test_move_and_sort(name, move_mode):
+    case, o = pair(name, move_mode=move_mode)
     case.set_tstep(1)
     case.Field()
     o.Field(1)
@@ -134,6 +136,91 @@ def test_steps_bit_exact(name, mode):
     assert same(case.grid("AVE_PHI"), p)
     assert case.status() == 0
     assert case.tstep() == n
+
+
+@pytest.mark.parametrize("name", list(DECKS))
+def test_walk_steps_bit_exact(name):
+    """move_mode 1 (cell-by-cell walk) with the separable field solve."""
+    case, o = pair(name, field_mode=2, move_mode=1)
+    n = 25
+    case.step(n)
+    o.run(0, n, accumulate=True)
+    check_particles(case, o, f"after {n} steps")
+    check_grids(case, o, ("DEN", "SOURCE"), "after steps")
+    assert same(case.grid("COND_CHARGE"), o.counters()[0][: case.info.nsp * case.info.cond_numr])
+    assert case.status() == 0
+
+
+def fast_electrons(case, o, cells_per_step, every=3):
+    """Give every `every`-th electron a velocity of `cells_per_step` cells per
+    step in x and half that in y (signs alternating), on both sides."""
+    info = case.info
+    counts, (x, y, vx, vy, vz) = case.particles(0)
+    vcx = np.float32(cells_per_step * info.dx / info.dt)
+    vcy = np.float32(0.5 * cells_per_step * info.dy / info.dt)
+    k = np.arange(x.size)
+    sel = k % every == 0
+    sign = np.where((k // every) % 2 == 0, 1, -1).astype(np.float32)
+    vx = np.where(sel, sign * vcx, vx).astype(np.float32)
+    vy = np.where(sel, -sign * vcy, vy).astype(np.float32)
+    case.set_particles(0, counts, x, y, vx, vy, vz)
+    o.set_particles(0, counts, x, y, vx, vy, vz)
+
+
+@pytest.mark.parametrize("cells", [2.6, 7.3])
+def test_far_movers_bit_exact(cells):
+    """Electrons crossing several cells per push: the walk, the reflections on
+    the side walls, absorption at the electrodes and the far-mover order."""
+    case, o = pair("ar_65x33", field_mode=2, move_mode=1)
+    fast_electrons(case, o, cells)
+    for t in (1, 2):
+        case.set_tstep(t)
+        case.Field()
+        o.Field(t)
+        case.Move()
+        o.Move()
+        gc, ga, gcode = case.movers(0)
+        oc, oa, ocode = o.movers(0)
+        assert np.array_equal(gc, oc) and np.array_equal(gcode, ocode)
+        assert (gcode == 14).sum() > 0, "no mover went beyond the 3x3 neighbourhood"
+        for a, b in zip(ga, oa):
+            assert same(a, b)
+        case.SortBoundary()
+        o.SortBoundary()
+        check_particles(case, o, f"after walk sort {t}")
+        assert same(case.grid("COND_CHARGE"), o.counters()[0][: case.info.nsp * case.info.cond_numr])
+    _, (x, y, *_rest) = case.particles(0)
+    assert x.min() >= 0 and x.max() < 1 and y.min() >= 0 and y.max() < 1
+    assert case.status() == 0
+
+
+def test_reference_wrap_leaves_offsets_outside_the_cell():
+    """move_mode 0 keeps the reference's single wrap: a particle faster than a
+    cell per push ends with an offset outside [0, 1)."""
+    case, o = pair("ar_65x33", field_mode=2, move_mode=0)
+    fast_electrons(case, o, 2.6)
+    case.set_tstep(1)
+    case.Field()
+    case.Move()
+    case.SortBoundary()
+    _, (x, *_rest) = case.particles(0)
+    assert x.max() >= 1 or x.min() < 0
+
+
+def test_walk_stays_finite_over_many_rf_periods_fraction():
+    """At the decks' dt (1/400 of the RF period) the reference wrap lets
+    offsets grow without bound within ~100 steps; the walk keeps every offset
+    in [0, 1) and the status clean over 400 steps (one RF period)."""
+    deck = ccp_deck(65, 33, 0.02, 0.01, ppc=30)
+    case = hpic.Case(deck, seed=5, field_mode=2, move_mode=1, gas_temp_mode=1)
+    case.step(400)
+    assert case.status() == 0
+    for s in range(case.info.nsp):
+        _, (x, y, vx, vy, vz) = case.particles(s)
+        assert x.size > 1000, f"species {s} nearly gone"
+        assert x.min() >= 0 and x.max() < 1 and y.min() >= 0 and y.max() < 1
+        assert np.isfinite(vx).all() and np.isfinite(vy).all() and np.isfinite(vz).all()
+    assert np.isfinite(case.grid("PHI")).all()
 
 
 def test_separable_solver_reaches_tolerance():
