@@ -214,7 +214,7 @@ hp_status hp_batch_step(hp_batch *b, int nsteps, void *stream) {
 
 hp_status hp_batch_set_tune(hp_batch *b, const hp_tune *t) {
     if (!b || !t) return HP_ERR_ARG;
-    if (t->warps_per_block_particles < 1 || t->warps_per_block_particles > 32) return HP_ERR_ARG;
+    if (t->warps_per_block_particles < 1 || t->warps_per_block_particles > 16) return HP_ERR_ARG;
     if (t->pcg_block < 64 || t->pcg_block > 512 || (t->pcg_block & 31)) return HP_ERR_ARG;
     if (t->pcg_cluster_max < 1 || t->pcg_cluster_max > 16 || (t->pcg_cluster_max & (t->pcg_cluster_max - 1)))
         return HP_ERR_ARG;

@@ -34,7 +34,8 @@ hp_status fast_plan_build(hp_case *const *cases, const std::vector<int> &idx, Fa
         const hp::DevCase &h = cases[q]->h;
         const int nx = h.fs_nx, ny = h.fs_ny;
         items[q + 1] = items[q] + nx * ny;
-        const int tn = (nx + 63) / 64, tm = (ny + 63) / 64;
+        const int tn = (nx + FS_TILE - 1) / FS_TILE, tm = (ny + FS_TILE - 1) / FS_TILE;
+        out.plan.final_chunks = std::max(out.plan.final_chunks, (h.G + FS_CHUNK - 1) / FS_CHUNK);
         GemmProb g[4];
         std::memset(g, 0, sizeof g);
         // A1 = X V ; Y = (W^T A1) .* inv ; A2 = Y V^T ; x64 += W A2
@@ -262,6 +263,7 @@ hp_status build_device(hp_case *c) {
         TRY(dalloc(c, &sp.code, nslot));
         TRY(dalloc(c, &sp.cnt, C));
         TRY(dalloc(c, &sp.nmov, C));
+        TRY(dalloc(c, &sp.dcount, (size_t)C * 9));
         TRY(dalloc(c, &h.cw[isp], C));
     }
     TRY(dalloc(c, &h.Ex, G));
@@ -311,6 +313,7 @@ hp_status build_device(hp_case *c) {
     TRY(dupload(c, (float **)&h.vsave, s.vsave));
     h.nvel = s.nvel;
     h.mcc_n = s.mcc_n;
+    if (s.mcc_n < 1 || s.mcc_n > 2047) return set_error("MCC subcycle count outside 1..2047"), HP_ERR_UNSUPPORTED;
     h.seed = c->opts.seed;
     TRY(dalloc(c, &h.tstep, 1));
     TRY(dalloc(c, &h.status, 1));
@@ -337,7 +340,7 @@ hp_status build_device(hp_case *c) {
             TRY(dalloc(c, &h.fs_x, nxy));
             TRY(dalloc(c, &h.fs_a1, nxy));
             TRY(dalloc(c, &h.fs_y, nxy));
-            TRY(dalloc(c, &h.fs_res, 2));
+            TRY(dalloc(c, &h.fs_res, 2 + 2 * (size_t)((G + FS_CHUNK - 1) / FS_CHUNK)));
         } else {
             h.field_mode = 1;
         }

@@ -6,6 +6,7 @@
 //     code[s][c*cap + k]                int8    (mover destination after Move)
 //     cnt[s][c]                         int32   particles resident in cell c
 //     nmov[s][c]                        int32   movers parked at the top of cell c
+//     dcount[s][c*9 + code]             int32   of those, movers to each of the 3x3 cells
 //   cell c = i*ncy + j for the cell whose lower-left node is (i, j); the
 //   reference indexes the same cell by its node i*ngy + j and strides its
 //   slots by Gsize (src/cuda_Particle.cu:44-52).  Slots of one cell are
@@ -32,6 +33,7 @@ struct DevSpecies {
     int8_t *code;
     int *cnt;
     int *nmov;
+    int *dcount; // [C*9] movers per cell and destination code 0..8 (after Move)
     int cap;
     float Ascale, q_density, Escale;
 };

@@ -5,8 +5,8 @@
 // One refinement pass for every case in the plan:
 //   k_fs_resid   X = D^-1 (b - A x64) on the rectangle of unknowns (FP64 residual, FP32 out)
 //   k_gemm x4    A1 = X V;  Y = (W^T A1) .* inv_eig;  A2 = Y V^T;  x64 += W A2
-// and after the last pass k_fs_final writes phi_Pois and the final relative
-// residual.  Each output element of a product is accumulated in k order from
+// and after the last pass k_fs_final + k_fs_norm write phi_Pois and the final
+// relative residual.  Each output element of a product is accumulated in k order from
 // zero with separate multiply and add roundings (the file is built with
 // --fmad=false), so a CPU loop reproduces it exactly.
 #include <cstdint>
@@ -52,10 +52,14 @@ __global__ void __launch_bounds__(256) k_fs_resid(const DevCase *__restrict__ ca
     d.fs_x[u] = (float)(r64 * (double)d.row_scale[node]);
 }
 
-// Grouped C = A B (row-major, contiguous) over a list of problems; 64x64
-// output tile per CTA, 16-deep K slices in shared memory, 4x4 outputs per
-// thread.
-__global__ void __launch_bounds__(256) k_gemm(const GemmProb *__restrict__ probs, int nprob) {
+// Grouped C = A B (row-major, contiguous) over a list of problems.  32x32
+// output tile per CTA of 128 threads (2x4 outputs per thread), so that even a
+// single 511 x 255 case spreads over ~128 SMs; 32-deep K slices staged in
+// shared memory, the next slice fetched into registers while the current one
+// is multiplied.  Each output is accumulated in k order from zero.
+constexpr int GT = 32, GK = 32, GTHREADS = 128;
+
+__global__ void __launch_bounds__(GTHREADS) k_gemm(const GemmProb *__restrict__ probs, int nprob) {
     int lo = 0, hi = nprob;
     const int t = (int)blockIdx.x;
     while (hi - lo > 1) {
@@ -66,44 +70,66 @@ __global__ void __launch_bounds__(256) k_gemm(const GemmProb *__restrict__ probs
     const GemmProb &P = probs[lo];
     const int lt = t - P.tile_start;
     const int tm = lt / P.tiles_n, tn = lt - tm * P.tiles_n;
-    const int m0 = tm * 64, n0 = tn * 64;
+    const int m0 = tm * GT, n0 = tn * GT;
     const int M = P.M, N = P.N, K = P.K;
-    __shared__ __align__(16) float As[16][64];
-    __shared__ __align__(16) float Bs[16][64];
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
-    float acc[4][4];
+    const float *__restrict__ A = P.A;
+    const float *__restrict__ B = P.B;
+    // As[k][m] (row stride 34 keeps float2 reads aligned, 2-way store conflicts)
+    __shared__ __align__(16) float As[GK][GT + 2];
+    __shared__ __align__(16) float Bs[GK][GT];
+    const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
+    // this thread's loads: rows (idx >> 5) = tid/32 + 4q, column lane = tid & 31
+    const int lr = tid >> 5, lc = tid & 31;
+    float ra[8], rb[8];
+    auto fetch = [&](int k0) {
 #pragma unroll
-    for (int a = 0; a < 4; a++)
+        for (int q = 0; q < 8; q++) {
+            const int r = lr + 4 * q;
+            const int gm = m0 + r, gk = k0 + lc;
+            ra[q] = (gm < M && gk < K) ? A[(size_t)gm * K + gk] : 0.0f;
+            const int gkb = k0 + r, gn = n0 + lc;
+            rb[q] = (gkb < K && gn < N) ? B[(size_t)gkb * N + gn] : 0.0f;
+        }
+    };
+    auto stage = [&]() {
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const int r = lr + 4 * q;
+            As[lc][r] = ra[q];
+            Bs[r][lc] = rb[q];
+        }
+    };
+    float acc[2][4];
+#pragma unroll
+    for (int a = 0; a < 2; a++)
 #pragma unroll
         for (int b = 0; b < 4; b++) acc[a][b] = 0.0f;
-    for (int k0 = 0; k0 < K; k0 += 16) {
-#pragma unroll
-        for (int q = 0; q < 4; q++) {
-            const int idx = tid + 256 * q;
-            const int r = idx >> 4, c = idx & 15;
-            const int gm = m0 + r, gk = k0 + c;
-            As[c][r] = (gm < M && gk < K) ? P.A[(size_t)gm * K + gk] : 0.0f;
-            const int rb = idx >> 6, cb = idx & 63;
-            const int gkb = k0 + rb, gn = n0 + cb;
-            Bs[rb][cb] = (gkb < K && gn < N) ? P.B[(size_t)gkb * N + gn] : 0.0f;
-        }
-        __syncthreads();
-        const int kmax = min(16, K - k0);
+    fetch(0);
+    stage();
+    __syncthreads();
+    for (int k0 = 0; k0 < K; k0 += GK) {
+        const bool more = k0 + GK < K;
+        if (more) fetch(k0 + GK);
+        const int kmax = min(GK, K - k0);
         for (int kk = 0; kk < kmax; kk++) {
-            const float4 av = *reinterpret_cast<const float4 *>(&As[kk][ty * 4]);
+            const float2 av = *reinterpret_cast<const float2 *>(&As[kk][ty * 2]);
             const float4 bv = *reinterpret_cast<const float4 *>(&Bs[kk][tx * 4]);
-            const float a4[4] = {av.x, av.y, av.z, av.w};
+            const float a2[2] = {av.x, av.y};
             const float b4[4] = {bv.x, bv.y, bv.z, bv.w};
 #pragma unroll
-            for (int a = 0; a < 4; a++)
+            for (int a = 0; a < 2; a++)
 #pragma unroll
-                for (int b = 0; b < 4; b++) acc[a][b] = acc[a][b] + a4[a] * b4[b];
+                for (int b = 0; b < 4; b++) acc[a][b] = acc[a][b] + a2[a] * b4[b];
         }
         __syncthreads();
+        if (more) {
+            stage();
+            __syncthreads();
+        }
     }
 #pragma unroll
-    for (int a = 0; a < 4; a++) {
-        const int gm = m0 + ty * 4 + a;
+    for (int a = 0; a < 2; a++) {
+        const int gm = m0 + ty * 2 + a;
         if (gm >= M) continue;
 #pragma unroll
         for (int b = 0; b < 4; b++) {
@@ -118,23 +144,25 @@ __global__ void __launch_bounds__(256) k_gemm(const GemmProb *__restrict__ probs
 }
 
 // After the passes: phi_Pois on every node of the case and the relative
-// residual ||b - A x64|| / ||b|| (one CTA per case; strided thread sums,
-// warp trees, warps in order).
+// residual ||b - A x64|| / ||b||.  k_fs_final: FS_CHUNK nodes per CTA, CTA
+// partial sums (warp trees, warps in order) into fs_res[2 + 2*chunk];
+// k_fs_norm: one warp per case adds the partials in a fixed order.
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     return v;
 }
 
-__global__ void __launch_bounds__(256) k_fs_final(const DevCase *__restrict__ cases, const int *__restrict__ list,
-                                                  int n) {
-    if ((int)blockIdx.x >= n) return;
-    const DevCase &d = cases[list[blockIdx.x]];
+__global__ void __launch_bounds__(256) k_fs_final(const DevCase *__restrict__ cases, const int *__restrict__ list) {
+    const DevCase &d = cases[list[blockIdx.y]];
     const int G = d.G, ngy = d.ngy;
+    const int n0 = (int)blockIdx.x * FS_CHUNK;
+    if (n0 >= G) return;
+    const int n1 = min(G, n0 + FS_CHUNK);
     const float *st = d.st;
     const double *v = d.x64;
     double rr = 0.0, bb = 0.0;
-    for (int node = threadIdx.x; node < G; node += blockDim.x) {
+    for (int node = n0 + (int)threadIdx.x; node < n1; node += blockDim.x) {
         const float cc = st[2 * G + node];
         if (cc == 0.0f) {
             d.phi_p[node] = 0.0f;
@@ -163,6 +191,22 @@ __global__ void __launch_bounds__(256) k_fs_final(const DevCase *__restrict__ ca
     if (threadIdx.x == 0) {
         double a = 0.0, b = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); w++) { a += s_r[w]; b += s_b[w]; }
+        d.fs_res[2 + 2 * blockIdx.x] = a;
+        d.fs_res[3 + 2 * blockIdx.x] = b;
+    }
+}
+
+__global__ void __launch_bounds__(32) k_fs_norm(const DevCase *__restrict__ cases, const int *__restrict__ list) {
+    const DevCase &d = cases[list[blockIdx.x]];
+    const int nch = (d.G + FS_CHUNK - 1) / FS_CHUNK;
+    double a = 0.0, b = 0.0;
+    for (int k = (int)threadIdx.x; k < nch; k += 32) {
+        a += d.fs_res[2 + 2 * k];
+        b += d.fs_res[3 + 2 * k];
+    }
+    a = warp_sum(a);
+    b = warp_sum(b);
+    if (threadIdx.x == 0) {
         d.fs_res[0] = sqrt(a);
         d.fs_res[1] = sqrt(b);
         d.pcg_iters[0] = d.fs_passes;
@@ -183,12 +227,15 @@ cudaError_t launch_fast_field(const DevCase *cases, const FastPlan &fp, cudaStre
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         for (int s = 0; s < 4; s++) {
-            k_gemm<<<(unsigned)fp.ntiles[s], 256, 0, st>>>(fp.probs[s], fp.n);
+            k_gemm<<<(unsigned)fp.ntiles[s], GTHREADS, 0, st>>>(fp.probs[s], fp.n);
             e = cudaGetLastError();
             if (e != cudaSuccess) return e;
         }
     }
-    k_fs_final<<<(unsigned)fp.n, 256, 0, st>>>(cases, fp.list, fp.n);
+    k_fs_final<<<dim3((unsigned)fp.final_chunks, (unsigned)fp.n), 256, 0, st>>>(cases, fp.list);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_fs_norm<<<(unsigned)fp.n, 32, 0, st>>>(cases, fp.list);
     return cudaGetLastError();
 }
 

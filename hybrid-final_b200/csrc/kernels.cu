@@ -11,6 +11,8 @@
 // every a*b+c is two roundings, exactly as the CPU checker evaluates it; the
 // elementary functions come from hp_math.h, identical on host and device.
 #include <cooperative_groups.h>
+
+#include <algorithm>
 #include <cstdint>
 
 #include "hp_math.h"
@@ -138,7 +140,7 @@ __device__ __forceinline__ int walk(const DevCase &d, int &i, int &j, float &lx,
 // 3x3 neighbourhood, CODE_FAR beyond it (also listed in the destination's
 // bucket as source<<18 | r), CODE_ABSORBED when it left
 // the domain.
-__global__ void __launch_bounds__(256) k_move(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
+__global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
                                               int ncases, int items) {
     const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
@@ -151,6 +153,7 @@ __global__ void __launch_bounds__(256) k_move(const DevCase *__restrict__ cases,
     const int n = sp.cnt[c];
     if (n == 0) {
         if (lane == 0) sp.nmov[c] = 0;
+        if (lane < 9) sp.dcount[(size_t)c * 9 + lane] = 0;
         return;
     }
     if (lane == 0) atomicAdd(&d.pushes[warp & 31], (unsigned long long)n);
@@ -160,6 +163,7 @@ __global__ void __launch_bounds__(256) k_move(const DevCase *__restrict__ cases,
             sp.nmov[c] = 0;
             atomicOr(d.status, ST_OVERFLOW);
         }
+        if (lane < 9) sp.dcount[(size_t)c * 9 + lane] = 0;
         return;
     }
     const int i = c / d.ncy, j = c - i * d.ncy;
@@ -170,6 +174,7 @@ __global__ void __launch_bounds__(256) k_move(const DevCase *__restrict__ cases,
     const size_t base = (size_t)c * cap;
     const unsigned lt = lanemask_lt();
     int m = 0;
+    int dc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     for (int k0 = 0; k0 < n; k0 += 32) {
         const int k = k0 + lane;
         const bool act = k < n;
@@ -222,23 +227,107 @@ __global__ void __launch_bounds__(256) k_move(const DevCase *__restrict__ cases,
             }
         }
         m += __popc(bout);
+#pragma unroll
+        for (int D = 0; D < 9; D++) dc[D] += __popc(__ballot_sync(FULL, out && code == D));
     }
     if (lane == 0) {
         sp.cnt[c] = n - m;
         sp.nmov[c] = m;
     }
+    int mine = 0;
+#pragma unroll
+    for (int D = 0; D < 9; D++)
+        if (lane == D) mine = dc[D];
+    if (lane < 9) sp.dcount[(size_t)c * 9 + lane] = mine;
 }
 
 // ------------------------------------------------------------------ Sort
 // SortBoundary_Basic re-bins movers by destination with an atomicAdd on the
 // destination count, so the order inside a cell depends on arrival order.
-// Here the warp that owns destination cell (i,j) pulls: it scans the mover
-// lists of the 3x3 source cells in increasing cell index and appends, in list
-// order, the movers whose code names (i,j), then the movers that travelled
-// further (this cell's bucket) in (source cell, r) order.  The boundary rules
-// were applied by Move.  The resulting order is a fixed function of the input.
-__global__ void __launch_bounds__(256) k_sort(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
-                                              int ncases, int items) {
+// Here the order is fixed: a destination cell keeps its stayers, then the
+// movers addressed to it from its 3x3 neighbourhood, sources in increasing
+// cell index and each source's movers in list order, then the movers that
+// travelled further (its bucket) in (source cell, r) order.  The boundary
+// rules were applied by Move, which also counted each cell's movers per
+// destination (dcount).  From those counts every source knows where its
+// movers go, so the re-binning is a push with no loop-carried dependency:
+//   k_sort_push  (warp per source cell) slot of each near mover = stayers of
+//                the destination + movers sent to it by lower-index sources
+//                + rank among this source's movers to it;
+//   k_sort_count (warp per destination cell) new count, then the far movers.
+constexpr int SORT_MAXW = 16; // warps per block, at most
+
+__global__ void __launch_bounds__(SORT_MAXW * 32) k_sort_push(const DevCase *__restrict__ cases,
+                                                        const int *__restrict__ item_start, int ncases, int items) {
+    __shared__ int s_off[SORT_MAXW][9], s_lim[SORT_MAXW][9];
+    const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    if (warp >= items) return;
+    const int ci = find_case(item_start, ncases, warp);
+    const DevCase &d = cases[ci];
+    const int w = warp - item_start[ci];
+    const int s = w / d.C, c = w - s * d.C;
+    const DevSpecies &sp = d.sp[s];
+    const int m = sp.nmov[c];
+    if (m == 0) return;
+    const int cap = sp.cap, ncy = d.ncy;
+    const int i = c / ncy, j = c - i * ncy;
+    // destination D = code (di+1)*3 + (dj+1): its stayers and slot limit
+    if (lane < 9) {
+        const int Di = i + lane / 3 - 1, Dj = j + lane % 3 - 1;
+        const bool ok = Di >= 0 && Di < d.ncx && Dj >= 0 && Dj < ncy;
+        const int D = Di * ncy + Dj;
+        s_off[wl][lane] = ok ? sp.cnt[D] : 0;
+        s_lim[wl][lane] = ok ? cap - sp.nmov[D] : 0;
+    }
+    __syncwarp();
+    // + movers sent to D by its other neighbours S < c; (D, S) pair p = 9*Dd + Ss,
+    // S = D + (Ss/3 - 1, Ss%3 - 1), and S's code for D is 8 - Ss
+    for (int p = lane; p < 81; p += 32) {
+        const int Dd = p / 9, Ss = p - 9 * Dd;
+        const int Di = i + Dd / 3 - 1, Dj = j + Dd % 3 - 1;
+        const int Si = Di + Ss / 3 - 1, Sj = Dj + Ss % 3 - 1;
+        const int S = Si * ncy + Sj;
+        if (Di >= 0 && Di < d.ncx && Dj >= 0 && Dj < ncy && Si >= 0 && Si < d.ncx && Sj >= 0 && Sj < ncy && S < c) {
+            const int v = sp.dcount[(size_t)S * 9 + (8 - Ss)];
+            if (v) atomicAdd(&s_off[wl][Dd], v);
+        }
+    }
+    __syncwarp();
+    const unsigned lt = lanemask_lt();
+    const size_t base = (size_t)c * cap;
+    int run[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    bool overflow = false;
+    for (int r0 = 0; r0 < m; r0 += 32) {
+        const int r = r0 + lane;
+        const size_t q = base + (size_t)(cap - 1 - r);
+        const int code = r < m ? (int)sp.code[q] : -1;
+        int rank = 0;
+#pragma unroll
+        for (int D = 0; D < 9; D++) {
+            const unsigned b = __ballot_sync(FULL, code == D);
+            if (code == D) rank = run[D] + __popc(b & lt);
+            run[D] += __popc(b);
+        }
+        if (code >= 0 && code < 9) {
+            const int slot = s_off[wl][code] + rank;
+            if (slot < s_lim[wl][code]) {
+                const size_t dst = (size_t)(c + (code / 3 - 1) * ncy + (code % 3 - 1)) * cap + (size_t)slot;
+                sp.x[dst] = sp.x[q];
+                sp.y[dst] = sp.y[q];
+                sp.vx[dst] = sp.vx[q];
+                sp.vy[dst] = sp.vy[q];
+                sp.vz[dst] = sp.vz[q];
+            } else {
+                overflow = true;
+            }
+        }
+    }
+    if (__any_sync(FULL, overflow) && lane == 0) atomicOr(d.status, ST_OVERFLOW);
+}
+
+__global__ void __launch_bounds__(SORT_MAXW * 32) k_sort_count(const DevCase *__restrict__ cases,
+                                                         const int *__restrict__ item_start, int ncases, int items) {
     const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (warp >= items) return;
@@ -247,45 +336,18 @@ __global__ void __launch_bounds__(256) k_sort(const DevCase *__restrict__ cases,
     const int w = warp - item_start[ci];
     const int s = w / d.C, c = w - s * d.C;
     const DevSpecies &sp = d.sp[s];
-    const int cap = sp.cap;
-    const int i = c / d.ncy, j = c - i * d.ncy;
-    const int n0 = sp.cnt[c];
-    const int mown = sp.nmov[c];
-    const int limit = cap - mown;
-    const size_t base = (size_t)c * cap;
-    const unsigned lt = lanemask_lt();
-    int out = n0;
-    bool overflow = false;
-    for (int si = i - 1; si <= i + 1; si++) {
-        if (si < 0 || si >= d.ncx) continue;
-        for (int sj = j - 1; sj <= j + 1; sj++) {
-            if (sj < 0 || sj >= d.ncy) continue;
-            const int src = si * d.ncy + sj;
-            const int want = (i - si + 1) * 3 + (j - sj + 1);
-            const int m = sp.nmov[src];
-            const size_t sbase = (size_t)src * cap;
-            for (int r0 = 0; r0 < m; r0 += 32) {
-                const int r = r0 + lane;
-                const bool match = r < m && sp.code[sbase + cap - 1 - r] == want;
-                const unsigned bm = __ballot_sync(FULL, match);
-                if (match) {
-                    const int slot = out + __popc(bm & lt);
-                    if (slot < limit) {
-                        const size_t q = sbase + (size_t)(cap - 1 - r);
-                        const size_t dst = base + (size_t)slot;
-                        sp.x[dst] = sp.x[q];
-                        sp.y[dst] = sp.y[q];
-                        sp.vx[dst] = sp.vx[q];
-                        sp.vy[dst] = sp.vy[q];
-                        sp.vz[dst] = sp.vz[q];
-                    } else {
-                        overflow = true;
-                    }
-                }
-                out += __popc(bm);
-            }
-        }
+    const int cap = sp.cap, ncy = d.ncy;
+    const int i = c / ncy, j = c - i * ncy;
+    // near movers in: source S = c + (Ss/3 - 1, Ss%3 - 1) sends code 8 - Ss
+    int in = 0;
+    if (lane < 9) {
+        const int Si = i + lane / 3 - 1, Sj = j + lane % 3 - 1;
+        if (Si >= 0 && Si < d.ncx && Sj >= 0 && Sj < ncy) in = sp.dcount[(size_t)(Si * ncy + Sj) * 9 + (8 - lane)];
     }
+    in = __reduce_add_sync(FULL, in);
+    const int limit = cap - sp.nmov[c];
+    int out = sp.cnt[c] + in;
+    bool overflow = false;
     // far movers: this cell's bucket, ordered by (source cell, r) with a
     // bitonic network across the lanes (keys are distinct)
     const size_t b = (size_t)s * d.C + c;
@@ -308,7 +370,7 @@ __global__ void __launch_bounds__(256) k_sort(const DevCase *__restrict__ cases,
             if (slot < limit) {
                 const int src = (int)(key >> 18), r = (int)(key & 0x3FFFF);
                 const size_t q = (size_t)src * cap + (size_t)(cap - 1 - r);
-                const size_t dst = base + (size_t)slot;
+                const size_t dst = (size_t)c * cap + (size_t)slot;
                 sp.x[dst] = sp.x[q];
                 sp.y[dst] = sp.y[q];
                 sp.vx[dst] = sp.vx[q];
@@ -416,11 +478,159 @@ __device__ __forceinline__ void newvel_ionsc_dev(float &vxs, float &vys, float &
 // reference draws from its per-cell curand state; where the reference passes
 // two curand_uniform() calls as arguments, the left one is drawn first.
 // Channel tallies go to the cell's own counters (the reference's MCCR).
-__global__ void __launch_bounds__(256) k_mcc_ar(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
-                                                int ncases, int items) {
+//
+// Most particles do not collide in a step (a few per cent), and a colliding
+// lane runs a long path (cross sections, scattering angles, the ionisation
+// energy split) while the rest of its warp would idle.  So each warp first
+// runs the cheap null-collision test over its cell and queues the colliders
+// in particle order in a shared-memory ring; every 32 queued colliders are
+// then processed by the whole warp, one per lane.  A collider's stream is
+// re-created from its key and advanced past the draws the test consumed, so
+// every particle's arithmetic and draws are exactly those of a lane-per-
+// particle loop, and new particles are still appended in particle order.
+constexpr int MCC_TPB = 256;
+constexpr int MCC_RING = 64;
+
+// advance a fresh stream by n draws; returns the last draw (n >= 1)
+__device__ __forceinline__ float stream_replay(hp_stream &rs, int n) {
+    float r = 0.f;
+    for (int t = 0; t < n; t++) r = hp_stream_next(&rs);
+    return r;
+}
+
+__device__ __forceinline__ void mcc_ion_collide(const DevCase &d, const DevSpecies &ion, size_t q, hp_stream &rs,
+                                                float bvel, unsigned *cnt_ch) {
+    const int nn = (int)((d.nvel - 1) * hp_stream_next(&rs));
+    float vnx, vny, vnz;
+    {
+        const float a = hp_stream_next(&rs);
+        const float b = hp_stream_next(&rs);
+        maxwellv_dev(vnx, vny, vnz, d.vsave[nn], bvel, a, b);
+    }
+    const float vx = ion.vx[q], vy = ion.vy[q], vz = ion.vz[q];
+    float VX = vx - vnx, VY = vy - vnz, VZ = vz - vny; // y/z of the neutral swapped as in src/cuda_mccAr.cu:200-202
+    const float dum = VX * VX + VY * VY + VZ * VZ;
+    const float engy = ion.Escale * dum;
+    const float vel = sqrtf(dum);
+    const float R1 = hp_stream_next(&rs) * d.sigv[2] / vel;
+    float SumSigma = xsec_lookup(d, 5, engy);
+    float ox, oy, oz;
+    if (R1 <= SumSigma) {
+        ox = vnx; oy = vny; oz = vnz;
+        cnt_ch[5]++;
+    } else if (R1 <= (SumSigma += xsec_lookup(d, 6, engy))) {
+        const float a = hp_stream_next(&rs);
+        const float b = hp_stream_next(&rs);
+        newvel_ionsc_dev(VX, VY, VZ, vel, a, b);
+        ox = VX + vnx; oy = VY + vny; oz = VZ + vnz;
+        cnt_ch[6]++;
+    } else {
+        ox = vx; oy = vy; oz = vz;
+    }
+    ion.vx[q] = ox;
+    ion.vy[q] = oy;
+    ion.vz[q] = oz;
+}
+
+struct NewPair {
+    float x, y, evx, evy, evz, ivx, ivy, ivz;
+};
+
+// one electron that passed the null-collision test with draw R1; returns
+// true when it ionised (the new electron/ion pair in np)
+__device__ __forceinline__ bool mcc_el_collide(const DevCase &d, const DevSpecies &el, size_t q, hp_stream &rs,
+                                               float R1, float P1, float bvel, unsigned *cnt_ch, NewPair &np) {
+    int colltype = 1;
+    const int target = (R1 <= P1) ? 0 : 1;
+    float VX = el.vx[q], VY = el.vy[q], VZ = el.vz[q];
+    const float dum = VX * VX + VY * VY + VZ * VZ;
+    float vel = sqrtf(dum);
+    VX /= vel; VY /= vel; VZ /= vel;
+    float engy = el.Escale * dum;
+    float rengy = 0.f, vel2 = 0.f;
+    if (target == 0) {
+        const float R2 = hp_stream_next(&rs) * d.sigv[0] / vel;
+        float SumSigma = xsec_lookup(d, 0, engy);
+        if (R2 <= SumSigma) {
+            colltype = 0;
+            cnt_ch[0]++;
+        } else if (engy > d.th[1] && R2 <= (SumSigma += xsec_lookup(d, 1, engy))) {
+            colltype = 0;
+            engy -= d.th[1];
+            vel = sqrtf(fabsf(engy) / el.Escale);
+            cnt_ch[1]++;
+        } else if (engy > d.th[2] && R2 <= (SumSigma += xsec_lookup(d, 2, engy))) {
+            colltype = 0;
+            engy -= d.th[2];
+            vel = sqrtf(fabsf(engy) / el.Escale);
+            cnt_ch[2]++;
+        } else if (engy > d.th[3] && R2 <= (SumSigma += xsec_lookup(d, 3, engy))) {
+            colltype = 2;
+            engy -= d.th[3];
+            const float u = hp_stream_next(&rs);
+            rengy = (float)(10.0 * (double)hp_tanf_q1(u * hp_atanf((float)(engy / 20.0))));
+            engy -= rengy;
+            vel = sqrtf(fabsf(rengy) / el.Escale);
+            vel2 = sqrtf(fabsf(engy) / el.Escale);
+            cnt_ch[3]++;
+        }
+    } else {
+        const float R2 = hp_stream_next(&rs) * d.sigv[1] / vel;
+        const float SumSigma = xsec_lookup(d, 4, engy);
+        if (engy > d.th[4] && R2 <= SumSigma) {
+            colltype = 2;
+            engy -= d.th[4];
+            const float u = hp_stream_next(&rs);
+            rengy = (float)(10.0 * (double)hp_tanf_q1(u * hp_atanf((float)(engy / 20.0))));
+            engy -= rengy;
+            vel = sqrtf(fabsf(rengy) / el.Escale);
+            vel2 = sqrtf(fabsf(engy) / el.Escale);
+            cnt_ch[4]++;
+        }
+    }
+    if (colltype == 0) {
+        const float a = hp_stream_next(&rs);
+        const float b = hp_stream_next(&rs);
+        anewvel_dev(engy, vel, VX, VY, VZ, a, b);
+        el.vx[q] = VX;
+        el.vy[q] = VY;
+        el.vz[q] = VZ;
+        return false;
+    }
+    if (colltype != 2) return false; // null collision: velocity unchanged
+    np.x = el.x[q];
+    np.y = el.y[q];
+    np.evx = VX; np.evy = VY; np.evz = VZ;
+    {
+        const float a = hp_stream_next(&rs);
+        const float b = hp_stream_next(&rs);
+        anewvel_dev(rengy, vel, np.evx, np.evy, np.evz, a, b);
+    }
+    np.ivx = VX; np.ivy = VY; np.ivz = VZ;
+    {
+        const int nn = (int)((d.nvel - 1) * hp_stream_next(&rs));
+        const float a = hp_stream_next(&rs);
+        const float b = hp_stream_next(&rs);
+        maxwellv_dev(np.ivx, np.ivy, np.ivz, d.vsave[nn], bvel, a, b);
+    }
+    {
+        const float a = hp_stream_next(&rs);
+        const float b = hp_stream_next(&rs);
+        anewvel_dev(engy, vel2, VX, VY, VZ, a, b);
+    }
+    el.vx[q] = VX;
+    el.vy[q] = VY;
+    el.vz[q] = VZ;
+    return true;
+}
+
+__global__ void __launch_bounds__(MCC_TPB) k_mcc_ar(const DevCase *__restrict__ cases,
+                                                    const int *__restrict__ item_start, int ncases, int items) {
+    __shared__ int ring_s[MCC_TPB / 32][MCC_RING];
     const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (warp >= items) return;
+    int *ring = ring_s[threadIdx.x >> 5];
     const int ci = find_case(item_start, ncases, warp);
     const DevCase &d = cases[ci];
     const int c = warp - item_start[ci];
@@ -431,167 +641,96 @@ __global__ void __launch_bounds__(256) k_mcc_ar(const DevCase *__restrict__ case
     const float bvel = d.back_vel1[node];
     const unsigned lt = lanemask_lt();
     unsigned cnt_ch[7] = {0, 0, 0, 0, 0, 0, 0};
-    // ---- ions
+    // ---- ions: test, queue, collide 32 at a time
     const DevSpecies &ion = d.sp[1];
     const int ni = ion.cnt[c];
     const size_t ibase = (size_t)c * ion.cap;
-    for (int k0 = 0; k0 < ni; k0 += 32) {
-        const int k = k0 + lane;
-        if (k >= ni) break;
-        hp_stream rs;
-        hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, 1u);
-        float R1 = hp_stream_next(&rs);
-        if (R1 > Pion) continue;
-        const int nn = (int)((d.nvel - 1) * hp_stream_next(&rs));
-        float vnx, vny, vnz;
-        {
-            const float a = hp_stream_next(&rs);
-            const float b = hp_stream_next(&rs);
-            maxwellv_dev(vnx, vny, vnz, d.vsave[nn], bvel, a, b);
+    int head = 0, tail = 0;
+    for (int k0 = 0; k0 < ni || tail > head; k0 += 32) {
+        if (k0 < ni) {
+            const int k = k0 + lane;
+            bool hit = false;
+            if (k < ni) {
+                hp_stream rs;
+                hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, 1u);
+                hit = hp_stream_next(&rs) <= Pion;
+            }
+            const unsigned b = __ballot_sync(FULL, hit);
+            if (hit) ring[(tail + __popc(b & lt)) & (MCC_RING - 1)] = k;
+            tail += __popc(b);
         }
-        const size_t q = ibase + k;
-        const float vx = ion.vx[q], vy = ion.vy[q], vz = ion.vz[q];
-        float VX = vx - vnx, VY = vy - vnz, VZ = vz - vny; // y/z of the neutral swapped as in src/cuda_mccAr.cu:200-202
-        const float dum = VX * VX + VY * VY + VZ * VZ;
-        const float engy = ion.Escale * dum;
-        const float vel = sqrtf(dum);
-        R1 = hp_stream_next(&rs) * d.sigv[2] / vel;
-        float SumSigma = xsec_lookup(d, 5, engy);
-        float ox, oy, oz;
-        if (R1 <= SumSigma) {
-            ox = vnx; oy = vny; oz = vnz;
-            cnt_ch[5]++;
-        } else if (R1 <= (SumSigma += xsec_lookup(d, 6, engy))) {
-            const float a = hp_stream_next(&rs);
-            const float b = hp_stream_next(&rs);
-            newvel_ionsc_dev(VX, VY, VZ, vel, a, b);
-            ox = VX + vnx; oy = VY + vny; oz = VZ + vnz;
-            cnt_ch[6]++;
-        } else {
-            ox = vx; oy = vy; oz = vz;
+        __syncwarp();
+        const bool last = k0 + 32 >= ni;
+        while (tail - head >= 32 || (last && tail > head)) {
+            const int e = head + lane;
+            if (e < tail) {
+                const int k = ring[e & (MCC_RING - 1)];
+                hp_stream rs;
+                hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, 1u);
+                stream_replay(rs, 1);
+                mcc_ion_collide(d, ion, ibase + k, rs, bvel, cnt_ch);
+            }
+            head = min(head + 32, tail);
+            __syncwarp();
         }
-        ion.vx[q] = ox;
-        ion.vy[q] = oy;
-        ion.vz[q] = oz;
     }
-    // ---- electrons
+    // ---- electrons: queue entries are slot | draws used << 20
     const DevSpecies &el = d.sp[0];
     const int ne = el.cnt[c];
     const size_t ebase = (size_t)c * el.cap;
     int add = 0;
     bool overflow = false;
-    for (int k0 = 0; k0 < ne; k0 += 32) {
-        const int k = k0 + lane;
-        bool create = false;
-        float nx = 0, ny = 0, nevx = 0, nevy = 0, nevz = 0, nivx = 0, nivy = 0, nivz = 0;
-        if (k < ne) {
-            hp_stream rs;
-            hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, 0u);
-            int colltype = 0;
-            float R1 = 0.f;
-            for (int jj = 0; jj < d.mcc_n; jj++) {
-                R1 = hp_stream_next(&rs);
-                if (R1 < P2) { colltype = 1; break; }
-            }
-            if (colltype) {
-                const int target = (R1 <= P1) ? 0 : 1;
-                const size_t q = ebase + k;
-                float VX = el.vx[q], VY = el.vy[q], VZ = el.vz[q];
-                const float dum = VX * VX + VY * VY + VZ * VZ;
-                float vel = sqrtf(dum);
-                VX /= vel; VY /= vel; VZ /= vel;
-                float engy = el.Escale * dum;
-                float rengy = 0.f, vel2 = 0.f;
-                if (target == 0) {
-                    const float R2 = hp_stream_next(&rs) * d.sigv[0] / vel;
-                    float SumSigma = xsec_lookup(d, 0, engy);
-                    if (R2 <= SumSigma) {
-                        colltype = 0;
-                        cnt_ch[0]++;
-                    } else if (engy > d.th[1] && R2 <= (SumSigma += xsec_lookup(d, 1, engy))) {
-                        colltype = 0;
-                        engy -= d.th[1];
-                        vel = sqrtf(fabsf(engy) / el.Escale);
-                        cnt_ch[1]++;
-                    } else if (engy > d.th[2] && R2 <= (SumSigma += xsec_lookup(d, 2, engy))) {
-                        colltype = 0;
-                        engy -= d.th[2];
-                        vel = sqrtf(fabsf(engy) / el.Escale);
-                        cnt_ch[2]++;
-                    } else if (engy > d.th[3] && R2 <= (SumSigma += xsec_lookup(d, 3, engy))) {
-                        colltype = 2;
-                        engy -= d.th[3];
-                        const float u = hp_stream_next(&rs);
-                        rengy = (float)(10.0 * (double)hp_tanf_q1(u * hp_atanf((float)(engy / 20.0))));
-                        engy -= rengy;
-                        vel = sqrtf(fabsf(rengy) / el.Escale);
-                        vel2 = sqrtf(fabsf(engy) / el.Escale);
-                        cnt_ch[3]++;
+    head = tail = 0;
+    for (int k0 = 0; k0 < ne || tail > head; k0 += 32) {
+        if (k0 < ne) {
+            const int k = k0 + lane;
+            int used = 0;
+            if (k < ne) {
+                hp_stream rs;
+                hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, 0u);
+                for (int jj = 0; jj < d.mcc_n; jj++) {
+                    if (hp_stream_next(&rs) < P2) {
+                        used = jj + 1;
+                        break;
                     }
+                }
+            }
+            const unsigned b = __ballot_sync(FULL, used > 0);
+            if (used) ring[(tail + __popc(b & lt)) & (MCC_RING - 1)] = k | (used << 20);
+            tail += __popc(b);
+        }
+        __syncwarp();
+        const bool last = k0 + 32 >= ne;
+        while (tail - head >= 32 || (last && tail > head)) {
+            const int e = head + lane;
+            bool create = false;
+            NewPair np;
+            if (e < tail) {
+                const int ent = ring[e & (MCC_RING - 1)];
+                const int k = ent & 0xFFFFF, used = ent >> 20;
+                hp_stream rs;
+                hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, 0u);
+                const float R1 = stream_replay(rs, used);
+                create = mcc_el_collide(d, el, ebase + k, rs, R1, P1, bvel, cnt_ch, np);
+            }
+            const unsigned bc = __ballot_sync(FULL, create);
+            if (create) {
+                const int off = add + __popc(bc & lt);
+                const int se = ne + off, sn = ni + off;
+                if (se < el.cap && sn < ion.cap) {
+                    const size_t qe = ebase + se, qi = ibase + sn;
+                    el.x[qe] = np.x; el.y[qe] = np.y;
+                    el.vx[qe] = np.evx; el.vy[qe] = np.evy; el.vz[qe] = np.evz;
+                    ion.x[qi] = np.x; ion.y[qi] = np.y;
+                    ion.vx[qi] = np.ivx; ion.vy[qi] = np.ivy; ion.vz[qi] = np.ivz;
                 } else {
-                    const float R2 = hp_stream_next(&rs) * d.sigv[1] / vel;
-                    const float SumSigma = xsec_lookup(d, 4, engy);
-                    if (engy > d.th[4] && R2 <= SumSigma) {
-                        colltype = 2;
-                        engy -= d.th[4];
-                        const float u = hp_stream_next(&rs);
-                        rengy = (float)(10.0 * (double)hp_tanf_q1(u * hp_atanf((float)(engy / 20.0))));
-                        engy -= rengy;
-                        vel = sqrtf(fabsf(rengy) / el.Escale);
-                        vel2 = sqrtf(fabsf(engy) / el.Escale);
-                        cnt_ch[4]++;
-                    }
-                }
-                if (colltype == 0) {
-                    const float a = hp_stream_next(&rs);
-                    const float b = hp_stream_next(&rs);
-                    anewvel_dev(engy, vel, VX, VY, VZ, a, b);
-                    el.vx[q] = VX;
-                    el.vy[q] = VY;
-                    el.vz[q] = VZ;
-                } else if (colltype == 2) {
-                    nx = el.x[q];
-                    ny = el.y[q];
-                    nevx = VX; nevy = VY; nevz = VZ;
-                    {
-                        const float a = hp_stream_next(&rs);
-                        const float b = hp_stream_next(&rs);
-                        anewvel_dev(rengy, vel, nevx, nevy, nevz, a, b);
-                    }
-                    nivx = VX; nivy = VY; nivz = VZ;
-                    {
-                        const int nn = (int)((d.nvel - 1) * hp_stream_next(&rs));
-                        const float a = hp_stream_next(&rs);
-                        const float b = hp_stream_next(&rs);
-                        maxwellv_dev(nivx, nivy, nivz, d.vsave[nn], bvel, a, b);
-                    }
-                    {
-                        const float a = hp_stream_next(&rs);
-                        const float b = hp_stream_next(&rs);
-                        anewvel_dev(engy, vel2, VX, VY, VZ, a, b);
-                    }
-                    el.vx[q] = VX;
-                    el.vy[q] = VY;
-                    el.vz[q] = VZ;
-                    create = true;
+                    overflow = true;
                 }
             }
+            add += __popc(bc);
+            head = min(head + 32, tail);
+            __syncwarp();
         }
-        const unsigned bc = __ballot_sync(FULL, create);
-        if (create) {
-            const int off = add + __popc(bc & lt);
-            const int se = ne + off, sn = ni + off;
-            if (se < el.cap && sn < ion.cap) {
-                const size_t qe = ebase + se, qi = ibase + sn;
-                el.x[qe] = nx; el.y[qe] = ny;
-                el.vx[qe] = nevx; el.vy[qe] = nevy; el.vz[qe] = nevz;
-                ion.x[qi] = nx; ion.y[qi] = ny;
-                ion.vx[qi] = nivx; ion.vy[qi] = nivy; ion.vz[qi] = nivz;
-            } else {
-                overflow = true;
-            }
-        }
-        add += __popc(bc);
     }
     if (__any_sync(FULL, overflow)) {
         if (lane == 0) atomicOr(d.status, ST_OVERFLOW);
@@ -620,7 +759,7 @@ __device__ __forceinline__ double warp_sum_d(double v) {
     return v;
 }
 
-__global__ void __launch_bounds__(256) k_deposit_cells(const DevCase *__restrict__ cases,
+__global__ void __launch_bounds__(512) k_deposit_cells(const DevCase *__restrict__ cases,
                                                        const int *__restrict__ item_start, int ncases, int items) {
     const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
@@ -1127,7 +1266,7 @@ inline unsigned blocks_for(long long threads, int per_block) { return (unsigned)
 cudaError_t launch_move(const DevCase *cases, const int *item_start, int ncases, int items, const LaunchCfg &lc,
                         cudaStream_t st) {
     if (items <= 0) return cudaSuccess;
-    const int tpb = 32 * lc.warps_per_block;
+    const int tpb = 32 * std::min(std::max(lc.warps_per_block, 1), 16);
     k_move<<<blocks_for((long long)items * 32, tpb), tpb, 0, st>>>(cases, item_start, ncases, items);
     return cudaGetLastError();
 }
@@ -1135,22 +1274,25 @@ cudaError_t launch_move(const DevCase *cases, const int *item_start, int ncases,
 cudaError_t launch_sort(const DevCase *cases, const int *item_start, int ncases, int items, const LaunchCfg &lc,
                         cudaStream_t st) {
     if (items <= 0) return cudaSuccess;
-    const int tpb = 32 * lc.warps_per_block;
-    k_sort<<<blocks_for((long long)items * 32, tpb), tpb, 0, st>>>(cases, item_start, ncases, items);
+    const int tpb = 32 * std::min(std::max(lc.warps_per_block, 1), SORT_MAXW);
+    k_sort_push<<<blocks_for((long long)items * 32, tpb), tpb, 0, st>>>(cases, item_start, ncases, items);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_sort_count<<<blocks_for((long long)items * 32, tpb), tpb, 0, st>>>(cases, item_start, ncases, items);
     return cudaGetLastError();
 }
 
 cudaError_t launch_mcc_ar(const DevCase *cases, const int *item_start, int ncases, int items, const LaunchCfg &lc,
                           cudaStream_t st) {
     if (items <= 0) return cudaSuccess;
-    const int tpb = 32 * lc.warps_per_block;
-    k_mcc_ar<<<blocks_for((long long)items * 32, tpb), tpb, 0, st>>>(cases, item_start, ncases, items);
+    (void)lc;
+    k_mcc_ar<<<blocks_for((long long)items * 32, MCC_TPB), MCC_TPB, 0, st>>>(cases, item_start, ncases, items);
     return cudaGetLastError();
 }
 
 cudaError_t launch_deposit(const DevCase *cases, const int *cell_items, const int *node_items, int ncases,
                            int n_cell_items, int n_node_items, const LaunchCfg &lc, cudaStream_t st) {
-    const int tpb = 32 * lc.warps_per_block;
+    const int tpb = 32 * std::min(std::max(lc.warps_per_block, 1), 16);
     if (n_cell_items > 0)
         k_deposit_cells<<<blocks_for((long long)n_cell_items * 32, tpb), tpb, 0, st>>>(cases, cell_items, ncases,
                                                                                         n_cell_items);

@@ -56,7 +56,12 @@ struct FastPlan {
     const GemmProb *probs[4] = {nullptr, nullptr, nullptr, nullptr}; // device, one list per product
     int ntiles[4] = {0, 0, 0, 0};
     int passes = 3;
+    int final_chunks = 0; // max over the cases of ceil(G / FS_CHUNK)
 };
+// nodes per CTA of the final residual pass; a case's fs_res holds
+// 2 + 2 * ceil(G / FS_CHUNK) doubles
+constexpr int FS_CHUNK = 1024;
+constexpr int FS_TILE = 32; // GEMM output tile edge
 cudaError_t launch_fast_field(const DevCase *cases, const FastPlan &fp, cudaStream_t st);
 cudaError_t launch_field(const DevCase *cases, const int *node_items, int ncases, int n_node_items,
                          const PcgGroup *groups, int ngroups, const FastPlan *fast, cudaStream_t st);

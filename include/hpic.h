@@ -235,7 +235,7 @@ hp_status hp_batch_destroy(hp_batch *b);
 hp_status hp_batch_step(hp_batch *b, int nsteps, void *stream);
 /* Per-phase launch shape chosen by the autotuner (hp_batch_autotune) or set here. */
 typedef struct hp_tune {
-    int warps_per_block_particles; /* Move/Sort/MCC/Deposit: warps per CTA (one warp per cell) */
+    int warps_per_block_particles; /* Move/Sort/Deposit: warps per CTA (one warp per cell), 1..16 */
     int pcg_block;                 /* PCG: threads per CTA */
     int pcg_cluster_max;           /* PCG: largest cluster per case */
 } hp_tune;

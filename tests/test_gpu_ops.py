@@ -31,12 +31,16 @@ DECKS = {
     "ar_65x33": (ccp_deck(65, 33, 0.02, 0.01, ppc=30), 99),
     "ar_block_33x21": (block_deck(), 4242),
 }
+# slots per cell where the deck's Max_np / Gsize leaves too little room for
+# the charge that gathers in front of the floating block
+CAP = {"ar_block_33x21": 256}
 
 
 def pair(name, field_mode=0, move_mode=0):
     deck, seed = DECKS[name]
-    S = hpic.Setup(deck, seed=seed, field_mode=field_mode, move_mode=move_mode)
-    case = hpic.Case(setup=S, seed=seed, field_mode=field_mode, move_mode=move_mode)
+    kw = dict(seed=seed, field_mode=field_mode, move_mode=move_mode, cap_per_cell=CAP.get(name, 0))
+    S = hpic.Setup(deck, **kw)
+    case = hpic.Case(setup=S, **kw)
     info = case.info
     o = oracle.Oracle(S.table, S.info, case.opts, 32, pcg_cluster=info.pcg_cluster, pcg_block=info.pcg_block)
     for s in range(S.info.nsp):
