@@ -45,14 +45,6 @@ def make_deck(w):
                     pressure_torr=w["pressure"])
 
 
-def launches_per_step(case):
-    """Kernels of one graph-captured step (counted from the launch sequence in
-    hybrid-final_b200/csrc/capi.cu one_step and kernels.cu launch_field)."""
-    mode = case.info.field_mode
-    field = (3 * 5 + 1) if mode == 2 else 1  # refinement passes (resid + 4 GEMMs) + final, or one PCG
-    return 1 + field + 2 + 1 + 1 + 1 + 2 + 1  # advance, field, potential+E, move, sort, mcc, deposit x2, accumulate
-
-
 class ClockSampler:
     """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
@@ -276,7 +268,7 @@ def run_ours(args, rank, world, local, dist):
         roofline=dict(bound="hbm", kernel="k_move", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
                       peak_source=peak_kind, traffic=traffic, algorithmic_bytes_per_launch=move_bytes),
         op_ms=op_ms,
-        gpu_launches=launches_per_step(case) * args.steps,
+        gpu_launches=case.step_kernels() * args.steps,
         clocks=clk,
     )
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -32,6 +32,7 @@ struct hp_batch {
     int device = 0;
     cudaStream_t own = nullptr;
     cudaGraphExec_t graph = nullptr;
+    int graph_kernels = 0;
 };
 
 namespace hpi {
@@ -135,6 +136,7 @@ hp_status capture(hp_batch *b) {
     cudaError_t e = cudaStreamEndCapture(b->own, &g);
     if (s1 != HP_OK) return s1;
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+    b->graph_kernels = hpi::count_kernel_nodes(g);
     e = cudaGraphInstantiate(&b->graph, g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
@@ -312,3 +314,9 @@ hp_status hp_batch_autotune(hp_batch *b, void *stream) {
 }
 
 } // extern "C"
+
+extern "C" hp_status hp_batch_step_kernels(const hp_batch *b, int *n) {
+    if (!b || !n) return HP_ERR_ARG;
+    *n = b->graph_kernels;
+    return HP_OK;
+}

@@ -18,6 +18,19 @@ thread_local std::string g_err;
 
 void set_error(const std::string &m) { g_err = m; }
 
+int count_kernel_nodes(cudaGraph_t g) {
+    size_t n = 0;
+    if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0) return 0;
+    std::vector<cudaGraphNode_t> nodes(n);
+    if (cudaGraphGetNodes(g, nodes.data(), &n) != cudaSuccess) return 0;
+    int k = 0;
+    for (size_t q = 0; q < n; q++) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nodes[q], &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) k++;
+    }
+    return k;
+}
+
 hp_status cuda_fail(cudaError_t e, const char *what) {
     set_error(std::string(what) + ": " + cudaGetErrorString(e));
     return HP_ERR_CUDA;
@@ -713,6 +726,7 @@ hp_status hp_step(hp_case *c, int nsteps, void *stream) {
         cudaError_t e = cudaStreamEndCapture(c->own_stream, &g);
         if (s1 != HP_OK) return s1;
         if (e != cudaSuccess) return cuda_fail(e, "cudaStreamEndCapture");
+        c->graph_kernels = hpi::count_kernel_nodes(g);
         e = cudaGraphInstantiate(&c->graph, g, 0);
         cudaGraphDestroy(g);
         if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
@@ -720,6 +734,12 @@ hp_status hp_step(hp_case *c, int nsteps, void *stream) {
     }
     for (int k = 0; k < nsteps; k++) CK(cudaGraphLaunch(c->graph, st));
     c->last_stream = st;
+    return HP_OK;
+}
+
+hp_status hp_step_kernels(const hp_case *c, int *n) {
+    if (!c || !n) return HP_ERR_ARG;
+    *n = c->graph_kernels;
     return HP_OK;
 }
 

@@ -47,6 +47,7 @@ struct hp_case {
     int fs_passes = 3;
     hpi::FastPlanDev fplan;        // its device lists (one-case plan)
     cudaGraphExec_t graph = nullptr;
+    int graph_kernels = 0; // kernel nodes in the captured step
     hp_batch *batch = nullptr;
     std::vector<float> prob; // [3*C]
 };
@@ -55,6 +56,8 @@ namespace hpi {
 hp_status fast_plan_build(hp_case *const *cases, const std::vector<int> &idx, FastPlanDev &out);
 void fast_plan_free(FastPlanDev &f);
 void set_error(const std::string &m);
+// kernel nodes of a captured graph
+int count_kernel_nodes(cudaGraph_t g);
 hp_status cuda_fail(cudaError_t e, const char *what);
 // Build the per-case prefix arrays and device descriptor array of a batch.
 struct BatchDev {

@@ -94,6 +94,8 @@ _SIGS = {
     "hp_MCC": (C.c_int, [_P, _P]),
     "hp_Deposit": (C.c_int, [_P, _P]),
     "hp_step": (C.c_int, [_P, C.c_int, _P]),
+    "hp_step_kernels": (C.c_int, [_P, C.POINTER(C.c_int)]),
+    "hp_batch_step_kernels": (C.c_int, [_P, C.POINTER(C.c_int)]),
     "hp_Deposit_noalloc": (C.c_int, [_P, _P, _P]),
     "hp_get_particles": (C.c_int, [_P, C.c_int, _I, _F, _F, _F, _F, _F, C.c_size_t, C.POINTER(C.c_size_t)]),
     "hp_set_particles": (C.c_int, [_P, C.c_int, _I, _F, _F, _F, _F, _F]),
@@ -274,6 +276,12 @@ class Case:
         _check(lib().hp_last_field_residual(self.h, C.byref(r)))
         return r.value
 
+    def step_kernels(self):
+        """Kernels one step launches (after the first step captured it)."""
+        n = C.c_int(0)
+        _check(lib().hp_step_kernels(self.h, C.byref(n)))
+        return n.value
+
     def pushes(self):
         n = C.c_int64(0)
         _check(lib().hp_case_pushes(self.h, C.byref(n)))
@@ -360,6 +368,11 @@ class Batch:
 
     def step(self, n=1, stream=None):
         _check(lib().hp_batch_step(self.h, n, stream))
+
+    def step_kernels(self):
+        n = C.c_int(0)
+        _check(lib().hp_batch_step_kernels(self.h, C.byref(n)))
+        return n.value
 
     def tune(self):
         t = Tune()

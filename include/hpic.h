@@ -167,6 +167,10 @@ hp_status hp_Deposit_noalloc(hp_case *c, double *den_out, void *stream);
  * diagnostics and dump calls), fused where results allow; replayed from a
  * CUDA graph after the first call on a stream. */
 hp_status hp_step(hp_case *c, int nsteps, void *stream);
+/* Kernels launched by one hp_step (the kernel nodes of its captured graph;
+ * 0 before the first hp_step).  No reference counterpart: launch accounting
+ * for benchmarks. */
+hp_status hp_step_kernels(const hp_case *c, int *n);
 
 /* ------------------------------------------------- state interchange (host) */
 /* Particles of species isp in cell-sorted order.  counts[Csize] receives the
@@ -233,6 +237,9 @@ typedef struct hp_batch hp_batch;
 hp_status hp_batch_create(hp_case *const *cases, int n, hp_batch **out);
 hp_status hp_batch_destroy(hp_batch *b);
 hp_status hp_batch_step(hp_batch *b, int nsteps, void *stream);
+/* Kernels launched by one hp_batch_step (0 before the first).  No reference
+ * counterpart. */
+hp_status hp_batch_step_kernels(const hp_batch *b, int *n);
 /* Per-phase launch shape chosen by the autotuner (hp_batch_autotune) or set here. */
 typedef struct hp_tune {
     int warps_per_block_particles; /* Move/Sort/Deposit: warps per CTA (one warp per cell), 1..16 */
