@@ -100,11 +100,14 @@ __device__ __forceinline__ int walk(const DevCase &d, int &i, int &j, float &lx,
                                     int &cond) {
     const int maxs = d.move_mode ? 2 * (d.ncx + d.ncy) + 4 : 1;
     for (int s = 0; s < maxs; s++) {
+        // the reference computes these in double and rounds back to float;
+        // for float operands a -+ 1 is exact in double, so the single
+        // float operation rounds the same exact value to the same result
         int di = 0, dj = 0;
-        if (ly >= 1) { dj = 1; ly = (float)((double)ly - 1.0); }
-        else if (ly < 0) { dj = -1; ly = (float)((double)ly + 1.0); }
-        if (lx >= 1) { di = 1; lx = (float)((double)lx - 1.0); }
-        else if (lx < 0) { di = -1; lx = (float)((double)lx + 1.0); }
+        if (ly >= 1) { dj = 1; ly = ly - 1.0f; }
+        else if (ly < 0) { dj = -1; ly = ly + 1.0f; }
+        if (lx >= 1) { di = 1; lx = lx - 1.0f; }
+        else if (lx < 0) { di = -1; lx = lx + 1.0f; }
         const MoverFate f = mover_fate(d, i, j, di, dj);
         if (f.absorbed) {
             cond = f.cond;
@@ -174,17 +177,29 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
     const size_t base = (size_t)c * cap;
     const unsigned lt = lanemask_lt();
     int m = 0;
-    int dc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    // per-lane mover counts per destination code, three 21-bit fields per word
+    unsigned long long pk0 = 0, pk1 = 0, pk2 = 0;
+    // software pipeline: the next chunk's loads are in flight while this one
+    // is pushed (stores only go to slots at or below the current chunk, or to
+    // the top region at or above cap - n >= n, so no unread slot is touched)
+    float lx = 0.f, ly = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
+    if (lane < n) {
+        lx = sp.x[base + lane];
+        ly = sp.y[base + lane];
+        vx = sp.vx[base + lane];
+        vy = sp.vy[base + lane];
+        vz = sp.vz[base + lane];
+    }
     for (int k0 = 0; k0 < n; k0 += 32) {
         const int k = k0 + lane;
         const bool act = k < n;
-        float lx = 0.f, ly = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
-        if (act) {
-            lx = sp.x[base + k];
-            ly = sp.y[base + k];
-            vx = sp.vx[base + k];
-            vy = sp.vy[base + k];
-            vz = sp.vz[base + k];
+        float nlx = 0.f, nly = 0.f, nvx = 0.f, nvy = 0.f, nvz = 0.f;
+        if (k + 32 < n) {
+            nlx = sp.x[base + k + 32];
+            nly = sp.y[base + k + 32];
+            nvx = sp.vx[base + k + 32];
+            nvy = sp.vy[base + k + 32];
+            nvz = sp.vz[base + k + 32];
         }
         const float del_vx = ex_ws * (1 - lx) * (1 - ly) + ex_wn * (1 - lx) * ly + ex_es * lx * (1 - ly) + ex_en * lx * ly;
         const float del_vy = ey_ws * (1 - lx) * (1 - ly) + ey_wn * (1 - lx) * ly + ey_es * lx * (1 - ly) + ey_en * lx * ly;
@@ -205,10 +220,17 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
                 const int ddi = fi - i, ddj = fj - j;
                 code = (ddi >= -1 && ddi <= 1 && ddj >= -1 && ddj <= 1) ? (ddi + 1) * 3 + (ddj + 1) : CODE_FAR;
             }
+            if (code < 9) {
+                const int q3 = code / 3;
+                const unsigned long long one = 1ull << (21 * (code - 3 * q3));
+                if (q3 == 0) pk0 += one;
+                else if (q3 == 1) pk1 += one;
+                else pk2 += one;
+            }
         }
         const unsigned bout = __ballot_sync(FULL, out);
         const int before = m + __popc(bout & lt);
-        __syncwarp();
+        __syncwarp(); // every lane's loads of this chunk precede the in-place stores
         if (act) {
             const size_t dst = out ? base + (size_t)(cap - 1 - before) : base + (size_t)(k - before);
             sp.x[dst] = lx;
@@ -227,8 +249,7 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
             }
         }
         m += __popc(bout);
-#pragma unroll
-        for (int D = 0; D < 9; D++) dc[D] += __popc(__ballot_sync(FULL, out && code == D));
+        lx = nlx; ly = nly; vx = nvx; vy = nvy; vz = nvz;
     }
     if (lane == 0) {
         sp.cnt[c] = n - m;
@@ -236,8 +257,11 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
     }
     int mine = 0;
 #pragma unroll
-    for (int D = 0; D < 9; D++)
-        if (lane == D) mine = dc[D];
+    for (int D = 0; D < 9; D++) {
+        const unsigned long long wv = D < 3 ? pk0 : D < 6 ? pk1 : pk2;
+        const unsigned t = __reduce_add_sync(FULL, (unsigned)((wv >> (21 * (D % 3))) & 0x1FFFFFull));
+        if (lane == D) mine = (int)t;
+    }
     if (lane < 9) sp.dcount[(size_t)c * 9 + lane] = mine;
 }
 

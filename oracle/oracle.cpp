@@ -252,11 +252,14 @@ template <class R> struct Sim : SimBase {
     int walk(int &i, int &j, R &lx, R &ly, R &vx, R &vy, int &cond) const {
         const int maxs = c.move_mode ? 2 * (c.ncx + c.ncy) + 4 : 1;
         for (int st = 0; st < maxs; st++) {
+            // the reference computes (float)((double)l -+ 1.0); for a float l
+            // the double difference is exact, so one operation in R rounds
+            // the same exact value identically
             int di = 0, dj = 0;
-            if (ly >= 1) { dj = 1; ly = (R)((double)ly - 1.0); }
-            else if (ly < 0) { dj = -1; ly = (R)((double)ly + 1.0); }
-            if (lx >= 1) { di = 1; lx = (R)((double)lx - 1.0); }
-            else if (lx < 0) { di = -1; lx = (R)((double)lx + 1.0); }
+            if (ly >= 1) { dj = 1; ly = ly - (R)1; }
+            else if (ly < 0) { dj = -1; ly = ly + (R)1; }
+            if (lx >= 1) { di = 1; lx = lx - (R)1; }
+            else if (lx < 0) { di = -1; lx = lx + (R)1; }
             const Fate f = fate(i, j, di, dj);
             if (f.absorbed) {
                 cond = f.cond;
@@ -1094,6 +1097,21 @@ void or_get_movers(or_sim *s, int isp, int *counts, float *x, float *y, float *v
 }
 void or_get_grid(or_sim *s, int which, void *out) { s->impl->get_grid(which, out); }
 void or_set_grid(or_sim *s, int which, const void *in) { s->impl->set_grid(which, in); }
+void or_math(int fn, const float *x, const float *y, float *out, int n) {
+    for (int k = 0; k < n; k++) {
+        float s_, c_;
+        switch (fn) {
+        case 0: out[k] = hp_expf(x[k]); break;
+        case 1: out[k] = hp_logf(x[k]); break;
+        case 2: out[k] = hp_log10f(x[k]); break;
+        case 3: out[k] = hp_powf(x[k], y[k]); break;
+        case 4: hp_sincos_turns(x[k], &s_, &c_); out[k] = s_; break;
+        case 5: hp_sincos_turns(x[k], &s_, &c_); out[k] = c_; break;
+        case 6: out[k] = hp_tanf_q1(x[k]); break;
+        default: out[k] = hp_atanf(x[k]); break;
+        }
+    }
+}
 int or_walk_bound_hit(or_sim *s) { return s->impl->walk_bound_hit ? 1 : 0; }
 void or_get_counters(or_sim *s, float *cond_charge, unsigned *mcc_count, int *pcg_iters) {
     SimBase *b = s->impl;

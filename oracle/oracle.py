@@ -69,6 +69,7 @@ def lib():
             "or_set_grid": (None, [P, C.c_int, P]),
             "or_get_counters": (None, [P, _F, C.POINTER(C.c_uint), _I]),
             "or_walk_bound_hit": (C.c_int, [P]),
+            "or_math": (None, [C.c_int, _F, _F, _F, C.c_int]),
             "or_field": (None, [P, C.c_int64]),
             "or_move": (None, [P]),
             "or_sort": (None, [P]),
