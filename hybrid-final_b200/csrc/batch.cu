@@ -158,6 +158,13 @@ hp_status hp_batch_create(hp_case *const *cases, int n, hp_batch **out) {
         for (int j = 0; j < i; j++)
             if (cases[j] == cases[i]) return set_error("case listed twice"), HP_ERR_ARG;
     }
+    int passes = 0; // the separable solves of a batch run their refinement passes together
+    for (int i = 0; i < n; i++) {
+        if (cases[i]->h.field_mode != 2) continue;
+        if (passes && cases[i]->h.fs_passes != passes)
+            return set_error("field_mode 2 cases of a batch need the same fs_passes"), HP_ERR_ARG;
+        passes = cases[i]->h.fs_passes;
+    }
     CK(cudaSetDevice(dev));
     for (int i = 0; i < n; i++) CK(cudaStreamSynchronize(cases[i]->last_stream));
     hp_batch *b = new hp_batch();

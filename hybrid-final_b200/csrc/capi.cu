@@ -344,6 +344,10 @@ hp_status build_device(hp_case *c) {
         if (build_fast_solver(s, c->fs)) {
             const size_t nxy = (size_t)c->fs.nx * c->fs.ny;
             h.fs_i0 = c->fs.i0; h.fs_j0 = c->fs.j0; h.fs_nx = c->fs.nx; h.fs_ny = c->fs.ny;
+            {
+                const double rtol = c->opts.pcg_rtol > 0 ? c->opts.pcg_rtol : 1e-8;
+                c->fs_passes = c->opts.fs_passes > 0 ? c->opts.fs_passes : (rtol >= 1e-10 ? 2 : 3);
+            }
             h.fs_passes = c->fs_passes;
             TRY(dupload(c, (float **)&h.fs_V, c->fs.V));
             TRY(dupload(c, (float **)&h.fs_Vt, c->fs.Vt));

@@ -506,20 +506,26 @@ __device__ __forceinline__ void newvel_ionsc_dev(float &vxs, float &vys, float &
 // Most particles do not collide in a step (a few per cent), and a colliding
 // lane runs a long path (cross sections, scattering angles, the ionisation
 // energy split) while the rest of its warp would idle.  So each warp first
-// runs the cheap null-collision test over its cell and queues the colliders
-// in particle order in a shared-memory ring; every 32 queued colliders are
-// then processed by the whole warp, one per lane.  A collider's stream is
-// re-created from its key and advanced past the draws the test consumed, so
-// every particle's arithmetic and draws are exactly those of a lane-per-
-// particle loop, and new particles are still appended in particle order.
+// runs the cheap null-collision test over its cell, four slots per lane and
+// one Philox block per lane (hp_test_block), and queues the colliders in
+// particle order in a shared-memory ring; every 32 queued colliders are then
+// processed by the whole warp, one per lane, each from its own stream.  Every
+// particle's arithmetic and draws are exactly those of a lane-per-particle
+// loop, and new particles are still appended in particle order.
 constexpr int MCC_TPB = 256;
-constexpr int MCC_RING = 64;
+constexpr int MCC_RING = 256; // >= 128 new entries per pass + 31 pending
 
-// advance a fresh stream by n draws; returns the last draw (n >= 1)
-__device__ __forceinline__ float stream_replay(hp_stream &rs, int n) {
-    float r = 0.f;
-    for (int t = 0; t < n; t++) r = hp_stream_next(&rs);
-    return r;
+// exclusive count of set bits of `mask4` (4 slots per lane) in lower lanes
+__device__ __forceinline__ int lower_lane_hits(unsigned mask4, unsigned lt, int &total) {
+    int pre = 0;
+    total = 0;
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+        const unsigned b = __ballot_sync(FULL, (mask4 >> t) & 1u);
+        pre += __popc(b & lt);
+        total += __popc(b);
+    }
+    return pre;
 }
 
 __device__ __forceinline__ void mcc_ion_collide(const DevCase &d, const DevSpecies &ion, size_t q, hp_stream &rs,
@@ -665,66 +671,75 @@ __global__ void __launch_bounds__(MCC_TPB) k_mcc_ar(const DevCase *__restrict__ 
     const float bvel = d.back_vel1[node];
     const unsigned lt = lanemask_lt();
     unsigned cnt_ch[7] = {0, 0, 0, 0, 0, 0, 0};
-    // ---- ions: test, queue, collide 32 at a time
+    // ---- ions: test (4 slots per lane), queue, collide 32 at a time
     const DevSpecies &ion = d.sp[1];
     const int ni = ion.cnt[c];
     const size_t ibase = (size_t)c * ion.cap;
     int head = 0, tail = 0;
-    for (int k0 = 0; k0 < ni || tail > head; k0 += 32) {
+    for (int k0 = 0; k0 < ni || tail > head; k0 += 128) {
         if (k0 < ni) {
-            const int k = k0 + lane;
-            bool hit = false;
+            const int k = k0 + 4 * lane;
+            unsigned hits = 0;
             if (k < ni) {
-                hp_stream rs;
-                hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, 1u);
-                hit = hp_stream_next(&rs) <= Pion;
+                const hp_u4 u = hp_test_block(d.seed, (uint32_t)(k >> 2), (uint32_t)c, step, 1u, 0u);
+#pragma unroll
+                for (int t = 0; t < 4; t++)
+                    if (k + t < ni && hp_u01(hp_word(u, (uint32_t)t)) <= Pion) hits |= 1u << t;
             }
-            const unsigned b = __ballot_sync(FULL, hit);
-            if (hit) ring[(tail + __popc(b & lt)) & (MCC_RING - 1)] = k;
-            tail += __popc(b);
+            int total;
+            int pos = tail + lower_lane_hits(hits, lt, total);
+#pragma unroll
+            for (int t = 0; t < 4; t++)
+                if ((hits >> t) & 1u) ring[(pos++) & (MCC_RING - 1)] = k + t;
+            tail += total;
         }
         __syncwarp();
-        const bool last = k0 + 32 >= ni;
+        const bool last = k0 + 128 >= ni;
         while (tail - head >= 32 || (last && tail > head)) {
             const int e = head + lane;
             if (e < tail) {
                 const int k = ring[e & (MCC_RING - 1)];
                 hp_stream rs;
                 hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, 1u);
-                stream_replay(rs, 1);
                 mcc_ion_collide(d, ion, ibase + k, rs, bvel, cnt_ch);
             }
             head = min(head + 32, tail);
             __syncwarp();
         }
     }
-    // ---- electrons: queue entries are slot | draws used << 20
+    // ---- electrons: queue entries are slot | sub-cycle of the hit + 1 << 20
     const DevSpecies &el = d.sp[0];
     const int ne = el.cnt[c];
     const size_t ebase = (size_t)c * el.cap;
     int add = 0;
     bool overflow = false;
     head = tail = 0;
-    for (int k0 = 0; k0 < ne || tail > head; k0 += 32) {
+    for (int k0 = 0; k0 < ne || tail > head; k0 += 128) {
         if (k0 < ne) {
-            const int k = k0 + lane;
-            int used = 0;
+            const int k = k0 + 4 * lane;
+            unsigned hits = 0;
+            int used[4] = {0, 0, 0, 0};
             if (k < ne) {
-                hp_stream rs;
-                hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, 0u);
-                for (int jj = 0; jj < d.mcc_n; jj++) {
-                    if (hp_stream_next(&rs) < P2) {
-                        used = jj + 1;
-                        break;
-                    }
+                const unsigned live = k + 4 <= ne ? 0xFu : (1u << (ne - k)) - 1u;
+                for (int jj = 0; jj < d.mcc_n && (hits != live); jj++) {
+                    const hp_u4 u = hp_test_block(d.seed, (uint32_t)(k >> 2), (uint32_t)c, step, 0u, (uint32_t)jj);
+#pragma unroll
+                    for (int t = 0; t < 4; t++)
+                        if (((live & ~hits) >> t) & 1u && hp_u01(hp_word(u, (uint32_t)t)) < P2) {
+                            hits |= 1u << t;
+                            used[t] = jj + 1;
+                        }
                 }
             }
-            const unsigned b = __ballot_sync(FULL, used > 0);
-            if (used) ring[(tail + __popc(b & lt)) & (MCC_RING - 1)] = k | (used << 20);
-            tail += __popc(b);
+            int total;
+            int pos = tail + lower_lane_hits(hits, lt, total);
+#pragma unroll
+            for (int t = 0; t < 4; t++)
+                if ((hits >> t) & 1u) ring[(pos++) & (MCC_RING - 1)] = (k + t) | (used[t] << 20);
+            tail += total;
         }
         __syncwarp();
-        const bool last = k0 + 32 >= ne;
+        const bool last = k0 + 128 >= ne;
         while (tail - head >= 32 || (last && tail > head)) {
             const int e = head + lane;
             bool create = false;
@@ -732,9 +747,10 @@ __global__ void __launch_bounds__(MCC_TPB) k_mcc_ar(const DevCase *__restrict__ 
             if (e < tail) {
                 const int ent = ring[e & (MCC_RING - 1)];
                 const int k = ent & 0xFFFFF, used = ent >> 20;
+                const float R1 =
+                    hp_test_draw(d.seed, (uint32_t)k, (uint32_t)c, step, 0u, (uint32_t)(used - 1));
                 hp_stream rs;
                 hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, 0u);
-                const float R1 = stream_replay(rs, used);
                 create = mcc_el_collide(d, el, ebase + k, rs, R1, P1, bvel, cnt_ch, np);
             }
             const unsigned bc = __ballot_sync(FULL, create);

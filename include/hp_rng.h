@@ -16,6 +16,14 @@
  * draw order depends on the per-cell loop; a per-particle key makes the
  * draws independent of how particles are mapped to threads.
  *
+ * The null-collision test, the one draw every particle makes in a step,
+ * comes from a separate block shared by four consecutive slots of a cell:
+ *     counter = (slot / 4, cell, step, species << 16 | 0x8000 | sub)
+ * slot 4g + t takes word t, and sub is the electron sub-cycle (0 for ions).
+ * So one Philox evaluation tests four particles; a particle that collides
+ * then draws everything else from its own stream above, starting at word 0
+ * of block 0.  Particle streams use block numbers below 0x8000.
+ *
  * Uniforms are (x >> 8 + 1) * 2^-24, in (0, 1] like curand_uniform.
  */
 #ifndef HP_RNG_H
@@ -93,6 +101,27 @@ HP_HD float hp_stream_next(hp_stream *s) {
     uint32_t v = (s->used == 0) ? s->buf.x : (s->used == 1) ? s->buf.y : (s->used == 2) ? s->buf.z : s->buf.w;
     s->used++;
     return hp_u01(v);
+}
+
+#define HP_TEST_BLOCK 0x8000u
+
+/* The null-collision test block of slots 4*group .. 4*group+3. */
+HP_HD hp_u4 hp_test_block(uint64_t seed, uint32_t group, uint32_t cell, uint32_t step, uint32_t species,
+                          uint32_t sub) {
+    hp_u4 ctr;
+    ctr.x = group;
+    ctr.y = cell;
+    ctr.z = step;
+    ctr.w = (species << 16) | HP_TEST_BLOCK | sub;
+    return hp_philox4x32_10(ctr, (uint32_t)seed, (uint32_t)(seed >> 32));
+}
+
+HP_HD uint32_t hp_word(hp_u4 b, uint32_t t) { return t == 0 ? b.x : t == 1 ? b.y : t == 2 ? b.z : b.w; }
+
+/* The null-collision test draw of one slot. */
+HP_HD float hp_test_draw(uint64_t seed, uint32_t slot, uint32_t cell, uint32_t step, uint32_t species,
+                         uint32_t sub) {
+    return hp_u01(hp_word(hp_test_block(seed, slot >> 2, cell, step, species, sub), slot & 3u));
 }
 
 #endif /* HP_RNG_H */

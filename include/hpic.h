@@ -94,6 +94,8 @@ typedef struct hp_case_opts {
                             step keeps an offset outside [0,1) and its later gathers read the wrong
                             cell); 1 = cross cell by cell, with the boundary rule of every cell entered,
                             until the offset is inside a cell */
+    int fs_passes;       /* field_mode 2: FP64 refinement passes per solve; 0 = 2 when pcg_rtol >= 1e-10
+                            (each pass gains ~6 digits), else 3 */
 } hp_case_opts;
 
 /* Default options. */

@@ -483,10 +483,9 @@ template <class R> struct Sim : SimBase {
             unsigned cnt_ch[7] = {0, 0, 0, 0, 0, 0, 0};
             const int ni = ion.cnt[cell];
             for (int k = 0; k < ni; k++) {
+                if (hp_test_draw(c.seed, (uint32_t)k, (uint32_t)cell, step, 1u, 0u) > Pion) continue;
                 hp_stream rs;
                 hp_stream_init(&rs, c.seed, (uint32_t)k, (uint32_t)cell, step, 1u);
-                float R1 = hp_stream_next(&rs);
-                if (R1 > Pion) continue;
                 const int nn = (int)((c.nvel - 1) * hp_stream_next(&rs));
                 R vnx, vny, vnz;
                 {
@@ -517,15 +516,15 @@ template <class R> struct Sim : SimBase {
             }
             const int ne = el.cnt[cell];
             for (int k = 0; k < ne; k++) {
-                hp_stream rs;
-                hp_stream_init(&rs, c.seed, (uint32_t)k, (uint32_t)cell, step, 0u);
                 int colltype = 0;
                 float R1 = 0.f;
                 for (int jj = 0; jj < c.mcc_n; jj++) {
-                    R1 = hp_stream_next(&rs);
+                    R1 = hp_test_draw(c.seed, (uint32_t)k, (uint32_t)cell, step, 0u, (uint32_t)jj);
                     if (R1 < P2) { colltype = 1; break; }
                 }
                 if (!colltype) continue;
+                hp_stream rs;
+                hp_stream_init(&rs, c.seed, (uint32_t)k, (uint32_t)cell, step, 0u);
                 const int target = (R1 <= P1) ? 0 : 1;
                 const size_t q = (size_t)el.start[cell] + k;
                 R VX = el.vx[q], VY = el.vy[q], VZ = el.vz[q];

@@ -103,7 +103,7 @@ class Oracle:
     GRID = dict(EX=0, EY=1, PHI=2, PHI_POIS=3, DEN=4, SOURCE=5, B=6, X=7)
 
     def __init__(self, tables, info, opts, precision=32, pcg_cluster=1, pcg_block=512, field_mode=None,
-                 fs_passes=3):
+                 fs_passes=None):
         self.info = info
         self.keep = {}
         t = tables
@@ -181,6 +181,9 @@ class Oracle:
             fi = t("fs_info")
             if fi[0]:
                 c.fs_i0, c.fs_j0, c.fs_nx, c.fs_ny = (int(v) for v in fi[1:5])
+                if fs_passes is None:  # the library's default
+                    rtol = opts.pcg_rtol if opts.pcg_rtol > 0 else 1e-8
+                    fs_passes = opts.fs_passes if opts.fs_passes > 0 else (2 if rtol >= 1e-10 else 3)
                 c.fs_passes = fs_passes
                 c.fs_V = keep("fsV", t("fs_V"), np.float32)
                 c.fs_Vt = keep("fsVt", t("fs_Vt"), np.float32)
