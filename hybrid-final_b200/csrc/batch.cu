@@ -223,13 +223,11 @@ hp_status hp_batch_step(hp_batch *b, int nsteps, void *stream) {
 
 hp_status hp_batch_set_tune(hp_batch *b, const hp_tune *t) {
     if (!b || !t) return HP_ERR_ARG;
-    if (t->warps_per_block_particles < 1 || t->warps_per_block_particles > 16) return HP_ERR_ARG;
-    if (t->pcg_block < 64 || t->pcg_block > 512 || (t->pcg_block & 31)) return HP_ERR_ARG;
-    if (t->pcg_cluster_max < 1 || t->pcg_cluster_max > 16 || (t->pcg_cluster_max & (t->pcg_cluster_max - 1)))
-        return HP_ERR_ARG;
+    if (!hpi::tune_valid(*t)) return set_error("hp_tune out of range"), HP_ERR_ARG;
     b->lc.warps_per_block = t->warps_per_block_particles;
     b->lc.pcg_block = t->pcg_block;
     b->lc.pcg_cluster_max = t->pcg_cluster_max;
+    b->lc.move_unroll = t->move_unroll;
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
@@ -242,6 +240,7 @@ hp_status hp_batch_get_tune(hp_batch *b, hp_tune *t) {
     t->warps_per_block_particles = b->lc.warps_per_block;
     t->pcg_block = b->lc.pcg_block;
     t->pcg_cluster_max = b->lc.pcg_cluster_max;
+    t->move_unroll = b->lc.move_unroll;
     return HP_OK;
 }
 
@@ -284,11 +283,14 @@ hp_status hp_batch_autotune(hp_batch *b, void *stream) {
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     hp_status result = HP_OK;
+    const int unrolls[3] = {1, 2, 4};
+    for (int pi = 0; pi < 3 && result == HP_OK; pi++)
     for (int wi = 0; wi < 3 && result == HP_OK; wi++)
         for (int bi = 0; bi < 3 && result == HP_OK; bi++)
             for (int ki = 0; ki < 3 && result == HP_OK; ki++) {
                 if (ki > 0 && clus[ki] == clus[ki - 1]) continue;
                 LaunchCfg lc = base;
+                lc.move_unroll = unrolls[pi];
                 lc.warps_per_block = warps[wi];
                 lc.pcg_block = blocks[bi];
                 lc.pcg_cluster_max = clus[ki];

@@ -18,6 +18,14 @@ thread_local std::string g_err;
 
 void set_error(const std::string &m) { g_err = m; }
 
+bool tune_valid(const hp_tune &t) {
+    if (t.warps_per_block_particles < 1 || t.warps_per_block_particles > 16) return false;
+    if (t.pcg_block < 64 || t.pcg_block > 512 || (t.pcg_block & 31)) return false;
+    if (t.pcg_cluster_max < 1 || t.pcg_cluster_max > 16 || (t.pcg_cluster_max & (t.pcg_cluster_max - 1)))
+        return false;
+    return t.move_unroll == 1 || t.move_unroll == 2 || t.move_unroll == 4;
+}
+
 int count_kernel_nodes(cudaGraph_t g) {
     size_t n = 0;
     if (cudaGraphGetNodes(g, nullptr, &n) != cudaSuccess || n == 0) return 0;
@@ -738,6 +746,32 @@ hp_status hp_step(hp_case *c, int nsteps, void *stream) {
     }
     for (int k = 0; k < nsteps; k++) CK(cudaGraphLaunch(c->graph, st));
     c->last_stream = st;
+    return HP_OK;
+}
+
+hp_status hp_case_set_tune(hp_case *c, const hp_tune *t) {
+    if (!c || !t) return HP_ERR_ARG;
+    if (c->batch) return set_error("case belongs to a batch: tune the batch"), HP_ERR_ARG;
+    if (!hpi::tune_valid(*t)) return set_error("hp_tune out of range"), HP_ERR_ARG;
+    c->lc.warps_per_block = t->warps_per_block_particles;
+    c->lc.pcg_block = t->pcg_block;
+    c->lc.pcg_cluster_max = t->pcg_cluster_max;
+    c->lc.move_unroll = t->move_unroll;
+    c->pcg_cluster = std::min(pcg_cluster_for_nodes(c->s.Gsize), t->pcg_cluster_max);
+    if (c->graph) {
+        cudaGraphExecDestroy(c->graph);
+        c->graph = nullptr;
+        c->graph_kernels = 0;
+    }
+    return HP_OK;
+}
+
+hp_status hp_case_get_tune(const hp_case *c, hp_tune *t) {
+    if (!c || !t) return HP_ERR_ARG;
+    t->warps_per_block_particles = c->lc.warps_per_block;
+    t->pcg_block = c->lc.pcg_block;
+    t->pcg_cluster_max = c->lc.pcg_cluster_max;
+    t->move_unroll = c->lc.move_unroll;
     return HP_OK;
 }
 

@@ -58,6 +58,8 @@ void fast_plan_free(FastPlanDev &f);
 void set_error(const std::string &m);
 // kernel nodes of a captured graph
 int count_kernel_nodes(cudaGraph_t g);
+// launch shapes the kernels accept
+bool tune_valid(const hp_tune &t);
 hp_status cuda_fail(cudaError_t e, const char *what);
 // Build the per-case prefix arrays and device descriptor array of a batch.
 struct BatchDev {

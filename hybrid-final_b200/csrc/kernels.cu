@@ -56,7 +56,17 @@ struct MoverFate {
     int cond; // conductor index or -1
 };
 
-__device__ __forceinline__ MoverFate mover_fate(const DevCase &d, int si, int sj, int di, int dj) {
+// The geometry a crossing needs, held in registers by the caller: the
+// particle stores of Move could alias the case descriptor as far as the
+// compiler knows, so fields read through it would be re-loaded after every
+// store.
+struct Geo {
+    const int *__restrict__ sidx;
+    int ncx, ncy, move_mode;
+};
+__device__ __forceinline__ Geo geo_of(const DevCase &d) { return Geo{d.sidx, d.ncx, d.ncy, d.move_mode}; }
+
+__device__ __forceinline__ MoverFate mover_fate(const Geo d, int si, int sj, int di, int dj) {
     MoverFate f;
     f.fi = si + di;
     f.fj = sj + dj;
@@ -96,7 +106,7 @@ constexpr int FAR_B = HP_FAR_BUCKET;
 // outside [0,1)); move_mode 1 crosses until the offset is back in [0,1).
 // Returns 0 when the particle stays in the domain, 1 when absorbed, 2 when the
 // crossing bound was hit (absorbed and flagged).
-__device__ __forceinline__ int walk(const DevCase &d, int &i, int &j, float &lx, float &ly, float &vx, float &vy,
+__device__ __forceinline__ int walk(const Geo d, int &i, int &j, float &lx, float &ly, float &vx, float &vy,
                                     int &cond) {
     const int maxs = d.move_mode ? 2 * (d.ncx + d.ncy) + 4 : 1;
     for (int s = 0; s < maxs; s++) {
@@ -133,6 +143,19 @@ __device__ __forceinline__ int walk(const DevCase &d, int &i, int &j, float &lx,
     return 0;
 }
 
+// exclusive count of set bits of `mask4` (4 slots per lane) in lower lanes
+__device__ __forceinline__ int lower_lane_hits(unsigned mask4, unsigned lt, int &total) {
+    int pre = 0;
+    total = 0;
+#pragma unroll
+    for (int t = 0; t < 4; t++) {
+        const unsigned b = __ballot_sync(FULL, (mask4 >> t) & 1u);
+        pre += __popc(b & lt);
+        total += __popc(b);
+    }
+    return pre;
+}
+
 // ------------------------------------------------------------------ Move
 // MoveE_Basic (src/cuda_Move.cu:181-270): bilinear gather of the node field,
 // v += Ascale E, x += v dt/dx in cell units.  A particle that leaves its
@@ -153,14 +176,27 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
     const int w = warp - item_start[ci];
     const int s = w / d.C, c = w - s * d.C;
     const DevSpecies &sp = d.sp[s];
+    const int cap = sp.cap;
+    const size_t base = (size_t)c * cap;
+    const int i = c / d.ncy, j = c - i * d.ncy;
+    const int node = i * d.ngy + j;
+    // the count, the cell's field corners and the first chunk are independent
+    // loads: issue them together (slots 0..31 of a cell are always inside the
+    // pool, cap >= 32; lanes past the count are ignored)
     const int n = sp.cnt[c];
+    const float ex_ws = d.Ex[node], ex_wn = d.Ex[node + 1], ex_es = d.Ex[node + d.ngy], ex_en = d.Ex[node + d.ngy + 1];
+    const float ey_ws = d.Ey[node], ey_wn = d.Ey[node + 1], ey_es = d.Ey[node + d.ngy], ey_en = d.Ey[node + d.ngy + 1];
+    float lx = sp.x[base + lane];
+    float ly = sp.y[base + lane];
+    float vx = sp.vx[base + lane];
+    float vy = sp.vy[base + lane];
+    float vz = sp.vz[base + lane];
     if (n == 0) {
         if (lane == 0) sp.nmov[c] = 0;
         if (lane < 9) sp.dcount[(size_t)c * 9 + lane] = 0;
         return;
     }
     if (lane == 0) atomicAdd(&d.pushes[warp & 31], (unsigned long long)n);
-    const int cap = sp.cap;
     if (2 * n > cap) { // the reference's ReArg condition (src/cuda_Sortboundary.cu:63-65)
         if (lane == 0) {
             sp.nmov[c] = 0;
@@ -169,12 +205,7 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
         if (lane < 9) sp.dcount[(size_t)c * 9 + lane] = 0;
         return;
     }
-    const int i = c / d.ncy, j = c - i * d.ncy;
-    const int node = i * d.ngy + j;
-    const float ex_ws = d.Ex[node], ex_wn = d.Ex[node + 1], ex_es = d.Ex[node + d.ngy], ex_en = d.Ex[node + d.ngy + 1];
-    const float ey_ws = d.Ey[node], ey_wn = d.Ey[node + 1], ey_es = d.Ey[node + d.ngy], ey_en = d.Ey[node + d.ngy + 1];
     const float As = sp.Ascale, dtdx = d.dt_dx, dtdy = d.dt_dy;
-    const size_t base = (size_t)c * cap;
     const unsigned lt = lanemask_lt();
     int m = 0;
     // per-lane mover counts per destination code, three 21-bit fields per word
@@ -182,14 +213,6 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
     // software pipeline: the next chunk's loads are in flight while this one
     // is pushed (stores only go to slots at or below the current chunk, or to
     // the top region at or above cap - n >= n, so no unread slot is touched)
-    float lx = 0.f, ly = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
-    if (lane < n) {
-        lx = sp.x[base + lane];
-        ly = sp.y[base + lane];
-        vx = sp.vx[base + lane];
-        vy = sp.vy[base + lane];
-        vz = sp.vz[base + lane];
-    }
     for (int k0 = 0; k0 < n; k0 += 32) {
         const int k = k0 + lane;
         const bool act = k < n;
@@ -211,7 +234,7 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
         int code = 4, fi = i, fj = j;
         if (out) {
             int cond = -1;
-            const int r = walk(d, fi, fj, lx, ly, mvX, mvY, cond);
+            const int r = walk(geo_of(d), fi, fj, lx, ly, mvX, mvY, cond);
             if (r) {
                 code = CODE_ABSORBED;
                 if (cond >= 0 && cond < d.cond_numr) atomicAdd(&d.cond_charge[s * d.cond_numr + cond], 1.0f);
@@ -261,6 +284,136 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
         const unsigned long long wv = D < 3 ? pk0 : D < 6 ? pk1 : pk2;
         const unsigned t = __reduce_add_sync(FULL, (unsigned)((wv >> (21 * (D % 3))) & 0x1FFFFFull));
         if (lane == D) mine = (int)t;
+    }
+    if (lane < 9) sp.dcount[(size_t)c * 9 + lane] = mine;
+}
+
+// The same push with U chunks of 32 particles loaded per iteration before
+// any of them is pushed (5*U independent loads in flight per lane instead of
+// a one-chunk prefetch).  In-place stores of a chunk only reach slots at or
+// below it, and all U chunks are loaded before the first store of the
+// iteration, so no unread slot is overwritten.  Results, slot order, codes
+// and counts are identical to k_move's.
+template <int U>
+__global__ void __launch_bounds__(512) k_move_u(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
+                                                int ncases, int items) {
+    const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    if (warp >= items) return;
+    const int ci = find_case(item_start, ncases, warp);
+    const DevCase &d = cases[ci];
+    const int w = warp - item_start[ci];
+    const int s = w / d.C, c = w - s * d.C;
+    const DevSpecies &sp = d.sp[s];
+    const int n = sp.cnt[c];
+    if (n == 0) {
+        if (lane == 0) sp.nmov[c] = 0;
+        if (lane < 9) sp.dcount[(size_t)c * 9 + lane] = 0;
+        return;
+    }
+    if (lane == 0) atomicAdd(&d.pushes[warp & 31], (unsigned long long)n);
+    const int cap = sp.cap;
+    if (2 * n > cap) { // the reference's ReArg condition (src/cuda_Sortboundary.cu:63-65)
+        if (lane == 0) {
+            sp.nmov[c] = 0;
+            atomicOr(d.status, ST_OVERFLOW);
+        }
+        if (lane < 9) sp.dcount[(size_t)c * 9 + lane] = 0;
+        return;
+    }
+    const int i = c / d.ncy, j = c - i * d.ncy;
+    const int node = i * d.ngy + j;
+    const float ex_ws = d.Ex[node], ex_wn = d.Ex[node + 1], ex_es = d.Ex[node + d.ngy], ex_en = d.Ex[node + d.ngy + 1];
+    const float ey_ws = d.Ey[node], ey_wn = d.Ey[node + 1], ey_es = d.Ey[node + d.ngy], ey_en = d.Ey[node + d.ngy + 1];
+    const float As = sp.Ascale, dtdx = d.dt_dx, dtdy = d.dt_dy;
+    const size_t base = (size_t)c * cap;
+    float *__restrict__ px = sp.x + base;
+    float *__restrict__ py = sp.y + base;
+    float *__restrict__ pvx = sp.vx + base;
+    float *__restrict__ pvy = sp.vy + base;
+    float *__restrict__ pvz = sp.vz + base;
+    const unsigned lt = lanemask_lt();
+    int m = 0;
+    unsigned long long pk0 = 0, pk1 = 0, pk2 = 0;
+    for (int k0 = 0; k0 < n; k0 += 32 * U) {
+        float lx[U], ly[U], mvx[U], mvy[U], vz[U];
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int k = k0 + 32 * u + lane;
+            lx[u] = ly[u] = mvx[u] = mvy[u] = vz[u] = 0.f;
+            if (k < n) {
+                lx[u] = px[k];
+                ly[u] = py[k];
+                mvx[u] = pvx[k];
+                mvy[u] = pvy[k];
+                vz[u] = pvz[k];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < U; u++) {
+            const int k = k0 + 32 * u + lane;
+            const bool act = k < n;
+            const float x0 = lx[u], y0 = ly[u];
+            const float del_vx = ex_ws * (1 - x0) * (1 - y0) + ex_wn * (1 - x0) * y0 + ex_es * x0 * (1 - y0) + ex_en * x0 * y0;
+            const float del_vy = ey_ws * (1 - x0) * (1 - y0) + ey_wn * (1 - x0) * y0 + ey_es * x0 * (1 - y0) + ey_en * x0 * y0;
+            float vX = mvx[u] + del_vx * As;
+            float vY = mvy[u] + del_vy * As;
+            float X = x0 + vX * dtdx;
+            float Y = y0 + vY * dtdy;
+            const bool out = act && (Y >= 1 || Y < 0 || X >= 1 || X < 0);
+            int code = 4, fi = i, fj = j;
+            if (out) {
+                int cond = -1;
+                const int r = walk(geo_of(d), fi, fj, X, Y, vX, vY, cond);
+                if (r) {
+                    code = CODE_ABSORBED;
+                    if (cond >= 0 && cond < d.cond_numr) atomicAdd(&d.cond_charge[s * d.cond_numr + cond], 1.0f);
+                    if (r == 2) atomicOr(d.status, ST_WALK);
+                } else {
+                    const int ddi = fi - i, ddj = fj - j;
+                    code = (ddi >= -1 && ddi <= 1 && ddj >= -1 && ddj <= 1) ? (ddi + 1) * 3 + (ddj + 1) : CODE_FAR;
+                }
+                if (code < 9) {
+                    const int q3 = code / 3;
+                    const unsigned long long one = 1ull << (21 * (code - 3 * q3));
+                    if (q3 == 0) pk0 += one;
+                    else if (q3 == 1) pk1 += one;
+                    else pk2 += one;
+                }
+            }
+            const unsigned bout = __ballot_sync(FULL, out);
+            const int before = m + __popc(bout & lt);
+            __syncwarp(); // every lane's loads of this iteration precede the in-place stores
+            if (act) {
+                const int dst = out ? cap - 1 - before : k - before;
+                px[dst] = X;
+                py[dst] = Y;
+                pvx[dst] = vX;
+                pvy[dst] = vY;
+                pvz[dst] = vz[u];
+                if (out) sp.code[base + dst] = (int8_t)code;
+                if (code == CODE_FAR) {
+                    const size_t b = (size_t)s * d.C + (size_t)(fi * d.ncy + fj);
+                    const int q = atomicAdd(&d.far_in[b], 1);
+                    if (q < FAR_B)
+                        d.far_key[b * FAR_B + q] = ((unsigned long long)c << 18) | (unsigned long long)before;
+                    else
+                        atomicOr(d.status, ST_OVERFLOW);
+                }
+            }
+            m += __popc(bout);
+        }
+    }
+    if (lane == 0) {
+        sp.cnt[c] = n - m;
+        sp.nmov[c] = m;
+    }
+    int mine = 0;
+#pragma unroll
+    for (int D = 0; D < 9; D++) {
+        const unsigned long long wv = D < 3 ? pk0 : D < 6 ? pk1 : pk2;
+        const unsigned tt = __reduce_add_sync(FULL, (unsigned)((wv >> (21 * (D % 3))) & 0x1FFFFFull));
+        if (lane == D) mine = (int)tt;
     }
     if (lane < 9) sp.dcount[(size_t)c * 9 + lane] = mine;
 }
@@ -515,18 +668,6 @@ __device__ __forceinline__ void newvel_ionsc_dev(float &vxs, float &vys, float &
 constexpr int MCC_TPB = 256;
 constexpr int MCC_RING = 256; // >= 128 new entries per pass + 31 pending
 
-// exclusive count of set bits of `mask4` (4 slots per lane) in lower lanes
-__device__ __forceinline__ int lower_lane_hits(unsigned mask4, unsigned lt, int &total) {
-    int pre = 0;
-    total = 0;
-#pragma unroll
-    for (int t = 0; t < 4; t++) {
-        const unsigned b = __ballot_sync(FULL, (mask4 >> t) & 1u);
-        pre += __popc(b & lt);
-        total += __popc(b);
-    }
-    return pre;
-}
 
 __device__ __forceinline__ void mcc_ion_collide(const DevCase &d, const DevSpecies &ion, size_t q, hp_stream &rs,
                                                 float bvel, unsigned *cnt_ch) {
@@ -1307,7 +1448,10 @@ cudaError_t launch_move(const DevCase *cases, const int *item_start, int ncases,
                         cudaStream_t st) {
     if (items <= 0) return cudaSuccess;
     const int tpb = 32 * std::min(std::max(lc.warps_per_block, 1), 16);
-    k_move<<<blocks_for((long long)items * 32, tpb), tpb, 0, st>>>(cases, item_start, ncases, items);
+    const unsigned nb = blocks_for((long long)items * 32, tpb);
+    if (lc.move_unroll == 2) k_move_u<2><<<nb, tpb, 0, st>>>(cases, item_start, ncases, items);
+    else if (lc.move_unroll == 4) k_move_u<4><<<nb, tpb, 0, st>>>(cases, item_start, ncases, items);
+    else k_move<<<nb, tpb, 0, st>>>(cases, item_start, ncases, items);
     return cudaGetLastError();
 }
 

@@ -13,6 +13,7 @@ struct LaunchCfg {
     int warps_per_block = 8;   // particle kernels: one warp per (species, cell)
     int pcg_block = 512;       // PCG: threads per CTA
     int pcg_cluster_max = 16;  // PCG: upper bound on CTAs per case
+    int move_unroll = 1;       // Move: chunks of 32 loaded per iteration (1: k_move, one-chunk prefetch)
 };
 
 // Move: gather + push + single-cell exit test (src/cuda_Move.cu:181-270)

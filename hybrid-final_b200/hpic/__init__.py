@@ -54,7 +54,11 @@ class CaseInfo(C.Structure):
 
 
 class Tune(C.Structure):
-    _fields_ = [("warps_per_block_particles", C.c_int), ("pcg_block", C.c_int), ("pcg_cluster_max", C.c_int)]
+    _fields_ = [("warps_per_block_particles", C.c_int), ("pcg_block", C.c_int), ("pcg_cluster_max", C.c_int),
+                ("move_unroll", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class ServerOpts(C.Structure):
@@ -96,6 +100,8 @@ _SIGS = {
     "hp_Deposit": (C.c_int, [_P, _P]),
     "hp_step": (C.c_int, [_P, C.c_int, _P]),
     "hp_step_kernels": (C.c_int, [_P, C.POINTER(C.c_int)]),
+    "hp_case_set_tune": (C.c_int, [_P, _P]),
+    "hp_case_get_tune": (C.c_int, [_P, _P]),
     "hp_batch_step_kernels": (C.c_int, [_P, C.POINTER(C.c_int)]),
     "hp_Deposit_noalloc": (C.c_int, [_P, _P, _P]),
     "hp_get_particles": (C.c_int, [_P, C.c_int, _I, _F, _F, _F, _F, _F, C.c_size_t, C.POINTER(C.c_size_t)]),
@@ -277,6 +283,17 @@ class Case:
         _check(lib().hp_last_field_residual(self.h, C.byref(r)))
         return r.value
 
+    def tune(self):
+        t = Tune()
+        _check(lib().hp_case_get_tune(self.h, C.byref(t)))
+        return t.as_dict()
+
+    def set_tune(self, **kw):
+        cur = self.tune()
+        cur.update(kw)
+        t = Tune(**cur)
+        _check(lib().hp_case_set_tune(self.h, C.byref(t)))
+
     def step_kernels(self):
         """Kernels one step launches (after the first step captured it)."""
         n = C.c_int(0)
@@ -378,11 +395,12 @@ class Batch:
     def tune(self):
         t = Tune()
         _check(lib().hp_batch_get_tune(self.h, C.byref(t)))
-        return dict(warps_per_block_particles=t.warps_per_block_particles, pcg_block=t.pcg_block,
-                    pcg_cluster_max=t.pcg_cluster_max)
+        return t.as_dict()
 
     def set_tune(self, **kw):
-        t = Tune(**kw)
+        cur = self.tune()
+        cur.update(kw)
+        t = Tune(**cur)
         _check(lib().hp_batch_set_tune(self.h, C.byref(t)))
 
     def autotune(self, stream=None):

@@ -247,9 +247,15 @@ typedef struct hp_tune {
     int warps_per_block_particles; /* Move/Sort/Deposit: warps per CTA (one warp per cell), 1..16 */
     int pcg_block;                 /* PCG: threads per CTA */
     int pcg_cluster_max;           /* PCG: largest cluster per case */
+    int move_unroll;               /* Move: chunks of 32 particles loaded per iteration: 1 (with a one-chunk
+                                      prefetch), 2 or 4 */
 } hp_tune;
 hp_status hp_batch_set_tune(hp_batch *b, const hp_tune *t);
 hp_status hp_batch_get_tune(hp_batch *b, hp_tune *t);
+/* The same launch shapes for a single case (hp_step re-captures its graph).
+ * No reference counterpart. */
+hp_status hp_case_set_tune(hp_case *c, const hp_tune *t);
+hp_status hp_case_get_tune(const hp_case *c, hp_tune *t);
 /* Time candidate launch shapes on the batch itself (state is saved and restored). */
 hp_status hp_batch_autotune(hp_batch *b, void *stream);
 

@@ -143,9 +143,12 @@ def test_steps_bit_exact(name, mode):
 
 
 @pytest.mark.parametrize("name", list(DECKS))
-def test_walk_steps_bit_exact(name):
-    """move_mode 1 (cell-by-cell walk) with the separable field solve."""
+@pytest.mark.parametrize("ppl", [1, 2, 4])
+def test_walk_steps_bit_exact(name, ppl):
+    """move_mode 1 (cell-by-cell walk) with the separable field solve; Move
+    with one or four particles per lane."""
     case, o = pair(name, field_mode=2, move_mode=1)
+    case.set_tune(move_unroll=ppl)
     n = 25
     case.step(n)
     o.run(0, n, accumulate=True)
@@ -172,10 +175,12 @@ def fast_electrons(case, o, cells_per_step, every=3):
 
 
 @pytest.mark.parametrize("cells", [2.6, 7.3])
-def test_far_movers_bit_exact(cells):
+@pytest.mark.parametrize("ppl", [1, 2, 4])
+def test_far_movers_bit_exact(cells, ppl):
     """Electrons crossing several cells per push: the walk, the reflections on
     the side walls, absorption at the electrodes and the far-mover order."""
     case, o = pair("ar_65x33", field_mode=2, move_mode=1)
+    case.set_tune(move_unroll=ppl)
     fast_electrons(case, o, cells)
     for t in (1, 2):
         case.set_tstep(t)
