@@ -607,7 +607,7 @@ hp_status hp_get_table(hp_case *c, int what, void *out, size_t bytes, size_t *ne
     return table_of(c->s, &c->prob, &c->fs, what, out, bytes, needed);
 }
 
-static hp_status case_from(const Setup &s, const hp_case_opts *opts, hp_case **out) {
+static hp_status case_from(Setup s, const hp_case_opts *opts, hp_case **out) {
     hp_case_opts o;
     hp_case_opts_default(&o);
     if (opts) o = *opts;
@@ -616,7 +616,7 @@ static hp_status case_from(const Setup &s, const hp_case_opts *opts, hp_case **o
     if (chk == -2) return set_error("device ordinal out of range"), HP_ERR_ARG;
     CK(cudaSetDevice(o.device));
     hp_case *c = new hp_case();
-    c->s = s;
+    c->s = std::move(s);
     c->opts = o;
     c->device = o.device;
     hp_status st = build_device(c);
@@ -652,7 +652,7 @@ hp_status hp_case_create(const char *deck, size_t len, const hp_case_opts *opts,
         return from_exception(e);
     }
     if (s.main_gas != GAS_AR) return set_error("MCC for this gas is not built"), HP_ERR_UNSUPPORTED;
-    return case_from(s, &o, out);
+    return case_from(std::move(s), &o, out);
 }
 
 hp_status hp_case_create_from_setup(const hp_setup *su, const hp_case_opts *opts, hp_case **out) {
@@ -661,6 +661,43 @@ hp_status hp_case_create_from_setup(const hp_setup *su, const hp_case_opts *opts
     if (opts) o = *opts;
     return case_from(su->s, &o, out);
 }
+} // extern "C"
+
+namespace hpi {
+hp_status case_from_setup_owned(hp::Setup &&s, const hp_case_opts &o, hp_case **out) {
+    if (s.main_gas != GAS_AR) return set_error("MCC for this gas is not built"), HP_ERR_UNSUPPORTED;
+    hp_status st = case_from(std::move(s), &o, out);
+    if (st != HP_OK) return st;
+    // the initial load now lives on the device
+    hp::Setup &h = (*out)->s;
+    for (int k = 0; k < hp::MAXSP; k++) {
+        std::vector<float>().swap(h.p_x[k]); std::vector<float>().swap(h.p_y[k]);
+        std::vector<float>().swap(h.p_vx[k]); std::vector<float>().swap(h.p_vy[k]);
+        std::vector<float>().swap(h.p_vz[k]);
+        std::vector<float>().swap(h.h_x[k]); std::vector<float>().swap(h.h_y[k]);
+        std::vector<float>().swap(h.h_vx[k]); std::vector<float>().swap(h.h_vy[k]);
+        std::vector<float>().swap(h.h_vz[k]); std::vector<int>().swap(h.h_cell[k]);
+    }
+    return HP_OK;
+}
+
+size_t estimate_device_bytes(const hp::Setup &s, const hp_case_opts &o) {
+
+    const size_t G = (size_t)s.Gsize, C = (size_t)s.Csize, nsp = (size_t)s.nsp;
+    size_t b = 0;
+    for (int k = 0; k < s.nsp; k++) {
+        const size_t cap = (size_t)s.cap[k]; // already sized by the cap_per_cell option
+        b += C * cap * 21 + C * (4 + 4 + 36 + 32);         // slots, counts, dcount, corner sums
+    }
+    b += nsp * C * (4 + 8 * HP_FAR_BUCKET) + 8 * C * 4;  // far buckets, channel counts
+    b += G * (16 * 4 + 8 * 8 + 16 * nsp) + C * 16 + (size_t)s.cond_numr * G * 4;
+    b += s.xsec.size() * 4 + s.vsave.size() * 4 + 3 * C * 4;
+    if (o.field_mode == 2) b += 2 * ((size_t)s.ngx * s.ngx + (size_t)s.ngy * s.ngy) * 4 + 5 * G * 4;
+    return b + b / 16 + (1u << 20); // allocation rounding and small arrays
+}
+} // namespace hpi
+
+extern "C" {
 
 hp_status hp_case_destroy(hp_case *c) {
     if (!c) return HP_OK;

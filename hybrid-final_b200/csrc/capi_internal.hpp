@@ -77,4 +77,8 @@ struct BatchDev {
 hp_status batch_dev_build(hp_case *const *cases, int n, BatchDev &b);
 void batch_dev_free(BatchDev &b);
 hp_status run_step(const BatchDev &b, const hp::LaunchCfg &lc, int gas, cudaStream_t st);
+// a case that takes over a set-up (its host particle load is released once uploaded)
+hp_status case_from_setup_owned(hp::Setup &&s, const hp_case_opts &o, hp_case **out);
+// an upper estimate of a case's device footprint before it is created
+size_t estimate_device_bytes(const hp::Setup &s, const hp_case_opts &o);
 } // namespace hpi

@@ -8,6 +8,7 @@ compiled library; there is no Python or CPU implementation of any operator
 here, and a missing library raises instead of falling back.
 """
 import ctypes as C
+import json
 import os
 
 import numpy as np
@@ -67,7 +68,7 @@ class ServerOpts(C.Structure):
 
 
 class Result(C.Structure):
-    _fields_ = [("request_id", C.c_int64), ("status", C.c_uint32), ("steps", C.c_int64),
+    _fields_ = [("request_id", C.c_int64), ("error", C.c_int), ("status", C.c_uint32), ("steps", C.c_int64),
                 ("particle_pushes", C.c_int64), ("t_submit", C.c_double), ("t_admit", C.c_double),
                 ("t_done", C.c_double), ("ngx", C.c_int), ("ngy", C.c_int), ("nsp", C.c_int)]
 
@@ -122,6 +123,7 @@ _SIGS = {
     "hp_batch_set_tune": (C.c_int, [_P, C.POINTER(Tune)]),
     "hp_batch_get_tune": (C.c_int, [_P, C.POINTER(Tune)]),
     "hp_batch_autotune": (C.c_int, [_P, _P]),
+    "hp_server_opts_default": (None, [C.POINTER(ServerOpts)]),
     "hp_server_create": (C.c_int, [C.POINTER(ServerOpts), C.POINTER(_P)]),
     "hp_server_destroy": (C.c_int, [_P]),
     "hp_server_submit": (C.c_int, [_P, C.c_char_p, C.c_size_t, C.c_int64, C.c_uint64, C.POINTER(C.c_int64)]),
@@ -409,6 +411,83 @@ class Batch:
     def close(self):
         if getattr(self, "h", None):
             lib().hp_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+
+class Server:
+    """The served form: a request loop over resident cases (continuous
+    batching).  `submit` queues a deck; `poll` runs one scheduling round
+    (admission by device footprint and free slots, a few batched steps,
+    retirement); `results` pops finished requests with their time-averaged
+    densities and potential."""
+
+    def __init__(self, mem_budget_bytes=None, max_slots=None, steps_per_launch=None, **case_opts):
+        o = ServerOpts()
+        lib().hp_server_opts_default(C.byref(o))
+        if mem_budget_bytes is not None:
+            o.mem_budget_bytes = int(mem_budget_bytes)
+        if max_slots is not None:
+            o.max_slots = int(max_slots)
+        if steps_per_launch is not None:
+            o.steps_per_launch = int(steps_per_launch)
+        for k, v in case_opts.items():
+            setattr(o.case_opts, k, v)
+        self.opts = o
+        h = _P()
+        _check(lib().hp_server_create(C.byref(o), C.byref(h)))
+        self.h = h
+        self.shapes = {}
+
+    def submit(self, deck, nsteps, seed=1):
+        text = deck_text(deck)
+        raw = text.encode()
+        rid = C.c_int64(0)
+        _check(lib().hp_server_submit(self.h, raw, len(raw), int(nsteps), int(seed), C.byref(rid)))
+        d = json.loads(text)
+        g = d["Geometry"]["SystemSpec"]
+        self.shapes[rid.value] = (int(g["NumGridx"]), int(g["NumGridy"]))
+        return rid.value
+
+    def poll(self, stream=None):
+        n = C.c_int(0)
+        _check(lib().hp_server_poll(self.h, stream, C.byref(n)))
+        return n.value
+
+    def results(self):
+        """Finished requests: list of (Result, ave_den[nsp, G], ave_phi[G])."""
+        out = []
+        while True:
+            r = Result()
+            got = C.c_int(0)
+            # buffers sized for the largest case submitted to this server
+            cap_g = max((a * b for a, b in self.shapes.values()), default=1)
+            den = np.zeros(5 * cap_g)
+            phi = np.zeros(cap_g)
+            _check(lib().hp_server_take_result(self.h, C.byref(r), den.ctypes.data_as(C.POINTER(C.c_double)),
+                                               den.size, phi.ctypes.data_as(C.POINTER(C.c_double)), phi.size,
+                                               C.byref(got)))
+            if not got.value:
+                return out
+            G = r.ngx * r.ngy
+            out.append((r, den[: r.nsp * G].reshape(r.nsp, G).copy() if r.nsp else den[:0],
+                        phi[:G].copy()))
+
+    def run(self, stream=None, max_rounds=10 ** 9):
+        """Poll until every submitted request has finished; returns results."""
+        res = []
+        for _ in range(max_rounds):
+            pending = self.poll(stream)
+            res += self.results()
+            if pending == 0:
+                break
+        return res + self.results()
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().hp_server_destroy(self.h)
             self.h = None
 
     def __del__(self):

@@ -48,6 +48,8 @@ typedef enum hp_status {
 #define HP_STATUS_NONFINITE 0x2u     /* NaN/Inf in the field solve (reference: src/cuda_main.cu:227) */
 #define HP_STATUS_PCG_NOCONV 0x4u    /* PCG hit its iteration cap */
 #define HP_STATUS_WAIT_TIMEOUT 0x8u  /* a bounded device-side wait gave up */
+#define HP_STATUS_WALK_BOUND 0x10u   /* move_mode 1: a particle crossed more cells than the domain spans
+                                        (non-finite velocity); it was absorbed */
 
 /* Text of the last error raised on the calling host thread. */
 const char *hp_last_error(void);
@@ -267,6 +269,8 @@ typedef struct hp_server_opts {
     int steps_per_launch;      /* steps between admission points */
     hp_case_opts case_opts;
 } hp_server_opts;
+/* Defaults: 150 GiB budget, 64 slots, 50 steps per round, hp_case_opts_default. */
+void hp_server_opts_default(hp_server_opts *o);
 hp_status hp_server_create(const hp_server_opts *o, hp_server **out);
 hp_status hp_server_destroy(hp_server *s);
 /* Queue a request: deck text and the number of steps to run.  Returns a
@@ -279,6 +283,7 @@ hp_status hp_server_submit(hp_server *s, const char *deck_json, size_t len, int6
 hp_status hp_server_poll(hp_server *s, void *stream, int *pending);
 typedef struct hp_result {
     int64_t request_id;
+    int error;                 /* HP_OK, or why the request was not run (bad deck, over the budget, ...) */
     uint32_t status;           /* device status word at retirement */
     int64_t steps;
     int64_t particle_pushes;   /* sum over steps of particles advanced */
