@@ -294,6 +294,160 @@ def run_reference(args):
                 e2e=dict(value=cb["value"], unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
 
 
+def _setups(specs, **opts):
+    """Host set-ups of many decks in parallel (the library releases the GIL)."""
+    import concurrent.futures as cf
+
+    import hpic
+    with cf.ThreadPoolExecutor(min(16, os.cpu_count() or 1)) as ex:
+        return list(ex.map(lambda sp: hpic.Setup(sp[0], seed=sp[1], **opts), specs))
+
+
+def _timed_steps(fn, steps, stream):
+    import torch
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    fn(steps, stream)
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b)
+
+
+def run_batched(args):
+    """Batched form: many independent Ar cases with uneven grids and particle
+    counts advanced by one graph-captured launch per phase, launch shapes set
+    by the autotuner; compared with the plain single-case path on the same
+    cases, one case at a time, both with the batched numerics (field_mode 2)
+    and with the reference's solver rule (field_mode 0, one cell crossing per
+    push)."""
+    import torch
+
+    import hpic
+    from hpic.workloads import batched_cases
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream().cuda_stream
+    specs = batched_cases(args.cases, seed=2024)
+    opts = dict(field_mode=2, gas_temp_mode=1, move_mode=1)
+    setups = _setups([(d, sd) for d, sd, _ in specs], **opts)
+
+    def plain(field_mode, move_mode):
+        pushes, ms = 0, 0.0
+        for S, (_, sd, _) in zip(setups, specs):
+            c = hpic.Case(setup=S, seed=sd, field_mode=field_mode, move_mode=move_mode, gas_temp_mode=1)
+            c.step(args.warmup, stream)
+            torch.cuda.synchronize()
+            p0 = c.pushes()
+            ms += _timed_steps(c.step, args.steps, stream)
+            pushes += c.pushes() - p0
+            c.close()
+        return pushes / (ms * 1e-3), ms
+
+    plain2, plain2_ms = plain(2, 1)
+    plain0, plain0_ms = plain(0, 0)
+    cases = [hpic.Case(setup=S, seed=sd, **opts) for S, (_, sd, _) in zip(setups, specs)]
+    batch = hpic.Batch(cases)
+    t0 = time.perf_counter()
+    batch.autotune(stream)
+    tune_s = time.perf_counter() - t0
+    batch.step(args.warmup, stream)
+    torch.cuda.synchronize()
+    p0 = sum(c.pushes() for c in cases)
+    clocks = ClockSampler(0)
+    clocks.start()
+    ms = _timed_steps(batch.step, args.steps, stream)
+    clk = clocks.stop()
+    pushes = sum(c.pushes() for c in cases) - p0
+    status = [c.status() for c in cases]
+    value = pushes / (ms * 1e-3)
+    res = dict(metric=METRIC, value=value, unit=UNIT, n_gpus=1, steps=args.steps, warmup=args.warmup,
+               ms_per_step=ms / args.steps, higher_is_better=True, scaling="weak", vs_baseline=None,
+               dtype="f32 particles / f64 charge and field refinement", data="synthetic", form="batched",
+               config=dict(workload=f"batched_ar_{args.cases}cases", cases=args.cases,
+                           grids="65x33/129x65/257x129", pressure_torr="10-200 mTorr log-uniform",
+                           rf_voltage="50-300 V", ppc="20-200", seeds="per case",
+                           particles=int(sum(sum(c.particles_count(s) for s in range(c.info.nsp)) for c in cases)),
+                           tune=batch.tune(), autotune_s=round(tune_s, 2)),
+               plain=dict(field_mode2_value=plain2, field_mode0_value=plain0,
+                          batched_over_plain_mode2=value / plain2, batched_over_plain_reference_rule=value / plain0,
+                          note="plain = each case alone through hp_step, one after another, same steps"),
+               gpu_launches=batch.step_kernels() * args.steps, clocks=clk,
+               device_status_nonzero=int(sum(1 for x in status if x)),
+               device_status_bits={f"0x{b:x}": int(sum(1 for x in status if x & b)) for b in (1, 2, 4, 8, 16)},
+               device_status_cases=[dict(specs[k][2], status=int(status[k])) for k in range(len(cases)) if status[k]])
+    batch.close()
+    for c in cases:
+        c.close()
+    return res
+
+
+def run_served(args):
+    """Served form: a Poisson stream of requests (Ar CCPs of every grid size,
+    1-10 RF periods each, scaled by --steps-scale) through the request loop,
+    against the same stream served one case at a time on the plain path."""
+    import torch
+
+    import hpic
+    from hpic.workloads import served_stream
+    torch.cuda.set_device(0)
+    stream = torch.cuda.current_stream().cuda_stream
+    steps_per_cycle = max(1, int(round(400 * args.steps_scale)))
+    reqs = served_stream(args.requests, rate_per_s=args.rate, seed=7, steps_per_cycle=steps_per_cycle)
+    opts = dict(field_mode=2, gas_temp_mode=1, move_mode=1)
+
+    def pct(v, q):
+        return float(np.percentile(np.asarray(v), q)) if v else None
+
+    # the request loop
+    srv = hpic.Server(max_slots=args.slots, steps_per_launch=args.steps_per_launch,
+                      mem_budget_bytes=int(args.budget_gb * (1 << 30)), **opts)
+    t_start = time.perf_counter()
+    arrival_clock = {}
+    k, results = 0, []
+    while k < len(reqs) or len(results) < len(reqs):
+        now = time.perf_counter() - t_start
+        while k < len(reqs) and reqs[k][0] <= now:
+            _, deck, nsteps, seed, _ = reqs[k]
+            arrival_clock[srv.submit(deck, nsteps, seed)] = reqs[k][0]
+            k += 1
+        pending = srv.poll(stream)
+        results += srv.results()
+        if pending == 0 and k < len(reqs):
+            time.sleep(max(0.0, min(0.05, reqs[k][0] - (time.perf_counter() - t_start))))
+    t_end = time.perf_counter() - t_start
+    srv.close()
+    lat = [r.t_done - r.t_submit for r, _, _ in results if r.error == 0]
+    pushes = sum(r.particle_pushes for r, _, _ in results)
+    errors = sum(1 for r, _, _ in results if r.error)
+    # the same stream, one case at a time on the plain path (set-up included)
+    t_start = time.perf_counter()
+    plain_lat, plain_pushes = [], 0
+    for t_arr, deck, nsteps, seed, _ in reqs:
+        now = time.perf_counter() - t_start
+        if now < t_arr:
+            time.sleep(t_arr - now)
+        c = hpic.Case(deck, seed=seed, **opts)
+        c.step(nsteps, stream)
+        n = c.average_count()
+        _ = c.grid("AVE_DEN") / n, c.grid("AVE_PHI") / n
+        plain_pushes += c.pushes()
+        c.close()
+        plain_lat.append(time.perf_counter() - t_start - t_arr)
+    plain_end = time.perf_counter() - t_start
+    value = pushes / t_end
+    return dict(metric=METRIC, value=value, unit=UNIT, n_gpus=1, steps=None, warmup=0, higher_is_better=True,
+                scaling="weak", vs_baseline=None, dtype="f32 particles / f64 charge and field refinement",
+                data="synthetic", form="served",
+                config=dict(workload=f"served_ar_{args.requests}req", requests=args.requests,
+                            arrivals=f"Poisson {args.rate}/s", grids="65x33/129x65/257x129/513x257",
+                            ppc="50-200", rf_periods="1-10", steps_per_rf_period=steps_per_cycle,
+                            slots=args.slots, steps_per_launch=args.steps_per_launch, budget_gb=args.budget_gb,
+                            gas="Ar (the Ar/O2 reaction set is not built)"),
+                latency_s=dict(p50=pct(lat, 50), p99=pct(lat, 99)), errors=errors, wall_s=t_end,
+                plain=dict(value=plain_pushes / plain_end, latency_s=dict(p50=pct(plain_lat, 50),
+                                                                          p99=pct(plain_lat, 99)),
+                           wall_s=plain_end, served_over_plain=value / (plain_pushes / plain_end)))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -304,9 +458,24 @@ def main():
     ap.add_argument("--field-mode", type=int, default=2)
     ap.add_argument("--move-mode", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--form", default="single", choices=["single", "batched", "served"],
+                    help="single: the large case (default); batched: --cases mixed cases in one batch; "
+                         "served: a request stream through hp_server")
+    ap.add_argument("--cases", type=int, default=64)
+    ap.add_argument("--requests", type=int, default=64)
+    ap.add_argument("--rate", type=float, default=4.0)
+    ap.add_argument("--steps-scale", type=float, default=0.1, help="served: steps per RF period / 400")
+    ap.add_argument("--slots", type=int, default=64)
+    ap.add_argument("--steps-per-launch", type=int, default=40)
+    ap.add_argument("--budget-gb", type=float, default=150.0)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))
+    if args.form != "single" and args.impl == "ours":
+        if rank == 0:
+            res = run_batched(args) if args.form == "batched" else run_served(args)
+            print(json.dumps(res), flush=True)
+        return
     if args.impl == "reference":
         if rank == 0:
             print(json.dumps(run_reference(args)), flush=True)

@@ -11,8 +11,8 @@
 //
 // The host-side set-up of a request (deck parsing, the BiCGSTAB solves for
 // the Laplace bases and the gas temperature, the particle load) is the slow
-// part of admission, so a worker thread builds set-ups ahead, in submission
-// order, while the device runs the current mix.
+// part of admission, so worker threads build set-ups ahead, claiming requests
+// in submission order, while the device runs the current mix.
 //
 // A case's steps depend only on its own state (per-case Philox keys and
 // step counter, per-case reduction trees), so a result is the same bit for
@@ -74,9 +74,9 @@ struct hp_server {
     std::mutex mu;
     std::condition_variable cv_work, cv_built;
     std::deque<std::unique_ptr<Request>> queue; // submitted, in order (built or not)
-    size_t next_build = 0;                      // queue index the worker builds next
+    size_t next_build = 0;                      // queue index the next idle worker claims
     bool stop = false;
-    std::thread worker;
+    std::vector<std::thread> workers;
     int64_t next_id = 1;
     // owned by the polling thread
     std::vector<Resident> resident;
@@ -95,7 +95,8 @@ void worker_main(hp_server *s) {
             std::unique_lock<std::mutex> lk(s->mu);
             s->cv_work.wait(lk, [&] { return s->stop || s->next_build < s->queue.size(); });
             if (s->stop) return;
-            r = s->queue[s->next_build].get();
+            r = s->queue[s->next_build].get(); // claim the oldest request nobody builds yet
+            s->next_build++;
         }
         // build outside the lock: the queue only grows at the back, and the
         // poller removes a request only after it is marked built
@@ -125,7 +126,6 @@ void worker_main(hp_server *s) {
             r->est_bytes = est;
             r->built = true;
             std::string().swap(r->deck);
-            s->next_build++;
         }
         s->cv_built.notify_all();
     }
@@ -275,7 +275,10 @@ hp_status hp_server_create(const hp_server_opts *o, hp_server **out) {
         return hpi::set_error("no CUDA device: libhpic has no CPU path"), HP_ERR_NO_CUDA;
     hp_server *s = new hp_server();
     s->o = *o;
-    s->worker = std::thread(worker_main, s);
+    // set-ups of several requests at once (each is partly threaded itself)
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const int nw = (int)std::min(4u, std::max(1u, hw / 4));
+    for (int k = 0; k < nw; k++) s->workers.emplace_back(worker_main, s);
     *out = s;
     return HP_OK;
 }
@@ -287,7 +290,7 @@ hp_status hp_server_destroy(hp_server *s) {
         s->stop = true;
     }
     s->cv_work.notify_all();
-    s->worker.join();
+    for (auto &w : s->workers) w.join();
     destroy_batches(s);
     for (Resident &r : s->resident) hp_case_destroy(r.c);
     delete s;

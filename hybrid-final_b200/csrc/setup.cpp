@@ -17,6 +17,7 @@
 #include <fstream>
 #include <sstream>
 #include <stdexcept>
+#include <thread>
 
 #include <dlfcn.h>
 
@@ -54,6 +55,33 @@ struct ParkMiller {
         return (float)(seed / 2147483646.0);
     }
 };
+
+// The generator's state k draws ahead: seed * 16807^k mod (2^31 - 1), by
+// square-and-multiply.  Each loaded particle takes exactly five draws, so the
+// load splits over threads with every thread starting at its own offset and
+// the result identical to the sequential loop.
+long pm_skip(long seed, unsigned long long k) {
+    const unsigned long long m = 2147483647ull;
+    unsigned long long a = 16807, r = 1;
+    while (k) {
+        if (k & 1) r = r * a % m;
+        a = a * a % m;
+        k >>= 1;
+    }
+    return (long)(r * (unsigned long long)seed % m);
+}
+
+template <class F> void par_range(long long n, F f) {
+    const unsigned hw = std::thread::hardware_concurrency();
+    const int T = (int)std::max<long long>(1, std::min<long long>(hw ? hw : 1, n / 65536));
+    if (T <= 1) {
+        f(0LL, n);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int t = 0; t < T; t++) th.emplace_back([&, t] { f(n * t / T, n * (t + 1) / T); });
+    for (auto &x : th) x.join();
+}
 
 // F(v) = -2 v e^{-v^2}/sqrt(pi) + erf(v): the Maxwellian speed CDF
 // (src/Particle.c:227-230), float argument, double evaluation.
@@ -719,22 +747,33 @@ std::vector<double> setup_solve(const Setup &s, const std::vector<float> &vals, 
 void laplace_and_gas(Setup &s, int gas_temp_mode) {
     const int N = s.n_unknowns, G = s.Gsize;
     // Laplace basis: conductor k at 1 V, the others at 0 V (src/cuda_Field.cu:192-219)
+    // the cond_numr + 1 independent solves run on their own threads
     s.lap_basis.assign((size_t)s.cond_numr * G, 0.0f);
-    for (int k = 0; k < s.cond_numr; k++) {
+    std::vector<std::vector<double>> xs((size_t)s.cond_numr + 1);
+    std::vector<std::thread> th;
+    for (int k = 0; k < s.cond_numr; k++)
+        th.emplace_back([&, k] {
+            std::vector<double> b(N);
+            for (int i = 0; i < N; i++) b[i] = s.cond_b[(size_t)k * N + i];
+            xs[(size_t)k] = setup_solve(s, s.a_val, b);
+        });
+    // gas temperature: TA x = temp_b (src/cuda_Field.cu:221-233)
+    th.emplace_back([&] {
         std::vector<double> b(N);
-        for (int i = 0; i < N; i++) b[i] = s.cond_b[(size_t)k * N + i];
-        std::vector<double> x = setup_solve(s, s.a_val, b);
+        for (int i = 0; i < N; i++) b[i] = s.temp_b[i];
+        xs[(size_t)s.cond_numr] = setup_solve(s, gas_temp_mode == 1 ? s.a_val : s.ta_val, b);
+    });
+    for (auto &t : th) t.join();
+    for (int k = 0; k < s.cond_numr; k++) {
+        const std::vector<double> &x = xs[(size_t)k];
         float *phi = &s.lap_basis[(size_t)k * G];
         for (int g = 0; g < G; g++) {
             if (s.a_idx[g]) phi[g] = (float)x[(size_t)s.a_idx[g] - 1];
             else if (s.cond_id[g] == k + 1) phi[g] = 1.0f;
         }
     }
-    // gas temperature: TA x = temp_b (src/cuda_Field.cu:221-233)
     {
-        std::vector<double> b(N);
-        for (int i = 0; i < N; i++) b[i] = s.temp_b[i];
-        std::vector<double> x = setup_solve(s, gas_temp_mode == 1 ? s.a_val : s.ta_val, b);
+        const std::vector<double> &x = xs[(size_t)s.cond_numr];
         s.node_temp = s.temp;
         for (int g = 0; g < G; g++)
             if (s.a_idx[g]) s.node_temp[g] = (float)x[(size_t)s.a_idx[g] - 1];
@@ -794,19 +833,31 @@ void gas_setting(Setup &s, const BuildOpts &o) { // src/start.c:1999-2051
         float x0 = l.x_center / s.dx, x1 = l.x_fall / s.dx - 1;
         auto &hx = s.h_x[isp], &hy = s.h_y[isp], &hvx = s.h_vx[isp], &hvy = s.h_vy[isp], &hvz = s.h_vz[isp];
         auto &hc = s.h_cell[isp];
+        // loading cells in the reference's order (i outer, j inner) and the
+        // first particle of each
+        std::vector<int> lc;
         for (int i = 0; i < s.ncx; i++)
             for (int j = 0; j < s.ncy; j++) {
                 if (s.plasma_region[(size_t)i * s.ncy + j] != 1) continue;
-                int Num = (i >= x0 && i <= x1 && j >= y0 && j <= y1) ? n_per_cell : 0;
-                for (int n = 0; n < Num; n++) {
-                    float vx, vy, vz;
-                    maxwellv(s, pm, p.vti, vx, vy, vz);
-                    float x = (float)i + pm.next();
-                    float y = (float)j + pm.next();
-                    hx.push_back(x); hy.push_back(y); hvx.push_back(vx); hvy.push_back(vy); hvz.push_back(vz);
-                    hc.push_back(i * s.ngy + j);
-                }
+                if (n_per_cell > 0 && i >= x0 && i <= x1 && j >= y0 && j <= y1) lc.push_back(i * s.ncy + j);
             }
+        const long long np = (long long)lc.size() * std::max(n_per_cell, 0);
+        hx.resize(np); hy.resize(np); hvx.resize(np); hvy.resize(np); hvz.resize(np); hc.resize(np);
+        const long seed0 = pm.seed;
+        par_range(np, [&](long long k0, long long k1) {
+            ParkMiller q{pm_skip(seed0, 5ull * (unsigned long long)k0)};
+            for (long long k = k0; k < k1; k++) {
+                const int c = lc[(size_t)(k / n_per_cell)];
+                const int i = c / s.ncy, j = c - i * s.ncy;
+                float vx, vy, vz;
+                maxwellv(s, q, p.vti, vx, vy, vz);
+                hx[k] = (float)i + q.next();
+                hy[k] = (float)j + q.next();
+                hvx[k] = vx; hvy[k] = vy; hvz[k] = vz;
+                hc[k] = i * s.ngy + j;
+            }
+        });
+        pm.seed = pm_skip(seed0, 5ull * (unsigned long long)np);
         p.np = (int)hx.size();
         // Copy_HCPtoGCP (src/cuda_Particle.cu:28-58): cell from the integer part
         std::vector<int> &cnt = s.p_count[isp];
@@ -818,26 +869,67 @@ void gas_setting(Setup &s, const BuildOpts &o) { // src/start.c:1999-2051
         // past the grid).  Such a particle stays in the last cell here, with
         // its offset just below 1.
         std::vector<float> offx(p.np), offy(p.np);
-        for (int k = 0; k < p.np; k++) {
-            int XID = (int)hx[k], YID = (int)hy[k];
-            float ox = hx[k] - XID, oy = hy[k] - YID;
-            if (XID >= s.ncx) { XID = s.ncx - 1; ox = 0.99999994f; }
-            if (YID >= s.ncy) { YID = s.ncy - 1; oy = 0.99999994f; }
-            offx[k] = ox;
-            offy[k] = oy;
-            cell_of[k] = XID * s.ncy + YID;
-            cnt[cell_of[k]]++;
+        // stable counting sort by cell, in fixed chunks: per-chunk counts,
+        // then each chunk scatters after the chunks before it
+        const int NCH = 64;
+        const long long npl = p.np;
+        std::vector<int> ccount((size_t)NCH * s.Csize, 0);
+        auto chunk_lo = [&](int t) { return npl * t / NCH; };
+        {
+            std::vector<std::thread> th;
+            const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+            for (unsigned w = 0; w < hw; w++)
+                th.emplace_back([&, w] {
+                    for (int t = (int)w; t < NCH; t += (int)hw) {
+                        int *cc = &ccount[(size_t)t * s.Csize];
+                        for (long long k = chunk_lo(t); k < chunk_lo(t + 1); k++) {
+                            int XID = (int)hx[k], YID = (int)hy[k];
+                            float ox = hx[k] - XID, oy = hy[k] - YID;
+                            if (XID >= s.ncx) { XID = s.ncx - 1; ox = 0.99999994f; }
+                            if (YID >= s.ncy) { YID = s.ncy - 1; oy = 0.99999994f; }
+                            offx[k] = ox;
+                            offy[k] = oy;
+                            cell_of[k] = XID * s.ncy + YID;
+                            cc[cell_of[k]]++;
+                        }
+                    }
+                });
+            for (auto &x : th) x.join();
         }
+        // fill[t][c]: where chunk t's first particle of cell c goes
         std::vector<int> start(s.Csize + 1, 0);
-        for (int c = 0; c < s.Csize; c++) start[c + 1] = start[c] + cnt[c];
-        std::vector<int> fill(start.begin(), start.end() - 1);
+        for (int c = 0; c < s.Csize; c++) {
+            int tot = 0;
+            for (int t = 0; t < NCH; t++) tot += ccount[(size_t)t * s.Csize + c];
+            cnt[c] = tot;
+            start[c + 1] = start[c] + tot;
+        }
+        std::vector<int> fill((size_t)NCH * s.Csize);
+        for (int c = 0; c < s.Csize; c++) {
+            int at = start[c];
+            for (int t = 0; t < NCH; t++) {
+                fill[(size_t)t * s.Csize + c] = at;
+                at += ccount[(size_t)t * s.Csize + c];
+            }
+        }
         s.p_x[isp].assign(p.np, 0); s.p_y[isp].assign(p.np, 0);
         s.p_vx[isp].assign(p.np, 0); s.p_vy[isp].assign(p.np, 0); s.p_vz[isp].assign(p.np, 0);
-        for (int k = 0; k < p.np; k++) {
-            int d = fill[cell_of[k]]++;
-            s.p_x[isp][d] = offx[k];
-            s.p_y[isp][d] = offy[k];
-            s.p_vx[isp][d] = hvx[k]; s.p_vy[isp][d] = hvy[k]; s.p_vz[isp][d] = hvz[k];
+        {
+            std::vector<std::thread> th;
+            const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+            for (unsigned w = 0; w < hw; w++)
+                th.emplace_back([&, w] {
+                    for (int t = (int)w; t < NCH; t += (int)hw) {
+                        int *fl = &fill[(size_t)t * s.Csize];
+                        for (long long k = chunk_lo(t); k < chunk_lo(t + 1); k++) {
+                            const int d = fl[cell_of[k]]++;
+                            s.p_x[isp][d] = offx[k];
+                            s.p_y[isp][d] = offy[k];
+                            s.p_vx[isp][d] = hvx[k]; s.p_vy[isp][d] = hvy[k]; s.p_vz[isp][d] = hvz[k];
+                        }
+                    }
+                });
+            for (auto &x : th) x.join();
         }
     }
 }
