@@ -165,6 +165,40 @@ def cpu_baseline(setup, case_opts, budget_s=20.0):
                        f"CPU restatement in FP32, {t_used:.1f} s")
 
 
+def fp64_check(stream, steps=400):
+    """Error of the precision form against the FP64 oracle on the reference's
+    CPU-sized Ar case (129x65 nodes, 4 cm x 2 cm, 50 particles per cell and
+    species, 100 V, 50 mTorr) over one RF period: relative L2 error of the
+    time-averaged n_e, n_i and potential.  The GPU runs the bench's numerics
+    (FP32 particles, FP64 charge grid, field_mode 2); the oracle runs the same
+    case and draws in FP64 on the host."""
+    import hpic
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import oracle
+    w = WORKLOADS["ar_129x65_50ppc"]
+    opts = dict(field_mode=2, gas_temp_mode=1, move_mode=1)
+    S = hpic.Setup(make_deck(w), seed=77, **opts)
+    c = hpic.Case(setup=S, seed=77, **opts)
+    c.step(steps, stream)
+    n = c.average_count()
+    d32 = c.grid("AVE_DEN").reshape(c.info.nsp, -1) / n
+    p32 = c.grid("AVE_PHI") / n
+    c.close()
+    t0 = time.perf_counter()
+    o = oracle.from_setup(S, 64, field_mode=2)
+    o.c.move_mode = 1
+    o.Deposit()
+    o.run(0, steps, accumulate=True)
+    d, p, m = o.averages()
+    d64, p64 = d.reshape(S.info.nsp, -1) / m, p / m
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    return dict(case="ar_129x65_50ppc", steps=steps, rf_periods=steps / 400, tolerance=0.01,
+                rel_l2_ave_n_e=rel(d32[0], d64[0]), rel_l2_ave_n_i=rel(d32[1], d64[1]), rel_l2_ave_phi=rel(p32, p64),
+                fp64_oracle_s=round(time.perf_counter() - t0, 1))
+
+
 def run_ours(args, rank, world, local, dist):
     import torch
 
@@ -273,6 +307,9 @@ def run_ours(args, rank, world, local, dist):
     )
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(setup, case.opts)
+    if rank == 0 and world == 1 and not args.no_fp64_check:
+        case.close()
+        result["fp64_check"] = fp64_check(stream)
     return result
 
 
@@ -458,6 +495,7 @@ def main():
     ap.add_argument("--field-mode", type=int, default=2)
     ap.add_argument("--move-mode", type=int, default=1)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-check", action="store_true")
     ap.add_argument("--form", default="single", choices=["single", "batched", "served"],
                     help="single: the large case (default); batched: --cases mixed cases in one batch; "
                          "served: a request stream through hp_server")

@@ -241,7 +241,10 @@ class Case:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: the library may be gone already
+            pass
 
     # per-step operators (reference names)
     def Field(self, stream=None):
@@ -414,7 +417,10 @@ class Batch:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: the library may be gone already
+            pass
 
 
 class Server:
@@ -491,4 +497,7 @@ class Server:
             self.h = None
 
     def __del__(self):
-        self.close()
+        try:
+            self.close()
+        except Exception:  # interpreter shutdown: the library may be gone already
+            pass
