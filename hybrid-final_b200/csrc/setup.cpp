@@ -395,7 +395,38 @@ void read_collisions(const JVal &root, Setup &s) { // src/start.c:1003-1057
         float mofm[10] = {me / mb, me / mb, me / mb, me / mb, me / mf, mb / mi, mb / mi, me / mf, mf / mb, mb / mf};
         for (int i = 0; i < 10; i++) s.collf[(size_t)i].mofM = mofm[i];
     } else {
-        unsupported(s.main_gas == GAS_O2 ? "O2 reaction set" : "Ar/O2 reaction set");
+        // the O2 (67 channels) and Ar/O2 (88) sets: deck keys and mofM mass
+        // pairs as the reference's reader lists them (src/start.c, the
+        // "OxygenCase" / "Argon/OxygenCase" blocks), from data/channels_*.txt
+        const bool aro2 = s.main_gas == GAS_ARO2;
+        std::ifstream in(data_path(aro2 ? "channels_aro2.txt" : "channels_o2.txt"));
+        if (!in) throw std::runtime_error("cannot open the reaction channel list");
+        const JVal &a = co.object(aro2 ? "Argon/OxygenCase" : "OxygenCase");
+        s.TnRct = aro2 ? 88 : 67;
+        s.collf.assign((size_t)s.TnRct, CollFP());
+        auto mass = [&](const std::string &m) -> float {
+            if (m == "-") return 0.0f;
+            const int k = std::atoi(m.c_str() + 2);
+            if (m.compare(0, 2, "SP") == 0) return s.sp[k].mass;
+            if (m.compare(0, 2, "BG") == 0) return s.bg[k].mass;
+            return s.fg[k].mass;
+        };
+        std::string line;
+        int nread = 0;
+        while (std::getline(in, line)) {
+            if (line.empty() || line[0] == '#') continue;
+            std::istringstream ls(line);
+            int k;
+            std::string key, num, den;
+            std::getline(ls >> k >> std::ws, key, '\t');
+            ls >> num >> den;
+            if (k < 0 || k >= s.TnRct) throw std::runtime_error("bad reaction channel list");
+            s.collf[(size_t)k].Flag = fnum(a, key.c_str());
+            const float md = mass(den);
+            s.collf[(size_t)k].mofM = md != 0.0f ? mass(num) / md : 0.0f;
+            nread++;
+        }
+        if (nread != s.TnRct) throw std::runtime_error("bad reaction channel list");
     }
     for (auto &c : s.collf)
         if (c.Flag < 0) c.Flag = 0.0f;
@@ -934,9 +965,85 @@ void gas_setting(Setup &s, const BuildOpts &o) { // src/start.c:1999-2051
     }
 }
 
+// sigma-v maximum of one (projectile, target) pair over the table: the sum
+// of the listed channels, summed in the reference's groups
+// (src/cuda_mcc.cu:277-466), times the projectile speed at each grid energy
+struct SigGroup {
+    int proj;                 // projectile species
+    std::vector<std::vector<int>> parts; // channel groups, summed separately then added
+};
+
+float sigv_max(const Setup &s, const SigGroup &g) {
+    const int W = 2 + s.n_cx;
+    double best = 0.0;
+    for (int i = 0; i < s.n_logx; i++) {
+        const float *row = &s.xsec[(size_t)i * W];
+        float engy = row[1];
+        float sig = 0.0f;
+        for (size_t p = 0; p < g.parts.size(); p++) {
+            float part = 0.0f;
+            for (size_t q = 0; q < g.parts[p].size(); q++) part = q ? part + row[2 + g.parts[p][q]] : row[2 + g.parts[p][q]];
+            sig = p ? sig + part : part;
+        }
+        best = std::max(best, sqrt(2 * 1.602e-19 * engy / s.sp[g.proj].mass) * sig);
+        best = (float)best;
+    }
+    return (float)best;
+}
+
+std::vector<int> span(int a, int b) {
+    std::vector<int> v;
+    for (int k = a; k <= b; k++) v.push_back(k);
+    return v;
+}
+
+void null_collision_oxygen(Setup &s) { // src/cuda_mcc.cu:277-466
+    const float prob_cut = 0.08f;
+    const bool aro2 = s.main_gas == GAS_ARO2;
+    std::vector<SigGroup> g;
+    // electron targets: (sigv index, target density) for the sub-cycle count
+    std::vector<float> edens;
+    if (aro2) {
+        g = {{0, {span(0, 3)}}, {0, {{4}}}, {0, {span(5, 9), span(10, 14), span(15, 18)}},
+             {0, {span(19, 23), span(24, 26)}}, {0, {span(27, 31), span(32, 34)}}, {0, {{35}}}, {0, {{36}}},
+             {0, {span(37, 41), span(42, 43)}}, {0, {span(44, 45)}}, {4, {span(46, 47)}}, {4, {{48}}},
+             {4, {{49}}}, {4, {{50}}}, {4, {{51}}}, {2, {{52}}}, {2, {span(53, 55)}}, {2, {{56}}}, {2, {{57}}},
+             {2, {span(58, 59)}}, {3, {span(60, 61)}}, {3, {{62}}}, {3, {{63}}}, {3, {{64}}}, {1, {span(65, 66)}},
+             {1, {{67}}}};
+        edens = {s.bg[0].InitDens, s.fg[0].InitDens, s.bg[1].InitDens, s.fg[1].InitDens, s.fg[2].InitDens,
+                 s.sp[4].InitDens, s.sp[2].InitDens, s.fg[3].InitDens, s.fg[4].InitDens};
+    } else {
+        g = {{0, {span(0, 4), span(5, 9), span(10, 13)}}, {0, {span(14, 18), span(19, 21)}},
+             {0, {span(22, 26), span(27, 29)}}, {0, {{30}}}, {0, {{31}}}, {0, {span(32, 36), span(37, 38)}},
+             {0, {span(39, 40)}}, {3, {span(41, 42)}}, {3, {{43}}}, {3, {{44}}}, {3, {{45}}}, {3, {{46}}},
+             {1, {{47}}}, {1, {span(48, 50)}}, {1, {{51}}}, {1, {{52}}}, {2, {span(53, 54)}}, {2, {{55}}},
+             {2, {{56}}}, {2, {{57}}}};
+        edens = {s.bg[0].InitDens, s.fg[0].InitDens, s.fg[1].InitDens, s.sp[3].InitDens, s.sp[1].InitDens,
+                 s.fg[2].InitDens, s.fg[3].InitDens};
+    }
+    s.sigv.assign(g.size(), 0.0f);
+    for (size_t k = 0; k < g.size(); k++) s.sigv[k] = sigv_max(s, g[k]);
+    float col0 = 0.0f;
+    for (size_t k = 0; k < edens.size(); k++) {
+        const float t = (float)(1.0 - exp((double)(-1 * s.dt * s.sigv[k] * edens[k])));
+        col0 = k ? col0 + t : t;
+    }
+    if (col0 > prob_cut) {
+        s.mcc_n = (int)ceil((double)(col0 / prob_cut));
+        float ratio = 1 / (float)s.mcc_n;
+        s.dt_mcc = s.dt * ratio;
+    } else {
+        s.mcc_n = 1;
+        s.dt_mcc = s.dt;
+    }
+}
+
 void null_collision(Setup &s) { // src/cuda_mcc.cu:202-276 (Ar)
     const float prob_cut = 0.08f;
-    if (s.main_gas != GAS_AR) return;
+    if (s.main_gas != GAS_AR) {
+        null_collision_oxygen(s);
+        return;
+    }
     s.sigv.assign(3, 0.0f);
     const int W = 2 + s.n_cx;
     for (int i = 0; i < s.n_logx; i++) {

@@ -30,6 +30,19 @@ def _channels(names):
     return {n: 1.0 for n in names}
 
 
+def _channel_keys(gas):
+    """Deck keys of the O2 or Ar/O2 reaction set (the library's channel list)."""
+    import os
+    path = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "data",
+                        "channels_o2.txt" if gas == "O2" else "channels_aro2.txt")
+    keys = []
+    for line in open(path):
+        if line.startswith("#") or not line.strip():
+            continue
+        keys.append(line.rstrip("\n").split("\t")[1])
+    return keys
+
+
 def ccp_deck(ngx, ngy, xlen, ylen, *, gas="Ar", pressure_torr=0.05, voltage=100.0,
              freq=13.56e6, steps_per_cycle=400, ppc=50, density=1e15, te_ev=2.0,
              ti_ev=0.026, gas_k=300.0, max_np_factor=4, aro2_ratio=(80, 20),
@@ -77,9 +90,10 @@ def ccp_deck(ngx, ngy, xlen, ylen, *, gas="Ar", pressure_torr=0.05, voltage=100.
               "Electron": sp(0, density, te_ev), "Ar+": sp(1, ion.get("Ar+", density) if isinstance(ion, dict) else ion, ti_ev)}
     if gas in ("O2", "ArO2"):
         dens = ion if isinstance(ion, dict) else {}
-        charge["O2+"] = sp(2, dens.get("O2+", 0.0), ti_ev)
-        charge["O+"] = sp(3, dens.get("O+", 0.0), ti_ev)
-        charge["O-"] = sp(4, dens.get("O-", 0.0), ti_ev)
+        base = 2 if gas == "ArO2" else 1  # species order: e, (Ar+), O2+, O+, O-
+        charge["O2+"] = sp(base, dens.get("O2+", 0.0), ti_ev)
+        charge["O+"] = sp(base + 1, dens.get("O+", 0.0), ti_ev)
+        charge["O-"] = sp(base + 2, dens.get("O-", 0.0), ti_ev)
     deck = {
         "GPU_Device_Number": {"GPUDevice": 0},
         "Geometry": {
@@ -120,8 +134,8 @@ def ccp_deck(ngx, ngy, xlen, ylen, *, gas="Ar", pressure_torr=0.05, voltage=100.
         },
         "Collision_On_Off": {
             "ArgonCase": _channels(ARGON_CASE),
-            "OxygenCase": {},
-            "Argon/OxygenCase": {},
+            "OxygenCase": _channels(_channel_keys("O2")) if gas == "O2" else {},
+            "Argon/OxygenCase": _channels(_channel_keys("ArO2")) if gas == "ArO2" else {},
         },
     }
     return deck

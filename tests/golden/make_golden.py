@@ -31,6 +31,10 @@ DECKS = {
     "ar_17x9": (ccp_deck(17, 9, 0.005, 0.0025, ppc=10), 12345),
     "ar_33x17": (ccp_deck(33, 17, 0.01, 0.005, ppc=20, pressure_torr=0.1, voltage=200.0), 777),
     "ar_block_33x21": (block_deck(), 4242),
+    "aro2_33x17": (ccp_deck(33, 17, 0.01, 0.005, gas="ArO2", ppc=12, pressure_torr=0.1, voltage=200.0, te_ev=3.0,
+                            ion_density={"Ar+": 1e15, "O2+": 2e14, "O+": 0.0, "O-": 2e14}), 515),
+    "o2_33x17": (ccp_deck(33, 17, 0.01, 0.005, gas="O2", ppc=12, pressure_torr=0.1, voltage=200.0, te_ev=3.0,
+                          ion_density={"O2+": 1e15, "O+": 1e14, "O-": 1e14}), 616),
 }
 
 
