@@ -136,6 +136,7 @@ void fill_info(const Setup &s, hp_case_info *out) {
     for (int i = 0; i < s.nsp && i < 8; i++) out->cap[i] = s.cap[i];
     out->mcc_subcycles = s.mcc_n;
     out->dt = s.dt; out->dx = s.dx; out->dy = s.dy;
+    out->mcc_stride = s.main_gas == GAS_AR ? 8 : 72;
 }
 
 // Collision probability per cell from its lower-left node
@@ -275,6 +276,7 @@ hp_status build_device(hp_case *c) {
         sp.Ascale = s.sp[isp].Ascale;
         sp.q_density = s.sp[isp].q_density;
         sp.Escale = s.sp[isp].Escale;
+        sp.np2c = s.sp[isp].np2c;
         size_t nslot = (size_t)C * sp.cap;
         TRY(dalloc(c, &sp.x, nslot));
         TRY(dalloc(c, &sp.y, nslot));
@@ -323,10 +325,18 @@ hp_status build_device(hp_case *c) {
     h.n_logx = s.n_logx;
     h.xw = 2 + s.n_cx;
     h.idlogx = s.idlogx;
-    for (size_t k = 0; k < s.sigv.size() && k < 8; k++) h.sigv[k] = s.sigv[k];
-    for (int k = 0; k < s.TnRct && k < 16; k++) {
+    if (s.sigv.size() > 32 || s.TnRct > 96) return set_error("reaction set larger than the device tables"), HP_ERR_UNSUPPORTED;
+    for (size_t k = 0; k < s.sigv.size(); k++) h.sigv[k] = s.sigv[k];
+    for (int k = 0; k < s.TnRct; k++) {
         h.th[k] = s.collf[k].Th_e;
         h.mofm[k] = s.collf[k].mofM;
+    }
+    h.mcc_stride = s.main_gas == GAS_AR ? 8 : 72;
+    if (s.main_gas != GAS_AR) {
+        TRY(dupload(c, (float **)&h.back_den1, s.back_den1));
+        TRY(dupload(c, (float **)&h.back_den2, s.back_den2));
+        TRY(dupload(c, (float **)&h.back_vel2, s.back_vel2));
+        TRY(dupload(c, (float **)&h.fluid_den, s.fluid_den));
     }
     c->prob = cell_probabilities(s);
     TRY(dupload(c, (float **)&h.prob, c->prob));
@@ -334,12 +344,13 @@ hp_status build_device(hp_case *c) {
     TRY(dupload(c, (float **)&h.vsave, s.vsave));
     h.nvel = s.nvel;
     h.mcc_n = s.mcc_n;
+    h.dt_mcc = s.dt_mcc;
     if (s.mcc_n < 1 || s.mcc_n > 2047) return set_error("MCC subcycle count outside 1..2047"), HP_ERR_UNSUPPORTED;
     h.seed = c->opts.seed;
     TRY(dalloc(c, &h.tstep, 1));
     TRY(dalloc(c, &h.status, 1));
     TRY(dalloc(c, &h.cond_charge, (size_t)s.nsp * s.cond_numr));
-    TRY(dalloc(c, &h.mcc_count, (size_t)8 * C));
+    TRY(dalloc(c, &h.mcc_count, (size_t)h.mcc_stride * C));
     TRY(dalloc(c, &h.pcg_iters, 2));
     TRY(dalloc(c, &h.ave_count, 1));
     TRY(dalloc(c, &h.pushes, 32));
@@ -410,6 +421,10 @@ hp_status op_sort(hp_case *c, cudaStream_t st) {
     return e == cudaSuccess ? HP_OK : cuda_fail(e, "sort");
 }
 hp_status op_mcc(hp_case *c, cudaStream_t st) {
+    if (c->s.main_gas == GAS_ARO2) {
+        cudaError_t e = launch_mcc_oxy(c->d_case, c->d_items + 2, 1, c->s.Csize, c->s.main_gas, st);
+        return e == cudaSuccess ? HP_OK : cuda_fail(e, "mcc");
+    }
     if (c->s.main_gas != GAS_AR) {
         set_error("MCC for this gas is not built");
         return HP_ERR_UNSUPPORTED;
@@ -651,7 +666,7 @@ hp_status hp_case_create(const char *deck, size_t len, const hp_case_opts *opts,
     } catch (const std::exception &e) {
         return from_exception(e);
     }
-    if (s.main_gas != GAS_AR) return set_error("MCC for this gas is not built"), HP_ERR_UNSUPPORTED;
+    if (s.main_gas == GAS_O2) return set_error("MCC for this gas is not built"), HP_ERR_UNSUPPORTED;
     return case_from(std::move(s), &o, out);
 }
 
@@ -665,7 +680,7 @@ hp_status hp_case_create_from_setup(const hp_setup *su, const hp_case_opts *opts
 
 namespace hpi {
 hp_status case_from_setup_owned(hp::Setup &&s, const hp_case_opts &o, hp_case **out) {
-    if (s.main_gas != GAS_AR) return set_error("MCC for this gas is not built"), HP_ERR_UNSUPPORTED;
+    if (s.main_gas == GAS_O2) return set_error("MCC for this gas is not built"), HP_ERR_UNSUPPORTED;
     hp_status st = case_from(std::move(s), &o, out);
     if (st != HP_OK) return st;
     // the initial load now lives on the device
@@ -720,6 +735,7 @@ hp_status hp_case_get_info(const hp_case *c, hp_case_info *out) {
     out->device_bytes = c->bytes;
     out->pcg_cluster = c->pcg_cluster;
     out->field_mode = c->h.field_mode;
+    out->mcc_stride = c->h.mcc_stride;
     out->pcg_block = c->lc.pcg_block;
     int64_t t = 0;
     cudaMemcpy(&t, c->h.tstep, 8, cudaMemcpyDeviceToHost);
@@ -907,7 +923,7 @@ static hp_status grid_ptr(hp_case *c, hp_grid_field f, void **p, size_t *nb) {
     case HP_GRID_AVE_DEN: *p = c->h.ave_den; *nb = (size_t)nsp * G * 8; break;
     case HP_GRID_AVE_PHI: *p = c->h.ave_phi; *nb = (size_t)G * 8; break;
     case HP_GRID_COND_CHARGE: *p = c->h.cond_charge; *nb = (size_t)nsp * c->s.cond_numr * 4; break;
-    case HP_GRID_MCC_COUNT: *p = c->h.mcc_count; *nb = (size_t)8 * c->s.Csize * 4; break;
+    case HP_GRID_MCC_COUNT: *p = c->h.mcc_count; *nb = (size_t)c->h.mcc_stride * c->s.Csize * 4; break;
     default: return set_error("unknown grid field"), HP_ERR_ARG;
     }
     return HP_OK;

@@ -35,7 +35,7 @@ struct DevSpecies {
     int *nmov;
     int *dcount; // [C*9] movers per cell and destination code 0..8 (after Move)
     int cap;
-    float Ascale, q_density, Escale;
+    float Ascale, q_density, Escale, np2c;
 };
 
 struct DevCase {
@@ -70,19 +70,23 @@ struct DevCase {
     const float *xsec;              // [n_logx * xw]
     int n_logx, xw;
     float idlogx;
-    float sigv[8];
-    float th[16];                   // CollF.Th_e
-    float mofm[16];
-    const float *prob;              // [3*C]: electron P1, P2; ion P
+    float sigv[32];                 // sigma-v maxima per (projectile, target): 3 Ar, 20 O2, 25 Ar/O2
+    float th[96];                   // CollF.Th_e per reaction channel
+    float mofm[96];
+    int mcc_stride;                 // counters per cell in mcc_count (8 for Ar, 72 for the oxygen sets)
+    const float *prob;              // [3*C]: electron P1, P2; ion P (Ar)
     const float *back_vel1;         // [G]
+    const float *back_den1, *back_den2, *back_vel2; // [G] (oxygen sets)
+    const float *fluid_den;         // [nfsp*G] metastable / radical densities (oxygen sets)
     const float *vsave;
     int nvel, mcc_n;
+    float dt_mcc;                   // electron collision sub-step (DT_MCCn sub-cycles)
     uint64_t seed;
     // bookkeeping
     int64_t *tstep;                 // device step counter
     uint32_t *status;
     float *cond_charge;             // [nsp*cond_numr]
-    unsigned int *mcc_count;        // [16*nsp]
+    unsigned int *mcc_count;        // [C*mcc_stride] collisions per cell and channel
     int *pcg_iters;                 // [2]: inner, outer of the last solve
     int64_t *ave_count;
     unsigned long long *pushes;     // [32] particles pushed by Move, spread over 32 counters

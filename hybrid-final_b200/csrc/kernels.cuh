@@ -23,6 +23,9 @@ cudaError_t launch_move(const DevCase *cases, const int *item_start, int ncases,
 cudaError_t launch_sort(const DevCase *cases, const int *item_start, int ncases, int items, const LaunchCfg &lc,
                         cudaStream_t st);
 // MCC, Ar set (src/cuda_mcc.cu:97-106, src/cuda_mccAr.cu:41-232)
+// MCC of the Ar/O2 (gas 2) reaction set, one warp per cell (mcc_oxy.cu)
+cudaError_t launch_mcc_oxy(const DevCase *cases, const int *item_start, int ncases, int items, int gas,
+                           cudaStream_t st);
 cudaError_t launch_mcc_ar(const DevCase *cases, const int *item_start, int ncases, int items, const LaunchCfg &lc,
                           cudaStream_t st);
 // Deposit: per-cell CIC sums, then node gather + boundary scale + rho/eps0 + RHS

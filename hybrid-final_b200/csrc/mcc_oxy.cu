@@ -1,0 +1,617 @@
+// mcc_oxy.cu -- null-collision MCC of the Ar/O2 reaction set (5 species:
+// e, Ar+, O2+, O+, O-), one warp per cell (MCC_ArO2_Basic,
+// src/cuda_mcc.cu:21-71; ArO2_Collision_Check and the species handlers,
+// src/cuda_mccArO2.cu:51-1265).
+//
+// The reference runs one thread per (species, node) with the species
+// handlers concurrently: a handler that creates or deletes particles of
+// another species races with that species' own thread.  Here one warp owns
+// the cell and the order is fixed:
+//   * every species' collision test uses the counts at the start of the call
+//     (particles created during the call are not tested this step);
+//   * the species are handled in order e, Ar+, O2+, O+, O-; within a species
+//     the colliders in slot order, 32 at a time (one per lane);
+//   * a collider that leaves its species (attachment, recombination, charge
+//     transfer to another ion, detachment) leaves a hole; particles created
+//     are appended to their species in collider order;
+//   * the O- that an electron detachment (e + O- -> 2e + O) removes is drawn
+//     uniformly among the O- present at the start of the call and still
+//     there (the reference copies the slot one past its count into the
+//     victim, a stale particle); a removed O- is not processed by the O-
+//     handler afterwards;
+//   * at the end every species' holes are filled with its last particles.
+// Draws: the collision test from the shared test blocks (hp_test_block), all
+// later draws of a collider from its own stream, in the reference's order.
+// Reference behaviour kept as is: the first channel of a ladder whose
+// threshold fails leaves the running cross-section sum at 0 (uninitialised in
+// the reference); ion ladders compare each channel alone where the reference
+// does; O2+ always takes its neutral velocity from the Ar temperature and O+
+// from the O2 one; an O- scatters with the reference's renormalised
+// direction and a detached electron takes the O-'s unit direction as its
+// velocity; recombination removes only the projectile; channel 16 loses the
+// threshold of channel 11.
+#include <cstdint>
+
+#include "devutil.cuh"
+#include "kernels.cuh"
+
+namespace hp {
+namespace {
+
+using namespace dv;
+
+constexpr int OXY_TPB = 128;
+constexpr int OXY_RING = 256;
+constexpr int HOLE_CAP = 64;
+constexpr int NSP_ARO2 = 5;
+
+enum : int { A_ELASTIC, A_LOSS, A_GAIN, A_ATTACH, A_IONIZE, A_RECOMB, A_DETACH };
+
+struct Rung {
+    int8_t ch, act, a1, a2; // a1: threshold index (loss) or first new species (ionisation); a2: second
+    float gain;
+};
+
+// electron ladders per target (src/cuda_mccArO2.cu:91-435)
+__constant__ Rung c_erung[] = {
+    // 0: e + Ar
+    {0, A_ELASTIC, 0, 0, 0}, {1, A_LOSS, 1, 0, 0}, {2, A_LOSS, 2, 0, 0}, {3, A_IONIZE, 0, 1, 0},
+    // 1: e + Ar*
+    {4, A_IONIZE, 0, 1, 0},
+    // 2: e + O2
+    {5, A_ELASTIC, 0, 0, 0}, {6, A_LOSS, 6, 0, 0}, {7, A_LOSS, 7, 0, 0}, {8, A_LOSS, 8, 0, 0},
+    {9, A_LOSS, 9, 0, 0}, {10, A_LOSS, 10, 0, 0}, {11, A_ATTACH, 0, 0, 0}, {12, A_LOSS, 12, 0, 0},
+    {13, A_LOSS, 13, 0, 0}, {14, A_LOSS, 14, 0, 0}, {15, A_IONIZE, 0, 2, 0}, {16, A_LOSS, 11, 0, 0},
+    {17, A_IONIZE, 3, 4, 0}, {18, A_IONIZE, 0, 3, 0},
+    // 3: e + O2(a)
+    {19, A_IONIZE, 0, 2, 0}, {20, A_ATTACH, 0, 0, 0}, {21, A_GAIN, 0, 0, 0.977f}, {22, A_GAIN, 0, 0, 0.977f},
+    {23, A_LOSS, 23, 0, 0}, {24, A_LOSS, 24, 0, 0}, {25, A_LOSS, 25, 0, 0}, {26, A_IONIZE, 0, 3, 0},
+    // 4: e + O2(b)
+    {27, A_IONIZE, 0, 2, 0}, {28, A_ATTACH, 0, 0, 0}, {29, A_GAIN, 0, 0, 1.627f}, {30, A_GAIN, 0, 0, 1.627f},
+    {31, A_LOSS, 31, 0, 0}, {32, A_LOSS, 32, 0, 0}, {33, A_LOSS, 33, 0, 0}, {34, A_IONIZE, 0, 3, 0},
+    // 5: e + O-
+    {35, A_DETACH, 0, 0, 0},
+    // 6: e + O2+
+    {36, A_RECOMB, 0, 0, 0},
+    // 7: e + O(3P)
+    {37, A_LOSS, 37, 0, 0}, {38, A_LOSS, 38, 0, 0}, {39, A_LOSS, 39, 0, 0}, {40, A_LOSS, 40, 0, 0},
+    {41, A_LOSS, 41, 0, 0}, {42, A_IONIZE, 0, 3, 0}, {43, A_LOSS, 43, 0, 0},
+    // 8: e + O(1D)
+    {44, A_IONIZE, 0, 3, 0}, {45, A_GAIN, 0, 0, 1.96f},
+};
+__constant__ int c_erung_start[10] = {0, 4, 5, 19, 27, 35, 36, 37, 44, 46};
+
+// collision probabilities of one cell (cumulative over the targets) from the
+// node's background, fluid and charged densities (ArO2_Collision_Check,
+// src/cuda_mccArO2.cu:1130-1190).  The electron sums run in float with 1.0f,
+// the ion sums in double as the reference's 1.0 literal makes them.
+struct CellProb {
+    float p[5][9];
+    int n[5];
+};
+
+__device__ __forceinline__ float xe(float a, float b, float c) { return hp_expf(-1 * a * b * c); }
+
+__device__ __forceinline__ float ion_acc(float prev, bool first, float e) {
+    return first ? (float)(1.0 - (double)e) : (float)((double)prev + 1.0 - (double)e);
+}
+
+__device__ void cell_prob(const DevCase &d, int node, CellProb &P) {
+    const int G = d.G;
+    const float bd1 = d.back_den1[node], bd2 = d.back_den2[node];
+    const float F0 = d.fluid_den[node], F1 = d.fluid_den[G + node], F2 = d.fluid_den[2 * G + node];
+    const float F3 = d.fluid_den[3 * G + node], F4 = d.fluid_den[4 * G + node];
+    // charged densities from the last deposit: den * np2c * idx * idy, in this order
+    auto nq = [&](int s, float sig, float dtx) {
+        float t = -1 * dtx;
+        t = t * sig;
+        t = t * (float)d.den[(size_t)s * G + node];
+        t = t * d.sp[s].np2c;
+        t = t * d.idx;
+        t = t * d.idy;
+        return hp_expf(t);
+    };
+    const float dtm = d.dt_mcc, dt = d.dt;
+    const float *sv = d.sigv;
+    float *e = P.p[0];
+    e[0] = 1.0f - xe(dtm, sv[0], bd1);
+    e[1] = e[0] + 1.0f - xe(dtm, sv[1], F0);
+    e[2] = e[1] + 1.0f - xe(dtm, sv[2], bd2);
+    e[3] = e[2] + 1.0f - xe(dtm, sv[3], F1);
+    e[4] = e[3] + 1.0f - xe(dtm, sv[4], F2);
+    e[5] = e[4] + 1.0f - nq(4, sv[5], dtm);
+    e[6] = e[5] + 1.0f - nq(2, sv[6], dtm);
+    e[7] = e[6] + 1.0f - xe(dtm, sv[7], F3);
+    e[8] = e[7] + 1.0f - xe(dtm, sv[8], F4);
+    P.n[0] = 9;
+    float *a = P.p[1]; // Ar+: Ar, O2
+    a[0] = ion_acc(0, true, xe(dt, sv[23], bd1));
+    a[1] = ion_acc(a[0], false, xe(dt, sv[24], bd2));
+    P.n[1] = 2;
+    float *o2 = P.p[2]; // O2+: OP, O2, O2A, O2B, Ar
+    o2[0] = ion_acc(0, true, xe(dt, sv[14], F3));
+    o2[1] = ion_acc(o2[0], false, xe(dt, sv[15], bd2));
+    o2[2] = ion_acc(o2[1], false, xe(dt, sv[16], F1));
+    o2[3] = ion_acc(o2[2], false, xe(dt, sv[17], F2));
+    o2[4] = ion_acc(o2[3], false, xe(dt, sv[18], bd1));
+    P.n[2] = 5;
+    float *op = P.p[3]; // O+: O2, OP, O2A, O2B
+    op[0] = ion_acc(0, true, xe(dt, sv[19], bd2));
+    op[1] = ion_acc(op[0], false, xe(dt, sv[20], F3));
+    op[2] = ion_acc(op[1], false, xe(dt, sv[21], F1));
+    op[3] = ion_acc(op[2], false, xe(dt, sv[22], F2));
+    P.n[3] = 4;
+    float *om = P.p[4]; // O-: O2, OP, O2+, O+, O2A
+    om[0] = ion_acc(0, true, xe(dt, sv[9], bd2));
+    om[1] = ion_acc(om[0], false, xe(dt, sv[10], F3));
+    om[2] = ion_acc(om[1], false, nq(2, sv[11], dt));
+    om[3] = ion_acc(om[2], false, nq(3, sv[12], dt));
+    om[4] = ion_acc(om[3], false, xe(dt, sv[13], F1));
+    P.n[4] = 5;
+}
+
+// target of a hit: the first cumulative probability R1 does not exceed
+__device__ __forceinline__ int target_of(const CellProb &P, int s, float R1) {
+    const int n = P.n[s];
+    for (int t = 0; t < n - 1; t++)
+        if (R1 <= P.p[s][t]) return t;
+    return n - 1;
+}
+
+// a particle created by a collision
+struct Born {
+    int sp; // -1: none
+    float vx, vy, vz;
+};
+
+// outcome of one collider
+struct Outcome {
+    bool keep;           // stays in its species (velocity updated in place)
+    float vx, vy, vz;    // its new velocity when kept
+    Born b[2];
+    bool kill_partner;   // electron detachment: remove one O-
+    float r2;            // the draw that picks it
+    int ch;              // channel counted (-1: null)
+};
+
+__device__ __forceinline__ void no_birth(Outcome &o) {
+    o.b[0].sp = o.b[1].sp = -1;
+    o.kill_partner = false;
+    o.r2 = 0.f;
+    o.ch = -1;
+}
+
+// ArO2_Electron (src/cuda_mccArO2.cu:51-560), one collider with target t
+__device__ void electron_collide(const DevCase &d, float vx, float vy, float vz, int t, float bv1, hp_stream &rs,
+                                 Outcome &o) {
+    no_birth(o);
+    const float Esc = d.sp[0].Escale;
+    float VX = vx, VY = vy, VZ = vz;
+    const float dum = VX * VX + VY * VY + VZ * VZ;
+    float vel = sqrtf(dum);
+    VX /= vel; VY /= vel; VZ /= vel;
+    float engy = Esc * dum;
+    int colltype = 1, i1 = 0, i2 = 0;
+    float rengy = 0.f, vel2 = 0.f;
+    float R1 = hp_stream_next(&rs);
+    R1 *= d.sigv[t] / vel;
+    float sum = 0.f;
+    bool hit = false;
+    for (int k = c_erung_start[t]; k < c_erung_start[t + 1]; k++) {
+        const Rung r = c_erung[k];
+        if (!(engy > d.th[r.ch])) continue;
+        sum = sum + xsec_lookup(d, r.ch, engy);
+        if (!(R1 <= sum)) continue;
+        hit = true;
+        o.ch = r.ch;
+        switch (r.act) {
+        case A_ELASTIC: break;
+        case A_LOSS:
+            engy -= d.th[r.a1];
+            vel = sqrtf(fabsf(engy) / Esc);
+            break;
+        case A_GAIN:
+            engy += r.gain;
+            vel = sqrtf(fabsf(engy) / Esc);
+            break;
+        case A_ATTACH: colltype = 2; break;
+        case A_RECOMB: colltype = 4; break;
+        case A_DETACH:
+            colltype = 5;
+            engy -= d.th[r.ch];
+            vel = sqrtf(fabsf(engy) / Esc);
+            break;
+        default: { // A_IONIZE
+            colltype = 3;
+            engy -= d.th[r.ch];
+            const float u = hp_stream_next(&rs);
+            rengy = (float)(10.0 * (double)hp_tanf_q1(u * hp_atanf((float)(engy / 20.0))));
+            engy -= rengy;
+            vel = sqrtf(fabsf(rengy) / Esc);
+            vel2 = sqrtf(fabsf(engy) / Esc);
+            i1 = r.a1;
+            i2 = r.a2;
+            break;
+        }
+        }
+        break;
+    }
+    if (!hit) colltype = 0;
+    o.keep = true;
+    o.vx = vx; o.vy = vy; o.vz = vz;
+    switch (colltype) {
+    case 0: break;
+    case 1: {
+        const float a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+        anewvel_dev(engy, vel, VX, VY, VZ, a, b);
+        o.vx = VX; o.vy = VY; o.vz = VZ;
+        break;
+    }
+    case 2: { // attachment: the electron becomes an O- at rest in the neutral frame
+        o.keep = false;
+        const int n = (int)((d.nvel - 1) * hp_stream_next(&rs));
+        const float a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+        o.b[0].sp = 4;
+        maxwellv_dev(o.b[0].vx, o.b[0].vy, o.b[0].vz, d.vsave[n], bv1, a, b);
+        break;
+    }
+    case 3: { // ionisation: two new charged particles, then the primary loses energy
+        const int isp[2] = {i1, i2};
+        for (int q = 0; q < 2; q++) {
+            Born &b = o.b[q];
+            b.sp = isp[q];
+            if (isp[q] == 0) {
+                b.vx = VX; b.vy = VY; b.vz = VZ;
+                const float a = hp_stream_next(&rs), c = hp_stream_next(&rs);
+                anewvel_dev(rengy, vel, b.vx, b.vy, b.vz, a, c);
+            } else {
+                const int n = (int)((d.nvel - 1) * hp_stream_next(&rs));
+                const float a = hp_stream_next(&rs), c = hp_stream_next(&rs);
+                maxwellv_dev(b.vx, b.vy, b.vz, d.vsave[n], bv1, a, c);
+            }
+        }
+        const float a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+        anewvel_dev(engy, vel2, VX, VY, VZ, a, b);
+        o.vx = VX; o.vy = VY; o.vz = VZ;
+        break;
+    }
+    case 4: o.keep = false; break; // recombination: only the electron goes
+    default: {                      // 5: detachment e + O- -> 2e + O
+        o.b[0].sp = 0;
+        o.b[0].vx = VX; o.b[0].vy = VY; o.b[0].vz = VZ; // the unit direction, as the reference
+        const float a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+        anewvel_dev(engy, vel, VX, VY, VZ, a, b);
+        o.vx = VX; o.vy = VY; o.vz = VZ;
+        o.kill_partner = true;
+        o.r2 = hp_stream_next(&rs);
+        break;
+    }
+    }
+}
+
+// ArO2_Ar_ion / _O2_ion / _O_ion / _O_negative (src/cuda_mccArO2.cu:561-1129)
+enum : int { I_NULL, I_SCAT, I_CX, I_TO_OP, I_TO_ARP, I_TO_O2P, I_DETACH, I_RECOMB };
+
+__device__ void ion_collide(const DevCase &d, int s, float vx, float vy, float vz, int t, float bv1, float bv2,
+                            hp_stream &rs, Outcome &o) {
+    no_birth(o);
+    o.keep = true;
+    o.vx = vx; o.vy = vy; o.vz = vz;
+    const float Esc = d.sp[s].Escale;
+    float vnx = 0.f, vny = 0.f, vnz = 0.f;
+    float VX, VY, VZ, vel, engy;
+    if (s == 4) { // O-: no neutral velocity; the direction is normalised
+        VX = vx; VY = vy; VZ = vz;
+        const float dum = VX * VX + VY * VY + VZ * VZ;
+        vel = sqrtf(dum);
+        VX /= vel; VY /= vel; VZ /= vel;
+        engy = Esc * dum;
+    } else {
+        const float vneut = s == 1 ? (t == 0 ? bv1 : bv2) : (s == 2 ? bv1 : bv2);
+        const int n = (int)((d.nvel - 1) * hp_stream_next(&rs));
+        const float a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+        maxwellv_dev(vnx, vny, vnz, d.vsave[n], vneut, a, b);
+        VX = vx - vnx; VY = vy - vny; VZ = vz - vnz;
+        const float dum = VX * VX + VY * VY + VZ * VZ;
+        vel = sqrtf(dum);
+        engy = Esc * dum;
+        if (s == 1) (void)hp_stream_next(&rs); // the reference draws R1 and overwrites it
+    }
+    // (sigma-v index, channels, actions, cumulative second rung)
+    int sv = 0, nr = 0, ch[3] = {0, 0, 0}, act[3] = {0, 0, 0};
+    bool cum = false;
+    switch (s) {
+    case 1:
+        sv = 23 + t;
+        if (t == 0) { nr = 2; ch[0] = 65; act[0] = I_CX; ch[1] = 66; act[1] = I_SCAT; }
+        else { nr = 1; ch[0] = 67; act[0] = I_SCAT; }
+        break;
+    case 2:
+        sv = 14 + t;
+        if (t == 0) { nr = 1; ch[0] = 52; act[0] = I_TO_OP; }
+        else if (t == 1) { nr = 3; ch[0] = 53; act[0] = I_CX; ch[1] = 54; act[1] = I_SCAT; ch[2] = 55; act[2] = I_TO_OP; }
+        else if (t == 2) { nr = 1; ch[0] = 56; act[0] = I_CX; }
+        else if (t == 3) { nr = 1; ch[0] = 57; act[0] = I_CX; }
+        else { nr = 2; ch[0] = 58; act[0] = I_TO_ARP; ch[1] = 59; act[1] = I_CX; }
+        break;
+    case 3:
+        sv = 19 + t;
+        if (t == 0) { nr = 2; ch[0] = 60; act[0] = I_TO_O2P; ch[1] = 61; act[1] = I_SCAT; }
+        else if (t == 1) { nr = 1; ch[0] = 62; act[0] = I_CX; }
+        else { nr = 1; ch[0] = 62 + t - 1; act[0] = I_TO_O2P; }
+        break;
+    default: // O-
+        sv = 9 + t;
+        if (t == 0) { nr = 2; ch[0] = 46; act[0] = I_SCAT; ch[1] = 47; act[1] = I_DETACH; cum = true; }
+        else if (t == 1) { nr = 1; ch[0] = 48; act[0] = I_DETACH; }
+        else if (t == 2) { nr = 1; ch[0] = 49; act[0] = I_RECOMB; }
+        else if (t == 3) { nr = 1; ch[0] = 50; act[0] = I_RECOMB; }
+        else { nr = 1; ch[0] = 51; act[0] = I_DETACH; }
+        break;
+    }
+    const float R1 = hp_stream_next(&rs) * d.sigv[sv] / vel;
+    int what = I_NULL;
+    float sum = 0.f;
+    for (int k = 0; k < nr; k++) {
+        if (!(engy > d.th[ch[k]])) continue;
+        const float xs = xsec_lookup(d, ch[k], engy);
+        sum = (k > 0 && cum) ? sum + xs : xs;
+        if (R1 <= sum) {
+            what = act[k];
+            o.ch = ch[k];
+            break;
+        }
+    }
+    switch (what) {
+    case I_NULL: break;
+    case I_SCAT: {
+        const float a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+        newvel_ionsc_dev(VX, VY, VZ, vel, a, b);
+        if (s == 4) { o.vx = VX; o.vy = VY; o.vz = VZ; }
+        else { o.vx = VX + vnx; o.vy = VY + vny; o.vz = VZ + vnz; }
+        break;
+    }
+    case I_CX: o.vx = vnx; o.vy = vny; o.vz = vnz; break;
+    case I_TO_OP: o.keep = false; o.b[0] = Born{3, vnx, vny, vnz}; break;
+    case I_TO_ARP: o.keep = false; o.b[0] = Born{1, vnx, vny, vnz}; break;
+    case I_TO_O2P: o.keep = false; o.b[0] = Born{2, vnx, vny, vnz}; break;
+    case I_DETACH: o.keep = false; o.b[0] = Born{0, VX, VY, VZ}; break;
+    default: o.keep = false; break; // I_RECOMB
+    }
+}
+
+__device__ __forceinline__ bool is_hole(float x) { return x != x; }
+
+__global__ void __launch_bounds__(OXY_TPB) k_mcc_aro2(const DevCase *__restrict__ cases,
+                                                      const int *__restrict__ item_start, int ncases, int items) {
+    __shared__ int ring_s[OXY_TPB / 32][OXY_RING];
+    __shared__ int holes_s[OXY_TPB / 32][NSP_ARO2][HOLE_CAP];
+    const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    if (warp >= items) return;
+    int *ring = ring_s[wl];
+    const int ci = find_case(item_start, ncases, warp);
+    const DevCase &d = cases[ci];
+    const int c = warp - item_start[ci];
+    const int i = c / d.ncy, j = c - i * d.ncy;
+    const int node = i * d.ngy + j;
+    const uint32_t step = (uint32_t)(*d.tstep);
+    const float bv1 = d.back_vel1[node], bv2 = d.back_vel2[node];
+    const unsigned lt = lanemask_lt();
+    CellProb P;
+    cell_prob(d, node, P);
+    int n0[NSP_ARO2], cnt[NSP_ARO2], nh[NSP_ARO2];
+#pragma unroll
+    for (int s = 0; s < NSP_ARO2; s++) {
+        n0[s] = d.sp[s].cnt[c];
+        cnt[s] = n0[s];
+        nh[s] = 0;
+    }
+    bool overflow = false, hole_over[NSP_ARO2] = {false, false, false, false, false};
+    unsigned *mcount = d.mcc_count + (size_t)c * d.mcc_stride;
+    auto add_hole = [&](int s, int slot) { // lane-uniform call
+        if (nh[s] < HOLE_CAP) holes_s[wl][s][nh[s]] = slot;
+        else hole_over[s] = true;
+        nh[s]++;
+    };
+#pragma unroll 1
+    for (int s = 0; s < NSP_ARO2; s++) {
+        const DevSpecies &sp = d.sp[s];
+        const size_t base = (size_t)c * sp.cap;
+        const int n = n0[s];
+        const int nsub = s == 0 ? d.mcc_n : 1;
+        const float Tprob = P.p[s][P.n[s] - 1];
+        int head = 0, tail = 0;
+        for (int k0 = 0; k0 < n || tail > head; k0 += 128) {
+            if (k0 < n) {
+                // the test: four slots per lane from one Philox block per sub-cycle
+                const int k = k0 + 4 * lane;
+                unsigned hits = 0;
+                int ent[4] = {0, 0, 0, 0};
+                if (k < n) {
+                    const unsigned live = k + 4 <= n ? 0xFu : (1u << (n - k)) - 1u;
+                    for (int jj = 0; jj < nsub && hits != live; jj++) {
+                        const hp_u4 u = hp_test_block(d.seed, (uint32_t)(k >> 2), (uint32_t)c, step, (uint32_t)s,
+                                                      (uint32_t)jj);
+#pragma unroll
+                        for (int t = 0; t < 4; t++) {
+                            const float R1 = hp_u01(hp_word(u, (uint32_t)t));
+                            if (((live & ~hits) >> t) & 1u && R1 < Tprob) {
+                                hits |= 1u << t;
+                                ent[t] = (k + t) | (target_of(P, s, R1) << 20);
+                            }
+                        }
+                    }
+                }
+                int total;
+                int pos = tail + lower_lane_hits(hits, lt, total);
+#pragma unroll
+                for (int t = 0; t < 4; t++)
+                    if ((hits >> t) & 1u) ring[(pos++) & (OXY_RING - 1)] = ent[t];
+                tail += total;
+            }
+            __syncwarp();
+            const bool last = k0 + 128 >= n;
+            while (tail - head >= 32 || (last && tail > head)) {
+                const int e = head + lane;
+                Outcome o;
+                no_birth(o);
+                o.keep = true;
+                bool active = false;
+                int k = 0;
+                float px = 0.f, py = 0.f;
+                if (e < tail) {
+                    const int ent = ring[e & (OXY_RING - 1)];
+                    k = ent & 0xFFFFF;
+                    const int t = ent >> 20;
+                    px = sp.x[base + k];
+                    if (!is_hole(px)) { // an O- removed earlier this call is gone
+                        active = true;
+                        py = sp.y[base + k];
+                        const float vx = sp.vx[base + k], vy = sp.vy[base + k], vz = sp.vz[base + k];
+                        hp_stream rs;
+                        hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, (uint32_t)s);
+                        if (s == 0) electron_collide(d, vx, vy, vz, t, bv1, rs, o);
+                        else ion_collide(d, s, vx, vy, vz, t, bv1, bv2, rs, o);
+                        if (o.ch >= 0) atomicAdd(&mcount[o.ch], 1u);
+                        if (o.keep) {
+                            sp.vx[base + k] = o.vx;
+                            sp.vy[base + k] = o.vy;
+                            sp.vz[base + k] = o.vz;
+                        } else {
+                            sp.x[base + k] = __int_as_float(0x7fc00000); // hole
+                        }
+                    }
+                }
+                // holes left by the colliders, in slot order
+                const unsigned bgone = __ballot_sync(FULL, active && !o.keep);
+                for (unsigned m = bgone; m; m &= m - 1) {
+                    const int src = __ffs(m) - 1;
+                    add_hole(s, __shfl_sync(FULL, k, src));
+                }
+                // births, per species in lane (= collider) order; a collider's
+                // two births, if any, go to two different species
+#pragma unroll 1
+                for (int t = 0; t < NSP_ARO2; t++) {
+                    const int q = (active && o.b[0].sp == t) ? 0 : (active && o.b[1].sp == t) ? 1 : -1;
+                    const unsigned bm = __ballot_sync(FULL, q >= 0);
+                    if (!bm) continue;
+                    if (q >= 0) {
+                        const int slot = cnt[t] + __popc(bm & lt);
+                        const DevSpecies &tp = d.sp[t];
+                        if (slot < tp.cap) {
+                            const size_t q2 = (size_t)c * tp.cap + slot;
+                            tp.x[q2] = px;
+                            tp.y[q2] = py;
+                            tp.vx[q2] = o.b[q].vx;
+                            tp.vy[q2] = o.b[q].vy;
+                            tp.vz[q2] = o.b[q].vz;
+                        } else {
+                            overflow = true;
+                        }
+                    }
+                    cnt[t] = min(cnt[t] + __popc(bm), d.sp[t].cap);
+                }
+                // O- removed by detachments, in lane order, among the O- present
+                // at the start of the call that are still there
+                const unsigned bk = __ballot_sync(FULL, active && o.kill_partner);
+                for (unsigned m = bk; m; m &= m - 1) {
+                    const int src = __ffs(m) - 1;
+                    const float r2 = __shfl_sync(FULL, o.r2, src);
+                    const DevSpecies &om = d.sp[4];
+                    const size_t ob = (size_t)c * om.cap;
+                    int victim = -1;
+                    if (lane == 0) {
+                        int nlive = 0;
+                        for (int q = 0; q < n0[4]; q++) nlive += is_hole(om.x[ob + q]) ? 0 : 1;
+                        if (nlive > 0) {
+                            int pick = 0;
+                            if (nlive > 1) {
+                                pick = (int)((float)nlive * r2);
+                                if (pick > nlive - 1) pick = nlive - 1;
+                            }
+                            for (int q = 0; q < n0[4]; q++) {
+                                if (is_hole(om.x[ob + q])) continue;
+                                if (pick-- == 0) { victim = q; break; }
+                            }
+                            om.x[ob + victim] = __int_as_float(0x7fc00000);
+                        }
+                    }
+                    victim = __shfl_sync(FULL, victim, 0);
+                    __syncwarp();
+                    if (victim >= 0) add_hole(4, victim);
+                }
+                head = min(head + 32, tail);
+                __syncwarp();
+            }
+        }
+    }
+    // fill every species' holes with its last particles
+#pragma unroll 1
+    for (int s = 0; s < NSP_ARO2; s++) {
+        const DevSpecies &sp = d.sp[s];
+        const size_t base = (size_t)c * sp.cap;
+        int n = cnt[s];
+        if (nh[s] == 0) {
+            if (lane == 0) sp.cnt[c] = n;
+            continue;
+        }
+        if (!hole_over[s]) {
+            if (lane == 0) {
+                int *h = holes_s[wl][s];
+                const int m = nh[s];
+                for (int a = 1; a < m; a++) { // insertion sort: the list is short
+                    const int v = h[a];
+                    int b = a - 1;
+                    while (b >= 0 && h[b] > v) { h[b + 1] = h[b]; b--; }
+                    h[b + 1] = v;
+                }
+                for (int a = 0; a < m; a++) {
+                    while (n > 0 && is_hole(sp.x[base + n - 1])) n--;
+                    const int hpos = h[a];
+                    if (hpos >= n) continue;
+                    const size_t from = base + n - 1, to = base + hpos;
+                    sp.x[to] = sp.x[from]; sp.y[to] = sp.y[from];
+                    sp.vx[to] = sp.vx[from]; sp.vy[to] = sp.vy[from]; sp.vz[to] = sp.vz[from];
+                    n--;
+                }
+                while (n > 0 && is_hole(sp.x[base + n - 1])) n--;
+                sp.cnt[c] = n;
+            }
+        } else {
+            // more holes than the list holds: stable compaction of the whole species
+            int out = 0;
+            for (int k0 = 0; k0 < n; k0 += 32) {
+                const int k = k0 + lane;
+                float x = 0.f, y = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
+                const bool in = k < n;
+                if (in) { x = sp.x[base + k]; y = sp.y[base + k]; vx = sp.vx[base + k]; vy = sp.vy[base + k]; vz = sp.vz[base + k]; }
+                const bool live = in && !is_hole(x);
+                const unsigned bl = __ballot_sync(FULL, live);
+                __syncwarp();
+                if (live) {
+                    const size_t to = base + out + __popc(bl & lt);
+                    sp.x[to] = x; sp.y[to] = y; sp.vx[to] = vx; sp.vy[to] = vy; sp.vz[to] = vz;
+                }
+                out += __popc(bl);
+                __syncwarp();
+            }
+            if (lane == 0) sp.cnt[c] = out;
+        }
+        __syncwarp();
+    }
+    if (__any_sync(FULL, overflow) && lane == 0) atomicOr(d.status, ST_OVERFLOW);
+}
+
+} // namespace
+
+cudaError_t launch_mcc_oxy(const DevCase *cases, const int *item_start, int ncases, int items, int gas,
+                           cudaStream_t st) {
+    if (items <= 0) return cudaSuccess;
+    if (gas != 2) return cudaErrorNotSupported;
+    k_mcc_aro2<<<(unsigned)((items * 32LL + OXY_TPB - 1) / OXY_TPB), OXY_TPB, 0, st>>>(cases, item_start, ncases,
+                                                                                          items);
+    return cudaGetLastError();
+}
+
+} // namespace hp

@@ -110,7 +110,7 @@ void worker_main(hp_server *s) {
         std::string msg;
         try {
             hp::build_setup(r->deck.data(), r->deck.size(), b, r->setup);
-            if (r->setup.main_gas != hp::GAS_AR) {
+            if (r->setup.main_gas == hp::GAS_O2) {
                 err = HP_ERR_UNSUPPORTED;
                 msg = "MCC for this gas is not built";
             }

@@ -51,7 +51,7 @@ class CaseInfo(C.Structure):
                 ("Csize", C.c_int), ("nsp", C.c_int), ("main_gas", C.c_int), ("cond_numr", C.c_int),
                 ("n_unknowns", C.c_int), ("cap", C.c_int * 8), ("mcc_subcycles", C.c_int), ("dt", C.c_double),
                 ("dx", C.c_double), ("dy", C.c_double), ("tstep", C.c_int64), ("device_bytes", C.c_size_t),
-                ("pcg_cluster", C.c_int), ("pcg_block", C.c_int), ("field_mode", C.c_int)]
+                ("pcg_cluster", C.c_int), ("pcg_block", C.c_int), ("field_mode", C.c_int), ("mcc_stride", C.c_int)]
 
 
 class Tune(C.Structure):
@@ -342,7 +342,7 @@ class Case:
                      DEN=(nsp * G, np.float64), SOURCE=(G, np.float64),
                      PCG_X=(G, np.float32 if self.opts.field_mode == 0 else np.float64),
                      PCG_B=(G, np.float64), AVE_DEN=(nsp * G, np.float64), AVE_PHI=(G, np.float64),
-                     COND_CHARGE=(nsp * info.cond_numr, np.float32), MCC_COUNT=(8 * info.Csize, np.uint32))
+                     COND_CHARGE=(nsp * info.cond_numr, np.float32), MCC_COUNT=(info.mcc_stride * info.Csize, np.uint32))
         n, dt = sizes[name]
         out = np.zeros(n, dtype=dt)
         _check(lib().hp_get_grid(self.h, GRID[name], out.ctypes.data_as(_P), out.nbytes))

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include <algorithm>
+#include <array>
 #include <thread>
 
 #include "hp_math.h"
@@ -140,7 +141,7 @@ template <class R> struct Sim : SimBase {
         source.assign(G, 0.0); b64.assign(G, 0.0); x64.assign(G, 0.0);
         pf_x.assign(G, 0.0f);
         cond_charge.assign((size_t)c.nsp * c.cond_numr, 0.0f);
-        mcc_count.assign((size_t)8 * C, 0u);
+        mcc_count.assign((size_t)(c.mcc_stride > 0 ? c.mcc_stride : 8) * C, 0u);
         ave_den.assign((size_t)c.nsp * G, 0.0);
         ave_phi.assign(G, 0.0);
     }
@@ -470,7 +471,413 @@ template <class R> struct Sim : SimBase {
         vzs = vel * coschi * (r31 * sinchi * cosphi + r32 * sinchi * sinphi + r33 * coschi);
     }
 
+    // ------------------------------------------------------------ MCC (Ar/O2)
+    // MCC_ArO2_Basic (src/cuda_mcc.cu:21-71), ArO2_Collision_Check and the
+    // species handlers (src/cuda_mccArO2.cu:51-1265), with the order this
+    // library defines: tests on the counts at the start of the call, species
+    // e, Ar+, O2+, O+, O- in turn, colliders in slot order, holes filled from
+    // the end of each species (a stable compaction when a species has more
+    // than 64 holes in a cell), births appended in collider order, the O-
+    // removed by a detachment drawn among the O- present at the start.
+    struct OxyOut {
+        bool keep = true;
+        R vx = 0, vy = 0, vz = 0;
+        int bsp[2] = {-1, -1};
+        R bv[2][3] = {{0, 0, 0}, {0, 0, 0}};
+        bool kill = false;
+        float r2 = 0.f;
+        int ch = -1;
+    };
+    static R ox_exp(R x) { return m_exp(x); }
+    // 1 - exp(-a b n) accumulated as the reference does: float with 1.0f for
+    // electrons, double (its 1.0 literal) for ions
+    static R e_acc(R prev, bool first, R ex) { return first ? (R)1.0f - ex : prev + (R)1.0f - ex; }
+    static R i_acc(R prev, bool first, R ex) {
+        return first ? (R)(1.0 - (double)ex) : (R)((double)prev + 1.0 - (double)ex);
+    }
+
+    void oxy_electron(R vx, R vy, R vz, int t, R bv1, hp_stream &rs, OxyOut &o) const {
+        // ladders: (channel, action, threshold index or first new species, second new species, gain)
+        enum { EL, LO, GA, AT, IO, RE, DE };
+        struct Rg { int ch, act, a1, a2; float gain; };
+        static const Rg rg[] = {
+            {0, EL, 0, 0, 0}, {1, LO, 1, 0, 0}, {2, LO, 2, 0, 0}, {3, IO, 0, 1, 0},
+            {4, IO, 0, 1, 0},
+            {5, EL, 0, 0, 0}, {6, LO, 6, 0, 0}, {7, LO, 7, 0, 0}, {8, LO, 8, 0, 0}, {9, LO, 9, 0, 0},
+            {10, LO, 10, 0, 0}, {11, AT, 0, 0, 0}, {12, LO, 12, 0, 0}, {13, LO, 13, 0, 0}, {14, LO, 14, 0, 0},
+            {15, IO, 0, 2, 0}, {16, LO, 11, 0, 0}, {17, IO, 3, 4, 0}, {18, IO, 0, 3, 0},
+            {19, IO, 0, 2, 0}, {20, AT, 0, 0, 0}, {21, GA, 0, 0, 0.977f}, {22, GA, 0, 0, 0.977f},
+            {23, LO, 23, 0, 0}, {24, LO, 24, 0, 0}, {25, LO, 25, 0, 0}, {26, IO, 0, 3, 0},
+            {27, IO, 0, 2, 0}, {28, AT, 0, 0, 0}, {29, GA, 0, 0, 1.627f}, {30, GA, 0, 0, 1.627f},
+            {31, LO, 31, 0, 0}, {32, LO, 32, 0, 0}, {33, LO, 33, 0, 0}, {34, IO, 0, 3, 0},
+            {35, DE, 0, 0, 0},
+            {36, RE, 0, 0, 0},
+            {37, LO, 37, 0, 0}, {38, LO, 38, 0, 0}, {39, LO, 39, 0, 0}, {40, LO, 40, 0, 0}, {41, LO, 41, 0, 0},
+            {42, IO, 0, 3, 0}, {43, LO, 43, 0, 0},
+            {44, IO, 0, 3, 0}, {45, GA, 0, 0, 1.96f},
+        };
+        static const int start[10] = {0, 4, 5, 19, 27, 35, 36, 37, 44, 46};
+        const R Esc = (R)c.Escale[0];
+        R VX = vx, VY = vy, VZ = vz;
+        const R dum = VX * VX + VY * VY + VZ * VZ;
+        R vel = std::sqrt(dum);
+        VX /= vel; VY /= vel; VZ /= vel;
+        R engy = Esc * dum;
+        int colltype = 1, i1 = 0, i2 = 0;
+        R rengy = 0, vel2 = 0;
+        R R1 = (R)hp_stream_next(&rs);
+        R1 *= (R)c.sigv[t] / vel;
+        R sum = 0;
+        bool hit = false;
+        for (int k = start[t]; k < start[t + 1]; k++) {
+            const Rg &r = rg[k];
+            if (!(engy > (R)c.th[r.ch])) continue;
+            sum = sum + xsec(r.ch, engy);
+            if (!(R1 <= sum)) continue;
+            hit = true;
+            o.ch = r.ch;
+            switch (r.act) {
+            case EL: break;
+            case LO: engy -= (R)c.th[r.a1]; vel = std::sqrt(std::fabs(engy) / Esc); break;
+            case GA: engy += (R)r.gain; vel = std::sqrt(std::fabs(engy) / Esc); break;
+            case AT: colltype = 2; break;
+            case RE: colltype = 4; break;
+            case DE:
+                colltype = 5;
+                engy -= (R)c.th[r.ch];
+                vel = std::sqrt(std::fabs(engy) / Esc);
+                break;
+            default: {
+                colltype = 3;
+                engy -= (R)c.th[r.ch];
+                const R u = (R)hp_stream_next(&rs);
+                rengy = (R)(10.0 * (double)m_tan(u * m_atan((R)(engy / 20.0))));
+                engy -= rengy;
+                vel = std::sqrt(std::fabs(rengy) / Esc);
+                vel2 = std::sqrt(std::fabs(engy) / Esc);
+                i1 = r.a1;
+                i2 = r.a2;
+                break;
+            }
+            }
+            break;
+        }
+        if (!hit) colltype = 0;
+        o.keep = true;
+        o.vx = vx; o.vy = vy; o.vz = vz;
+        switch (colltype) {
+        case 0: break;
+        case 1: {
+            const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+            anewvel(engy, vel, VX, VY, VZ, a, b);
+            o.vx = VX; o.vy = VY; o.vz = VZ;
+            break;
+        }
+        case 2: {
+            o.keep = false;
+            const int n = (int)((c.nvel - 1) * hp_stream_next(&rs));
+            const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+            o.bsp[0] = 4;
+            maxwellv(o.bv[0][0], o.bv[0][1], o.bv[0][2], (R)c.vsave[n], bv1, a, b);
+            break;
+        }
+        case 3: {
+            const int isp[2] = {i1, i2};
+            for (int q = 0; q < 2; q++) {
+                o.bsp[q] = isp[q];
+                if (isp[q] == 0) {
+                    o.bv[q][0] = VX; o.bv[q][1] = VY; o.bv[q][2] = VZ;
+                    const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+                    anewvel(rengy, vel, o.bv[q][0], o.bv[q][1], o.bv[q][2], a, b);
+                } else {
+                    const int n = (int)((c.nvel - 1) * hp_stream_next(&rs));
+                    const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+                    maxwellv(o.bv[q][0], o.bv[q][1], o.bv[q][2], (R)c.vsave[n], bv1, a, b);
+                }
+            }
+            const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+            anewvel(engy, vel2, VX, VY, VZ, a, b);
+            o.vx = VX; o.vy = VY; o.vz = VZ;
+            break;
+        }
+        case 4: o.keep = false; break;
+        default: {
+            o.bsp[0] = 0;
+            o.bv[0][0] = VX; o.bv[0][1] = VY; o.bv[0][2] = VZ;
+            const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+            anewvel(engy, vel, VX, VY, VZ, a, b);
+            o.vx = VX; o.vy = VY; o.vz = VZ;
+            o.kill = true;
+            o.r2 = hp_stream_next(&rs);
+            break;
+        }
+        }
+    }
+
+    void oxy_ion(int s, R vx, R vy, R vz, int t, R bv1, R bv2, hp_stream &rs, OxyOut &o) const {
+        enum { NUL, SCAT, CX, TO_OP, TO_ARP, TO_O2P, DET, REC };
+        o.keep = true;
+        o.vx = vx; o.vy = vy; o.vz = vz;
+        const R Esc = (R)c.Escale[s];
+        R vnx = 0, vny = 0, vnz = 0, VX, VY, VZ, vel, engy;
+        if (s == 4) {
+            VX = vx; VY = vy; VZ = vz;
+            const R dum = VX * VX + VY * VY + VZ * VZ;
+            vel = std::sqrt(dum);
+            VX /= vel; VY /= vel; VZ /= vel;
+            engy = Esc * dum;
+        } else {
+            const R vneut = s == 1 ? (t == 0 ? bv1 : bv2) : (s == 2 ? bv1 : bv2);
+            const int n = (int)((c.nvel - 1) * hp_stream_next(&rs));
+            const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+            maxwellv(vnx, vny, vnz, (R)c.vsave[n], vneut, a, b);
+            VX = vx - vnx; VY = vy - vny; VZ = vz - vnz;
+            const R dum = VX * VX + VY * VY + VZ * VZ;
+            vel = std::sqrt(dum);
+            engy = Esc * dum;
+            if (s == 1) (void)hp_stream_next(&rs);
+        }
+        int sv = 0, nr = 0, ch[3] = {0, 0, 0}, act[3] = {0, 0, 0};
+        bool cum = false;
+        switch (s) {
+        case 1:
+            sv = 23 + t;
+            if (t == 0) { nr = 2; ch[0] = 65; act[0] = CX; ch[1] = 66; act[1] = SCAT; }
+            else { nr = 1; ch[0] = 67; act[0] = SCAT; }
+            break;
+        case 2:
+            sv = 14 + t;
+            if (t == 0) { nr = 1; ch[0] = 52; act[0] = TO_OP; }
+            else if (t == 1) { nr = 3; ch[0] = 53; act[0] = CX; ch[1] = 54; act[1] = SCAT; ch[2] = 55; act[2] = TO_OP; }
+            else if (t == 2) { nr = 1; ch[0] = 56; act[0] = CX; }
+            else if (t == 3) { nr = 1; ch[0] = 57; act[0] = CX; }
+            else { nr = 2; ch[0] = 58; act[0] = TO_ARP; ch[1] = 59; act[1] = CX; }
+            break;
+        case 3:
+            sv = 19 + t;
+            if (t == 0) { nr = 2; ch[0] = 60; act[0] = TO_O2P; ch[1] = 61; act[1] = SCAT; }
+            else if (t == 1) { nr = 1; ch[0] = 62; act[0] = CX; }
+            else { nr = 1; ch[0] = 61 + t; act[0] = TO_O2P; }
+            break;
+        default:
+            sv = 9 + t;
+            if (t == 0) { nr = 2; ch[0] = 46; act[0] = SCAT; ch[1] = 47; act[1] = DET; cum = true; }
+            else if (t == 1) { nr = 1; ch[0] = 48; act[0] = DET; }
+            else if (t == 2) { nr = 1; ch[0] = 49; act[0] = REC; }
+            else if (t == 3) { nr = 1; ch[0] = 50; act[0] = REC; }
+            else { nr = 1; ch[0] = 51; act[0] = DET; }
+            break;
+        }
+        const R R1 = (R)hp_stream_next(&rs) * (R)c.sigv[sv] / vel;
+        int what = NUL;
+        R sum = 0;
+        for (int k = 0; k < nr; k++) {
+            if (!(engy > (R)c.th[ch[k]])) continue;
+            const R xs = xsec(ch[k], engy);
+            sum = (k > 0 && cum) ? sum + xs : xs;
+            if (R1 <= sum) { what = act[k]; o.ch = ch[k]; break; }
+        }
+        auto born = [&](int sp_, R a, R b, R cc) { o.keep = false; o.bsp[0] = sp_; o.bv[0][0] = a; o.bv[0][1] = b; o.bv[0][2] = cc; };
+        switch (what) {
+        case NUL: break;
+        case SCAT: {
+            const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+            newvel_ionsc(VX, VY, VZ, vel, a, b);
+            if (s == 4) { o.vx = VX; o.vy = VY; o.vz = VZ; }
+            else { o.vx = VX + vnx; o.vy = VY + vny; o.vz = VZ + vnz; }
+            break;
+        }
+        case CX: o.vx = vnx; o.vy = vny; o.vz = vnz; break;
+        case TO_OP: born(3, vnx, vny, vnz); break;
+        case TO_ARP: born(1, vnx, vny, vnz); break;
+        case TO_O2P: born(2, vnx, vny, vnz); break;
+        case DET: born(0, VX, VY, VZ); break;
+        default: o.keep = false; break;
+        }
+    }
+
+    void mcc_aro2(int64_t tstep) {
+        const uint32_t step = (uint32_t)tstep;
+        const int NS = 5, STRIDE = c.mcc_stride, HOLE_CAP = 64;
+        struct P5 { std::vector<R> x, y, vx, vy, vz; };
+        std::vector<std::array<P5, 5>> out((size_t)C);
+        par_for(C, [&](int cell) {
+            const int i = cell / c.ncy, j = cell - i * c.ncy, node = i * c.ngy + j, Gn = G;
+            const R bd1 = c.back_den1[node], bd2 = c.back_den2[node];
+            const R F0 = c.fluid_den[node], F1 = c.fluid_den[Gn + node], F2 = c.fluid_den[2 * Gn + node];
+            const R F3 = c.fluid_den[3 * Gn + node], F4 = c.fluid_den[4 * Gn + node];
+            auto xe = [&](R a, R b, R n) { return ox_exp(-1 * a * b * n); };
+            auto nq = [&](int s, R sig, R dtx) {
+                R t = -1 * dtx;
+                t = t * sig;
+                t = t * (R)(float)den[(size_t)s * Gn + node];
+                t = t * (R)c.np2c[s];
+                t = t * (R)c.idx;
+                t = t * (R)c.idy;
+                return ox_exp(t);
+            };
+            const R dtm = c.dt_mcc, dt = c.dt;
+            const float *sv = c.sigv;
+            R p[5][9];
+            int np[5] = {9, 2, 5, 4, 5};
+            {
+                R *e = p[0];
+                e[0] = e_acc(0, true, xe(dtm, sv[0], bd1));
+                e[1] = e_acc(e[0], false, xe(dtm, sv[1], F0));
+                e[2] = e_acc(e[1], false, xe(dtm, sv[2], bd2));
+                e[3] = e_acc(e[2], false, xe(dtm, sv[3], F1));
+                e[4] = e_acc(e[3], false, xe(dtm, sv[4], F2));
+                e[5] = e_acc(e[4], false, nq(4, sv[5], dtm));
+                e[6] = e_acc(e[5], false, nq(2, sv[6], dtm));
+                e[7] = e_acc(e[6], false, xe(dtm, sv[7], F3));
+                e[8] = e_acc(e[7], false, xe(dtm, sv[8], F4));
+                R *a = p[1];
+                a[0] = i_acc(0, true, xe(dt, sv[23], bd1));
+                a[1] = i_acc(a[0], false, xe(dt, sv[24], bd2));
+                R *o2 = p[2];
+                o2[0] = i_acc(0, true, xe(dt, sv[14], F3));
+                o2[1] = i_acc(o2[0], false, xe(dt, sv[15], bd2));
+                o2[2] = i_acc(o2[1], false, xe(dt, sv[16], F1));
+                o2[3] = i_acc(o2[2], false, xe(dt, sv[17], F2));
+                o2[4] = i_acc(o2[3], false, xe(dt, sv[18], bd1));
+                R *op = p[3];
+                op[0] = i_acc(0, true, xe(dt, sv[19], bd2));
+                op[1] = i_acc(op[0], false, xe(dt, sv[20], F3));
+                op[2] = i_acc(op[1], false, xe(dt, sv[21], F1));
+                op[3] = i_acc(op[2], false, xe(dt, sv[22], F2));
+                R *om = p[4];
+                om[0] = i_acc(0, true, xe(dt, sv[9], bd2));
+                om[1] = i_acc(om[0], false, xe(dt, sv[10], F3));
+                om[2] = i_acc(om[1], false, nq(2, sv[11], dt));
+                om[3] = i_acc(om[2], false, nq(3, sv[12], dt));
+                om[4] = i_acc(om[3], false, xe(dt, sv[13], F1));
+            }
+            const R bv1 = c.back_vel1[node], bv2 = c.back_vel2[node];
+            std::array<P5, 5> &L = out[(size_t)cell];
+            std::vector<char> gone[5];
+            int n0[5];
+            std::vector<int> holes[5];
+            for (int s = 0; s < NS; s++) {
+                Sp &q = sp[s];
+                const int a = q.start[cell], b = q.start[cell + 1];
+                L[s].x.assign(q.x.begin() + a, q.x.begin() + b);
+                L[s].y.assign(q.y.begin() + a, q.y.begin() + b);
+                L[s].vx.assign(q.vx.begin() + a, q.vx.begin() + b);
+                L[s].vy.assign(q.vy.begin() + a, q.vy.begin() + b);
+                L[s].vz.assign(q.vz.begin() + a, q.vz.begin() + b);
+                n0[s] = b - a;
+                gone[s].assign((size_t)n0[s], 0);
+            }
+            unsigned *cnt = &mcc_count[(size_t)cell * STRIDE];
+            for (int s = 0; s < NS; s++) {
+                const int nsub = s == 0 ? c.mcc_n : 1;
+                const R Tprob = p[s][np[s] - 1];
+                for (int k = 0; k < n0[s]; k++) {
+                    int t = -1;
+                    for (int jj = 0; jj < nsub; jj++) {
+                        const float R1 = hp_test_draw(c.seed, (uint32_t)k, (uint32_t)cell, step, (uint32_t)s, (uint32_t)jj);
+                        if ((R)R1 < Tprob) {
+                            t = np[s] - 1;
+                            for (int q = 0; q < np[s] - 1; q++)
+                                if ((R)R1 <= p[s][q]) { t = q; break; }
+                            break;
+                        }
+                    }
+                    if (t < 0 || gone[s][(size_t)k]) continue;
+                    hp_stream rs;
+                    hp_stream_init(&rs, c.seed, (uint32_t)k, (uint32_t)cell, step, (uint32_t)s);
+                    OxyOut o;
+                    const R vx = L[s].vx[(size_t)k], vy = L[s].vy[(size_t)k], vz = L[s].vz[(size_t)k];
+                    if (s == 0) oxy_electron(vx, vy, vz, t, bv1, rs, o);
+                    else oxy_ion(s, vx, vy, vz, t, bv1, bv2, rs, o);
+                    if (o.ch >= 0) cnt[o.ch]++;
+                    const R px = L[s].x[(size_t)k], py = L[s].y[(size_t)k];
+                    if (o.keep) {
+                        L[s].vx[(size_t)k] = o.vx; L[s].vy[(size_t)k] = o.vy; L[s].vz[(size_t)k] = o.vz;
+                    } else {
+                        gone[s][(size_t)k] = 1;
+                        holes[s].push_back(k);
+                    }
+                    for (int q = 0; q < 2; q++) {
+                        const int t2 = o.bsp[q];
+                        if (t2 < 0) continue;
+                        L[t2].x.push_back(px); L[t2].y.push_back(py);
+                        L[t2].vx.push_back(o.bv[q][0]); L[t2].vy.push_back(o.bv[q][1]); L[t2].vz.push_back(o.bv[q][2]);
+                        gone[t2].push_back(0);
+                    }
+                    if (o.kill) {
+                        int nlive = 0;
+                        for (int q = 0; q < n0[4]; q++) nlive += gone[4][(size_t)q] ? 0 : 1;
+                        if (nlive > 0) {
+                            int pick = 0;
+                            if (nlive > 1) {
+                                pick = (int)((float)nlive * o.r2);
+                                if (pick > nlive - 1) pick = nlive - 1;
+                            }
+                            for (int q = 0; q < n0[4]; q++) {
+                                if (gone[4][(size_t)q]) continue;
+                                if (pick-- == 0) {
+                                    gone[4][(size_t)q] = 1;
+                                    holes[4].push_back(q);
+                                    break;
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            for (int s = 0; s < NS; s++) {
+                P5 &l = L[s];
+                int n = (int)l.x.size();
+                if (holes[s].empty()) continue;
+                if ((int)holes[s].size() <= HOLE_CAP) {
+                    std::vector<int> h = holes[s];
+                    std::sort(h.begin(), h.end());
+                    for (int hp : h) {
+                        while (n > 0 && gone[s][(size_t)n - 1]) n--;
+                        if (hp >= n) continue;
+                        l.x[(size_t)hp] = l.x[(size_t)n - 1]; l.y[(size_t)hp] = l.y[(size_t)n - 1];
+                        l.vx[(size_t)hp] = l.vx[(size_t)n - 1]; l.vy[(size_t)hp] = l.vy[(size_t)n - 1];
+                        l.vz[(size_t)hp] = l.vz[(size_t)n - 1];
+                        gone[s][(size_t)hp] = 0;
+                        n--;
+                    }
+                    while (n > 0 && gone[s][(size_t)n - 1]) n--;
+                } else {
+                    int w = 0;
+                    for (int k = 0; k < n; k++) {
+                        if (gone[s][(size_t)k]) continue;
+                        l.x[(size_t)w] = l.x[(size_t)k]; l.y[(size_t)w] = l.y[(size_t)k];
+                        l.vx[(size_t)w] = l.vx[(size_t)k]; l.vy[(size_t)w] = l.vy[(size_t)k];
+                        l.vz[(size_t)w] = l.vz[(size_t)k];
+                        w++;
+                    }
+                    n = w;
+                }
+                l.x.resize((size_t)n); l.y.resize((size_t)n); l.vx.resize((size_t)n); l.vy.resize((size_t)n);
+                l.vz.resize((size_t)n);
+            }
+        });
+        for (int s = 0; s < NS; s++) {
+            Sp &q = sp[s];
+            std::vector<R> nx, ny, nvx, nvy, nvz;
+            for (int cell = 0; cell < C; cell++) {
+                const P5 &l = out[(size_t)cell][(size_t)s];
+                nx.insert(nx.end(), l.x.begin(), l.x.end()); ny.insert(ny.end(), l.y.begin(), l.y.end());
+                nvx.insert(nvx.end(), l.vx.begin(), l.vx.end()); nvy.insert(nvy.end(), l.vy.begin(), l.vy.end());
+                nvz.insert(nvz.end(), l.vz.begin(), l.vz.end());
+                q.cnt[cell] = (int)l.x.size();
+            }
+            q.x.swap(nx); q.y.swap(ny); q.vx.swap(nvx); q.vy.swap(nvy); q.vz.swap(nvz);
+            q.restart();
+        }
+    }
+
     void mcc(int64_t tstep) override {
+        if (c.gas == 2) {
+            mcc_aro2(tstep);
+            return;
+        }
         Sp &el = sp[0], &ion = sp[1];
         const uint32_t step = (uint32_t)tstep;
         std::vector<int> ecnt(C), icnt(C);

@@ -36,7 +36,7 @@ typedef struct or_case {
     const float *xsec;
     int n_logx, xw;
     float idlogx;
-    float sigv[8], th[16];
+    float sigv[32], th[96];
     const float *prob; /* [3*C] */
     const float *back_vel1;
     const float *vsave;
@@ -57,6 +57,10 @@ typedef struct or_case {
     const float *fs_V, *fs_Vt, *fs_W, *fs_Wt, *fs_inv;
     /* cell crossings per push: 0 one (reference), 1 until inside a cell */
     int move_mode;
+    /* reaction set (0 Ar, 2 Ar/O2) and what the oxygen sets need */
+    int gas, mcc_stride;
+    float dt_mcc, np2c[5];
+    const float *back_den1, *back_den2, *back_vel2, *fluid_den;
 } or_case;
 
 typedef struct or_sim or_sim;

@@ -28,7 +28,7 @@ class OrCase(C.Structure):
         ("sidx", _I), ("boundary", _I), ("face", _I), ("cond_id", _I), ("eps", _F), ("dep_factor", _F),
         ("Ascale", C.c_float * 5), ("q_density", C.c_float * 5), ("Escale", C.c_float * 5),
         ("xsec", _F), ("n_logx", C.c_int), ("xw", C.c_int), ("idlogx", C.c_float),
-        ("sigv", C.c_float * 8), ("th", C.c_float * 16), ("prob", _F), ("back_vel1", _F), ("vsave", _F),
+        ("sigv", C.c_float * 32), ("th", C.c_float * 96), ("prob", _F), ("back_vel1", _F), ("vsave", _F),
         ("nvel", C.c_int), ("mcc_n", C.c_int), ("seed", C.c_uint64),
         ("st", _F), ("st_sym", _F), ("row_scale", _F), ("lap", _F),
         ("src_num", C.c_int), ("src_mid", C.c_int * 8), ("efield_flag", C.c_int * 8),
@@ -39,6 +39,8 @@ class OrCase(C.Structure):
         ("fs_i0", C.c_int), ("fs_j0", C.c_int), ("fs_nx", C.c_int), ("fs_ny", C.c_int), ("fs_passes", C.c_int),
         ("fs_V", _F), ("fs_Vt", _F), ("fs_W", _F), ("fs_Wt", _F), ("fs_inv", _F),
         ("move_mode", C.c_int),
+        ("gas", C.c_int), ("mcc_stride", C.c_int), ("dt_mcc", C.c_float), ("np2c", C.c_float * 5),
+        ("back_den1", _F), ("back_den2", _F), ("back_vel2", _F), ("fluid_den", _F),
     ]
 
 
@@ -139,11 +141,21 @@ class Oracle:
         c.xw = self.keep["xsec"].size // c.n_logx
         c.idlogx = sc[15]
         sigv = t("sigv")
-        for k in range(min(8, sigv.size)):
+        for k in range(min(32, sigv.size)):
             c.sigv[k] = sigv[k]
         collf = t("collf").reshape(-1, 4)
-        for k in range(min(16, collf.shape[0])):
+        for k in range(min(96, collf.shape[0])):
             c.th[k] = collf[k, 2]
+        c.gas = info.main_gas
+        c.mcc_stride = info.mcc_stride
+        c.dt_mcc = sc[1]
+        for s in range(info.nsp):
+            c.np2c[s] = spc[s, 0]
+        if info.main_gas != 0:
+            c.back_den1 = keep("bd1", t("back_den1"), np.float32)
+            c.back_den2 = keep("bd2", t("back_den2"), np.float32)
+            c.back_vel2 = keep("bv2", t("back_vel2"), np.float32)
+            c.fluid_den = keep("fd", t("fluid_den"), np.float32)
         c.prob = keep("prob", t("prob"), np.float32)
         c.back_vel1 = keep("bv1", t("back_vel1"), np.float32)
         c.vsave = keep("vsave", t("vsave"), np.float32)
@@ -253,7 +265,7 @@ class Oracle:
 
     def counters(self):
         cc = np.zeros(max(1, self.info.nsp * self.info.cond_numr), np.float32)
-        mc = np.zeros(8 * self.info.Csize, np.uint32)
+        mc = np.zeros(self.info.mcc_stride * self.info.Csize, np.uint32)
         it = np.zeros(2, np.int32)
         lib().or_get_counters(self.h, _fp(cc), mc.ctypes.data_as(C.POINTER(C.c_uint)), _ip(it))
         return cc, mc, it
