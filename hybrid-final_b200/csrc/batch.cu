@@ -109,13 +109,12 @@ void batch_dev_free(BatchDev &b) {
 }
 
 hp_status run_step(const BatchDev &b, const LaunchCfg &lc, int gas, cudaStream_t st) {
-    if (gas == GAS_O2) return set_error("MCC for this gas is not built"), HP_ERR_UNSUPPORTED;
     CK(launch_advance(b.d_cases, b.n, st));
     const std::vector<PcgGroup> g = b.groups(lc.pcg_cluster_max, lc.pcg_block);
     CK(launch_field(b.d_cases, b.d_node, b.n, b.n_node, g.data(), (int)g.size(), &b.fast.plan, st));
     CK(launch_move(b.d_cases, b.d_part, b.n, b.n_part, lc, st));
     CK(launch_sort(b.d_cases, b.d_part, b.n, b.n_part, lc, st));
-    if (gas == GAS_ARO2) CK(launch_mcc_oxy(b.d_cases, b.d_cell, b.n, b.n_cell, gas, st));
+    if (gas != GAS_AR) CK(launch_mcc_oxy(b.d_cases, b.d_cell, b.n, b.n_cell, gas, st));
     else CK(launch_mcc_ar(b.d_cases, b.d_cell, b.n, b.n_cell, lc, st));
     CK(launch_deposit(b.d_cases, b.d_part, b.d_node, b.n, b.n_part, b.n_node, lc, st));
     CK(launch_accumulate(b.d_cases, b.d_node, b.n, b.n_node, st));

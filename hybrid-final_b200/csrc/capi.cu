@@ -332,6 +332,7 @@ hp_status build_device(hp_case *c) {
         h.mofm[k] = s.collf[k].mofM;
     }
     h.mcc_stride = s.main_gas == GAS_AR ? 8 : 72;
+    h.mcc_all_species = c->opts.o2_all_species ? 1 : 0;
     if (s.main_gas != GAS_AR) {
         TRY(dupload(c, (float **)&h.back_den1, s.back_den1));
         TRY(dupload(c, (float **)&h.back_den2, s.back_den2));
@@ -421,7 +422,7 @@ hp_status op_sort(hp_case *c, cudaStream_t st) {
     return e == cudaSuccess ? HP_OK : cuda_fail(e, "sort");
 }
 hp_status op_mcc(hp_case *c, cudaStream_t st) {
-    if (c->s.main_gas == GAS_ARO2) {
+    if (c->s.main_gas == GAS_ARO2 || c->s.main_gas == GAS_O2) {
         cudaError_t e = launch_mcc_oxy(c->d_case, c->d_items + 2, 1, c->s.Csize, c->s.main_gas, st);
         return e == cudaSuccess ? HP_OK : cuda_fail(e, "mcc");
     }
@@ -666,7 +667,6 @@ hp_status hp_case_create(const char *deck, size_t len, const hp_case_opts *opts,
     } catch (const std::exception &e) {
         return from_exception(e);
     }
-    if (s.main_gas == GAS_O2) return set_error("MCC for this gas is not built"), HP_ERR_UNSUPPORTED;
     return case_from(std::move(s), &o, out);
 }
 
@@ -680,7 +680,6 @@ hp_status hp_case_create_from_setup(const hp_setup *su, const hp_case_opts *opts
 
 namespace hpi {
 hp_status case_from_setup_owned(hp::Setup &&s, const hp_case_opts &o, hp_case **out) {
-    if (s.main_gas == GAS_O2) return set_error("MCC for this gas is not built"), HP_ERR_UNSUPPORTED;
     hp_status st = case_from(std::move(s), &o, out);
     if (st != HP_OK) return st;
     // the initial load now lives on the device

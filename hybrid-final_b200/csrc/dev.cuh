@@ -74,6 +74,7 @@ struct DevCase {
     float th[96];                   // CollF.Th_e per reaction channel
     float mofm[96];
     int mcc_stride;                 // counters per cell in mcc_count (8 for Ar, 72 for the oxygen sets)
+    int mcc_all_species;            // O2 set: 0 electrons only (the reference's launch), 1 every species
     const float *prob;              // [3*C]: electron P1, P2; ion P (Ar)
     const float *back_vel1;         // [G]
     const float *back_den1, *back_den2, *back_vel2; // [G] (oxygen sets)

@@ -1,7 +1,8 @@
 // mcc_oxy.cu -- null-collision MCC of the Ar/O2 reaction set (5 species:
-// e, Ar+, O2+, O+, O-), one warp per cell (MCC_ArO2_Basic,
-// src/cuda_mcc.cu:21-71; ArO2_Collision_Check and the species handlers,
-// src/cuda_mccArO2.cu:51-1265).
+// e, Ar+, O2+, O+, O-) and of the O2 set (4 species: e, O2+, O+, O-), one
+// warp per cell (MCC_ArO2_Basic and MCC_O2_Basic, src/cuda_mcc.cu:21-96;
+// the collision checks and species handlers of src/cuda_mccArO2.cu:51-1265
+// and src/cuda_mccO2.cu:2-977).
 //
 // The reference runs one thread per (species, node) with the species
 // handlers concurrently: a handler that creates or deletes particles of
@@ -81,6 +82,31 @@ __constant__ Rung c_erung[] = {
 };
 __constant__ int c_erung_start[10] = {0, 4, 5, 19, 27, 35, 36, 37, 44, 46};
 
+// the O2 set's electron ladders (src/cuda_mccO2.cu:2-429)
+__constant__ Rung c_orung[] = {
+    // 0: e + O2
+    {0, A_ELASTIC, 0, 0, 0}, {1, A_LOSS, 1, 0, 0}, {2, A_LOSS, 2, 0, 0}, {3, A_LOSS, 3, 0, 0},
+    {4, A_LOSS, 4, 0, 0}, {5, A_LOSS, 5, 0, 0}, {6, A_ATTACH, 0, 0, 0}, {7, A_LOSS, 7, 0, 0},
+    {8, A_LOSS, 8, 0, 0}, {9, A_LOSS, 9, 0, 0}, {10, A_IONIZE, 0, 1, 0}, {11, A_LOSS, 11, 0, 0},
+    {12, A_IONIZE, 2, 3, 0}, {13, A_IONIZE, 0, 2, 0},
+    // 1: e + O2(a)
+    {14, A_IONIZE, 0, 1, 0}, {15, A_ATTACH, 0, 0, 0}, {16, A_GAIN, 0, 0, 0.977f}, {17, A_GAIN, 0, 0, 0.977f},
+    {18, A_LOSS, 18, 0, 0}, {19, A_LOSS, 19, 0, 0}, {20, A_LOSS, 20, 0, 0}, {21, A_IONIZE, 0, 2, 0},
+    // 2: e + O2(b)
+    {22, A_IONIZE, 0, 1, 0}, {23, A_ATTACH, 0, 0, 0}, {24, A_GAIN, 0, 0, 1.627f}, {25, A_GAIN, 0, 0, 1.627f},
+    {26, A_LOSS, 26, 0, 0}, {27, A_LOSS, 27, 0, 0}, {28, A_LOSS, 28, 0, 0}, {29, A_IONIZE, 0, 2, 0},
+    // 3: e + O-
+    {30, A_DETACH, 0, 0, 0},
+    // 4: e + O2+
+    {31, A_RECOMB, 0, 0, 0},
+    // 5: e + O(3P)
+    {32, A_LOSS, 32, 0, 0}, {33, A_LOSS, 33, 0, 0}, {34, A_LOSS, 34, 0, 0}, {35, A_LOSS, 35, 0, 0},
+    {36, A_LOSS, 36, 0, 0}, {37, A_IONIZE, 0, 2, 0}, {38, A_LOSS, 38, 0, 0},
+    // 6: e + O(1D)
+    {39, A_IONIZE, 0, 2, 0}, {40, A_GAIN, 0, 0, 1.96f},
+};
+__constant__ int c_orung_start[8] = {0, 14, 22, 30, 31, 32, 39, 41};
+
 // collision probabilities of one cell (cumulative over the targets) from the
 // node's background, fluid and charged densities (ArO2_Collision_Check,
 // src/cuda_mccArO2.cu:1130-1190).  The electron sums run in float with 1.0f,
@@ -150,6 +176,55 @@ __device__ void cell_prob(const DevCase &d, int node, CellProb &P) {
     P.n[4] = 5;
 }
 
+// the O2 set (O2Collision_Check, src/cuda_mccO2.cu:867-911): species e,
+// O2+, O+, O-; the O2+ line uses the electron sub-step, as the reference does
+__device__ void cell_prob_o2(const DevCase &d, int node, CellProb &P) {
+    const int G = d.G;
+    const float bd1 = d.back_den1[node];
+    const float F0 = d.fluid_den[node], F1 = d.fluid_den[G + node], F2 = d.fluid_den[2 * G + node];
+    const float F3 = d.fluid_den[3 * G + node];
+    auto nq = [&](int s, float sig, float dtx) {
+        float t = -1 * dtx;
+        t = t * sig;
+        t = t * (float)d.den[(size_t)s * G + node];
+        t = t * d.sp[s].np2c;
+        t = t * d.idx;
+        t = t * d.idy;
+        return hp_expf(t);
+    };
+    const float dtm = d.dt_mcc, dt = d.dt;
+    const float *sv = d.sigv;
+    float *e = P.p[0];
+    e[0] = 1.0f - xe(dtm, sv[0], bd1);
+    e[1] = e[0] + 1.0f - xe(dtm, sv[1], F0);
+    e[2] = e[1] + 1.0f - xe(dtm, sv[2], F1);
+    e[3] = e[2] + 1.0f - nq(3, sv[3], dtm);
+    e[4] = e[3] + 1.0f - nq(1, sv[4], dtm);
+    e[5] = e[4] + 1.0f - xe(dtm, sv[5], F2);
+    e[6] = e[5] + 1.0f - xe(dtm, sv[6], F3);
+    P.n[0] = 7;
+    float *a = P.p[1]; // O2+: OP, O2, O2A, O2B
+    a[0] = ion_acc(0, true, xe(dtm, sv[12], F2));
+    a[1] = ion_acc(a[0], false, xe(dtm, sv[13], bd1));
+    a[2] = ion_acc(a[1], false, xe(dtm, sv[14], F0));
+    a[3] = ion_acc(a[2], false, xe(dtm, sv[15], F1));
+    P.n[1] = 4;
+    float *b = P.p[2]; // O+: O2, OP, O2A, O2B
+    b[0] = ion_acc(0, true, xe(dt, sv[16], bd1));
+    b[1] = ion_acc(b[0], false, xe(dt, sv[17], F2));
+    b[2] = ion_acc(b[1], false, xe(dt, sv[18], F0));
+    b[3] = ion_acc(b[2], false, xe(dt, sv[19], F1));
+    P.n[2] = 4;
+    float *m = P.p[3]; // O-: O2, OP, O2+, O+, O2A
+    m[0] = ion_acc(0, true, xe(dt, sv[7], bd1));
+    m[1] = ion_acc(m[0], false, xe(dt, sv[8], F2));
+    m[2] = ion_acc(m[1], false, nq(1, sv[9], dt));
+    m[3] = ion_acc(m[2], false, nq(2, sv[10], dt));
+    m[4] = ion_acc(m[3], false, xe(dt, sv[11], F0));
+    P.n[3] = 5;
+    P.n[4] = 1;
+}
+
 // target of a hit: the first cumulative probability R1 does not exceed
 __device__ __forceinline__ int target_of(const CellProb &P, int s, float R1) {
     const int n = P.n[s];
@@ -181,9 +256,16 @@ __device__ __forceinline__ void no_birth(Outcome &o) {
     o.ch = -1;
 }
 
-// ArO2_Electron (src/cuda_mccArO2.cu:51-560), one collider with target t
+// ArO2_Electron (src/cuda_mccArO2.cu:51-560) and O2_Electron
+// (src/cuda_mccO2.cu:2-429), one collider with target t.  The two differ in
+// how R1 is scaled (R1 *= sigma_v/v vs R1 = U sigma_v / v) and in ionisation:
+// the Ar/O2 set splits the energy with 10 tan(U atan(E/20)) and scatters the
+// new electron, the O2 set gives the new electron the primary's unit
+// direction as its velocity.
+template <int GAS>
 __device__ void electron_collide(const DevCase &d, float vx, float vy, float vz, int t, float bv1, hp_stream &rs,
                                  Outcome &o) {
+    constexpr int OMINUS = GAS == 2 ? 4 : 3;
     no_birth(o);
     const float Esc = d.sp[0].Escale;
     float VX = vx, VY = vy, VZ = vz;
@@ -193,12 +275,20 @@ __device__ void electron_collide(const DevCase &d, float vx, float vy, float vz,
     float engy = Esc * dum;
     int colltype = 1, i1 = 0, i2 = 0;
     float rengy = 0.f, vel2 = 0.f;
-    float R1 = hp_stream_next(&rs);
-    R1 *= d.sigv[t] / vel;
+    float R1;
+    if (GAS == 2) {
+        R1 = hp_stream_next(&rs);
+        R1 *= d.sigv[t] / vel;
+    } else {
+        R1 = hp_stream_next(&rs) * d.sigv[t] / vel;
+    }
+    const Rung *rung = GAS == 2 ? c_erung : c_orung;
+    const int k0 = GAS == 2 ? c_erung_start[t] : c_orung_start[t];
+    const int k1 = GAS == 2 ? c_erung_start[t + 1] : c_orung_start[t + 1];
     float sum = 0.f;
     bool hit = false;
-    for (int k = c_erung_start[t]; k < c_erung_start[t + 1]; k++) {
-        const Rung r = c_erung[k];
+    for (int k = k0; k < k1; k++) {
+        const Rung r = rung[k];
         if (!(engy > d.th[r.ch])) continue;
         sum = sum + xsec_lookup(d, r.ch, engy);
         if (!(R1 <= sum)) continue;
@@ -224,11 +314,15 @@ __device__ void electron_collide(const DevCase &d, float vx, float vy, float vz,
         default: { // A_IONIZE
             colltype = 3;
             engy -= d.th[r.ch];
-            const float u = hp_stream_next(&rs);
-            rengy = (float)(10.0 * (double)hp_tanf_q1(u * hp_atanf((float)(engy / 20.0))));
-            engy -= rengy;
-            vel = sqrtf(fabsf(rengy) / Esc);
-            vel2 = sqrtf(fabsf(engy) / Esc);
+            if (GAS == 2) {
+                const float u = hp_stream_next(&rs);
+                rengy = (float)(10.0 * (double)hp_tanf_q1(u * hp_atanf((float)(engy / 20.0))));
+                engy -= rengy;
+                vel = sqrtf(fabsf(rengy) / Esc);
+                vel2 = sqrtf(fabsf(engy) / Esc);
+            } else {
+                vel = sqrtf(fabsf(engy) / Esc);
+            }
             i1 = r.a1;
             i2 = r.a2;
             break;
@@ -247,11 +341,11 @@ __device__ void electron_collide(const DevCase &d, float vx, float vy, float vz,
         o.vx = VX; o.vy = VY; o.vz = VZ;
         break;
     }
-    case 2: { // attachment: the electron becomes an O- at rest in the neutral frame
+    case 2: { // attachment: the electron becomes an O- with a neutral's thermal velocity
         o.keep = false;
         const int n = (int)((d.nvel - 1) * hp_stream_next(&rs));
         const float a = hp_stream_next(&rs), b = hp_stream_next(&rs);
-        o.b[0].sp = 4;
+        o.b[0].sp = OMINUS;
         maxwellv_dev(o.b[0].vx, o.b[0].vy, o.b[0].vz, d.vsave[n], bv1, a, b);
         break;
     }
@@ -262,8 +356,10 @@ __device__ void electron_collide(const DevCase &d, float vx, float vy, float vz,
             b.sp = isp[q];
             if (isp[q] == 0) {
                 b.vx = VX; b.vy = VY; b.vz = VZ;
-                const float a = hp_stream_next(&rs), c = hp_stream_next(&rs);
-                anewvel_dev(rengy, vel, b.vx, b.vy, b.vz, a, c);
+                if (GAS == 2) {
+                    const float a = hp_stream_next(&rs), c = hp_stream_next(&rs);
+                    anewvel_dev(rengy, vel, b.vx, b.vy, b.vz, a, c);
+                }
             } else {
                 const int n = (int)((d.nvel - 1) * hp_stream_next(&rs));
                 const float a = hp_stream_next(&rs), c = hp_stream_next(&rs);
@@ -271,7 +367,7 @@ __device__ void electron_collide(const DevCase &d, float vx, float vy, float vz,
             }
         }
         const float a = hp_stream_next(&rs), b = hp_stream_next(&rs);
-        anewvel_dev(engy, vel2, VX, VY, VZ, a, b);
+        anewvel_dev(engy, GAS == 2 ? vel2 : vel, VX, VY, VZ, a, b);
         o.vx = VX; o.vy = VY; o.vz = VZ;
         break;
     }
@@ -290,24 +386,29 @@ __device__ void electron_collide(const DevCase &d, float vx, float vy, float vz,
 }
 
 // ArO2_Ar_ion / _O2_ion / _O_ion / _O_negative (src/cuda_mccArO2.cu:561-1129)
+// and O2_O2_ion / _O_ion / _O_negative (src/cuda_mccO2.cu:430-866)
 enum : int { I_NULL, I_SCAT, I_CX, I_TO_OP, I_TO_ARP, I_TO_O2P, I_DETACH, I_RECOMB };
 
+template <int GAS>
 __device__ void ion_collide(const DevCase &d, int s, float vx, float vy, float vz, int t, float bv1, float bv2,
                             hp_stream &rs, Outcome &o) {
+    constexpr int OMINUS = GAS == 2 ? 4 : 3, O2P = GAS == 2 ? 2 : 1, OP = GAS == 2 ? 3 : 2;
     no_birth(o);
     o.keep = true;
     o.vx = vx; o.vy = vy; o.vz = vz;
     const float Esc = d.sp[s].Escale;
     float vnx = 0.f, vny = 0.f, vnz = 0.f;
     float VX, VY, VZ, vel, engy;
-    if (s == 4) { // O-: no neutral velocity; the direction is normalised
+    if (s == OMINUS) { // O-: no neutral velocity; the direction is normalised
         VX = vx; VY = vy; VZ = vz;
         const float dum = VX * VX + VY * VY + VZ * VZ;
         vel = sqrtf(dum);
         VX /= vel; VY /= vel; VZ /= vel;
         engy = Esc * dum;
     } else {
-        const float vneut = s == 1 ? (t == 0 ? bv1 : bv2) : (s == 2 ? bv1 : bv2);
+        float vneut;
+        if (GAS == 2) vneut = s == 1 ? (t == 0 ? bv1 : bv2) : (s == 2 ? bv1 : bv2);
+        else vneut = bv1;
         const int n = (int)((d.nvel - 1) * hp_stream_next(&rs));
         const float a = hp_stream_next(&rs), b = hp_stream_next(&rs);
         maxwellv_dev(vnx, vny, vnz, d.vsave[n], vneut, a, b);
@@ -315,39 +416,64 @@ __device__ void ion_collide(const DevCase &d, int s, float vx, float vy, float v
         const float dum = VX * VX + VY * VY + VZ * VZ;
         vel = sqrtf(dum);
         engy = Esc * dum;
-        if (s == 1) (void)hp_stream_next(&rs); // the reference draws R1 and overwrites it
+        if (GAS == 2 && s == 1) (void)hp_stream_next(&rs); // the reference draws R1 and overwrites it
     }
     // (sigma-v index, channels, actions, cumulative second rung)
     int sv = 0, nr = 0, ch[3] = {0, 0, 0}, act[3] = {0, 0, 0};
     bool cum = false;
-    switch (s) {
-    case 1:
-        sv = 23 + t;
-        if (t == 0) { nr = 2; ch[0] = 65; act[0] = I_CX; ch[1] = 66; act[1] = I_SCAT; }
-        else { nr = 1; ch[0] = 67; act[0] = I_SCAT; }
-        break;
-    case 2:
-        sv = 14 + t;
-        if (t == 0) { nr = 1; ch[0] = 52; act[0] = I_TO_OP; }
-        else if (t == 1) { nr = 3; ch[0] = 53; act[0] = I_CX; ch[1] = 54; act[1] = I_SCAT; ch[2] = 55; act[2] = I_TO_OP; }
-        else if (t == 2) { nr = 1; ch[0] = 56; act[0] = I_CX; }
-        else if (t == 3) { nr = 1; ch[0] = 57; act[0] = I_CX; }
-        else { nr = 2; ch[0] = 58; act[0] = I_TO_ARP; ch[1] = 59; act[1] = I_CX; }
-        break;
-    case 3:
-        sv = 19 + t;
-        if (t == 0) { nr = 2; ch[0] = 60; act[0] = I_TO_O2P; ch[1] = 61; act[1] = I_SCAT; }
-        else if (t == 1) { nr = 1; ch[0] = 62; act[0] = I_CX; }
-        else { nr = 1; ch[0] = 62 + t - 1; act[0] = I_TO_O2P; }
-        break;
-    default: // O-
-        sv = 9 + t;
-        if (t == 0) { nr = 2; ch[0] = 46; act[0] = I_SCAT; ch[1] = 47; act[1] = I_DETACH; cum = true; }
-        else if (t == 1) { nr = 1; ch[0] = 48; act[0] = I_DETACH; }
-        else if (t == 2) { nr = 1; ch[0] = 49; act[0] = I_RECOMB; }
-        else if (t == 3) { nr = 1; ch[0] = 50; act[0] = I_RECOMB; }
-        else { nr = 1; ch[0] = 51; act[0] = I_DETACH; }
-        break;
+    if (GAS == 2) {
+        switch (s) {
+        case 1:
+            sv = 23 + t;
+            if (t == 0) { nr = 2; ch[0] = 65; act[0] = I_CX; ch[1] = 66; act[1] = I_SCAT; }
+            else { nr = 1; ch[0] = 67; act[0] = I_SCAT; }
+            break;
+        case 2:
+            sv = 14 + t;
+            if (t == 0) { nr = 1; ch[0] = 52; act[0] = I_TO_OP; }
+            else if (t == 1) { nr = 3; ch[0] = 53; act[0] = I_CX; ch[1] = 54; act[1] = I_SCAT; ch[2] = 55; act[2] = I_TO_OP; }
+            else if (t == 2) { nr = 1; ch[0] = 56; act[0] = I_CX; }
+            else if (t == 3) { nr = 1; ch[0] = 57; act[0] = I_CX; }
+            else { nr = 2; ch[0] = 58; act[0] = I_TO_ARP; ch[1] = 59; act[1] = I_CX; }
+            break;
+        case 3:
+            sv = 19 + t;
+            if (t == 0) { nr = 2; ch[0] = 60; act[0] = I_TO_O2P; ch[1] = 61; act[1] = I_SCAT; }
+            else if (t == 1) { nr = 1; ch[0] = 62; act[0] = I_CX; }
+            else { nr = 1; ch[0] = 61 + t; act[0] = I_TO_O2P; }
+            break;
+        default: // O-
+            sv = 9 + t;
+            if (t == 0) { nr = 2; ch[0] = 46; act[0] = I_SCAT; ch[1] = 47; act[1] = I_DETACH; cum = true; }
+            else if (t == 1) { nr = 1; ch[0] = 48; act[0] = I_DETACH; }
+            else if (t == 2) { nr = 1; ch[0] = 49; act[0] = I_RECOMB; }
+            else if (t == 3) { nr = 1; ch[0] = 50; act[0] = I_RECOMB; }
+            else { nr = 1; ch[0] = 51; act[0] = I_DETACH; }
+            break;
+        }
+    } else {
+        switch (s) {
+        case 1: // O2+
+            sv = 12 + t;
+            if (t == 0) { nr = 1; ch[0] = 47; act[0] = I_TO_OP; }
+            else if (t == 1) { nr = 3; ch[0] = 48; act[0] = I_CX; ch[1] = 49; act[1] = I_SCAT; ch[2] = 50; act[2] = I_TO_OP; }
+            else { nr = 1; ch[0] = 49 + t; act[0] = I_CX; }
+            break;
+        case 2: // O+
+            sv = 16 + t;
+            if (t == 0) { nr = 2; ch[0] = 53; act[0] = I_TO_O2P; ch[1] = 54; act[1] = I_SCAT; }
+            else if (t == 1) { nr = 1; ch[0] = 55; act[0] = I_CX; }
+            else { nr = 1; ch[0] = 54 + t; act[0] = I_TO_O2P; }
+            break;
+        default: // O-: the handler scales R1 by sigma_v 9..13 (the check used 7..11)
+            sv = 9 + t;
+            if (t == 0) { nr = 2; ch[0] = 41; act[0] = I_SCAT; ch[1] = 42; act[1] = I_DETACH; cum = true; }
+            else if (t == 1) { nr = 1; ch[0] = 43; act[0] = I_DETACH; }
+            else if (t == 2) { nr = 1; ch[0] = 44; act[0] = I_RECOMB; }
+            else if (t == 3) { nr = 1; ch[0] = 45; act[0] = I_RECOMB; }
+            else { nr = 1; ch[0] = 46; act[0] = I_DETACH; }
+            break;
+        }
     }
     const float R1 = hp_stream_next(&rs) * d.sigv[sv] / vel;
     int what = I_NULL;
@@ -367,14 +493,14 @@ __device__ void ion_collide(const DevCase &d, int s, float vx, float vy, float v
     case I_SCAT: {
         const float a = hp_stream_next(&rs), b = hp_stream_next(&rs);
         newvel_ionsc_dev(VX, VY, VZ, vel, a, b);
-        if (s == 4) { o.vx = VX; o.vy = VY; o.vz = VZ; }
+        if (s == OMINUS) { o.vx = VX; o.vy = VY; o.vz = VZ; }
         else { o.vx = VX + vnx; o.vy = VY + vny; o.vz = VZ + vnz; }
         break;
     }
     case I_CX: o.vx = vnx; o.vy = vny; o.vz = vnz; break;
-    case I_TO_OP: o.keep = false; o.b[0] = Born{3, vnx, vny, vnz}; break;
+    case I_TO_OP: o.keep = false; o.b[0] = Born{OP, vnx, vny, vnz}; break;
     case I_TO_ARP: o.keep = false; o.b[0] = Born{1, vnx, vny, vnz}; break;
-    case I_TO_O2P: o.keep = false; o.b[0] = Born{2, vnx, vny, vnz}; break;
+    case I_TO_O2P: o.keep = false; o.b[0] = Born{O2P, vnx, vny, vnz}; break;
     case I_DETACH: o.keep = false; o.b[0] = Born{0, VX, VY, VZ}; break;
     default: o.keep = false; break; // I_RECOMB
     }
@@ -382,8 +508,11 @@ __device__ void ion_collide(const DevCase &d, int s, float vx, float vy, float v
 
 __device__ __forceinline__ bool is_hole(float x) { return x != x; }
 
-__global__ void __launch_bounds__(OXY_TPB) k_mcc_aro2(const DevCase *__restrict__ cases,
-                                                      const int *__restrict__ item_start, int ncases, int items) {
+template <int GAS>
+__global__ void __launch_bounds__(OXY_TPB) k_mcc_oxy(const DevCase *__restrict__ cases,
+                                                     const int *__restrict__ item_start, int ncases, int items) {
+    constexpr int NSP = GAS == 2 ? 5 : 4;
+    constexpr int OMINUS = GAS == 2 ? 4 : 3;
     __shared__ int ring_s[OXY_TPB / 32][OXY_RING];
     __shared__ int holes_s[OXY_TPB / 32][NSP_ARO2][HOLE_CAP];
     const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
@@ -399,10 +528,14 @@ __global__ void __launch_bounds__(OXY_TPB) k_mcc_aro2(const DevCase *__restrict_
     const float bv1 = d.back_vel1[node], bv2 = d.back_vel2[node];
     const unsigned lt = lanemask_lt();
     CellProb P;
-    cell_prob(d, node, P);
+    if (GAS == 2) cell_prob(d, node, P);
+    else cell_prob_o2(d, node, P);
+    // the reference's O2 launch covers Gsize threads, so only its electrons
+    // collide (src/cuda_mcc.cu:76-77); mcc_all_species extends it to every species
+    const int nactive = (GAS == 2 || d.mcc_all_species) ? NSP : 1;
     int n0[NSP_ARO2], cnt[NSP_ARO2], nh[NSP_ARO2];
 #pragma unroll
-    for (int s = 0; s < NSP_ARO2; s++) {
+    for (int s = 0; s < NSP; s++) {
         n0[s] = d.sp[s].cnt[c];
         cnt[s] = n0[s];
         nh[s] = 0;
@@ -415,11 +548,11 @@ __global__ void __launch_bounds__(OXY_TPB) k_mcc_aro2(const DevCase *__restrict_
         nh[s]++;
     };
 #pragma unroll 1
-    for (int s = 0; s < NSP_ARO2; s++) {
+    for (int s = 0; s < nactive; s++) {
         const DevSpecies &sp = d.sp[s];
         const size_t base = (size_t)c * sp.cap;
         const int n = n0[s];
-        const int nsub = s == 0 ? d.mcc_n : 1;
+        const int nsub = (s == 0 || (GAS == 1 && s == 1)) ? d.mcc_n : 1; // O2: O2+ sub-cycles too
         const float Tprob = P.p[s][P.n[s] - 1];
         int head = 0, tail = 0;
         for (int k0 = 0; k0 < n || tail > head; k0 += 128) {
@@ -471,8 +604,8 @@ __global__ void __launch_bounds__(OXY_TPB) k_mcc_aro2(const DevCase *__restrict_
                         const float vx = sp.vx[base + k], vy = sp.vy[base + k], vz = sp.vz[base + k];
                         hp_stream rs;
                         hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, (uint32_t)s);
-                        if (s == 0) electron_collide(d, vx, vy, vz, t, bv1, rs, o);
-                        else ion_collide(d, s, vx, vy, vz, t, bv1, bv2, rs, o);
+                        if (s == 0) electron_collide<GAS>(d, vx, vy, vz, t, bv1, rs, o);
+                        else ion_collide<GAS>(d, s, vx, vy, vz, t, bv1, bv2, rs, o);
                         if (o.ch >= 0) atomicAdd(&mcount[o.ch], 1u);
                         if (o.keep) {
                             sp.vx[base + k] = o.vx;
@@ -492,7 +625,7 @@ __global__ void __launch_bounds__(OXY_TPB) k_mcc_aro2(const DevCase *__restrict_
                 // births, per species in lane (= collider) order; a collider's
                 // two births, if any, go to two different species
 #pragma unroll 1
-                for (int t = 0; t < NSP_ARO2; t++) {
+                for (int t = 0; t < NSP; t++) {
                     const int q = (active && o.b[0].sp == t) ? 0 : (active && o.b[1].sp == t) ? 1 : -1;
                     const unsigned bm = __ballot_sync(FULL, q >= 0);
                     if (!bm) continue;
@@ -518,19 +651,19 @@ __global__ void __launch_bounds__(OXY_TPB) k_mcc_aro2(const DevCase *__restrict_
                 for (unsigned m = bk; m; m &= m - 1) {
                     const int src = __ffs(m) - 1;
                     const float r2 = __shfl_sync(FULL, o.r2, src);
-                    const DevSpecies &om = d.sp[4];
+                    const DevSpecies &om = d.sp[OMINUS];
                     const size_t ob = (size_t)c * om.cap;
                     int victim = -1;
                     if (lane == 0) {
                         int nlive = 0;
-                        for (int q = 0; q < n0[4]; q++) nlive += is_hole(om.x[ob + q]) ? 0 : 1;
+                        for (int q = 0; q < n0[OMINUS]; q++) nlive += is_hole(om.x[ob + q]) ? 0 : 1;
                         if (nlive > 0) {
                             int pick = 0;
                             if (nlive > 1) {
                                 pick = (int)((float)nlive * r2);
                                 if (pick > nlive - 1) pick = nlive - 1;
                             }
-                            for (int q = 0; q < n0[4]; q++) {
+                            for (int q = 0; q < n0[OMINUS]; q++) {
                                 if (is_hole(om.x[ob + q])) continue;
                                 if (pick-- == 0) { victim = q; break; }
                             }
@@ -539,7 +672,7 @@ __global__ void __launch_bounds__(OXY_TPB) k_mcc_aro2(const DevCase *__restrict_
                     }
                     victim = __shfl_sync(FULL, victim, 0);
                     __syncwarp();
-                    if (victim >= 0) add_hole(4, victim);
+                    if (victim >= 0) add_hole(OMINUS, victim);
                 }
                 head = min(head + 32, tail);
                 __syncwarp();
@@ -548,7 +681,7 @@ __global__ void __launch_bounds__(OXY_TPB) k_mcc_aro2(const DevCase *__restrict_
     }
     // fill every species' holes with its last particles
 #pragma unroll 1
-    for (int s = 0; s < NSP_ARO2; s++) {
+    for (int s = 0; s < NSP; s++) {
         const DevSpecies &sp = d.sp[s];
         const size_t base = (size_t)c * sp.cap;
         int n = cnt[s];
@@ -608,9 +741,10 @@ __global__ void __launch_bounds__(OXY_TPB) k_mcc_aro2(const DevCase *__restrict_
 cudaError_t launch_mcc_oxy(const DevCase *cases, const int *item_start, int ncases, int items, int gas,
                            cudaStream_t st) {
     if (items <= 0) return cudaSuccess;
-    if (gas != 2) return cudaErrorNotSupported;
-    k_mcc_aro2<<<(unsigned)((items * 32LL + OXY_TPB - 1) / OXY_TPB), OXY_TPB, 0, st>>>(cases, item_start, ncases,
-                                                                                          items);
+    const unsigned nb = (unsigned)((items * 32LL + OXY_TPB - 1) / OXY_TPB);
+    if (gas == 2) k_mcc_oxy<2><<<nb, OXY_TPB, 0, st>>>(cases, item_start, ncases, items);
+    else if (gas == 1) k_mcc_oxy<1><<<nb, OXY_TPB, 0, st>>>(cases, item_start, ncases, items);
+    else return cudaErrorNotSupported;
     return cudaGetLastError();
 }
 

@@ -110,10 +110,7 @@ void worker_main(hp_server *s) {
         std::string msg;
         try {
             hp::build_setup(r->deck.data(), r->deck.size(), b, r->setup);
-            if (r->setup.main_gas == hp::GAS_O2) {
-                err = HP_ERR_UNSUPPORTED;
-                msg = "MCC for this gas is not built";
-            }
+
         } catch (const std::exception &e) {
             msg = e.what();
             err = msg.rfind("unsupported", 0) == 0 ? HP_ERR_UNSUPPORTED : HP_ERR_DECK;

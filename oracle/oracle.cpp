@@ -517,6 +517,25 @@ template <class R> struct Sim : SimBase {
             {44, IO, 0, 3, 0}, {45, GA, 0, 0, 1.96f},
         };
         static const int start[10] = {0, 4, 5, 19, 27, 35, 36, 37, 44, 46};
+        // the O2 set (src/cuda_mccO2.cu:2-429)
+        static const Rg rgo[] = {
+            {0, EL, 0, 0, 0}, {1, LO, 1, 0, 0}, {2, LO, 2, 0, 0}, {3, LO, 3, 0, 0}, {4, LO, 4, 0, 0},
+            {5, LO, 5, 0, 0}, {6, AT, 0, 0, 0}, {7, LO, 7, 0, 0}, {8, LO, 8, 0, 0}, {9, LO, 9, 0, 0},
+            {10, IO, 0, 1, 0}, {11, LO, 11, 0, 0}, {12, IO, 2, 3, 0}, {13, IO, 0, 2, 0},
+            {14, IO, 0, 1, 0}, {15, AT, 0, 0, 0}, {16, GA, 0, 0, 0.977f}, {17, GA, 0, 0, 0.977f},
+            {18, LO, 18, 0, 0}, {19, LO, 19, 0, 0}, {20, LO, 20, 0, 0}, {21, IO, 0, 2, 0},
+            {22, IO, 0, 1, 0}, {23, AT, 0, 0, 0}, {24, GA, 0, 0, 1.627f}, {25, GA, 0, 0, 1.627f},
+            {26, LO, 26, 0, 0}, {27, LO, 27, 0, 0}, {28, LO, 28, 0, 0}, {29, IO, 0, 2, 0},
+            {30, DE, 0, 0, 0},
+            {31, RE, 0, 0, 0},
+            {32, LO, 32, 0, 0}, {33, LO, 33, 0, 0}, {34, LO, 34, 0, 0}, {35, LO, 35, 0, 0}, {36, LO, 36, 0, 0},
+            {37, IO, 0, 2, 0}, {38, LO, 38, 0, 0},
+            {39, IO, 0, 2, 0}, {40, GA, 0, 0, 1.96f},
+        };
+        static const int starto[8] = {0, 14, 22, 30, 31, 32, 39, 41};
+        const bool aro2 = c.gas == 2;
+        const Rg *ladder = aro2 ? rg : rgo;
+        const int *lstart = aro2 ? start : starto;
         const R Esc = (R)c.Escale[0];
         R VX = vx, VY = vy, VZ = vz;
         const R dum = VX * VX + VY * VY + VZ * VZ;
@@ -525,12 +544,17 @@ template <class R> struct Sim : SimBase {
         R engy = Esc * dum;
         int colltype = 1, i1 = 0, i2 = 0;
         R rengy = 0, vel2 = 0;
-        R R1 = (R)hp_stream_next(&rs);
-        R1 *= (R)c.sigv[t] / vel;
+        R R1;
+        if (aro2) {
+            R1 = (R)hp_stream_next(&rs);
+            R1 *= (R)c.sigv[t] / vel;
+        } else {
+            R1 = (R)hp_stream_next(&rs) * (R)c.sigv[t] / vel;
+        }
         R sum = 0;
         bool hit = false;
-        for (int k = start[t]; k < start[t + 1]; k++) {
-            const Rg &r = rg[k];
+        for (int k = lstart[t]; k < lstart[t + 1]; k++) {
+            const Rg &r = ladder[k];
             if (!(engy > (R)c.th[r.ch])) continue;
             sum = sum + xsec(r.ch, engy);
             if (!(R1 <= sum)) continue;
@@ -550,11 +574,15 @@ template <class R> struct Sim : SimBase {
             default: {
                 colltype = 3;
                 engy -= (R)c.th[r.ch];
-                const R u = (R)hp_stream_next(&rs);
-                rengy = (R)(10.0 * (double)m_tan(u * m_atan((R)(engy / 20.0))));
-                engy -= rengy;
-                vel = std::sqrt(std::fabs(rengy) / Esc);
-                vel2 = std::sqrt(std::fabs(engy) / Esc);
+                if (aro2) {
+                    const R u = (R)hp_stream_next(&rs);
+                    rengy = (R)(10.0 * (double)m_tan(u * m_atan((R)(engy / 20.0))));
+                    engy -= rengy;
+                    vel = std::sqrt(std::fabs(rengy) / Esc);
+                    vel2 = std::sqrt(std::fabs(engy) / Esc);
+                } else {
+                    vel = std::sqrt(std::fabs(engy) / Esc);
+                }
                 i1 = r.a1;
                 i2 = r.a2;
                 break;
@@ -577,7 +605,7 @@ template <class R> struct Sim : SimBase {
             o.keep = false;
             const int n = (int)((c.nvel - 1) * hp_stream_next(&rs));
             const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
-            o.bsp[0] = 4;
+            o.bsp[0] = aro2 ? 4 : 3;
             maxwellv(o.bv[0][0], o.bv[0][1], o.bv[0][2], (R)c.vsave[n], bv1, a, b);
             break;
         }
@@ -587,8 +615,10 @@ template <class R> struct Sim : SimBase {
                 o.bsp[q] = isp[q];
                 if (isp[q] == 0) {
                     o.bv[q][0] = VX; o.bv[q][1] = VY; o.bv[q][2] = VZ;
-                    const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
-                    anewvel(rengy, vel, o.bv[q][0], o.bv[q][1], o.bv[q][2], a, b);
+                    if (aro2) {
+                        const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+                        anewvel(rengy, vel, o.bv[q][0], o.bv[q][1], o.bv[q][2], a, b);
+                    }
                 } else {
                     const int n = (int)((c.nvel - 1) * hp_stream_next(&rs));
                     const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
@@ -596,7 +626,7 @@ template <class R> struct Sim : SimBase {
                 }
             }
             const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
-            anewvel(engy, vel2, VX, VY, VZ, a, b);
+            anewvel(engy, aro2 ? vel2 : vel, VX, VY, VZ, a, b);
             o.vx = VX; o.vy = VY; o.vz = VZ;
             break;
         }
@@ -616,18 +646,20 @@ template <class R> struct Sim : SimBase {
 
     void oxy_ion(int s, R vx, R vy, R vz, int t, R bv1, R bv2, hp_stream &rs, OxyOut &o) const {
         enum { NUL, SCAT, CX, TO_OP, TO_ARP, TO_O2P, DET, REC };
+        const bool aro2 = c.gas == 2;
+        const int OMINUS = aro2 ? 4 : 3, O2P = aro2 ? 2 : 1, OPL = aro2 ? 3 : 2;
         o.keep = true;
         o.vx = vx; o.vy = vy; o.vz = vz;
         const R Esc = (R)c.Escale[s];
         R vnx = 0, vny = 0, vnz = 0, VX, VY, VZ, vel, engy;
-        if (s == 4) {
+        if (s == OMINUS) {
             VX = vx; VY = vy; VZ = vz;
             const R dum = VX * VX + VY * VY + VZ * VZ;
             vel = std::sqrt(dum);
             VX /= vel; VY /= vel; VZ /= vel;
             engy = Esc * dum;
         } else {
-            const R vneut = s == 1 ? (t == 0 ? bv1 : bv2) : (s == 2 ? bv1 : bv2);
+            const R vneut = aro2 ? (s == 1 ? (t == 0 ? bv1 : bv2) : (s == 2 ? bv1 : bv2)) : bv1;
             const int n = (int)((c.nvel - 1) * hp_stream_next(&rs));
             const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
             maxwellv(vnx, vny, vnz, (R)c.vsave[n], vneut, a, b);
@@ -635,10 +667,34 @@ template <class R> struct Sim : SimBase {
             const R dum = VX * VX + VY * VY + VZ * VZ;
             vel = std::sqrt(dum);
             engy = Esc * dum;
-            if (s == 1) (void)hp_stream_next(&rs);
+            if (aro2 && s == 1) (void)hp_stream_next(&rs);
         }
         int sv = 0, nr = 0, ch[3] = {0, 0, 0}, act[3] = {0, 0, 0};
         bool cum = false;
+        if (!aro2) {
+            switch (s) {
+            case 1:
+                sv = 12 + t;
+                if (t == 0) { nr = 1; ch[0] = 47; act[0] = TO_OP; }
+                else if (t == 1) { nr = 3; ch[0] = 48; act[0] = CX; ch[1] = 49; act[1] = SCAT; ch[2] = 50; act[2] = TO_OP; }
+                else { nr = 1; ch[0] = 49 + t; act[0] = CX; }
+                break;
+            case 2:
+                sv = 16 + t;
+                if (t == 0) { nr = 2; ch[0] = 53; act[0] = TO_O2P; ch[1] = 54; act[1] = SCAT; }
+                else if (t == 1) { nr = 1; ch[0] = 55; act[0] = CX; }
+                else { nr = 1; ch[0] = 54 + t; act[0] = TO_O2P; }
+                break;
+            default:
+                sv = 9 + t;
+                if (t == 0) { nr = 2; ch[0] = 41; act[0] = SCAT; ch[1] = 42; act[1] = DET; cum = true; }
+                else if (t == 1) { nr = 1; ch[0] = 43; act[0] = DET; }
+                else if (t == 2) { nr = 1; ch[0] = 44; act[0] = REC; }
+                else if (t == 3) { nr = 1; ch[0] = 45; act[0] = REC; }
+                else { nr = 1; ch[0] = 46; act[0] = DET; }
+                break;
+            }
+        } else
         switch (s) {
         case 1:
             sv = 23 + t;
@@ -683,14 +739,14 @@ template <class R> struct Sim : SimBase {
         case SCAT: {
             const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
             newvel_ionsc(VX, VY, VZ, vel, a, b);
-            if (s == 4) { o.vx = VX; o.vy = VY; o.vz = VZ; }
+            if (s == OMINUS) { o.vx = VX; o.vy = VY; o.vz = VZ; }
             else { o.vx = VX + vnx; o.vy = VY + vny; o.vz = VZ + vnz; }
             break;
         }
         case CX: o.vx = vnx; o.vy = vny; o.vz = vnz; break;
-        case TO_OP: born(3, vnx, vny, vnz); break;
+        case TO_OP: born(OPL, vnx, vny, vnz); break;
         case TO_ARP: born(1, vnx, vny, vnz); break;
-        case TO_O2P: born(2, vnx, vny, vnz); break;
+        case TO_O2P: born(O2P, vnx, vny, vnz); break;
         case DET: born(0, VX, VY, VZ); break;
         default: o.keep = false; break;
         }
@@ -698,14 +754,17 @@ template <class R> struct Sim : SimBase {
 
     void mcc_aro2(int64_t tstep) {
         const uint32_t step = (uint32_t)tstep;
-        const int NS = 5, STRIDE = c.mcc_stride, HOLE_CAP = 64;
+        const bool aro2 = c.gas == 2;
+        const int NS = aro2 ? 5 : 4, STRIDE = c.mcc_stride, HOLE_CAP = 64, OMINUS = aro2 ? 4 : 3;
+        // the reference's O2 launch collides electrons only (src/cuda_mcc.cu:76-77)
+        const int NACT = (aro2 || c.mcc_all_species) ? NS : 1;
         struct P5 { std::vector<R> x, y, vx, vy, vz; };
         std::vector<std::array<P5, 5>> out((size_t)C);
         par_for(C, [&](int cell) {
             const int i = cell / c.ncy, j = cell - i * c.ncy, node = i * c.ngy + j, Gn = G;
-            const R bd1 = c.back_den1[node], bd2 = c.back_den2[node];
+            const R bd1 = c.back_den1[node], bd2 = aro2 ? (R)c.back_den2[node] : (R)0;
             const R F0 = c.fluid_den[node], F1 = c.fluid_den[Gn + node], F2 = c.fluid_den[2 * Gn + node];
-            const R F3 = c.fluid_den[3 * Gn + node], F4 = c.fluid_den[4 * Gn + node];
+            const R F3 = c.fluid_den[3 * Gn + node], F4 = aro2 ? (R)c.fluid_den[4 * Gn + node] : (R)0;
             auto xe = [&](R a, R b, R n) { return ox_exp(-1 * a * b * n); };
             auto nq = [&](int s, R sig, R dtx) {
                 R t = -1 * dtx;
@@ -720,7 +779,33 @@ template <class R> struct Sim : SimBase {
             const float *sv = c.sigv;
             R p[5][9];
             int np[5] = {9, 2, 5, 4, 5};
-            {
+            if (!aro2) { // O2Collision_Check (src/cuda_mccO2.cu:867-911)
+                np[0] = 7; np[1] = 4; np[2] = 4; np[3] = 5; np[4] = 1;
+                R *e = p[0];
+                e[0] = e_acc(0, true, xe(dtm, sv[0], bd1));
+                e[1] = e_acc(e[0], false, xe(dtm, sv[1], F0));
+                e[2] = e_acc(e[1], false, xe(dtm, sv[2], F1));
+                e[3] = e_acc(e[2], false, nq(3, sv[3], dtm));
+                e[4] = e_acc(e[3], false, nq(1, sv[4], dtm));
+                e[5] = e_acc(e[4], false, xe(dtm, sv[5], F2));
+                e[6] = e_acc(e[5], false, xe(dtm, sv[6], F3));
+                R *a = p[1];
+                a[0] = i_acc(0, true, xe(dtm, sv[12], F2));
+                a[1] = i_acc(a[0], false, xe(dtm, sv[13], bd1));
+                a[2] = i_acc(a[1], false, xe(dtm, sv[14], F0));
+                a[3] = i_acc(a[2], false, xe(dtm, sv[15], F1));
+                R *b = p[2];
+                b[0] = i_acc(0, true, xe(dt, sv[16], bd1));
+                b[1] = i_acc(b[0], false, xe(dt, sv[17], F2));
+                b[2] = i_acc(b[1], false, xe(dt, sv[18], F0));
+                b[3] = i_acc(b[2], false, xe(dt, sv[19], F1));
+                R *m = p[3];
+                m[0] = i_acc(0, true, xe(dt, sv[7], bd1));
+                m[1] = i_acc(m[0], false, xe(dt, sv[8], F2));
+                m[2] = i_acc(m[1], false, nq(1, sv[9], dt));
+                m[3] = i_acc(m[2], false, nq(2, sv[10], dt));
+                m[4] = i_acc(m[3], false, xe(dt, sv[11], F0));
+            } else {
                 R *e = p[0];
                 e[0] = e_acc(0, true, xe(dtm, sv[0], bd1));
                 e[1] = e_acc(e[0], false, xe(dtm, sv[1], F0));
@@ -752,7 +837,7 @@ template <class R> struct Sim : SimBase {
                 om[3] = i_acc(om[2], false, nq(3, sv[12], dt));
                 om[4] = i_acc(om[3], false, xe(dt, sv[13], F1));
             }
-            const R bv1 = c.back_vel1[node], bv2 = c.back_vel2[node];
+            const R bv1 = c.back_vel1[node], bv2 = aro2 ? (R)c.back_vel2[node] : (R)0;
             std::array<P5, 5> &L = out[(size_t)cell];
             std::vector<char> gone[5];
             int n0[5];
@@ -769,8 +854,8 @@ template <class R> struct Sim : SimBase {
                 gone[s].assign((size_t)n0[s], 0);
             }
             unsigned *cnt = &mcc_count[(size_t)cell * STRIDE];
-            for (int s = 0; s < NS; s++) {
-                const int nsub = s == 0 ? c.mcc_n : 1;
+            for (int s = 0; s < NACT; s++) {
+                const int nsub = (s == 0 || (!aro2 && s == 1)) ? c.mcc_n : 1;
                 const R Tprob = p[s][np[s] - 1];
                 for (int k = 0; k < n0[s]; k++) {
                     int t = -1;
@@ -806,19 +891,20 @@ template <class R> struct Sim : SimBase {
                         gone[t2].push_back(0);
                     }
                     if (o.kill) {
+                        const int om = OMINUS;
                         int nlive = 0;
-                        for (int q = 0; q < n0[4]; q++) nlive += gone[4][(size_t)q] ? 0 : 1;
+                        for (int q = 0; q < n0[om]; q++) nlive += gone[om][(size_t)q] ? 0 : 1;
                         if (nlive > 0) {
                             int pick = 0;
                             if (nlive > 1) {
                                 pick = (int)((float)nlive * o.r2);
                                 if (pick > nlive - 1) pick = nlive - 1;
                             }
-                            for (int q = 0; q < n0[4]; q++) {
-                                if (gone[4][(size_t)q]) continue;
+                            for (int q = 0; q < n0[om]; q++) {
+                                if (gone[om][(size_t)q]) continue;
                                 if (pick-- == 0) {
-                                    gone[4][(size_t)q] = 1;
-                                    holes[4].push_back(q);
+                                    gone[om][(size_t)q] = 1;
+                                    holes[om].push_back(q);
                                     break;
                                 }
                             }
@@ -874,7 +960,7 @@ template <class R> struct Sim : SimBase {
     }
 
     void mcc(int64_t tstep) override {
-        if (c.gas == 2) {
+        if (c.gas == 1 || c.gas == 2) {
             mcc_aro2(tstep);
             return;
         }

@@ -58,7 +58,7 @@ typedef struct or_case {
     /* cell crossings per push: 0 one (reference), 1 until inside a cell */
     int move_mode;
     /* reaction set (0 Ar, 2 Ar/O2) and what the oxygen sets need */
-    int gas, mcc_stride;
+    int gas, mcc_stride, mcc_all_species;
     float dt_mcc, np2c[5];
     const float *back_den1, *back_den2, *back_vel2, *fluid_den;
 } or_case;

@@ -39,7 +39,8 @@ class OrCase(C.Structure):
         ("fs_i0", C.c_int), ("fs_j0", C.c_int), ("fs_nx", C.c_int), ("fs_ny", C.c_int), ("fs_passes", C.c_int),
         ("fs_V", _F), ("fs_Vt", _F), ("fs_W", _F), ("fs_Wt", _F), ("fs_inv", _F),
         ("move_mode", C.c_int),
-        ("gas", C.c_int), ("mcc_stride", C.c_int), ("dt_mcc", C.c_float), ("np2c", C.c_float * 5),
+        ("gas", C.c_int), ("mcc_stride", C.c_int), ("mcc_all_species", C.c_int), ("dt_mcc", C.c_float),
+        ("np2c", C.c_float * 5),
         ("back_den1", _F), ("back_den2", _F), ("back_vel2", _F), ("fluid_den", _F),
     ]
 
@@ -148,6 +149,7 @@ class Oracle:
             c.th[k] = collf[k, 2]
         c.gas = info.main_gas
         c.mcc_stride = info.mcc_stride
+        c.mcc_all_species = 1 if opts.o2_all_species else 0
         c.dt_mcc = sc[1]
         for s in range(info.nsp):
             c.np2c[s] = spc[s, 0]
