@@ -36,13 +36,19 @@ WORKLOADS = {
     "ar_513x257_200ppc": dict(ngx=513, ngy=257, xlen=0.16, ylen=0.08, ppc=200, voltage=100.0, pressure=0.05),
     "ar_257x129_200ppc": dict(ngx=257, ngy=129, xlen=0.08, ylen=0.04, ppc=200, voltage=100.0, pressure=0.05),
     "ar_129x65_50ppc": dict(ngx=129, ngy=65, xlen=0.04, ylen=0.02, ppc=50, voltage=100.0, pressure=0.05),
+    # 80/20 Ar/O2 at 100 mTorr, 200 V: e 3 eV, Ar+ 1e15, O2+ 2e14, O+ 0, O- 2e14 m^-3
+    "aro2_257x129_100ppc": dict(ngx=257, ngy=129, xlen=0.08, ylen=0.04, ppc=100, voltage=200.0, pressure=0.1,
+                                gas="ArO2", te=3.0, ions={"Ar+": 1e15, "O2+": 2e14, "O+": 0.0, "O-": 2e14}),
 }
 
 
 def make_deck(w):
     from hpic.decks import ccp_deck
+    extra = {}
+    if w.get("gas", "Ar") != "Ar":
+        extra = dict(gas=w["gas"], te_ev=w["te"], ion_density=w["ions"], aro2_ratio=(80, 20))
     return ccp_deck(w["ngx"], w["ngy"], w["xlen"], w["ylen"], ppc=w["ppc"], voltage=w["voltage"],
-                    pressure_torr=w["pressure"])
+                    pressure_torr=w["pressure"], **extra)
 
 
 class ClockSampler:
@@ -294,7 +300,8 @@ def run_ours(args, rank, world, local, dist):
         vs_baseline=None, dtype="f32 particles / f64 charge and field refinement", data="synthetic",
         config=dict(workload=args.workload, nodes=f"{w['ngx']}x{w['ngy']}", ppc_per_species=w["ppc"],
                     particles=int(sum(case.particles_count(s) for s in range(nsp))),
-                    gas="Ar", pressure_torr=w["pressure"], rf_voltage=w["voltage"], field_mode=case.info.field_mode,
+                    gas=w.get("gas", "Ar"), pressure_torr=w["pressure"], rf_voltage=w["voltage"],
+                    field_mode=case.info.field_mode,
                     parallelism=f"replicas x{world}", l2="state (>4 GB) larger than L2: no flush needed",
                     field_relative_residual=resid, device_status=status),
         e2e=dict(value=e2e_pushes / (e2e_ms * 1e-3), unit=UNIT, h2d_bytes_per_step=h2d / args.steps,
@@ -478,7 +485,7 @@ def run_served(args):
                             arrivals=f"Poisson {args.rate}/s", grids="65x33/129x65/257x129/513x257",
                             ppc="50-200", rf_periods="1-10", steps_per_rf_period=steps_per_cycle,
                             slots=args.slots, steps_per_launch=args.steps_per_launch, budget_gb=args.budget_gb,
-                            gas="Ar (the Ar/O2 reaction set is not built)"),
+                            gas="Ar or 80/20 Ar/O2"),
                 latency_s=dict(p50=pct(lat, 50), p99=pct(lat, 99)), errors=errors, wall_s=t_end,
                 plain=dict(value=plain_pushes / plain_end, latency_s=dict(p50=pct(plain_lat, 50),
                                                                           p99=pct(plain_lat, 99)),
