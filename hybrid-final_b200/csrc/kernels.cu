@@ -122,7 +122,9 @@ __device__ __forceinline__ int walk(const Geo d, int &i, int &j, float &lx, floa
 
 // ------------------------------------------------------------------ Move
 // MoveE_Basic (src/cuda_Move.cu:181-270): bilinear gather of the node field,
-// v += Ascale E, x += v dt/dx in cell units.  A particle that leaves its
+// v += Ascale E, x += v dt/dx in cell units (the reference's sums of
+// products, built with contraction, evaluated here as bilinear weights and
+// explicit fused multiply-adds).  A particle that leaves its
 // cell is resolved here (walk), including the boundary rules the reference
 // applies in SortBoundary.  Stayers are compacted in place (order kept);
 // movers are parked at the top of the cell's slots, r-th mover at slot
@@ -188,12 +190,15 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
             nvy = sp.vy[base + k + 32];
             nvz = sp.vz[base + k + 32];
         }
-        const float del_vx = ex_ws * (1 - lx) * (1 - ly) + ex_wn * (1 - lx) * ly + ex_es * lx * (1 - ly) + ex_en * lx * ly;
-        const float del_vy = ey_ws * (1 - lx) * (1 - ly) + ey_wn * (1 - lx) * ly + ey_es * lx * (1 - ly) + ey_en * lx * ly;
-        float mvX = vx + del_vx * As;
-        float mvY = vy + del_vy * As;
-        lx += mvX * dtdx;
-        ly += mvY * dtdy;
+        // bilinear weights once, then fused multiply-adds (one rounding each)
+        const float wx = 1 - lx, wy = 1 - ly;
+        const float w00 = wx * wy, w01 = wx * ly, w10 = lx * wy, w11 = lx * ly;
+        const float del_vx = __fmaf_rn(ex_en, w11, __fmaf_rn(ex_es, w10, __fmaf_rn(ex_wn, w01, ex_ws * w00)));
+        const float del_vy = __fmaf_rn(ey_en, w11, __fmaf_rn(ey_es, w10, __fmaf_rn(ey_wn, w01, ey_ws * w00)));
+        float mvX = __fmaf_rn(del_vx, As, vx);
+        float mvY = __fmaf_rn(del_vy, As, vy);
+        lx = __fmaf_rn(mvX, dtdx, lx);
+        ly = __fmaf_rn(mvY, dtdy, ly);
         const bool out = act && (ly >= 1 || ly < 0 || lx >= 1 || lx < 0);
         int code = 4, fi = i, fj = j;
         if (out) {
@@ -318,12 +323,14 @@ __global__ void __launch_bounds__(512) k_move_u(const DevCase *__restrict__ case
             const int k = k0 + 32 * u + lane;
             const bool act = k < n;
             const float x0 = lx[u], y0 = ly[u];
-            const float del_vx = ex_ws * (1 - x0) * (1 - y0) + ex_wn * (1 - x0) * y0 + ex_es * x0 * (1 - y0) + ex_en * x0 * y0;
-            const float del_vy = ey_ws * (1 - x0) * (1 - y0) + ey_wn * (1 - x0) * y0 + ey_es * x0 * (1 - y0) + ey_en * x0 * y0;
-            float vX = mvx[u] + del_vx * As;
-            float vY = mvy[u] + del_vy * As;
-            float X = x0 + vX * dtdx;
-            float Y = y0 + vY * dtdy;
+            const float wx = 1 - x0, wy = 1 - y0;
+            const float w00 = wx * wy, w01 = wx * y0, w10 = x0 * wy, w11 = x0 * y0;
+            const float del_vx = __fmaf_rn(ex_en, w11, __fmaf_rn(ex_es, w10, __fmaf_rn(ex_wn, w01, ex_ws * w00)));
+            const float del_vy = __fmaf_rn(ey_en, w11, __fmaf_rn(ey_es, w10, __fmaf_rn(ey_wn, w01, ey_ws * w00)));
+            float vX = __fmaf_rn(del_vx, As, mvx[u]);
+            float vY = __fmaf_rn(del_vy, As, mvy[u]);
+            float X = __fmaf_rn(vX, dtdx, x0);
+            float Y = __fmaf_rn(vY, dtdy, y0);
             const bool out = act && (Y >= 1 || Y < 0 || X >= 1 || X < 0);
             int code = 4, fi = i, fj = j;
             if (out) {

@@ -310,12 +310,15 @@ template <class R> struct Sim : SimBase {
                 for (int q = p.start[cell]; q < p.start[cell + 1]; q++) {
                     R lx = p.x[q], ly = p.y[q];
                     const R vx = p.vx[q], vy = p.vy[q], vz = p.vz[q];
-                    const R del_vx = ex_ws * (1 - lx) * (1 - ly) + ex_wn * (1 - lx) * ly + ex_es * lx * (1 - ly) + ex_en * lx * ly;
-                    const R del_vy = ey_ws * (1 - lx) * (1 - ly) + ey_wn * (1 - lx) * ly + ey_es * lx * (1 - ly) + ey_en * lx * ly;
-                    R mvX = vx + del_vx * As;
-                    R mvY = vy + del_vy * As;
-                    lx += mvX * dtdx;
-                    ly += mvY * dtdy;
+                    // bilinear weights, then fused multiply-adds (as the kernel)
+                    const R wx = 1 - lx, wy = 1 - ly;
+                    const R w00 = wx * wy, w01 = wx * ly, w10 = lx * wy, w11 = lx * ly;
+                    const R del_vx = std::fma(ex_en, w11, std::fma(ex_es, w10, std::fma(ex_wn, w01, ex_ws * w00)));
+                    const R del_vy = std::fma(ey_en, w11, std::fma(ey_es, w10, std::fma(ey_wn, w01, ey_ws * w00)));
+                    R mvX = std::fma(del_vx, As, vx);
+                    R mvY = std::fma(del_vy, As, vy);
+                    lx = std::fma(mvX, dtdx, lx);
+                    ly = std::fma(mvY, dtdy, ly);
                     if (ly >= 1 || ly < 0 || lx >= 1 || lx < 0) {
                         int fi = i, fj = j, cond = -1, code;
                         const int r = walk(fi, fj, lx, ly, mvX, mvY, cond);
