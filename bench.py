@@ -175,20 +175,23 @@ def fp64_check(stream, steps=400):
     """Error of the precision form against the FP64 oracle on the reference's
     CPU-sized Ar case (129x65 nodes, 4 cm x 2 cm, 50 particles per cell and
     species, 100 V, 50 mTorr) over one RF period: relative L2 error of the
-    time-averaged n_e, n_i and potential.  The GPU runs the bench's numerics
+    time-averaged n_e, n_i and potential, and the electron energy distribution
+    (sampled every 4th step) as total-variation distance and relative error of
+    the mean energy.  The GPU runs the bench's numerics
     (FP32 particles, FP64 charge grid, field_mode 2); the oracle runs the same
     case and draws in FP64 on the host."""
     import hpic
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle
     w = WORKLOADS["ar_129x65_50ppc"]
-    opts = dict(field_mode=2, gas_temp_mode=1, move_mode=1)
+    opts = dict(field_mode=2, gas_temp_mode=1, move_mode=1, eedf_every=4)
     S = hpic.Setup(make_deck(w), seed=77, **opts)
     c = hpic.Case(setup=S, seed=77, **opts)
     c.step(steps, stream)
     n = c.average_count()
     d32 = c.grid("AVE_DEN").reshape(c.info.nsp, -1) / n
     p32 = c.grid("AVE_PHI") / n
+    h32 = c.grid("EEDF").astype(np.float64)
     c.close()
     t0 = time.perf_counter()
     o = oracle.from_setup(S, 64, field_mode=2)
@@ -197,11 +200,16 @@ def fp64_check(stream, steps=400):
     o.run(0, steps, accumulate=True)
     d, p, m = o.averages()
     d64, p64 = d.reshape(S.info.nsp, -1) / m, p / m
+    h64 = o.eedf().astype(np.float64)
 
     def rel(a, b):
         return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    pe, qe = h32 / h32.sum(), h64 / h64.sum()
+    ebin = (np.arange(pe.size) + 0.5) * hpic.EEDF_DE
     return dict(case="ar_129x65_50ppc", steps=steps, rf_periods=steps / 400, tolerance=0.01,
                 rel_l2_ave_n_e=rel(d32[0], d64[0]), rel_l2_ave_n_i=rel(d32[1], d64[1]), rel_l2_ave_phi=rel(p32, p64),
+                eedf_tv=round(0.5 * float(np.abs(pe - qe).sum()), 6),
+                eedf_mean_energy_rel=round(abs(float(pe @ ebin) / float(qe @ ebin) - 1.0), 6),
                 fp64_oracle_s=round(time.perf_counter() - t0, 1))
 
 

@@ -354,6 +354,8 @@ hp_status build_device(hp_case *c) {
     TRY(dalloc(c, &h.mcc_count, (size_t)h.mcc_stride * C));
     TRY(dalloc(c, &h.pcg_iters, 2));
     TRY(dalloc(c, &h.ave_count, 1));
+    TRY(dalloc(c, &h.eedf, HP_EEDF_BINS + 1));
+    h.eedf_every = c->opts.eedf_every > 0 ? c->opts.eedf_every : 0;
     TRY(dalloc(c, &h.pushes, 32));
     TRY(dalloc(c, &h.far_in, (size_t)s.nsp * C));
     TRY(dalloc(c, &h.far_key, (size_t)s.nsp * C * HP_FAR_BUCKET));
@@ -448,6 +450,7 @@ hp_status one_step(hp_case *c, cudaStream_t st) {
     TRY(op_mcc(c, st));
     TRY(op_deposit(c, st));
     e = launch_accumulate(c->d_case, c->d_items + 4, 1, c->s.Gsize, st);
+    if (e == cudaSuccess && c->h.eedf_every > 0) e = launch_eedf(c->d_case, c->d_items + 2, 1, c->s.Csize, st);
     return e == cudaSuccess ? HP_OK : cuda_fail(e, "accumulate");
 }
 
@@ -923,6 +926,7 @@ static hp_status grid_ptr(hp_case *c, hp_grid_field f, void **p, size_t *nb) {
     case HP_GRID_AVE_PHI: *p = c->h.ave_phi; *nb = (size_t)G * 8; break;
     case HP_GRID_COND_CHARGE: *p = c->h.cond_charge; *nb = (size_t)nsp * c->s.cond_numr * 4; break;
     case HP_GRID_MCC_COUNT: *p = c->h.mcc_count; *nb = (size_t)c->h.mcc_stride * c->s.Csize * 4; break;
+    case HP_GRID_EEDF: *p = c->h.eedf; *nb = (size_t)(HP_EEDF_BINS + 1) * 8; break;
     default: return set_error("unknown grid field"), HP_ERR_ARG;
     }
     return HP_OK;
@@ -959,6 +963,7 @@ hp_status hp_reset_averages(hp_case *c) {
     CK(cudaMemset(c->h.ave_den, 0, (size_t)c->s.nsp * c->s.Gsize * 8));
     CK(cudaMemset(c->h.ave_phi, 0, (size_t)c->s.Gsize * 8));
     CK(cudaMemset(c->h.ave_count, 0, 8));
+    CK(cudaMemset(c->h.eedf, 0, (HP_EEDF_BINS + 1) * 8));
     return HP_OK;
 }
 

@@ -22,6 +22,10 @@
 // step and species; more sets the overflow status
 #define HP_FAR_BUCKET 32
 
+// electron energy distribution: bins of HP_EEDF_DE eV from 0, one overflow bin
+#define HP_EEDF_BINS 200
+#define HP_EEDF_DE 0.25f
+
 namespace hp {
 
 constexpr int DMAXSP = 5;
@@ -90,6 +94,8 @@ struct DevCase {
     unsigned int *mcc_count;        // [C*mcc_stride] collisions per cell and channel
     int *pcg_iters;                 // [2]: inner, outer of the last solve
     int64_t *ave_count;
+    unsigned long long *eedf;       // [HP_EEDF_BINS+1] electron energy histogram since the last reset
+    int eedf_every;                 // 0: off; k: sample every k-th step
     unsigned long long *pushes;     // [32] particles pushed by Move, spread over 32 counters
     unsigned long long *far_key;    // [nsp*C*HP_FAR_BUCKET] movers arriving from beyond the 3x3 neighbourhood
     int *far_in;                    // [nsp*C] entries in each bucket (cleared by Sort)

@@ -1304,6 +1304,47 @@ __global__ void __launch_bounds__(256) k_accumulate(const DevCase *__restrict__ 
     if (n == 0) *d.ave_count += 1;
 }
 
+// Electron energy distribution: every eedf_every steps, a histogram of
+// E = Escale |v|^2 (eV) over all electrons, HP_EEDF_BINS bins of
+// HP_EEDF_DE eV and one overflow bin (the reference has no EEDF; its deck
+// keys for one are commented out, src/start.c:935-968).  One warp per cell,
+// counts gathered per block in shared memory and added to the case's
+// 64-bit histogram: integer counts, so the result does not depend on order.
+__global__ void __launch_bounds__(256) k_eedf(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
+                                              int ncases, int items) {
+    __shared__ unsigned int h[HP_EEDF_BINS + 1];
+    __shared__ int case_of_block;
+    for (int b = threadIdx.x; b <= HP_EEDF_BINS; b += blockDim.x) h[b] = 0;
+    const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31;
+    const int first_warp = (int)(blockIdx.x * (blockDim.x >> 5));
+    if (threadIdx.x == 0) case_of_block = first_warp < items ? find_case(item_start, ncases, first_warp) : -1;
+    __syncthreads();
+    if (warp < items) {
+        const int ci = find_case(item_start, ncases, warp);
+        const DevCase &d = cases[ci];
+        const int c = warp - item_start[ci];
+        if (d.eedf_every > 0 && (*d.tstep % d.eedf_every) == 0) {
+            const DevSpecies &el = d.sp[0];
+            const int n = el.cnt[c];
+            const size_t base = (size_t)c * el.cap;
+            for (int k = lane; k < n; k += 32) {
+                const float vx = el.vx[base + k], vy = el.vy[base + k], vz = el.vz[base + k];
+                const float e = el.Escale * (vx * vx + vy * vy + vz * vz);
+                const int b = e < HP_EEDF_BINS * HP_EEDF_DE ? (int)(e * (1.0f / HP_EEDF_DE)) : HP_EEDF_BINS;
+                if (ci == case_of_block) atomicAdd(&h[b], 1u);
+                else atomicAdd(&d.eedf[b], 1ull); // a block that straddles two cases
+            }
+        }
+    }
+    __syncthreads();
+    if (case_of_block >= 0) {
+        const DevCase &d = cases[case_of_block];
+        for (int b = threadIdx.x; b <= HP_EEDF_BINS; b += blockDim.x)
+            if (h[b]) atomicAdd(&d.eedf[b], (unsigned long long)h[b]);
+    }
+}
+
 // CSR particle arrays (cell order, start[c] = first particle of cell c) into
 // the cell-blocked slot pool of one species; one warp per cell.
 __global__ void __launch_bounds__(256) k_scatter(DevSpecies sp, int C, const int *__restrict__ start,
@@ -1424,6 +1465,12 @@ cudaError_t launch_scatter(const DevSpecies &sp, int C, const int *start, const 
 
 cudaError_t launch_advance(const DevCase *cases, int ncases, cudaStream_t st) {
     k_advance<<<blocks_for(ncases, 128), 128, 0, st>>>(cases, ncases);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_eedf(const DevCase *cases, const int *cell_items, int ncases, int n_cell_items, cudaStream_t st) {
+    if (n_cell_items <= 0) return cudaSuccess;
+    k_eedf<<<blocks_for((long long)n_cell_items * 32, 256), 256, 0, st>>>(cases, cell_items, ncases, n_cell_items);
     return cudaGetLastError();
 }
 

@@ -77,6 +77,8 @@ cudaError_t launch_scatter(const DevSpecies &sp, int C, const int *start, const 
 // tstep += 1 for every case (device-side step counter, graph friendly)
 cudaError_t launch_advance(const DevCase *cases, int ncases, cudaStream_t st);
 // running sums of den and phi (N_ave accumulation, src/cuda_Diagnostic.cu:505-547)
+// electron energy histogram of the cases whose eedf_every divides the step
+cudaError_t launch_eedf(const DevCase *cases, const int *cell_items, int ncases, int n_cell_items, cudaStream_t st);
 cudaError_t launch_accumulate(const DevCase *cases, const int *node_items, int ncases, int n_node_items,
                               cudaStream_t st);
 

@@ -23,7 +23,8 @@ HP_OK, HP_ERR_ARG, HP_ERR_DECK, HP_ERR_CUDA, HP_ERR_OOM, HP_ERR_UNSUPPORTED, HP_
 STATUS_CELL_OVERFLOW, STATUS_NONFINITE, STATUS_PCG_NOCONV, STATUS_WAIT_TIMEOUT = 1, 2, 4, 8
 
 GRID = dict(EX=0, EY=1, PHI=2, PHI_POIS=3, DEN=4, SOURCE=5, PCG_X=6, PCG_B=7, AVE_DEN=8, AVE_PHI=9,
-            COND_CHARGE=10, MCC_COUNT=11)
+            COND_CHARGE=10, MCC_COUNT=11, EEDF=12)
+EEDF_BINS, EEDF_DE = 200, 0.25  # electron energy histogram: 0.25 eV bins from 0, one overflow bin
 TABLE = dict(sidx=0, a_idx=1, boundary=2, face=3, cond_id=4, area=5, back_den1=6, back_vel1=7, lap=8,
              stencil=9, vsave=10, xsec=11, collf=12, sigv=13, dens_region=14, prob=15, eps_r=16,
              back_den2=17, back_vel2=18, a_val=19, ai=20, aj=21, matm=22, cond_b=23, temp_b=24, ta_val=25,
@@ -43,7 +44,7 @@ class CaseOpts(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("cap_per_cell", C.c_int), ("field_mode", C.c_int),
                 ("pcg_rtol", C.c_double), ("pcg_max_iter", C.c_int), ("o2_all_species", C.c_int),
                 ("device", C.c_int), ("gas_temp_mode", C.c_int), ("move_mode", C.c_int),
-                ("fs_passes", C.c_int)]
+                ("fs_passes", C.c_int), ("eedf_every", C.c_int)]
 
 
 class CaseInfo(C.Structure):
@@ -342,7 +343,8 @@ class Case:
                      DEN=(nsp * G, np.float64), SOURCE=(G, np.float64),
                      PCG_X=(G, np.float32 if self.opts.field_mode == 0 else np.float64),
                      PCG_B=(G, np.float64), AVE_DEN=(nsp * G, np.float64), AVE_PHI=(G, np.float64),
-                     COND_CHARGE=(nsp * info.cond_numr, np.float32), MCC_COUNT=(info.mcc_stride * info.Csize, np.uint32))
+                     COND_CHARGE=(nsp * info.cond_numr, np.float32), MCC_COUNT=(info.mcc_stride * info.Csize, np.uint32),
+                     EEDF=(EEDF_BINS + 1, np.uint64))
         n, dt = sizes[name]
         out = np.zeros(n, dtype=dt)
         _check(lib().hp_get_grid(self.h, GRID[name], out.ctypes.data_as(_P), out.nbytes))

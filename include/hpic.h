@@ -98,6 +98,7 @@ typedef struct hp_case_opts {
                             until the offset is inside a cell */
     int fs_passes;       /* field_mode 2: FP64 refinement passes per solve; 0 = 2 when pcg_rtol >= 1e-10
                             (each pass gains ~6 digits), else 3 */
+    int eedf_every;      /* electron energy distribution (HP_GRID_EEDF): 0 = off, k = sample every k-th step */
 } hp_case_opts;
 
 /* Default options. */
@@ -206,7 +207,10 @@ typedef enum hp_grid_field {
     HP_GRID_AVE_DEN = 8, /* double[nsp*Gsize] running sum of den since hp_reset_averages */
     HP_GRID_AVE_PHI = 9, /* double[Gsize] running sum of TotPotential */
     HP_GRID_COND_CHARGE = 10, /* float[nsp*CondNUMR] absorbed particles per conductor */
-    HP_GRID_MCC_COUNT = 11    /* uint32[nsp*16] collisions per channel since creation */
+    HP_GRID_MCC_COUNT = 11,   /* uint32[Csize*mcc_stride] collisions per cell and channel since creation */
+    HP_GRID_EEDF = 12         /* uint64[201] electron energy histogram (0.25 eV bins, last = above 50 eV),
+                                 sampled every eedf_every steps since hp_reset_averages; no reference
+                                 counterpart (the reference computes no EEDF) */
 } hp_grid_field;
 hp_status hp_get_grid(hp_case *c, hp_grid_field f, void *out, size_t bytes);
 hp_status hp_set_grid(hp_case *c, hp_grid_field f, const void *in, size_t bytes);

@@ -90,6 +90,8 @@ struct SimBase {
     std::vector<double> ave_den, ave_phi;
     int64_t ave_count = 0;
     bool walk_bound_hit = false; // a walk that reached its crossing bound
+    std::vector<unsigned long long> eedf = std::vector<unsigned long long>(201, 0ull);
+    virtual void eedf_sample() = 0;
     virtual ~SimBase() {}
     virtual void set_particles(int, const int *, const float *, const float *, const float *, const float *,
                                const float *) = 0;
@@ -1553,6 +1555,18 @@ template <class R> struct Sim : SimBase {
         for (int n = 0; n < G; n++) ave_phi[n] += (double)phi[n];
         ave_count++;
     }
+    // electron energy histogram (the library's EEDF: 200 bins of 0.25 eV and
+    // an overflow bin), E = Escale |v|^2 as the MCC computes it
+    void eedf_sample() override {
+        const Sp &e = sp[0];
+        const R Esc = (R)c.Escale[0], top = (R)(200 * 0.25f), inv = (R)(1.0f / 0.25f);
+        for (size_t k = 0; k < e.vx.size(); k++) {
+            const R v = e.vx[k] * e.vx[k] + e.vy[k] * e.vy[k] + e.vz[k] * e.vz[k];
+            const R en = Esc * v;
+            const int b = en < top ? (int)(en * inv) : 200;
+            eedf[(size_t)b]++;
+        }
+    }
 };
 
 } // namespace
@@ -1627,9 +1641,14 @@ void or_run(or_sim *s, int64_t tstep0, int nsteps, int accumulate) {
         s->impl->sort();
         s->impl->mcc(t);
         s->impl->deposit();
-        if (accumulate) s->impl->accumulate();
+        if (accumulate) {
+            s->impl->accumulate();
+            const int ev = s->impl->c.eedf_every;
+            if (ev > 0 && t % ev == 0) s->impl->eedf_sample();
+        }
     }
 }
+void or_get_eedf(or_sim *s, unsigned long long *h) { std::memcpy(h, s->impl->eedf.data(), 201 * 8); }
 void or_get_averages(or_sim *s, double *ave_den, double *ave_phi, int64_t *count) {
     SimBase *b = s->impl;
     if (ave_den) std::memcpy(ave_den, b->ave_den.data(), b->ave_den.size() * 8);

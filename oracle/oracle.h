@@ -59,6 +59,7 @@ typedef struct or_case {
     int move_mode;
     /* reaction set (0 Ar, 2 Ar/O2) and what the oxygen sets need */
     int gas, mcc_stride, mcc_all_species;
+    int eedf_every; /* electron energy histogram every k-th step in or_run with accumulation (0 off) */
     float dt_mcc, np2c[5];
     const float *back_den1, *back_den2, *back_vel2, *fluid_den;
 } or_case;
@@ -97,6 +98,8 @@ void or_deposit(or_sim *s);
 /* n full steps from tstep+1; accumulates node averages when ave != 0 */
 void or_run(or_sim *s, int64_t tstep0, int nsteps, int accumulate);
 void or_get_averages(or_sim *s, double *ave_den, double *ave_phi, int64_t *count);
+/* the electron energy histogram: 201 counts (0.25 eV bins, last = overflow) */
+void or_get_eedf(or_sim *s, unsigned long long *h);
 int or_num_threads(void);
 void or_set_threads(int n);
 

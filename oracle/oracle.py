@@ -39,7 +39,8 @@ class OrCase(C.Structure):
         ("fs_i0", C.c_int), ("fs_j0", C.c_int), ("fs_nx", C.c_int), ("fs_ny", C.c_int), ("fs_passes", C.c_int),
         ("fs_V", _F), ("fs_Vt", _F), ("fs_W", _F), ("fs_Wt", _F), ("fs_inv", _F),
         ("move_mode", C.c_int),
-        ("gas", C.c_int), ("mcc_stride", C.c_int), ("mcc_all_species", C.c_int), ("dt_mcc", C.c_float),
+        ("gas", C.c_int), ("mcc_stride", C.c_int), ("mcc_all_species", C.c_int), ("eedf_every", C.c_int),
+        ("dt_mcc", C.c_float),
         ("np2c", C.c_float * 5),
         ("back_den1", _F), ("back_den2", _F), ("back_vel2", _F), ("fluid_den", _F),
     ]
@@ -72,6 +73,7 @@ def lib():
             "or_set_grid": (None, [P, C.c_int, P]),
             "or_get_counters": (None, [P, _F, C.POINTER(C.c_uint), _I]),
             "or_walk_bound_hit": (C.c_int, [P]),
+            "or_get_eedf": (None, [P, C.POINTER(C.c_uint64)]),
             "or_math": (None, [C.c_int, _F, _F, _F, C.c_int]),
             "or_field": (None, [P, C.c_int64]),
             "or_move": (None, [P]),
@@ -150,6 +152,7 @@ class Oracle:
         c.gas = info.main_gas
         c.mcc_stride = info.mcc_stride
         c.mcc_all_species = 1 if opts.o2_all_species else 0
+        c.eedf_every = max(0, opts.eedf_every)
         c.dt_mcc = sc[1]
         for s in range(info.nsp):
             c.np2c[s] = spc[s, 0]
@@ -292,6 +295,11 @@ class Oracle:
 
     def run(self, tstep0, nsteps, accumulate=True):
         lib().or_run(self.h, tstep0, nsteps, 1 if accumulate else 0)
+
+    def eedf(self):
+        h = np.zeros(201, np.uint64)
+        lib().or_get_eedf(self.h, h.ctypes.data_as(C.POINTER(C.c_uint64)))
+        return h
 
     def averages(self):
         G, nsp = self.info.Gsize, self.info.nsp

@@ -5,8 +5,11 @@ grid and an FP64-refined field solve.  The oracle's FP64 form runs the same
 case with the same random draws entirely in double precision.  Single
 trajectories decorrelate (the discharge is chaotic), so the comparison is on
 the time-averaged ion density and potential over one RF period (400 steps),
-as relative L2 errors; the stated tolerance is 1 %.  Every input is seeded, so
-the numbers below are fixed, not a random pass/fail."""
+as relative L2 errors; the stated tolerance is 1 %.  The electron energy
+distribution (EEDF, sampled every 4th step over the period) is compared as
+normalised histograms: total-variation distance at most 2 % and mean energy
+within 1 %.  Every input is seeded, so the numbers below are fixed, not a
+random pass/fail."""
 import numpy as np
 import pytest
 
@@ -15,11 +18,21 @@ import oracle
 from hpic.decks import ccp_deck
 
 TOL = 0.01
-OPTS = dict(field_mode=2, gas_temp_mode=1, move_mode=1)
+EEDF_TV_TOL = 0.02
+OPTS = dict(field_mode=2, gas_temp_mode=1, move_mode=1, eedf_every=4)
 
 
 def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def eedf_errors(h, h64):
+    """(total-variation distance, relative mean-energy error) of two
+    electron energy histograms; bin centres (k + 1/2) 0.25 eV."""
+    p = np.asarray(h, np.float64) / float(np.sum(h))
+    q = np.asarray(h64, np.float64) / float(np.sum(h64))
+    e = (np.arange(p.size) + 0.5) * hpic.EEDF_DE
+    return 0.5 * float(np.abs(p - q).sum()), abs(float(p @ e) / float(q @ e) - 1.0)
 
 
 def fp64_averages(S, nsteps):
@@ -28,7 +41,7 @@ def fp64_averages(S, nsteps):
     o.Deposit()
     o.run(0, nsteps, accumulate=True)
     d, p, n = o.averages()
-    return d.reshape(S.info.nsp, -1) / n, p / n
+    return d.reshape(S.info.nsp, -1) / n, p / n, o.eedf()
 
 
 def test_fp32_oracle_within_tolerance_of_fp64():
@@ -40,9 +53,11 @@ def test_fp32_oracle_within_tolerance_of_fp64():
     o.run(0, 400, accumulate=True)
     d, p, n = o.averages()
     d32, p32 = d.reshape(S.info.nsp, -1) / n, p / n
-    d64, p64 = fp64_averages(S, 400)
+    d64, p64, h64 = fp64_averages(S, 400)
     assert rel_l2(d32[1], d64[1]) <= TOL
     assert rel_l2(p32, p64) <= TOL
+    tv, de = eedf_errors(o.eedf(), h64)
+    assert tv <= EEDF_TV_TOL and de <= TOL
 
 
 @pytest.mark.gpu
@@ -57,7 +72,9 @@ def test_gpu_within_tolerance_of_fp64():
     d32 = c.grid("AVE_DEN").reshape(c.info.nsp, -1) / n
     p32 = c.grid("AVE_PHI") / n
     assert c.status() == 0
-    d64, p64 = fp64_averages(S, 400)
+    d64, p64, h64 = fp64_averages(S, 400)
     err_ni, err_phi = rel_l2(d32[1], d64[1]), rel_l2(p32, p64)
-    print(f"time-averaged n_i rel L2 {err_ni:.3e}, phi {err_phi:.3e}")
+    tv, de = eedf_errors(c.grid("EEDF"), h64)
+    print(f"time-averaged n_i rel L2 {err_ni:.3e}, phi {err_phi:.3e}; EEDF TV {tv:.3e}, mean energy {de:.3e}")
     assert err_ni <= TOL and err_phi <= TOL
+    assert tv <= EEDF_TV_TOL and de <= TOL

@@ -36,9 +36,9 @@ DECKS = {
 CAP = {"ar_block_33x21": 256}
 
 
-def pair(name, field_mode=0, move_mode=0):
+def pair(name, field_mode=0, move_mode=0, **extra):
     deck, seed = DECKS[name]
-    kw = dict(seed=seed, field_mode=field_mode, move_mode=move_mode, cap_per_cell=CAP.get(name, 0))
+    kw = dict(seed=seed, field_mode=field_mode, move_mode=move_mode, cap_per_cell=CAP.get(name, 0), **extra)
     S = hpic.Setup(deck, **kw)
     case = hpic.Case(setup=S, **kw)
     info = case.info
@@ -156,6 +156,23 @@ def test_walk_steps_bit_exact(name, ppl):
     check_grids(case, o, ("DEN", "SOURCE"), "after steps")
     assert same(case.grid("COND_CHARGE"), o.counters()[0][: case.info.nsp * case.info.cond_numr])
     assert case.status() == 0
+
+
+@pytest.mark.parametrize("name", ["ar_33x17_hv", "ar_block_33x21"])
+def test_eedf_counts(name):
+    """The electron energy histogram (every 5th step) counts the same
+    electrons into the same 0.25 eV bins as the oracle."""
+    case, o = pair(name, field_mode=2, move_mode=1, eedf_every=5)
+    n = 23
+    case.step(n)
+    o.run(0, n, accumulate=True)
+    h = case.grid("EEDF")
+    assert h.dtype == np.uint64 and h.size == hpic.EEDF_BINS + 1
+    assert np.array_equal(h, o.eedf())
+    # four samples (steps 5, 10, 15, 20) of every electron present then
+    assert 0 < int(h.sum()) <= 4 * case.info.cap[0] * case.info.Csize
+    case.reset_averages()
+    assert int(case.grid("EEDF").sum()) == 0
 
 
 def fast_electrons(case, o, cells_per_step, every=3):
