@@ -231,6 +231,7 @@ hp_status hp_batch_set_tune(hp_batch *b, const hp_tune *t) {
     b->lc.pcg_block = t->pcg_block;
     b->lc.pcg_cluster_max = t->pcg_cluster_max;
     b->lc.move_unroll = t->move_unroll;
+    b->lc.mcc_cells = t->mcc_cells_per_warp;
     if (b->graph) {
         cudaGraphExecDestroy(b->graph);
         b->graph = nullptr;
@@ -244,6 +245,7 @@ hp_status hp_batch_get_tune(hp_batch *b, hp_tune *t) {
     t->pcg_block = b->lc.pcg_block;
     t->pcg_cluster_max = b->lc.pcg_cluster_max;
     t->move_unroll = b->lc.move_unroll;
+    t->mcc_cells_per_warp = b->lc.mcc_cells;
     return HP_OK;
 }
 
@@ -286,32 +288,47 @@ hp_status hp_batch_autotune(hp_batch *b, void *stream) {
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     hp_status result = HP_OK;
+    // time 3 steps of one candidate (after a warm-up step), then restore the state
+    auto trial = [&](const LaunchCfg &lc) {
+        b->lc = lc;
+        hp_status s = hpi::run_step(b->dev, b->lc, b->gas, st); // warm-up
+        if (s != HP_OK) { result = s; return; }
+        cudaEventRecord(e0, st);
+        for (int k = 0; k < 3 && s == HP_OK; k++) s = hpi::run_step(b->dev, b->lc, b->gas, st);
+        cudaEventRecord(e1, st);
+        if (s != HP_OK) { result = s; return; }
+        e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) { result = cuda_fail(e, "autotune trial"); return; }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms < best_ms) { best_ms = ms; best = lc; }
+        e = copy_all(false);
+        if (e != cudaSuccess) result = cuda_fail(e, "autotune restore");
+    };
     const int unrolls[3] = {1, 2, 4};
     for (int pi = 0; pi < 3 && result == HP_OK; pi++)
-    for (int wi = 0; wi < 3 && result == HP_OK; wi++)
-        for (int bi = 0; bi < 3 && result == HP_OK; bi++)
-            for (int ki = 0; ki < 3 && result == HP_OK; ki++) {
-                if (ki > 0 && clus[ki] == clus[ki - 1]) continue;
-                LaunchCfg lc = base;
-                lc.move_unroll = unrolls[pi];
-                lc.warps_per_block = warps[wi];
-                lc.pcg_block = blocks[bi];
-                lc.pcg_cluster_max = clus[ki];
-                b->lc = lc;
-                hp_status s = hpi::run_step(b->dev, b->lc, b->gas, st); // warm-up
-                if (s != HP_OK) { result = s; break; }
-                cudaEventRecord(e0, st);
-                for (int k = 0; k < 3 && s == HP_OK; k++) s = hpi::run_step(b->dev, b->lc, b->gas, st);
-                cudaEventRecord(e1, st);
-                if (s != HP_OK) { result = s; break; }
-                e = cudaEventSynchronize(e1);
-                if (e != cudaSuccess) { result = cuda_fail(e, "autotune trial"); break; }
-                float ms = 0;
-                cudaEventElapsedTime(&ms, e0, e1);
-                if (ms < best_ms) { best_ms = ms; best = lc; }
-                e = copy_all(false);
-                if (e != cudaSuccess) { result = cuda_fail(e, "autotune restore"); break; }
-            }
+        for (int wi = 0; wi < 3 && result == HP_OK; wi++)
+            for (int bi = 0; bi < 3 && result == HP_OK; bi++)
+                for (int ki = 0; ki < 3 && result == HP_OK; ki++) {
+                    if (ki > 0 && clus[ki] == clus[ki - 1]) continue;
+                    LaunchCfg lc = base;
+                    lc.move_unroll = unrolls[pi];
+                    lc.warps_per_block = warps[wi];
+                    lc.pcg_block = blocks[bi];
+                    lc.pcg_cluster_max = clus[ki];
+                    trial(lc);
+                }
+    // then the MCC cell grouping around the best of those
+    if (b->gas == GAS_AR) {
+        const LaunchCfg around = best;
+        const int groups[5] = {1, 2, 4, 8, 16};
+        for (int gi = 0; gi < 5 && result == HP_OK; gi++) {
+            if (groups[gi] == around.mcc_cells) continue;
+            LaunchCfg lc = around;
+            lc.mcc_cells = groups[gi];
+            trial(lc);
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     copy_all(false);

@@ -23,6 +23,8 @@ bool tune_valid(const hp_tune &t) {
     if (t.pcg_block < 64 || t.pcg_block > 512 || (t.pcg_block & 31)) return false;
     if (t.pcg_cluster_max < 1 || t.pcg_cluster_max > 16 || (t.pcg_cluster_max & (t.pcg_cluster_max - 1)))
         return false;
+    const int g = t.mcc_cells_per_warp;
+    if (g != 1 && g != 2 && g != 4 && g != 8 && g != 16) return false;
     return t.move_unroll == 1 || t.move_unroll == 2 || t.move_unroll == 4;
 }
 
@@ -812,6 +814,7 @@ hp_status hp_case_set_tune(hp_case *c, const hp_tune *t) {
     c->lc.pcg_block = t->pcg_block;
     c->lc.pcg_cluster_max = t->pcg_cluster_max;
     c->lc.move_unroll = t->move_unroll;
+    c->lc.mcc_cells = t->mcc_cells_per_warp;
     c->pcg_cluster = std::min(pcg_cluster_for_nodes(c->s.Gsize), t->pcg_cluster_max);
     if (c->graph) {
         cudaGraphExecDestroy(c->graph);
@@ -827,6 +830,7 @@ hp_status hp_case_get_tune(const hp_case *c, hp_tune *t) {
     t->pcg_block = c->lc.pcg_block;
     t->pcg_cluster_max = c->lc.pcg_cluster_max;
     t->move_unroll = c->lc.move_unroll;
+    t->mcc_cells_per_warp = c->lc.mcc_cells;
     return HP_OK;
 }
 

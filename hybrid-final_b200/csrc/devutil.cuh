@@ -57,21 +57,58 @@ __device__ __forceinline__ int lower_lane_hits(unsigned mask4, unsigned lt, int 
 // reference reads one row past the table when log10(E) equals the last grid
 // point exactly; the index is clamped here.
 // (the same for every reaction set: one column per channel)
-__device__ __forceinline__ float xsec_lookup(const DevCase &d, int ch, float engy) {
-    if (engy == 0) return 0.0f;
+// Where an energy falls on that grid.  A collider evaluates it once and reads
+// every channel of its ladder from it; each channel value is computed with
+// the same operations as a lookup of that channel alone.
+struct XsecPos {
+    const float *row; // table row of the lower grid point (or the clamped end)
+    float a1, a2;     // interpolation weights (mode 3)
+    float tail;       // exp(-(log10 E - last grid point)) (mode 2)
+    int mode;         // 0: E == 0; 1: below the grid; 2: above it; 3: inside
+    int W;            // row width
+};
+
+__device__ __forceinline__ XsecPos xsec_pos(const DevCase &d, float engy) {
+    XsecPos p;
+    p.W = d.xw;
+    p.row = d.xsec;
+    p.a1 = p.a2 = p.tail = 0.f;
+    if (engy == 0) {
+        p.mode = 0;
+        return p;
+    }
     const float lengy = hp_log10f(engy);
     const float *t = d.xsec;
-    const int W = d.xw;
-    const float xe0 = t[0], xeN = t[(d.n_logx - 1) * W];
-    if (lengy < xe0) return t[2 + ch];
-    if (lengy > xeN) return t[(d.n_logx - 1) * W + 2 + ch] * 0.1f * hp_expf(-1 * (lengy - xeN));
+    const float xe0 = t[0], xeN = t[(d.n_logx - 1) * p.W];
+    if (lengy < xe0) {
+        p.mode = 1;
+        return p;
+    }
+    if (lengy > xeN) {
+        p.mode = 2;
+        p.row = t + (d.n_logx - 1) * p.W;
+        p.tail = hp_expf(-1 * (lengy - xeN));
+        return p;
+    }
     const float ee1 = d.idlogx * (lengy - xe0);
     int ee2 = (int)ee1;
     if (ee2 > d.n_logx - 2) ee2 = d.n_logx - 2;
     if (ee2 < 0) ee2 = 0; // NaN energy: keep the read inside the table
-    const float a1 = ee1 - ee2;
-    const float a2 = 1 - a1;
-    return a2 * t[ee2 * W + 2 + ch] + a1 * t[(ee2 + 1) * W + 2 + ch];
+    p.a1 = ee1 - ee2;
+    p.a2 = 1 - p.a1;
+    p.row = t + ee2 * p.W;
+    p.mode = 3;
+    return p;
+}
+
+__device__ __forceinline__ float xsec_at(const XsecPos &p, int ch) {
+    if (p.mode == 3) return p.a2 * p.row[2 + ch] + p.a1 * p.row[p.W + 2 + ch];
+    if (p.mode == 2) return p.row[2 + ch] * 0.1f * p.tail;
+    return p.mode == 1 ? p.row[2 + ch] : 0.0f;
+}
+
+__device__ __forceinline__ float xsec_lookup(const DevCase &d, int ch, float engy) {
+    return xsec_at(xsec_pos(d, engy), ch);
 }
 
 // dev_maxwellv (src/cuda_mcc.cu:139-147); cos/sin of 2*pi*Rphi in turns

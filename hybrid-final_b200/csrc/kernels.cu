@@ -555,9 +555,10 @@ __global__ void __launch_bounds__(SORT_MAXW * 32) k_sort_count(const DevCase *__
 constexpr int MCC_TPB = 256;
 constexpr int MCC_RING = 256; // >= 128 new entries per pass + 31 pending
 
-
-__device__ __forceinline__ void mcc_ion_collide(const DevCase &d, const DevSpecies &ion, size_t q, hp_stream &rs,
-                                                float bvel, unsigned *cnt_ch) {
+// one ion that passed the null-collision test; returns the channel tallied
+// (5 charge exchange, 6 scattering) or -1 for a null collision
+__device__ __forceinline__ int mcc_ion_collide(const DevCase &d, const DevSpecies &ion, size_t q, hp_stream &rs,
+                                               float bvel) {
     const int nn = (int)((d.nvel - 1) * hp_stream_next(&rs));
     float vnx, vny, vnz;
     {
@@ -571,34 +572,38 @@ __device__ __forceinline__ void mcc_ion_collide(const DevCase &d, const DevSpeci
     const float engy = ion.Escale * dum;
     const float vel = sqrtf(dum);
     const float R1 = hp_stream_next(&rs) * d.sigv[2] / vel;
-    float SumSigma = xsec_lookup(d, 5, engy);
+    const XsecPos xp = xsec_pos(d, engy);
+    float SumSigma = xsec_at(xp, 5);
     float ox, oy, oz;
+    int ch = -1;
     if (R1 <= SumSigma) {
         ox = vnx; oy = vny; oz = vnz;
-        cnt_ch[5]++;
-    } else if (R1 <= (SumSigma += xsec_lookup(d, 6, engy))) {
+        ch = 5;
+    } else if (R1 <= (SumSigma += xsec_at(xp, 6))) {
         const float a = hp_stream_next(&rs);
         const float b = hp_stream_next(&rs);
         newvel_ionsc_dev(VX, VY, VZ, vel, a, b);
         ox = VX + vnx; oy = VY + vny; oz = VZ + vnz;
-        cnt_ch[6]++;
+        ch = 6;
     } else {
-        ox = vx; oy = vy; oz = vz;
+        return -1; // velocity unchanged
     }
     ion.vx[q] = ox;
     ion.vy[q] = oy;
     ion.vz[q] = oz;
+    return ch;
 }
 
 struct NewPair {
     float x, y, evx, evy, evz, ivx, ivy, ivz;
 };
 
-// one electron that passed the null-collision test with draw R1; returns
-// true when it ionised (the new electron/ion pair in np)
-__device__ __forceinline__ bool mcc_el_collide(const DevCase &d, const DevSpecies &el, size_t q, hp_stream &rs,
-                                               float R1, float P1, float bvel, unsigned *cnt_ch, NewPair &np) {
-    int colltype = 1;
+// one electron that passed the null-collision test with draw R1; returns the
+// channel tallied (0-4; 3 and 4 ionise, the new electron/ion pair in np) or
+// -1 for a null collision
+__device__ __forceinline__ int mcc_el_collide(const DevCase &d, const DevSpecies &el, size_t q, hp_stream &rs,
+                                              float R1, float P1, float bvel, NewPair &np) {
+    int colltype = 1, ch = -1;
     const int target = (R1 <= P1) ? 0 : 1;
     float VX = el.vx[q], VY = el.vy[q], VZ = el.vz[q];
     const float dum = VX * VX + VY * VY + VZ * VZ;
@@ -606,187 +611,174 @@ __device__ __forceinline__ bool mcc_el_collide(const DevCase &d, const DevSpecie
     VX /= vel; VY /= vel; VZ /= vel;
     float engy = el.Escale * dum;
     float rengy = 0.f, vel2 = 0.f;
+    const XsecPos xp = xsec_pos(d, engy);
     if (target == 0) {
         const float R2 = hp_stream_next(&rs) * d.sigv[0] / vel;
-        float SumSigma = xsec_lookup(d, 0, engy);
+        float SumSigma = xsec_at(xp, 0);
         if (R2 <= SumSigma) {
             colltype = 0;
-            cnt_ch[0]++;
-        } else if (engy > d.th[1] && R2 <= (SumSigma += xsec_lookup(d, 1, engy))) {
+            ch = 0;
+        } else if (engy > d.th[1] && R2 <= (SumSigma += xsec_at(xp, 1))) {
             colltype = 0;
             engy -= d.th[1];
             vel = sqrtf(fabsf(engy) / el.Escale);
-            cnt_ch[1]++;
-        } else if (engy > d.th[2] && R2 <= (SumSigma += xsec_lookup(d, 2, engy))) {
+            ch = 1;
+        } else if (engy > d.th[2] && R2 <= (SumSigma += xsec_at(xp, 2))) {
             colltype = 0;
             engy -= d.th[2];
             vel = sqrtf(fabsf(engy) / el.Escale);
-            cnt_ch[2]++;
-        } else if (engy > d.th[3] && R2 <= (SumSigma += xsec_lookup(d, 3, engy))) {
+            ch = 2;
+        } else if (engy > d.th[3] && R2 <= (SumSigma += xsec_at(xp, 3))) {
             colltype = 2;
-            engy -= d.th[3];
-            const float u = hp_stream_next(&rs);
-            rengy = (float)(10.0 * (double)hp_tanf_q1(u * hp_atanf((float)(engy / 20.0))));
-            engy -= rengy;
-            vel = sqrtf(fabsf(rengy) / el.Escale);
-            vel2 = sqrtf(fabsf(engy) / el.Escale);
-            cnt_ch[3]++;
+            ch = 3;
         }
     } else {
         const float R2 = hp_stream_next(&rs) * d.sigv[1] / vel;
-        const float SumSigma = xsec_lookup(d, 4, engy);
-        if (engy > d.th[4] && R2 <= SumSigma) {
+        if (engy > d.th[4] && R2 <= xsec_at(xp, 4)) {
             colltype = 2;
-            engy -= d.th[4];
-            const float u = hp_stream_next(&rs);
-            rengy = (float)(10.0 * (double)hp_tanf_q1(u * hp_atanf((float)(engy / 20.0))));
-            engy -= rengy;
-            vel = sqrtf(fabsf(rengy) / el.Escale);
-            vel2 = sqrtf(fabsf(engy) / el.Escale);
-            cnt_ch[4]++;
+            ch = 4;
         }
     }
-    if (colltype == 0) {
-        const float a = hp_stream_next(&rs);
-        const float b = hp_stream_next(&rs);
-        anewvel_dev(engy, vel, VX, VY, VZ, a, b);
-        el.vx[q] = VX;
-        el.vy[q] = VY;
-        el.vz[q] = VZ;
-        return false;
+    if (colltype == 1) return -1; // null collision: velocity unchanged
+    if (colltype == 2) {          // ionisation: energy split (src/cuda_mccAr.cu:120-170)
+        engy -= d.th[ch];
+        const float u = hp_stream_next(&rs);
+        rengy = (float)(10.0 * (double)hp_tanf_q1(u * hp_atanf((float)(engy / 20.0))));
+        engy -= rengy;
+        vel = sqrtf(fabsf(rengy) / el.Escale);
+        vel2 = sqrtf(fabsf(engy) / el.Escale);
+        np.x = el.x[q];
+        np.y = el.y[q];
+        np.evx = VX; np.evy = VY; np.evz = VZ;
+        {
+            const float a = hp_stream_next(&rs);
+            const float b = hp_stream_next(&rs);
+            anewvel_dev(rengy, vel, np.evx, np.evy, np.evz, a, b);
+        }
+        np.ivx = VX; np.ivy = VY; np.ivz = VZ;
+        {
+            const int nn = (int)((d.nvel - 1) * hp_stream_next(&rs));
+            const float a = hp_stream_next(&rs);
+            const float b = hp_stream_next(&rs);
+            maxwellv_dev(np.ivx, np.ivy, np.ivz, d.vsave[nn], bvel, a, b);
+        }
+        vel = vel2; // the primary scatters with the energy left
     }
-    if (colltype != 2) return false; // null collision: velocity unchanged
-    np.x = el.x[q];
-    np.y = el.y[q];
-    np.evx = VX; np.evy = VY; np.evz = VZ;
-    {
-        const float a = hp_stream_next(&rs);
-        const float b = hp_stream_next(&rs);
-        anewvel_dev(rengy, vel, np.evx, np.evy, np.evz, a, b);
-    }
-    np.ivx = VX; np.ivy = VY; np.ivz = VZ;
-    {
-        const int nn = (int)((d.nvel - 1) * hp_stream_next(&rs));
-        const float a = hp_stream_next(&rs);
-        const float b = hp_stream_next(&rs);
-        maxwellv_dev(np.ivx, np.ivy, np.ivz, d.vsave[nn], bvel, a, b);
-    }
-    {
-        const float a = hp_stream_next(&rs);
-        const float b = hp_stream_next(&rs);
-        anewvel_dev(engy, vel2, VX, VY, VZ, a, b);
-    }
+    const float a = hp_stream_next(&rs);
+    const float b = hp_stream_next(&rs);
+    anewvel_dev(engy, vel, VX, VY, VZ, a, b);
     el.vx[q] = VX;
     el.vy[q] = VY;
     el.vz[q] = VZ;
-    return true;
+    return ch;
 }
 
-__global__ void __launch_bounds__(MCC_TPB) k_mcc_ar(const DevCase *__restrict__ cases,
-                                                    const int *__restrict__ item_start, int ncases, int items) {
-    __shared__ int ring_s[MCC_TPB / 32][MCC_RING];
-    const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31;
-    if (warp >= items) return;
-    int *ring = ring_s[threadIdx.x >> 5];
-    const int ci = find_case(item_start, ncases, warp);
-    const DevCase &d = cases[ci];
-    const int c = warp - item_start[ci];
-    const int i = c / d.ncy, j = c - i * d.ncy;
-    const int node = i * d.ngy + j;
-    const float P1 = d.prob[c], P2 = d.prob[d.C + c], Pion = d.prob[2 * d.C + c];
+// The cells one warp works on, with what its lanes need while colliding.
+struct MccCell {
+    int c, ne, ni, add; // cell, electrons and ions before the step, births so far
+    float P1, P2, Pion, bvel;
+};
+
+#ifndef MCC_MINB
+#define MCC_MINB 3 // 80 registers: three 256-thread blocks per SM
+#endif
+
+// Ions of up to G consecutive cells of one case, then their electrons.  Each
+// queue entry is (slot | cell-in-group << 24, test draw); the queue is
+// drained 32 colliders at a time, so the cells of a group share collision
+// batches.  A cell's new pairs are appended behind its own particles in
+// queue order, which is the cell's particle order.
+template <int G>
+__device__ __forceinline__ void mcc_ar_cells(const DevCase &d, int c0, int n, int2 *ring, MccCell *cs,
+                                             unsigned *tally, int lane, unsigned lt, bool &overflow) {
     const uint32_t step = (uint32_t)(*d.tstep);
-    const float bvel = d.back_vel1[node];
-    const unsigned lt = lanemask_lt();
-    unsigned cnt_ch[7] = {0, 0, 0, 0, 0, 0, 0};
-    // ---- ions: test (4 slots per lane), queue, collide 32 at a time
+    const DevSpecies &el = d.sp[0];
     const DevSpecies &ion = d.sp[1];
-    const int ni = ion.cnt[c];
-    const size_t ibase = (size_t)c * ion.cap;
+    if (lane < n) {
+        const int c = c0 + lane;
+        const int i = c / d.ncy, j = c - i * d.ncy;
+        MccCell m;
+        m.c = c;
+        m.ne = el.cnt[c];
+        m.ni = ion.cnt[c];
+        m.add = 0;
+        m.P1 = d.prob[c];
+        m.P2 = d.prob[d.C + c];
+        m.Pion = d.prob[2 * d.C + c];
+        m.bvel = d.back_vel1[i * d.ngy + j];
+        cs[lane] = m;
+    }
+    for (int k = lane; k < G * 8; k += 32) tally[k] = 0u;
+    __syncwarp();
     int head = 0, tail = 0;
-    for (int k0 = 0; k0 < ni || tail > head; k0 += 128) {
-        if (k0 < ni) {
+    // queue the slots of `hits` (four per lane, slot k + t) behind the tail
+    auto enqueue = [&](unsigned hits, int k, int cl, const float *R) {
+        int total;
+        int pos = tail + lower_lane_hits(hits, lt, total);
+#pragma unroll
+        for (int t = 0; t < 4; t++)
+            if ((hits >> t) & 1u) ring[(pos++) & (MCC_RING - 1)] = make_int2((k + t) | (cl << 24), __float_as_int(R[t]));
+        tail += total;
+        __syncwarp();
+    };
+    // ---- ions: test four slots per lane from one Philox block, queue, collide
+    auto ion_batch = [&]() {
+        const int e = head + lane;
+        if (e < tail) {
+            const int2 ent = ring[e & (MCC_RING - 1)];
+            const int k = ent.x & 0xFFFFFF, q = ent.x >> 24;
+            const int c = cs[q].c;
+            hp_stream rs;
+            hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, 1u);
+            const int ch = mcc_ion_collide(d, ion, (size_t)c * ion.cap + k, rs, cs[q].bvel);
+            if (ch >= 0) atomicAdd(&tally[q * 8 + ch], 1u);
+        }
+        head = min(head + 32, tail);
+        __syncwarp();
+    };
+    for (int cl = 0; cl < n; cl++) {
+        const int c = cs[cl].c, ni = cs[cl].ni;
+        const float Pion = cs[cl].Pion;
+        for (int k0 = 0; k0 < ni; k0 += 128) {
             const int k = k0 + 4 * lane;
             unsigned hits = 0;
+            float R[4] = {0.f, 0.f, 0.f, 0.f};
             if (k < ni) {
                 const hp_u4 u = hp_test_block(d.seed, (uint32_t)(k >> 2), (uint32_t)c, step, 1u, 0u);
 #pragma unroll
                 for (int t = 0; t < 4; t++)
                     if (k + t < ni && hp_u01(hp_word(u, (uint32_t)t)) <= Pion) hits |= 1u << t;
             }
-            int total;
-            int pos = tail + lower_lane_hits(hits, lt, total);
-#pragma unroll
-            for (int t = 0; t < 4; t++)
-                if ((hits >> t) & 1u) ring[(pos++) & (MCC_RING - 1)] = k + t;
-            tail += total;
-        }
-        __syncwarp();
-        const bool last = k0 + 128 >= ni;
-        while (tail - head >= 32 || (last && tail > head)) {
-            const int e = head + lane;
-            if (e < tail) {
-                const int k = ring[e & (MCC_RING - 1)];
-                hp_stream rs;
-                hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, 1u);
-                mcc_ion_collide(d, ion, ibase + k, rs, bvel, cnt_ch);
-            }
-            head = min(head + 32, tail);
-            __syncwarp();
+            enqueue(hits, k, cl, R);
+            while (tail - head >= 32) ion_batch();
         }
     }
-    // ---- electrons: queue entries are slot | sub-cycle of the hit + 1 << 20
-    const DevSpecies &el = d.sp[0];
-    const int ne = el.cnt[c];
-    const size_t ebase = (size_t)c * el.cap;
-    int add = 0;
-    bool overflow = false;
-    head = tail = 0;
-    for (int k0 = 0; k0 < ne || tail > head; k0 += 128) {
-        if (k0 < ne) {
-            const int k = k0 + 4 * lane;
-            unsigned hits = 0;
-            int used[4] = {0, 0, 0, 0};
-            if (k < ne) {
-                const unsigned live = k + 4 <= ne ? 0xFu : (1u << (ne - k)) - 1u;
-                for (int jj = 0; jj < d.mcc_n && (hits != live); jj++) {
-                    const hp_u4 u = hp_test_block(d.seed, (uint32_t)(k >> 2), (uint32_t)c, step, 0u, (uint32_t)jj);
-#pragma unroll
-                    for (int t = 0; t < 4; t++)
-                        if (((live & ~hits) >> t) & 1u && hp_u01(hp_word(u, (uint32_t)t)) < P2) {
-                            hits |= 1u << t;
-                            used[t] = jj + 1;
-                        }
-                }
-            }
-            int total;
-            int pos = tail + lower_lane_hits(hits, lt, total);
-#pragma unroll
-            for (int t = 0; t < 4; t++)
-                if ((hits >> t) & 1u) ring[(pos++) & (MCC_RING - 1)] = (k + t) | (used[t] << 20);
-            tail += total;
+    while (tail > head) ion_batch();
+    // ---- electrons: up to mcc_n test blocks (sub-cycles) per four slots
+    auto el_batch = [&]() {
+        const int e = head + lane;
+        int q = -1, ch = -1;
+        NewPair np;
+        if (e < tail) {
+            const int2 ent = ring[e & (MCC_RING - 1)];
+            const int k = ent.x & 0xFFFFFF;
+            q = ent.x >> 24;
+            const int c = cs[q].c;
+            hp_stream rs;
+            hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, 0u);
+            ch = mcc_el_collide(d, el, (size_t)c * el.cap + k, rs, __int_as_float(ent.y), cs[q].P1, cs[q].bvel, np);
+            if (ch >= 0) atomicAdd(&tally[q * 8 + ch], 1u);
         }
-        __syncwarp();
-        const bool last = k0 + 128 >= ne;
-        while (tail - head >= 32 || (last && tail > head)) {
-            const int e = head + lane;
-            bool create = false;
-            NewPair np;
-            if (e < tail) {
-                const int ent = ring[e & (MCC_RING - 1)];
-                const int k = ent & 0xFFFFF, used = ent >> 20;
-                const float R1 =
-                    hp_test_draw(d.seed, (uint32_t)k, (uint32_t)c, step, 0u, (uint32_t)(used - 1));
-                hp_stream rs;
-                hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, 0u);
-                create = mcc_el_collide(d, el, ebase + k, rs, R1, P1, bvel, cnt_ch, np);
-            }
-            const unsigned bc = __ballot_sync(FULL, create);
+        const bool create = ch >= 3;
+        const unsigned bc = __ballot_sync(FULL, create);
+        if (bc) {
+            const unsigned same = __match_any_sync(FULL, q); // lanes of the same cell (contiguous)
             if (create) {
-                const int off = add + __popc(bc & lt);
-                const int se = ne + off, sn = ni + off;
+                const MccCell m = cs[q];
+                const int off = m.add + __popc(bc & same & lt);
+                const int se = m.ne + off, sn = m.ni + off;
                 if (se < el.cap && sn < ion.cap) {
-                    const size_t qe = ebase + se, qi = ibase + sn;
+                    const size_t qe = (size_t)m.c * el.cap + se, qi = (size_t)m.c * ion.cap + sn;
                     el.x[qe] = np.x; el.y[qe] = np.y;
                     el.vx[qe] = np.evx; el.vy[qe] = np.evy; el.vz[qe] = np.evz;
                     ion.x[qi] = np.x; ion.y[qi] = np.y;
@@ -795,25 +787,74 @@ __global__ void __launch_bounds__(MCC_TPB) k_mcc_ar(const DevCase *__restrict__ 
                     overflow = true;
                 }
             }
-            add += __popc(bc);
-            head = min(head + 32, tail);
             __syncwarp();
+            if (q >= 0 && (same & lt) == 0) cs[q].add += __popc(bc & same);
+        }
+        head = min(head + 32, tail);
+        __syncwarp();
+    };
+    for (int cl = 0; cl < n; cl++) {
+        const int c = cs[cl].c, ne = cs[cl].ne;
+        const float P2 = cs[cl].P2;
+        for (int k0 = 0; k0 < ne; k0 += 128) {
+            const int k = k0 + 4 * lane;
+            unsigned hits = 0;
+            float R[4] = {0.f, 0.f, 0.f, 0.f};
+            if (k < ne) {
+                const unsigned live = k + 4 <= ne ? 0xFu : (1u << (ne - k)) - 1u;
+                for (int jj = 0; jj < d.mcc_n && (hits != live); jj++) {
+                    const hp_u4 u = hp_test_block(d.seed, (uint32_t)(k >> 2), (uint32_t)c, step, 0u, (uint32_t)jj);
+#pragma unroll
+                    for (int t = 0; t < 4; t++) {
+                        const float r = hp_u01(hp_word(u, (uint32_t)t));
+                        if (((live & ~hits) >> t) & 1u && r < P2) {
+                            hits |= 1u << t;
+                            R[t] = r;
+                        }
+                    }
+                }
+            }
+            enqueue(hits, k, cl, R);
+            while (tail - head >= 32) el_batch();
         }
     }
-    if (__any_sync(FULL, overflow)) {
-        if (lane == 0) atomicOr(d.status, ST_OVERFLOW);
-        const int room = min(el.cap - ne, ion.cap - ni);
-        add = min(add, room);
-    }
-    if (lane == 0) {
-        el.cnt[c] = ne + add;
-        ion.cnt[c] = ni + add;
+    while (tail > head) el_batch();
+    __syncwarp();
+    // counts with this step's pairs (clamped to the room left when a cell overflowed)
+    if (lane < n) {
+        const MccCell m = cs[lane];
+        const int add = min(m.add, min(el.cap - m.ne, ion.cap - m.ni));
+        el.cnt[m.c] = m.ne + add;
+        ion.cnt[m.c] = m.ni + add;
     }
     // per-cell channel tallies (the reference's MCCR per node)
-#pragma unroll
-    for (int ch = 0; ch < 7; ch++) {
-        const unsigned tot = __reduce_add_sync(FULL, cnt_ch[ch]);
-        if (lane == ch && tot) d.mcc_count[(size_t)c * 8 + ch] += tot;
+    for (int k = lane; k < n * 8; k += 32)
+        if (tally[k]) d.mcc_count[(size_t)cs[k >> 3].c * 8 + (k & 7)] += tally[k];
+    __syncwarp();
+}
+
+template <int G>
+__global__ void __launch_bounds__(MCC_TPB, MCC_MINB) k_mcc_ar(const DevCase *__restrict__ cases,
+                                                              const int *__restrict__ item_start, int ncases,
+                                                              int items) {
+    __shared__ int2 ring_s[MCC_TPB / 32][MCC_RING];
+    __shared__ MccCell cell_s[MCC_TPB / 32][G];
+    __shared__ unsigned tally_s[MCC_TPB / 32][G * 8];
+    const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int first = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5) * G;
+    if (first >= items) return;
+    const unsigned lt = lanemask_lt();
+    const int end = min(first + G, items);
+    bool overflow = false;
+    // a group that straddles two cases of a batch runs as two groups
+    for (int g0 = first; g0 < end;) {
+        const int ci = find_case(item_start, ncases, g0);
+        const int g1 = min(end, item_start[ci + 1]);
+        const DevCase &d = cases[ci];
+        overflow = false;
+        mcc_ar_cells<G>(d, g0 - item_start[ci], g1 - g0, ring_s[wl], cell_s[wl], tally_s[wl], lane, lt, overflow);
+        if (__any_sync(FULL, overflow) && lane == 0) atomicOr(d.status, ST_OVERFLOW);
+        g0 = g1;
     }
 }
 
@@ -1397,8 +1438,13 @@ cudaError_t launch_sort(const DevCase *cases, const int *item_start, int ncases,
 cudaError_t launch_mcc_ar(const DevCase *cases, const int *item_start, int ncases, int items, const LaunchCfg &lc,
                           cudaStream_t st) {
     if (items <= 0) return cudaSuccess;
-    (void)lc;
-    k_mcc_ar<<<blocks_for((long long)items * 32, MCC_TPB), MCC_TPB, 0, st>>>(cases, item_start, ncases, items);
+    const int g = lc.mcc_cells;
+    const long long threads = (long long)((items + g - 1) / g) * 32;
+    if (g == 1) k_mcc_ar<1><<<blocks_for(threads, MCC_TPB), MCC_TPB, 0, st>>>(cases, item_start, ncases, items);
+    else if (g == 2) k_mcc_ar<2><<<blocks_for(threads, MCC_TPB), MCC_TPB, 0, st>>>(cases, item_start, ncases, items);
+    else if (g == 8) k_mcc_ar<8><<<blocks_for(threads, MCC_TPB), MCC_TPB, 0, st>>>(cases, item_start, ncases, items);
+    else if (g == 16) k_mcc_ar<16><<<blocks_for(threads, MCC_TPB), MCC_TPB, 0, st>>>(cases, item_start, ncases, items);
+    else k_mcc_ar<4><<<blocks_for(threads, MCC_TPB), MCC_TPB, 0, st>>>(cases, item_start, ncases, items);
     return cudaGetLastError();
 }
 

@@ -287,10 +287,11 @@ __device__ void electron_collide(const DevCase &d, float vx, float vy, float vz,
     const int k1 = GAS == 2 ? c_erung_start[t + 1] : c_orung_start[t + 1];
     float sum = 0.f;
     bool hit = false;
+    const XsecPos xp = xsec_pos(d, engy); // engy is fixed until the hit
     for (int k = k0; k < k1; k++) {
         const Rung r = rung[k];
         if (!(engy > d.th[r.ch])) continue;
-        sum = sum + xsec_lookup(d, r.ch, engy);
+        sum = sum + xsec_at(xp, r.ch);
         if (!(R1 <= sum)) continue;
         hit = true;
         o.ch = r.ch;
@@ -478,9 +479,10 @@ __device__ void ion_collide(const DevCase &d, int s, float vx, float vy, float v
     const float R1 = hp_stream_next(&rs) * d.sigv[sv] / vel;
     int what = I_NULL;
     float sum = 0.f;
+    const XsecPos xp = xsec_pos(d, engy);
     for (int k = 0; k < nr; k++) {
         if (!(engy > d.th[ch[k]])) continue;
-        const float xs = xsec_lookup(d, ch[k], engy);
+        const float xs = xsec_at(xp, ch[k]);
         sum = (k > 0 && cum) ? sum + xs : xs;
         if (R1 <= sum) {
             what = act[k];

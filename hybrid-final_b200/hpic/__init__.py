@@ -57,7 +57,7 @@ class CaseInfo(C.Structure):
 
 class Tune(C.Structure):
     _fields_ = [("warps_per_block_particles", C.c_int), ("pcg_block", C.c_int), ("pcg_cluster_max", C.c_int),
-                ("move_unroll", C.c_int)]
+                ("move_unroll", C.c_int), ("mcc_cells_per_warp", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -256,6 +256,8 @@ typedef struct hp_tune {
     int pcg_cluster_max;           /* PCG: largest cluster per case */
     int move_unroll;               /* Move: chunks of 32 particles loaded per iteration: 1 (with a one-chunk
                                       prefetch), 2 or 4 */
+    int mcc_cells_per_warp;        /* MCC (Ar): consecutive cells per warp sharing collision batches: 1, 2, 4, 8
+                                      or 16 */
 } hp_tune;
 hp_status hp_batch_set_tune(hp_batch *b, const hp_tune *t);
 hp_status hp_batch_get_tune(hp_batch *b, hp_tune *t);

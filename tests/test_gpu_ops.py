@@ -111,8 +111,11 @@ def test_move_and_sort(name, move_mode):
 
 
 @pytest.mark.parametrize("name", list(DECKS))
-def test_mcc(name):
+@pytest.mark.parametrize("group", [1, 2, 4, 8, 16])
+def test_mcc(name, group):
+    """Ar MCC with 1-16 consecutive cells per warp sharing collision batches."""
     case, o = pair(name)
+    case.set_tune(mcc_cells_per_warp=group)
     for t in (1, 2, 3):
         case.set_tstep(t)
         case.MCC()
@@ -304,9 +307,12 @@ def test_graph_replay_matches_operator_calls():
             assert same(x, y)
 
 
-def test_batch_equals_alone():
-    """A case advanced inside a batch gives the same bits as alone."""
-    decks = [DECKS["ar_17x9"], DECKS["ar_33x17_hv"], DECKS["ar_65x33"]]
+@pytest.mark.parametrize("group", [1, 16])
+def test_batch_equals_alone(group):
+    """A case advanced inside a batch gives the same bits as alone, also when
+    MCC cell groups straddle two cases (the 19x10 deck has 162 cells)."""
+    decks = [(ccp_deck(19, 10, 0.005625, 0.0028125, ppc=12), 31), DECKS["ar_17x9"], DECKS["ar_33x17_hv"],
+             DECKS["ar_65x33"]]
     alone = []
     for deck, seed in decks:
         c = hpic.Case(deck, seed=seed)
@@ -314,6 +320,7 @@ def test_batch_equals_alone():
         alone.append(c)
     mixed = [hpic.Case(deck, seed=seed) for deck, seed in decks]
     b = hpic.Batch(mixed)
+    b.set_tune(mcc_cells_per_warp=group)
     b.step(10)
     b.close()
     for a, m in zip(alone, mixed):
