@@ -405,6 +405,35 @@ __global__ void __launch_bounds__(512) k_move_u(const DevCase *__restrict__ case
 //   k_sort_count (warp per destination cell) new count, then the far movers.
 constexpr int SORT_MAXW = 16; // warps per block, at most
 
+// Memory-level parallelism: every read a source warp needs (its first
+// SORT_PRE chunks of 32 movers, the nine destinations' counts and the 81
+// pair counts) is issued before the first result is used, so a warp waits
+// for one round trip instead of one per dependent step.
+#ifndef SORT_PRE
+#define SORT_PRE 4
+#endif
+
+struct MoverRegs {
+    float x, y, vx, vy, vz;
+    int code;
+};
+
+__device__ __forceinline__ MoverRegs load_mover(const DevSpecies &sp, size_t base, int cap, int r, int m) {
+    MoverRegs v;
+    v.code = -1;
+    v.x = v.y = v.vx = v.vy = v.vz = 0.f;
+    if (r < m) {
+        const size_t q = base + (size_t)(cap - 1 - r);
+        v.code = (int)sp.code[q];
+        v.x = sp.x[q];
+        v.y = sp.y[q];
+        v.vx = sp.vx[q];
+        v.vy = sp.vy[q];
+        v.vz = sp.vz[q];
+    }
+    return v;
+}
+
 __global__ void __launch_bounds__(SORT_MAXW * 32) k_sort_push(const DevCase *__restrict__ cases,
                                                         const int *__restrict__ item_start, int ncases, int items) {
     __shared__ int s_off[SORT_MAXW][9], s_lim[SORT_MAXW][9];
@@ -420,56 +449,80 @@ __global__ void __launch_bounds__(SORT_MAXW * 32) k_sort_push(const DevCase *__r
     if (m == 0) return;
     const int cap = sp.cap, ncy = d.ncy;
     const int i = c / ncy, j = c - i * ncy;
-    // destination D = code (di+1)*3 + (dj+1): its stayers and slot limit
+    const size_t base = (size_t)c * cap;
+    // issue every read first: the movers ...
+    MoverRegs mv[SORT_PRE];
+#pragma unroll
+    for (int h = 0; h < SORT_PRE; h++) mv[h] = load_mover(sp, base, cap, h * 32 + lane, m);
+    // ... destination D = code (di+1)*3 + (dj+1): its stayers and slot limit ...
+    int off9 = 0, lim9 = 0;
     if (lane < 9) {
         const int Di = i + lane / 3 - 1, Dj = j + lane % 3 - 1;
-        const bool ok = Di >= 0 && Di < d.ncx && Dj >= 0 && Dj < ncy;
-        const int D = Di * ncy + Dj;
-        s_off[wl][lane] = ok ? sp.cnt[D] : 0;
-        s_lim[wl][lane] = ok ? cap - sp.nmov[D] : 0;
-    }
-    __syncwarp();
-    // + movers sent to D by its other neighbours S < c; (D, S) pair p = 9*Dd + Ss,
-    // S = D + (Ss/3 - 1, Ss%3 - 1), and S's code for D is 8 - Ss
-    for (int p = lane; p < 81; p += 32) {
-        const int Dd = p / 9, Ss = p - 9 * Dd;
-        const int Di = i + Dd / 3 - 1, Dj = j + Dd % 3 - 1;
-        const int Si = Di + Ss / 3 - 1, Sj = Dj + Ss % 3 - 1;
-        const int S = Si * ncy + Sj;
-        if (Di >= 0 && Di < d.ncx && Dj >= 0 && Dj < ncy && Si >= 0 && Si < d.ncx && Sj >= 0 && Sj < ncy && S < c) {
-            const int v = sp.dcount[(size_t)S * 9 + (8 - Ss)];
-            if (v) atomicAdd(&s_off[wl][Dd], v);
+        if (Di >= 0 && Di < d.ncx && Dj >= 0 && Dj < ncy) {
+            const int D = Di * ncy + Dj;
+            off9 = sp.cnt[D];
+            lim9 = cap - sp.nmov[D];
         }
     }
+    // ... and the movers sent to D by its other neighbours S < c; (D, S) pair
+    // p = 9*Dd + Ss, S = D + (Ss/3 - 1, Ss%3 - 1), and S's code for D is 8 - Ss
+    int pv[3];
+#pragma unroll
+    for (int t = 0; t < 3; t++) {
+        const int p = lane + 32 * t;
+        pv[t] = 0;
+        if (p < 81) {
+            const int Dd = p / 9, Ss = p - 9 * Dd;
+            const int Di = i + Dd / 3 - 1, Dj = j + Dd % 3 - 1;
+            const int Si = Di + Ss / 3 - 1, Sj = Dj + Ss % 3 - 1;
+            const int S = Si * ncy + Sj;
+            if (Di >= 0 && Di < d.ncx && Dj >= 0 && Dj < ncy && Si >= 0 && Si < d.ncx && Sj >= 0 && Sj < ncy && S < c)
+                pv[t] = sp.dcount[(size_t)S * 9 + (8 - Ss)];
+        }
+    }
+    if (lane < 9) {
+        s_off[wl][lane] = off9;
+        s_lim[wl][lane] = lim9;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int t = 0; t < 3; t++)
+        if (pv[t]) atomicAdd(&s_off[wl][(lane + 32 * t) / 9], pv[t]);
     __syncwarp();
     const unsigned lt = lanemask_lt();
-    const size_t base = (size_t)c * cap;
     int run[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     bool overflow = false;
-    for (int r0 = 0; r0 < m; r0 += 32) {
-        const int r = r0 + lane;
-        const size_t q = base + (size_t)(cap - 1 - r);
-        const int code = r < m ? (int)sp.code[q] : -1;
+    auto place = [&](const MoverRegs &v) {
         int rank = 0;
 #pragma unroll
         for (int D = 0; D < 9; D++) {
-            const unsigned b = __ballot_sync(FULL, code == D);
-            if (code == D) rank = run[D] + __popc(b & lt);
+            const unsigned b = __ballot_sync(FULL, v.code == D);
+            if (v.code == D) rank = run[D] + __popc(b & lt);
             run[D] += __popc(b);
         }
-        if (code >= 0 && code < 9) {
-            const int slot = s_off[wl][code] + rank;
-            if (slot < s_lim[wl][code]) {
-                const size_t dst = (size_t)(c + (code / 3 - 1) * ncy + (code % 3 - 1)) * cap + (size_t)slot;
-                sp.x[dst] = sp.x[q];
-                sp.y[dst] = sp.y[q];
-                sp.vx[dst] = sp.vx[q];
-                sp.vy[dst] = sp.vy[q];
-                sp.vz[dst] = sp.vz[q];
+        if (v.code >= 0 && v.code < 9) {
+            const int slot = s_off[wl][v.code] + rank;
+            if (slot < s_lim[wl][v.code]) {
+                const size_t dst = (size_t)(c + (v.code / 3 - 1) * ncy + (v.code % 3 - 1)) * cap + (size_t)slot;
+                sp.x[dst] = v.x;
+                sp.y[dst] = v.y;
+                sp.vx[dst] = v.vx;
+                sp.vy[dst] = v.vy;
+                sp.vz[dst] = v.vz;
             } else {
                 overflow = true;
             }
         }
+    };
+#pragma unroll
+    for (int h = 0; h < SORT_PRE; h++)
+        if (h * 32 < m) place(mv[h]);
+    for (int r0 = SORT_PRE * 32; r0 < m; r0 += SORT_PRE * 32) {
+#pragma unroll
+        for (int h = 0; h < SORT_PRE; h++) mv[h] = load_mover(sp, base, cap, r0 + h * 32 + lane, m);
+#pragma unroll
+        for (int h = 0; h < SORT_PRE; h++)
+            if (r0 + h * 32 < m) place(mv[h]);
     }
     if (__any_sync(FULL, overflow) && lane == 0) atomicOr(d.status, ST_OVERFLOW);
 }

@@ -122,107 +122,78 @@ __device__ __forceinline__ float ion_acc(float prev, bool first, float e) {
     return first ? (float)(1.0 - (double)e) : (float)((double)prev + 1.0 - (double)e);
 }
 
-__device__ void cell_prob(const DevCase &d, int node, CellProb &P) {
-    const int G = d.G;
-    const float bd1 = d.back_den1[node], bd2 = d.back_den2[node];
-    const float F0 = d.fluid_den[node], F1 = d.fluid_den[G + node], F2 = d.fluid_den[2 * G + node];
-    const float F3 = d.fluid_den[3 * G + node], F4 = d.fluid_den[4 * G + node];
-    // charged densities from the last deposit: den * np2c * idx * idy, in this order
-    auto nq = [&](int s, float sig, float dtx) {
-        float t = -1 * dtx;
-        t = t * sig;
-        t = t * (float)d.den[(size_t)s * G + node];
-        t = t * d.sp[s].np2c;
-        t = t * d.idx;
-        t = t * d.idy;
-        return hp_expf(t);
-    };
-    const float dtm = d.dt_mcc, dt = d.dt;
-    const float *sv = d.sigv;
-    float *e = P.p[0];
-    e[0] = 1.0f - xe(dtm, sv[0], bd1);
-    e[1] = e[0] + 1.0f - xe(dtm, sv[1], F0);
-    e[2] = e[1] + 1.0f - xe(dtm, sv[2], bd2);
-    e[3] = e[2] + 1.0f - xe(dtm, sv[3], F1);
-    e[4] = e[3] + 1.0f - xe(dtm, sv[4], F2);
-    e[5] = e[4] + 1.0f - nq(4, sv[5], dtm);
-    e[6] = e[5] + 1.0f - nq(2, sv[6], dtm);
-    e[7] = e[6] + 1.0f - xe(dtm, sv[7], F3);
-    e[8] = e[7] + 1.0f - xe(dtm, sv[8], F4);
-    P.n[0] = 9;
-    float *a = P.p[1]; // Ar+: Ar, O2
-    a[0] = ion_acc(0, true, xe(dt, sv[23], bd1));
-    a[1] = ion_acc(a[0], false, xe(dt, sv[24], bd2));
-    P.n[1] = 2;
-    float *o2 = P.p[2]; // O2+: OP, O2, O2A, O2B, Ar
-    o2[0] = ion_acc(0, true, xe(dt, sv[14], F3));
-    o2[1] = ion_acc(o2[0], false, xe(dt, sv[15], bd2));
-    o2[2] = ion_acc(o2[1], false, xe(dt, sv[16], F1));
-    o2[3] = ion_acc(o2[2], false, xe(dt, sv[17], F2));
-    o2[4] = ion_acc(o2[3], false, xe(dt, sv[18], bd1));
-    P.n[2] = 5;
-    float *op = P.p[3]; // O+: O2, OP, O2A, O2B
-    op[0] = ion_acc(0, true, xe(dt, sv[19], bd2));
-    op[1] = ion_acc(op[0], false, xe(dt, sv[20], F3));
-    op[2] = ion_acc(op[1], false, xe(dt, sv[21], F1));
-    op[3] = ion_acc(op[2], false, xe(dt, sv[22], F2));
-    P.n[3] = 4;
-    float *om = P.p[4]; // O-: O2, OP, O2+, O+, O2A
-    om[0] = ion_acc(0, true, xe(dt, sv[9], bd2));
-    om[1] = ion_acc(om[0], false, xe(dt, sv[10], F3));
-    om[2] = ion_acc(om[1], false, nq(2, sv[11], dt));
-    om[3] = ion_acc(om[2], false, nq(3, sv[12], dt));
-    om[4] = ion_acc(om[3], false, xe(dt, sv[13], F1));
-    P.n[4] = 5;
-}
+// One survival factor exp(-dt sigma_v n) of the check: time step (1: the
+// electron sub-step dt_mcc, 0: dt), sigma-v maximum, and the density it
+// multiplies (0 Ar background, 1 O2 background, 2-6 fluid species 0-4,
+// 8 + s charged species s from the last deposit).
+struct Term {
+    unsigned char sub, sv, src;
+};
+// ArO2_Collision_Check (src/cuda_mccArO2.cu:1130-1190), per species in target
+// order: e (O2-scaled targets Ar, Ar*, O2, O2A, O2B, O-, O2+, OP, OD),
+// Ar+ (Ar, O2), O2+ (OP, O2, O2A, O2B, Ar), O+ (O2, OP, O2A, O2B),
+// O- (O2, OP, O2+, O+, O2A)
+__constant__ Term c_terms_aro2[25] = {
+    {1, 0, 0}, {1, 1, 2}, {1, 2, 1}, {1, 3, 3}, {1, 4, 4}, {1, 5, 12}, {1, 6, 10}, {1, 7, 5}, {1, 8, 6},
+    {0, 23, 0}, {0, 24, 1},
+    {0, 14, 5}, {0, 15, 1}, {0, 16, 3}, {0, 17, 4}, {0, 18, 0},
+    {0, 19, 1}, {0, 20, 5}, {0, 21, 3}, {0, 22, 4},
+    {0, 9, 1}, {0, 10, 5}, {0, 11, 10}, {0, 12, 11}, {0, 13, 3}};
+__constant__ int c_first_aro2[6] = {0, 9, 11, 16, 20, 25};
+// O2Collision_Check (src/cuda_mccO2.cu:867-911): e (O2, O2A, O2B, O-, O2+,
+// OP, OD), O2+ on the electron sub-step (OP, O2, O2A, O2B), O+ (O2, OP, O2A,
+// O2B), O- (O2, OP, O2+, O+, O2A)
+__constant__ Term c_terms_o2[20] = {
+    {1, 0, 0}, {1, 1, 2}, {1, 2, 3}, {1, 3, 11}, {1, 4, 9}, {1, 5, 4}, {1, 6, 5},
+    {1, 12, 4}, {1, 13, 0}, {1, 14, 2}, {1, 15, 3},
+    {0, 16, 0}, {0, 17, 4}, {0, 18, 2}, {0, 19, 3},
+    {0, 7, 0}, {0, 8, 4}, {0, 9, 9}, {0, 10, 10}, {0, 11, 2}};
+__constant__ int c_first_o2[5] = {0, 7, 11, 15, 20};
 
-// the O2 set (O2Collision_Check, src/cuda_mccO2.cu:867-911): species e,
-// O2+, O+, O-; the O2+ line uses the electron sub-step, as the reference does
-__device__ void cell_prob_o2(const DevCase &d, int node, CellProb &P) {
-    const int G = d.G;
-    const float bd1 = d.back_den1[node];
-    const float F0 = d.fluid_den[node], F1 = d.fluid_den[G + node], F2 = d.fluid_den[2 * G + node];
-    const float F3 = d.fluid_den[3 * G + node];
-    auto nq = [&](int s, float sig, float dtx) {
-        float t = -1 * dtx;
-        t = t * sig;
-        t = t * (float)d.den[(size_t)s * G + node];
-        t = t * d.sp[s].np2c;
-        t = t * d.idx;
-        t = t * d.idy;
-        return hp_expf(t);
-    };
-    const float dtm = d.dt_mcc, dt = d.dt;
-    const float *sv = d.sigv;
-    float *e = P.p[0];
-    e[0] = 1.0f - xe(dtm, sv[0], bd1);
-    e[1] = e[0] + 1.0f - xe(dtm, sv[1], F0);
-    e[2] = e[1] + 1.0f - xe(dtm, sv[2], F1);
-    e[3] = e[2] + 1.0f - nq(3, sv[3], dtm);
-    e[4] = e[3] + 1.0f - nq(1, sv[4], dtm);
-    e[5] = e[4] + 1.0f - xe(dtm, sv[5], F2);
-    e[6] = e[5] + 1.0f - xe(dtm, sv[6], F3);
-    P.n[0] = 7;
-    float *a = P.p[1]; // O2+: OP, O2, O2A, O2B
-    a[0] = ion_acc(0, true, xe(dtm, sv[12], F2));
-    a[1] = ion_acc(a[0], false, xe(dtm, sv[13], bd1));
-    a[2] = ion_acc(a[1], false, xe(dtm, sv[14], F0));
-    a[3] = ion_acc(a[2], false, xe(dtm, sv[15], F1));
-    P.n[1] = 4;
-    float *b = P.p[2]; // O+: O2, OP, O2A, O2B
-    b[0] = ion_acc(0, true, xe(dt, sv[16], bd1));
-    b[1] = ion_acc(b[0], false, xe(dt, sv[17], F2));
-    b[2] = ion_acc(b[1], false, xe(dt, sv[18], F0));
-    b[3] = ion_acc(b[2], false, xe(dt, sv[19], F1));
-    P.n[2] = 4;
-    float *m = P.p[3]; // O-: O2, OP, O2+, O+, O2A
-    m[0] = ion_acc(0, true, xe(dt, sv[7], bd1));
-    m[1] = ion_acc(m[0], false, xe(dt, sv[8], F2));
-    m[2] = ion_acc(m[1], false, nq(1, sv[9], dt));
-    m[3] = ion_acc(m[2], false, nq(2, sv[10], dt));
-    m[4] = ion_acc(m[3], false, xe(dt, sv[11], F0));
-    P.n[3] = 5;
-    P.n[4] = 1;
+// The collision probabilities of one cell, cumulative over the targets (the
+// electron sums run in float with 1.0f, the ion sums in double as the
+// reference's 1.0 literal makes them).  Lane l evaluates factor l; lane 0
+// accumulates them in the reference's order into shared memory.
+template <int GAS>
+__device__ void cell_prob(const DevCase &d, int node, CellProb &P, int lane) {
+    constexpr int NT = GAS == 2 ? 25 : 20;
+    constexpr int NSPC = GAS == 2 ? 5 : 4;
+    const Term *terms = GAS == 2 ? c_terms_aro2 : c_terms_o2;
+    const int *first = GAS == 2 ? c_first_aro2 : c_first_o2;
+    float x = 0.f;
+    if (lane < NT) {
+        const Term T = terms[lane];
+        const float dtx = T.sub ? d.dt_mcc : d.dt;
+        const float sig = d.sigv[T.sv];
+        if (T.src >= 8) { // charged density: den * np2c * idx * idy, in this order
+            const int sp = T.src - 8;
+            float t = -1 * dtx;
+            t = t * sig;
+            t = t * (float)d.den[(size_t)sp * d.G + node];
+            t = t * d.sp[sp].np2c;
+            t = t * d.idx;
+            t = t * d.idy;
+            x = hp_expf(t);
+        } else {
+            const float dens = T.src == 0 ? d.back_den1[node]
+                             : T.src == 1 ? d.back_den2[node]
+                                          : d.fluid_den[(size_t)(T.src - 2) * d.G + node];
+            x = xe(dtx, sig, dens);
+        }
+    }
+    float acc = 0.f;
+    int s = 0;
+#pragma unroll
+    for (int k = 0; k < NT; k++) {
+        const float xk = __shfl_sync(FULL, x, k);
+        while (k >= first[s + 1]) s++;
+        const bool head = k == first[s];
+        if (s == 0) acc = head ? 1.0f - xk : acc + 1.0f - xk;
+        else acc = ion_acc(acc, head, xk);
+        if (lane == 0) P.p[s][k - first[s]] = acc;
+    }
+    if (lane < 5) P.n[lane] = lane < NSPC ? first[lane + 1] - first[lane] : 1;
+    __syncwarp();
 }
 
 // target of a hit: the first cumulative probability R1 does not exceed
@@ -510,13 +481,18 @@ __device__ void ion_collide(const DevCase &d, int s, float vx, float vy, float v
 
 __device__ __forceinline__ bool is_hole(float x) { return x != x; }
 
+#ifndef OXY_MINB
+#define OXY_MINB 5 // 96 registers: five 128-thread blocks per SM
+#endif
+
 template <int GAS>
-__global__ void __launch_bounds__(OXY_TPB) k_mcc_oxy(const DevCase *__restrict__ cases,
+__global__ void __launch_bounds__(OXY_TPB, OXY_MINB) k_mcc_oxy(const DevCase *__restrict__ cases,
                                                      const int *__restrict__ item_start, int ncases, int items) {
     constexpr int NSP = GAS == 2 ? 5 : 4;
     constexpr int OMINUS = GAS == 2 ? 4 : 3;
     __shared__ int ring_s[OXY_TPB / 32][OXY_RING];
     __shared__ int holes_s[OXY_TPB / 32][NSP_ARO2][HOLE_CAP];
+    __shared__ CellProb prob_s[OXY_TPB / 32];
     const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
     if (warp >= items) return;
@@ -529,9 +505,8 @@ __global__ void __launch_bounds__(OXY_TPB) k_mcc_oxy(const DevCase *__restrict__
     const uint32_t step = (uint32_t)(*d.tstep);
     const float bv1 = d.back_vel1[node], bv2 = d.back_vel2[node];
     const unsigned lt = lanemask_lt();
-    CellProb P;
-    if (GAS == 2) cell_prob(d, node, P);
-    else cell_prob_o2(d, node, P);
+    CellProb &P = prob_s[wl];
+    cell_prob<GAS>(d, node, P, lane);
     // the reference's O2 launch covers Gsize threads, so only its electrons
     // collide (src/cuda_mcc.cu:76-77); mcc_all_species extends it to every species
     const int nactive = (GAS == 2 || d.mcc_all_species) ? NSP : 1;
