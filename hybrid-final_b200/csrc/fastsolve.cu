@@ -53,11 +53,13 @@ __global__ void __launch_bounds__(256) k_fs_resid(const DevCase *__restrict__ ca
 }
 
 // Grouped C = A B (row-major, contiguous) over a list of problems.  32x32
-// output tile per CTA of 128 threads (2x4 outputs per thread), so that even a
-// single 511 x 255 case spreads over ~128 SMs; 32-deep K slices staged in
-// shared memory, the next slice fetched into registers while the current one
-// is multiplied.  Each output is accumulated in k order from zero.
-constexpr int GT = 32, GK = 32, GTHREADS = 128;
+// output tile per CTA of 256 threads (2x2 outputs per thread: eight warps a
+// tile, so that a single 511 x 255 case keeps ~1000 warps busy); 32-deep K
+// slices staged in shared memory, the next slice fetched into registers while
+// the current one is multiplied.  Each output is accumulated in k order from
+// zero, whatever the tiling.
+constexpr int GT = FS_TILE, GK = 32, GTHREADS = 256;
+static_assert(GT == 32, "the thread layout assumes 32x32 tiles");
 
 __global__ void __launch_bounds__(GTHREADS) k_gemm(const GemmProb *__restrict__ probs, int nprob) {
     int lo = 0, hi = nprob;
@@ -77,14 +79,14 @@ __global__ void __launch_bounds__(GTHREADS) k_gemm(const GemmProb *__restrict__ 
     // As[k][m] (row stride 34 keeps float2 reads aligned, 2-way store conflicts)
     __shared__ __align__(16) float As[GK][GT + 2];
     __shared__ __align__(16) float Bs[GK][GT];
-    const int tid = threadIdx.x, tx = tid & 7, ty = tid >> 3;
-    // this thread's loads: rows (idx >> 5) = tid/32 + 4q, column lane = tid & 31
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    // this thread's loads: rows tid/32 + 8q, column lane = tid & 31
     const int lr = tid >> 5, lc = tid & 31;
-    float ra[8], rb[8];
+    float ra[4], rb[4];
     auto fetch = [&](int k0) {
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
-            const int r = lr + 4 * q;
+        for (int q = 0; q < 4; q++) {
+            const int r = lr + 8 * q;
             const int gm = m0 + r, gk = k0 + lc;
             ra[q] = (gm < M && gk < K) ? A[(size_t)gm * K + gk] : 0.0f;
             const int gkb = k0 + r, gn = n0 + lc;
@@ -93,33 +95,33 @@ __global__ void __launch_bounds__(GTHREADS) k_gemm(const GemmProb *__restrict__ 
     };
     auto stage = [&]() {
 #pragma unroll
-        for (int q = 0; q < 8; q++) {
-            const int r = lr + 4 * q;
+        for (int q = 0; q < 4; q++) {
+            const int r = lr + 8 * q;
             As[lc][r] = ra[q];
             Bs[r][lc] = rb[q];
         }
     };
-    float acc[2][4];
-#pragma unroll
-    for (int a = 0; a < 2; a++)
-#pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = 0.0f;
+    float c00 = 0.0f, c01 = 0.0f, c10 = 0.0f, c11 = 0.0f;
+    auto mac = [&](int kk) {
+        const float2 av = *reinterpret_cast<const float2 *>(&As[kk][ty * 2]);
+        const float2 bv = *reinterpret_cast<const float2 *>(&Bs[kk][tx * 2]);
+        c00 = c00 + av.x * bv.x;
+        c01 = c01 + av.x * bv.y;
+        c10 = c10 + av.y * bv.x;
+        c11 = c11 + av.y * bv.y;
+    };
     fetch(0);
     stage();
     __syncthreads();
     for (int k0 = 0; k0 < K; k0 += GK) {
         const bool more = k0 + GK < K;
         if (more) fetch(k0 + GK);
-        const int kmax = min(GK, K - k0);
-        for (int kk = 0; kk < kmax; kk++) {
-            const float2 av = *reinterpret_cast<const float2 *>(&As[kk][ty * 2]);
-            const float4 bv = *reinterpret_cast<const float4 *>(&Bs[kk][tx * 4]);
-            const float a2[2] = {av.x, av.y};
-            const float b4[4] = {bv.x, bv.y, bv.z, bv.w};
+        if (more) {
 #pragma unroll
-            for (int a = 0; a < 2; a++)
-#pragma unroll
-                for (int b = 0; b < 4; b++) acc[a][b] = acc[a][b] + a2[a] * b4[b];
+            for (int kk = 0; kk < GK; kk++) mac(kk);
+        } else { // the last slice: exactly K - k0 terms, no padded ones
+            const int kmax = K - k0;
+            for (int kk = 0; kk < kmax; kk++) mac(kk);
         }
         __syncthreads();
         if (more) {
@@ -127,18 +129,19 @@ __global__ void __launch_bounds__(GTHREADS) k_gemm(const GemmProb *__restrict__ 
             __syncthreads();
         }
     }
+    const float cv[2][2] = {{c00, c01}, {c10, c11}};
 #pragma unroll
     for (int a = 0; a < 2; a++) {
         const int gm = m0 + ty * 2 + a;
         if (gm >= M) continue;
 #pragma unroll
-        for (int b = 0; b < 4; b++) {
-            const int gn = n0 + tx * 4 + b;
+        for (int b = 0; b < 2; b++) {
+            const int gn = n0 + tx * 2 + b;
             if (gn >= N) continue;
             const size_t o = (size_t)gm * N + gn;
-            if (P.epi == 0) P.C[o] = acc[a][b];
-            else if (P.epi == 1) P.C[o] = acc[a][b] * P.S[o];
-            else P.x64[(size_t)(P.i0 + gn) * P.ngy + (P.j0 + gm)] += (double)acc[a][b];
+            if (P.epi == 0) P.C[o] = cv[a][b];
+            else if (P.epi == 1) P.C[o] = cv[a][b] * P.S[o];
+            else P.x64[(size_t)(P.i0 + gn) * P.ngy + (P.j0 + gm)] += (double)cv[a][b];
         }
     }
 }
