@@ -132,7 +132,12 @@ __device__ __forceinline__ int walk(const Geo d, int &i, int &j, float &lx, floa
 // 3x3 neighbourhood, CODE_FAR beyond it (also listed in the destination's
 // bucket as source<<18 | r), CODE_ABSORBED when it left
 // the domain.
-__global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
+#ifdef MOVE_MINB
+#define MOVE_BOUNDS __launch_bounds__(256, MOVE_MINB)
+#else
+#define MOVE_BOUNDS __launch_bounds__(512)
+#endif
+__global__ void MOVE_BOUNDS k_move(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
                                               int ncases, int items) {
     const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
@@ -157,6 +162,10 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
     float vx = sp.vx[base + lane];
     float vy = sp.vy[base + lane];
     float vz = sp.vz[base + lane];
+    // an interior cell whose 3x3 neighbourhood is all plasma (ghost code 0):
+    // a particle that ends in a neighbour after one wrap needs no walk
+    const int g3 = lane < 9 ? d.sidx[(i + lane / 3) * (d.ncy + 2) + (j + lane % 3)] : 0;
+    const bool open3 = __ballot_sync(FULL, g3 != 0) == 0u && i >= 1 && i + 1 < d.ncx && j >= 1 && j + 1 < d.ncy;
     if (n == 0) {
         if (lane == 0) sp.nmov[c] = 0;
         if (lane < 9) sp.dcount[(size_t)c * 9 + lane] = 0;
@@ -201,7 +210,21 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
         ly = __fmaf_rn(mvY, dtdy, ly);
         const bool out = act && (ly >= 1 || ly < 0 || lx >= 1 || lx < 0);
         int code = 4, fi = i, fj = j;
-        if (out) {
+        bool near = false;
+        if (out && open3) { // the walk's first crossing with ghost code 0: a wrap, no flip
+            const float wy = ly >= 1 ? ly - 1.0f : ly < 0 ? ly + 1.0f : ly;
+            const float wx = lx >= 1 ? lx - 1.0f : lx < 0 ? lx + 1.0f : lx;
+            if (!(wy >= 1 || wy < 0 || wx >= 1 || wx < 0)) {
+                const int dj = ly >= 1 ? 1 : ly < 0 ? -1 : 0, di = lx >= 1 ? 1 : lx < 0 ? -1 : 0;
+                lx = wx;
+                ly = wy;
+                fi = i + di;
+                fj = j + dj;
+                code = (di + 1) * 3 + (dj + 1);
+                near = true;
+            }
+        }
+        if (out && !near) {
             int cond = -1;
             const int r = walk(geo_of(d), fi, fj, lx, ly, mvX, mvY, cond);
             if (r) {
@@ -212,13 +235,13 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
                 const int ddi = fi - i, ddj = fj - j;
                 code = (ddi >= -1 && ddi <= 1 && ddj >= -1 && ddj <= 1) ? (ddi + 1) * 3 + (ddj + 1) : CODE_FAR;
             }
-            if (code < 9) {
-                const int q3 = code / 3;
-                const unsigned long long one = 1ull << (21 * (code - 3 * q3));
-                if (q3 == 0) pk0 += one;
-                else if (q3 == 1) pk1 += one;
-                else pk2 += one;
-            }
+        }
+        if (out && code < 9) {
+            const int q3 = code / 3;
+            const unsigned long long one = 1ull << (21 * (code - 3 * q3));
+            if (q3 == 0) pk0 += one;
+            else if (q3 == 1) pk1 += one;
+            else pk2 += one;
         }
         const unsigned bout = __ballot_sync(FULL, out);
         const int before = m + __popc(bout & lt);
@@ -931,15 +954,31 @@ __global__ void __launch_bounds__(512) k_deposit_cells(const DevCase *__restrict
     const int w = warp - item_start[ci];
     const int s = w / d.C, c = w - s * d.C;
     const DevSpecies &sp = d.sp[s];
-    const int n = sp.cnt[c];
     const size_t base = (size_t)c * sp.cap;
+    // the count and the first chunk are independent loads (cap >= 32); later
+    // chunks are loaded four at a time before any is added.  Each lane adds
+    // its slots lane, lane + 32, ... in that order.
+    const int n = sp.cnt[c];
+    const float x0 = sp.x[base + lane], y0 = sp.y[base + lane];
     float WS = 0.f, WN = 0.f, ES = 0.f, EN = 0.f;
-    for (int k = lane; k < n; k += 32) {
-        const float lx = sp.x[base + k], ly = sp.y[base + k];
+    auto add = [&](float lx, float ly) {
         WS += (1 - lx) * (1 - ly);
         WN += (1 - lx) * ly;
         ES += lx * (1 - ly);
         EN += lx * ly;
+    };
+    if (lane < n) add(x0, y0);
+    for (int k0 = 32; k0 < n; k0 += 128) {
+        float xs[4], ys[4];
+#pragma unroll
+        for (int h = 0; h < 4; h++) {
+            const int k = k0 + 32 * h + lane;
+            xs[h] = k < n ? sp.x[base + k] : 0.f;
+            ys[h] = k < n ? sp.y[base + k] : 0.f;
+        }
+#pragma unroll
+        for (int h = 0; h < 4; h++)
+            if (k0 + 32 * h + lane < n) add(xs[h], ys[h]);
     }
     const double a = warp_sum_d(WS), b = warp_sum_d(WN), e = warp_sum_d(ES), f = warp_sum_d(EN);
     if (lane == 0) d.cw[s][c] = make_double4(a, b, e, f);
