@@ -120,6 +120,18 @@ __device__ __forceinline__ int walk(const Geo d, int &i, int &j, float &lx, floa
     return 0;
 }
 
+// asynchronous global -> shared copies (LDGSTS): 4 bytes per lane, committed
+// per chunk; a lane waits for its own groups and reads only what it copied
+__device__ __forceinline__ void cp_async4(float *smem, const float *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // ------------------------------------------------------------------ Move
 // MoveE_Basic (src/cuda_Move.cu:181-270): bilinear gather of the node field,
 // v += Ascale E, x += v dt/dx in cell units (the reference's sums of
@@ -132,13 +144,16 @@ __device__ __forceinline__ int walk(const Geo d, int &i, int &j, float &lx, floa
 // 3x3 neighbourhood, CODE_FAR beyond it (also listed in the destination's
 // bucket as source<<18 | r), CODE_ABSORBED when it left
 // the domain.
-#ifdef MOVE_MINB
-#define MOVE_BOUNDS __launch_bounds__(256, MOVE_MINB)
-#else
-#define MOVE_BOUNDS __launch_bounds__(512)
-#endif
-__global__ void MOVE_BOUNDS k_move(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
-                                              int ncases, int items) {
+// The particle loads are asynchronous copies into a ring of R chunk slots per
+// warp in shared memory, so that R - 1 chunks of every warp are in flight
+// without holding registers.
+constexpr int MOVE_RING = 4;
+
+template <int R>
+__global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
+                                                   const int *__restrict__ item_start, int ncases, int items) {
+    extern __shared__ float move_ring_s[];
+    float *ring = move_ring_s + (threadIdx.x >> 5) * (R * 5 * 32);
     const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (warp >= items) return;
@@ -157,16 +172,27 @@ __global__ void MOVE_BOUNDS k_move(const DevCase *__restrict__ cases, const int 
     const int n = sp.cnt[c];
     const float ex_ws = d.Ex[node], ex_wn = d.Ex[node + 1], ex_es = d.Ex[node + d.ngy], ex_en = d.Ex[node + d.ngy + 1];
     const float ey_ws = d.Ey[node], ey_wn = d.Ey[node + 1], ey_es = d.Ey[node + d.ngy], ey_en = d.Ey[node + d.ngy + 1];
-    float lx = sp.x[base + lane];
-    float ly = sp.y[base + lane];
-    float vx = sp.vx[base + lane];
-    float vy = sp.vy[base + lane];
-    float vz = sp.vz[base + lane];
+    // chunk q of the cell goes to ring slot q % R, one asynchronous 4-byte copy
+    // per lane and array, one commit group per chunk (possibly empty)
+    auto issue = [&](int k0, int lim) {
+        const int kk = k0 + lane;
+        float *sl = ring + ((k0 >> 5) % R) * 160;
+        if (kk < lim) {
+            cp_async4(sl + lane, sp.x + base + kk);
+            cp_async4(sl + 32 + lane, sp.y + base + kk);
+            cp_async4(sl + 64 + lane, sp.vx + base + kk);
+            cp_async4(sl + 96 + lane, sp.vy + base + kk);
+            cp_async4(sl + 128 + lane, sp.vz + base + kk);
+        }
+        cp_async_commit();
+    };
+    issue(0, 32); // slots 0..31 of a cell are always inside the pool (cap >= 32)
     // an interior cell whose 3x3 neighbourhood is all plasma (ghost code 0):
     // a particle that ends in a neighbour after one wrap needs no walk
     const int g3 = lane < 9 ? d.sidx[(i + lane / 3) * (d.ncy + 2) + (j + lane % 3)] : 0;
     const bool open3 = __ballot_sync(FULL, g3 != 0) == 0u && i >= 1 && i + 1 < d.ncx && j >= 1 && j + 1 < d.ncy;
     if (n == 0) {
+        cp_async_wait_all();
         if (lane == 0) sp.nmov[c] = 0;
         if (lane < 9) sp.dcount[(size_t)c * 9 + lane] = 0;
         return;
@@ -178,27 +204,27 @@ __global__ void MOVE_BOUNDS k_move(const DevCase *__restrict__ cases, const int 
             atomicOr(d.status, ST_OVERFLOW);
         }
         if (lane < 9) sp.dcount[(size_t)c * 9 + lane] = 0;
+        cp_async_wait_all();
         return;
     }
+#pragma unroll
+    for (int q = 1; q < R - 1; q++) issue(q * 32, n);
     const float As = sp.Ascale, dtdx = d.dt_dx, dtdy = d.dt_dy;
     const unsigned lt = lanemask_lt();
     int m = 0;
     // per-lane mover counts per destination code, three 21-bit fields per word
     unsigned long long pk0 = 0, pk1 = 0, pk2 = 0;
-    // software pipeline: the next chunk's loads are in flight while this one
-    // is pushed (stores only go to slots at or below the current chunk, or to
-    // the top region at or above cap - n >= n, so no unread slot is touched)
+    // R - 1 chunks in flight while one is pushed (stores only go to slots at
+    // or below the current chunk, or to the top region at or above
+    // cap - n >= n, so no slot still to be copied is touched)
     for (int k0 = 0; k0 < n; k0 += 32) {
         const int k = k0 + lane;
         const bool act = k < n;
-        float nlx = 0.f, nly = 0.f, nvx = 0.f, nvy = 0.f, nvz = 0.f;
-        if (k + 32 < n) {
-            nlx = sp.x[base + k + 32];
-            nly = sp.y[base + k + 32];
-            nvx = sp.vx[base + k + 32];
-            nvy = sp.vy[base + k + 32];
-            nvz = sp.vz[base + k + 32];
-        }
+        issue(k0 + (R - 1) * 32, n);
+        cp_async_wait<R - 1>();
+        const float *sl = ring + ((k0 >> 5) % R) * 160;
+        float lx = sl[lane], ly = sl[32 + lane], vx = sl[64 + lane], vy = sl[96 + lane];
+        const float vz = sl[128 + lane];
         // bilinear weights once, then fused multiply-adds (one rounding each)
         const float wx = 1 - lx, wy = 1 - ly;
         const float w00 = wx * wy, w01 = wx * ly, w10 = lx * wy, w11 = lx * ly;
@@ -264,8 +290,8 @@ __global__ void MOVE_BOUNDS k_move(const DevCase *__restrict__ cases, const int 
             }
         }
         m += __popc(bout);
-        lx = nlx; ly = nly; vx = nvx; vy = nvy; vz = nvz;
     }
+    cp_async_wait_all();
     if (lane == 0) {
         sp.cnt[c] = n - m;
         sp.nmov[c] = m;
@@ -425,7 +451,7 @@ __global__ void __launch_bounds__(512) k_move_u(const DevCase *__restrict__ case
 //   k_sort_push  (warp per source cell) slot of each near mover = stayers of
 //                the destination + movers sent to it by lower-index sources
 //                + rank among this source's movers to it;
-//   k_sort_count (warp per destination cell) new count, then the far movers.
+//   k_sort_count (lane per destination cell) new count, then the far movers.
 constexpr int SORT_MAXW = 16; // warps per block, at most
 
 // Memory-level parallelism: every read a source warp needs (its first
@@ -550,37 +576,50 @@ __global__ void __launch_bounds__(SORT_MAXW * 32) k_sort_push(const DevCase *__r
     if (__any_sync(FULL, overflow) && lane == 0) atomicOr(d.status, ST_OVERFLOW);
 }
 
+// One lane per destination cell (32 cells per warp): the new count is its
+// stayers plus the near movers addressed to it (nine dcount entries, all
+// loads independent); the cells with a far bucket are then finished one at a
+// time by the whole warp (bucket ordered by (source cell, r), then copied).
 __global__ void __launch_bounds__(SORT_MAXW * 32) k_sort_count(const DevCase *__restrict__ cases,
                                                          const int *__restrict__ item_start, int ncases, int items) {
     const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
-    if (warp >= items) return;
-    const int ci = find_case(item_start, ncases, warp);
-    const DevCase &d = cases[ci];
-    const int w = warp - item_start[ci];
-    const int s = w / d.C, c = w - s * d.C;
-    const DevSpecies &sp = d.sp[s];
-    const int cap = sp.cap, ncy = d.ncy;
-    const int i = c / ncy, j = c - i * ncy;
-    // near movers in: source S = c + (Ss/3 - 1, Ss%3 - 1) sends code 8 - Ss
-    int in = 0;
-    if (lane < 9) {
-        const int Si = i + lane / 3 - 1, Sj = j + lane % 3 - 1;
-        if (Si >= 0 && Si < d.ncx && Sj >= 0 && Sj < ncy) in = sp.dcount[(size_t)(Si * ncy + Sj) * 9 + (8 - lane)];
+    if (warp * 32 >= items) return;
+    const int item = warp * 32 + lane;
+    int ci = 0, s = 0, c = 0, out = 0, limit = 0, nf = 0;
+    if (item < items) {
+        ci = find_case(item_start, ncases, item);
+        const DevCase &d = cases[ci];
+        const int w = item - item_start[ci];
+        s = w / d.C;
+        c = w - s * d.C;
+        const DevSpecies &sp = d.sp[s];
+        const int ncy = d.ncy, i = c / ncy, j = c - i * ncy;
+        // near movers in: source S = c + (q/3 - 1, q%3 - 1) sends code 8 - q
+        int in = 0;
+#pragma unroll
+        for (int q = 0; q < 9; q++) {
+            const int Si = i + q / 3 - 1, Sj = j + q % 3 - 1;
+            if (Si >= 0 && Si < d.ncx && Sj >= 0 && Sj < ncy) in += sp.dcount[(size_t)(Si * ncy + Sj) * 9 + (8 - q)];
+        }
+        limit = sp.cap - sp.nmov[c];
+        out = sp.cnt[c] + in;
+        nf = d.far_in[(size_t)s * d.C + c];
     }
-    in = __reduce_add_sync(FULL, in);
-    const int limit = cap - sp.nmov[c];
-    int out = sp.cnt[c] + in;
     bool overflow = false;
-    // far movers: this cell's bucket, ordered by (source cell, r) with a
-    // bitonic network across the lanes (keys are distinct)
-    const size_t b = (size_t)s * d.C + c;
-    int nf = d.far_in[b];
-    if (nf) {
+    for (unsigned fm = __ballot_sync(FULL, nf > 0); fm; fm &= fm - 1) {
+        const int src = __ffs(fm) - 1;
+        const int fci = __shfl_sync(FULL, ci, src), fs = __shfl_sync(FULL, s, src), fc = __shfl_sync(FULL, c, src);
+        const int fout = __shfl_sync(FULL, out, src), flimit = __shfl_sync(FULL, limit, src);
+        const int fnf = min(__shfl_sync(FULL, nf, src), FAR_B); // Move flagged an overflow
+        const DevCase &d = cases[fci];
+        const DevSpecies &sp = d.sp[fs];
+        const int cap = sp.cap;
+        const size_t b = (size_t)fs * d.C + fc;
+        unsigned long long key = lane < fnf ? d.far_key[b * FAR_B + lane] : ~0ull;
         __syncwarp();
         if (lane == 0) d.far_in[b] = 0;
-        if (nf > FAR_B) nf = FAR_B; // Move flagged the overflow
-        unsigned long long key = lane < nf ? d.far_key[b * FAR_B + lane] : ~0ull;
+        // bitonic network across the lanes (keys are distinct)
 #pragma unroll
         for (int k = 2; k <= 32; k <<= 1)
 #pragma unroll
@@ -589,25 +628,33 @@ __global__ void __launch_bounds__(SORT_MAXW * 32) k_sort_count(const DevCase *__
                 const bool keep_min = ((lane & jj) == 0) == ((lane & k) == 0);
                 key = keep_min ? (o < key ? o : key) : (o > key ? o : key);
             }
-        if (lane < nf) {
-            const int slot = out + lane;
-            if (slot < limit) {
-                const int src = (int)(key >> 18), r = (int)(key & 0x3FFFF);
-                const size_t q = (size_t)src * cap + (size_t)(cap - 1 - r);
-                const size_t dst = (size_t)c * cap + (size_t)slot;
+        bool ov = false;
+        if (lane < fnf) {
+            const int slot = fout + lane;
+            if (slot < flimit) {
+                const int sc = (int)(key >> 18), r = (int)(key & 0x3FFFF);
+                const size_t q = (size_t)sc * cap + (size_t)(cap - 1 - r);
+                const size_t dst = (size_t)fc * cap + (size_t)slot;
                 sp.x[dst] = sp.x[q];
                 sp.y[dst] = sp.y[q];
                 sp.vx[dst] = sp.vx[q];
                 sp.vy[dst] = sp.vy[q];
                 sp.vz[dst] = sp.vz[q];
             } else {
-                overflow = true;
+                ov = true;
             }
         }
-        out += nf;
+        const bool any_ov = __any_sync(FULL, ov);
+        if (lane == src) {
+            out += fnf;
+            overflow |= any_ov;
+        }
     }
-    if (__any_sync(FULL, overflow) && lane == 0) atomicOr(d.status, ST_OVERFLOW);
-    if (lane == 0) sp.cnt[c] = out < limit ? out : limit;
+    if (item < items) {
+        const DevCase &d = cases[ci];
+        if (overflow) atomicOr(d.status, ST_OVERFLOW);
+        d.sp[s].cnt[c] = out < limit ? out : limit;
+    }
 }
 
 // ------------------------------------------------------------------ MCC (Ar)
@@ -1512,7 +1559,9 @@ cudaError_t launch_move(const DevCase *cases, const int *item_start, int ncases,
     const unsigned nb = blocks_for((long long)items * 32, tpb);
     if (lc.move_unroll == 2) k_move_u<2><<<nb, tpb, 0, st>>>(cases, item_start, ncases, items);
     else if (lc.move_unroll == 4) k_move_u<4><<<nb, tpb, 0, st>>>(cases, item_start, ncases, items);
-    else k_move<<<nb, tpb, 0, st>>>(cases, item_start, ncases, items);
+    else
+        k_move<MOVE_RING><<<nb, tpb, (size_t)(tpb / 32) * MOVE_RING * 5 * 32 * sizeof(float), st>>>(
+            cases, item_start, ncases, items);
     return cudaGetLastError();
 }
 
@@ -1523,7 +1572,8 @@ cudaError_t launch_sort(const DevCase *cases, const int *item_start, int ncases,
     k_sort_push<<<blocks_for((long long)items * 32, tpb), tpb, 0, st>>>(cases, item_start, ncases, items);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    k_sort_count<<<blocks_for((long long)items * 32, tpb), tpb, 0, st>>>(cases, item_start, ncases, items);
+    k_sort_count<<<blocks_for((long long)(items + 31) / 32 * 32, tpb), tpb, 0, st>>>(cases, item_start, ncases,
+                                                                                     items);
     return cudaGetLastError();
 }
 
