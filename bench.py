@@ -118,13 +118,22 @@ def dist_init(n_gpus):
     return rank, world, local, dist
 
 
-def allreduce(dist, v, op):
+def allreduce(dist, v, op, device="cuda"):
     if dist is None:
         return v
     import torch
-    t = torch.tensor([float(v)], device="cuda", dtype=torch.float64)
+    t = torch.tensor([float(v)], device=device, dtype=torch.float64)
     dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.SUM)
     return float(t.item())
+
+
+def replica_throughput(dist, units, ms, device="cuda"):
+    """Whole-job throughput of independent replicas: the units every rank
+    processed over the slowest rank's device time.  Returns (units/s, max ms,
+    total units)."""
+    ms_max = allreduce(dist, ms, "max", device)
+    units_all = allreduce(dist, units, "sum", device)
+    return units_all / (ms_max * 1e-3), ms_max, units_all
 
 
 def move_traffic(workload):
@@ -243,8 +252,7 @@ def run_ours(args, rank, world, local, dist):
     clk = clocks.stop()
     ms = e0.elapsed_time(e1)
     pushes = case.pushes() - p0
-    ms_max = allreduce(dist, ms, "max")
-    pushes_all = allreduce(dist, pushes, "sum")
+    _, ms_max, pushes_all = replica_throughput(dist, pushes, ms)
     status = case.status()
     resid = case.field_residual()
 
