@@ -358,7 +358,7 @@ hp_status build_device(hp_case *c) {
     TRY(dalloc(c, &h.ave_count, 1));
     TRY(dalloc(c, &h.eedf, HP_EEDF_BINS + 1));
     h.eedf_every = c->opts.eedf_every > 0 ? c->opts.eedf_every : 0;
-    TRY(dalloc(c, &h.pushes, 32));
+    TRY(dalloc(c, &h.pushes, 64));
     TRY(dalloc(c, &h.far_in, (size_t)s.nsp * C));
     TRY(dalloc(c, &h.far_key, (size_t)s.nsp * C * HP_FAR_BUCKET));
     h.move_mode = c->opts.move_mode;
@@ -988,6 +988,18 @@ hp_status hp_case_pushes(hp_case *c, int64_t *pushes) {
     int64_t t = 0;
     for (int k = 0; k < 32; k++) t += (int64_t)v[k];
     *pushes = t;
+    return HP_OK;
+}
+
+hp_status hp_case_slot_changes(hp_case *c, int64_t *changes) {
+    if (!c || !changes) return HP_ERR_ARG;
+    unsigned long long v[32];
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->last_stream));
+    CK(cudaMemcpy(v, c->h.pushes + 32, sizeof v, cudaMemcpyDeviceToHost));
+    int64_t t = 0;
+    for (int k = 0; k < 32; k++) t += (int64_t)v[k];
+    *changes = t;
     return HP_OK;
 }
 

@@ -96,7 +96,8 @@ struct DevCase {
     int64_t *ave_count;
     unsigned long long *eedf;       // [HP_EEDF_BINS+1] electron energy histogram since the last reset
     int eedf_every;                 // 0: off; k: sample every k-th step
-    unsigned long long *pushes;     // [32] particles pushed by Move, spread over 32 counters
+    unsigned long long *pushes;     // [64] particles pushed by Move, spread over 32 counters, then
+                                    // those of them whose slot changed (their vz was rewritten)
     unsigned long long *far_key;    // [nsp*C*HP_FAR_BUCKET] movers arriving from beyond the 3x3 neighbourhood
     int *far_in;                    // [nsp*C] entries in each bucket (cleared by Sort)
     int move_mode;                  // 0 one cell crossing per step (reference), 1 cross until inside a cell

@@ -170,11 +170,13 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
     // loads: issue them together (slots 0..31 of a cell are always inside the
     // pool, cap >= 32; lanes past the count are ignored)
     const int n = sp.cnt[c];
+    const int prev_m = sp.nmov[c]; // movers of the last step
     const float ex_ws = d.Ex[node], ex_wn = d.Ex[node + 1], ex_es = d.Ex[node + d.ngy], ex_en = d.Ex[node + d.ngy + 1];
     const float ey_ws = d.Ey[node], ey_wn = d.Ey[node + 1], ey_es = d.Ey[node + d.ngy], ey_en = d.Ey[node + d.ngy + 1];
     // chunk q of the cell goes to ring slot q % R, one asynchronous 4-byte copy
     // per lane and array, one commit group per chunk (possibly empty)
-    auto issue = [&](int k0, int lim) {
+    // (vz only when asked: a particle that keeps its slot keeps its vz)
+    auto issue = [&](int k0, int lim, bool with_vz) {
         const int kk = k0 + lane;
         float *sl = ring + ((k0 >> 5) % R) * 160;
         if (kk < lim) {
@@ -182,11 +184,11 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
             cp_async4(sl + 32 + lane, sp.y + base + kk);
             cp_async4(sl + 64 + lane, sp.vx + base + kk);
             cp_async4(sl + 96 + lane, sp.vy + base + kk);
-            cp_async4(sl + 128 + lane, sp.vz + base + kk);
+            if (with_vz) cp_async4(sl + 128 + lane, sp.vz + base + kk);
         }
         cp_async_commit();
     };
-    issue(0, 32); // slots 0..31 of a cell are always inside the pool (cap >= 32)
+    issue(0, 32, true); // slots 0..31 of a cell are always inside the pool (cap >= 32)
     // an interior cell whose 3x3 neighbourhood is all plasma (ghost code 0):
     // a particle that ends in a neighbour after one wrap needs no walk
     const int g3 = lane < 9 ? d.sidx[(i + lane / 3) * (d.ncy + 2) + (j + lane % 3)] : 0;
@@ -207,11 +209,14 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
         cp_async_wait_all();
         return;
     }
+    // a cell that had movers last step will most likely shift its particles
+    // again: copy vz ahead too; otherwise only the shifted ones read it
+    const bool eager_vz = prev_m > 0;
 #pragma unroll
-    for (int q = 1; q < R - 1; q++) issue(q * 32, n);
+    for (int q = 1; q < R - 1; q++) issue(q * 32, n, eager_vz);
     const float As = sp.Ascale, dtdx = d.dt_dx, dtdy = d.dt_dy;
     const unsigned lt = lanemask_lt();
-    int m = 0;
+    int m = 0, shifted = 0;
     // per-lane mover counts per destination code, three 21-bit fields per word
     unsigned long long pk0 = 0, pk1 = 0, pk2 = 0;
     // R - 1 chunks in flight while one is pushed (stores only go to slots at
@@ -220,11 +225,12 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
     for (int k0 = 0; k0 < n; k0 += 32) {
         const int k = k0 + lane;
         const bool act = k < n;
-        issue(k0 + (R - 1) * 32, n);
+        issue(k0 + (R - 1) * 32, n, eager_vz);
         cp_async_wait<R - 1>();
         const float *sl = ring + ((k0 >> 5) % R) * 160;
         float lx = sl[lane], ly = sl[32 + lane], vx = sl[64 + lane], vy = sl[96 + lane];
-        const float vz = sl[128 + lane];
+        const bool have_vz = k0 == 0 || eager_vz;
+        float vz = have_vz ? sl[128 + lane] : 0.f;
         // bilinear weights once, then fused multiply-adds (one rounding each)
         const float wx = 1 - lx, wy = 1 - ly;
         const float w00 = wx * wy, w01 = wx * ly, w10 = lx * wy, w11 = lx * ly;
@@ -271,6 +277,9 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
         }
         const unsigned bout = __ballot_sync(FULL, out);
         const int before = m + __popc(bout & lt);
+        const bool moved = act && (out || before != 0); // its slot changes
+        if (moved && !have_vz) vz = sp.vz[base + k];
+        shifted += __popc(__ballot_sync(FULL, moved));
         __syncwarp(); // every lane's loads of this chunk precede the in-place stores
         if (act) {
             const size_t dst = out ? base + (size_t)(cap - 1 - before) : base + (size_t)(k - before);
@@ -278,7 +287,7 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
             sp.y[dst] = ly;
             sp.vx[dst] = mvX;
             sp.vy[dst] = mvY;
-            sp.vz[dst] = vz;
+            if (moved) sp.vz[dst] = vz;
             if (out) sp.code[dst] = (int8_t)code;
             if (code == CODE_FAR) {
                 const size_t b = (size_t)s * d.C + (size_t)(fi * d.ncy + fj);
@@ -295,6 +304,7 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
     if (lane == 0) {
         sp.cnt[c] = n - m;
         sp.nmov[c] = m;
+        atomicAdd(&d.pushes[32 + (warp & 31)], (unsigned long long)shifted);
     }
     int mine = 0;
 #pragma unroll
@@ -351,7 +361,7 @@ __global__ void __launch_bounds__(512) k_move_u(const DevCase *__restrict__ case
     float *__restrict__ pvy = sp.vy + base;
     float *__restrict__ pvz = sp.vz + base;
     const unsigned lt = lanemask_lt();
-    int m = 0;
+    int m = 0, shifted = 0;
     unsigned long long pk0 = 0, pk1 = 0, pk2 = 0;
     for (int k0 = 0; k0 < n; k0 += 32 * U) {
         float lx[U], ly[U], mvx[U], mvy[U], vz[U];
@@ -403,6 +413,7 @@ __global__ void __launch_bounds__(512) k_move_u(const DevCase *__restrict__ case
             }
             const unsigned bout = __ballot_sync(FULL, out);
             const int before = m + __popc(bout & lt);
+            shifted += __popc(__ballot_sync(FULL, act && (out || before != 0)));
             __syncwarp(); // every lane's loads of this iteration precede the in-place stores
             if (act) {
                 const int dst = out ? cap - 1 - before : k - before;
@@ -427,6 +438,7 @@ __global__ void __launch_bounds__(512) k_move_u(const DevCase *__restrict__ case
     if (lane == 0) {
         sp.cnt[c] = n - m;
         sp.nmov[c] = m;
+        atomicAdd(&d.pushes[32 + (warp & 31)], (unsigned long long)shifted);
     }
     int mine = 0;
 #pragma unroll

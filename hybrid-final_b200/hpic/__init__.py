@@ -117,6 +117,7 @@ _SIGS = {
     "hp_last_pcg_iters": (C.c_int, [_P, _I, _I]),
     "hp_last_field_residual": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "hp_case_pushes": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "hp_case_slot_changes": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "hp_get_table": (C.c_int, [_P, C.c_int, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
     "hp_batch_create": (C.c_int, [C.POINTER(_P), C.c_int, C.POINTER(_P)]),
     "hp_batch_destroy": (C.c_int, [_P]),
@@ -309,6 +310,12 @@ class Case:
     def pushes(self):
         n = C.c_int64(0)
         _check(lib().hp_case_pushes(self.h, C.byref(n)))
+        return n.value
+
+    def slot_changes(self):
+        """Pushed particles whose slot changed (cumulative)."""
+        n = C.c_int64(0)
+        _check(lib().hp_case_slot_changes(self.h, C.byref(n)))
         return n.value
 
     def particles(self, isp):

@@ -226,6 +226,11 @@ hp_status hp_last_field_residual(hp_case *c, double *rel);
 /* Particles advanced by Move since the case was created (the unit of the
  * particle-pushes/s metric). */
 hp_status hp_case_pushes(hp_case *c, int64_t *pushes);
+/* Cumulative count of pushed particles whose slot changed in Move (they
+ * rewrite all five components; a particle that keeps its slot rewrites four:
+ * vz does not change in a push).  Feeds the push's algorithmic bytes
+ * (32 B per particle + 8 B per slot change).  No reference counterpart. */
+hp_status hp_case_slot_changes(hp_case *c, int64_t *changes);
 
 /* Case tables (constant over a run), for checkers and tools.  `what`:
  * 0 StructureIndex int[(ncx+2)(ncy+2)], 1 A_idx int[Gsize], 2 node Boundary int[Gsize],

@@ -291,6 +291,20 @@ def test_non_separable_geometry_falls_back():
     assert c.status() == 0
 
 
+def test_slot_changes_count_the_shifted_particles():
+    """Move counts the particles whose slot changed (movers, and stayers
+    compacted below a mover): at most the particles pushed, and every
+    mover is one."""
+    case, o = pair("ar_65x33", field_mode=2, move_mode=1)
+    p0, s0 = case.pushes(), case.slot_changes()
+    case.set_tstep(1)
+    case.Field()
+    case.Move()
+    pushed, changed = case.pushes() - p0, case.slot_changes() - s0
+    movers = sum(int(case.movers(s)[0].sum()) for s in range(case.info.nsp))
+    assert 0 < movers <= changed <= pushed
+
+
 def test_graph_replay_matches_operator_calls():
     deck, seed = DECKS["ar_33x17_hv"]
     a = hpic.Case(deck, seed=seed)
