@@ -1003,44 +1003,80 @@ __device__ __forceinline__ double warp_sum_d(double v) {
     return v;
 }
 
+// DEP_G consecutive (species, cell) items per warp: lanes 0..G-1 resolve
+// their item's case, count and array bases together, every lane then loads
+// its first slot of all G cells at once, and the cells are summed one after
+// the other (each lane adds its slots lane, lane + 32, ... of a cell in that
+// order, the warp tree reduces in FP64), so the sums are those of one cell
+// per warp.
+#ifndef DEP_G
+#define DEP_G 2
+#endif
 __global__ void __launch_bounds__(512) k_deposit_cells(const DevCase *__restrict__ cases,
                                                        const int *__restrict__ item_start, int ncases, int items) {
+    constexpr int G = DEP_G;
     const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
-    if (warp >= items) return;
-    const int ci = find_case(item_start, ncases, warp);
-    const DevCase &d = cases[ci];
-    const int w = warp - item_start[ci];
-    const int s = w / d.C, c = w - s * d.C;
-    const DevSpecies &sp = d.sp[s];
-    const size_t base = (size_t)c * sp.cap;
-    // the count and the first chunk are independent loads (cap >= 32); later
-    // chunks are loaded four at a time before any is added.  Each lane adds
-    // its slots lane, lane + 32, ... in that order.
-    const int n = sp.cnt[c];
-    const float x0 = sp.x[base + lane], y0 = sp.y[base + lane];
-    float WS = 0.f, WN = 0.f, ES = 0.f, EN = 0.f;
-    auto add = [&](float lx, float ly) {
-        WS += (1 - lx) * (1 - ly);
-        WN += (1 - lx) * ly;
-        ES += lx * (1 - ly);
-        EN += lx * ly;
-    };
-    if (lane < n) add(x0, y0);
-    for (int k0 = 32; k0 < n; k0 += 128) {
-        float xs[4], ys[4];
-#pragma unroll
-        for (int h = 0; h < 4; h++) {
-            const int k = k0 + 32 * h + lane;
-            xs[h] = k < n ? sp.x[base + k] : 0.f;
-            ys[h] = k < n ? sp.y[base + k] : 0.f;
-        }
-#pragma unroll
-        for (int h = 0; h < 4; h++)
-            if (k0 + 32 * h + lane < n) add(xs[h], ys[h]);
+    if (warp * G >= items) return;
+    int my_n = 0;
+    const float *my_x = nullptr, *my_y = nullptr;
+    double4 *my_cw = nullptr;
+    if (lane < G && warp * G + lane < items) {
+        const int item = warp * G + lane;
+        const int ci = find_case(item_start, ncases, item);
+        const DevCase &d = cases[ci];
+        const int w = item - item_start[ci];
+        const int s = w / d.C, c = w - s * d.C;
+        const DevSpecies &sp = d.sp[s];
+        const size_t base = (size_t)c * sp.cap;
+        my_n = sp.cnt[c];
+        my_x = sp.x + base;
+        my_y = sp.y + base;
+        my_cw = d.cw[s] + c;
     }
-    const double a = warp_sum_d(WS), b = warp_sum_d(WN), e = warp_sum_d(ES), f = warp_sum_d(EN);
-    if (lane == 0) d.cw[s][c] = make_double4(a, b, e, f);
+    int n[G];
+    const float *px[G], *py[G];
+    float x0[G], y0[G];
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+        n[g] = __shfl_sync(FULL, my_n, g);
+        px[g] = (const float *)__shfl_sync(FULL, (unsigned long long)my_x, g);
+        py[g] = (const float *)__shfl_sync(FULL, (unsigned long long)my_y, g);
+    }
+    // the first chunk of every cell: slots 0..31 are inside the pool (cap >= 32)
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+        x0[g] = px[g] ? px[g][lane] : 0.f;
+        y0[g] = py[g] ? py[g][lane] : 0.f;
+    }
+#pragma unroll
+    for (int g = 0; g < G; g++) {
+        if (!px[g]) continue; // past the last item (warp-uniform)
+        float WS = 0.f, WN = 0.f, ES = 0.f, EN = 0.f;
+        auto add = [&](float lx, float ly) {
+            WS += (1 - lx) * (1 - ly);
+            WN += (1 - lx) * ly;
+            ES += lx * (1 - ly);
+            EN += lx * ly;
+        };
+        const int ng = n[g];
+        if (lane < ng) add(x0[g], y0[g]);
+        for (int k0 = 32; k0 < ng; k0 += 128) {
+            float xs[4], ys[4];
+#pragma unroll
+            for (int h = 0; h < 4; h++) {
+                const int k = k0 + 32 * h + lane;
+                xs[h] = k < ng ? px[g][k] : 0.f;
+                ys[h] = k < ng ? py[g][k] : 0.f;
+            }
+#pragma unroll
+            for (int h = 0; h < 4; h++)
+                if (k0 + 32 * h + lane < ng) add(xs[h], ys[h]);
+        }
+        const double a = warp_sum_d(WS), b = warp_sum_d(WN), e = warp_sum_d(ES), f = warp_sum_d(EN);
+        double4 *cw = (double4 *)__shfl_sync(FULL, (unsigned long long)my_cw, g);
+        if (lane == 0) *cw = make_double4(a, b, e, f);
+    }
 }
 
 // DepositBoundary + SumSource + PCG_Set (src/cuda_Deposit.cu:277-288,35-104,30-34)
@@ -1606,7 +1642,7 @@ cudaError_t launch_deposit(const DevCase *cases, const int *cell_items, const in
                            int n_cell_items, int n_node_items, const LaunchCfg &lc, cudaStream_t st) {
     const int tpb = 32 * std::min(std::max(lc.warps_per_block, 1), 16);
     if (n_cell_items > 0)
-        k_deposit_cells<<<blocks_for((long long)n_cell_items * 32, tpb), tpb, 0, st>>>(cases, cell_items, ncases,
+        k_deposit_cells<<<blocks_for((long long)(n_cell_items + DEP_G - 1) / DEP_G * 32, tpb), tpb, 0, st>>>(cases, cell_items, ncases,
                                                                                         n_cell_items);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;

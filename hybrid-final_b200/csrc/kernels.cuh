@@ -10,7 +10,7 @@
 namespace hp {
 
 struct LaunchCfg {
-    int warps_per_block = 8;   // particle kernels: one warp per (species, cell)
+    int warps_per_block = 4;   // particle kernels: one warp per (species, cell)
     int pcg_block = 512;       // PCG: threads per CTA
     int pcg_cluster_max = 16;  // PCG: upper bound on CTAs per case
     int move_unroll = 1;       // Move: chunks of 32 loaded per iteration (1: k_move, one-chunk prefetch)
