@@ -484,56 +484,175 @@ __device__ __forceinline__ bool is_hole(float x) { return x != x; }
 #ifndef OXY_MINB
 #define OXY_MINB 5 // 96 registers: five 128-thread blocks per SM
 #endif
+#ifndef OXY_G
+#define OXY_G 4
+#endif
 
-template <int GAS>
-__global__ void __launch_bounds__(OXY_TPB, OXY_MINB) k_mcc_oxy(const DevCase *__restrict__ cases,
-                                                     const int *__restrict__ item_start, int ncases, int items) {
+// The per-cell state a warp keeps for each cell of its group.
+struct OxyCell {
+    int c, n0[NSP_ARO2], cnt[NSP_ARO2], nh[NSP_ARO2];
+    float bv1, bv2;
+    bool hole_over[NSP_ARO2];
+};
+
+// Up to G consecutive cells of one case per warp.  Species by species (e,
+// Ar+, O2+, O+, O- in every cell), the colliders of the group's cells are
+// queued together as (slot | target << 20 | cell-in-group << 24) and
+// collided 32 at a time, so sparse species share batches.  Within a cell
+// everything keeps the order of one cell per warp: colliders in slot order,
+// births appended per species in collider order, holes recorded in collider
+// order, detachment victims drawn in collider order.
+template <int GAS, int G>
+__device__ __forceinline__ void mcc_oxy_cells(const DevCase &d, int c0, int ncell, int *ring,
+                                              int (*holes)[NSP_ARO2][HOLE_CAP], CellProb *P, OxyCell *cs,
+                                              int lane, unsigned lt, bool &overflow) {
     constexpr int NSP = GAS == 2 ? 5 : 4;
     constexpr int OMINUS = GAS == 2 ? 4 : 3;
-    __shared__ int ring_s[OXY_TPB / 32][OXY_RING];
-    __shared__ int holes_s[OXY_TPB / 32][NSP_ARO2][HOLE_CAP];
-    __shared__ CellProb prob_s[OXY_TPB / 32];
-    const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
-    if (warp >= items) return;
-    int *ring = ring_s[wl];
-    const int ci = find_case(item_start, ncases, warp);
-    const DevCase &d = cases[ci];
-    const int c = warp - item_start[ci];
-    const int i = c / d.ncy, j = c - i * d.ncy;
-    const int node = i * d.ngy + j;
     const uint32_t step = (uint32_t)(*d.tstep);
-    const float bv1 = d.back_vel1[node], bv2 = d.back_vel2[node];
-    const unsigned lt = lanemask_lt();
-    CellProb &P = prob_s[wl];
-    cell_prob<GAS>(d, node, P, lane);
+    for (int cl = 0; cl < ncell; cl++) {
+        const int c = c0 + cl;
+        const int i = c / d.ncy, j = c - i * d.ncy;
+        const int node = i * d.ngy + j;
+        cell_prob<GAS>(d, node, P[cl], lane);
+        if (lane < NSP) {
+            const int n = d.sp[lane].cnt[c];
+            cs[cl].n0[lane] = n;
+            cs[cl].cnt[lane] = n;
+            cs[cl].nh[lane] = 0;
+            cs[cl].hole_over[lane] = false;
+        }
+        if (lane == 0) {
+            cs[cl].c = c;
+            cs[cl].bv1 = d.back_vel1[node];
+            cs[cl].bv2 = d.back_vel2[node];
+        }
+    }
+    __syncwarp();
+    // lane-uniform call: one hole of species s in cell cl
+    auto add_hole = [&](int cl, int s, int slot) {
+        const int h = cs[cl].nh[s];
+        if (lane == 0) {
+            if (h < HOLE_CAP) holes[cl][s][h] = slot;
+            else cs[cl].hole_over[s] = true;
+            cs[cl].nh[s] = h + 1;
+        }
+        __syncwarp();
+    };
     // the reference's O2 launch covers Gsize threads, so only its electrons
     // collide (src/cuda_mcc.cu:76-77); mcc_all_species extends it to every species
     const int nactive = (GAS == 2 || d.mcc_all_species) ? NSP : 1;
-    int n0[NSP_ARO2], cnt[NSP_ARO2], nh[NSP_ARO2];
-#pragma unroll
-    for (int s = 0; s < NSP; s++) {
-        n0[s] = d.sp[s].cnt[c];
-        cnt[s] = n0[s];
-        nh[s] = 0;
-    }
-    bool overflow = false, hole_over[NSP_ARO2] = {false, false, false, false, false};
-    unsigned *mcount = d.mcc_count + (size_t)c * d.mcc_stride;
-    auto add_hole = [&](int s, int slot) { // lane-uniform call
-        if (nh[s] < HOLE_CAP) holes_s[wl][s][nh[s]] = slot;
-        else hole_over[s] = true;
-        nh[s]++;
-    };
 #pragma unroll 1
     for (int s = 0; s < nactive; s++) {
         const DevSpecies &sp = d.sp[s];
-        const size_t base = (size_t)c * sp.cap;
-        const int n = n0[s];
         const int nsub = (s == 0 || (GAS == 1 && s == 1)) ? d.mcc_n : 1; // O2: O2+ sub-cycles too
-        const float Tprob = P.p[s][P.n[s] - 1];
         int head = 0, tail = 0;
-        for (int k0 = 0; k0 < n || tail > head; k0 += 128) {
-            if (k0 < n) {
+        // one batch: up to 32 queued colliders, one per lane
+        auto batch = [&]() {
+            const int e = head + lane;
+            Outcome o;
+            no_birth(o);
+            o.keep = true;
+            bool active = false;
+            int k = 0, q = -1;
+            float px = 0.f, py = 0.f;
+            if (e < tail) {
+                const int ent = ring[e & (OXY_RING - 1)];
+                k = ent & 0xFFFFF;
+                const int t = (ent >> 20) & 0xF;
+                q = ent >> 24;
+                const int c = cs[q].c;
+                const size_t base = (size_t)c * sp.cap;
+                px = sp.x[base + k];
+                if (!is_hole(px)) { // an O- removed earlier this call is gone
+                    active = true;
+                    py = sp.y[base + k];
+                    const float vx = sp.vx[base + k], vy = sp.vy[base + k], vz = sp.vz[base + k];
+                    hp_stream rs;
+                    hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, (uint32_t)s);
+                    if (s == 0) electron_collide<GAS>(d, vx, vy, vz, t, cs[q].bv1, rs, o);
+                    else ion_collide<GAS>(d, s, vx, vy, vz, t, cs[q].bv1, cs[q].bv2, rs, o);
+                    if (o.ch >= 0) atomicAdd(&d.mcc_count[(size_t)c * d.mcc_stride + o.ch], 1u);
+                    if (o.keep) {
+                        sp.vx[base + k] = o.vx;
+                        sp.vy[base + k] = o.vy;
+                        sp.vz[base + k] = o.vz;
+                    } else {
+                        sp.x[base + k] = __int_as_float(0x7fc00000); // hole
+                    }
+                }
+            }
+            // holes left by the colliders, in slot order
+            const unsigned bgone = __ballot_sync(FULL, active && !o.keep);
+            for (unsigned m = bgone; m; m &= m - 1) {
+                const int src = __ffs(m) - 1;
+                add_hole(__shfl_sync(FULL, q, src), s, __shfl_sync(FULL, k, src));
+            }
+            // births, per species in lane (= collider) order and per cell; a
+            // collider's two births, if any, go to two different species
+            const unsigned same = __match_any_sync(FULL, q); // lanes of one cell (contiguous)
+#pragma unroll 1
+            for (int t = 0; t < NSP; t++) {
+                const int b = (active && o.b[0].sp == t) ? 0 : (active && o.b[1].sp == t) ? 1 : -1;
+                const unsigned bm = __ballot_sync(FULL, b >= 0);
+                if (!bm) continue;
+                const DevSpecies &tp = d.sp[t];
+                if (b >= 0) {
+                    const int slot = cs[q].cnt[t] + __popc(bm & same & lt);
+                    if (slot < tp.cap) {
+                        const size_t q2 = (size_t)cs[q].c * tp.cap + slot;
+                        tp.x[q2] = px;
+                        tp.y[q2] = py;
+                        tp.vx[q2] = o.b[b].vx;
+                        tp.vy[q2] = o.b[b].vy;
+                        tp.vz[q2] = o.b[b].vz;
+                    } else {
+                        overflow = true;
+                    }
+                }
+                __syncwarp();
+                if (q >= 0 && (same & lt) == 0 && (bm & same))
+                    cs[q].cnt[t] = min(cs[q].cnt[t] + __popc(bm & same), tp.cap);
+                __syncwarp();
+            }
+            // O- removed by detachments, in lane order, among the O- of the
+            // collider's cell present at the start of the call that are still there
+            const unsigned bk = __ballot_sync(FULL, active && o.kill_partner);
+            for (unsigned m = bk; m; m &= m - 1) {
+                const int src = __ffs(m) - 1;
+                const float r2 = __shfl_sync(FULL, o.r2, src);
+                const int qc = __shfl_sync(FULL, q, src);
+                const DevSpecies &om = d.sp[OMINUS];
+                const size_t ob = (size_t)cs[qc].c * om.cap;
+                const int nom = cs[qc].n0[OMINUS];
+                int victim = -1;
+                if (lane == 0) {
+                    int nlive = 0;
+                    for (int a = 0; a < nom; a++) nlive += is_hole(om.x[ob + a]) ? 0 : 1;
+                    if (nlive > 0) {
+                        int pick = 0;
+                        if (nlive > 1) {
+                            pick = (int)((float)nlive * r2);
+                            if (pick > nlive - 1) pick = nlive - 1;
+                        }
+                        for (int a = 0; a < nom; a++) {
+                            if (is_hole(om.x[ob + a])) continue;
+                            if (pick-- == 0) { victim = a; break; }
+                        }
+                        om.x[ob + victim] = __int_as_float(0x7fc00000);
+                    }
+                }
+                victim = __shfl_sync(FULL, victim, 0);
+                __syncwarp();
+                if (victim >= 0) add_hole(qc, OMINUS, victim);
+            }
+            head = min(head + 32, tail);
+            __syncwarp();
+        };
+        for (int cl = 0; cl < ncell; cl++) {
+            const int c = cs[cl].c, n = cs[cl].n0[s];
+            const CellProb &Pc = P[cl];
+            const float Tprob = Pc.p[s][Pc.n[s] - 1];
+            for (int k0 = 0; k0 < n; k0 += 128) {
                 // the test: four slots per lane from one Philox block per sub-cycle
                 const int k = k0 + 4 * lane;
                 unsigned hits = 0;
@@ -548,7 +667,7 @@ __global__ void __launch_bounds__(OXY_TPB, OXY_MINB) k_mcc_oxy(const DevCase *__
                             const float R1 = hp_u01(hp_word(u, (uint32_t)t));
                             if (((live & ~hits) >> t) & 1u && R1 < Tprob) {
                                 hits |= 1u << t;
-                                ent[t] = (k + t) | (target_of(P, s, R1) << 20);
+                                ent[t] = (k + t) | (target_of(Pc, s, R1) << 20) | (cl << 24);
                             }
                         }
                     }
@@ -559,158 +678,94 @@ __global__ void __launch_bounds__(OXY_TPB, OXY_MINB) k_mcc_oxy(const DevCase *__
                 for (int t = 0; t < 4; t++)
                     if ((hits >> t) & 1u) ring[(pos++) & (OXY_RING - 1)] = ent[t];
                 tail += total;
+                __syncwarp();
+                while (tail - head >= 32) batch();
+            }
+        }
+        while (tail > head) batch();
+    }
+    // fill every species' holes with its last particles, cell by cell
+    for (int cl = 0; cl < ncell; cl++) {
+        const int c = cs[cl].c;
+#pragma unroll 1
+        for (int s = 0; s < NSP; s++) {
+            const DevSpecies &sp = d.sp[s];
+            const size_t base = (size_t)c * sp.cap;
+            int n = cs[cl].cnt[s];
+            const int nh = cs[cl].nh[s];
+            if (nh == 0) {
+                if (lane == 0) sp.cnt[c] = n;
+                continue;
+            }
+            if (!cs[cl].hole_over[s]) {
+                if (lane == 0) {
+                    int *h = holes[cl][s];
+                    for (int a = 1; a < nh; a++) { // insertion sort: the list is short
+                        const int v = h[a];
+                        int b = a - 1;
+                        while (b >= 0 && h[b] > v) { h[b + 1] = h[b]; b--; }
+                        h[b + 1] = v;
+                    }
+                    for (int a = 0; a < nh; a++) {
+                        while (n > 0 && is_hole(sp.x[base + n - 1])) n--;
+                        const int hpos = h[a];
+                        if (hpos >= n) continue;
+                        const size_t from = base + n - 1, to = base + hpos;
+                        sp.x[to] = sp.x[from]; sp.y[to] = sp.y[from];
+                        sp.vx[to] = sp.vx[from]; sp.vy[to] = sp.vy[from]; sp.vz[to] = sp.vz[from];
+                        n--;
+                    }
+                    while (n > 0 && is_hole(sp.x[base + n - 1])) n--;
+                    sp.cnt[c] = n;
+                }
+            } else {
+                // more holes than the list holds: stable compaction of the whole species
+                int out = 0;
+                for (int k0 = 0; k0 < n; k0 += 32) {
+                    const int k = k0 + lane;
+                    float x = 0.f, y = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
+                    const bool in = k < n;
+                    if (in) { x = sp.x[base + k]; y = sp.y[base + k]; vx = sp.vx[base + k]; vy = sp.vy[base + k]; vz = sp.vz[base + k]; }
+                    const bool live = in && !is_hole(x);
+                    const unsigned bl = __ballot_sync(FULL, live);
+                    __syncwarp();
+                    if (live) {
+                        const size_t to = base + out + __popc(bl & lt);
+                        sp.x[to] = x; sp.y[to] = y; sp.vx[to] = vx; sp.vy[to] = vy; sp.vz[to] = vz;
+                    }
+                    out += __popc(bl);
+                    __syncwarp();
+                }
+                if (lane == 0) sp.cnt[c] = out;
             }
             __syncwarp();
-            const bool last = k0 + 128 >= n;
-            while (tail - head >= 32 || (last && tail > head)) {
-                const int e = head + lane;
-                Outcome o;
-                no_birth(o);
-                o.keep = true;
-                bool active = false;
-                int k = 0;
-                float px = 0.f, py = 0.f;
-                if (e < tail) {
-                    const int ent = ring[e & (OXY_RING - 1)];
-                    k = ent & 0xFFFFF;
-                    const int t = ent >> 20;
-                    px = sp.x[base + k];
-                    if (!is_hole(px)) { // an O- removed earlier this call is gone
-                        active = true;
-                        py = sp.y[base + k];
-                        const float vx = sp.vx[base + k], vy = sp.vy[base + k], vz = sp.vz[base + k];
-                        hp_stream rs;
-                        hp_stream_init(&rs, d.seed, (uint32_t)k, (uint32_t)c, step, (uint32_t)s);
-                        if (s == 0) electron_collide<GAS>(d, vx, vy, vz, t, bv1, rs, o);
-                        else ion_collide<GAS>(d, s, vx, vy, vz, t, bv1, bv2, rs, o);
-                        if (o.ch >= 0) atomicAdd(&mcount[o.ch], 1u);
-                        if (o.keep) {
-                            sp.vx[base + k] = o.vx;
-                            sp.vy[base + k] = o.vy;
-                            sp.vz[base + k] = o.vz;
-                        } else {
-                            sp.x[base + k] = __int_as_float(0x7fc00000); // hole
-                        }
-                    }
-                }
-                // holes left by the colliders, in slot order
-                const unsigned bgone = __ballot_sync(FULL, active && !o.keep);
-                for (unsigned m = bgone; m; m &= m - 1) {
-                    const int src = __ffs(m) - 1;
-                    add_hole(s, __shfl_sync(FULL, k, src));
-                }
-                // births, per species in lane (= collider) order; a collider's
-                // two births, if any, go to two different species
-#pragma unroll 1
-                for (int t = 0; t < NSP; t++) {
-                    const int q = (active && o.b[0].sp == t) ? 0 : (active && o.b[1].sp == t) ? 1 : -1;
-                    const unsigned bm = __ballot_sync(FULL, q >= 0);
-                    if (!bm) continue;
-                    if (q >= 0) {
-                        const int slot = cnt[t] + __popc(bm & lt);
-                        const DevSpecies &tp = d.sp[t];
-                        if (slot < tp.cap) {
-                            const size_t q2 = (size_t)c * tp.cap + slot;
-                            tp.x[q2] = px;
-                            tp.y[q2] = py;
-                            tp.vx[q2] = o.b[q].vx;
-                            tp.vy[q2] = o.b[q].vy;
-                            tp.vz[q2] = o.b[q].vz;
-                        } else {
-                            overflow = true;
-                        }
-                    }
-                    cnt[t] = min(cnt[t] + __popc(bm), d.sp[t].cap);
-                }
-                // O- removed by detachments, in lane order, among the O- present
-                // at the start of the call that are still there
-                const unsigned bk = __ballot_sync(FULL, active && o.kill_partner);
-                for (unsigned m = bk; m; m &= m - 1) {
-                    const int src = __ffs(m) - 1;
-                    const float r2 = __shfl_sync(FULL, o.r2, src);
-                    const DevSpecies &om = d.sp[OMINUS];
-                    const size_t ob = (size_t)c * om.cap;
-                    int victim = -1;
-                    if (lane == 0) {
-                        int nlive = 0;
-                        for (int q = 0; q < n0[OMINUS]; q++) nlive += is_hole(om.x[ob + q]) ? 0 : 1;
-                        if (nlive > 0) {
-                            int pick = 0;
-                            if (nlive > 1) {
-                                pick = (int)((float)nlive * r2);
-                                if (pick > nlive - 1) pick = nlive - 1;
-                            }
-                            for (int q = 0; q < n0[OMINUS]; q++) {
-                                if (is_hole(om.x[ob + q])) continue;
-                                if (pick-- == 0) { victim = q; break; }
-                            }
-                            om.x[ob + victim] = __int_as_float(0x7fc00000);
-                        }
-                    }
-                    victim = __shfl_sync(FULL, victim, 0);
-                    __syncwarp();
-                    if (victim >= 0) add_hole(OMINUS, victim);
-                }
-                head = min(head + 32, tail);
-                __syncwarp();
-            }
         }
     }
-    // fill every species' holes with its last particles
-#pragma unroll 1
-    for (int s = 0; s < NSP; s++) {
-        const DevSpecies &sp = d.sp[s];
-        const size_t base = (size_t)c * sp.cap;
-        int n = cnt[s];
-        if (nh[s] == 0) {
-            if (lane == 0) sp.cnt[c] = n;
-            continue;
-        }
-        if (!hole_over[s]) {
-            if (lane == 0) {
-                int *h = holes_s[wl][s];
-                const int m = nh[s];
-                for (int a = 1; a < m; a++) { // insertion sort: the list is short
-                    const int v = h[a];
-                    int b = a - 1;
-                    while (b >= 0 && h[b] > v) { h[b + 1] = h[b]; b--; }
-                    h[b + 1] = v;
-                }
-                for (int a = 0; a < m; a++) {
-                    while (n > 0 && is_hole(sp.x[base + n - 1])) n--;
-                    const int hpos = h[a];
-                    if (hpos >= n) continue;
-                    const size_t from = base + n - 1, to = base + hpos;
-                    sp.x[to] = sp.x[from]; sp.y[to] = sp.y[from];
-                    sp.vx[to] = sp.vx[from]; sp.vy[to] = sp.vy[from]; sp.vz[to] = sp.vz[from];
-                    n--;
-                }
-                while (n > 0 && is_hole(sp.x[base + n - 1])) n--;
-                sp.cnt[c] = n;
-            }
-        } else {
-            // more holes than the list holds: stable compaction of the whole species
-            int out = 0;
-            for (int k0 = 0; k0 < n; k0 += 32) {
-                const int k = k0 + lane;
-                float x = 0.f, y = 0.f, vx = 0.f, vy = 0.f, vz = 0.f;
-                const bool in = k < n;
-                if (in) { x = sp.x[base + k]; y = sp.y[base + k]; vx = sp.vx[base + k]; vy = sp.vy[base + k]; vz = sp.vz[base + k]; }
-                const bool live = in && !is_hole(x);
-                const unsigned bl = __ballot_sync(FULL, live);
-                __syncwarp();
-                if (live) {
-                    const size_t to = base + out + __popc(bl & lt);
-                    sp.x[to] = x; sp.y[to] = y; sp.vx[to] = vx; sp.vy[to] = vy; sp.vz[to] = vz;
-                }
-                out += __popc(bl);
-                __syncwarp();
-            }
-            if (lane == 0) sp.cnt[c] = out;
-        }
-        __syncwarp();
+}
+
+template <int GAS, int G>
+__global__ void __launch_bounds__(OXY_TPB, OXY_MINB) k_mcc_oxy(const DevCase *__restrict__ cases,
+                                                     const int *__restrict__ item_start, int ncases, int items) {
+    __shared__ int ring_s[OXY_TPB / 32][OXY_RING];
+    __shared__ int holes_s[OXY_TPB / 32][G][NSP_ARO2][HOLE_CAP];
+    __shared__ CellProb prob_s[OXY_TPB / 32][G];
+    __shared__ OxyCell cell_s[OXY_TPB / 32][G];
+    const int wl = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int first = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5) * G;
+    if (first >= items) return;
+    const unsigned lt = lanemask_lt();
+    const int end = min(first + G, items);
+    // a group that straddles two cases of a batch runs as two groups
+    for (int g0 = first; g0 < end;) {
+        const int ci = find_case(item_start, ncases, g0);
+        const int g1 = min(end, item_start[ci + 1]);
+        const DevCase &d = cases[ci];
+        bool overflow = false;
+        mcc_oxy_cells<GAS, G>(d, g0 - item_start[ci], g1 - g0, ring_s[wl], holes_s[wl], prob_s[wl], cell_s[wl],
+                              lane, lt, overflow);
+        if (__any_sync(FULL, overflow) && lane == 0) atomicOr(d.status, ST_OVERFLOW);
+        g0 = g1;
     }
-    if (__any_sync(FULL, overflow) && lane == 0) atomicOr(d.status, ST_OVERFLOW);
 }
 
 } // namespace
@@ -718,9 +773,10 @@ __global__ void __launch_bounds__(OXY_TPB, OXY_MINB) k_mcc_oxy(const DevCase *__
 cudaError_t launch_mcc_oxy(const DevCase *cases, const int *item_start, int ncases, int items, int gas,
                            cudaStream_t st) {
     if (items <= 0) return cudaSuccess;
-    const unsigned nb = (unsigned)((items * 32LL + OXY_TPB - 1) / OXY_TPB);
-    if (gas == 2) k_mcc_oxy<2><<<nb, OXY_TPB, 0, st>>>(cases, item_start, ncases, items);
-    else if (gas == 1) k_mcc_oxy<1><<<nb, OXY_TPB, 0, st>>>(cases, item_start, ncases, items);
+    constexpr int G = OXY_G;
+    const unsigned nb = (unsigned)(((items + G - 1) / G * 32LL + OXY_TPB - 1) / OXY_TPB);
+    if (gas == 2) k_mcc_oxy<2, G><<<nb, OXY_TPB, 0, st>>>(cases, item_start, ncases, items);
+    else if (gas == 1) k_mcc_oxy<1, G><<<nb, OXY_TPB, 0, st>>>(cases, item_start, ncases, items);
     else return cudaErrorNotSupported;
     return cudaGetLastError();
 }
