@@ -126,6 +126,10 @@ __device__ __forceinline__ void cp_async4(float *smem, const float *gmem) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async16(float *smem, const float *gmem) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N> __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
@@ -173,18 +177,17 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
     const int prev_m = sp.nmov[c]; // movers of the last step
     const float ex_ws = d.Ex[node], ex_wn = d.Ex[node + 1], ex_es = d.Ex[node + d.ngy], ex_en = d.Ex[node + d.ngy + 1];
     const float ey_ws = d.Ey[node], ey_wn = d.Ey[node + 1], ey_es = d.Ey[node + d.ngy], ey_en = d.Ey[node + d.ngy + 1];
-    // chunk q of the cell goes to ring slot q % R, one asynchronous 4-byte copy
-    // per lane and array, one commit group per chunk (possibly empty)
-    // (vz only when asked: a particle that keeps its slot keeps its vz)
+    // chunk q of the cell (all 32 slots: k0 + 32 <= cap, as cap is a multiple
+    // of 32 and k0 < n <= cap) goes to ring slot q % R as 16-byte copies: lanes
+    // 0-7 x, 8-15 y, 16-23 vx, 24-31 vy, then lanes 0-7 vz; one commit group
+    // per chunk (possibly empty).  vz only when asked: a particle that keeps
+    // its slot keeps its vz.
+    const float *arr4 = lane < 8 ? sp.x : lane < 16 ? sp.y : lane < 24 ? sp.vx : sp.vy;
     auto issue = [&](int k0, int lim, bool with_vz) {
-        const int kk = k0 + lane;
         float *sl = ring + ((k0 >> 5) % R) * 160;
-        if (kk < lim) {
-            cp_async4(sl + lane, sp.x + base + kk);
-            cp_async4(sl + 32 + lane, sp.y + base + kk);
-            cp_async4(sl + 64 + lane, sp.vx + base + kk);
-            cp_async4(sl + 96 + lane, sp.vy + base + kk);
-            if (with_vz) cp_async4(sl + 128 + lane, sp.vz + base + kk);
+        if (k0 < lim) {
+            cp_async16(sl + 4 * lane, arr4 + base + k0 + 4 * (lane & 7));
+            if (with_vz && lane < 8) cp_async16(sl + 128 + 4 * lane, sp.vz + base + k0 + 4 * lane);
         }
         cp_async_commit();
     };
@@ -227,6 +230,7 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
         const bool act = k < n;
         issue(k0 + (R - 1) * 32, n, eager_vz);
         cp_async_wait<R - 1>();
+        __syncwarp(); // the chunk was copied by eight lanes per array
         const float *sl = ring + ((k0 >> 5) % R) * 160;
         float lx = sl[lane], ly = sl[32 + lane], vx = sl[64 + lane], vy = sl[96 + lane];
         const bool have_vz = k0 == 0 || eager_vz;
@@ -1616,7 +1620,9 @@ cudaError_t launch_move(const DevCase *cases, const int *item_start, int ncases,
 cudaError_t launch_sort(const DevCase *cases, const int *item_start, int ncases, int items, const LaunchCfg &lc,
                         cudaStream_t st) {
     if (items <= 0) return cudaSuccess;
-    const int tpb = 32 * std::min(std::max(lc.warps_per_block, 1), SORT_MAXW);
+    // at least 8 warps per block: the push gains from them even where Move
+    // and Deposit prefer smaller blocks
+    const int tpb = 32 * std::min(std::max(lc.warps_per_block, 8), SORT_MAXW);
     k_sort_push<<<blocks_for((long long)items * 32, tpb), tpb, 0, st>>>(cases, item_start, ncases, items);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
