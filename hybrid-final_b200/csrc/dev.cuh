@@ -22,9 +22,7 @@
 // step and species; more sets the overflow status
 #define HP_FAR_BUCKET 32
 
-// electron energy distribution: bins of HP_EEDF_DE eV from 0, one overflow bin
-#define HP_EEDF_BINS 200
-#define HP_EEDF_DE 0.25f
+#include "hpic.h" // HP_EEDF_BINS, HP_EEDF_DE
 
 namespace hp {
 

@@ -23,6 +23,11 @@
 #include <stddef.h>
 #include <stdint.h>
 
+/* electron energy distribution (HP_GRID_EEDF): bins of HP_EEDF_DE eV from 0,
+ * then one overflow bin */
+#define HP_EEDF_BINS 200
+#define HP_EEDF_DE 0.25f
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -208,7 +213,8 @@ typedef enum hp_grid_field {
     HP_GRID_AVE_PHI = 9, /* double[Gsize] running sum of TotPotential */
     HP_GRID_COND_CHARGE = 10, /* float[nsp*CondNUMR] absorbed particles per conductor */
     HP_GRID_MCC_COUNT = 11,   /* uint32[Csize*mcc_stride] collisions per cell and channel since creation */
-    HP_GRID_EEDF = 12         /* uint64[201] electron energy histogram (0.25 eV bins, last = above 50 eV),
+    HP_GRID_EEDF = 12         /* uint64[HP_EEDF_BINS + 1] electron energy histogram (HP_EEDF_DE eV bins,
+                                 last = above HP_EEDF_BINS * HP_EEDF_DE eV),
                                  sampled every eedf_every steps since hp_reset_averages; no reference
                                  counterpart (the reference computes no EEDF) */
 } hp_grid_field;
