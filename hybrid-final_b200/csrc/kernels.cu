@@ -499,19 +499,10 @@ __device__ __forceinline__ MoverRegs load_mover(const DevSpecies &sp, size_t bas
     return v;
 }
 
-__global__ void __launch_bounds__(SORT_MAXW * 32) k_sort_push(const DevCase *__restrict__ cases,
-                                                        const int *__restrict__ item_start, int ncases, int items) {
-    __shared__ int s_off[SORT_MAXW][9], s_lim[SORT_MAXW][9];
-    const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
-    if (warp >= items) return;
-    const int ci = find_case(item_start, ncases, warp);
-    const DevCase &d = cases[ci];
-    const int w = warp - item_start[ci];
-    const int s = w / d.C, c = w - s * d.C;
+// the movers of one source cell (m > 0) of species s
+__device__ __forceinline__ void sort_push_cell(const DevCase &d, int s, int c, int m, int *s_off, int *s_lim,
+                                               int lane) {
     const DevSpecies &sp = d.sp[s];
-    const int m = sp.nmov[c];
-    if (m == 0) return;
     const int cap = sp.cap, ncy = d.ncy;
     const int i = c / ncy, j = c - i * ncy;
     const size_t base = (size_t)c * cap;
@@ -546,13 +537,13 @@ __global__ void __launch_bounds__(SORT_MAXW * 32) k_sort_push(const DevCase *__r
         }
     }
     if (lane < 9) {
-        s_off[wl][lane] = off9;
-        s_lim[wl][lane] = lim9;
+        s_off[lane] = off9;
+        s_lim[lane] = lim9;
     }
     __syncwarp();
 #pragma unroll
     for (int t = 0; t < 3; t++)
-        if (pv[t]) atomicAdd(&s_off[wl][(lane + 32 * t) / 9], pv[t]);
+        if (pv[t]) atomicAdd(&s_off[(lane + 32 * t) / 9], pv[t]);
     __syncwarp();
     const unsigned lt = lanemask_lt();
     int run[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -566,8 +557,8 @@ __global__ void __launch_bounds__(SORT_MAXW * 32) k_sort_push(const DevCase *__r
             run[D] += __popc(b);
         }
         if (v.code >= 0 && v.code < 9) {
-            const int slot = s_off[wl][v.code] + rank;
-            if (slot < s_lim[wl][v.code]) {
+            const int slot = s_off[v.code] + rank;
+            if (slot < s_lim[v.code]) {
                 const size_t dst = (size_t)(c + (v.code / 3 - 1) * ncy + (v.code % 3 - 1)) * cap + (size_t)slot;
                 sp.x[dst] = v.x;
                 sp.y[dst] = v.y;
@@ -590,6 +581,41 @@ __global__ void __launch_bounds__(SORT_MAXW * 32) k_sort_push(const DevCase *__r
             if (r0 + h * 32 < m) place(mv[h]);
     }
     if (__any_sync(FULL, overflow) && lane == 0) atomicOr(d.status, ST_OVERFLOW);
+    __syncwarp(); // s_off / s_lim are reused by the warp's next cell
+}
+
+// SORT_G consecutive (species, cell) items per warp: one lane per item reads
+// its mover count, then the warp places the movers of the items that have
+// any, one cell after the other.  One item per warp is fastest on B200 (the
+// cells' dependent load chains then overlap across warps instead of running
+// one after the other inside a warp); larger groups only save the idle ion
+// warps.
+#ifndef SORT_G
+#define SORT_G 1
+#endif
+__global__ void __launch_bounds__(SORT_MAXW * 32, 2) k_sort_push(const DevCase *__restrict__ cases,
+                                                           const int *__restrict__ item_start, int ncases, int items) {
+    __shared__ int s_off[SORT_MAXW][9], s_lim[SORT_MAXW][9];
+    const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    const int first = warp * SORT_G;
+    if (first >= items) return;
+    int ci = 0, m = 0;
+    if (lane < SORT_G && first + lane < items) {
+        ci = find_case(item_start, ncases, first + lane);
+        const DevCase &d = cases[ci];
+        const int w = first + lane - item_start[ci];
+        const int s = w / d.C, c = w - s * d.C;
+        m = d.sp[s].nmov[c];
+    }
+    for (unsigned todo = __ballot_sync(FULL, m > 0); todo; todo &= todo - 1) {
+        const int src = __ffs(todo) - 1;
+        const int fci = __shfl_sync(FULL, ci, src), fm = __shfl_sync(FULL, m, src);
+        const DevCase &d = cases[fci];
+        const int w = first + src - item_start[fci];
+        const int s = w / d.C, c = w - s * d.C;
+        sort_push_cell(d, s, c, fm, s_off[wl], s_lim[wl], lane);
+    }
 }
 
 // One lane per destination cell (32 cells per warp): the new count is its
@@ -1623,7 +1649,8 @@ cudaError_t launch_sort(const DevCase *cases, const int *item_start, int ncases,
     // at least 8 warps per block: the push gains from them even where Move
     // and Deposit prefer smaller blocks
     const int tpb = 32 * std::min(std::max(lc.warps_per_block, 8), SORT_MAXW);
-    k_sort_push<<<blocks_for((long long)items * 32, tpb), tpb, 0, st>>>(cases, item_start, ncases, items);
+    k_sort_push<<<blocks_for((long long)(items + SORT_G - 1) / SORT_G * 32, tpb), tpb, 0, st>>>(cases, item_start,
+                                                                                               ncases, items);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_sort_count<<<blocks_for((long long)(items + 31) / 32 * 32, tpb), tpb, 0, st>>>(cases, item_start, ncases,
