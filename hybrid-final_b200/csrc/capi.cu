@@ -314,6 +314,9 @@ hp_status build_device(hp_case *c) {
     TRY(dalloc(c, &h.source, G));
     TRY(dalloc(c, &h.ave_den, (size_t)s.nsp * G));
     TRY(dalloc(c, &h.ave_phi, G));
+    TRY(dalloc(c, &h.ave_src, G));
+    TRY(dalloc(c, &h.ave_ex, G));
+    TRY(dalloc(c, &h.ave_ey, G));
     h.src_num = s.src_num;
     for (int k = 0; k < s.src_num; k++) {
         h.src_mid[k] = s.src_mid[k];
@@ -928,6 +931,9 @@ static hp_status grid_ptr(hp_case *c, hp_grid_field f, void **p, size_t *nb) {
     case HP_GRID_PCG_B: *p = c->h.b64; *nb = (size_t)G * 8; break;
     case HP_GRID_AVE_DEN: *p = c->h.ave_den; *nb = (size_t)nsp * G * 8; break;
     case HP_GRID_AVE_PHI: *p = c->h.ave_phi; *nb = (size_t)G * 8; break;
+    case HP_GRID_AVE_SOURCE: *p = c->h.ave_src; *nb = (size_t)G * 8; break;
+    case HP_GRID_AVE_EX: *p = c->h.ave_ex; *nb = (size_t)G * 8; break;
+    case HP_GRID_AVE_EY: *p = c->h.ave_ey; *nb = (size_t)G * 8; break;
     case HP_GRID_COND_CHARGE: *p = c->h.cond_charge; *nb = (size_t)nsp * c->s.cond_numr * 4; break;
     case HP_GRID_MCC_COUNT: *p = c->h.mcc_count; *nb = (size_t)c->h.mcc_stride * c->s.Csize * 4; break;
     case HP_GRID_EEDF: *p = c->h.eedf; *nb = (size_t)(HP_EEDF_BINS + 1) * 8; break;
@@ -966,6 +972,9 @@ hp_status hp_reset_averages(hp_case *c) {
     CK(cudaStreamSynchronize(c->last_stream));
     CK(cudaMemset(c->h.ave_den, 0, (size_t)c->s.nsp * c->s.Gsize * 8));
     CK(cudaMemset(c->h.ave_phi, 0, (size_t)c->s.Gsize * 8));
+    CK(cudaMemset(c->h.ave_src, 0, (size_t)c->s.Gsize * 8));
+    CK(cudaMemset(c->h.ave_ex, 0, (size_t)c->s.Gsize * 8));
+    CK(cudaMemset(c->h.ave_ey, 0, (size_t)c->s.Gsize * 8));
     CK(cudaMemset(c->h.ave_count, 0, 8));
     CK(cudaMemset(c->h.eedf, 0, (HP_EEDF_BINS + 1) * 8));
     return HP_OK;

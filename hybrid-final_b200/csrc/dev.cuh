@@ -63,6 +63,7 @@ struct DevCase {
     double *source;                 // [G]
     double4 *cw[DMAXSP];            // [C] per-cell corner weight sums
     double *ave_den, *ave_phi;      // [nsp*G], [G]
+    double *ave_src, *ave_ex, *ave_ey; // [G] time sums of the charge source and of E
     // sources (src/cuda_Field.cu:10-20)
     int src_num;
     int src_mid[DMAXSRC];

@@ -1559,6 +1559,9 @@ __global__ void __launch_bounds__(256) k_accumulate(const DevCase *__restrict__ 
     const int n = t - item_start[ci];
     for (int s = 0; s < d.nsp; s++) d.ave_den[(size_t)s * d.G + n] += d.den[(size_t)s * d.G + n];
     d.ave_phi[n] += (double)d.phi[n];
+    d.ave_src[n] += d.source[n];
+    d.ave_ex[n] += (double)d.Ex[n];
+    d.ave_ey[n] += (double)d.Ey[n];
     if (n == 0) *d.ave_count += 1;
 }
 

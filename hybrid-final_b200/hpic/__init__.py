@@ -23,7 +23,7 @@ HP_OK, HP_ERR_ARG, HP_ERR_DECK, HP_ERR_CUDA, HP_ERR_OOM, HP_ERR_UNSUPPORTED, HP_
 STATUS_CELL_OVERFLOW, STATUS_NONFINITE, STATUS_PCG_NOCONV, STATUS_WAIT_TIMEOUT = 1, 2, 4, 8
 
 GRID = dict(EX=0, EY=1, PHI=2, PHI_POIS=3, DEN=4, SOURCE=5, PCG_X=6, PCG_B=7, AVE_DEN=8, AVE_PHI=9,
-            COND_CHARGE=10, MCC_COUNT=11, EEDF=12)
+            COND_CHARGE=10, MCC_COUNT=11, EEDF=12, AVE_SOURCE=13, AVE_EX=14, AVE_EY=15)
 EEDF_BINS, EEDF_DE = 200, 0.25  # electron energy histogram: 0.25 eV bins from 0, one overflow bin
 TABLE = dict(sidx=0, a_idx=1, boundary=2, face=3, cond_id=4, area=5, back_den1=6, back_vel1=7, lap=8,
              stencil=9, vsave=10, xsec=11, collf=12, sigv=13, dens_region=14, prob=15, eps_r=16,
@@ -351,7 +351,8 @@ class Case:
                      PCG_X=(G, np.float32 if self.opts.field_mode == 0 else np.float64),
                      PCG_B=(G, np.float64), AVE_DEN=(nsp * G, np.float64), AVE_PHI=(G, np.float64),
                      COND_CHARGE=(nsp * info.cond_numr, np.float32), MCC_COUNT=(info.mcc_stride * info.Csize, np.uint32),
-                     EEDF=(EEDF_BINS + 1, np.uint64))
+                     EEDF=(EEDF_BINS + 1, np.uint64), AVE_SOURCE=(G, np.float64), AVE_EX=(G, np.float64),
+                     AVE_EY=(G, np.float64))
         n, dt = sizes[name]
         out = np.zeros(n, dtype=dt)
         _check(lib().hp_get_grid(self.h, GRID[name], out.ctypes.data_as(_P), out.nbytes))

@@ -213,10 +213,14 @@ typedef enum hp_grid_field {
     HP_GRID_AVE_PHI = 9, /* double[Gsize] running sum of TotPotential */
     HP_GRID_COND_CHARGE = 10, /* float[nsp*CondNUMR] absorbed particles per conductor */
     HP_GRID_MCC_COUNT = 11,   /* uint32[Csize*mcc_stride] collisions per cell and channel since creation */
-    HP_GRID_EEDF = 12         /* uint64[HP_EEDF_BINS + 1] electron energy histogram (HP_EEDF_DE eV bins,
+    HP_GRID_EEDF = 12,        /* uint64[HP_EEDF_BINS + 1] electron energy histogram (HP_EEDF_DE eV bins,
                                  last = above HP_EEDF_BINS * HP_EEDF_DE eV),
                                  sampled every eedf_every steps since hp_reset_averages; no reference
                                  counterpart (the reference computes no EEDF) */
+    HP_GRID_AVE_SOURCE = 13,  /* double[Gsize] running sum of the charge source rho/eps0 (the reference's
+                                 ave_Source, src/cuda_SaveDump.cu:91-92) */
+    HP_GRID_AVE_EX = 14,      /* double[Gsize] running sums of Ex and Ey (ave_Ex, ave_Ey) */
+    HP_GRID_AVE_EY = 15
 } hp_grid_field;
 hp_status hp_get_grid(hp_case *c, hp_grid_field f, void *out, size_t bytes);
 hp_status hp_set_grid(hp_case *c, hp_grid_field f, const void *in, size_t bytes);

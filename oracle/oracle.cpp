@@ -87,7 +87,7 @@ struct SimBase {
     std::vector<float> cond_charge;
     std::vector<unsigned> mcc_count;
     int pcg_iters[2] = {0, 0};
-    std::vector<double> ave_den, ave_phi;
+    std::vector<double> ave_den, ave_phi, ave_src, ave_ex, ave_ey;
     int64_t ave_count = 0;
     bool walk_bound_hit = false; // a walk that reached its crossing bound
     std::vector<unsigned long long> eedf = std::vector<unsigned long long>(201, 0ull);
@@ -146,6 +146,9 @@ template <class R> struct Sim : SimBase {
         mcc_count.assign((size_t)(c.mcc_stride > 0 ? c.mcc_stride : 8) * C, 0u);
         ave_den.assign((size_t)c.nsp * G, 0.0);
         ave_phi.assign(G, 0.0);
+        ave_src.assign(G, 0.0);
+        ave_ex.assign(G, 0.0);
+        ave_ey.assign(G, 0.0);
     }
 
     // ------------------------------------------------------------ state
@@ -1553,6 +1556,9 @@ template <class R> struct Sim : SimBase {
     void accumulate() override {
         for (size_t k = 0; k < den.size(); k++) ave_den[k] += den[k];
         for (int n = 0; n < G; n++) ave_phi[n] += (double)phi[n];
+        for (int n = 0; n < G; n++) ave_src[n] += source[n];
+        for (int n = 0; n < G; n++) ave_ex[n] += (double)Ex[n];
+        for (int n = 0; n < G; n++) ave_ey[n] += (double)Ey[n];
         ave_count++;
     }
     // electron energy histogram (the library's EEDF: 200 bins of 0.25 eV and
@@ -1649,6 +1655,12 @@ void or_run(or_sim *s, int64_t tstep0, int nsteps, int accumulate) {
     }
 }
 void or_get_eedf(or_sim *s, unsigned long long *h) { std::memcpy(h, s->impl->eedf.data(), 201 * 8); }
+void or_get_field_averages(or_sim *s, double *ave_src, double *ave_ex, double *ave_ey) {
+    SimBase *b = s->impl;
+    if (ave_src) std::memcpy(ave_src, b->ave_src.data(), b->ave_src.size() * 8);
+    if (ave_ex) std::memcpy(ave_ex, b->ave_ex.data(), b->ave_ex.size() * 8);
+    if (ave_ey) std::memcpy(ave_ey, b->ave_ey.data(), b->ave_ey.size() * 8);
+}
 void or_get_averages(or_sim *s, double *ave_den, double *ave_phi, int64_t *count) {
     SimBase *b = s->impl;
     if (ave_den) std::memcpy(ave_den, b->ave_den.data(), b->ave_den.size() * 8);

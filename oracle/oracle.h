@@ -98,6 +98,8 @@ void or_deposit(or_sim *s);
 /* n full steps from tstep+1; accumulates node averages when ave != 0 */
 void or_run(or_sim *s, int64_t tstep0, int nsteps, int accumulate);
 void or_get_averages(or_sim *s, double *ave_den, double *ave_phi, int64_t *count);
+/* running sums of the charge source and of Ex, Ey (double[G] each) */
+void or_get_field_averages(or_sim *s, double *ave_src, double *ave_ex, double *ave_ey);
 /* the electron energy histogram: 201 counts (0.25 eV bins, last = overflow) */
 void or_get_eedf(or_sim *s, unsigned long long *h);
 int or_num_threads(void);

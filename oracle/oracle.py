@@ -74,6 +74,7 @@ def lib():
             "or_get_counters": (None, [P, _F, C.POINTER(C.c_uint), _I]),
             "or_walk_bound_hit": (C.c_int, [P]),
             "or_get_eedf": (None, [P, C.POINTER(C.c_uint64)]),
+            "or_get_field_averages": (None, [P, P, P, P]),
             "or_math": (None, [C.c_int, _F, _F, _F, C.c_int]),
             "or_field": (None, [P, C.c_int64]),
             "or_move": (None, [P]),
@@ -295,6 +296,13 @@ class Oracle:
 
     def run(self, tstep0, nsteps, accumulate=True):
         lib().or_run(self.h, tstep0, nsteps, 1 if accumulate else 0)
+
+    def field_averages(self):
+        """Running sums of the charge source, Ex and Ey (double[G] each)."""
+        G = self.info.Gsize
+        out = [np.zeros(G, np.float64) for _ in range(3)]
+        lib().or_get_field_averages(self.h, *[a.ctypes.data_as(C.c_void_p) for a in out])
+        return out
 
     def eedf(self):
         h = np.zeros(201, np.uint64)

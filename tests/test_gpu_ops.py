@@ -141,6 +141,10 @@ def test_steps_bit_exact(name, mode):
     assert case.average_count() == cnt == n
     assert same(case.grid("AVE_DEN"), d)
     assert same(case.grid("AVE_PHI"), p)
+    src, ex, ey = o.field_averages()
+    assert same(case.grid("AVE_SOURCE"), src)
+    assert same(case.grid("AVE_EX"), ex)
+    assert same(case.grid("AVE_EY"), ey)
     assert case.status() == 0
     assert case.tstep() == n
 
