@@ -942,6 +942,9 @@ static hp_status grid_ptr(hp_case *c, hp_grid_field f, void **p, size_t *nb) {
     return HP_OK;
 }
 
+// device address and size of a grid field, for the checkpoint writer
+hp_status hpi_grid_ptr(hp_case *c, hp_grid_field f, void **p, size_t *nb) { return grid_ptr(c, f, p, nb); }
+
 hp_status hp_get_grid(hp_case *c, hp_grid_field f, void *out, size_t bytes) {
     if (!c || !out) return HP_ERR_ARG;
     void *p;

@@ -52,6 +52,8 @@ struct hp_case {
     std::vector<float> prob; // [3*C]
 };
 
+extern "C" hp_status hpi_grid_ptr(hp_case *c, hp_grid_field f, void **p, size_t *nb);
+
 namespace hpi {
 hp_status fast_plan_build(hp_case *const *cases, const std::vector<int> &idx, FastPlanDev &out);
 void fast_plan_free(FastPlanDev &f);

@@ -118,6 +118,8 @@ _SIGS = {
     "hp_last_field_residual": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "hp_case_pushes": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "hp_case_slot_changes": (C.c_int, [_P, C.POINTER(C.c_int64)]),
+    "hp_case_save": (C.c_int, [_P, C.c_char_p]),
+    "hp_case_load": (C.c_int, [_P, C.c_char_p]),
     "hp_get_table": (C.c_int, [_P, C.c_int, _P, C.c_size_t, C.POINTER(C.c_size_t)]),
     "hp_batch_create": (C.c_int, [C.POINTER(_P), C.c_int, C.POINTER(_P)]),
     "hp_batch_destroy": (C.c_int, [_P]),
@@ -311,6 +313,14 @@ class Case:
         n = C.c_int64(0)
         _check(lib().hp_case_pushes(self.h, C.byref(n)))
         return n.value
+
+    def save(self, path):
+        """Checkpoint: the reference's V000 dump plus the exact-resume extension."""
+        _check(lib().hp_case_save(self.h, str(path).encode()))
+
+    def load(self, path):
+        """Resume from a checkpoint written by save() for the same deck and options."""
+        _check(lib().hp_case_load(self.h, str(path).encode()))
 
     def slot_changes(self):
         """Pushed particles whose slot changed (cumulative)."""

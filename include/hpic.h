@@ -227,6 +227,18 @@ hp_status hp_set_grid(hp_case *c, hp_grid_field f, const void *in, size_t bytes)
 /* Running averages (N_ave accumulation, src/cuda_Diagnostic.cu:505-547):
  * the sums above and the number of accumulated steps. */
 hp_status hp_reset_averages(hp_case *c);
+
+/* ------------------------------------------------------------ checkpoint */
+/* Checkpoint of a case: the reference's V000 dump (V000_DUMP,
+ * src/cuda_SaveDump.cu:5-106; readable by V000_LoadDUMP, src/load.c:5-120)
+ * followed by an "HPICX001" extension holding the exact state a resumed run
+ * needs (step counter and seed that key the random streams, particles as
+ * in-cell offsets, field-solver warm start, charge grid, running sums,
+ * tallies).  hp_case_load restores it into a case created from the same
+ * deck and options, so that the run continues bit for bit as if it had not
+ * stopped.  Not for a case inside a batch. */
+hp_status hp_case_save(hp_case *c, const char *path);
+hp_status hp_case_load(hp_case *c, const char *path);
 hp_status hp_get_average_count(hp_case *c, int64_t *n);
 
 /* Field-solver iteration count of the last hp_Field (reference: *FIter). */
