@@ -457,7 +457,8 @@ def run_served(args):
     stream = torch.cuda.current_stream().cuda_stream
     steps_per_cycle = max(1, int(round(400 * args.steps_scale)))
     reqs = served_stream(args.requests, rate_per_s=args.rate, seed=7, steps_per_cycle=steps_per_cycle)
-    opts = dict(field_mode=2, gas_temp_mode=1, move_mode=1)
+    # initial particles generated on the device unless --host-load (both loops alike)
+    opts = dict(field_mode=2, gas_temp_mode=1, move_mode=1, gpu_load=0 if args.host_load else 1)
 
     def pct(v, q):
         return float(np.percentile(np.asarray(v), q)) if v else None
@@ -506,7 +507,7 @@ def run_served(args):
                             arrivals=f"Poisson {args.rate}/s", grids="65x33/129x65/257x129/513x257",
                             ppc="50-200", rf_periods="1-10", steps_per_rf_period=steps_per_cycle,
                             slots=args.slots, steps_per_launch=args.steps_per_launch, budget_gb=args.budget_gb,
-                            gas="Ar or 80/20 Ar/O2"),
+                            gas="Ar or 80/20 Ar/O2", particle_load="host" if args.host_load else "device"),
                 latency_s=dict(p50=pct(lat, 50), p99=pct(lat, 99)), errors=errors, wall_s=t_end,
                 plain=dict(value=plain_pushes / plain_end, latency_s=dict(p50=pct(plain_lat, 50),
                                                                           p99=pct(plain_lat, 99)),
@@ -534,6 +535,8 @@ def main():
     ap.add_argument("--slots", type=int, default=64)
     ap.add_argument("--steps-per-launch", type=int, default=40)
     ap.add_argument("--budget-gb", type=float, default=150.0)
+    ap.add_argument("--host-load", action="store_true",
+                    help="served: load the initial particles on the host (the reference's loader) instead of the device")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     rank = int(os.environ.get("RANK", "0"))

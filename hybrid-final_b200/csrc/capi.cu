@@ -126,6 +126,7 @@ BuildOpts build_opts(const hp_case_opts *o) {
         b.seed = o->seed;
         b.cap_per_cell = o->cap_per_cell;
         b.gas_temp_mode = o->gas_temp_mode;
+        b.defer_load = o->gpu_load != 0;
     }
     return b;
 }
@@ -399,9 +400,12 @@ hp_status build_device(hp_case *c) {
         std::vector<int> items = {0, s.nsp * C, 0, C, 0, G};
         TRY(dupload(c, &c->d_items, items));
     }
-    for (int isp = 0; isp < s.nsp; isp++)
-        TRY(upload_particles(c, isp, s.p_count[isp].data(), s.p_x[isp].data(), s.p_y[isp].data(), s.p_vx[isp].data(),
-                             s.p_vy[isp].data(), s.p_vz[isp].data()));
+    for (int isp = 0; isp < s.nsp; isp++) {
+        if (s.load_deferred) TRY(hpi::device_load(c, isp));
+        else
+            TRY(upload_particles(c, isp, s.p_count[isp].data(), s.p_x[isp].data(), s.p_y[isp].data(),
+                                 s.p_vx[isp].data(), s.p_vy[isp].data(), s.p_vz[isp].data()));
+    }
     c->pcg_cluster = pcg_cluster_for_nodes(G);
     if (h.field_mode == 2) {
         hp_case *one[1] = {c};
@@ -511,6 +515,9 @@ hp_status hp_setup_get_particles(const hp_setup *su, int isp, int layout, int *c
                                  float *vy, float *vz, size_t cap, size_t *n_out) {
     if (!su || isp < 0 || isp >= su->s.nsp) return set_error("bad species"), HP_ERR_ARG;
     const Setup &s = su->s;
+    if (s.load_deferred)
+        return set_error("this set-up leaves the particle load to the device (gpu_load): read the case's particles"),
+               HP_ERR_ARG;
     size_t n = (size_t)s.sp[isp].np;
     if (n_out) *n_out = n;
     if (cap < n) return set_error("output arrays too small"), HP_ERR_ARG;

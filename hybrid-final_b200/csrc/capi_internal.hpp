@@ -82,6 +82,7 @@ void batch_dev_free(BatchDev &b);
 hp_status run_step(const BatchDev &b, const hp::LaunchCfg &lc, int gas, cudaStream_t st);
 // a case that takes over a set-up (its host particle load is released once uploaded)
 hp_status case_from_setup_owned(hp::Setup &&s, const hp_case_opts &o, hp_case **out);
+hp_status device_load(hp_case *c, int isp); // the initial particles of a deferred load (load.cu)
 // an upper estimate of a case's device footprint before it is created
 size_t estimate_device_bytes(const hp::Setup &s, const hp_case_opts &o);
 } // namespace hpi

@@ -106,6 +106,7 @@ void worker_main(hp_server *s) {
         b.seed = o.seed;
         b.cap_per_cell = o.cap_per_cell;
         b.gas_temp_mode = o.gas_temp_mode;
+        b.defer_load = o.gpu_load != 0;
         hp_status err = HP_OK;
         std::string msg;
         try {

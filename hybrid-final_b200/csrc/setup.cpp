@@ -873,6 +873,15 @@ void gas_setting(Setup &s, const BuildOpts &o) { // src/start.c:1999-2051
                 if (n_per_cell > 0 && i >= x0 && i <= x1 && j >= y0 && j <= y1) lc.push_back(i * s.ncy + j);
             }
         const long long np = (long long)lc.size() * std::max(n_per_cell, 0);
+        if (o.defer_load) {
+            s.load_deferred = true;
+            s.load_cells[isp] = lc;
+            s.load_npc[isp] = std::max(n_per_cell, 0);
+            s.load_seed[isp] = pm.seed;
+            pm.seed = pm_skip(pm.seed, 5ull * (unsigned long long)np);
+            p.np = (int)np;
+            continue;
+        }
         hx.resize(np); hy.resize(np); hvx.resize(np); hvy.resize(np); hvz.resize(np); hc.resize(np);
         const long seed0 = pm.seed;
         par_range(np, [&](long long k0, long long k1) {

@@ -112,12 +112,20 @@ struct Setup {
     std::vector<int> h_cell[MAXSP];
     int cap[MAXSP] = {0};                                  // slots per cell
     uint64_t seed = 1;
+    // a load left to the device (BuildOpts::defer_load): the loading cells in
+    // load order, particles per loading cell, and the generator state at the
+    // species' first draw; p_count etc. stay empty
+    bool load_deferred = false;
+    std::vector<int> load_cells[MAXSP];
+    int load_npc[MAXSP] = {0};
+    long load_seed[MAXSP] = {0};
 };
 
 struct BuildOpts {
     uint64_t seed = 1;
     int cap_per_cell = 0;
     int gas_temp_mode = 0; // 0 reference temperature operator, 1 potential operator (uniform for equal walls)
+    bool defer_load = false; // leave the particle load to the device (hp_case_opts.gpu_load)
 };
 
 // Throws std::runtime_error with a message; the message starts with

@@ -44,7 +44,7 @@ class CaseOpts(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("cap_per_cell", C.c_int), ("field_mode", C.c_int),
                 ("pcg_rtol", C.c_double), ("pcg_max_iter", C.c_int), ("o2_all_species", C.c_int),
                 ("device", C.c_int), ("gas_temp_mode", C.c_int), ("move_mode", C.c_int),
-                ("fs_passes", C.c_int), ("eedf_every", C.c_int)]
+                ("fs_passes", C.c_int), ("eedf_every", C.c_int), ("gpu_load", C.c_int)]
 
 
 class CaseInfo(C.Structure):

@@ -104,6 +104,10 @@ typedef struct hp_case_opts {
     int fs_passes;       /* field_mode 2: FP64 refinement passes per solve; 0 = 2 when pcg_rtol >= 1e-10
                             (each pass gains ~6 digits), else 3 */
     int eedf_every;      /* electron energy distribution (HP_GRID_EEDF): 0 = off, k = sample every k-th step */
+    int gpu_load;        /* 1 = generate the initial particles on the device at case creation (same
+                            Park-Miller draws and cell order as the host load; a cos() in the Maxwellian
+                            may differ in its last double bit, so rare vx/vy differ by one float ulp);
+                            0 = the reference's host load (default) */
 } hp_case_opts;
 
 /* Default options. */

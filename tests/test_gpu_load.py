@@ -1,0 +1,70 @@
+"""The initial particle load generated on the device (hp_case_opts.gpu_load)
+against the host load the reference's loader defines.
+
+Counts per cell, in-cell offsets and vz are compared bit for bit.  vx and vy
+multiply by a double cos/sin, whose last bit may differ between the host's
+libm and the device (both within their documented error); after the cast to
+float that changes at most one ulp, in a tiny fraction of particles.
+Two seeds are chosen so that the first electron's x (and y) draw is exactly
+1.0f: that particle belongs to the next cell, as in the reference."""
+import numpy as np
+import pytest
+
+import hpic
+from hpic.decks import block_deck, ccp_deck
+
+pytestmark = pytest.mark.gpu
+
+M = 2 ** 31 - 1
+
+
+def edge_seed(draw_index, target=2147483600):
+    """A loader seed whose draw number `draw_index` (1-based) is within 64 of
+    2^31 - 2, i.e. returns 1.0f."""
+    return target * pow(pow(16807, draw_index, M), M - 2, M) % M
+
+
+CASES = {
+    "edge_x": (ccp_deck(17, 9, 0.005, 0.0025, ppc=10), edge_seed(4)),
+    "edge_y": (ccp_deck(17, 9, 0.005, 0.0025, ppc=10), edge_seed(5)),
+    "ar_65x33": (ccp_deck(65, 33, 0.02, 0.01, ppc=30), 99),
+    "aro2": (ccp_deck(33, 17, 0.01, 0.005, gas="ArO2", ppc=20, pressure_torr=0.1, voltage=200.0, te_ev=3.0,
+                      ion_density={"Ar+": 1e15, "O2+": 2e14, "O+": 0.0, "O-": 2e14}), 4242),
+    "block": (block_deck(), 4242),
+}
+
+
+def ulps(a, b):
+    ia = np.ascontiguousarray(a, np.float32).view(np.int32).astype(np.int64)
+    ib = np.ascontiguousarray(b, np.float32).view(np.int32).astype(np.int64)
+    return np.abs(ia - ib)
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_device_load_equals_host_load(name):
+    deck, seed = CASES[name]
+    kw = dict(seed=seed, cap_per_cell=256 if name == "block" else 0)
+    host = hpic.Case(deck, **kw)
+    dev = hpic.Case(deck, gpu_load=1, **kw)
+    for s in range(host.info.nsp):
+        ch, (xh, yh, vxh, vyh, vzh) = host.particles(s)
+        cd, (xd, yd, vxd, vyd, vzd) = dev.particles(s)
+        assert np.array_equal(ch, cd), f"species {s}: counts"
+        for a, b in ((xh, xd), (yh, yd), (vzh, vzd)):
+            assert np.array_equal(a.view(np.uint32), b.view(np.uint32)), f"species {s}"
+        for a, b in ((vxh, vxd), (vyh, vyd)):
+            d = ulps(a, b)
+            assert d.max(initial=0) <= 1
+            assert int((d > 0).sum()) <= max(2, a.size // 1_000_000)
+    if name.startswith("edge"):
+        counts, _ = host.particles(0)
+        assert counts.max() == counts.min() + 2  # one cell lost its edge particle to a neighbour
+
+
+def test_device_load_set_up_has_no_host_particles():
+    deck, seed = CASES["ar_65x33"]
+    S = hpic.Setup(deck, seed=seed, gpu_load=1)
+    with pytest.raises(hpic.HpicError):
+        S.particles(0)
+    c = hpic.Case(setup=S, seed=seed, gpu_load=1)
+    assert c.particles(0)[0].sum() > 0
