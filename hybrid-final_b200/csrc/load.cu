@@ -6,11 +6,13 @@
 // per particle (speed index, azimuth, polar cosine, x, y), the cell from the
 // integer part of the position.  Particle k of a species starts at draw 5k,
 // reached by jump-ahead (16807^5k mod 2^31-1), so every thread generates its
-// own run of particles.  A draw of exactly 1.0f (seeds within 64 of 2^31-2)
-// puts a particle on the next cell's edge: such "edge" particles are listed,
-// the list is ordered on the host, and each particle's slot follows from it:
-//   own particle of cell L: edges into L first, then L's own particles in
-//     load order less those that left;
+// own run of particles.  A position whose float sum i + r rounds up to i + 1
+// (r within half an ulp of 1 at that magnitude, or a draw of exactly 1.0f)
+// puts the particle in the next cell: such "edge" particles (about one in
+// 10^5 on a 512-column grid) are listed, the list is ordered on the host, and
+// every particle's slot follows from it:
+//   own particle of cell L: edges into L first (they come from cells loaded
+//     earlier), then L's own particles in load order less those that left;
 //   edge particle into D: after the edges into D with smaller k.
 // These are the places the host's stable counting sort gives.
 #include <algorithm>
@@ -26,8 +28,7 @@ namespace {
 
 constexpr uint32_t PM_M = 2147483647u;
 constexpr int LOAD_RUN = 16;       // particles per thread (one jump-ahead each)
-constexpr int EDGE_CAP = 4096;     // edge particles listed per species
-constexpr int EDGE_SCAN_MAX = 256; // above this the host places the species
+constexpr int EDGE_CAP = 1 << 20;  // edge particles listed per species
 
 // a * b mod 2^31 - 1 for a, b < 2^31
 __device__ __forceinline__ uint32_t pm_mul(uint32_t a, uint32_t b) {
@@ -65,6 +66,7 @@ struct LoadArgs {
     int *dest;         // [np] cell of each particle
     int *edge_n;       // edge particles found
     long long *edge_k; // [EDGE_CAP]
+    int *edge_d;       // [EDGE_CAP] their cells
 };
 
 constexpr double MPI_D = 3.14159265358979323846;
@@ -101,7 +103,10 @@ __global__ void k_load_gen(LoadArgs a) {
         a.dest[k] = D;
         if (D != L) {
             const int e = atomicAdd(a.edge_n, 1);
-            if (e < EDGE_CAP) a.edge_k[e] = k;
+            if (e < EDGE_CAP) {
+                a.edge_k[e] = k;
+                a.edge_d[e] = D;
+            }
         }
     }
 }
@@ -113,8 +118,10 @@ struct PlaceArgs {
     const float *tmp;
     const int *dest;
     const long long *ek; // edge particles, ascending k
-    const int *esrc, *edst;
+    const int *eslot;    // the slot of each in its cell
     int ne;
+    const int *in_n;     // [C] edges into the cell
+    const int *out_first, *out_n; // [C] the cell's own edges: first index in ek, count
     DevSpecies sp;
 };
 
@@ -125,16 +132,17 @@ __global__ void k_load_place(PlaceArgs a) {
     const int D = a.dest[k];
     int slot;
     if (D == L) {
-        int in = 0, out_before = 0;
-        for (int e = 0; e < a.ne; e++) {
-            in += a.edst[e] == L;
-            out_before += a.esrc[e] == L && a.ek[e] < k;
-        }
-        slot = in + (int)(k % a.npc) - out_before;
+        int ob = 0; // own edges that left before k
+        for (int e = a.out_first[L], e1 = e + a.out_n[L]; e < e1; e++) ob += a.ek[e] < k;
+        slot = a.in_n[L] + (int)(k % a.npc) - ob;
     } else {
-        int before = 0;
-        for (int e = 0; e < a.ne; e++) before += a.edst[e] == D && a.ek[e] < k;
-        slot = before;
+        int lo = 0, hi = a.ne; // k is in ek: find it
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (a.ek[mid] <= k) lo = mid;
+            else hi = mid;
+        }
+        slot = a.eslot[lo];
     }
     const size_t q = (size_t)D * a.sp.cap + (size_t)slot;
     a.sp.x[q] = a.tmp[k];
@@ -168,14 +176,13 @@ hp_status device_load(hp_case *c, int isp) {
             return cuda_fail(cudaGetLastError(), "device load");
         return HP_OK;
     }
-    DevBuf<int> d_lc, d_dest, d_en, d_esrc, d_edst;
+    DevBuf<int> d_lc, d_dest, d_en, d_ed;
     DevBuf<float> d_tmp;
     DevBuf<long long> d_ek;
     cudaError_t e;
     if ((e = d_lc.alloc(lc.size())) != cudaSuccess || (e = d_dest.alloc((size_t)np)) != cudaSuccess ||
         (e = d_en.alloc(1)) != cudaSuccess || (e = d_tmp.alloc(5 * (size_t)np)) != cudaSuccess ||
-        (e = d_ek.alloc(EDGE_CAP)) != cudaSuccess || (e = d_esrc.alloc(EDGE_SCAN_MAX)) != cudaSuccess ||
-        (e = d_edst.alloc(EDGE_SCAN_MAX)) != cudaSuccess)
+        (e = d_ek.alloc(EDGE_CAP)) != cudaSuccess || (e = d_ed.alloc(EDGE_CAP)) != cudaSuccess)
         return cuda_fail(e, "device load buffers");
     if ((e = cudaMemcpy(d_lc.p, lc.data(), lc.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemset(d_en.p, 0, 4)) != cudaSuccess)
@@ -194,43 +201,54 @@ hp_status device_load(hp_case *c, int isp) {
     a.dest = d_dest.p;
     a.edge_n = d_en.p;
     a.edge_k = d_ek.p;
+    a.edge_d = d_ed.p;
     const long long runs = (np + LOAD_RUN - 1) / LOAD_RUN;
     k_load_gen<<<(unsigned)((runs + 255) / 256), 256>>>(a);
     int ne = 0;
     if ((e = cudaGetLastError()) != cudaSuccess || (e = cudaMemcpy(&ne, d_en.p, 4, cudaMemcpyDeviceToHost)) != cudaSuccess)
         return cuda_fail(e, "device load (generate)");
-    // edge particles, ascending k, with their source and destination cells
-    std::vector<long long> ek((size_t)std::min(ne, EDGE_CAP));
-    std::vector<int> esrc(ek.size()), edst(ek.size());
-    if (!ek.empty() && (e = cudaMemcpy(ek.data(), d_ek.p, ek.size() * 8, cudaMemcpyDeviceToHost)) != cudaSuccess)
-        return cuda_fail(e, "device load (edges)");
-    std::sort(ek.begin(), ek.end());
-    for (size_t q = 0; q < ek.size(); q++) {
-        esrc[q] = lc[(size_t)(ek[q] / npc)];
-        if ((e = cudaMemcpy(&edst[q], d_dest.p + ek[q], 4, cudaMemcpyDeviceToHost)) != cudaSuccess)
-            return cuda_fail(e, "device load (edges)");
-    }
-    if (ne > EDGE_SCAN_MAX) {
+    if (ne > EDGE_CAP) {
         set_error("device load: " + std::to_string(ne) + " particles on cell edges; load this deck on the host");
         return HP_ERR_UNSUPPORTED;
     }
-    for (int L : lc) cnt[(size_t)L] = npc;
-    for (size_t q = 0; q < ek.size(); q++) {
-        cnt[(size_t)esrc[q]]--;
-        cnt[(size_t)edst[q]]++;
+    // edge particles in ascending k, their cells and their slots there
+    std::vector<long long> ek((size_t)ne);
+    std::vector<int> ed((size_t)ne);
+    if (ne && ((e = cudaMemcpy(ek.data(), d_ek.p, ek.size() * 8, cudaMemcpyDeviceToHost)) != cudaSuccess ||
+               (e = cudaMemcpy(ed.data(), d_ed.p, ed.size() * 4, cudaMemcpyDeviceToHost)) != cudaSuccess))
+        return cuda_fail(e, "device load (edges)");
+    std::vector<size_t> ord((size_t)ne);
+    for (size_t q = 0; q < ord.size(); q++) ord[q] = q;
+    std::sort(ord.begin(), ord.end(), [&](size_t u, size_t v) { return ek[u] < ek[v]; });
+    std::vector<long long> eks((size_t)ne);
+    std::vector<int> eslot((size_t)ne), in_n((size_t)s.Csize, 0), out_first((size_t)s.Csize, 0),
+        out_n((size_t)s.Csize, 0);
+    for (size_t q = 0; q < ord.size(); q++) {
+        eks[q] = ek[ord[q]];
+        const int D = ed[ord[q]], L = lc[(size_t)(eks[q] / npc)];
+        eslot[q] = in_n[(size_t)D]++;
+        if (out_n[(size_t)L]++ == 0) out_first[(size_t)L] = (int)q;
     }
-    for (int cell = 0; cell < s.Csize; cell++)
+    for (int L : lc) cnt[(size_t)L] = npc;
+    for (int cell = 0; cell < s.Csize; cell++) {
+        cnt[(size_t)cell] += in_n[(size_t)cell] - out_n[(size_t)cell];
         if (2 * cnt[(size_t)cell] > sp.cap) {
             set_error("cell " + std::to_string(cell) + " holds " + std::to_string(cnt[(size_t)cell]) +
                       " particles; the slot pool takes at most " + std::to_string(sp.cap / 2));
             return HP_ERR_CAPACITY;
         }
+    }
     DevBuf<long long> d_eks;
-    if ((e = d_eks.alloc(ek.size())) != cudaSuccess) return cuda_fail(e, "device load buffers");
-    if (!ek.empty() &&
-        ((e = cudaMemcpy(d_eks.p, ek.data(), ek.size() * 8, cudaMemcpyHostToDevice)) != cudaSuccess ||
-         (e = cudaMemcpy(d_esrc.p, esrc.data(), esrc.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess ||
-         (e = cudaMemcpy(d_edst.p, edst.data(), edst.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess))
+    DevBuf<int> d_eslot, d_in, d_of, d_on;
+    if ((e = d_eks.alloc(eks.size())) != cudaSuccess || (e = d_eslot.alloc(eslot.size())) != cudaSuccess ||
+        (e = d_in.alloc(in_n.size())) != cudaSuccess || (e = d_of.alloc(out_first.size())) != cudaSuccess ||
+        (e = d_on.alloc(out_n.size())) != cudaSuccess)
+        return cuda_fail(e, "device load buffers");
+    if ((ne && ((e = cudaMemcpy(d_eks.p, eks.data(), eks.size() * 8, cudaMemcpyHostToDevice)) != cudaSuccess ||
+                (e = cudaMemcpy(d_eslot.p, eslot.data(), eslot.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess)) ||
+        (e = cudaMemcpy(d_in.p, in_n.data(), in_n.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(d_of.p, out_first.data(), out_first.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(d_on.p, out_n.data(), out_n.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess)
         return cuda_fail(e, "device load (edges)");
     PlaceArgs b;
     b.lc = d_lc.p;
@@ -239,9 +257,11 @@ hp_status device_load(hp_case *c, int isp) {
     b.tmp = d_tmp.p;
     b.dest = d_dest.p;
     b.ek = d_eks.p;
-    b.esrc = d_esrc.p;
-    b.edst = d_edst.p;
-    b.ne = (int)ek.size();
+    b.eslot = d_eslot.p;
+    b.ne = ne;
+    b.in_n = d_in.p;
+    b.out_first = d_of.p;
+    b.out_n = d_on.p;
     b.sp = sp;
     k_load_place<<<(unsigned)((np + 255) / 256), 256>>>(b);
     if ((e = cudaGetLastError()) != cudaSuccess ||

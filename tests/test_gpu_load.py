@@ -28,6 +28,9 @@ CASES = {
     "edge_x": (ccp_deck(17, 9, 0.005, 0.0025, ppc=10), edge_seed(4)),
     "edge_y": (ccp_deck(17, 9, 0.005, 0.0025, ppc=10), edge_seed(5)),
     "ar_65x33": (ccp_deck(65, 33, 0.02, 0.01, ppc=30), 99),
+    # i + r rounds up to i + 1 for r within half an ulp of 1: tens of edge
+    # particles per species at 256 columns
+    "ar_257x129": (ccp_deck(257, 129, 0.08, 0.04, ppc=50), 2024),
     "aro2": (ccp_deck(33, 17, 0.01, 0.005, gas="ArO2", ppc=20, pressure_torr=0.1, voltage=200.0, te_ev=3.0,
                       ion_density={"Ar+": 1e15, "O2+": 2e14, "O+": 0.0, "O-": 2e14}), 4242),
     "block": (block_deck(), 4242),
@@ -59,6 +62,9 @@ def test_device_load_equals_host_load(name):
     if name.startswith("edge"):
         counts, _ = host.particles(0)
         assert counts.max() == counts.min() + 2  # one cell lost its edge particle to a neighbour
+    if name == "ar_257x129":
+        counts, _ = host.particles(0)
+        assert (counts != counts.max()).sum() + (counts != counts.min()).sum() > 10  # many edges met
 
 
 def test_device_load_set_up_has_no_host_particles():
