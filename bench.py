@@ -167,7 +167,7 @@ def cpu_baseline(setup, case_opts, budget_s=20.0):
     for s in range(setup.info.nsp):
         counts, arrs = setup.particles(s, layout=0)
         o.set_particles(s, counts, *arrs)
-    o.Deposit()
+    o.DepositBasic()
     pushes, t_used, steps = 0, 0.0, 0
     while steps < 1 or (t_used < budget_s and steps < 20):
         n = sum(int(oracle.lib().or_num_particles(o.h, s)) for s in range(setup.info.nsp))
@@ -208,7 +208,7 @@ def fp64_check(stream, steps=400):
     t0 = time.perf_counter()
     o = oracle.from_setup(S, 64, field_mode=2)
     o.c.move_mode = 1
-    o.Deposit()
+    o.DepositBasic()
     o.run(0, steps, accumulate=True)
     d, p, m = o.averages()
     d64, p64 = d.reshape(S.info.nsp, -1) / m, p / m

@@ -42,9 +42,11 @@ hp_status batch_dev_build(hp_case *const *cases, int n, BatchDev &b) {
     std::vector<int> part(n + 1, 0), cell(n + 1, 0), node(n + 1, 0);
     b.max_g = 0;
     b.any_eedf = false;
+    b.max_smt = 0;
     for (int i = 0; i < n; i++) {
         hd[i] = cases[i]->h;
         b.any_eedf |= cases[i]->h.eedf_every > 0;
+        b.max_smt = std::max(b.max_smt, cases[i]->s.N_smt);
         const Setup &s = cases[i]->s;
         part[i + 1] = part[i] + s.nsp * s.Csize;
         cell[i + 1] = cell[i] + s.Csize;
@@ -118,7 +120,7 @@ hp_status run_step(const BatchDev &b, const LaunchCfg &lc, int gas, cudaStream_t
     CK(launch_sort(b.d_cases, b.d_part, b.n, b.n_part, lc, st));
     if (gas != GAS_AR) CK(launch_mcc_oxy(b.d_cases, b.d_cell, b.n, b.n_cell, gas, st));
     else CK(launch_mcc_ar(b.d_cases, b.d_cell, b.n, b.n_cell, lc, st));
-    CK(launch_deposit(b.d_cases, b.d_part, b.d_node, b.n, b.n_part, b.n_node, lc, st));
+    CK(launch_deposit(b.d_cases, b.d_part, b.d_node, b.n, b.n_part, b.n_node, lc, st, b.max_smt));
     CK(launch_accumulate(b.d_cases, b.d_node, b.n, b.n_node, st));
     if (b.any_eedf) CK(launch_eedf(b.d_cases, b.d_cell, b.n, b.n_cell, st));
     return HP_OK;

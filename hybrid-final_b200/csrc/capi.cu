@@ -140,6 +140,7 @@ void fill_info(const Setup &s, hp_case_info *out) {
     out->mcc_subcycles = s.mcc_n;
     out->dt = s.dt; out->dx = s.dx; out->dy = s.dy;
     out->mcc_stride = s.main_gas == GAS_AR ? 8 : 72;
+    out->n_smt = s.N_smt;
 }
 
 // Collision probability per cell from its lower-left node
@@ -268,6 +269,9 @@ hp_status build_device(hp_case *c) {
         TRY(dupload(c, (float **)&h.eps, eps));
     }
     TRY(dupload(c, (float **)&h.dep_factor, s.dep_factor));
+    h.n_smt = s.N_smt;
+    TRY(dupload(c, (int **)&h.dens_region, s.dens_region));
+    if (s.N_smt > 0) TRY(dalloc(c, &h.smt, (size_t)s.nsp * G));
     if (c->opts.move_mode != 0 && c->opts.move_mode != 1) return set_error("move_mode must be 0 or 1"), HP_ERR_ARG;
     for (int isp = 0; isp < s.nsp; isp++) {
         // a far mover's key holds its rank r < cap/2 in 18 bits
@@ -444,9 +448,12 @@ hp_status op_mcc(hp_case *c, cudaStream_t st) {
     cudaError_t e = launch_mcc_ar(c->d_case, c->d_items + 2, 1, c->s.Csize, c->lc, st);
     return e == cudaSuccess ? HP_OK : cuda_fail(e, "mcc");
 }
-hp_status op_deposit(hp_case *c, cudaStream_t st) {
+// smooth: DEPOSIT = Deposit_cuda with its DensitySmoothing passes
+// (src/cuda_start.cu:32, src/cuda_Deposit.cu:3-20); the initial deposit
+// before the loop is Deposit_Basic, without them (src/cuda_main.cu:28)
+hp_status op_deposit(hp_case *c, cudaStream_t st, bool smooth) {
     cudaError_t e = launch_deposit(c->d_case, c->d_items, c->d_items + 4, 1, c->s.nsp * c->s.Csize, c->s.Gsize,
-                                   c->lc, st);
+                                   c->lc, st, smooth ? c->s.N_smt : 0);
     return e == cudaSuccess ? HP_OK : cuda_fail(e, "deposit");
 }
 
@@ -457,7 +464,7 @@ hp_status one_step(hp_case *c, cudaStream_t st) {
     TRY(op_move(c, st));
     TRY(op_sort(c, st));
     TRY(op_mcc(c, st));
-    TRY(op_deposit(c, st));
+    TRY(op_deposit(c, st, true));
     e = launch_accumulate(c->d_case, c->d_items + 4, 1, c->s.Gsize, st);
     if (e == cudaSuccess && c->h.eedf_every > 0) e = launch_eedf(c->d_case, c->d_items + 2, 1, c->s.Csize, st);
     return e == cudaSuccess ? HP_OK : cuda_fail(e, "accumulate");
@@ -655,7 +662,7 @@ static hp_status case_from(Setup s, const hp_case_opts *opts, hp_case **out) {
         cudaError_t e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) st = cuda_fail(e, "cudaStreamCreate");
     }
-    if (st == HP_OK) st = op_deposit(c, c->own_stream); // Deposit_Basic before the loop (src/cuda_main.cu:28)
+    if (st == HP_OK) st = op_deposit(c, c->own_stream, false); // Deposit_Basic before the loop (src/cuda_main.cu:28)
     if (st == HP_OK) {
         cudaError_t e = cudaStreamSynchronize(c->own_stream);
         if (e != cudaSuccess) st = cuda_fail(e, "initial deposit");
@@ -785,7 +792,8 @@ hp_status hp_Field(hp_case *c, void *stream) { OP_BODY(op_field) }
 hp_status hp_Move(hp_case *c, void *stream) { OP_BODY(op_move) }
 hp_status hp_SortBoundary(hp_case *c, void *stream) { OP_BODY(op_sort) }
 hp_status hp_MCC(hp_case *c, void *stream) { OP_BODY(op_mcc) }
-hp_status hp_Deposit(hp_case *c, void *stream) { OP_BODY(op_deposit) }
+static hp_status op_deposit_step(hp_case *c, cudaStream_t st) { return op_deposit(c, st, true); }
+hp_status hp_Deposit(hp_case *c, void *stream) { OP_BODY(op_deposit_step) }
 
 hp_status hp_step(hp_case *c, int nsteps, void *stream) {
     if (!c || nsteps < 0) return HP_ERR_ARG;

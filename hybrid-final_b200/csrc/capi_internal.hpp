@@ -70,6 +70,7 @@ struct BatchDev {
     int n = 0, n_part = 0, n_cell = 0, n_node = 0;
     int max_g = 0;
     bool any_eedf = false;
+    int max_smt = 0; // most density smoothing passes of any case
     // PCG groups for every cluster cap 1,2,4,8,16: lists of case indices per
     // cluster size, concatenated in d_lists
     int *d_lists = nullptr;

@@ -49,6 +49,9 @@ struct DevCase {
     const int *boundary, *face, *cond_id; // [G]
     const float *eps;       // [C] EPS0 * eps_r
     const float *dep_factor;// [G]
+    int n_smt;                      // 1-2-1 smoothing passes per Deposit (DensitySmoothing)
+    const int *dens_region;         // [G] nodes the smoothing treats as inside
+    double *smt;                    // [nsp*G] smoothing scratch (n_smt > 0)
     DevSpecies sp[DMAXSP];
     // field
     float *Ex, *Ey, *phi, *phi_p;   // [G]

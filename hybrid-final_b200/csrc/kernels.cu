@@ -1136,6 +1136,60 @@ __global__ void __launch_bounds__(256) k_deposit_nodes(const DevCase *__restrict
     d.b64[n] = d.st[2 * d.G + n] != 0.0f ? source : 0.0;
 }
 
+// Smooth_121_x / Smooth_121_y (src/cuda_Deposit.cu:105-170): one pass of the
+// 1-2-1 filter along x (den -> smt), then along y (smt -> den), with the
+// reference's weights at the edges of the density region (a doubled
+// neighbour at a wall, 8/4 on an isolated node).  A neighbour whose weight is
+// 0 is not read (the densities are non-negative, so 0 * it adds nothing).
+__device__ __forceinline__ double smooth_121(const int *dr, const double *v, int id, int at, int last, int step) {
+    int a1 = 0, a2 = 1, a3 = 0;
+    if (dr[id]) {
+        if (at == 0) a3 = 2;
+        else if (at == last) a1 = 2;
+        else if (dr[id - step] == 0 && dr[id + step] != 0) a3 = 2;
+        else if (dr[id - step] != 0 && dr[id + step] == 0) a1 = 2;
+        else if (dr[id - step] == 0 && dr[id + step] == 0) a2 = 4;
+        else { a1 = 1; a3 = 1; }
+    } else {
+        a2 = 0;
+    }
+    const double l = a1 ? (double)a1 * v[id - step] : 0.0;
+    const double r = a3 ? (double)a3 * v[id + step] : 0.0;
+    return 0.25 * (l + (double)(2 * a2) * v[id] + r);
+}
+
+__global__ void __launch_bounds__(256) k_smooth(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
+                                                int ncases, int items, int pass, int along_y) {
+    const int t = (int)(blockIdx.x * (unsigned)blockDim.x + threadIdx.x);
+    if (t >= items) return;
+    const int ci = find_case(item_start, ncases, t);
+    const DevCase &d = cases[ci];
+    if (pass >= d.n_smt) return;
+    const int n = t - item_start[ci];
+    const int x = n / d.ngy, y = n - x * d.ngy;
+    for (int s = 0; s < d.nsp; s++) {
+        const size_t o = (size_t)s * d.G;
+        if (!along_y) d.smt[o + n] = smooth_121(d.dens_region, d.den + o, n, x, d.ngx - 1, d.ngy);
+        else d.den[o + n] = smooth_121(d.dens_region, d.smt + o, n, y, d.ngy - 1, 1);
+    }
+}
+
+// SumSource + PCG_Set after the smoothing: rho/eps0 and the right-hand side
+__global__ void __launch_bounds__(256) k_source(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
+                                                int ncases, int items) {
+    const int t = (int)(blockIdx.x * (unsigned)blockDim.x + threadIdx.x);
+    if (t >= items) return;
+    const int ci = find_case(item_start, ncases, t);
+    const DevCase &d = cases[ci];
+    if (d.n_smt <= 0) return;
+    const int n = t - item_start[ci];
+    double sum = 0.0;
+    for (int s = 0; s < d.nsp; s++) sum += d.den[(size_t)s * d.G + n] * (double)d.sp[s].q_density;
+    const double source = sum / 8.8542e-12;
+    d.source[n] = source;
+    d.b64[n] = d.st[2 * d.G + n] != 0.0f ? source : 0.0;
+}
+
 // ------------------------------------------------------------------ Field
 __device__ __forceinline__ float spmv_f(const float *__restrict__ st, int G, int ngy, int n, int i, int j, int ngx,
                                         const float *__restrict__ v) {
@@ -1675,7 +1729,7 @@ cudaError_t launch_mcc_ar(const DevCase *cases, const int *item_start, int ncase
 }
 
 cudaError_t launch_deposit(const DevCase *cases, const int *cell_items, const int *node_items, int ncases,
-                           int n_cell_items, int n_node_items, const LaunchCfg &lc, cudaStream_t st) {
+                           int n_cell_items, int n_node_items, const LaunchCfg &lc, cudaStream_t st, int max_smt) {
     const int tpb = 32 * std::min(std::max(lc.warps_per_block, 1), 16);
     if (n_cell_items > 0)
         k_deposit_cells<<<blocks_for((long long)(n_cell_items + DEP_G - 1) / DEP_G * 32, tpb), tpb, 0, st>>>(cases, cell_items, ncases,
@@ -1684,6 +1738,12 @@ cudaError_t launch_deposit(const DevCase *cases, const int *cell_items, const in
     if (e != cudaSuccess) return e;
     if (n_node_items > 0)
         k_deposit_nodes<<<blocks_for(n_node_items, 256), 256, 0, st>>>(cases, node_items, ncases, n_node_items);
+    if (max_smt > 0 && n_node_items > 0) {
+        for (int p = 0; p < max_smt; p++)
+            for (int yy = 0; yy < 2; yy++)
+                k_smooth<<<blocks_for(n_node_items, 256), 256, 0, st>>>(cases, node_items, ncases, n_node_items, p, yy);
+        k_source<<<blocks_for(n_node_items, 256), 256, 0, st>>>(cases, node_items, ncases, n_node_items);
+    }
     return cudaGetLastError();
 }
 

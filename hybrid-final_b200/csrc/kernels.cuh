@@ -31,8 +31,9 @@ cudaError_t launch_mcc_ar(const DevCase *cases, const int *item_start, int ncase
                           cudaStream_t st);
 // Deposit: per-cell CIC sums, then node gather + boundary scale + rho/eps0 + RHS
 // (src/cuda_Deposit.cu:3-20,30-104,277-325)
+// max_smt: the most 1-2-1 smoothing passes any of the cases asks for (0: none)
 cudaError_t launch_deposit(const DevCase *cases, const int *cell_items, const int *node_items, int ncases,
-                           int n_cell_items, int n_node_items, const LaunchCfg &lc, cudaStream_t st);
+                           int n_cell_items, int n_node_items, const LaunchCfg &lc, cudaStream_t st, int max_smt);
 // Field: PCG (src/cuda_Field.cu:133-181,942-1072), potential assembly and
 // E at nodes (src/cuda_Field.cu:2-42,500-558,698-846).  The PCG runs one
 // cluster per case; cases are grouped by cluster size (a launch has one

@@ -77,6 +77,9 @@ __global__ void __launch_bounds__(256) k_na_nodes(const hp::DevCase *__restrict_
 
 extern "C" hp_status hp_Deposit_noalloc(hp_case *c, double *den_out, void *stream) {
     if (!c || !den_out) return hpi::set_error("null argument"), HP_ERR_ARG;
+    if (c->s.N_smt > 0)
+        return hpi::set_error("hp_Deposit_noalloc: the deck smooths its densities (DensitySmoothing); use hp_Deposit"),
+               HP_ERR_UNSUPPORTED;
     const long long need = (long long)c->s.nsp * c->s.Csize;
     if (need > HP_NOALLOC_CELLS) {
         hpi::set_error("hp_Deposit_noalloc: the case has " + std::to_string(need) +

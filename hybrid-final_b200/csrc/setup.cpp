@@ -313,7 +313,7 @@ void read_method(const JVal &root, Setup &s) { // src/start.c:732-747
     ivnzc(m, "HistoryDivide");
     s.N_ave = ivnzc(m, "AverageIter");
     s.N_smt = inum(m, "DensitySmoothing");
-    if (s.N_smt > 0) unsupported("density smoothing (DensitySmoothing > 0)");
+    if (s.N_smt < 0) s.N_smt = 0;
     ivnzc(m, "ParticleLimit");
     if (inum(m, "ConstB_Flag")) unsupported("constant magnetic field (ConstB_Flag)");
 }

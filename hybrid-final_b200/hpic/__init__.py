@@ -52,7 +52,8 @@ class CaseInfo(C.Structure):
                 ("Csize", C.c_int), ("nsp", C.c_int), ("main_gas", C.c_int), ("cond_numr", C.c_int),
                 ("n_unknowns", C.c_int), ("cap", C.c_int * 8), ("mcc_subcycles", C.c_int), ("dt", C.c_double),
                 ("dx", C.c_double), ("dy", C.c_double), ("tstep", C.c_int64), ("device_bytes", C.c_size_t),
-                ("pcg_cluster", C.c_int), ("pcg_block", C.c_int), ("field_mode", C.c_int), ("mcc_stride", C.c_int)]
+                ("pcg_cluster", C.c_int), ("pcg_block", C.c_int), ("field_mode", C.c_int), ("mcc_stride", C.c_int),
+                ("n_smt", C.c_int)]
 
 
 class Tune(C.Structure):

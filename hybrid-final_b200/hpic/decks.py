@@ -46,7 +46,7 @@ def _channel_keys(gas):
 def ccp_deck(ngx, ngy, xlen, ylen, *, gas="Ar", pressure_torr=0.05, voltage=100.0,
              freq=13.56e6, steps_per_cycle=400, ppc=50, density=1e15, te_ev=2.0,
              ti_ev=0.026, gas_k=300.0, max_np_factor=4, aro2_ratio=(80, 20),
-             ion_density=None, pcg_tol=1e-3):
+             ion_density=None, pcg_tol=1e-3, smoothing=0):
     """Build one CCP deck.
 
     ppc is the macro-particles per cell per species at `density`; np2c is
@@ -113,7 +113,7 @@ def ccp_deck(ngx, ngy, xlen, ylen, *, gas="Ar", pressure_torr=0.05, voltage=100.
             "TimeStep_PIC": steps_per_cycle, "TimeStep_Conti": 200,
             "FieldTest": {"Laplace_Test_Flag": 0, "Laplace_Field_Solver": 8, "Laplace_Field_Tec_Save": 0},
             "PCGMarginOfError": pcg_tol, "HistoryMax": 1000000, "HistoryDivide": 4,
-            "AverageIter": steps_per_cycle, "DensitySmoothing": 0,
+            "AverageIter": steps_per_cycle, "DensitySmoothing": smoothing,
             "ParticleLimit": max_np, "ConstB_Flag": 0,
             "ContinuitySteadyState": {"Flag": 0, "Check": 1, "Margin": 1.0},
             "PowerDrivenOption": {"Interval": 5.0, "VoltageUpDownRatio": 0.05},

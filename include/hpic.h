@@ -133,6 +133,7 @@ typedef struct hp_case_info {
     int pcg_block;         /* threads per CTA in the field solve */
     int field_mode;        /* solver in use: 2 falls back to 1 when the operator is not separable */
     int mcc_stride;        /* collision counters per cell in HP_GRID_MCC_COUNT (8 Ar, 72 O2 and Ar/O2) */
+    int n_smt;             /* 1-2-1 density smoothing passes per Deposit (the deck's DensitySmoothing) */
 } hp_case_info;
 hp_status hp_case_get_info(const hp_case *c, hp_case_info *out);
 hp_status hp_setup_get_info(const hp_setup *s, hp_case_info *out);

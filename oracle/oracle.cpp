@@ -106,7 +106,7 @@ struct SimBase {
     virtual void move() = 0;
     virtual void sort() = 0;
     virtual void mcc(int64_t) = 0;
-    virtual void deposit() = 0;
+    virtual void deposit(bool smooth) = 0;
     virtual void accumulate() = 0;
 };
 
@@ -1124,7 +1124,26 @@ template <class R> struct Sim : SimBase {
     }
 
     // ------------------------------------------------------------ Deposit
-    void deposit() override {
+    // Smooth_121_x/_y (src/cuda_Deposit.cu:105-170) in double, as the kernels
+    double smooth_121(const std::vector<double> &v, size_t o, int id, int at, int last, int step) const {
+        const int *dr = c.dens_region;
+        int a1 = 0, a2 = 1, a3 = 0;
+        if (dr[id]) {
+            if (at == 0) a3 = 2;
+            else if (at == last) a1 = 2;
+            else if (dr[id - step] == 0 && dr[id + step] != 0) a3 = 2;
+            else if (dr[id - step] != 0 && dr[id + step] == 0) a1 = 2;
+            else if (dr[id - step] == 0 && dr[id + step] == 0) a2 = 4;
+            else { a1 = 1; a3 = 1; }
+        } else {
+            a2 = 0;
+        }
+        const double l = a1 ? (double)a1 * v[o + (size_t)(id - step)] : 0.0;
+        const double r = a3 ? (double)a3 * v[o + (size_t)(id + step)] : 0.0;
+        return 0.25 * (l + (double)(2 * a2) * v[o + (size_t)id] + r);
+    }
+
+    void deposit(bool smooth) override {
         for (int s = 0; s < c.nsp; s++) {
             Sp &p = sp[s];
             par_for(C, [&](int cell) {
@@ -1149,7 +1168,6 @@ template <class R> struct Sim : SimBase {
         }
         for (int n = 0; n < G; n++) {
             const int i = n / c.ngy, j = n - i * c.ngy, ncy = c.ncy;
-            double sum = 0.0;
             for (int s = 0; s < c.nsp; s++) {
                 double d = 0.0;
                 if (i < c.ncx && j < ncy) d += cw[s][0][i * ncy + j];
@@ -1158,8 +1176,22 @@ template <class R> struct Sim : SimBase {
                 if (i > 0 && j > 0) d += cw[s][3][(i - 1) * ncy + j - 1];
                 d *= (double)c.dep_factor[n];
                 den[(size_t)s * G + n] = d;
-                sum += d * (double)c.q_density[s];
             }
+        }
+        if (smooth && c.n_smt > 0) {
+            std::vector<double> smt(den.size());
+            for (int pass = 0; pass < c.n_smt; pass++) {
+                for (int s = 0; s < c.nsp; s++)
+                    for (int n = 0; n < G; n++)
+                        smt[(size_t)s * G + n] = smooth_121(den, (size_t)s * G, n, n / c.ngy, c.ngx - 1, c.ngy);
+                for (int s = 0; s < c.nsp; s++)
+                    for (int n = 0; n < G; n++)
+                        den[(size_t)s * G + n] = smooth_121(smt, (size_t)s * G, n, n % c.ngy, c.ngy - 1, 1);
+            }
+        }
+        for (int n = 0; n < G; n++) {
+            double sum = 0.0;
+            for (int s = 0; s < c.nsp; s++) sum += den[(size_t)s * G + n] * (double)c.q_density[s];
             const double src = sum / 8.8542e-12;
             source[n] = src;
             b64[n] = c.st[2 * G + n] != 0.0f ? src : 0.0;
@@ -1638,7 +1670,8 @@ void or_field(or_sim *s, int64_t tstep) { s->impl->field(tstep); }
 void or_move(or_sim *s) { s->impl->move(); }
 void or_sort(or_sim *s) { s->impl->sort(); }
 void or_mcc(or_sim *s, int64_t tstep) { s->impl->mcc(tstep); }
-void or_deposit(or_sim *s) { s->impl->deposit(); }
+void or_deposit(or_sim *s) { s->impl->deposit(true); }
+void or_deposit_basic(or_sim *s) { s->impl->deposit(false); }
 void or_run(or_sim *s, int64_t tstep0, int nsteps, int accumulate) {
     for (int k = 1; k <= nsteps; k++) {
         const int64_t t = tstep0 + k;
@@ -1646,7 +1679,7 @@ void or_run(or_sim *s, int64_t tstep0, int nsteps, int accumulate) {
         s->impl->move();
         s->impl->sort();
         s->impl->mcc(t);
-        s->impl->deposit();
+        s->impl->deposit(true);
         if (accumulate) {
             s->impl->accumulate();
             const int ev = s->impl->c.eedf_every;

@@ -62,6 +62,9 @@ typedef struct or_case {
     int eedf_every; /* electron energy histogram every k-th step in or_run with accumulation (0 off) */
     float dt_mcc, np2c[5];
     const float *back_den1, *back_den2, *back_vel2, *fluid_den;
+    /* 1-2-1 density smoothing in Deposit (DensitySmoothing passes) */
+    int n_smt;
+    const int *dens_region; /* [G] */
 } or_case;
 
 typedef struct or_sim or_sim;
@@ -94,7 +97,9 @@ void or_field(or_sim *s, int64_t tstep);
 void or_move(or_sim *s);
 void or_sort(or_sim *s);
 void or_mcc(or_sim *s, int64_t tstep);
+/* DEPOSIT (with the deck's smoothing passes) and the initial Deposit_Basic (without) */
 void or_deposit(or_sim *s);
+void or_deposit_basic(or_sim *s);
 /* n full steps from tstep+1; accumulates node averages when ave != 0 */
 void or_run(or_sim *s, int64_t tstep0, int nsteps, int accumulate);
 void or_get_averages(or_sim *s, double *ave_den, double *ave_phi, int64_t *count);

@@ -43,6 +43,7 @@ class OrCase(C.Structure):
         ("dt_mcc", C.c_float),
         ("np2c", C.c_float * 5),
         ("back_den1", _F), ("back_den2", _F), ("back_vel2", _F), ("fluid_den", _F),
+        ("n_smt", C.c_int), ("dens_region", _I),
     ]
 
 
@@ -81,6 +82,7 @@ def lib():
             "or_sort": (None, [P]),
             "or_mcc": (None, [P, C.c_int64]),
             "or_deposit": (None, [P]),
+            "or_deposit_basic": (None, [P]),
             "or_run": (None, [P, C.c_int64, C.c_int, C.c_int]),
             "or_get_averages": (None, [P, _D, _D, C.POINTER(C.c_int64)]),
             "or_num_threads": (C.c_int, []),
@@ -162,6 +164,8 @@ class Oracle:
             c.back_den2 = keep("bd2", t("back_den2"), np.float32)
             c.back_vel2 = keep("bv2", t("back_vel2"), np.float32)
             c.fluid_den = keep("fd", t("fluid_den"), np.float32)
+        c.n_smt = info.n_smt
+        c.dens_region = keep("dr", t("dens_region"), np.int32)
         c.prob = keep("prob", t("prob"), np.float32)
         c.back_vel1 = keep("bv1", t("back_vel1"), np.float32)
         c.vsave = keep("vsave", t("vsave"), np.float32)
@@ -292,7 +296,12 @@ class Oracle:
         lib().or_mcc(self.h, tstep)
 
     def Deposit(self):
+        """DEPOSIT: the per-step deposit, with the deck's smoothing passes."""
         lib().or_deposit(self.h)
+
+    def DepositBasic(self):
+        """Deposit_Basic: the initial deposit before the loop, no smoothing."""
+        lib().or_deposit_basic(self.h)
 
     def run(self, tstep0, nsteps, accumulate=True):
         lib().or_run(self.h, tstep0, nsteps, 1 if accumulate else 0)

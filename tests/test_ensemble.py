@@ -38,7 +38,7 @@ def eedf_errors(h, h64):
 def fp64_averages(S, nsteps):
     o = oracle.from_setup(S, 64, field_mode=2)
     o.c.move_mode = 1
-    o.Deposit()
+    o.DepositBasic()
     o.run(0, nsteps, accumulate=True)
     d, p, n = o.averages()
     return d.reshape(S.info.nsp, -1) / n, p / n, o.eedf()
@@ -49,7 +49,7 @@ def test_fp32_oracle_within_tolerance_of_fp64():
     S = hpic.Setup(ccp_deck(33, 17, 0.01, 0.005, ppc=60), seed=5, **OPTS)
     o = oracle.from_setup(S, 32, field_mode=2)
     o.c.move_mode = 1
-    o.Deposit()
+    o.DepositBasic()
     o.run(0, 400, accumulate=True)
     d, p, n = o.averages()
     d32, p32 = d.reshape(S.info.nsp, -1) / n, p / n

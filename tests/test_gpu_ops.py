@@ -30,6 +30,8 @@ DECKS = {
     "ar_33x17_hv": (ccp_deck(33, 17, 0.01, 0.005, ppc=20, pressure_torr=0.1, voltage=300.0), 777),
     "ar_65x33": (ccp_deck(65, 33, 0.02, 0.01, ppc=30), 99),
     "ar_block_33x21": (block_deck(), 4242),
+    # two 1-2-1 density smoothing passes per Deposit (Smooth_121_x/_y)
+    "ar_33x17_smooth2": (ccp_deck(33, 17, 0.01, 0.005, ppc=20, pressure_torr=0.1, voltage=300.0, smoothing=2), 778),
 }
 # slots per cell where the deck's Max_np / Gsize leaves too little room for
 # the charge that gathers in front of the floating block
@@ -46,7 +48,7 @@ def pair(name, field_mode=0, move_mode=0, **extra):
     for s in range(S.info.nsp):
         counts, arrs = S.particles(s, layout=0)
         o.set_particles(s, counts, *arrs)
-    o.Deposit()  # the library's initial Deposit_Basic
+    o.DepositBasic()  # the library's initial Deposit_Basic
     return case, o
 
 

@@ -49,7 +49,7 @@ def pair(name):
     for s in range(S.info.nsp):
         counts, arrs = S.particles(s, layout=0)
         o.set_particles(s, counts, *arrs)
-    o.Deposit()
+    o.DepositBasic()
     return case, o
 
 

@@ -30,7 +30,7 @@ def _oracle(move_mode, cells_per_step=None, every=3, deck=None):
         vx = np.where(sel, sign * vcx, vx).astype(np.float32)
         vy = np.where(sel, -sign * vcy, vy).astype(np.float32)
         o.set_particles(0, counts, x, y, vx, vy, vz)
-    o.Deposit()
+    o.DepositBasic()
     return S, o
 
 
