@@ -2,7 +2,7 @@
 //
 // The same load as the host's (SetParticleLoad/Copy_HCPtoGCP,
 // src/Particle.c:3-226, src/cuda_Particle.cu:28-58): loading cells in the
-// reference's order, n particles per loading cell, five Park-Miller draws
+// reference's order with their particle counts, five Park-Miller draws
 // per particle (speed index, azimuth, polar cosine, x, y), the cell from the
 // integer part of the position.  Particle k of a species starts at draw 5k,
 // reached by jump-ahead (16807^5k mod 2^31-1), so every thread generates its
@@ -56,7 +56,8 @@ __device__ __forceinline__ float pm_next(uint32_t &seed) {
 
 struct LoadArgs {
     const int *lc;     // loading cells
-    int npc;           // particles per loading cell
+    const long long *ls; // [cells + 1] first particle of each loading cell
+    int nlc;
     long long np;
     uint32_t seed0;
     float vti;
@@ -71,13 +72,26 @@ struct LoadArgs {
 
 constexpr double MPI_D = 3.14159265358979323846;
 
+// the loading cell q with ls[q] <= k < ls[q + 1]
+__device__ __forceinline__ int loading_cell(const long long *ls, int n, long long k) {
+    int lo = 0, hi = n;
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (ls[mid] <= k) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
 __global__ void k_load_gen(LoadArgs a) {
     const long long k0 = ((long long)blockIdx.x * blockDim.x + threadIdx.x) * LOAD_RUN;
     if (k0 >= a.np) return;
     uint32_t q = pm_skip_dev(a.seed0, 5ull * (unsigned long long)k0);
     const long long k1 = k0 + LOAD_RUN < a.np ? k0 + LOAD_RUN : a.np;
+    int li = loading_cell(a.ls, a.nlc, k0);
     for (long long k = k0; k < k1; k++) {
-        const int L = a.lc[k / a.npc];
+        while (k >= a.ls[li + 1]) li++;
+        const int L = a.lc[li];
         const int i = L / a.ncy, j = L - i * a.ncy;
         // maxwellv (src/Particle.c:203-209), in the host's arithmetic
         const int n = (int)((a.nvel - 1) * pm_next(q));
@@ -113,7 +127,8 @@ __global__ void k_load_gen(LoadArgs a) {
 
 struct PlaceArgs {
     const int *lc;
-    int npc;
+    const long long *ls;
+    int nlc;
     long long np;
     const float *tmp;
     const int *dest;
@@ -128,13 +143,14 @@ struct PlaceArgs {
 __global__ void k_load_place(PlaceArgs a) {
     const long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= a.np) return;
-    const int L = a.lc[k / a.npc];
+    const int li = loading_cell(a.ls, a.nlc, k);
+    const int L = a.lc[li];
     const int D = a.dest[k];
     int slot;
     if (D == L) {
         int ob = 0; // own edges that left before k
         for (int e = a.out_first[L], e1 = e + a.out_n[L]; e < e1; e++) ob += a.ek[e] < k;
-        slot = a.in_n[L] + (int)(k % a.npc) - ob;
+        slot = a.in_n[L] + (int)(k - a.ls[li]) - ob;
     } else {
         int lo = 0, hi = a.ne; // k is in ek: find it
         while (hi - lo > 1) {
@@ -168,8 +184,8 @@ hp_status device_load(hp_case *c, int isp) {
     const Setup &s = c->s;
     const DevSpecies &sp = c->h.sp[isp];
     const std::vector<int> &lc = s.load_cells[isp];
-    const int npc = s.load_npc[isp];
-    const long long np = (long long)lc.size() * npc;
+    const std::vector<long long> &ls = s.load_start[isp];
+    const long long np = ls.empty() ? 0 : ls.back();
     std::vector<int> cnt((size_t)s.Csize, 0);
     if (np == 0) {
         if (cudaMemcpy(sp.cnt, cnt.data(), cnt.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess)
@@ -178,18 +194,20 @@ hp_status device_load(hp_case *c, int isp) {
     }
     DevBuf<int> d_lc, d_dest, d_en, d_ed;
     DevBuf<float> d_tmp;
-    DevBuf<long long> d_ek;
+    DevBuf<long long> d_ek, d_ls;
     cudaError_t e;
-    if ((e = d_lc.alloc(lc.size())) != cudaSuccess || (e = d_dest.alloc((size_t)np)) != cudaSuccess ||
+    if ((e = d_lc.alloc(lc.size())) != cudaSuccess || (e = d_ls.alloc(ls.size())) != cudaSuccess || (e = d_dest.alloc((size_t)np)) != cudaSuccess ||
         (e = d_en.alloc(1)) != cudaSuccess || (e = d_tmp.alloc(5 * (size_t)np)) != cudaSuccess ||
         (e = d_ek.alloc(EDGE_CAP)) != cudaSuccess || (e = d_ed.alloc(EDGE_CAP)) != cudaSuccess)
         return cuda_fail(e, "device load buffers");
     if ((e = cudaMemcpy(d_lc.p, lc.data(), lc.size() * 4, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = cudaMemcpy(d_ls.p, ls.data(), ls.size() * 8, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = cudaMemset(d_en.p, 0, 4)) != cudaSuccess)
         return cuda_fail(e, "device load");
     LoadArgs a;
     a.lc = d_lc.p;
-    a.npc = npc;
+    a.ls = d_ls.p;
+    a.nlc = (int)lc.size();
     a.np = np;
     a.seed0 = (uint32_t)s.load_seed[isp];
     a.vti = s.sp[isp].vti;
@@ -225,11 +243,12 @@ hp_status device_load(hp_case *c, int isp) {
         out_n((size_t)s.Csize, 0);
     for (size_t q = 0; q < ord.size(); q++) {
         eks[q] = ek[ord[q]];
-        const int D = ed[ord[q]], L = lc[(size_t)(eks[q] / npc)];
+        const size_t li = (size_t)(std::upper_bound(ls.begin(), ls.end(), eks[q]) - ls.begin()) - 1;
+        const int D = ed[ord[q]], L = lc[li];
         eslot[q] = in_n[(size_t)D]++;
         if (out_n[(size_t)L]++ == 0) out_first[(size_t)L] = (int)q;
     }
-    for (int L : lc) cnt[(size_t)L] = npc;
+    for (size_t q = 0; q < lc.size(); q++) cnt[(size_t)lc[q]] = (int)(ls[q + 1] - ls[q]);
     for (int cell = 0; cell < s.Csize; cell++) {
         cnt[(size_t)cell] += in_n[(size_t)cell] - out_n[(size_t)cell];
         if (2 * cnt[(size_t)cell] > sp.cap) {
@@ -252,7 +271,8 @@ hp_status device_load(hp_case *c, int isp) {
         return cuda_fail(e, "device load (edges)");
     PlaceArgs b;
     b.lc = d_lc.p;
-    b.npc = npc;
+    b.ls = d_ls.p;
+    b.nlc = (int)lc.size();
     b.np = np;
     b.tmp = d_tmp.p;
     b.dest = d_dest.p;

@@ -90,6 +90,51 @@ float maxwell_cdf(float v) {
     return (float)(-2 * v * exp((double)(-v * v)) / sqrt(MPI) + erf((double)v));
 }
 
+// The cells SetParticleLoad (src/Particle.c:3-175) fills, in its order, and
+// the prefix of their counts (start[q] = first particle of cell lc[q]):
+// UNIFORM n_per_cell in the window; EXPONETIAL and COSINE n_per_cell scaled
+// by a Gaussian or cosine profile of the cell centre over every plasma cell
+// (at least Ratio); NP_RATIO Ratio per cell in the window (strict upper bounds).
+void load_cells(const Setup &s, const SpeciesP &p, const SpeciesP &l, std::vector<int> &lc,
+                std::vector<long long> &start) {
+    const int n_per_cell = (int)(p.InitDens * s.dx * s.dy * s.zlength / p.np2c);
+    const float x_left = l.x_center, x_right = l.x_fall, y_top = l.y_center, y_bottom = l.y_fall;
+    const float y0 = y_top / s.dy, y1 = y_bottom / s.dy - 1;
+    const float x0 = x_left / s.dx, x1 = x_right / s.dx - 1;
+    lc.clear();
+    start.assign(1, 0);
+    for (int i = 0; i < s.ncx; i++)
+        for (int j = 0; j < s.ncy; j++) {
+            if (s.plasma_region[(size_t)i * s.ncy + j] != 1) continue;
+            int num = 0;
+            const float xx = (float)i * s.dx + s.dx / 2, yy = (float)j * s.dy + s.dy / 2;
+            switch (l.loadtype) {
+            case 0: num = (i >= x0 && i <= x1 && j >= y0 && j <= y1) ? n_per_cell : 0; break;
+            case 1: {
+                // C semantics: the float arguments promoted to double
+                const float ax = -1 * ((xx - x_left) / x_right) * ((xx - x_left) / x_right);
+                const float ay = -1 * ((yy - y_bottom) / y_top) * ((yy - y_bottom) / y_top);
+                const float wv = (float)(::exp((double)ax) * ::exp((double)ay));
+                num = (int)(n_per_cell * wv);
+                if (num < 1) num = p.Ratio;
+                break;
+            }
+            case 2: {
+                float wv;
+                if (xx >= 0.06) wv = 0;
+                else wv = (float)(::cos((xx - x_left) * MPI / 2 / x_right) * ::cos((yy - y_bottom) * MPI / 2 / y_top));
+                num = (int)(n_per_cell * wv);
+                if (num < 1) num = p.Ratio;
+                break;
+            }
+            default: num = (i >= x0 && i < x1 && j >= y0 && j < y1) ? p.Ratio : 0; break;
+            }
+            if (num <= 0) continue;
+            lc.push_back(i * s.ncy + j);
+            start.push_back(start.back() + num);
+        }
+}
+
 void build_vsave(Setup &s) { // src/Particle.c:183-201
     const float NVTS = 3.3f;
     int nvel = (int)(1. / (1 - maxwell_cdf((float)NVTS)));
@@ -855,28 +900,20 @@ void gas_setting(Setup &s, const BuildOpts &o) { // src/start.c:1999-2051
         int cap = o.cap_per_cell > 0 ? o.cap_per_cell : p.MAXNP / s.Gsize;
         cap = std::max(cap, 32);
         s.cap[isp] = (cap + 31) / 32 * 32;
-        // SetParticleLoad (src/Particle.c:3-50) with SP[0]'s load type and window
+        // SetParticleLoad (src/Particle.c:3-175) with SP[0]'s load type and
+        // window: the loading cells in the reference's order (i outer, j
+        // inner), each with its particle count, and the first particle of each
         const SpeciesP &l = s.sp[0];
-        if (l.loadtype != 0) unsupported("particle load types other than UNIFORM");
-        float Ninit = p.InitDens;
-        int n_per_cell = (int)(Ninit * s.dx * s.dy * s.zlength / p.np2c);
-        float y0 = l.y_center / s.dy, y1 = l.y_fall / s.dy - 1;
-        float x0 = l.x_center / s.dx, x1 = l.x_fall / s.dx - 1;
+        if (l.loadtype == 4) unsupported("particle load type SMARTLOAD (the reference exits on it)");
+        std::vector<int> lc;
+        std::vector<long long> &lstart = s.load_start[isp];
+        load_cells(s, p, l, lc, lstart);
+        const long long np = lstart.back();
         auto &hx = s.h_x[isp], &hy = s.h_y[isp], &hvx = s.h_vx[isp], &hvy = s.h_vy[isp], &hvz = s.h_vz[isp];
         auto &hc = s.h_cell[isp];
-        // loading cells in the reference's order (i outer, j inner) and the
-        // first particle of each
-        std::vector<int> lc;
-        for (int i = 0; i < s.ncx; i++)
-            for (int j = 0; j < s.ncy; j++) {
-                if (s.plasma_region[(size_t)i * s.ncy + j] != 1) continue;
-                if (n_per_cell > 0 && i >= x0 && i <= x1 && j >= y0 && j <= y1) lc.push_back(i * s.ncy + j);
-            }
-        const long long np = (long long)lc.size() * std::max(n_per_cell, 0);
         if (o.defer_load) {
             s.load_deferred = true;
             s.load_cells[isp] = lc;
-            s.load_npc[isp] = std::max(n_per_cell, 0);
             s.load_seed[isp] = pm.seed;
             pm.seed = pm_skip(pm.seed, 5ull * (unsigned long long)np);
             p.np = (int)np;
@@ -886,8 +923,11 @@ void gas_setting(Setup &s, const BuildOpts &o) { // src/start.c:1999-2051
         const long seed0 = pm.seed;
         par_range(np, [&](long long k0, long long k1) {
             ParkMiller q{pm_skip(seed0, 5ull * (unsigned long long)k0)};
+            // the loading cell of particle k0, then walk forward
+            size_t li = (size_t)(std::upper_bound(lstart.begin(), lstart.end(), k0) - lstart.begin()) - 1;
             for (long long k = k0; k < k1; k++) {
-                const int c = lc[(size_t)(k / n_per_cell)];
+                while (k >= lstart[li + 1]) li++;
+                const int c = lc[li];
                 const int i = c / s.ncy, j = c - i * s.ncy;
                 float vx, vy, vz;
                 maxwellv(s, q, p.vti, vx, vy, vz);

@@ -117,8 +117,9 @@ struct Setup {
     // species' first draw; p_count etc. stay empty
     bool load_deferred = false;
     std::vector<int> load_cells[MAXSP];
-    int load_npc[MAXSP] = {0};
     long load_seed[MAXSP] = {0};
+    // first particle of each loading cell (prefix of the counts; size cells + 1)
+    std::vector<long long> load_start[MAXSP];
 };
 
 struct BuildOpts {

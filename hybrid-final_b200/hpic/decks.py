@@ -46,7 +46,7 @@ def _channel_keys(gas):
 def ccp_deck(ngx, ngy, xlen, ylen, *, gas="Ar", pressure_torr=0.05, voltage=100.0,
              freq=13.56e6, steps_per_cycle=400, ppc=50, density=1e15, te_ev=2.0,
              ti_ev=0.026, gas_k=300.0, max_np_factor=4, aro2_ratio=(80, 20),
-             ion_density=None, pcg_tol=1e-3, smoothing=0):
+             ion_density=None, pcg_tol=1e-3, smoothing=0, load_type=0, load_pos=None, ratio=1):
     """Build one CCP deck.
 
     ppc is the macro-particles per cell per species at `density`; np2c is
@@ -82,11 +82,15 @@ def ccp_deck(ngx, ngy, xlen, ylen, *, gas="Ar", pressure_torr=0.05, voltage=100.
         neutral[name] = {"Density": 0.0, "Temp(eV)": 0.026, "Quenching": 1.0}
 
     def sp(sid, dens, temp):
-        return {"S_ID": sid, "Density": dens, "Temp(eV)": temp, "np2c": np2c, "Ratio": 1,
+        return {"S_ID": sid, "Density": dens, "Temp(eV)": temp, "np2c": np2c, "Ratio": ratio,
                 "Max_np": max_np}
 
     ion = density if ion_density is None else ion_density
-    charge = {"Loadtype": 0, "LoadPosition(m)": dict(load),
+    # charged load (src/Particle.c:3-175): 0 uniform in the window, 1 Gaussian
+    # and 2 cosine profiles (X0/Y1 centres, X1/Y0 widths), 3 Ratio per cell in
+    # the window
+    cload = dict(load) if load_pos is None else dict(zip(("X0", "X1", "Y0", "Y1"), load_pos))
+    charge = {"Loadtype": load_type, "LoadPosition(m)": cload,
               "Electron": sp(0, density, te_ev), "Ar+": sp(1, ion.get("Ar+", density) if isinstance(ion, dict) else ion, ti_ev)}
     if gas in ("O2", "ArO2"):
         dens = ion if isinstance(ion, dict) else {}

@@ -7,7 +7,7 @@ tests/golden/setup_<name>.npz together with the deck text and seed.  Needs
 the reference tree, so it runs only where that exists; the .npz files are
 committed and the tests read only them.
 
-usage: python tests/golden/make_golden.py
+usage: python tests/golden/make_golden.py [deck names]
 """
 import json
 import os
@@ -35,6 +35,11 @@ DECKS = {
                             ion_density={"Ar+": 1e15, "O2+": 2e14, "O+": 0.0, "O-": 2e14}), 515),
     "o2_33x17": (ccp_deck(33, 17, 0.01, 0.005, gas="O2", ppc=12, pressure_torr=0.1, voltage=200.0, te_ev=3.0,
                           ion_density={"O2+": 1e15, "O+": 1e14, "O-": 1e14}), 616),
+    # the reference's other load types (src/Particle.c:52-175)
+    "ar_33x17_exp": (ccp_deck(33, 17, 0.01, 0.005, ppc=20, load_type=1, load_pos=(0.005, 0.003, 0.002, 0.0025)), 31),
+    "ar_33x17_cos": (ccp_deck(33, 17, 0.01, 0.005, ppc=20, load_type=2, load_pos=(0.005, 0.006, 0.004, 0.0025)), 32),
+    "ar_33x17_npr": (ccp_deck(33, 17, 0.01, 0.005, ppc=20, load_type=3, load_pos=(0.002, 0.008, 0.001, 0.004),
+                              ratio=5), 33),
 }
 
 
@@ -67,6 +72,9 @@ def dump(name, deck, seed):
 
 
 if __name__ == "__main__":
+    only = set(sys.argv[1:])  # names to (re)generate; all when none are given
     for name, (deck, seed) in DECKS.items():
+        if only and name not in only:
+            continue
         dump(name, deck, seed)
         print("wrote", name)

@@ -34,6 +34,10 @@ CASES = {
     "aro2": (ccp_deck(33, 17, 0.01, 0.005, gas="ArO2", ppc=20, pressure_torr=0.1, voltage=200.0, te_ev=3.0,
                       ion_density={"Ar+": 1e15, "O2+": 2e14, "O+": 0.0, "O-": 2e14}), 4242),
     "block": (block_deck(), 4242),
+    # Gaussian profile and Ratio-per-cell loads: uneven counts per loading cell
+    "exp_load": (ccp_deck(33, 17, 0.01, 0.005, ppc=20, load_type=1, load_pos=(0.005, 0.003, 0.002, 0.0025)), 31),
+    "npr_load": (ccp_deck(33, 17, 0.01, 0.005, ppc=20, load_type=3, load_pos=(0.002, 0.008, 0.001, 0.004),
+                          ratio=5), 33),
 }
 
 

@@ -133,6 +133,12 @@ def test_deck_errors():
     with pytest.raises(hpic.HpicError) as e:
         hpic.Setup("{ not json")
     assert e.value.status == hpic.HP_ERR_DECK
+    # SMARTLOAD passes the reader, but the reference's loader exits on it
+    bad = json.loads(json.dumps(deck))
+    bad["GasSpecies"]["ChargeSpecies"]["Loadtype"] = 4
+    with pytest.raises(hpic.HpicError) as e:
+        hpic.Setup(bad)
+    assert e.value.status == hpic.HP_ERR_UNSUPPORTED
 
 
 def test_no_gpu_is_a_loud_error():
