@@ -141,6 +141,7 @@ void fill_info(const Setup &s, hp_case_info *out) {
     out->dt = s.dt; out->dx = s.dx; out->dy = s.dy;
     out->mcc_stride = s.main_gas == GAS_AR ? 8 : 72;
     out->n_smt = s.N_smt;
+    out->n_dielectric = s.diel_num;
 }
 
 // Collision probability per cell from its lower-left node
@@ -272,6 +273,35 @@ hp_status build_device(hp_case *c) {
     h.n_smt = s.N_smt;
     TRY(dupload(c, (int **)&h.dens_region, s.dens_region));
     if (s.N_smt > 0) TRY(dalloc(c, &h.smt, (size_t)s.nsp * G));
+    if (s.diel_num > 0) {
+        TRY(dalloc(c, &h.sig, (size_t)s.nsp * G));
+        TRY(dupload(c, (int **)&h.sig_mode, s.sig_mode));
+        TRY(dupload(c, (float **)&h.area, s.area));
+        TRY(dalloc(c, &h.sigma, (size_t)G));
+        // the crossings one step can queue: every particle a cell next to a
+        // dielectric cell can hold (the mover half of its slots), per species
+        long long adj = 0;
+        for (int i = 0; i < s.ncx; i++)
+            for (int j = 0; j < s.ncy; j++) {
+                if (s.plasma_region[(size_t)i * s.ncy + j] != 1) continue;
+                bool near = false;
+                for (int a = -1; a <= 1 && !near; a++)
+                    for (int b = -1; b <= 1 && !near; b++) {
+                        const int S = s.sidx[(size_t)(i + 1 + a) * (s.ncy + 2) + (j + 1 + b)];
+                        near = S >= 1 && S < 100;
+                    }
+                adj += near;
+            }
+        long long cap = 0;
+        for (int isp = 0; isp < s.nsp; isp++) cap += adj * ((s.cap[isp] + 1) / 2);
+        cap = std::max(cap, 4096LL);
+        if (cap > (1LL << 30)) return set_error("dielectric crossing queue above 2^30 entries"), HP_ERR_ARG;
+        h.dq_cap = (int)cap;
+        TRY(dalloc(c, &h.dq_n, 1));
+        TRY(dalloc(c, &h.dq_k, (size_t)cap));
+        TRY(dalloc(c, &h.dq_v, (size_t)cap));
+        if ((long long)C >= (1LL << 24)) return set_error("dielectric decks hold at most 2^24 cells"), HP_ERR_ARG;
+    }
     if (c->opts.move_mode != 0 && c->opts.move_mode != 1) return set_error("move_mode must be 0 or 1"), HP_ERR_ARG;
     for (int isp = 0; isp < s.nsp; isp++) {
         // a far mover's key holds its rank r < cap/2 in 18 bits
@@ -433,7 +463,7 @@ hp_status op_move(hp_case *c, cudaStream_t st) {
     return e == cudaSuccess ? HP_OK : cuda_fail(e, "move");
 }
 hp_status op_sort(hp_case *c, cudaStream_t st) {
-    cudaError_t e = launch_sort(c->d_case, c->d_items, 1, c->s.nsp * c->s.Csize, c->lc, st);
+    cudaError_t e = launch_sort(c->d_case, c->d_items, 1, c->s.nsp * c->s.Csize, c->lc, st, c->s.diel_num > 0);
     return e == cudaSuccess ? HP_OK : cuda_fail(e, "sort");
 }
 hp_status op_mcc(hp_case *c, cudaStream_t st) {
@@ -617,6 +647,7 @@ static hp_status table_of(const Setup &s, const std::vector<float> *prob, const 
     case 36: if (fs) { src = fs->W.data(); nb = fs->W.size() * 4; } break;
     case 37: if (fs) { src = fs->Wt.data(); nb = fs->Wt.size() * 4; } break;
     case 38: if (fs) { src = fs->inv_eig.data(); nb = fs->inv_eig.size() * 4; } break;
+    case 39: src = s.sig_mode.data(); nb = s.sig_mode.size() * 4; break;
     default: set_error("unknown table id"); return HP_ERR_ARG;
     }
     if (needed) *needed = nb;
@@ -952,6 +983,8 @@ static hp_status grid_ptr(hp_case *c, hp_grid_field f, void **p, size_t *nb) {
     case HP_GRID_COND_CHARGE: *p = c->h.cond_charge; *nb = (size_t)nsp * c->s.cond_numr * 4; break;
     case HP_GRID_MCC_COUNT: *p = c->h.mcc_count; *nb = (size_t)c->h.mcc_stride * c->s.Csize * 4; break;
     case HP_GRID_EEDF: *p = c->h.eedf; *nb = (size_t)(HP_EEDF_BINS + 1) * 8; break;
+    case HP_GRID_SURFACE_CHARGE: *p = c->h.sig; *nb = c->h.sig ? (size_t)nsp * G * 8 : 0; break;
+    case HP_GRID_SIGMA: *p = c->h.sigma; *nb = c->h.sigma ? (size_t)G * 8 : 0; break;
     default: return set_error("unknown grid field"), HP_ERR_ARG;
     }
     return HP_OK;
@@ -968,7 +1001,7 @@ hp_status hp_get_grid(hp_case *c, hp_grid_field f, void *out, size_t bytes) {
     if (bytes < nb) return set_error("output buffer too small (" + std::to_string(nb) + " needed)"), HP_ERR_ARG;
     CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(c->last_stream));
-    CK(cudaMemcpy(out, p, nb, cudaMemcpyDeviceToHost));
+    if (nb) CK(cudaMemcpy(out, p, nb, cudaMemcpyDeviceToHost));
     return HP_OK;
 }
 
@@ -980,7 +1013,7 @@ hp_status hp_set_grid(hp_case *c, hp_grid_field f, const void *in, size_t bytes)
     if (bytes != nb) return set_error("input size mismatch (" + std::to_string(nb) + " expected)"), HP_ERR_ARG;
     CK(cudaSetDevice(c->device));
     CK(cudaStreamSynchronize(c->last_stream));
-    CK(cudaMemcpy(p, in, nb, cudaMemcpyHostToDevice));
+    if (nb) CK(cudaMemcpy(p, in, nb, cudaMemcpyHostToDevice));
     return HP_OK;
 }
 

@@ -71,6 +71,7 @@ struct BatchDev {
     int max_g = 0;
     bool any_eedf = false;
     int max_smt = 0; // most density smoothing passes of any case
+    bool surface = false; // some case has dielectric blocks
     // PCG groups for every cluster cap 1,2,4,8,16: lists of case indices per
     // cluster size, concatenated in d_lists
     int *d_lists = nullptr;

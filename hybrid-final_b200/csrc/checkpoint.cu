@@ -8,11 +8,11 @@
 // densities, background gas, potentials, fields and their time averages.
 // Quantities this library does not model are written as the reference's
 // neutral values: no continuity solve (Conti_Flag 0, fluid densities the
-// deck's constants, sources and fluxes 0), no history records, no
-// dielectric charge (sigma 0), MCC rates 0 (the exact per-cell tallies are
-// in the extension).
+// deck's constants, sources and fluxes 0), no history records, MCC rates 0
+// (the exact per-cell tallies are in the extension).  The dielectric surface
+// charge goes out as the reference's float sigma per (species, node).
 //
-// An extension block follows ("HPICX001"): everything a resumed run needs to
+// An extension block follows ("HPICX002"): everything a resumed run needs to
 // continue bit for bit -- the step counter that keys the Philox streams, the
 // case seed, the particles as in-cell offsets in the device's cell order,
 // the field solver's warm start, the charge grid and right-hand side, the
@@ -61,19 +61,20 @@ struct File {
     }
 };
 
-const char MAGIC[8] = {'H', 'P', 'I', 'C', 'X', '0', '0', '1'};
+const char MAGIC[8] = {'H', 'P', 'I', 'C', 'X', '0', '0', '2'};
 const char TAIL[8] = {'H', 'P', 'I', 'C', 'E', 'N', 'D', '1'};
 // grid fields carried by the extension, in file order
 const hp_grid_field EXT_GRIDS[] = {HP_GRID_EX,         HP_GRID_EY,          HP_GRID_PHI,     HP_GRID_PHI_POIS,
                                    HP_GRID_DEN,        HP_GRID_SOURCE,      HP_GRID_PCG_X,   HP_GRID_PCG_B,
                                    HP_GRID_AVE_DEN,    HP_GRID_AVE_PHI,     HP_GRID_AVE_SOURCE, HP_GRID_AVE_EX,
-                                   HP_GRID_AVE_EY,     HP_GRID_COND_CHARGE, HP_GRID_MCC_COUNT, HP_GRID_EEDF};
+                                   HP_GRID_AVE_EY,     HP_GRID_COND_CHARGE, HP_GRID_MCC_COUNT, HP_GRID_EEDF,
+                                   HP_GRID_SURFACE_CHARGE, HP_GRID_SIGMA};
 
 template <class T> std::vector<T> fetch(hp_case *c, hp_grid_field f) {
     void *p = nullptr;
     size_t nb = 0;
     std::vector<T> v;
-    if (hpi_grid_ptr(c, f, &p, &nb) != HP_OK) return v;
+    if (hpi_grid_ptr(c, f, &p, &nb) != HP_OK || nb == 0) return v;
     v.resize(nb / sizeof(T));
     if (cudaMemcpy(v.data(), p, nb, cudaMemcpyDeviceToHost) != cudaSuccess) v.clear();
     return v;
@@ -100,7 +101,7 @@ hp_status write_v000(hp_case *c, File &F, int64_t tstep, int64_t ave_count, cons
                      const std::vector<float> &phi, const std::vector<float> &phi_p, const std::vector<float> &ex,
                      const std::vector<float> &ey, const std::vector<double> &ave_phi,
                      const std::vector<double> &ave_src, const std::vector<double> &ave_ex,
-                     const std::vector<double> &ave_ey) {
+                     const std::vector<double> &ave_ey, const std::vector<long long> &sig) {
     const Setup &s = c->s;
     const int G = s.Gsize, ngy = s.ngy, ncy = s.ncy;
     F.put1<double>((double)tstep * (double)s.dt); // t
@@ -160,7 +161,7 @@ hp_status write_v000(hp_case *c, File &F, int64_t tstep, int64_t ave_count, cons
         for (size_t k = 0; k < (size_t)s.nsp * G; k++) {
             rec[3 * k] = (float)den[k];
             rec[3 * k + 1] = ave_count > 0 ? (float)(ave_den[k] / (double)ave_count) : 0.f;
-            rec[3 * k + 2] = 0.f;
+            rec[3 * k + 2] = sig.empty() ? 0.f : (float)((double)sig[k] / (double)(1ll << HP_SIGMA_FRAC_BITS));
         }
         F.put(rec.data(), rec.size() * 4);
     }
@@ -239,13 +240,14 @@ hp_status hp_case_save(hp_case *c, const char *path) {
     const auto ex = fetch<float>(c, HP_GRID_EX), ey = fetch<float>(c, HP_GRID_EY);
     const auto ave_phi = fetch<double>(c, HP_GRID_AVE_PHI), ave_src = fetch<double>(c, HP_GRID_AVE_SOURCE);
     const auto ave_ex = fetch<double>(c, HP_GRID_AVE_EX), ave_ey = fetch<double>(c, HP_GRID_AVE_EY);
+    const auto sig = fetch<long long>(c, HP_GRID_SURFACE_CHARGE);
     if (phi.size() != (size_t)s.Gsize || ave_ey.size() != (size_t)s.Gsize)
         return hpi::cuda_fail(cudaGetLastError(), "checkpoint grid read-back");
     File F;
     F.f = fopen(path, "wb");
     if (!F.f) return hpi::set_error(std::string("cannot open ") + path), HP_ERR_ARG;
     hp_status st = write_v000(c, F, tstep, ave_count, ps, den, ave_den, phi, phi_p, ex, ey, ave_phi, ave_src,
-                              ave_ex, ave_ey);
+                              ave_ex, ave_ey, sig);
     if (st != HP_OK) return st;
     // extension
     F.put(MAGIC, 8);
@@ -271,7 +273,7 @@ hp_status hp_case_save(hp_case *c, const char *path) {
         size_t nb = 0;
         if ((st = hpi_grid_ptr(c, g, &p, &nb)) != HP_OK) return st;
         std::vector<char> b(nb);
-        if (cudaMemcpy(b.data(), p, nb, cudaMemcpyDeviceToHost) != cudaSuccess)
+        if (nb && cudaMemcpy(b.data(), p, nb, cudaMemcpyDeviceToHost) != cudaSuccess)
             return hpi::cuda_fail(cudaGetLastError(), "checkpoint grid");
         F.put1<int32_t>((int32_t)g);
         F.put1<uint64_t>((uint64_t)nb);
@@ -359,7 +361,7 @@ hp_status hp_case_load(hp_case *c, const char *path) {
         void *p = nullptr;
         size_t nb = 0;
         hpi_grid_ptr(c, g, &p, &nb);
-        if (cudaMemcpy(p, grids[k].data(), nb, cudaMemcpyHostToDevice) != cudaSuccess)
+        if (nb && cudaMemcpy(p, grids[k].data(), nb, cudaMemcpyHostToDevice) != cudaSuccess)
             return hpi::cuda_fail(cudaGetLastError(), "checkpoint grid restore");
         k++;
     }

@@ -52,6 +52,17 @@ struct DevCase {
     int n_smt;                      // 1-2-1 smoothing passes per Deposit (DensitySmoothing)
     const int *dens_region;         // [G] nodes the smoothing treats as inside
     double *smt;                    // [nsp*G] smoothing scratch (n_smt > 0)
+    // dielectric surface charge (null without dielectric blocks): per
+    // (species, node) particle weight in fixed point, HP_SIGMA_FRAC_BITS
+    // fraction bits, added by Move's surface split and summed by SumSource
+    long long *sig;                 // [nsp*G]
+    const int *sig_mode;            // [G] SumSource class (0 none, 1 dielectric, 2 on a domain edge, 3 conductor)
+    const float *area;              // [G] node Area
+    double *sigma;                  // [G] Sigma: surface charge density where SumSource sets it
+    int *dq_n;                      // dielectric crossings queued by Move for the Sort phase
+    int dq_cap;
+    int *dq_k;                      // [dq_cap] (cell << 7) | (species << 4) | direction
+    float4 *dq_v;                   // [dq_cap] offset after the wrap and velocity (x, y, vx, vy)
     DevSpecies sp[DMAXSP];
     // field
     float *Ex, *Ey, *phi, *phi_p;   // [G]

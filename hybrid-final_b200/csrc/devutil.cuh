@@ -13,7 +13,7 @@ namespace hp {
 namespace dv {
 
 constexpr unsigned FULL = 0xffffffffu;
-constexpr uint32_t ST_OVERFLOW = 0x1u, ST_NONFINITE = 0x2u, ST_NOCONV = 0x4u, ST_WALK = 0x10u;
+constexpr uint32_t ST_OVERFLOW = 0x1u, ST_NONFINITE = 0x2u, ST_NOCONV = 0x4u, ST_WALK = 0x10u, ST_SURFACE = 0x20u;
 
 __device__ __forceinline__ int find_case(const int *start, int n, int w) {
     int lo = 0, hi = n;

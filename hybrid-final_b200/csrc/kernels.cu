@@ -30,7 +30,7 @@ using namespace dv;
 struct MoverFate {
     int fi, fj;
     bool absorbed, flipx, flipy;
-    int cond; // conductor index or -1
+    int cond; // conductor index, -2 - (di+1)*3 - (dj+1) on a dielectric, else -1
 };
 
 // The geometry a crossing needs, held in registers by the caller: the
@@ -64,10 +64,106 @@ __device__ __forceinline__ MoverFate mover_fate(const Geo d, int si, int sj, int
     default:
         f.absorbed = true;
         if (S >= 100) f.cond = S - 101;
+        else if (S >= 1) f.cond = -2 - ((di + 1) * 3 + (dj + 1));
         break;
     }
     if (!f.absorbed && (f.fi < 0 || f.fi >= d.ncx || f.fj < 0 || f.fj >= d.ncy)) f.absorbed = true;
     return f;
+}
+
+// One share of a particle's weight on a dielectric surface node, in fixed
+// point.  A share that is not finite or not below 2^20 in magnitude (a
+// crossing with a vanishing velocity component) is dropped, as is a node
+// outside the grid (the reference's index would reach another species' or
+// no array there).
+__device__ __forceinline__ void surface_add(long long *sig, int G, int s, int node, float w) {
+    if (node < 0 || node >= G || !(fabsf(w) < 1048576.0f)) return;
+    const long long q = __float2ll_rn(w * (float)(1 << HP_SIGMA_FRAC_BITS));
+    atomicAdd((unsigned long long *)&sig[(size_t)s * G + node], (unsigned long long)q);
+}
+
+// A particle that entered a dielectric cell: Move queues the crossing and
+// the Sort phase applies it (surface_split), as the reference's Move leaves
+// the mover for SortBoundary.  The queue keeps Move's register budget: two
+// stores on this rare path instead of the split's arithmetic.
+__device__ __noinline__ void surface_enqueue(const DevCase &d, int s, int i, int j, int dir, float x, float y,
+                                             float vx, float vy) {
+    const int q = atomicAdd(d.dq_n, 1);
+    if (q >= d.dq_cap) {
+        atomicOr(d.status, ST_SURFACE);
+        return;
+    }
+    d.dq_k[q] = ((i * d.ncy + j) << 7) | (s << 4) | dir;
+    d.dq_v[q] = make_float4(x, y, vx, vy);
+}
+
+// SortBoundary's dielectric branch (src/cuda_Sortboundary.cu:93-207): a
+// particle that entered a dielectric cell from cell (i, j) in direction dir
+// = (di+1)*3 + (dj+1) leaves its weight on the two nodes of the face it
+// crossed, split linearly by where it crossed.  (x, y) is its offset after
+// the wrap, in the frame of the cell entered; for a diagonal crossing the
+// cell passed first decides the face when it is not plasma.  The node
+// arithmetic is the reference's, on the flat node index, including its
+// choice of node for the lower-left diagonal (CID where the face's node is
+// CID+1).
+__device__ __forceinline__ void surface_split(const DevCase &d, int s, int i, int j, int dir, float x, float y, float vx,
+                                           float vy) {
+    const int ngy = d.ngy, SY = d.ncy + 2;
+    const int di = dir / 3 - 1, dj = dir % 3 - 1;
+    const int T = i * ngy + j, C = T + di * ngy + dj;
+    const int g = (i + 1 + di) * SY + (j + 1 + dj);
+    const int *SI = d.sidx;
+    int pa = 0, pb = 0;
+    float a = 0.0f, b = 0.0f, delta;
+    switch (dir) {
+    case 5: delta = x - vx / vy * y; pa = C; a = 1 - delta; pb = C + ngy; b = delta; break;
+    case 3: delta = x + vx / vy * (1 - y); pa = T; a = 1 - delta; pb = T + ngy; b = delta; break;
+    case 7: delta = y - vy / vx * x; pa = C; a = 1 - delta; pb = C + 1; b = delta; break;
+    case 1: delta = y + vy / vx * (1 - x); pa = T; a = 1 - delta; pb = T + 1; b = delta; break;
+    case 8:
+        delta = x - vx / vy * y;
+        if (delta >= 0) {
+            if (SI[g - 1]) { delta = y - vy / vx * x; pa = C - 1; a = -delta; pb = C; b = 1 + delta; }
+            else { pa = C; a = 1 - delta; pb = C + ngy; b = delta; }
+        } else {
+            if (SI[g - SY]) { pa = T + 1; a = -delta; pb = C; b = 1 + delta; }
+            else { delta = y - vy / vx * x; pa = C; a = 1 - delta; pb = C + 1; b = delta; }
+        }
+        break;
+    case 6:
+        delta = x + vx / vy * (1 - y);
+        if (delta >= 0) {
+            if (SI[g + 1]) { delta = y - vy / vx * x; pa = C + 1; a = 2 - delta; pb = C + 2; b = delta - 1; }
+            else { pa = C + 1; a = 1 - delta; pb = C + 1 + ngy; b = delta; }
+        } else {
+            if (SI[g - SY]) { pa = T; a = -delta; pb = C + 1; b = 1 + delta; }
+            else { delta = y - vy / vx * x; pa = C; a = 1 - delta; pb = C + 1; b = delta; }
+        }
+        break;
+    case 2:
+        delta = x - vx / vy * y;
+        if (delta < 1) {
+            if (SI[g - 1]) { delta = y + vy / vx * (1 - x); pa = C + ngy - 1; a = -delta; pb = C + ngy; b = 1 + delta; }
+            else { pa = C; a = 1 - delta; pb = C + ngy; b = delta; }
+        } else {
+            if (SI[g + SY]) { pa = T + 1; a = 2 - delta; pb = T + 1 + ngy; b = delta - 1; }
+            else { delta = y + vy / vx * (1 - x); pa = T + 1; a = 1 - delta; pb = T + 2; b = delta; }
+        }
+        break;
+    case 0:
+        delta = x + vx / vy * (1 - y);
+        if (delta < 1) {
+            if (SI[g + 1]) { delta = y + vy / vx * (1 - x); pa = T; a = 2 - delta; pb = T + 1; b = delta - 1; }
+            else { pa = C; a = 1 - delta; pb = T; b = delta; }
+        } else {
+            if (SI[g + SY]) { pa = T; a = 2 - delta; pb = T + ngy; b = delta - 1; }
+            else { delta = y + vy / vx * (1 - x); pa = T - 1; a = 1 - delta; pb = T; b = delta; }
+        }
+        break;
+    default: return;
+    }
+    surface_add(d.sig, d.G, s, pa, a);
+    surface_add(d.sig, d.G, s, pb, b);
 }
 
 constexpr int CODE_FAR = 14, CODE_ABSORBED = 15;
@@ -266,6 +362,7 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
             if (r) {
                 code = CODE_ABSORBED;
                 if (cond >= 0 && cond < d.cond_numr) atomicAdd(&d.cond_charge[s * d.cond_numr + cond], 1.0f);
+                else if (cond <= -2 && d.sig) surface_enqueue(d, s, fi, fj, -2 - cond, lx, ly, mvX, mvY);
                 if (r == 2) atomicOr(d.status, ST_WALK);
             } else {
                 const int ddi = fi - i, ddj = fj - j;
@@ -402,6 +499,7 @@ __global__ void __launch_bounds__(512) k_move_u(const DevCase *__restrict__ case
                 if (r) {
                     code = CODE_ABSORBED;
                     if (cond >= 0 && cond < d.cond_numr) atomicAdd(&d.cond_charge[s * d.cond_numr + cond], 1.0f);
+                    else if (cond <= -2 && d.sig) surface_enqueue(d, s, fi, fj, -2 - cond, X, Y, vX, vY);
                     if (r == 2) atomicOr(d.status, ST_WALK);
                 } else {
                     const int ddi = fi - i, ddj = fj - j;
@@ -1109,6 +1207,42 @@ __global__ void __launch_bounds__(512) k_deposit_cells(const DevCase *__restrict
     }
 }
 
+// The Sort phase's pass over the dielectric crossings Move queued: one block
+// per case, then the queue is emptied for the next step.  The fixed-point
+// sums make the result independent of the order of the entries.
+__global__ void __launch_bounds__(256) k_surface(const DevCase *__restrict__ cases, int ncases) {
+    const DevCase &d = cases[blockIdx.x];
+    if (!d.sig) return;
+    const int n = min(*d.dq_n, d.dq_cap);
+    for (int q = threadIdx.x; q < n; q += blockDim.x) {
+        const int k = d.dq_k[q];
+        const float4 v = d.dq_v[q];
+        const int cell = k >> 7, i = cell / d.ncy, j = cell - i * d.ncy;
+        surface_split(d, (k >> 4) & 7, i, j, k & 15, v.x, v.y, v.z, v.w);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *d.dq_n = 0;
+    (void)ncases;
+}
+
+// SumSource's surface-charge term (src/cuda_Deposit.cu:40-97): at a node of
+// dielectric class the species' surface weights times q*np2c, which also
+// sets Sigma (that charge over the node Area, doubled on a domain edge); a
+// node of conductor class clears its surface weights.
+__device__ __forceinline__ double surface_charge(const DevCase &d, int n) {
+    const int m = d.sig_mode[n];
+    if (m == 0) return 0.0;
+    if (m == 3) {
+        for (int s = 0; s < d.nsp; s++) d.sig[(size_t)s * d.G + n] = 0;
+        return 0.0;
+    }
+    double q = 0.0;
+    for (int s = 0; s < d.nsp; s++)
+        q += (double)d.sig[(size_t)s * d.G + n] * (1.0 / (double)(1ll << HP_SIGMA_FRAC_BITS)) * (double)d.sp[s].q_density;
+    d.sigma[n] = (m == 2 ? 2.0 : 1.0) * q / (double)d.area[n];
+    return q;
+}
+
 // DepositBoundary + SumSource + PCG_Set (src/cuda_Deposit.cu:277-288,35-104,30-34)
 __global__ void __launch_bounds__(256) k_deposit_nodes(const DevCase *__restrict__ cases,
                                                        const int *__restrict__ item_start, int ncases, int items) {
@@ -1131,6 +1265,7 @@ __global__ void __launch_bounds__(256) k_deposit_nodes(const DevCase *__restrict
         d.den[(size_t)s * d.G + n] = den;
         sum += den * (double)d.sp[s].q_density;
     }
+    if (d.sig) sum += surface_charge(d, n);
     const double source = sum / 8.8542e-12;
     d.source[n] = source;
     d.b64[n] = d.st[2 * d.G + n] != 0.0f ? source : 0.0;
@@ -1185,6 +1320,7 @@ __global__ void __launch_bounds__(256) k_source(const DevCase *__restrict__ case
     const int n = t - item_start[ci];
     double sum = 0.0;
     for (int s = 0; s < d.nsp; s++) sum += d.den[(size_t)s * d.G + n] * (double)d.sp[s].q_density;
+    if (d.sig) sum += surface_charge(d, n);
     const double source = sum / 8.8542e-12;
     d.source[n] = source;
     d.b64[n] = d.st[2 * d.G + n] != 0.0f ? source : 0.0;
@@ -1457,6 +1593,9 @@ __global__ void __launch_bounds__(256) k_potential(const DevCase *__restrict__ c
 __device__ float cond_sigma(const DevCase &d, int n, int x, int y, int eT, int eL, int eD, int eX, int pL, int pR,
                             int pD, int pU) {
     const int b = d.boundary[n], f = d.face[n];
+    // a Neumann node keeps the Sigma that SumSource left there (0 unless its
+    // inward neighbour is dielectric)
+    if (b == 2) return d.sigma ? (float)d.sigma[n] : 0.0f;
     if (!((b == 3 || b == 1) && f != 8)) return 0.0f;
     float SumSig = 0.0f;
     for (int s = 0; s < d.nsp; s++) SumSig += (float)d.den[(size_t)s * d.G + n] * d.sp[s].q_density;
@@ -1701,8 +1840,13 @@ cudaError_t launch_move(const DevCase *cases, const int *item_start, int ncases,
 }
 
 cudaError_t launch_sort(const DevCase *cases, const int *item_start, int ncases, int items, const LaunchCfg &lc,
-                        cudaStream_t st) {
+                        cudaStream_t st, bool surface) {
     if (items <= 0) return cudaSuccess;
+    if (surface) {
+        k_surface<<<ncases, 256, 0, st>>>(cases, ncases);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
     // at least 8 warps per block: the push gains from them even where Move
     // and Deposit prefer smaller blocks
     const int tpb = 32 * std::min(std::max(lc.warps_per_block, 8), SORT_MAXW);

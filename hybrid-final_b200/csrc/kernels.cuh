@@ -21,8 +21,9 @@ struct LaunchCfg {
 cudaError_t launch_move(const DevCase *cases, const int *item_start, int ncases, int items, const LaunchCfg &lc,
                         cudaStream_t st);
 // SortBoundary: boundary handling + deterministic re-bin (src/cuda_Sortboundary.cu:41-258)
+// surface: some case has dielectric blocks (apply the crossings Move queued)
 cudaError_t launch_sort(const DevCase *cases, const int *item_start, int ncases, int items, const LaunchCfg &lc,
-                        cudaStream_t st);
+                        cudaStream_t st, bool surface);
 // MCC, Ar set (src/cuda_mcc.cu:97-106, src/cuda_mccAr.cu:41-232)
 // MCC of the Ar/O2 (gas 2) reaction set, one warp per cell (mcc_oxy.cu)
 cudaError_t launch_mcc_oxy(const DevCase *cases, const int *item_start, int ncases, int items, int gas,

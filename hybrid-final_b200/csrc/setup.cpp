@@ -233,8 +233,31 @@ void read_geometry(const JVal &root, Setup &s, std::vector<int> &bx0, std::vecto
         s.src_rphase.push_back((float)(MPI / 180 * ph));
         if (fr != 0) s.max_freq = std::max(s.max_freq, fr);
     }
+    // dielectric blocks (src/start.c:226-300): M_ID > 0, non-decreasing, none
+    // shared with a conductor; node extents inside the grid; Epsilon = eps_r
     const auto &diel = geo.array("DielectricSpec");
-    if (!diel.empty()) unsupported("dielectric blocks (DielectricSpec) are outside this library's step path");
+    s.diel_num = (int)diel.size();
+    int last_id = 0;
+    for (size_t i = 0; i < diel.size(); i++) {
+        const JVal &c = diel[i];
+        const std::string line = "DielectricSpec line " + std::to_string(i + 1);
+        int id = inum(c, "M_ID");
+        if (id == 0) deck_fail("\"M_ID\" > 0");
+        if (i > 0 && last_id > id) deck_fail("\"M_ID\" must be written in order.");
+        last_id = id;
+        if (std::find(s.cond_mid.begin(), s.cond_mid.end(), id) != s.cond_mid.end())
+            deck_fail(line + ": M_ID is duplicated with a conductor");
+        // StructureIndex holds a dielectric as its M_ID in 1..99 (src/start.c:1778)
+        if (id < 0 || id > 99) deck_fail(line + ": M_ID must be in 1..99");
+        int x0 = inum(c, "X0"), x1 = inum(c, "X1"), y0 = inum(c, "Y0"), y1 = inum(c, "Y1");
+        if (x0 > x1) deck_fail(line + ": X0 > X1");
+        if (x1 >= s.ngx) deck_fail(line + ": X1 >= NumGridx");
+        if (y0 > y1) deck_fail(line + ": Y0 > Y1");
+        if (y1 >= s.ngy) deck_fail(line + ": Y1 >= NumGridy");
+        s.diel_mid.push_back(id);
+        s.diel_x0.push_back(x0); s.diel_x1.push_back(x1); s.diel_y0.push_back(y0); s.diel_y1.push_back(y1);
+        s.diel_eps.push_back(fnum(c, "Epsilon"));
+    }
 }
 
 void read_species_block(const JVal &cs, const char *key, SpeciesP &p, float mass, float q) {
@@ -519,6 +542,18 @@ void geometry(Setup &s, const std::vector<int> &bx0, const std::vector<int> &bx1
                 }
             }
         }
+    // dielectrics (src/start.c:1507-1520)
+    for (int k = 0; k < s.diel_num; k++)
+        for (int i = s.diel_x0[k]; i <= s.diel_x1[k]; i++)
+            for (int j = s.diel_y0[k]; j <= s.diel_y1[k]; j++) {
+                int ID = i * ngy + j;
+                if (s.boundary[ID] == 0) s.boundary[ID] = BC_DIELECTRIC;
+                if (i < s.diel_x1[k] && j < s.diel_y1[k]) {
+                    int CID = i * ncy + j;
+                    s.plasma_region[CID] = 0;
+                    s.eps_r[CID] = s.diel_eps[k];
+                }
+            }
     // conductors (src/start.c:1521-1537)
     for (int k = 0; k < s.cond_num; k++)
         for (int i = s.cond_x0[k]; i <= s.cond_x1[k]; i++)
@@ -547,7 +582,9 @@ void geometry(Setup &s, const std::vector<int> &bx0, const std::vector<int> &bx1
             int ID = i * ngy + j, CID = i * ncy + j;
             int P1 = (int)s.eps_r[CID], P2 = (int)s.eps_r[CID - ncy], P3 = (int)s.eps_r[CID - 1],
                 P4 = (int)s.eps_r[CID - ncy - 1];
-            if (s.boundary[ID] != BC_CONDUCTOR) continue; // dielectric decks are rejected above
+            // dielectric and conductor nodes share the rule and the areas
+            // (Face_To_Area, src/start.c:2053-2083)
+            if (s.boundary[ID] != BC_CONDUCTOR && s.boundary[ID] != BC_DIELECTRIC) continue;
             int f = -1;
             if ((P2 == 1 && P1 == 1 && P4 == 1) || (P2 != 0 && P1 != 0 && P4 != 0 && P3 == 0)) f = F_UL;
             else if ((P2 == 1 && P1 == 1 && P3 == 1) || (P2 != 0 && P1 != 0 && P3 != 0 && P4 == 0)) f = F_UR;
@@ -648,6 +685,9 @@ void geometry(Setup &s, const std::vector<int> &bx0, const std::vector<int> &bx1
     for (int i = 0; i < ncx; i++)
         for (int j = 0; j < ncy; j++) {
             si(i + 1, j + 1) = 0;
+            for (int k = 0; k < s.diel_num; k++)
+                if (i >= s.diel_x0[k] && i < s.diel_x1[k] && j >= s.diel_y0[k] && j < s.diel_y1[k])
+                    si(i + 1, j + 1) = s.diel_mid[k];
             for (int k = 0; k < s.cond_num; k++)
                 if (i >= s.cond_x0[k] && i < s.cond_x1[k] && j >= s.cond_y0[k] && j < s.cond_y1[k])
                     si(i + 1, j + 1) = 100 + s.cond_mid[k];
@@ -688,6 +728,23 @@ void geometry(Setup &s, const std::vector<int> &bx0, const std::vector<int> &bx1
         else if (s.boundary[ID] == BC_DIRICHLET && fc != F_NONE && s.cond_id[ID] != 0) f *= 2;
         s.dep_factor[ID] = f;
     }
+    // SumSource's node classes (src/cuda_Deposit.cu:35-104): on the domain
+    // edges the node looks at its inward neighbour (x edges first), inside at
+    // itself; a dielectric there adds its surface charge (Sigma = factor x
+    // charge / Area), a conductor clears it
+    s.sig_mode.assign(G, 0);
+    if (s.diel_num > 0)
+        for (int ID = 0; ID < G; ID++) {
+            const int x = ID / ngy, y = ID % ngy;
+            int nb = ID, edge = 1;
+            if (x == 0) nb = ID + ngy;
+            else if (x == ngx - 1) nb = ID - ngy;
+            else if (y == 0) nb = ID + 1;
+            else if (y == ngy - 1) nb = ID - 1;
+            else edge = 0;
+            if (s.boundary[nb] == BC_DIELECTRIC) s.sig_mode[ID] = edge ? 2 : 1;
+            else if (s.boundary[nb] == BC_CONDUCTOR) s.sig_mode[ID] = 3;
+        }
 }
 
 // ---------------------------------------------------------------- field solver matrix

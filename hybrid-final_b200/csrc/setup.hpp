@@ -69,6 +69,9 @@ struct Setup {
     std::vector<int> src_mid;
     std::vector<float> src_dc, src_ac, src_freq, src_2pifreq, src_rphase;
     std::vector<int> efield_flag; // per conductor (src/Efield.c:34-60)
+    int diel_num = 0;             // DielectricSpec blocks
+    std::vector<int> diel_mid, diel_x0, diel_x1, diel_y0, diel_y1;
+    std::vector<float> diel_eps;
     float max_freq = 0;
 
     // --- geometry (src/start.c:1432-1642) ---
@@ -78,6 +81,7 @@ struct Setup {
     std::vector<float> eps_r;                              // [Csize]
     std::vector<int> sidx;                                 // [(ncx+2)*(ncy+2)] StructureIndex
     std::vector<float> dep_factor;                         // [Gsize] DepositBoundary scale
+    std::vector<int> sig_mode; // [Gsize] SumSource class: 0 none, 1 dielectric, 2 dielectric edge (x2), 3 conductor
 
     // --- field solver (src/start.c:1911-1998, src/load.c:121-246) ---
     int n_unknowns = 0;

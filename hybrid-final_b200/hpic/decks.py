@@ -166,6 +166,22 @@ def block_deck():
     return d
 
 
+def dielectric_deck(ppc=8, voltage=200.0):
+    """A 33 x 21 CCP whose driven electrode (node row 0) is covered by a
+    dielectric slab (M_ID 3, eps_r 4, node rows 0-3 across the whole width, so
+    it meets both Neumann side walls) with a floating dielectric block inside
+    (M_ID 4, eps_r 3.9, nodes 12-18 x 9-12): exercises the dielectric faces and
+    areas, the 1..99 StructureIndex codes, the surface-charge split of
+    SortBoundary for straight and diagonal crossings, and SumSource's interior
+    and wall classes."""
+    d = ccp_deck(33, 21, 0.01, 0.00625, ppc=ppc, voltage=voltage)
+    d["Geometry"]["DielectricSpec"] = [
+        {"M_ID": 3, "X0": 0, "X1": 32, "Y0": 0, "Y1": 3, "Epsilon": 4.0},
+        {"M_ID": 4, "X0": 12, "X1": 18, "Y0": 9, "Y1": 12, "Epsilon": 3.9},
+    ]
+    return d
+
+
 def write_deck(path, deck):
     with open(path, "w") as f:
         json.dump(deck, f, indent=1)

@@ -25,6 +25,10 @@
 
 /* electron energy distribution (HP_GRID_EEDF): bins of HP_EEDF_DE eV from 0,
  * then one overflow bin */
+/* Dielectric surface charge is kept per (species, node) as particle weight in
+ * fixed point with this many fraction bits, so that its sums do not depend on
+ * the order of the additions. */
+#define HP_SIGMA_FRAC_BITS 28
 #define HP_EEDF_BINS 200
 #define HP_EEDF_DE 0.25f
 
@@ -55,6 +59,8 @@ typedef enum hp_status {
 #define HP_STATUS_WAIT_TIMEOUT 0x8u  /* a bounded device-side wait gave up */
 #define HP_STATUS_WALK_BOUND 0x10u   /* move_mode 1: a particle crossed more cells than the domain spans
                                         (non-finite velocity); it was absorbed */
+#define HP_STATUS_SURFACE_OVERFLOW 0x20u /* more dielectric crossings in one step than the case's queue holds;
+                                            the excess left no surface charge */
 
 /* Text of the last error raised on the calling host thread. */
 const char *hp_last_error(void);
@@ -134,6 +140,7 @@ typedef struct hp_case_info {
     int field_mode;        /* solver in use: 2 falls back to 1 when the operator is not separable */
     int mcc_stride;        /* collision counters per cell in HP_GRID_MCC_COUNT (8 Ar, 72 O2 and Ar/O2) */
     int n_smt;             /* 1-2-1 density smoothing passes per Deposit (the deck's DensitySmoothing) */
+    int n_dielectric;      /* DielectricSpec blocks (surface charge kept when > 0) */
 } hp_case_info;
 hp_status hp_case_get_info(const hp_case *c, hp_case_info *out);
 hp_status hp_setup_get_info(const hp_setup *s, hp_case_info *out);
@@ -225,7 +232,12 @@ typedef enum hp_grid_field {
     HP_GRID_AVE_SOURCE = 13,  /* double[Gsize] running sum of the charge source rho/eps0 (the reference's
                                  ave_Source, src/cuda_SaveDump.cu:91-92) */
     HP_GRID_AVE_EX = 14,      /* double[Gsize] running sums of Ex and Ey (ave_Ex, ave_Ey) */
-    HP_GRID_AVE_EY = 15
+    HP_GRID_AVE_EY = 15,
+    HP_GRID_SURFACE_CHARGE = 16, /* int64[nsp*Gsize] dielectric surface charge per species and node, in
+                                    particle weights with HP_SIGMA_FRAC_BITS fraction bits (the reference's
+                                    GPG.sigma); 0 bytes in a case without dielectric blocks */
+    HP_GRID_SIGMA = 17        /* double[Gsize] Sigma, the surface charge density SumSource sets at
+                                 dielectric nodes (src/cuda_Deposit.cu:35-104); 0 bytes without dielectrics */
 } hp_grid_field;
 hp_status hp_get_grid(hp_case *c, hp_grid_field f, void *out, size_t bytes);
 hp_status hp_set_grid(hp_case *c, hp_grid_field f, const void *in, size_t bytes);
@@ -266,7 +278,9 @@ hp_status hp_case_slot_changes(hp_case *c, int64_t *changes);
  * 9 stencil float[5*N] (W,S,C,N,E per unknown, 0 where absent), 10 vsave float[nvel],
  * 11 cross-section table float[N_LOGX*(2+nch)], 12 CollF float[4*TnRct],
  * 13 sigma-v max float[n], 14 node DensRegion int[Gsize], 15 MCC probabilities float[3*Gsize],
- * 16 cell eps_r float[Csize], 17 BackDen2 float[Gsize], 18 BackVel2 float[Gsize]. */
+ * 16 cell eps_r float[Csize], 17 BackDen2 float[Gsize], 18 BackVel2 float[Gsize],
+ * 39 SumSource node class int[Gsize] (0 none, 1 dielectric, 2 dielectric on a
+ * domain edge: Sigma doubled, 3 conductor: surface charge cleared). */
 hp_status hp_get_table(hp_case *c, int what, void *out, size_t bytes, size_t *bytes_needed);
 hp_status hp_setup_get_table(const hp_setup *s, int what, void *out, size_t bytes, size_t *bytes_needed);
 

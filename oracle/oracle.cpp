@@ -22,6 +22,7 @@
 
 #include "hp_math.h"
 #include "hp_rng.h"
+#include "hpic.h"
 
 namespace {
 
@@ -88,6 +89,8 @@ struct SimBase {
     std::vector<unsigned> mcc_count;
     int pcg_iters[2] = {0, 0};
     std::vector<double> ave_den, ave_phi, ave_src, ave_ex, ave_ey;
+    std::vector<long long> sig; // [nsp*G] dielectric surface weights, fixed point
+    std::vector<double> sigma;  // [G] Sigma where SumSource sets it
     int64_t ave_count = 0;
     bool walk_bound_hit = false; // a walk that reached its crossing bound
     std::vector<unsigned long long> eedf = std::vector<unsigned long long>(201, 0ull);
@@ -149,6 +152,8 @@ template <class R> struct Sim : SimBase {
         ave_src.assign(G, 0.0);
         ave_ex.assign(G, 0.0);
         ave_ey.assign(G, 0.0);
+        sig.assign((size_t)c.nsp * G, 0);
+        sigma.assign(G, 0.0);
     }
 
     // ------------------------------------------------------------ state
@@ -205,6 +210,8 @@ template <class R> struct Sim : SimBase {
             if (precision == 32 && c.field_mode == 0) for (int n = 0; n < G; n++) d[n] = pf_x[n];
             else std::memcpy(d, x64.data(), x64.size() * 8);
             break;
+        case 8: std::memcpy(out, sig.data(), sig.size() * 8); break;
+        case 9: std::memcpy(d, sigma.data(), sigma.size() * 8); break;
         }
     }
     void set_grid(int which, const void *in) override {
@@ -222,6 +229,8 @@ template <class R> struct Sim : SimBase {
             if (precision == 32 && c.field_mode == 0) for (int n = 0; n < G; n++) pf_x[n] = (float)d[n];
             else std::memcpy(x64.data(), d, x64.size() * 8);
             break;
+        case 8: std::memcpy(sig.data(), in, sig.size() * 8); break;
+        case 9: std::memcpy(sigma.data(), d, sigma.size() * 8); break;
         }
     }
 
@@ -244,10 +253,103 @@ template <class R> struct Sim : SimBase {
         default:
             f.absorbed = true;
             if (S >= 100) f.cond = S - 101;
+            else if (S >= 1) f.cond = -2 - ((di + 1) * 3 + (dj + 1)); // a dielectric: the direction entered
             break;
         }
         if (!f.absorbed && (f.fi < 0 || f.fi >= c.ncx || f.fj < 0 || f.fj >= c.ncy)) f.absorbed = true;
         return f;
+    }
+
+    // ------------------------------------------------------------ dielectric surface charge
+    // A crossing into a dielectric cell, kept from Move for SortBoundary.
+    struct Hit {
+        int s, i, j, dir;
+        R x, y, vx, vy;
+    };
+    std::vector<Hit> hits;
+
+    // One share in fixed point; shares that are not finite or reach 2^20 in
+    // magnitude, and nodes off the grid, are dropped (the kernels' rule).
+    void surface_add(int s, int node, R w) {
+        if (node < 0 || node >= G || !(std::fabs(w) < (R)1048576)) return;
+        sig[(size_t)s * G + node] += (long long)std::llrint((double)w * (double)(1ll << HP_SIGMA_FRAC_BITS));
+    }
+
+    // SortBoundary's dielectric branch (src/cuda_Sortboundary.cu:93-207), on
+    // the flat node index as the reference computes it.
+    void surface_split(const Hit &h) {
+        const int ngy = c.ngy, SY = c.ncy + 2;
+        const int di = h.dir / 3 - 1, dj = h.dir % 3 - 1;
+        const int T = h.i * ngy + h.j, C_ = T + di * ngy + dj;
+        const int g = (h.i + 1 + di) * SY + (h.j + 1 + dj);
+        const int *SI = c.sidx;
+        const R x = h.x, y = h.y, vx = h.vx, vy = h.vy;
+        int pa = 0, pb = 0;
+        R a = 0, b = 0, delta;
+        switch (h.dir) {
+        case 5: delta = x - vx / vy * y; pa = C_; a = 1 - delta; pb = C_ + ngy; b = delta; break;     // top
+        case 3: delta = x + vx / vy * (1 - y); pa = T; a = 1 - delta; pb = T + ngy; b = delta; break; // bottom
+        case 7: delta = y - vy / vx * x; pa = C_; a = 1 - delta; pb = C_ + 1; b = delta; break;       // right
+        case 1: delta = y + vy / vx * (1 - x); pa = T; a = 1 - delta; pb = T + 1; b = delta; break;   // left
+        case 8: // up-right: ngy+1
+            delta = x - vx / vy * y;
+            if (delta >= 0) {
+                if (SI[g - 1]) { delta = y - vy / vx * x; pa = C_ - 1; a = -delta; pb = C_; b = 1 + delta; }
+                else { pa = C_; a = 1 - delta; pb = C_ + ngy; b = delta; }
+            } else {
+                if (SI[g - SY]) { pa = T + 1; a = -delta; pb = C_; b = 1 + delta; }
+                else { delta = y - vy / vx * x; pa = C_; a = 1 - delta; pb = C_ + 1; b = delta; }
+            }
+            break;
+        case 6: // down-right: ngy-1
+            delta = x + vx / vy * (1 - y);
+            if (delta >= 0) {
+                if (SI[g + 1]) { delta = y - vy / vx * x; pa = C_ + 1; a = 2 - delta; pb = C_ + 2; b = delta - 1; }
+                else { pa = C_ + 1; a = 1 - delta; pb = C_ + 1 + ngy; b = delta; }
+            } else {
+                if (SI[g - SY]) { pa = T; a = -delta; pb = C_ + 1; b = 1 + delta; }
+                else { delta = y - vy / vx * x; pa = C_; a = 1 - delta; pb = C_ + 1; b = delta; }
+            }
+            break;
+        case 2: // up-left: -ngy+1
+            delta = x - vx / vy * y;
+            if (delta < 1) {
+                if (SI[g - 1]) { delta = y + vy / vx * (1 - x); pa = C_ + ngy - 1; a = -delta; pb = C_ + ngy; b = 1 + delta; }
+                else { pa = C_; a = 1 - delta; pb = C_ + ngy; b = delta; }
+            } else {
+                if (SI[g + SY]) { pa = T + 1; a = 2 - delta; pb = T + 1 + ngy; b = delta - 1; }
+                else { delta = y + vy / vx * (1 - x); pa = T + 1; a = 1 - delta; pb = T + 2; b = delta; }
+            }
+            break;
+        case 0: // down-left: -ngy-1
+            delta = x + vx / vy * (1 - y);
+            if (delta < 1) {
+                if (SI[g + 1]) { delta = y + vy / vx * (1 - x); pa = T; a = 2 - delta; pb = T + 1; b = delta - 1; }
+                else { pa = C_; a = 1 - delta; pb = T; b = delta; }
+            } else {
+                if (SI[g + SY]) { pa = T; a = 2 - delta; pb = T + ngy; b = delta - 1; }
+                else { delta = y + vy / vx * (1 - x); pa = T - 1; a = 1 - delta; pb = T; b = delta; }
+            }
+            break;
+        default: return;
+        }
+        surface_add(h.s, pa, a);
+        surface_add(h.s, pb, b);
+    }
+
+    // SumSource's surface term (src/cuda_Deposit.cu:40-97)
+    double surface_charge(int n) {
+        const int m = c.sig_mode[n];
+        if (m == 0) return 0.0;
+        if (m == 3) {
+            for (int s = 0; s < c.nsp; s++) sig[(size_t)s * G + n] = 0;
+            return 0.0;
+        }
+        double q = 0.0;
+        for (int s = 0; s < c.nsp; s++)
+            q += (double)sig[(size_t)s * G + n] * (1.0 / (double)(1ll << HP_SIGMA_FRAC_BITS)) * (double)c.q_density[s];
+        sigma[n] = (m == 2 ? 2.0 : 1.0) * q / (double)c.area[n];
+        return q;
     }
 
     // One wrap per crossing (src/cuda_Move.cu:227-255) and the rule of the
@@ -330,6 +432,7 @@ template <class R> struct Sim : SimBase {
                         if (r) {
                             code = 15;
                             if (cond >= 0 && cond < c.cond_numr) cond_charge[(size_t)s * c.cond_numr + cond] += 1.0f;
+                            else if (cond <= -2 && c.n_diel > 0) hits.push_back({s, fi, fj, -2 - cond, lx, ly, mvX, mvY});
                             if (r == 2) walk_bound_hit = true;
                         } else {
                             const int ddi = fi - i, ddj = fj - j;
@@ -361,6 +464,8 @@ template <class R> struct Sim : SimBase {
     // movers addressed to it (sources in increasing cell index, movers in
     // list order), then the far movers in (source, r) order.
     void sort() override {
+        for (const Hit &h : hits) surface_split(h);
+        hits.clear();
         for (int s = 0; s < c.nsp; s++) {
             Sp &p = sp[s];
             std::vector<int> ncnt(C, 0);
@@ -1192,6 +1297,7 @@ template <class R> struct Sim : SimBase {
         for (int n = 0; n < G; n++) {
             double sum = 0.0;
             for (int s = 0; s < c.nsp; s++) sum += den[(size_t)s * G + n] * (double)c.q_density[s];
+            if (c.n_diel > 0) sum += surface_charge(n);
             const double src = sum / 8.8542e-12;
             source[n] = src;
             b64[n] = c.st[2 * G + n] != 0.0f ? src : 0.0;
@@ -1449,6 +1555,7 @@ template <class R> struct Sim : SimBase {
 
     R cond_sigma(int n, int eT, int eL, int eD, int eX, int pL, int pR, int pD, int pU) const {
         const int b = c.boundary[n], f = c.face[n];
+        if (b == 2) return c.n_diel > 0 ? (R)sigma[n] : (R)0; // Sigma left by SumSource
         if (!((b == 3 || b == 1) && f != 8)) return 0;
         R SumSig = 0;
         for (int s = 0; s < c.nsp; s++) SumSig += (R)den[(size_t)s * G + n] * (R)c.q_density[s];

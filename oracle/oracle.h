@@ -65,6 +65,10 @@ typedef struct or_case {
     /* 1-2-1 density smoothing in Deposit (DensitySmoothing passes) */
     int n_smt;
     const int *dens_region; /* [G] */
+    /* dielectric surface charge: present when n_diel > 0 */
+    int n_diel;
+    const int *sig_mode; /* [G] SumSource class: 0 none, 1 dielectric, 2 on a domain edge, 3 conductor */
+    const float *area;   /* [G] node Area */
 } or_case;
 
 typedef struct or_sim or_sim;
@@ -82,7 +86,8 @@ size_t or_num_movers(or_sim *s, int isp);
 void or_get_movers(or_sim *s, int isp, int *counts, float *x, float *y, float *vx, float *vy, float *vz,
                    int8_t *codes);
 /* node fields: which 0 Ex, 1 Ey, 2 phi, 3 phi_pois (float[G]); 4 den (double[nsp*G]);
- * 5 source (double[G]); 6 b (double[G]); 7 x (double[G]) */
+ * 5 source (double[G]); 6 b (double[G]); 7 x (double[G]);
+ * 8 dielectric surface weights (int64[nsp*G], HP_SIGMA_FRAC_BITS fraction bits); 9 Sigma (double[G]) */
 void or_get_grid(or_sim *s, int which, void *out);
 void or_set_grid(or_sim *s, int which, const void *in);
 void or_get_counters(or_sim *s, float *cond_charge, unsigned *mcc_count, int *pcg_iters);

@@ -44,6 +44,7 @@ class OrCase(C.Structure):
         ("np2c", C.c_float * 5),
         ("back_den1", _F), ("back_den2", _F), ("back_vel2", _F), ("fluid_den", _F),
         ("n_smt", C.c_int), ("dens_region", _I),
+        ("n_diel", C.c_int), ("sig_mode", _I), ("area", _F),
     ]
 
 
@@ -108,7 +109,7 @@ class Oracle:
     """CPU restatement of one case.  `tables` is a callable name -> array
     (hpic.Case.table or hpic.Setup.table); `info` the case info."""
 
-    GRID = dict(EX=0, EY=1, PHI=2, PHI_POIS=3, DEN=4, SOURCE=5, B=6, X=7)
+    GRID = dict(EX=0, EY=1, PHI=2, PHI_POIS=3, DEN=4, SOURCE=5, B=6, X=7, SURFACE_CHARGE=8, SIGMA=9)
 
     def __init__(self, tables, info, opts, precision=32, pcg_cluster=1, pcg_block=512, field_mode=None,
                  fs_passes=None):
@@ -166,6 +167,9 @@ class Oracle:
             c.fluid_den = keep("fd", t("fluid_den"), np.float32)
         c.n_smt = info.n_smt
         c.dens_region = keep("dr", t("dens_region"), np.int32)
+        c.n_diel = info.n_dielectric
+        c.sig_mode = keep("sgm", t("sig_mode"), np.int32)
+        c.area = keep("area", t("area"), np.float32)
         c.prob = keep("prob", t("prob"), np.float32)
         c.back_vel1 = keep("bv1", t("back_vel1"), np.float32)
         c.vsave = keep("vsave", t("vsave"), np.float32)
@@ -262,6 +266,8 @@ class Oracle:
             out = np.zeros(G, np.float32)
         elif w == 4:
             out = np.zeros(nsp * G, np.float64)
+        elif w == 8:
+            out = np.zeros(nsp * G, np.int64)
         else:
             out = np.zeros(G, np.float64)
         lib().or_get_grid(self.h, w, out.ctypes.data_as(C.c_void_p))
@@ -269,7 +275,7 @@ class Oracle:
 
     def set_grid(self, name, arr):
         w = self.GRID[name]
-        dt = np.float32 if w <= 3 else np.float64
+        dt = np.float32 if w <= 3 else np.int64 if w == 8 else np.float64
         a = np.ascontiguousarray(arr, dtype=dt)
         lib().or_set_grid(self.h, w, a.ctypes.data_as(C.c_void_p))
 

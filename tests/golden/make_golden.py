@@ -20,7 +20,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(REPO, "hybrid-final_b200"))
-from hpic.decks import block_deck, ccp_deck  # noqa: E402
+from hpic.decks import block_deck, ccp_deck, dielectric_deck  # noqa: E402
 
 GGA = np.dtype([("Boundary", "i4"), ("CondID", "i4"), ("Face", "i4"), ("DensRegion", "i4"), ("Area", "f4"),
                 ("Temp", "f4"), ("BackDen1", "f4"), ("BackVel1", "f4"), ("BackDen2", "f4"), ("BackVel2", "f4"),
@@ -31,6 +31,7 @@ DECKS = {
     "ar_17x9": (ccp_deck(17, 9, 0.005, 0.0025, ppc=10), 12345),
     "ar_33x17": (ccp_deck(33, 17, 0.01, 0.005, ppc=20, pressure_torr=0.1, voltage=200.0), 777),
     "ar_block_33x21": (block_deck(), 4242),
+    "ar_diel_33x21": (dielectric_deck(), 4343),
     "aro2_33x17": (ccp_deck(33, 17, 0.01, 0.005, gas="ArO2", ppc=12, pressure_torr=0.1, voltage=200.0, te_ev=3.0,
                             ion_density={"Ar+": 1e15, "O2+": 2e14, "O+": 0.0, "O-": 2e14}), 515),
     "o2_33x17": (ccp_deck(33, 17, 0.01, 0.005, gas="O2", ppc=12, pressure_torr=0.1, voltage=200.0, te_ev=3.0,

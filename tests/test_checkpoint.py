@@ -11,7 +11,7 @@ import numpy as np
 import pytest
 
 import hpic
-from hpic.decks import ccp_deck
+from hpic.decks import ccp_deck, dielectric_deck
 
 pytestmark = pytest.mark.gpu
 
@@ -29,9 +29,11 @@ DECKS = {
     "ar": (ccp_deck(33, 17, 0.01, 0.005, ppc=20, pressure_torr=0.1, voltage=300.0), 777),
     "aro2": (ccp_deck(33, 17, 0.01, 0.005, gas="ArO2", ppc=20, pressure_torr=0.1, voltage=200.0, te_ev=3.0,
                       ion_density={"Ar+": 1e15, "O2+": 2e14, "O+": 0.0, "O-": 2e14}), 4242),
+    "diel": (dielectric_deck(), 4343),
 }
+CAP = {"diel": 256}
 GRIDS = ("EX", "EY", "PHI", "PHI_POIS", "DEN", "SOURCE", "PCG_X", "PCG_B", "AVE_DEN", "AVE_PHI", "AVE_SOURCE",
-         "AVE_EX", "AVE_EY", "MCC_COUNT", "EEDF")
+         "AVE_EX", "AVE_EY", "MCC_COUNT", "EEDF", "SURFACE_CHARGE", "SIGMA")
 
 
 def read_v000_head(path, nsp):
@@ -51,7 +53,7 @@ def read_v000_head(path, nsp):
 @pytest.mark.parametrize("field_mode", [0, 2])
 def test_resume_is_bit_exact(tmp_path, name, field_mode):
     deck, seed = DECKS[name]
-    opts = dict(field_mode=field_mode, move_mode=1, gas_temp_mode=1, eedf_every=3)
+    opts = dict(field_mode=field_mode, move_mode=1, gas_temp_mode=1, eedf_every=3, cap_per_cell=CAP.get(name, 0))
     a = hpic.Case(deck, seed=seed, **opts)
     a.step(9)
     path = tmp_path / "case.dump"
@@ -72,6 +74,8 @@ def test_resume_is_bit_exact(tmp_path, name, field_mode):
         assert same(a.grid(g), b.grid(g)), g
     assert a.pushes() == b.pushes()
     assert a.status() == b.status() == 0
+    if name == "diel":
+        assert a.grid("SURFACE_CHARGE").sum() > 0
 
 
 def test_v000_part_holds_the_reference_records(tmp_path):

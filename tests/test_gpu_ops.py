@@ -10,7 +10,7 @@ import pytest
 
 import hpic
 import oracle
-from hpic.decks import block_deck, ccp_deck
+from hpic.decks import block_deck, ccp_deck, dielectric_deck
 
 pytestmark = pytest.mark.gpu
 
@@ -32,10 +32,12 @@ DECKS = {
     "ar_block_33x21": (block_deck(), 4242),
     # two 1-2-1 density smoothing passes per Deposit (Smooth_121_x/_y)
     "ar_33x17_smooth2": (ccp_deck(33, 17, 0.01, 0.005, ppc=20, pressure_torr=0.1, voltage=300.0, smoothing=2), 778),
+    # a dielectric slab on the driven electrode and a dielectric block inside
+    "ar_diel_33x21": (dielectric_deck(), 4343),
 }
 # slots per cell where the deck's Max_np / Gsize leaves too little room for
 # the charge that gathers in front of the floating block
-CAP = {"ar_block_33x21": 256}
+CAP = {"ar_block_33x21": 256, "ar_diel_33x21": 256}
 
 
 def pair(name, field_mode=0, move_mode=0, **extra):
@@ -59,6 +61,14 @@ def check_particles(case, o, what=""):
         assert np.array_equal(gc, oc), f"{what} species {s}: counts differ"
         for k, (a, b) in enumerate(zip(ga, oa)):
             assert same(a, b), f"{what} species {s}: component {k} differs"
+
+
+def check_surface(case, o, what=""):
+    """Dielectric surface weights and Sigma, where the deck has dielectrics."""
+    if not case.info.n_dielectric:
+        return
+    assert np.array_equal(case.grid("SURFACE_CHARGE"), o.grid("SURFACE_CHARGE")), f"{what}: surface charge differs"
+    assert same(case.grid("SIGMA"), o.grid("SIGMA")), f"{what}: Sigma differs"
 
 
 def check_grids(case, o, names=("DEN", "SOURCE"), what=""):
@@ -110,6 +120,7 @@ def test_move_and_sort(name, move_mode):
     o.SortBoundary()
     check_particles(case, o, "after SortBoundary")
     assert same(case.grid("COND_CHARGE"), o.counters()[0][: case.info.nsp * case.info.cond_numr])
+    check_surface(case, o, "after SortBoundary")
 
 
 @pytest.mark.parametrize("name", list(DECKS))
@@ -136,6 +147,7 @@ def test_steps_bit_exact(name, mode):
     o.run(0, n, accumulate=True)
     check_particles(case, o, f"after {n} steps")
     check_grids(case, o, ("DEN", "SOURCE"), "after steps")
+    check_surface(case, o, f"after {n} steps")
     for g in ("PHI", "EX", "EY"):
         assert same(case.grid(g), o.grid(g)), g
     assert np.array_equal(case.grid("MCC_COUNT"), o.counters()[1])
@@ -163,6 +175,7 @@ def test_walk_steps_bit_exact(name, ppl):
     o.run(0, n, accumulate=True)
     check_particles(case, o, f"after {n} steps")
     check_grids(case, o, ("DEN", "SOURCE"), "after steps")
+    check_surface(case, o, f"after {n} walk steps")
     assert same(case.grid("COND_CHARGE"), o.counters()[0][: case.info.nsp * case.info.cond_numr])
     assert case.status() == 0
 
@@ -365,3 +378,37 @@ def test_rng_matches_curand_philox(tmp_path):
                    check=True)
     out = subprocess.run([exe], capture_output=True, text=True).stdout
     assert "mismatches 0 host-vs-device 0" in out, out
+
+
+def test_dielectric_crossings_bit_exact():
+    """Hand-placed electrons entering the dielectric slab and block in every
+    direction (E = 0): the surface weights after SortBoundary, then the
+    source and Sigma after Deposit, against the oracle."""
+    from test_dielectric import place
+
+    case, o = pair("ar_diel_33x21")
+    info = case.info
+    for s in range(info.nsp):
+        z = np.zeros(0, np.float32)
+        zc = np.zeros(info.Csize, np.int32)
+        case.set_particles(s, zc, z, z, z, z, z)
+        o.set_particles(s, zc, z, z, z, z, z)
+    S = hpic.Setup(DECKS["ar_diel_33x21"][0], seed=4343, cap_per_cell=CAP["ar_diel_33x21"])
+    place(S, o)
+    counts, arrs = o.particles(0)
+    case.set_particles(0, counts, *arrs)
+    case.set_grid("EX", np.zeros(info.Gsize, np.float32))
+    case.set_grid("EY", np.zeros(info.Gsize, np.float32))
+    case.Move()
+    o.Move()
+    gc, _, gcode = case.movers(0)
+    assert np.all(gcode == 15) and gcode.size > 10
+    case.SortBoundary()
+    o.SortBoundary()
+    sig = case.grid("SURFACE_CHARGE")
+    assert np.array_equal(sig, o.grid("SURFACE_CHARGE")) and sig.sum() > 0
+    case.Deposit()
+    o.Deposit()
+    check_grids(case, o, ("DEN", "SOURCE"), "after Deposit")
+    check_surface(case, o, "after Deposit")
+    assert case.status() == 0

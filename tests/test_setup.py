@@ -38,6 +38,32 @@ def test_geometry_tables(pair):
     assert np.array_equal(bits(s.table("area")), bits(g["gga_Area"]))
 
 
+def test_cell_permittivity(pair):
+    s, g = pair
+    gca = np.frombuffer(g["gca"].tobytes(), dtype=np.dtype([("PlasmaRegion", "i4"), ("eps_r", "f4"), ("eps", "f4")]))
+    assert np.array_equal(bits(s.table("eps_r")), bits(np.ascontiguousarray(gca["eps_r"])))
+
+
+def test_surface_charge_node_classes(pair):
+    """SumSource (src/cuda_Deposit.cu:35-104) reads the inward neighbour's
+    class on the domain edges (x edges first) and the node's own inside."""
+    s, g = pair
+    b = g["gga_Boundary"].reshape(s.info.ngx, s.info.ngy)
+    ngx, ngy = b.shape
+    want = np.zeros_like(b)
+    if len(json.loads(str(g["deck"]))["Geometry"]["DielectricSpec"]):
+        for x in range(ngx):
+            for y in range(ngy):
+                nx, ny, edge = x, y, 1
+                if x == 0: nx = 1
+                elif x == ngx - 1: nx = ngx - 2
+                elif y == 0: ny = 1
+                elif y == ngy - 1: ny = ngy - 2
+                else: edge = 0
+                want[x, y] = {4: 2 if edge else 1, 3: 3}.get(int(b[nx, ny]), 0)
+    assert np.array_equal(s.table("sig_mode").reshape(ngx, ngy), want)
+
+
 def test_matrix(pair):
     s, g = pair
     for mine, ref in (("a_val", "a_val"), ("ta_val", "ta_val"), ("matm", "matm"), ("temp_b", "temp_b"),
