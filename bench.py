@@ -183,10 +183,10 @@ def cpu_baseline(setup, case_opts, budget_s=20.0):
                        f"CPU restatement in FP32, {t_used:.1f} s")
 
 
-def fp64_check(stream, steps=400):
+def fp64_check(stream, steps=800):
     """Error of the precision form against the FP64 oracle on the reference's
     CPU-sized Ar case (129x65 nodes, 4 cm x 2 cm, 50 particles per cell and
-    species, 100 V, 50 mTorr) over one RF period: relative L2 error of the
+    species, 100 V, 50 mTorr) over two RF periods: relative L2 error of the
     time-averaged n_e, n_i and potential, and the electron energy distribution
     (sampled every 4th step) as total-variation distance and relative error of
     the mean energy.  The GPU runs the bench's numerics
