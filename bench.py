@@ -383,8 +383,10 @@ def run_batched(args):
     counts advanced by one graph-captured launch per phase, launch shapes set
     by the autotuner; compared with the plain single-case path on the same
     cases, one case at a time, both with the batched numerics (field_mode 2)
-    and with the reference's solver rule (field_mode 0, one cell crossing per
-    push)."""
+    and with the reference's solver rule (field_mode 0: FP32 PCG to the
+    absolute tolerance).  Both plain runs cross cells one by one (move_mode
+    1): the reference's single wrap lets the state go non-finite within ~100
+    steps at these time steps, which would time a broken run."""
     import torch
 
     import hpic
@@ -396,7 +398,7 @@ def run_batched(args):
     setups = _setups([(d, sd) for d, sd, _ in specs], **opts)
 
     def plain(field_mode, move_mode):
-        pushes, ms = 0, 0.0
+        pushes, ms, bad = 0, 0.0, 0
         for S, (_, sd, _) in zip(setups, specs):
             c = hpic.Case(setup=S, seed=sd, field_mode=field_mode, move_mode=move_mode, gas_temp_mode=1)
             c.step(args.warmup, stream)
@@ -404,11 +406,12 @@ def run_batched(args):
             p0 = c.pushes()
             ms += _timed_steps(c.step, args.steps, stream)
             pushes += c.pushes() - p0
+            bad += 1 if c.status() else 0
             c.close()
-        return pushes / (ms * 1e-3), ms
+        return pushes / (ms * 1e-3), ms, bad
 
-    plain2, plain2_ms = plain(2, 1)
-    plain0, plain0_ms = plain(0, 0)
+    plain2, plain2_ms, plain2_bad = plain(2, 1)
+    plain0, plain0_ms, plain0_bad = plain(0, 1)
     cases = [hpic.Case(setup=S, seed=sd, **opts) for S, (_, sd, _) in zip(setups, specs)]
     batch = hpic.Batch(cases)
     t0 = time.perf_counter()
@@ -434,6 +437,7 @@ def run_batched(args):
                            tune=batch.tune(), autotune_s=round(tune_s, 2)),
                plain=dict(field_mode2_value=plain2, field_mode0_value=plain0,
                           batched_over_plain_mode2=value / plain2, batched_over_plain_reference_rule=value / plain0,
+                          status_nonzero_mode2=plain2_bad, status_nonzero_reference_rule=plain0_bad,
                           note="plain = each case alone through hp_step, one after another, same steps"),
                gpu_launches=batch.step_kernels() * args.steps, clocks=clk,
                device_status_nonzero=int(sum(1 for x in status if x)),

@@ -19,8 +19,9 @@
 #include <cstdint>
 
 // far movers (beyond the 3x3 neighbourhood) one destination cell accepts per
-// step and species; more sets the overflow status
-#define HP_FAR_BUCKET 32
+// step and species; more sets the overflow status.  Strongly driven small
+// cases (65x33 nodes at 260-290 V) send up to ~45 into one cell in a step.
+#define HP_FAR_BUCKET 128
 
 #include "hpic.h" // HP_EEDF_BINS, HP_EEDF_DE
 

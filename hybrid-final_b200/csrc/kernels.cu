@@ -169,6 +169,8 @@ __device__ __forceinline__ void surface_split(const DevCase &d, int s, int i, in
 constexpr int CODE_FAR = 14, CODE_ABSORBED = 15;
 // far movers a destination cell accepts per step (per species)
 constexpr int FAR_B = HP_FAR_BUCKET;
+constexpr int FAR_W = FAR_B / 32; // bucket keys per lane when a warp sorts a bucket
+static_assert(FAR_B % 32 == 0, "far buckets hold whole warps of keys");
 
 // Where a particle that left cell (i, j) ends.  Each crossing wraps the
 // offset by one cell (src/cuda_Move.cu:227-255) and applies the rule of the
@@ -756,23 +758,50 @@ __global__ void __launch_bounds__(SORT_MAXW * 32) k_sort_count(const DevCase *__
         const DevSpecies &sp = d.sp[fs];
         const int cap = sp.cap;
         const size_t b = (size_t)fs * d.C + fc;
-        unsigned long long key = lane < fnf ? d.far_key[b * FAR_B + lane] : ~0ull;
+        // key w*32 + lane of the bucket in key[w]; its place in (source
+        // cell, r) order in pos[w] (the keys are distinct)
+        unsigned long long key[FAR_W];
+        int pos[FAR_W];
+#pragma unroll
+        for (int w = 0; w < FAR_W; w++) {
+            key[w] = w * 32 + lane < fnf ? d.far_key[b * FAR_B + w * 32 + lane] : ~0ull;
+            pos[w] = w * 32 + lane;
+        }
         __syncwarp();
         if (lane == 0) d.far_in[b] = 0;
-        // bitonic network across the lanes (keys are distinct)
+        if (fnf <= 32) {
+            // bitonic network across the lanes
 #pragma unroll
-        for (int k = 2; k <= 32; k <<= 1)
+            for (int k = 2; k <= 32; k <<= 1)
 #pragma unroll
-            for (int jj = k >> 1; jj > 0; jj >>= 1) {
-                const unsigned long long o = __shfl_xor_sync(FULL, key, jj);
-                const bool keep_min = ((lane & jj) == 0) == ((lane & k) == 0);
-                key = keep_min ? (o < key ? o : key) : (o > key ? o : key);
+                for (int jj = k >> 1; jj > 0; jj >>= 1) {
+                    const unsigned long long o = __shfl_xor_sync(FULL, key[0], jj);
+                    const bool keep_min = ((lane & jj) == 0) == ((lane & k) == 0);
+                    key[0] = keep_min ? (o < key[0] ? o : key[0]) : (o > key[0] ? o : key[0]);
+                }
+        } else {
+            // a rare full bucket: rank every key against all the others
+#pragma unroll
+            for (int w = 0; w < FAR_W; w++) pos[w] = 0;
+            for (int w2 = 0; w2 * 32 < fnf; w2++) {
+                unsigned long long kw = key[0];
+#pragma unroll
+                for (int w = 1; w < FAR_W; w++)
+                    if (w == w2) kw = key[w];
+                for (int l = 0; l < 32; l++) {
+                    const unsigned long long o = __shfl_sync(FULL, kw, l);
+#pragma unroll
+                    for (int w = 0; w < FAR_W; w++) pos[w] += o < key[w] ? 1 : 0;
+                }
             }
+        }
         bool ov = false;
-        if (lane < fnf) {
-            const int slot = fout + lane;
+#pragma unroll
+        for (int w = 0; w < FAR_W; w++) {
+            if (w * 32 + lane >= fnf) continue;
+            const int slot = fout + pos[w];
             if (slot < flimit) {
-                const int sc = (int)(key >> 18), r = (int)(key & 0x3FFFF);
+                const int sc = (int)(key[w] >> 18), r = (int)(key[w] & 0x3FFFF);
                 const size_t q = (size_t)sc * cap + (size_t)(cap - 1 - r);
                 const size_t dst = (size_t)fc * cap + (size_t)slot;
                 sp.x[dst] = sp.x[q];

@@ -111,6 +111,7 @@ struct SimBase {
     virtual void mcc(int64_t) = 0;
     virtual void deposit(bool smooth) = 0;
     virtual void accumulate() = 0;
+    virtual int far_max() const = 0;
 };
 
 template <class R> struct Sim : SimBase {
@@ -395,6 +396,12 @@ template <class R> struct Sim : SimBase {
 
     // movers beyond the 3x3 neighbourhood: (species, dest) -> (source<<18 | r, mover index)
     std::vector<std::vector<std::pair<uint64_t, size_t>>> far[5];
+    int far_max() const override {
+        size_t m = 0;
+        for (int s = 0; s < c.nsp; s++)
+            for (const auto &v : far[s]) m = std::max(m, v.size());
+        return (int)m;
+    }
 
     // MoveE_Basic (src/cuda_Move.cu:181-270) with the boundary rules applied
     // per crossing; mover codes: destination (di+1)*3+(dj+1) within the 3x3
@@ -1767,6 +1774,7 @@ void or_math(int fn, const float *x, const float *y, float *out, int n) {
     }
 }
 int or_walk_bound_hit(or_sim *s) { return s->impl->walk_bound_hit ? 1 : 0; }
+int or_far_max(or_sim *s) { return s->impl->far_max(); }
 void or_get_counters(or_sim *s, float *cond_charge, unsigned *mcc_count, int *pcg_iters) {
     SimBase *b = s->impl;
     if (cond_charge) std::memcpy(cond_charge, b->cond_charge.data(), b->cond_charge.size() * 4);

@@ -93,6 +93,8 @@ void or_set_grid(or_sim *s, int which, const void *in);
 void or_get_counters(or_sim *s, float *cond_charge, unsigned *mcc_count, int *pcg_iters);
 /* 1 once a move_mode 1 walk reached its crossing bound (the particle was absorbed) */
 int or_walk_bound_hit(or_sim *s);
+/* most movers from beyond the 3x3 neighbourhood that one cell received in the last Move */
+int or_far_max(or_sim *s);
 /* the shared elementary functions (include/hp_math.h), for accuracy tests:
  * fn 0 exp, 1 log, 2 log10, 3 pow(x, y), 4 sin(2 pi x), 5 cos(2 pi x), 6 tan (x in [0, pi/2)), 7 atan */
 void or_math(int fn, const float *x, const float *y, float *out, int n);

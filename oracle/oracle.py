@@ -289,6 +289,9 @@ class Oracle:
     def walk_bound_hit(self):
         return bool(lib().or_walk_bound_hit(self.h))
 
+    def far_max(self):
+        return int(lib().or_far_max(self.h))
+
     def Field(self, tstep):
         lib().or_field(self.h, tstep)
 

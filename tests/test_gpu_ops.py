@@ -412,3 +412,33 @@ def test_dielectric_crossings_bit_exact():
     check_grids(case, o, ("DEN", "SOURCE"), "after Deposit")
     check_surface(case, o, "after Deposit")
     assert case.status() == 0
+
+
+def test_far_bucket_beyond_one_warp():
+    """Every electron moved three cells in x at E = 0: each destination
+    cell receives a whole source cell's electrons (about 50, more than one
+    warp of keys), placed in (source cell, rank) order as the oracle does."""
+    deck = ccp_deck(33, 17, 0.01, 0.005, ppc=50)
+    S = hpic.Setup(deck, seed=31, field_mode=2, move_mode=1)
+    case = hpic.Case(setup=S, seed=31, field_mode=2, move_mode=1)
+    info = case.info
+    o = oracle.Oracle(S.table, S.info, case.opts, 32, pcg_cluster=info.pcg_cluster, pcg_block=info.pcg_block)
+    for s in range(info.nsp):
+        counts, arrs = S.particles(s, layout=0)
+        o.set_particles(s, counts, *arrs)
+    counts, (x, y, vx, vy, vz) = case.particles(0)
+    vx = np.full_like(vx, np.float32(3.0 * info.dx / info.dt))
+    vy = np.zeros_like(vy)
+    case.set_particles(0, counts, x, y, vx, vy, vz)
+    o.set_particles(0, counts, x, y, vx, vy, vz)
+    for g in ("EX", "EY"):
+        z = np.zeros(info.Gsize, np.float32)
+        case.set_grid(g, z)
+        o.set_grid(g, z)
+    case.Move()
+    o.Move()
+    assert o.far_max() > 32
+    case.SortBoundary()
+    o.SortBoundary()
+    check_particles(case, o, "after a sort with full far buckets")
+    assert case.status() == 0
