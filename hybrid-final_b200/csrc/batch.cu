@@ -44,11 +44,13 @@ hp_status batch_dev_build(hp_case *const *cases, int n, BatchDev &b) {
     b.any_eedf = false;
     b.max_smt = 0;
     b.surface = false;
+    b.power = false;
     for (int i = 0; i < n; i++) {
         hd[i] = cases[i]->h;
         b.any_eedf |= cases[i]->h.eedf_every > 0;
         b.max_smt = std::max(b.max_smt, cases[i]->s.N_smt);
         b.surface = b.surface || cases[i]->s.diel_num > 0;
+        b.power = b.power || cases[i]->s.power_driven();
         const Setup &s = cases[i]->s;
         part[i + 1] = part[i] + s.nsp * s.Csize;
         cell[i + 1] = cell[i] + s.Csize;
@@ -125,6 +127,7 @@ hp_status run_step(const BatchDev &b, const LaunchCfg &lc, int gas, cudaStream_t
     CK(launch_deposit(b.d_cases, b.d_part, b.d_node, b.n, b.n_part, b.n_node, lc, st, b.max_smt));
     CK(launch_accumulate(b.d_cases, b.d_node, b.n, b.n_node, st));
     if (b.any_eedf) CK(launch_eedf(b.d_cases, b.d_cell, b.n, b.n_cell, st));
+    if (b.power) CK(launch_power(b.d_cases, b.n, st));
     return HP_OK;
 }
 

@@ -142,6 +142,8 @@ void fill_info(const Setup &s, hp_case_info *out) {
     out->mcc_stride = s.main_gas == GAS_AR ? 8 : 72;
     out->n_smt = s.N_smt;
     out->n_dielectric = s.diel_num;
+    out->n_sources = s.src_num;
+    out->power_driven = s.power_driven() ? 1 : 0;
 }
 
 // Collision probability per cell from its lower-left node
@@ -276,8 +278,6 @@ hp_status build_device(hp_case *c) {
     if (s.diel_num > 0) {
         TRY(dalloc(c, &h.sig, (size_t)s.nsp * G));
         TRY(dupload(c, (int **)&h.sig_mode, s.sig_mode));
-        TRY(dupload(c, (float **)&h.area, s.area));
-        TRY(dalloc(c, &h.sigma, (size_t)G));
         // the crossings one step can queue: every particle a cell next to a
         // dielectric cell can hold (the mover half of its slots), per species
         long long adj = 0;
@@ -361,6 +361,28 @@ hp_status build_device(hp_case *c) {
         h.src_rphase[k] = s.src_rphase[k];
     }
     for (int k = 0; k < s.cond_numr; k++) h.efield_flag[k] = s.efield_flag[k];
+    TRY(dupload(c, (float **)&h.src_amp, std::vector<float>(s.src_ac.begin(), s.src_ac.end())));
+    if (s.power_driven()) {
+        for (int k = 0; k < s.src_num; k++) h.src_power[k] = s.src_power[k];
+        for (int k = 0; k < s.cond_numr; k++) {
+            h.cond_src_num[k] = s.cond_src_num[k];
+            h.cond_power_id[k] = s.cond_power_id[k];
+        }
+        h.pd_intv = s.pd_intv;
+        h.pd_ratio = s.pd_ratio;
+        TRY(dalloc(c, &h.pw, 1));
+        TRY(dalloc(c, &h.cond_step, (size_t)s.nsp * s.cond_numr));
+        std::vector<int> cn;
+        for (int n = 0; n < G; n++)
+            if (s.cond_id[n]) cn.push_back(n | ((s.cond_id[n] - 1) << 24));
+        if (G >= (1 << 24)) return set_error("power-driven decks hold at most 2^24 nodes"), HP_ERR_ARG;
+        h.n_cond_nodes = (int)cn.size();
+        TRY(dupload(c, (int **)&h.cond_nodes, cn));
+    }
+    if (s.power_driven() || s.diel_num > 0) {
+        TRY(dupload(c, (float **)&h.area, s.area));
+        TRY(dalloc(c, &h.sigma, (size_t)G));
+    }
     TRY(dupload(c, (float **)&h.xsec, s.xsec));
     h.n_logx = s.n_logx;
     h.xw = 2 + s.n_cx;
@@ -497,6 +519,7 @@ hp_status one_step(hp_case *c, cudaStream_t st) {
     TRY(op_deposit(c, st, true));
     e = launch_accumulate(c->d_case, c->d_items + 4, 1, c->s.Gsize, st);
     if (e == cudaSuccess && c->h.eedf_every > 0) e = launch_eedf(c->d_case, c->d_items + 2, 1, c->s.Csize, st);
+    if (e == cudaSuccess && c->h.pw) e = launch_power(c->d_case, 1, st);
     return e == cudaSuccess ? HP_OK : cuda_fail(e, "accumulate");
 }
 
@@ -648,6 +671,15 @@ static hp_status table_of(const Setup &s, const std::vector<float> *prob, const 
     case 37: if (fs) { src = fs->Wt.data(); nb = fs->Wt.size() * 4; } break;
     case 38: if (fs) { src = fs->inv_eig.data(); nb = fs->inv_eig.size() * 4; } break;
     case 39: src = s.sig_mode.data(); nb = s.sig_mode.size() * 4; break;
+    case 40: // power-driven sources: pd_intv, pd_ratio, target power per source, (count, first) per conductor
+        tmpf.push_back((float)s.pd_intv);
+        tmpf.push_back(s.pd_ratio);
+        for (int k = 0; k < s.src_num; k++) tmpf.push_back(s.src_power[k]);
+        for (int k = 0; k < s.cond_numr; k++) {
+            tmpf.push_back((float)s.cond_src_num[k]);
+            tmpf.push_back((float)s.cond_power_id[k]);
+        }
+        src = tmpf.data(); nb = tmpf.size() * 4; break;
     default: set_error("unknown table id"); return HP_ERR_ARG;
     }
     if (needed) *needed = nb;
@@ -985,6 +1017,8 @@ static hp_status grid_ptr(hp_case *c, hp_grid_field f, void **p, size_t *nb) {
     case HP_GRID_EEDF: *p = c->h.eedf; *nb = (size_t)(HP_EEDF_BINS + 1) * 8; break;
     case HP_GRID_SURFACE_CHARGE: *p = c->h.sig; *nb = c->h.sig ? (size_t)nsp * G * 8 : 0; break;
     case HP_GRID_SIGMA: *p = c->h.sigma; *nb = c->h.sigma ? (size_t)G * 8 : 0; break;
+    case HP_GRID_SOURCE_AC: *p = c->h.src_amp; *nb = (size_t)c->s.src_num * 4; break;
+    case HP_GRID_POWER_STATE: *p = c->h.pw; *nb = c->h.pw ? sizeof(PowerState) : 0; break;
     default: return set_error("unknown grid field"), HP_ERR_ARG;
     }
     return HP_OK;

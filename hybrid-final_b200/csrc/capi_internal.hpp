@@ -72,6 +72,7 @@ struct BatchDev {
     bool any_eedf = false;
     int max_smt = 0; // most density smoothing passes of any case
     bool surface = false; // some case has dielectric blocks
+    bool power = false;   // some case has power-driven sources
     // PCG groups for every cluster cap 1,2,4,8,16: lists of case indices per
     // cluster size, concatenated in d_lists
     int *d_lists = nullptr;

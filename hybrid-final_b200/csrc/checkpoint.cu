@@ -68,7 +68,7 @@ const hp_grid_field EXT_GRIDS[] = {HP_GRID_EX,         HP_GRID_EY,          HP_G
                                    HP_GRID_DEN,        HP_GRID_SOURCE,      HP_GRID_PCG_X,   HP_GRID_PCG_B,
                                    HP_GRID_AVE_DEN,    HP_GRID_AVE_PHI,     HP_GRID_AVE_SOURCE, HP_GRID_AVE_EX,
                                    HP_GRID_AVE_EY,     HP_GRID_COND_CHARGE, HP_GRID_MCC_COUNT, HP_GRID_EEDF,
-                                   HP_GRID_SURFACE_CHARGE, HP_GRID_SIGMA};
+                                   HP_GRID_SURFACE_CHARGE, HP_GRID_SIGMA, HP_GRID_SOURCE_AC, HP_GRID_POWER_STATE};
 
 template <class T> std::vector<T> fetch(hp_case *c, hp_grid_field f) {
     void *p = nullptr;

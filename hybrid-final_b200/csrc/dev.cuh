@@ -41,6 +41,18 @@ struct DevSpecies {
     float Ascale, q_density, Escale, np2c;
 };
 
+// The power controller of the reference's Diagnostic (src/cuda_Diagnostic.cu:
+// 365-420) per case: conductor surface charges of the last three steps,
+// power accumulated since the last revision and the revision count.
+struct PowerState {
+    double surf[DMAXCOND], old[DMAXCOND], old2[DMAXCOND];
+    float power[DMAXCOND];
+    int count[DMAXCOND];
+    int power_init;
+    int pad;
+};
+static_assert(sizeof(PowerState) == 8 * DMAXCOND * 3 + 4 * DMAXCOND * 2 + 8, "PowerState layout (the Python binding sizes it)");
+
 struct DevCase {
     // geometry
     int ngx, ngy, ncx, ncy, G, C, nsp, gas, cond_numr, n_unknowns;
@@ -84,6 +96,16 @@ struct DevCase {
     int src_mid[DMAXSRC];
     float src_dc[DMAXSRC], src_ac[DMAXSRC], src_2pif[DMAXSRC], src_rphase[DMAXSRC];
     int efield_flag[DMAXCOND];
+    float *src_amp;                 // [src_num] AC amplitudes in use (the power controller revises them)
+    // power-driven sources (null pw without any)
+    PowerState *pw;
+    unsigned int *cond_step;        // [nsp*cond_numr] particles absorbed per conductor in this step
+    const int *cond_nodes;          // [n_cond_nodes] node | (conductor index << 24), nodes with a CondID
+    int n_cond_nodes;
+    int cond_src_num[DMAXCOND], cond_power_id[DMAXCOND];
+    float src_power[DMAXSRC];
+    int pd_intv;
+    float pd_ratio;
     // collisions
     const float *xsec;              // [n_logx * xw]
     int n_logx, xw;

@@ -363,8 +363,12 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
             const int r = walk(geo_of(d), fi, fj, lx, ly, mvX, mvY, cond);
             if (r) {
                 code = CODE_ABSORBED;
-                if (cond >= 0 && cond < d.cond_numr) atomicAdd(&d.cond_charge[s * d.cond_numr + cond], 1.0f);
-                else if (cond <= -2 && d.sig) surface_enqueue(d, s, fi, fj, -2 - cond, lx, ly, mvX, mvY);
+                if (cond >= 0 && cond < d.cond_numr) {
+                    atomicAdd(&d.cond_charge[s * d.cond_numr + cond], 1.0f);
+                    if (d.cond_step) atomicAdd(&d.cond_step[s * d.cond_numr + cond], 1u);
+                } else if (cond <= -2 && d.sig) {
+                    surface_enqueue(d, s, fi, fj, -2 - cond, lx, ly, mvX, mvY);
+                }
                 if (r == 2) atomicOr(d.status, ST_WALK);
             } else {
                 const int ddi = fi - i, ddj = fj - j;
@@ -500,8 +504,12 @@ __global__ void __launch_bounds__(512) k_move_u(const DevCase *__restrict__ case
                 const int r = walk(geo_of(d), fi, fj, X, Y, vX, vY, cond);
                 if (r) {
                     code = CODE_ABSORBED;
-                    if (cond >= 0 && cond < d.cond_numr) atomicAdd(&d.cond_charge[s * d.cond_numr + cond], 1.0f);
-                    else if (cond <= -2 && d.sig) surface_enqueue(d, s, fi, fj, -2 - cond, X, Y, vX, vY);
+                    if (cond >= 0 && cond < d.cond_numr) {
+                        atomicAdd(&d.cond_charge[s * d.cond_numr + cond], 1.0f);
+                        if (d.cond_step) atomicAdd(&d.cond_step[s * d.cond_numr + cond], 1u);
+                    } else if (cond <= -2 && d.sig) {
+                        surface_enqueue(d, s, fi, fj, -2 - cond, X, Y, vX, vY);
+                    }
                     if (r == 2) atomicOr(d.status, ST_WALK);
                 } else {
                     const int ddi = fi - i, ddj = fj - j;
@@ -1593,6 +1601,20 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
 }
 
 // Efield_cuda_Basic potential assembly (src/cuda_Field.cu:9-34):
+// V_k(t) of conductor k (src/cuda_Field.cu:10-20): its sources' DC + AC
+// sin(2 pi f t + phase), summed in the reference's precision; the AC
+// amplitudes are the ones in use (a power controller revises them)
+__device__ __forceinline__ float cond_voltage(const DevCase &d, int k, double time) {
+    float vk = 0.0f;
+    if (d.efield_flag[k]) {
+        for (int q = 0; q < d.src_num; q++)
+            if (d.src_mid[q] == k + 1)
+                vk = (float)((double)vk + ((double)d.src_dc[q] +
+                                           (double)d.src_amp[q] * sin((double)d.src_2pif[q] * time + (double)d.src_rphase[q])));
+    }
+    return vk;
+}
+
 // TotPotential = sum_k V_k(t) * phi_Lap,k + phi_Pois, in the reference's
 // order and precision (float accumulation, V_k(t) from a double sine).
 __global__ void __launch_bounds__(256) k_potential(const DevCase *__restrict__ cases, const int *__restrict__ item_start,
@@ -1604,16 +1626,7 @@ __global__ void __launch_bounds__(256) k_potential(const DevCase *__restrict__ c
     const int n = t - item_start[ci];
     const double time = (double)(*d.tstep) * (double)d.dt;
     float tot = 0.0f;
-    for (int k = 0; k < d.cond_numr; k++) {
-        float vk = 0.0f;
-        if (d.efield_flag[k]) {
-            for (int q = 0; q < d.src_num; q++)
-                if (d.src_mid[q] == k + 1)
-                    vk = (float)((double)vk + ((double)d.src_dc[q] +
-                                               (double)d.src_ac[q] * sin((double)d.src_2pif[q] * time + (double)d.src_rphase[q])));
-        }
-        tot += vk * d.lap[(size_t)k * d.G + n];
-    }
+    for (int k = 0; k < d.cond_numr; k++) tot += cond_voltage(d, k, time) * d.lap[(size_t)k * d.G + n];
     tot += 1 * d.phi_p[n];
     d.phi[n] = tot;
 }
@@ -1672,6 +1685,10 @@ __global__ void __launch_bounds__(256) k_efield(const DevCase *__restrict__ case
     const float idx = d.idx, idy = d.idy, hdx = d.hdx, hdy = d.hdy, dx = d.dx, dy = d.dy;
     float Ex, Ey;
     bool write = true;
+    // Cond_Sigma's Sigma at conductor and Dirichlet face nodes, kept for the
+    // power controller's surface charge
+    if (d.sigma && (b == 3 || b == 1) && f != 8)
+        d.sigma[n] = (double)cond_sigma(d, n, x, y, eT, eL, eD, eX, pL, pR, pD, pU);
     if (f == 0) { // LEFT
         if (b == 3 || b == 2 || b == 1) {
             Ex = -2.0f * cond_sigma(d, n, x, y, eT, eL, eD, eX, pL, pR, pD, pU) / (E[eL] + E[eX]);
@@ -1765,6 +1782,74 @@ __global__ void __launch_bounds__(256) k_efield(const DevCase *__restrict__ case
         d.Ex[n] = Ex;
         d.Ey[n] = Ey;
     }
+}
+
+// The reference's power controller (Diagnostic, src/cuda_Diagnostic.cu:
+// 365-420), once per step after Deposit, one block per case: the conductor
+// surface charges sum Sigma * Area over the nodes with a CondID (FP64; each
+// thread a strided share of the node list, then a fixed tree), the
+// conduction current of this step's absorbed particles, the displacement
+// current from the last three surface charges, and every pd_intv steps the
+// revision of the first power-driven source's amplitude: (target / mean
+// power)^0.2 times the amplitude, or at most 5 % up when that would exceed
+// (1 + VoltageUpDownRatio) times it; the first revision only arms the
+// controller.  hp_powf stands for the reference's double pow.
+constexpr int PW_T = 256;
+__global__ void __launch_bounds__(PW_T) k_power(DevCase *cases, int ncases) {
+    const DevCase &d = cases[blockIdx.x];
+    if (!d.pw) return;
+    __shared__ double part[PW_T][DMAXCOND];
+    const int t = threadIdx.x, nc = d.cond_numr;
+    double acc[DMAXCOND];
+#pragma unroll
+    for (int k = 0; k < DMAXCOND; k++) acc[k] = 0.0;
+    for (int q = t; q < d.n_cond_nodes; q += PW_T) {
+        const int v = d.cond_nodes[q], n = v & 0xFFFFFF, k = v >> 24;
+        const double a = d.sigma[n] * (double)d.area[n];
+#pragma unroll
+        for (int kk = 0; kk < DMAXCOND; kk++)
+            if (kk == k) acc[kk] += a;
+    }
+#pragma unroll
+    for (int k = 0; k < DMAXCOND; k++) part[t][k] = acc[k];
+    __syncthreads();
+    for (int h = PW_T / 2; h > 0; h >>= 1) {
+        if (t < h)
+            for (int k = 0; k < nc; k++) part[t][k] += part[t + h][k];
+        __syncthreads();
+    }
+    if (t != 0) return;
+    PowerState &P = *d.pw;
+    const double time = (double)(*d.tstep) * (double)d.dt;
+    for (int i = 0; i < nc; i++) {
+        P.old2[i] = P.old[i];
+        P.old[i] = P.surf[i];
+        P.surf[i] = part[0][i];
+        float cond_current = 0.0f;
+        for (int s = 0; s < d.nsp; s++) {
+            unsigned int &cnt = d.cond_step[s * nc + i];
+            cond_current += d.sp[s].q_density * (float)cnt / d.dt;
+            cnt = 0;
+        }
+        const float dis_current = (float)(0.5 * (3.0 * P.surf[i] - 4.0 * P.old[i] + P.old2[i]) / (double)d.dt);
+        const float current = dis_current - cond_current;
+        if (d.cond_src_num[i] != 1) continue; // voltage driven, or the reference's (empty) dual-power branch
+        float phi_now = cond_voltage(d, i, time);
+        P.power[i] += phi_now * current;
+        P.count[i]++;
+        if (P.count[i] != d.pd_intv) continue;
+        P.power[i] /= (float)P.count[i];
+        P.count[i] = 0;
+        const int q = d.cond_power_id[i];
+        if (P.power[i] > 0) phi_now = d.src_amp[q] * hp_powf(fabsf(d.src_power[q] / P.power[i]), 0.2f);
+        if (P.power_init) {
+            if (phi_now > (1.0f + d.pd_ratio) * d.src_amp[q]) d.src_amp[q] = (float)((double)d.src_amp[q] * 1.05);
+            else d.src_amp[q] = phi_now;
+        }
+        P.power[i] = 0.0f;
+        P.power_init++;
+    }
+    (void)ncases;
 }
 
 __global__ void k_advance(const DevCase *__restrict__ cases, int ncases) {
@@ -1865,6 +1950,12 @@ cudaError_t launch_move(const DevCase *cases, const int *item_start, int ncases,
     else
         k_move<MOVE_RING><<<nb, tpb, (size_t)(tpb / 32) * MOVE_RING * 5 * 32 * sizeof(float), st>>>(
             cases, item_start, ncases, items);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_power(DevCase *cases, int ncases, cudaStream_t st) {
+    if (ncases <= 0) return cudaSuccess;
+    k_power<<<ncases, PW_T, 0, st>>>(cases, ncases);
     return cudaGetLastError();
 }
 

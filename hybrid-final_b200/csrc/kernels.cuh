@@ -21,6 +21,9 @@ struct LaunchCfg {
 cudaError_t launch_move(const DevCase *cases, const int *item_start, int ncases, int items, const LaunchCfg &lc,
                         cudaStream_t st);
 // SortBoundary: boundary handling + deterministic re-bin (src/cuda_Sortboundary.cu:41-258)
+// the power controller of power-driven cases, after Deposit (cases without
+// one return at once)
+cudaError_t launch_power(DevCase *cases, int ncases, cudaStream_t st);
 // surface: some case has dielectric blocks (apply the crossings Move queued)
 cudaError_t launch_sort(const DevCase *cases, const int *item_start, int ncases, int items, const LaunchCfg &lc,
                         cudaStream_t st, bool surface);

@@ -224,8 +224,8 @@ void read_geometry(const JVal &root, Setup &s, std::vector<int> &bx0, std::vecto
         float dc = fnum(c, "DC(V)"), pw = fnum(c, "Power(W)"), ac = fnum(c, "AC(V)"), fr = fnum(c, "Freq(1/s)");
         float ph = fnum(c, "Phase(deg)");
         if (dc == 0 && pw == 0 && ac == 0) deck_fail("Source line " + std::to_string(i + 1) + " is error");
-        if (pw != 0) unsupported("power-driven sources are outside this library's step path");
         s.src_mid.push_back(mid);
+        s.src_power.push_back(pw);
         s.src_dc.push_back(dc);
         s.src_ac.push_back(ac);
         s.src_freq.push_back(fr);
@@ -384,6 +384,13 @@ void read_method(const JVal &root, Setup &s) { // src/start.c:732-747
     if (s.N_smt < 0) s.N_smt = 0;
     ivnzc(m, "ParticleLimit");
     if (inum(m, "ConstB_Flag")) unsupported("constant magnetic field (ConstB_Flag)");
+    // power-driven sources (src/start.c:786-790): the amplitude is revised
+    // every Interval RF periods, by at most VoltageUpDownRatio upwards
+    const JVal &pd = m.object("PowerDrivenOption");
+    s.pd_intv = (int)((float)s.DT_PIC * fnum(pd, "Interval"));
+    if (s.pd_intv == 0) s.pd_intv = 5 * s.DT_PIC;
+    s.pd_ratio = fnum(pd, "VoltageUpDownRatio");
+    if (s.pd_ratio == 0.0f) s.pd_ratio = 0.05f;
 }
 
 // ---------------------------------------------------------------- tables
@@ -1203,6 +1210,18 @@ void build_setup(const char *json, size_t len, const BuildOpts &o, Setup &s) {
             if (i + 1 == s.src_mid[j]) n++;
         s.efield_flag[i] = (n > 0 && n < 4) ? 1 : 0;
     }
+    // power-driven sources per conductor (src/Efield.c:29-66): the first
+    // one's amplitude is what the controller revises; two make the
+    // reference's dual-power mode, which revises nothing
+    s.cond_src_num.assign(s.cond_numr, 0);
+    s.cond_power_id.assign(s.cond_numr, -1);
+    for (int i = 0; i < s.cond_numr; i++)
+        for (int j = 0; j < s.src_num; j++)
+            if (i + 1 == s.src_mid[j] && s.src_power[j] != 0) {
+                if (s.cond_src_num[i] == 2) deck_fail("no more than two power-driven sources per conductor");
+                if (s.cond_src_num[i] == 0) s.cond_power_id[i] = j;
+                s.cond_src_num[i]++;
+            }
     field_matrix(s);
     gas_setting(s, o);
     null_collision(s);

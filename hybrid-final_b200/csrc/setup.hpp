@@ -69,6 +69,15 @@ struct Setup {
     std::vector<int> src_mid;
     std::vector<float> src_dc, src_ac, src_freq, src_2pifreq, src_rphase;
     std::vector<int> efield_flag; // per conductor (src/Efield.c:34-60)
+    std::vector<float> src_power; // per source: target power (W), 0 for a voltage source
+    std::vector<int> cond_src_num, cond_power_id; // per conductor: power-driven sources, the first one's index
+    int pd_intv = 0;              // steps between amplitude revisions (PowerDrivenOption.Interval x DT_PIC)
+    float pd_ratio = 0.05f;       // PowerDrivenOption.VoltageUpDownRatio
+    bool power_driven() const {
+        for (int n : cond_src_num)
+            if (n > 0) return true;
+        return false;
+    }
     int diel_num = 0;             // DielectricSpec blocks
     std::vector<int> diel_mid, diel_x0, diel_x1, diel_y0, diel_y1;
     std::vector<float> diel_eps;

@@ -24,14 +24,15 @@ STATUS_CELL_OVERFLOW, STATUS_NONFINITE, STATUS_PCG_NOCONV, STATUS_WAIT_TIMEOUT =
 
 GRID = dict(EX=0, EY=1, PHI=2, PHI_POIS=3, DEN=4, SOURCE=5, PCG_X=6, PCG_B=7, AVE_DEN=8, AVE_PHI=9,
             COND_CHARGE=10, MCC_COUNT=11, EEDF=12, AVE_SOURCE=13, AVE_EX=14, AVE_EY=15,
-            SURFACE_CHARGE=16, SIGMA=17)
+            SURFACE_CHARGE=16, SIGMA=17, SOURCE_AC=18, POWER_STATE=19)
 SIGMA_FRAC_BITS = 28  # fixed-point fraction bits of SURFACE_CHARGE (particle weights)
+POWER_STATE_BYTES = 8 * 8 * 3 + 4 * 8 * 2 + 8  # PowerState: surf, old, old2 (double[8]); power, count; flags
 EEDF_BINS, EEDF_DE = 200, 0.25  # electron energy histogram: 0.25 eV bins from 0, one overflow bin
 TABLE = dict(sidx=0, a_idx=1, boundary=2, face=3, cond_id=4, area=5, back_den1=6, back_vel1=7, lap=8,
              stencil=9, vsave=10, xsec=11, collf=12, sigv=13, dens_region=14, prob=15, eps_r=16,
              back_den2=17, back_vel2=18, a_val=19, ai=20, aj=21, matm=22, cond_b=23, temp_b=24, ta_val=25,
              species=26, node_temp=27, dep_factor=28, fluid_den=29, scalars=30, sources=31, unk_node=32,
-             fs_info=33, fs_V=34, fs_Vt=35, fs_W=36, fs_Wt=37, fs_inv=38, sig_mode=39)
+             fs_info=33, fs_V=34, fs_Vt=35, fs_W=36, fs_Wt=37, fs_inv=38, sig_mode=39, power=40)
 TABLE_DTYPE = {0: np.int32, 1: np.int32, 2: np.int32, 3: np.int32, 4: np.int32, 14: np.int32, 20: np.int32,
                21: np.int32, 32: np.int32, 33: np.int32, 39: np.int32}
 
@@ -55,7 +56,8 @@ class CaseInfo(C.Structure):
                 ("n_unknowns", C.c_int), ("cap", C.c_int * 8), ("mcc_subcycles", C.c_int), ("dt", C.c_double),
                 ("dx", C.c_double), ("dy", C.c_double), ("tstep", C.c_int64), ("device_bytes", C.c_size_t),
                 ("pcg_cluster", C.c_int), ("pcg_block", C.c_int), ("field_mode", C.c_int), ("mcc_stride", C.c_int),
-                ("n_smt", C.c_int), ("n_dielectric", C.c_int)]
+                ("n_smt", C.c_int), ("n_dielectric", C.c_int), ("n_sources", C.c_int),
+                ("power_driven", C.c_int)]
 
 
 class Tune(C.Structure):
@@ -367,7 +369,9 @@ class Case:
                      EEDF=(EEDF_BINS + 1, np.uint64), AVE_SOURCE=(G, np.float64), AVE_EX=(G, np.float64),
                      AVE_EY=(G, np.float64),
                      SURFACE_CHARGE=(nsp * G if info.n_dielectric else 0, np.int64),
-                     SIGMA=(G if info.n_dielectric else 0, np.float64))
+                     SIGMA=(G if (info.n_dielectric or info.power_driven) else 0, np.float64),
+                     SOURCE_AC=(info.n_sources, np.float32),
+                     POWER_STATE=(POWER_STATE_BYTES if info.power_driven else 0, np.uint8))
         n, dt = sizes[name]
         out = np.zeros(n, dtype=dt)
         _check(lib().hp_get_grid(self.h, GRID[name], out.ctypes.data_as(_P), out.nbytes))

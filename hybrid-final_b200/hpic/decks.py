@@ -46,7 +46,8 @@ def _channel_keys(gas):
 def ccp_deck(ngx, ngy, xlen, ylen, *, gas="Ar", pressure_torr=0.05, voltage=100.0,
              freq=13.56e6, steps_per_cycle=400, ppc=50, density=1e15, te_ev=2.0,
              ti_ev=0.026, gas_k=300.0, max_np_factor=4, aro2_ratio=(80, 20),
-             ion_density=None, pcg_tol=1e-3, smoothing=0, load_type=0, load_pos=None, ratio=1):
+             ion_density=None, pcg_tol=1e-3, smoothing=0, load_type=0, load_pos=None, ratio=1,
+             power_w=0.0, pd_interval=5.0):
     """Build one CCP deck.
 
     ppc is the macro-particles per cell per species at `density`; np2c is
@@ -72,7 +73,7 @@ def ccp_deck(ngx, ngy, xlen, ylen, *, gas="Ar", pressure_torr=0.05, voltage=100.
         {"M_ID": 2, "X0": 0, "X1": ngx - 1, "Y0": ngy - 1, "Y1": ngy - 1, "Temp": gas_k,
          "R(Ohm)": 0.0, "L(H)": 0.0, "C(F)": 1.0},
     ]
-    src = [{"M_ID": 1, "DC(V)": 0, "Power(W)": 0, "AC(V)": voltage, "Freq(1/s)": freq,
+    src = [{"M_ID": 1, "DC(V)": 0, "Power(W)": power_w, "AC(V)": voltage, "Freq(1/s)": freq,
             "Phase(deg)": 0.0}]
     load = {"X0": 0.0, "X1": xlen, "Y0": 0.0, "Y1": ylen}
     gas_type = {"Ar": 0, "O2": 1, "ArO2": 2}[gas]
@@ -120,7 +121,7 @@ def ccp_deck(ngx, ngy, xlen, ylen, *, gas="Ar", pressure_torr=0.05, voltage=100.
             "AverageIter": steps_per_cycle, "DensitySmoothing": smoothing,
             "ParticleLimit": max_np, "ConstB_Flag": 0,
             "ContinuitySteadyState": {"Flag": 0, "Check": 1, "Margin": 1.0},
-            "PowerDrivenOption": {"Interval": 5.0, "VoltageUpDownRatio": 0.05},
+            "PowerDrivenOption": {"Interval": pd_interval, "VoltageUpDownRatio": 0.05},
             "SimulationStop": {"EndTime(s)": 1e-3,
                                "SteadyStatePrint": {"Flag": 0, "AveMargin(%)": 0.05, "SatGoal": 50}},
         },

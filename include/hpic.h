@@ -141,6 +141,8 @@ typedef struct hp_case_info {
     int mcc_stride;        /* collision counters per cell in HP_GRID_MCC_COUNT (8 Ar, 72 O2 and Ar/O2) */
     int n_smt;             /* 1-2-1 density smoothing passes per Deposit (the deck's DensitySmoothing) */
     int n_dielectric;      /* DielectricSpec blocks (surface charge kept when > 0) */
+    int n_sources;         /* Source entries */
+    int power_driven;      /* 1 when a conductor has a power-driven source (Power(W) != 0) */
 } hp_case_info;
 hp_status hp_case_get_info(const hp_case *c, hp_case_info *out);
 hp_status hp_setup_get_info(const hp_setup *s, hp_case_info *out);
@@ -236,8 +238,14 @@ typedef enum hp_grid_field {
     HP_GRID_SURFACE_CHARGE = 16, /* int64[nsp*Gsize] dielectric surface charge per species and node, in
                                     particle weights with HP_SIGMA_FRAC_BITS fraction bits (the reference's
                                     GPG.sigma); 0 bytes in a case without dielectric blocks */
-    HP_GRID_SIGMA = 17        /* double[Gsize] Sigma, the surface charge density SumSource sets at
-                                 dielectric nodes (src/cuda_Deposit.cu:35-104); 0 bytes without dielectrics */
+    HP_GRID_SIGMA = 17,       /* double[Gsize] Sigma (the reference's dev_Sigma): the surface charge density
+                                 SumSource sets at dielectric nodes (src/cuda_Deposit.cu:35-104) and
+                                 Cond_Sigma at conductor and Dirichlet face nodes (src/cuda_Field.cu:500-558);
+                                 0 bytes in a case with neither dielectrics nor power-driven sources */
+    HP_GRID_SOURCE_AC = 18,   /* float[number of sources] AC amplitudes in use (V): the deck's, as revised by
+                                 the power controller of power-driven sources */
+    HP_GRID_POWER_STATE = 19  /* the power controller's state (opaque bytes; 0 bytes without power-driven
+                                 sources), carried by checkpoints */
 } hp_grid_field;
 hp_status hp_get_grid(hp_case *c, hp_grid_field f, void *out, size_t bytes);
 hp_status hp_set_grid(hp_case *c, hp_grid_field f, const void *in, size_t bytes);
@@ -280,7 +288,10 @@ hp_status hp_case_slot_changes(hp_case *c, int64_t *changes);
  * 13 sigma-v max float[n], 14 node DensRegion int[Gsize], 15 MCC probabilities float[3*Gsize],
  * 16 cell eps_r float[Csize], 17 BackDen2 float[Gsize], 18 BackVel2 float[Gsize],
  * 39 SumSource node class int[Gsize] (0 none, 1 dielectric, 2 dielectric on a
- * domain edge: Sigma doubled, 3 conductor: surface charge cleared). */
+ * domain edge: Sigma doubled, 3 conductor: surface charge cleared),
+ * 40 power-driven sources float[2 + nsrc + 2*CondNUMR]: steps between
+ * revisions, VoltageUpDownRatio, target power per source, then per conductor
+ * its number of power-driven sources and the first one's index. */
 hp_status hp_get_table(hp_case *c, int what, void *out, size_t bytes, size_t *bytes_needed);
 hp_status hp_setup_get_table(const hp_setup *s, int what, void *out, size_t bytes, size_t *bytes_needed);
 

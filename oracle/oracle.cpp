@@ -90,7 +90,17 @@ struct SimBase {
     int pcg_iters[2] = {0, 0};
     std::vector<double> ave_den, ave_phi, ave_src, ave_ex, ave_ey;
     std::vector<long long> sig; // [nsp*G] dielectric surface weights, fixed point
-    std::vector<double> sigma;  // [G] Sigma where SumSource sets it
+    std::vector<double> sigma;  // [G] Sigma where SumSource or Cond_Sigma sets it
+    std::vector<float> src_amp; // AC amplitudes in use
+    std::vector<unsigned> cond_step; // [nsp*cond_numr] absorbed in this step
+    struct {
+        double surf[8], old[8], old2[8];
+        float power[8];
+        int count[8];
+        int power_init;
+    } pw{};
+    std::vector<int> cond_list; // nodes with a CondID, in node order
+    virtual void power(int64_t tstep) = 0;
     int64_t ave_count = 0;
     bool walk_bound_hit = false; // a walk that reached its crossing bound
     std::vector<unsigned long long> eedf = std::vector<unsigned long long>(201, 0ull);
@@ -155,6 +165,10 @@ template <class R> struct Sim : SimBase {
         ave_ey.assign(G, 0.0);
         sig.assign((size_t)c.nsp * G, 0);
         sigma.assign(G, 0.0);
+        src_amp.assign(c.src_ac, c.src_ac + c.src_num);
+        cond_step.assign((size_t)c.nsp * c.cond_numr, 0u);
+        for (int n = 0; n < G; n++)
+            if (c.cond_id[n]) cond_list.push_back(n);
     }
 
     // ------------------------------------------------------------ state
@@ -213,6 +227,7 @@ template <class R> struct Sim : SimBase {
             break;
         case 8: std::memcpy(out, sig.data(), sig.size() * 8); break;
         case 9: std::memcpy(d, sigma.data(), sigma.size() * 8); break;
+        case 10: std::memcpy(f, src_amp.data(), src_amp.size() * 4); break;
         }
     }
     void set_grid(int which, const void *in) override {
@@ -438,8 +453,10 @@ template <class R> struct Sim : SimBase {
                         const int r = walk(fi, fj, lx, ly, mvX, mvY, cond);
                         if (r) {
                             code = 15;
-                            if (cond >= 0 && cond < c.cond_numr) cond_charge[(size_t)s * c.cond_numr + cond] += 1.0f;
-                            else if (cond <= -2 && c.n_diel > 0) hits.push_back({s, fi, fj, -2 - cond, lx, ly, mvX, mvY});
+                            if (cond >= 0 && cond < c.cond_numr) {
+                                cond_charge[(size_t)s * c.cond_numr + cond] += 1.0f;
+                                if (c.n_power > 0) cond_step[(size_t)s * c.cond_numr + cond]++;
+                            } else if (cond <= -2 && c.n_diel > 0) hits.push_back({s, fi, fj, -2 - cond, lx, ly, mvX, mvY});
                             if (r == 2) walk_bound_hit = true;
                         } else {
                             const int ddi = fi - i, ddj = fj - j;
@@ -1594,7 +1611,7 @@ template <class R> struct Sim : SimBase {
                 for (int q = 0; q < c.src_num; q++)
                     if (c.src_mid[q] == k + 1)
                         v = (R)((double)v + ((double)c.src_dc[q] +
-                                             (double)c.src_ac[q] * std::sin((double)c.src_2pif[q] * time + (double)c.src_rphase[q])));
+                                             (double)src_amp[q] * std::sin((double)c.src_2pif[q] * time + (double)c.src_rphase[q])));
             vk[k] = v;
         }
         for (int n = 0; n < G; n++) {
@@ -1624,6 +1641,9 @@ template <class R> struct Sim : SimBase {
             const int f = c.face[n], b = c.boundary[n];
             R ex, ey;
             bool write = true;
+            // Cond_Sigma's Sigma at conductor and Dirichlet face nodes (the power controller's input)
+            if ((c.n_power > 0 || c.n_diel > 0) && (b == 3 || b == 1) && f != 8)
+                sigma[n] = (double)cond_sigma(n, eT, eL, eD, eX, pL, pR, pD, pU);
             if (f == 0) {
                 if (b == 3 || b == 2 || b == 1) {
                     ex = (R)-2.0f * cond_sigma(n, eT, eL, eD, eX, pL, pR, pD, pU) / (E(eL) + E(eX));
@@ -1696,6 +1716,56 @@ template <class R> struct Sim : SimBase {
                 ey = hdy * (P[pD] - P[pU]);
             }
             if (write) { Ex[n] = ex; Ey[n] = ey; }
+        }
+    }
+
+    // The reference's power controller (src/cuda_Diagnostic.cu:365-420) as
+    // the kernel computes it: surface charge per conductor in FP64, list entry
+    // q added to partial q % 256, the 256 partials reduced by halving.
+    void power(int64_t tstep) override {
+        if (c.n_power <= 0) return;
+        const int nc = c.cond_numr;
+        std::vector<double> part((size_t)256 * 8, 0.0);
+        for (size_t q = 0; q < cond_list.size(); q++) {
+            const int n = cond_list[q];
+            part[(q % 256) * 8 + (c.cond_id[n] - 1)] += sigma[n] * (double)c.area[n];
+        }
+        for (int h = 128; h > 0; h >>= 1)
+            for (int t = 0; t < h; t++)
+                for (int k = 0; k < nc; k++) part[(size_t)t * 8 + k] += part[(size_t)(t + h) * 8 + k];
+        const double time = (double)tstep * (double)c.dt;
+        for (int i = 0; i < nc; i++) {
+            pw.old2[i] = pw.old[i];
+            pw.old[i] = pw.surf[i];
+            pw.surf[i] = part[i];
+            float cond_current = 0.0f;
+            for (int s = 0; s < c.nsp; s++) {
+                unsigned &cnt = cond_step[(size_t)s * nc + i];
+                cond_current += c.q_density[s] * (float)cnt / c.dt;
+                cnt = 0;
+            }
+            const float dis_current = (float)(0.5 * (3.0 * pw.surf[i] - 4.0 * pw.old[i] + pw.old2[i]) / (double)c.dt);
+            const float current = dis_current - cond_current;
+            if (c.cond_src_num[i] != 1) continue;
+            float phi_now = 0.0f; // V_t: the conductor's voltage at this step (float, as the kernels)
+            if (c.efield_flag[i])
+                for (int q = 0; q < c.src_num; q++)
+                    if (c.src_mid[q] == i + 1)
+                        phi_now = (float)((double)phi_now + ((double)c.src_dc[q] +
+                                          (double)src_amp[q] * std::sin((double)c.src_2pif[q] * time + (double)c.src_rphase[q])));
+            pw.power[i] += phi_now * current;
+            pw.count[i]++;
+            if (pw.count[i] != c.pd_intv) continue;
+            pw.power[i] /= (float)pw.count[i];
+            pw.count[i] = 0;
+            const int q = c.cond_power_id[i];
+            if (pw.power[i] > 0) phi_now = src_amp[q] * hp_powf(std::fabs(c.src_power[q] / pw.power[i]), 0.2f);
+            if (pw.power_init) {
+                if (phi_now > (1.0f + c.pd_ratio) * src_amp[q]) src_amp[q] = (float)((double)src_amp[q] * 1.05);
+                else src_amp[q] = phi_now;
+            }
+            pw.power[i] = 0.0f;
+            pw.power_init++;
         }
     }
 
@@ -1800,6 +1870,7 @@ void or_run(or_sim *s, int64_t tstep0, int nsteps, int accumulate) {
             const int ev = s->impl->c.eedf_every;
             if (ev > 0 && t % ev == 0) s->impl->eedf_sample();
         }
+        s->impl->power(t);
     }
 }
 void or_get_eedf(or_sim *s, unsigned long long *h) { std::memcpy(h, s->impl->eedf.data(), 201 * 8); }

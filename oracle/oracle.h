@@ -69,6 +69,12 @@ typedef struct or_case {
     int n_diel;
     const int *sig_mode; /* [G] SumSource class: 0 none, 1 dielectric, 2 on a domain edge, 3 conductor */
     const float *area;   /* [G] node Area */
+    /* power-driven sources: present when n_power > 0 */
+    int n_power;
+    float src_power[8];
+    int cond_src_num[8], cond_power_id[8];
+    int pd_intv;
+    float pd_ratio;
 } or_case;
 
 typedef struct or_sim or_sim;
@@ -87,7 +93,8 @@ void or_get_movers(or_sim *s, int isp, int *counts, float *x, float *y, float *v
                    int8_t *codes);
 /* node fields: which 0 Ex, 1 Ey, 2 phi, 3 phi_pois (float[G]); 4 den (double[nsp*G]);
  * 5 source (double[G]); 6 b (double[G]); 7 x (double[G]);
- * 8 dielectric surface weights (int64[nsp*G], HP_SIGMA_FRAC_BITS fraction bits); 9 Sigma (double[G]) */
+ * 8 dielectric surface weights (int64[nsp*G], HP_SIGMA_FRAC_BITS fraction bits); 9 Sigma (double[G]);
+ * 10 AC amplitudes in use (float[src_num]) */
 void or_get_grid(or_sim *s, int which, void *out);
 void or_set_grid(or_sim *s, int which, const void *in);
 void or_get_counters(or_sim *s, float *cond_charge, unsigned *mcc_count, int *pcg_iters);

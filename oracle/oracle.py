@@ -45,6 +45,8 @@ class OrCase(C.Structure):
         ("back_den1", _F), ("back_den2", _F), ("back_vel2", _F), ("fluid_den", _F),
         ("n_smt", C.c_int), ("dens_region", _I),
         ("n_diel", C.c_int), ("sig_mode", _I), ("area", _F),
+        ("n_power", C.c_int), ("src_power", C.c_float * 8), ("cond_src_num", C.c_int * 8),
+        ("cond_power_id", C.c_int * 8), ("pd_intv", C.c_int), ("pd_ratio", C.c_float),
     ]
 
 
@@ -109,7 +111,7 @@ class Oracle:
     """CPU restatement of one case.  `tables` is a callable name -> array
     (hpic.Case.table or hpic.Setup.table); `info` the case info."""
 
-    GRID = dict(EX=0, EY=1, PHI=2, PHI_POIS=3, DEN=4, SOURCE=5, B=6, X=7, SURFACE_CHARGE=8, SIGMA=9)
+    GRID = dict(EX=0, EY=1, PHI=2, PHI_POIS=3, DEN=4, SOURCE=5, B=6, X=7, SURFACE_CHARGE=8, SIGMA=9, SOURCE_AC=10)
 
     def __init__(self, tables, info, opts, precision=32, pcg_cluster=1, pcg_block=512, field_mode=None,
                  fs_passes=None):
@@ -170,6 +172,15 @@ class Oracle:
         c.n_diel = info.n_dielectric
         c.sig_mode = keep("sgm", t("sig_mode"), np.int32)
         c.area = keep("area", t("area"), np.float32)
+        c.n_power = info.power_driven
+        pw = t("power")
+        c.pd_intv, c.pd_ratio = int(pw[0]), pw[1]
+        nsrc = info.n_sources
+        for k in range(nsrc):
+            c.src_power[k] = pw[2 + k]
+        for k in range(info.cond_numr):
+            c.cond_src_num[k] = int(pw[2 + nsrc + 2 * k])
+            c.cond_power_id[k] = int(pw[3 + nsrc + 2 * k])
         c.prob = keep("prob", t("prob"), np.float32)
         c.back_vel1 = keep("bv1", t("back_vel1"), np.float32)
         c.vsave = keep("vsave", t("vsave"), np.float32)
@@ -268,6 +279,8 @@ class Oracle:
             out = np.zeros(nsp * G, np.float64)
         elif w == 8:
             out = np.zeros(nsp * G, np.int64)
+        elif w == 10:
+            out = np.zeros(max(1, self.info.n_sources), np.float32)
         else:
             out = np.zeros(G, np.float64)
         lib().or_get_grid(self.h, w, out.ctypes.data_as(C.c_void_p))

@@ -30,10 +30,11 @@ DECKS = {
     "aro2": (ccp_deck(33, 17, 0.01, 0.005, gas="ArO2", ppc=20, pressure_torr=0.1, voltage=200.0, te_ev=3.0,
                       ion_density={"Ar+": 1e15, "O2+": 2e14, "O+": 0.0, "O-": 2e14}), 4242),
     "diel": (dielectric_deck(), 4343),
+    "power": (ccp_deck(33, 17, 0.01, 0.005, ppc=20, power_w=0.5, pd_interval=0.02), 56),
 }
 CAP = {"diel": 256}
 GRIDS = ("EX", "EY", "PHI", "PHI_POIS", "DEN", "SOURCE", "PCG_X", "PCG_B", "AVE_DEN", "AVE_PHI", "AVE_SOURCE",
-         "AVE_EX", "AVE_EY", "MCC_COUNT", "EEDF", "SURFACE_CHARGE", "SIGMA")
+         "AVE_EX", "AVE_EY", "MCC_COUNT", "EEDF", "SURFACE_CHARGE", "SIGMA", "SOURCE_AC", "POWER_STATE")
 
 
 def read_v000_head(path, nsp):

@@ -34,6 +34,8 @@ DECKS = {
     "ar_33x17_smooth2": (ccp_deck(33, 17, 0.01, 0.005, ppc=20, pressure_torr=0.1, voltage=300.0, smoothing=2), 778),
     # a dielectric slab on the driven electrode and a dielectric block inside
     "ar_diel_33x21": (dielectric_deck(), 4343),
+    # a power-driven source (0.5 W), its amplitude revised every 20 steps
+    "ar_33x17_power": (ccp_deck(33, 17, 0.01, 0.005, ppc=20, power_w=0.5, pd_interval=0.05), 55),
 }
 # slots per cell where the deck's Max_np / Gsize leaves too little room for
 # the charge that gathers in front of the floating block
@@ -441,4 +443,25 @@ def test_far_bucket_beyond_one_warp():
     case.SortBoundary()
     o.SortBoundary()
     check_particles(case, o, "after a sort with full far buckets")
+    assert case.status() == 0
+
+
+@pytest.mark.parametrize("mode", [1, 2])
+def test_power_controller_bit_exact(mode):
+    """A power-driven source over 65 steps (revisions at steps 20, 40, 60;
+    the first arms the controller): amplitudes, particles and fields as the
+    oracle's."""
+    case, o = pair("ar_33x17_power", field_mode=mode, move_mode=1)
+    assert case.info.power_driven == 1
+    a0 = case.grid("SOURCE_AC").copy()
+    n = 65
+    case.step(n)
+    o.run(0, n, accumulate=True)
+    amp = case.grid("SOURCE_AC")
+    assert same(amp, o.grid("SOURCE_AC")[: amp.size])
+    assert amp[0] != a0[0], "the controller revised nothing"
+    check_particles(case, o, f"after {n} power-driven steps")
+    for g in ("PHI", "EX", "EY"):
+        assert same(case.grid(g), o.grid(g)), g
+    assert same(case.grid("SIGMA"), o.grid("SIGMA"))
     assert case.status() == 0
