@@ -144,6 +144,7 @@ void fill_info(const Setup &s, hp_case_info *out) {
     out->n_dielectric = s.diel_num;
     out->n_sources = s.src_num;
     out->power_driven = s.power_driven() ? 1 : 0;
+    out->n_reactions = s.TnRct;
 }
 
 // Collision probability per cell from its lower-left node
@@ -1062,6 +1063,46 @@ hp_status hp_reset_averages(hp_case *c) {
     CK(cudaMemset(c->h.ave_ey, 0, (size_t)c->s.Gsize * 8));
     CK(cudaMemset(c->h.ave_count, 0, 8));
     CK(cudaMemset(c->h.eedf, 0, (HP_EEDF_BINS + 1) * 8));
+    c->mcc_base.resize((size_t)c->h.mcc_stride * c->s.Csize);
+    CK(cudaMemcpy(c->mcc_base.data(), c->h.mcc_count, c->mcc_base.size() * 4, cudaMemcpyDeviceToHost));
+    return HP_OK;
+}
+
+// The reference's averaged collision rates (Average_Argon/Oxygen/ArO2_MCC_rate,
+// src/cuda_Diagnostic.cu:548-632): per node (the lower-left node of the cell
+// the collision happened in) and reaction channel, the collisions since
+// hp_reset_averages times Denscale of the channel's projectile species over
+// (steps accumulated x dt), in the reference's float arithmetic.  Channels
+// without a tally here (Ar 7-8, Ar/O2 68 and 71 on) are 0.
+hp_status hp_get_mcc_rates(hp_case *c, float *out, size_t count) {
+    if (!c || !out) return HP_ERR_ARG;
+    const Setup &s = c->s;
+    const int T = s.TnRct, G = s.Gsize, C = s.Csize, st = c->h.mcc_stride;
+    if (count < (size_t)G * T) return set_error("output buffer too small (Gsize x TnRct floats)"), HP_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->last_stream));
+    std::vector<uint32_t> now((size_t)st * C);
+    int64_t n = 0;
+    CK(cudaMemcpy(now.data(), c->h.mcc_count, now.size() * 4, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&n, c->h.ave_count, 8, cudaMemcpyDeviceToHost));
+    std::fill(out, out + (size_t)G * T, 0.0f);
+    if (n <= 0) return HP_OK;
+    // projectile species of each channel (the reference's scaling ranges)
+    std::vector<int> proj(T, -1);
+    auto range = [&](int a, int b, int sp) { for (int k = a; k <= b && k < T; k++) proj[k] = sp; };
+    if (s.main_gas == GAS_AR) range(0, 6, 0);
+    else if (s.main_gas == GAS_O2) { range(0, 40, 0); range(41, 46, 3); range(47, 52, 1); range(53, 57, 2); range(58, 58, 3); }
+    else { range(0, 45, 0); range(46, 51, 4); range(52, 59, 2); range(60, 64, 3); range(65, 67, 1); range(69, 70, 3); }
+    for (int k = 0; k < T && k < st; k++) {
+        if (proj[k] < 0) continue;
+        const float temp = s.sp[proj[k]].Denscale / (float)n / s.dt;
+        for (int cell = 0; cell < C; cell++) {
+            const size_t q = (size_t)cell * st + k;
+            const uint32_t cnt = now[q] - (c->mcc_base.empty() ? 0u : c->mcc_base[q]);
+            const int i = cell / s.ncy, j = cell - i * s.ncy;
+            out[(size_t)(i * s.ngy + j) * T + k] = temp * (float)cnt;
+        }
+    }
     return HP_OK;
 }
 

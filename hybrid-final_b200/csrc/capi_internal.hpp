@@ -50,6 +50,7 @@ struct hp_case {
     int graph_kernels = 0; // kernel nodes in the captured step
     hp_batch *batch = nullptr;
     std::vector<float> prob; // [3*C]
+    std::vector<uint32_t> mcc_base; // collision tallies at the last hp_reset_averages (empty: zeros)
 };
 
 extern "C" hp_status hpi_grid_ptr(hp_case *c, hp_grid_field f, void **p, size_t *nb);

@@ -57,7 +57,7 @@ class CaseInfo(C.Structure):
                 ("dx", C.c_double), ("dy", C.c_double), ("tstep", C.c_int64), ("device_bytes", C.c_size_t),
                 ("pcg_cluster", C.c_int), ("pcg_block", C.c_int), ("field_mode", C.c_int), ("mcc_stride", C.c_int),
                 ("n_smt", C.c_int), ("n_dielectric", C.c_int), ("n_sources", C.c_int),
-                ("power_driven", C.c_int)]
+                ("power_driven", C.c_int), ("n_reactions", C.c_int)]
 
 
 class Tune(C.Structure):
@@ -118,6 +118,7 @@ _SIGS = {
     "hp_get_grid": (C.c_int, [_P, C.c_int, _P, C.c_size_t]),
     "hp_set_grid": (C.c_int, [_P, C.c_int, _P, C.c_size_t]),
     "hp_reset_averages": (C.c_int, [_P]),
+    "hp_get_mcc_rates": (C.c_int, [_P, C.POINTER(C.c_float), C.c_size_t]),
     "hp_get_average_count": (C.c_int, [_P, C.POINTER(C.c_int64)]),
     "hp_last_pcg_iters": (C.c_int, [_P, _I, _I]),
     "hp_last_field_residual": (C.c_int, [_P, C.POINTER(C.c_double)]),
@@ -383,6 +384,13 @@ class Case:
 
     def reset_averages(self):
         _check(lib().hp_reset_averages(self.h))
+
+    def mcc_rates(self):
+        """Averaged collision rates [Gsize, TnRct] (the reference's ave_MCC_rate)."""
+        info = self.info
+        out = np.zeros(info.Gsize * info.n_reactions, np.float32)
+        _check(lib().hp_get_mcc_rates(self.h, out.ctypes.data_as(C.POINTER(C.c_float)), out.size))
+        return out.reshape(info.Gsize, info.n_reactions)
 
     def average_count(self):
         n = C.c_int64(0)

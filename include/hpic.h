@@ -143,6 +143,7 @@ typedef struct hp_case_info {
     int n_dielectric;      /* DielectricSpec blocks (surface charge kept when > 0) */
     int n_sources;         /* Source entries */
     int power_driven;      /* 1 when a conductor has a power-driven source (Power(W) != 0) */
+    int n_reactions;       /* TnRct: reaction channels of the gas's collision set */
 } hp_case_info;
 hp_status hp_case_get_info(const hp_case *c, hp_case_info *out);
 hp_status hp_setup_get_info(const hp_setup *s, hp_case_info *out);
@@ -252,6 +253,13 @@ hp_status hp_set_grid(hp_case *c, hp_grid_field f, const void *in, size_t bytes)
 /* Running averages (N_ave accumulation, src/cuda_Diagnostic.cu:505-547):
  * the sums above and the number of accumulated steps. */
 hp_status hp_reset_averages(hp_case *c);
+/* Averaged collision rates as the reference's ave_MCC_rate
+ * (src/cuda_Diagnostic.cu:548-632): out[node * TnRct + channel], collisions
+ * per m^3 and s since hp_reset_averages (Denscale of the projectile over
+ * steps x dt), at the lower-left node of the cell they happened in.  `count`
+ * is the capacity of out in floats (Gsize x TnRct; TnRct = hp_case_info
+ * .n_reactions). */
+hp_status hp_get_mcc_rates(hp_case *c, float *out, size_t count);
 
 /* ------------------------------------------------------------ checkpoint */
 /* Checkpoint of a case: the reference's V000 dump (V000_DUMP,

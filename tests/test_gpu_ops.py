@@ -465,3 +465,29 @@ def test_power_controller_bit_exact(mode):
         assert same(case.grid(g), o.grid(g)), g
     assert same(case.grid("SIGMA"), o.grid("SIGMA"))
     assert case.status() == 0
+
+
+def test_mcc_rates_since_reset():
+    """hp_get_mcc_rates: the collisions tallied since hp_reset_averages per
+    cell and channel, at the cell's lower-left node, times Denscale / (steps
+    x dt) in float as the reference's Average_Argon_MCC_rate."""
+    case, _ = pair("ar_33x17_hv", field_mode=2, move_mode=1)
+    info = case.info
+    case.step(10)
+    c0 = case.grid("MCC_COUNT").reshape(info.Csize, info.mcc_stride).astype(np.int64)
+    case.reset_averages()
+    case.step(15)
+    c1 = case.grid("MCC_COUNT").reshape(info.Csize, info.mcc_stride).astype(np.int64)
+    r = case.mcc_rates()
+    assert r.shape == (info.Gsize, info.n_reactions)
+    S = hpic.Setup(DECKS["ar_33x17_hv"][0], seed=DECKS["ar_33x17_hv"][1])
+    denscale = np.float32(S.table("species").reshape(-1, 16)[0, 8])
+    dt = np.float32(S.table("scalars")[0])
+    temp = denscale / np.float32(15) / dt
+    want = np.zeros_like(r)
+    cells = np.arange(info.Csize)
+    nodes = (cells // info.ncy) * info.ngy + cells % info.ncy
+    for k in range(7):
+        want[nodes, k] = temp * (c1 - c0)[:, k].astype(np.float32)
+    assert np.array_equal(r, want)
+    assert r.sum() > 0
