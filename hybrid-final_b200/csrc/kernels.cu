@@ -701,7 +701,10 @@ __device__ __forceinline__ void sort_push_cell(const DevCase &d, int s, int c, i
 #ifndef SORT_G
 #define SORT_G 1
 #endif
-__global__ void __launch_bounds__(SORT_MAXW * 32, 2) k_sort_push(const DevCase *__restrict__ cases,
+#ifndef SORT_MINB
+#define SORT_MINB 2 // resident blocks per SM the register budget is set for
+#endif
+__global__ void __launch_bounds__(SORT_MAXW * 32, SORT_MINB) k_sort_push(const DevCase *__restrict__ cases,
                                                            const int *__restrict__ item_start, int ncases, int items) {
     __shared__ int s_off[SORT_MAXW][9], s_lim[SORT_MAXW][9];
     const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
