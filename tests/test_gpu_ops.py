@@ -491,3 +491,34 @@ def test_mcc_rates_since_reset():
         want[nodes, k] = temp * (c1 - c0)[:, k].astype(np.float32)
     assert np.array_equal(r, want)
     assert r.sum() > 0
+
+
+def test_batch_with_dielectric_and_power_cases_equals_alone():
+    """Dielectric and power-driven cases inside a batch with a plain one:
+    each ends with the same bits as alone (the Sort-phase surface pass and
+    the power controller run one block per case of the batch)."""
+    decks = [DECKS["ar_diel_33x21"], DECKS["ar_33x17_power"], DECKS["ar_17x9"]]
+    kw = [dict(cap_per_cell=CAP["ar_diel_33x21"]), {}, {}]
+    opts = dict(field_mode=1, move_mode=1)
+    n = 45  # power revisions at steps 20 and 40
+    alone = []
+    for (deck, seed), k in zip(decks, kw):
+        c = hpic.Case(deck, seed=seed, **opts, **k)
+        c.step(n)
+        alone.append(c)
+    mixed = [hpic.Case(deck, seed=seed, **opts, **k) for (deck, seed), k in zip(decks, kw)]
+    b = hpic.Batch(mixed)
+    b.step(n)
+    b.close()
+    for a, m in zip(alone, mixed):
+        for s in range(a.info.nsp):
+            ca, pa = a.particles(s)
+            cm, pm = m.particles(s)
+            assert np.array_equal(ca, cm)
+            for x, y in zip(pa, pm):
+                assert same(x, y)
+        for g in ("PHI", "SURFACE_CHARGE", "SIGMA", "SOURCE_AC"):
+            assert np.array_equal(a.grid(g).view(np.uint8), m.grid(g).view(np.uint8)), g
+        assert a.status() == m.status() == 0
+    assert alone[0].grid("SURFACE_CHARGE").sum() > 0
+    assert alone[1].grid("SOURCE_AC")[0] != np.float32(100.0)
