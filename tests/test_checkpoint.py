@@ -111,3 +111,25 @@ def test_load_refuses_another_grid(tmp_path):
     with pytest.raises(hpic.HpicError):
         other.load(path)
     assert other.tstep() == t0  # nothing was changed
+
+
+def test_v000_sigma_is_the_dielectric_surface_charge(tmp_path):
+    """The V000 per-(species, node) records (den, ave_den, sigma) carry the
+    dielectric surface charge as the reference's float GPG.sigma."""
+    deck, seed = DECKS["diel"]
+    c = hpic.Case(deck, seed=seed, field_mode=1, move_mode=1, cap_per_cell=CAP["diel"])
+    c.step(12)
+    path = tmp_path / "diel.dump"
+    c.save(path)
+    info = c.info
+    t, tstep, cstep, gas, sp = read_v000_head(path, info.nsp)
+    off = 20 + sum(8 + 24 * rec.size for _, rec in sp)
+    ncx, ncy, ngx, ngy, G = info.ncx, info.ncy, info.ngx, info.ngy, info.Gsize
+    nfsp = 1  # the Ar set carries one fluid species (Ar*)
+    off += 4 + nfsp * 4 * (2 * ncx * ncy + ngx * ncy + ncx * ngy)  # Conti_Flag, fluid arrays
+    off += 3 * 4  # history counters
+    raw = np.fromfile(path, dtype="<f4", count=3 * info.nsp * G, offset=off).reshape(info.nsp * G, 3)
+    want = (c.grid("SURFACE_CHARGE").astype(np.float64) / 2.0 ** hpic.SIGMA_FRAC_BITS).astype(np.float32)
+    assert want.sum() > 0
+    assert same(raw[:, 2].copy(), want)
+    assert same(raw[:, 0].copy(), c.grid("DEN").astype(np.float32))
