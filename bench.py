@@ -489,6 +489,8 @@ def run_served(args):
     pushes = sum(r.particle_pushes for r, _, _ in results)
     errors = sum(1 for r, _, _ in results if r.error)
     status_nonzero = sum(1 for r, _, _ in results if r.error == 0 and r.status)
+    status_bits = {f"0x{b:x}": int(sum(1 for r, _, _ in results if r.error == 0 and r.status & b))
+                   for b in (1, 2, 4, 8, 16, 32)}
     # the same stream, one case at a time on the plain path (set-up included)
     t_start = time.perf_counter()
     plain_lat, plain_pushes = [], 0
@@ -514,7 +516,7 @@ def run_served(args):
                             slots=args.slots, steps_per_launch=args.steps_per_launch, budget_gb=args.budget_gb,
                             gas="Ar or 80/20 Ar/O2", particle_load="host" if args.host_load else "device"),
                 latency_s=dict(p50=pct(lat, 50), p99=pct(lat, 99)), errors=errors,
-                device_status_nonzero=status_nonzero, wall_s=t_end,
+                device_status_nonzero=status_nonzero, device_status_bits=status_bits, wall_s=t_end,
                 plain=dict(value=plain_pushes / plain_end, latency_s=dict(p50=pct(plain_lat, 50),
                                                                           p99=pct(plain_lat, 99)),
                            wall_s=plain_end, served_over_plain=value / (plain_pushes / plain_end)))
