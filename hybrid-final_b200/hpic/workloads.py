@@ -23,7 +23,7 @@ GRIDS = {  # nodes -> domain size (m): the cell stays 312.5 um
 }
 
 
-def _case(rng, grids, ppc_range, gas="Ar"):
+def _case(rng, grids, ppc_range, gas="Ar", max_np_factor=8):
     g = grids[rng.integers(len(grids))]
     xlen, ylen = GRIDS[g]
     p_torr = float(np.exp(rng.uniform(np.log(0.010), np.log(0.200))))
@@ -34,8 +34,10 @@ def _case(rng, grids, ppc_range, gas="Ar"):
         extra = dict(gas="ArO2", aro2_ratio=(80, 20), te_ev=3.0,
                      ion_density={"Ar+": 1e15, "O2+": 2e14, "O+": 0.0, "O-": 2e14})
     # 8x the initial count per cell: small, strongly driven cases compress the
-    # plasma well beyond the load density in their first steps
-    deck = ccp_deck(g[0], g[1], xlen, ylen, ppc=ppc, voltage=volts, pressure_torr=p_torr, max_np_factor=8, **extra)
+    # plasma well beyond the load density in their first steps (16x for the
+    # served stream, whose requests run up to 10 RF periods)
+    deck = ccp_deck(g[0], g[1], xlen, ylen, ppc=ppc, voltage=volts, pressure_torr=p_torr,
+                    max_np_factor=max_np_factor, **extra)
     desc = dict(nodes=f"{g[0]}x{g[1]}", gas=gas, pressure_torr=round(p_torr, 5), voltage=round(volts, 2), ppc=ppc)
     return deck, desc
 
@@ -61,7 +63,7 @@ def served_stream(n=512, rate_per_s=4.0, seed=7, steps_per_cycle=400, cycles=(1,
     for k in range(n):
         t += float(rng.exponential(1.0 / rate_per_s))
         gas = "ArO2" if rng.random() < 0.5 else "Ar"
-        deck, desc = _case(rng, grids, (50, 200), gas=gas)
+        deck, desc = _case(rng, grids, (50, 200), gas=gas, max_np_factor=16)
         ncyc = int(rng.integers(cycles[0], cycles[1] + 1))
         desc["rf_periods"] = ncyc
         out.append((t, deck, ncyc * steps_per_cycle, int(rng.integers(1, 2 ** 31 - 2)), desc))
