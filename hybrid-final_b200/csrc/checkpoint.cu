@@ -62,6 +62,8 @@ struct File {
 };
 
 const char MAGIC[8] = {'H', 'P', 'I', 'C', 'X', '0', '0', '2'};
+// the extension's format version; the magic's last digits carry the same number
+constexpr uint32_t EXT_VERSION = 2u;
 const char TAIL[8] = {'H', 'P', 'I', 'C', 'E', 'N', 'D', '1'};
 // grid fields carried by the extension, in file order
 const hp_grid_field EXT_GRIDS[] = {HP_GRID_EX,         HP_GRID_EY,          HP_GRID_PHI,     HP_GRID_PHI_POIS,
@@ -251,7 +253,7 @@ hp_status hp_case_save(hp_case *c, const char *path) {
     if (st != HP_OK) return st;
     // extension
     F.put(MAGIC, 8);
-    F.put1<uint32_t>(1u);
+    F.put1<uint32_t>(EXT_VERSION);
     F.put1<int32_t>(s.nsp);
     F.put1<int32_t>(s.Gsize);
     F.put1<int32_t>(s.Csize);
@@ -307,10 +309,11 @@ hp_status hp_case_load(hp_case *c, const char *path) {
     if (fseek(F.f, (long)v000_bytes(s, np), SEEK_SET) != 0) return bad("truncated");
     char magic[8];
     F.get(magic, 8);
-    if (!F.ok || std::memcmp(magic, MAGIC, 8) != 0) return bad("no HPICX001 extension after the V000 part");
+    if (!F.ok || std::memcmp(magic, MAGIC, 8) != 0)
+        return bad("no " + std::string(MAGIC, 8) + " extension after the V000 part");
     const uint32_t ver = F.get1<uint32_t>();
     const int32_t nsp = F.get1<int32_t>(), G = F.get1<int32_t>(), C = F.get1<int32_t>(), fm = F.get1<int32_t>();
-    if (!F.ok || ver != 1u) return bad("unknown extension version");
+    if (!F.ok || ver != EXT_VERSION) return bad("unknown extension version");
     if (nsp != s.nsp || G != s.Gsize || C != s.Csize) return bad("grid or species do not match the case");
     if (fm != c->opts.field_mode) return bad("field_mode differs from the case's");
     const int64_t tstep = F.get1<int64_t>();
@@ -324,6 +327,13 @@ hp_status hp_case_load(hp_case *c, const char *path) {
         if (!F.ok || n < 0 || n != np[(size_t)isp]) return bad("particle counts differ between the two parts");
         P.cnt.resize((size_t)C);
         F.get(P.cnt.data(), (size_t)C * 4);
+        if (!F.ok) return bad("truncated particles");
+        int64_t total = 0;
+        for (int32_t k : P.cnt) {
+            if (k < 0) return bad("negative cell count");
+            total += k;
+        }
+        if (total != n) return bad("cell counts do not sum to the particle count");
         for (int a = 0; a < 5; a++) {
             P.a[a].resize(n ? (size_t)n : 1);
             F.get(P.a[a].data(), (size_t)n * 4);

@@ -73,10 +73,29 @@ __global__ void __launch_bounds__(256) k_na_nodes(const hp::DevCase *__restrict_
     }
 }
 
+// Makes the case's device current for the call and puts the caller's back.
+struct DeviceGuard {
+    int prev = -1;
+    cudaError_t set(int dev) {
+        cudaError_t e = cudaGetDevice(&prev);
+        if (e != cudaSuccess) {
+            prev = -1;
+            return e;
+        }
+        return prev == dev ? cudaSuccess : cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        if (prev >= 0) cudaSetDevice(prev);
+    }
+};
+
 } // namespace
 
 extern "C" hp_status hp_Deposit_noalloc(hp_case *c, double *den_out, void *stream) {
     if (!c || !den_out) return hpi::set_error("null argument"), HP_ERR_ARG;
+    // a batched case is stepped on the batch's stream; reading its pools here
+    // would not be ordered after that step
+    if (c->batch) return hpi::set_error("case belongs to a batch"), HP_ERR_ARG;
     if (c->s.N_smt > 0)
         return hpi::set_error("hp_Deposit_noalloc: the deck smooths its densities (DensitySmoothing); use hp_Deposit"),
                HP_ERR_UNSUPPORTED;
@@ -87,22 +106,32 @@ extern "C" hp_status hp_Deposit_noalloc(hp_case *c, double *den_out, void *strea
         return HP_ERR_CAPACITY;
     }
     if (c->device < 0 || c->device >= kMaxDevices) return hpi::set_error("device ordinal too large"), HP_ERR_ARG;
-    cudaError_t e = cudaSetDevice(c->device);
+    DeviceGuard guard;
+    cudaError_t e = guard.set(c->device);
     if (e != cudaSuccess) return hpi::cuda_fail(e, "cudaSetDevice");
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(st, &cap);
+    if (e != cudaSuccess) return hpi::cuda_fail(e, "cudaStreamIsCapturing");
     double4 *scratch;
     {
-        // once per device, with that device current: the device address of
-        // the scratch array (its host-side name is not a device address)
+        // The device address of the scratch array (its host-side name is not
+        // a device address), looked up with the case's device current.  It is
+        // looked up again on every call outside stream capture, so a context
+        // that was torn down and recreated (cudaDeviceReset) is followed; a
+        // call under capture uses the address of the last call outside it.
         std::lock_guard<std::mutex> lk(g_mu);
-        if (!g_scratch_ptr[c->device]) {
+        if (cap == cudaStreamCaptureStatusNone) {
             void *p = nullptr;
             e = cudaGetSymbolAddress(&p, g_corner_scratch);
             if (e != cudaSuccess) return hpi::cuda_fail(e, "cudaGetSymbolAddress (deposit scratch)");
             g_scratch_ptr[c->device] = (double4 *)p;
+        } else if (!g_scratch_ptr[c->device]) {
+            return hpi::set_error("hp_Deposit_noalloc: the first call on a device must come before any stream capture"),
+                   HP_ERR_ARG;
         }
         scratch = g_scratch_ptr[c->device];
     }
-    cudaStream_t st = (cudaStream_t)stream;
     const long long threads = need * 32;
     k_na_cells<<<(unsigned)((threads + 255) / 256), 256, 0, st>>>(c->d_case, scratch);
     e = cudaGetLastError();

@@ -2,8 +2,9 @@
 # Regenerate xsec_*.txt from the reference's own table builder
 # (src/PhysicsData.c).  Development-time only: needs the reference tree.
 set -e
-REF=${REF:-/root/reference}
 HERE=$(cd "$(dirname "$0")" && pwd)
+# the reference tree: $REF, by default the directory `reference` beside this repository
+REF=${REF:-$(cd "$HERE/../../.." && pwd)/reference}
 TMP=$(mktemp -d)
 gcc -c -O1 -w -I"$REF/inc" "$REF/src/PhysicsData.c" -o "$TMP/PhysicsData.o"
 nvcc -c -w -Wno-deprecated-gpu-targets -I"$REF/inc" "$REF/src/Variables.cu" -o "$TMP/Variables.o"

@@ -183,11 +183,14 @@ hp_status hp_Deposit(hp_case *c, void *stream);
  * case's own density, source and right-hand side untouched.  Its per-cell
  * scratch is one fixed array inside the library, 2^19 (species x cells)
  * entries (16 MiB), held on every GPU that loads the library until the
- * process exits; larger cases get HP_ERR_CAPACITY.  The first call on a
- * device looks up that array's device address, so make it before any stream
- * capture.  All calls share the one array: calls whose work overlaps on the
- * GPU (other streams, other host threads) race and must be ordered by the
- * caller.  Every scratch entry a call reads it has written first. */
+ * process exits; larger cases get HP_ERR_CAPACITY, and a case that belongs
+ * to a batch gets HP_ERR_ARG (the batch steps it on its own stream).  Each
+ * call outside stream capture looks up that array's device address with the
+ * case's device current (and puts the caller's current device back), so the
+ * first call on a device must come before any stream capture.  All calls
+ * share the one array: calls whose work overlaps on the GPU (other streams,
+ * other host threads) race and must be ordered by the caller.  Every scratch
+ * entry a call reads it has written first. */
 hp_status hp_Deposit_noalloc(hp_case *c, double *den_out, void *stream);
 /* n steps of the main loop body (src/cuda_main.cu:114-183 without the
  * diagnostics and dump calls), fused where results allow; replayed from a

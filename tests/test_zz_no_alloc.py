@@ -44,6 +44,21 @@ def test_noalloc_deposit_matches_deposit_twice():
     assert np.array_equal(noalloc_density(small).view(np.uint64), small.grid("DEN").view(np.uint64))
 
 
+def test_noalloc_rejects_batched_cases_and_keeps_the_current_device():
+    import torch
+    cases = [hpic.Case(ccp_deck(17, 9, 0.005, 0.0025, ppc=8), seed=s) for s in (3, 4)]
+    batch = hpic.Batch(cases)
+    with pytest.raises(hpic.HpicError) as e:
+        hpic._check(hpic.lib().hp_Deposit_noalloc(cases[0].h, C.c_void_p(1), None))
+    assert e.value.status == hpic.HP_ERR_ARG
+    batch.close()
+    dev = torch.cuda.current_device()
+    alone = hpic.Case(ccp_deck(17, 9, 0.005, 0.0025, ppc=8), seed=6)
+    alone.Deposit()
+    noalloc_density(alone)
+    assert torch.cuda.current_device() == dev
+
+
 def test_noalloc_rejects_cases_beyond_the_scratch():
     # 1027 x 257 nodes: 2 x 1026 x 256 = 525312 (species x cells) > 2^19; the
     # check runs before any device work, so a light load is enough
