@@ -17,6 +17,7 @@
 #include <vector>
 
 #include <algorithm>
+#include <atomic>
 #include <array>
 #include <thread>
 
@@ -100,6 +101,34 @@ struct SimBase {
         int power_init;
     } pw{};
     std::vector<int> cond_list; // nodes with a CondID, in node order
+    // Scripted uniforms, for pinning against the reference's own MCC code:
+    // when on, every MCC draw (null-collision tests included) is taken in
+    // order from a per-key list instead of Philox; key = cell, or species *
+    // Csize + cell with by_species.  The reference's kernels, fed the same
+    // lists through their curand_uniform calls (one thread per key), then
+    // see the same numbers in the same order.  A list that runs out yields
+    // 1.0 (no collision) and counts an overrun.
+    struct Script {
+        bool on = false;
+        int by_species = 0;
+        int pair_rl = 0; // kinematics calls (PAIR_* bits) whose two draws are taken right to left
+        std::vector<float> u;
+        std::vector<int64_t> start, pos;
+    } script;
+    std::atomic<long long> script_overrun{0};
+    float u_script(uint32_t species, uint32_t cell) {
+        const size_t key = script.by_species ? (size_t)species * (size_t)C + cell : cell;
+        if (key + 1 >= script.start.size()) {
+            script_overrun++;
+            return 1.0f;
+        }
+        int64_t &p = script.pos[key];
+        if (script.start[key] + p >= script.start[key + 1]) {
+            script_overrun++;
+            return 1.0f;
+        }
+        return script.u[(size_t)(script.start[key] + p++)];
+    }
     virtual void power(int64_t tstep) = 0;
     int64_t ave_count = 0;
     bool walk_bound_hit = false; // a walk that reached its crossing bound
@@ -122,6 +151,10 @@ struct SimBase {
     virtual void deposit(bool smooth) = 0;
     virtual void accumulate() = 0;
     virtual int far_max() const = 0;
+    virtual void xsec_n(int ch, const float *engy, float *out, int n) const = 0;
+    virtual void kinematics(int kind, const float *in, float *out, int n) const = 0;
+    virtual int collide_oxy(int isp, int t, const float *v, float bv1, float bv2, const float *u, int nu, int pair_rl,
+                            int *ch, int *keep, float *vout, int *bsp, float *bv, int *kill) = 0;
 };
 
 template <class R> struct Sim : SimBase {
@@ -537,6 +570,43 @@ template <class R> struct Sim : SimBase {
         }
     }
 
+    // ------------------------------------------------------------ MCC draws
+    // the null-collision test draw and a particle stream's next draw, or the
+    // scripted list of the same (species, cell)
+    float u_test(uint32_t slot, int cell, uint32_t step, uint32_t species, uint32_t sub) {
+        return script.on ? u_script(species, (uint32_t)cell)
+                         : hp_test_draw(c.seed, slot, (uint32_t)cell, step, species, sub);
+    }
+    float nextu(hp_stream &rs) { return script.on ? u_script(rs.ctr.w >> 16, rs.ctr.y) : hp_stream_next(&rs); }
+    // one collider's own list (single-collision entry points)
+    struct ListStream {
+        const float *u;
+        int n, pos;
+        bool overrun;
+        int pair_rl;
+    };
+    static float nextu(ListStream &ls) {
+        if (ls.pos >= ls.n) {
+            ls.overrun = true;
+            return 1.0f;
+        }
+        return ls.u[ls.pos++];
+    }
+    // The two uniforms a collision passes to one kinematics call
+    // (anewvel, maxwellv, newvel_ionsc).  C++ leaves the order in which the
+    // reference's two curand_uniform() arguments are evaluated open; the
+    // Philox streams take the left one first, and a scripted list can be
+    // read right to left for the calls whose bit (PAIR_*) is set in the
+    // script's pair mask, as the reference's nvcc build evaluates them.
+    enum { PAIR_ANEWVEL = 1, PAIR_MAXWELLV = 2, PAIR_IONSC = 4 };
+    int pair_rl(const hp_stream &) const { return script.on ? script.pair_rl : 0; }
+    static int pair_rl(const ListStream &ls) { return ls.pair_rl; }
+    template <class S> void draw2(S &rs, R &a, R &b, int call) {
+        const R first = (R)nextu(rs), second = (R)nextu(rs);
+        if (pair_rl(rs) & call) { a = second; b = first; }
+        else { a = first; b = second; }
+    }
+
     // ------------------------------------------------------------ MCC (Ar)
     R xsec(int ch, R engy) const {
         if (engy == 0) return (R)0;
@@ -608,6 +678,46 @@ template <class R> struct Sim : SimBase {
         vzs = vel * coschi * (r31 * sinchi * cosphi + r32 * sinchi * sinphi + r33 * coschi);
     }
 
+    void xsec_n(int ch, const float *engy, float *out, int n) const override {
+        for (int k = 0; k < n; k++) out[k] = (float)xsec(ch, (R)engy[k]);
+    }
+    void kinematics(int kind, const float *in, float *out, int n) const override {
+        for (int k = 0; k < n; k++) {
+            R x = 0, y = 0, z = 0;
+            if (kind == 0) {
+                const float *a = in + 7 * (size_t)k;
+                x = a[2]; y = a[3]; z = a[4];
+                anewvel((R)a[0], (R)a[1], x, y, z, (R)a[5], (R)a[6]);
+            } else if (kind == 1) {
+                const float *a = in + 6 * (size_t)k;
+                x = a[0]; y = a[1]; z = a[2];
+                newvel_ionsc(x, y, z, (R)a[3], (R)a[4], (R)a[5]);
+            } else {
+                const float *a = in + 4 * (size_t)k;
+                maxwellv(x, y, z, (R)a[0], (R)a[1], (R)a[2], (R)a[3]);
+            }
+            out[3 * (size_t)k] = (float)x;
+            out[3 * (size_t)k + 1] = (float)y;
+            out[3 * (size_t)k + 2] = (float)z;
+        }
+    }
+    int collide_oxy(int isp, int t, const float *v, float bv1, float bv2, const float *u, int nu, int pair_rl_,
+                    int *ch, int *keep, float *vout, int *bsp, float *bv, int *kill) override {
+        ListStream ls{u, nu, 0, false, pair_rl_};
+        OxyOut o;
+        if (isp == 0) oxy_electron((R)v[0], (R)v[1], (R)v[2], t, (R)bv1, ls, o);
+        else oxy_ion(isp, (R)v[0], (R)v[1], (R)v[2], t, (R)bv1, (R)bv2, ls, o);
+        *ch = o.ch;
+        *keep = o.keep ? 1 : 0;
+        vout[0] = (float)o.vx; vout[1] = (float)o.vy; vout[2] = (float)o.vz;
+        for (int q = 0; q < 2; q++) {
+            bsp[q] = o.bsp[q];
+            for (int d = 0; d < 3; d++) bv[3 * q + d] = (float)o.bv[q][d];
+        }
+        *kill = o.kill ? 1 : 0;
+        return ls.overrun ? 1 : 0;
+    }
+
     // ------------------------------------------------------------ MCC (Ar/O2)
     // MCC_ArO2_Basic (src/cuda_mcc.cu:21-71), ArO2_Collision_Check and the
     // species handlers (src/cuda_mccArO2.cu:51-1265), with the order this
@@ -633,7 +743,7 @@ template <class R> struct Sim : SimBase {
         return first ? (R)(1.0 - (double)ex) : (R)((double)prev + 1.0 - (double)ex);
     }
 
-    void oxy_electron(R vx, R vy, R vz, int t, R bv1, hp_stream &rs, OxyOut &o) const {
+    template <class S> void oxy_electron(R vx, R vy, R vz, int t, R bv1, S &rs, OxyOut &o) {
         // ladders: (channel, action, threshold index or first new species, second new species, gain)
         enum { EL, LO, GA, AT, IO, RE, DE };
         struct Rg { int ch, act, a1, a2; float gain; };
@@ -683,10 +793,10 @@ template <class R> struct Sim : SimBase {
         R rengy = 0, vel2 = 0;
         R R1;
         if (aro2) {
-            R1 = (R)hp_stream_next(&rs);
+            R1 = (R)nextu(rs);
             R1 *= (R)c.sigv[t] / vel;
         } else {
-            R1 = (R)hp_stream_next(&rs) * (R)c.sigv[t] / vel;
+            R1 = (R)nextu(rs) * (R)c.sigv[t] / vel;
         }
         R sum = 0;
         bool hit = false;
@@ -712,7 +822,7 @@ template <class R> struct Sim : SimBase {
                 colltype = 3;
                 engy -= (R)c.th[r.ch];
                 if (aro2) {
-                    const R u = (R)hp_stream_next(&rs);
+                    const R u = (R)nextu(rs);
                     rengy = (R)(10.0 * (double)m_tan(u * m_atan((R)(engy / 20.0))));
                     engy -= rengy;
                     vel = std::sqrt(std::fabs(rengy) / Esc);
@@ -733,15 +843,17 @@ template <class R> struct Sim : SimBase {
         switch (colltype) {
         case 0: break;
         case 1: {
-            const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+            R a, b;
+            draw2(rs, a, b, PAIR_ANEWVEL);
             anewvel(engy, vel, VX, VY, VZ, a, b);
             o.vx = VX; o.vy = VY; o.vz = VZ;
             break;
         }
         case 2: {
             o.keep = false;
-            const int n = (int)((c.nvel - 1) * hp_stream_next(&rs));
-            const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+            const int n = (int)((c.nvel - 1) * nextu(rs));
+            R a, b;
+            draw2(rs, a, b, PAIR_MAXWELLV);
             o.bsp[0] = aro2 ? 4 : 3;
             maxwellv(o.bv[0][0], o.bv[0][1], o.bv[0][2], (R)c.vsave[n], bv1, a, b);
             break;
@@ -753,16 +865,19 @@ template <class R> struct Sim : SimBase {
                 if (isp[q] == 0) {
                     o.bv[q][0] = VX; o.bv[q][1] = VY; o.bv[q][2] = VZ;
                     if (aro2) {
-                        const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+                        R a, b;
+                        draw2(rs, a, b, PAIR_ANEWVEL);
                         anewvel(rengy, vel, o.bv[q][0], o.bv[q][1], o.bv[q][2], a, b);
                     }
                 } else {
-                    const int n = (int)((c.nvel - 1) * hp_stream_next(&rs));
-                    const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+                    const int n = (int)((c.nvel - 1) * nextu(rs));
+                    R a, b;
+                    draw2(rs, a, b, PAIR_MAXWELLV);
                     maxwellv(o.bv[q][0], o.bv[q][1], o.bv[q][2], (R)c.vsave[n], bv1, a, b);
                 }
             }
-            const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+            R a, b;
+            draw2(rs, a, b, PAIR_ANEWVEL);
             anewvel(engy, aro2 ? vel2 : vel, VX, VY, VZ, a, b);
             o.vx = VX; o.vy = VY; o.vz = VZ;
             break;
@@ -771,17 +886,18 @@ template <class R> struct Sim : SimBase {
         default: {
             o.bsp[0] = 0;
             o.bv[0][0] = VX; o.bv[0][1] = VY; o.bv[0][2] = VZ;
-            const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+            R a, b;
+            draw2(rs, a, b, PAIR_ANEWVEL);
             anewvel(engy, vel, VX, VY, VZ, a, b);
             o.vx = VX; o.vy = VY; o.vz = VZ;
             o.kill = true;
-            o.r2 = hp_stream_next(&rs);
+            o.r2 = nextu(rs);
             break;
         }
         }
     }
 
-    void oxy_ion(int s, R vx, R vy, R vz, int t, R bv1, R bv2, hp_stream &rs, OxyOut &o) const {
+    template <class S> void oxy_ion(int s, R vx, R vy, R vz, int t, R bv1, R bv2, S &rs, OxyOut &o) {
         enum { NUL, SCAT, CX, TO_OP, TO_ARP, TO_O2P, DET, REC };
         const bool aro2 = c.gas == 2;
         const int OMINUS = aro2 ? 4 : 3, O2P = aro2 ? 2 : 1, OPL = aro2 ? 3 : 2;
@@ -797,14 +913,15 @@ template <class R> struct Sim : SimBase {
             engy = Esc * dum;
         } else {
             const R vneut = aro2 ? (s == 1 ? (t == 0 ? bv1 : bv2) : (s == 2 ? bv1 : bv2)) : bv1;
-            const int n = (int)((c.nvel - 1) * hp_stream_next(&rs));
-            const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+            const int n = (int)((c.nvel - 1) * nextu(rs));
+            R a, b;
+            draw2(rs, a, b, PAIR_MAXWELLV);
             maxwellv(vnx, vny, vnz, (R)c.vsave[n], vneut, a, b);
             VX = vx - vnx; VY = vy - vny; VZ = vz - vnz;
             const R dum = VX * VX + VY * VY + VZ * VZ;
             vel = std::sqrt(dum);
             engy = Esc * dum;
-            if (aro2 && s == 1) (void)hp_stream_next(&rs);
+            if (aro2 && s == 1) (void)nextu(rs);
         }
         int sv = 0, nr = 0, ch[3] = {0, 0, 0}, act[3] = {0, 0, 0};
         bool cum = false;
@@ -861,7 +978,7 @@ template <class R> struct Sim : SimBase {
             else { nr = 1; ch[0] = 51; act[0] = DET; }
             break;
         }
-        const R R1 = (R)hp_stream_next(&rs) * (R)c.sigv[sv] / vel;
+        const R R1 = (R)nextu(rs) * (R)c.sigv[sv] / vel;
         int what = NUL;
         R sum = 0;
         for (int k = 0; k < nr; k++) {
@@ -874,7 +991,8 @@ template <class R> struct Sim : SimBase {
         switch (what) {
         case NUL: break;
         case SCAT: {
-            const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+            R a, b;
+            draw2(rs, a, b, PAIR_IONSC);
             newvel_ionsc(VX, VY, VZ, vel, a, b);
             if (s == OMINUS) { o.vx = VX; o.vy = VY; o.vz = VZ; }
             else { o.vx = VX + vnx; o.vy = VY + vny; o.vz = VZ + vnz; }
@@ -997,7 +1115,7 @@ template <class R> struct Sim : SimBase {
                 for (int k = 0; k < n0[s]; k++) {
                     int t = -1;
                     for (int jj = 0; jj < nsub; jj++) {
-                        const float R1 = hp_test_draw(c.seed, (uint32_t)k, (uint32_t)cell, step, (uint32_t)s, (uint32_t)jj);
+                        const float R1 = u_test((uint32_t)k, cell, step, (uint32_t)s, (uint32_t)jj);
                         if ((R)R1 < Tprob) {
                             t = np[s] - 1;
                             for (int q = 0; q < np[s] - 1; q++)
@@ -1113,13 +1231,14 @@ template <class R> struct Sim : SimBase {
             unsigned cnt_ch[7] = {0, 0, 0, 0, 0, 0, 0};
             const int ni = ion.cnt[cell];
             for (int k = 0; k < ni; k++) {
-                if (hp_test_draw(c.seed, (uint32_t)k, (uint32_t)cell, step, 1u, 0u) > Pion) continue;
+                if (u_test((uint32_t)k, cell, step, 1u, 0u) > Pion) continue;
                 hp_stream rs;
                 hp_stream_init(&rs, c.seed, (uint32_t)k, (uint32_t)cell, step, 1u);
-                const int nn = (int)((c.nvel - 1) * hp_stream_next(&rs));
+                const int nn = (int)((c.nvel - 1) * nextu(rs));
                 R vnx, vny, vnz;
                 {
-                    const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+                    R a, b;
+                    draw2(rs, a, b, PAIR_MAXWELLV);
                     maxwellv(vnx, vny, vnz, (R)c.vsave[nn], bvel, a, b);
                 }
                 const size_t q = (size_t)ion.start[cell] + k;
@@ -1128,14 +1247,15 @@ template <class R> struct Sim : SimBase {
                 const R dum = VX * VX + VY * VY + VZ * VZ;
                 const R engy = (R)c.Escale[1] * dum;
                 const R vel = std::sqrt(dum);
-                const R Rr = (R)hp_stream_next(&rs) * (R)c.sigv[2] / vel;
+                const R Rr = (R)nextu(rs) * (R)c.sigv[2] / vel;
                 R SumSigma = xsec(5, engy);
                 R ox, oy, oz;
                 if (Rr <= SumSigma) {
                     ox = vnx; oy = vny; oz = vnz;
                     cnt_ch[5]++;
                 } else if (Rr <= (SumSigma += xsec(6, engy))) {
-                    const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+                    R a, b;
+                    draw2(rs, a, b, PAIR_IONSC);
                     newvel_ionsc(VX, VY, VZ, vel, a, b);
                     ox = VX + vnx; oy = VY + vny; oz = VZ + vnz;
                     cnt_ch[6]++;
@@ -1149,7 +1269,7 @@ template <class R> struct Sim : SimBase {
                 int colltype = 0;
                 float R1 = 0.f;
                 for (int jj = 0; jj < c.mcc_n; jj++) {
-                    R1 = hp_test_draw(c.seed, (uint32_t)k, (uint32_t)cell, step, 0u, (uint32_t)jj);
+                    R1 = u_test((uint32_t)k, cell, step, 0u, (uint32_t)jj);
                     if (R1 < P2) { colltype = 1; break; }
                 }
                 if (!colltype) continue;
@@ -1167,14 +1287,14 @@ template <class R> struct Sim : SimBase {
                 auto ionize = [&](float th) {
                     colltype = 2;
                     engy -= (R)th;
-                    const R u = hp_stream_next(&rs);
+                    const R u = nextu(rs);
                     rengy = (R)(10.0 * (double)m_tan(u * m_atan((R)(engy / 20.0))));
                     engy -= rengy;
                     vel = std::sqrt(std::fabs(rengy) / Esc);
                     vel2 = std::sqrt(std::fabs(engy) / Esc);
                 };
                 if (target == 0) {
-                    const R R2 = (R)hp_stream_next(&rs) * (R)c.sigv[0] / vel;
+                    const R R2 = (R)nextu(rs) * (R)c.sigv[0] / vel;
                     R SumSigma = xsec(0, engy);
                     if (R2 <= SumSigma) {
                         colltype = 0;
@@ -1194,7 +1314,7 @@ template <class R> struct Sim : SimBase {
                         cnt_ch[3]++;
                     }
                 } else {
-                    const R R2 = (R)hp_stream_next(&rs) * (R)c.sigv[1] / vel;
+                    const R R2 = (R)nextu(rs) * (R)c.sigv[1] / vel;
                     const R SumSigma = xsec(4, engy);
                     if (engy > (R)c.th[4] && R2 <= SumSigma) {
                         ionize(c.th[4]);
@@ -1202,23 +1322,27 @@ template <class R> struct Sim : SimBase {
                     }
                 }
                 if (colltype == 0) {
-                    const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+                    R a, b;
+                    draw2(rs, a, b, PAIR_ANEWVEL);
                     anewvel(engy, vel, VX, VY, VZ, a, b);
                     el.vx[q] = VX; el.vy[q] = VY; el.vz[q] = VZ;
                 } else if (colltype == 2) {
                     R nevx = VX, nevy = VY, nevz = VZ;
                     {
-                        const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+                        R a, b;
+                        draw2(rs, a, b, PAIR_ANEWVEL);
                         anewvel(rengy, vel, nevx, nevy, nevz, a, b);
                     }
                     R nivx = VX, nivy = VY, nivz = VZ;
                     {
-                        const int nn = (int)((c.nvel - 1) * hp_stream_next(&rs));
-                        const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+                        const int nn = (int)((c.nvel - 1) * nextu(rs));
+                        R a, b;
+                        draw2(rs, a, b, PAIR_MAXWELLV);
                         maxwellv(nivx, nivy, nivz, (R)c.vsave[nn], bvel, a, b);
                     }
                     {
-                        const R a = hp_stream_next(&rs), b = hp_stream_next(&rs);
+                        R a, b;
+                        draw2(rs, a, b, PAIR_ANEWVEL);
                         anewvel(engy, vel2, VX, VY, VZ, a, b);
                     }
                     el.vx[q] = VX; el.vy[q] = VY; el.vz[q] = VZ;
@@ -1850,6 +1974,27 @@ void or_get_counters(or_sim *s, float *cond_charge, unsigned *mcc_count, int *pc
     if (cond_charge) std::memcpy(cond_charge, b->cond_charge.data(), b->cond_charge.size() * 4);
     if (mcc_count) std::memcpy(mcc_count, b->mcc_count.data(), b->mcc_count.size() * 4);
     if (pcg_iters) { pcg_iters[0] = b->pcg_iters[0]; pcg_iters[1] = b->pcg_iters[1]; }
+}
+void or_set_script(or_sim *s, int flags, const float *u, const int64_t *start, int nkeys) {
+    SimBase *b = s->impl;
+    b->script_overrun = 0;
+    if (!u || nkeys <= 0) {
+        b->script = SimBase::Script();
+        return;
+    }
+    b->script.on = true;
+    b->script.by_species = flags & 1;
+    b->script.pair_rl = (flags >> 1) & 7;
+    b->script.start.assign(start, start + nkeys + 1);
+    b->script.u.assign(u, u + start[nkeys]);
+    b->script.pos.assign((size_t)nkeys, 0);
+}
+long long or_script_overrun(or_sim *s) { return s->impl->script_overrun.load(); }
+void or_xsec(or_sim *s, int ch, const float *engy, float *out, int n) { s->impl->xsec_n(ch, engy, out, n); }
+void or_kinematics(or_sim *s, int kind, const float *in, float *out, int n) { s->impl->kinematics(kind, in, out, n); }
+int or_collide_oxy(or_sim *s, int isp, int t, const float *v, float bv1, float bv2, const float *u, int nu,
+                   int pair_rl, int *ch, int *keep, float *vout, int *bsp, float *bv, int *kill) {
+    return s->impl->collide_oxy(isp, t, v, bv1, bv2, u, nu, pair_rl, ch, keep, vout, bsp, bv, kill);
 }
 void or_field(or_sim *s, int64_t tstep) { s->impl->field(tstep); }
 void or_move(or_sim *s) { s->impl->move(); }

@@ -121,6 +121,32 @@ void or_get_averages(or_sim *s, double *ave_den, double *ave_phi, int64_t *count
 void or_get_field_averages(or_sim *s, double *ave_src, double *ave_ex, double *ave_ey);
 /* the electron energy histogram: 201 counts (0.25 eV bins, last = overflow) */
 void or_get_eedf(or_sim *s, unsigned long long *h);
+/* Scripted uniforms, for pinning the oracle against the reference's own MCC
+ * code: u holds the draw lists of nkeys keys back to back, start[nkeys + 1]
+ * their offsets; key = cell (flags bit 0 clear) or species * Csize + cell
+ * (bit 0 set).  Every MCC draw (null-collision tests included) is then taken
+ * in order from its key's list; flags bits 1, 2, 3 take the two draws passed
+ * to one anewvel, maxwellv, newvel_ionsc call right to left (the pair mask,
+ * bits 0-2 of flags >> 1).  u = NULL goes back to Philox.
+ * or_script_overrun counts the draws asked for beyond a list's end (those
+ * yield 1.0). */
+void or_set_script(or_sim *s, int flags, const float *u, const int64_t *start, int nkeys);
+long long or_script_overrun(or_sim *s);
+/* the MCC's cross-section lookup: channel ch at energies engy[n] (eV) */
+void or_xsec(or_sim *s, int ch, const float *engy, float *out, int n);
+/* scattering kinematics with given uniforms, out[3n] = new velocity:
+ * kind 0 anewvel:      in[7n] = energy, vel, unit direction x, y, z, rand1, rand2
+ * kind 1 newvel_ionsc: in[6n] = relative velocity x, y, z, its magnitude, rand1, rand2
+ * kind 2 maxwellv:     in[4n] = vsave sample, thermal speed, Rphi, Rthe */
+void or_kinematics(or_sim *s, int kind, const float *in, float *out, int n);
+/* One collision of a particle of species isp (velocity v[3]) with target t
+ * of the Ar/O2 or O2 set, drawing from u[nu] (pair_rl: the pair mask of
+ * or_set_script): ch the reaction channel (-1 none), keep
+ * whether the particle stays (with velocity vout[3]), bsp[2] the species born
+ * (-1 none) with velocities bv[6], kill whether an O- is removed.  Returns 1
+ * when the list ran out. */
+int or_collide_oxy(or_sim *s, int isp, int t, const float *v, float bv1, float bv2, const float *u, int nu,
+                   int pair_rl, int *ch, int *keep, float *vout, int *bsp, float *bv, int *kill);
 int or_num_threads(void);
 void or_set_threads(int n);
 

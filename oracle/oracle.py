@@ -88,6 +88,12 @@ def lib():
             "or_deposit_basic": (None, [P]),
             "or_run": (None, [P, C.c_int64, C.c_int, C.c_int]),
             "or_get_averages": (None, [P, _D, _D, C.POINTER(C.c_int64)]),
+            "or_set_script": (None, [P, C.c_int, _F, C.POINTER(C.c_int64), C.c_int]),
+            "or_script_overrun": (C.c_longlong, [P]),
+            "or_xsec": (None, [P, C.c_int, _F, _F, C.c_int]),
+            "or_kinematics": (None, [P, C.c_int, _F, _F, C.c_int]),
+            "or_collide_oxy": (C.c_int, [P, C.c_int, C.c_int, _F, C.c_float, C.c_float, _F, C.c_int, C.c_int, _I,
+                                         _I, _F, _I, _F, _I]),
             "or_num_threads": (C.c_int, []),
             "or_set_threads": (None, [C.c_int]),
         }
@@ -339,6 +345,48 @@ class Oracle:
         h = np.zeros(201, np.uint64)
         lib().or_get_eedf(self.h, h.ctypes.data_as(C.POINTER(C.c_uint64)))
         return h
+
+    def set_script(self, u, start, by_species=False, pair_rl=0):
+        """Scripted uniforms for the MCC (see oracle.h); u=None goes back to
+        Philox.  pair_rl: mask of the kinematics calls (1 anewvel, 2 maxwellv,
+        4 newvel_ionsc) whose two draws are taken right to left."""
+        if u is None:
+            lib().or_set_script(self.h, 0, None, None, 0)
+            return
+        self.keep["script_u"] = u = np.ascontiguousarray(u, np.float32)
+        self.keep["script_s"] = st = np.ascontiguousarray(start, np.int64)
+        flags = (1 if by_species else 0) | (int(pair_rl) << 1)
+        lib().or_set_script(self.h, flags, _fp(u), st.ctypes.data_as(C.POINTER(C.c_int64)), st.size - 1)
+
+    def script_overrun(self):
+        return int(lib().or_script_overrun(self.h))
+
+    def xsec(self, ch, engy):
+        e = np.ascontiguousarray(engy, np.float32)
+        out = np.zeros(e.size, np.float32)
+        lib().or_xsec(self.h, ch, _fp(e), _fp(out), e.size)
+        return out
+
+    def kinematics(self, kind, inp):
+        inp = np.ascontiguousarray(inp, np.float32)
+        n = inp.size // {0: 7, 1: 6, 2: 4}[kind]
+        out = np.zeros(3 * n, np.float32)
+        lib().or_kinematics(self.h, kind, _fp(inp), _fp(out), n)
+        return out.reshape(n, 3)
+
+    def collide_oxy(self, isp, t, v, bv1, bv2, u, pair_rl=0):
+        """One collision (Ar/O2 or O2 set) from the draws u: (channel, keep,
+        velocity, born species[2], their velocities[2][3], O- removed)."""
+        v = np.ascontiguousarray(v, np.float32)
+        u = np.ascontiguousarray(u, np.float32)
+        ch, keep, kill = C.c_int(0), C.c_int(0), C.c_int(0)
+        vout = np.zeros(3, np.float32)
+        bsp = np.zeros(2, np.int32)
+        bv = np.zeros(6, np.float32)
+        over = lib().or_collide_oxy(self.h, isp, t, _fp(v), np.float32(bv1), np.float32(bv2), _fp(u), u.size,
+                                    int(pair_rl), C.byref(ch), C.byref(keep), _fp(vout), _ip(bsp), _fp(bv),
+                                    C.byref(kill))
+        return ch.value, bool(keep.value), vout, bsp, bv.reshape(2, 3), bool(kill.value), bool(over)
 
     def averages(self):
         G, nsp = self.info.Gsize, self.info.nsp

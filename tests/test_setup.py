@@ -134,6 +134,32 @@ def test_symmetrised_operator_is_symmetric(pair):
             assert np.isclose(st[u, k] / d[u], st[v, back] / d[v], rtol=1e-6)
 
 
+def test_stencil_is_the_reference_matrix(pair):
+    """The field solvers apply the 5-point node stencil; every row must be the
+    reference's own CSR row (src/load.c:121-246, golden a_val/ai/aj) of that
+    unknown, coefficient for coefficient."""
+    s, g = pair
+    st = s.table("stencil").reshape(-1, 5)
+    unk = s.table("unk_node")
+    aidx = g["aidx"]
+    ai, aj, av = g["ai"], g["aj"], g["a_val"]
+    ngy = s.info.ngy
+    offs = [-ngy, -1, 0, 1, ngy]
+    assert unk.size == int(aidx.max())
+    for u, n in enumerate(unk):
+        row = int(aidx[n]) - 1
+        want = {int(aj[k]) - 1: av[k] for k in range(ai[row] - 1, ai[row + 1] - 1)}
+        got = {}
+        for k, off in enumerate(offs):
+            if k == 2 or st[u, k] != 0:
+                col = int(aidx[int(n) + off]) - 1
+                assert col >= 0, "stencil reaches a node that is not an unknown"
+                got[col] = st[u, k]
+        assert got.keys() == want.keys(), f"row {row}: columns {sorted(got)} vs {sorted(want)}"
+        for col in want:
+            assert bits(np.float32(got[col])) == bits(np.float32(want[col])), f"row {row} col {col}"
+
+
 def test_deck_errors():
     deck = json.loads(str(np.load(GOLD[0])["deck"]))
     bad = json.loads(json.dumps(deck))
