@@ -11,8 +11,10 @@ particles, FP64 charge grid and FP64-refined field solve (field_mode 2).
 
 Under torchrun each rank advances its own replica of the case (one case does
 not shard: replicas only); value = pushes of all ranks / max rank time.
-`--impl reference` times the CPU restatement of the step (the reference has
-no CPU step of its own) on this host's cores, on the same workload.
+`--impl reference` times the reference's CPU path on this host's cores, on the
+same workload: the reference's own set-up code (oracle/_ref) and the CPU
+restatement of its step (the reference has no CPU step of its own), with its
+own numerics; it loads nothing of this library.
 """
 import argparse
 import json
@@ -45,8 +47,19 @@ WORKLOADS = {
 }
 
 
+def _decks():
+    """hpic/decks.py loaded on its own (plain Python deck writer), so that the
+    reference arm imports nothing of the library."""
+    import importlib.util
+    path = os.path.join(REPO, "hybrid-final_b200", "hpic", "decks.py")
+    spec = importlib.util.spec_from_file_location("case_decks", path)
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
 def make_deck(w):
-    from hpic.decks import ccp_deck
+    ccp_deck = _decks().ccp_deck
     extra = {}
     if w.get("gas", "Ar") != "Ar":
         extra = dict(gas=w["gas"], te_ev=w["te"], ion_density=w["ions"], aro2_ratio=(80, 20))
@@ -158,7 +171,7 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def cpu_baseline(setup, case_opts, budget_s=20.0):
+def cpu_baseline(setup, case_opts, budget_s=20.0, what="CPU restatement"):
     """The CPU restatement (oracle, FP32 form) on this host: a bounded number
     of full steps of the same case."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
@@ -180,7 +193,7 @@ def cpu_baseline(setup, case_opts, budget_s=20.0):
             break
     return dict(value=pushes / t_used, unit=UNIT, cores=int(oracle.lib().or_num_threads()), kind="port",
                 sample=f"{steps} full step(s) of the same case ({pushes} particle-pushes) on the host, "
-                       f"CPU restatement in FP32, {t_used:.1f} s")
+                       f"{what} in FP32, {t_used:.1f} s")
 
 
 def fp64_check(stream, steps=800):
@@ -342,18 +355,29 @@ def run_ours(args, rank, world, local, dist):
 
 
 def run_reference(args):
-    """CPU restatement of the step on this host (all its cores), same workload."""
-    import hpic
+    """The reference's CPU path on this host, on the same workload: its own
+    set-up code (oracle/_ref/ref_dump: deck, geometry, matrix, sources,
+    species, particle load; the CUDA-side set-up restated in
+    oracle/refsetup.py) and the oracle's restatement of its step with its own
+    numerics (PCG to its absolute tolerance, one cell crossing per push), on
+    all host threads.  Nothing of this library is imported or loaded."""
     sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import refsetup
     w = WORKLOADS[args.workload]
-    setup = hpic.Setup(make_deck(w), seed=1000, field_mode=args.field_mode, gas_temp_mode=1,
-                       move_mode=args.move_mode)
+    base = dict(metric=METRIC, unit=UNIT, impl="reference")
+    if not refsetup.available():
+        return dict(base, unavailable="oracle/_ref/ref_dump (the reference's set-up code) was not built")
+    if w.get("gas", "Ar") != "Ar":
+        return dict(base, unavailable="the reference arm's set-up covers the Ar reaction set only")
+    setup = refsetup.RefSetup(json.dumps(make_deck(w)), seed=1000, field_mode=0, move_mode=0)
     budget = float(os.environ.get("HPIC_REF_BUDGET_S", "90"))
-    cb = cpu_baseline(setup, setup.opts, budget_s=budget)
-    return dict(metric=METRIC, value=cb["value"], unit=UNIT, n_gpus=int(os.environ.get("WORLD_SIZE", "1")),
+    cb = cpu_baseline(setup, setup.opts, budget_s=budget, what="the reference's set-up and step algorithm")
+    return dict(base, value=cb["value"], n_gpus=int(os.environ.get("WORLD_SIZE", "1")),
                 steps=args.steps, warmup=args.warmup, higher_is_better=True, scaling="weak", vs_baseline=None,
-                dtype="f32", data="synthetic", impl="reference",
-                config=dict(workload=args.workload, nodes=f"{w['ngx']}x{w['ngy']}", ppc_per_species=w["ppc"]),
+                dtype="f32", data="synthetic",
+                config=dict(workload=args.workload, nodes=f"{w['ngx']}x{w['ngy']}", ppc_per_species=w["ppc"],
+                            field="PCG, absolute r'z tolerance (the reference's rule)",
+                            move="one cell crossing per push (the reference's rule)"),
                 cpu_baseline=dict(kind=cb["kind"], cores=cb["cores"], sample=cb["sample"], value=cb["value"],
                                   unit=UNIT),
                 e2e=dict(value=cb["value"], unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))
