@@ -1482,6 +1482,9 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
         }
         double rz = cluster_sum2(cl, part, 0.0, sh, parity, nullptr);
         parity ^= 1;
+        // a non-finite right-hand side or warm start: the reference's loop
+        // test (r'z > tol^2) is false for NaN and leaves x as it was
+        if (!(rz == rz) || isinf(rz)) bad = true;
         int iter = 1;
         while (rz > (double)d.pcg_tol2 && iter <= maxit) {
             part = 0.0;

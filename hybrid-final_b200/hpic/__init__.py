@@ -21,6 +21,7 @@ DECK_DIR = os.path.join(PKG, "decks")
 HP_OK, HP_ERR_ARG, HP_ERR_DECK, HP_ERR_CUDA, HP_ERR_OOM, HP_ERR_UNSUPPORTED, HP_ERR_DEVICE, HP_ERR_CAPACITY, \
     HP_ERR_NO_CUDA = range(9)
 STATUS_CELL_OVERFLOW, STATUS_NONFINITE, STATUS_PCG_NOCONV, STATUS_WAIT_TIMEOUT = 1, 2, 4, 8
+STATUS_WALK_BOUND, STATUS_SURFACE_OVERFLOW = 0x10, 0x20
 
 GRID = dict(EX=0, EY=1, PHI=2, PHI_POIS=3, DEN=4, SOURCE=5, PCG_X=6, PCG_B=7, AVE_DEN=8, AVE_PHI=9,
             COND_CHARGE=10, MCC_COUNT=11, EEDF=12, AVE_SOURCE=13, AVE_EX=14, AVE_EY=15,
