@@ -41,6 +41,9 @@ WORKLOADS = {
     "ar_513x257_200ppc": dict(ngx=513, ngy=257, xlen=0.16, ylen=0.08, ppc=200, voltage=100.0, pressure=0.05),
     "ar_257x129_200ppc": dict(ngx=257, ngy=129, xlen=0.08, ylen=0.04, ppc=200, voltage=100.0, pressure=0.05),
     "ar_129x65_50ppc": dict(ngx=129, ngy=65, xlen=0.04, ylen=0.02, ppc=50, voltage=100.0, pressure=0.05),
+    # the Ar/O2 case's gas, pressure, voltage and densities on the 129x65 grid (FP64 check)
+    "aro2_129x65_50ppc": dict(ngx=129, ngy=65, xlen=0.04, ylen=0.02, ppc=50, voltage=200.0, pressure=0.1,
+                              gas="ArO2", te=3.0, ions={"Ar+": 1e15, "O2+": 2e14, "O+": 0.0, "O-": 2e14}),
     # 80/20 Ar/O2 at 100 mTorr, 200 V: e 3 eV, Ar+ 1e15, O2+ 2e14, O+ 0, O- 2e14 m^-3
     "aro2_257x129_100ppc": dict(ngx=257, ngy=129, xlen=0.08, ylen=0.04, ppc=100, voltage=200.0, pressure=0.1,
                                 gas="ArO2", te=3.0, ions={"Ar+": 1e15, "O2+": 2e14, "O+": 0.0, "O-": 2e14}),
@@ -196,19 +199,24 @@ def cpu_baseline(setup, case_opts, budget_s=20.0, what="CPU restatement"):
                        f"{what} in FP32, {t_used:.1f} s")
 
 
-def fp64_check(stream, steps=800):
-    """Error of the precision form against the FP64 oracle on the reference's
-    CPU-sized Ar case (129x65 nodes, 4 cm x 2 cm, 50 particles per cell and
-    species, 100 V, 50 mTorr) over two RF periods: relative L2 error of the
-    time-averaged n_e, n_i and potential, and the electron energy distribution
-    (sampled every 4th step) as total-variation distance and relative error of
-    the mean energy.  The GPU runs the bench's numerics
-    (FP32 particles, FP64 charge grid, field_mode 2); the oracle runs the same
-    case and draws in FP64 on the host."""
+SPECIES = {"Ar": ["e", "Ar+"], "ArO2": ["e", "Ar+", "O2+", "O+", "O-"]}
+
+
+def fp64_check(stream, workload="ar_129x65_50ppc", steps=800):
+    """Error of the precision form against the FP64 oracle over two RF
+    periods, on the reference's CPU-sized Ar case (129x65 nodes, 4 cm x 2 cm,
+    50 particles per cell and species, 100 V, 50 mTorr) or the 80/20 Ar/O2
+    case on the same grid (100 mTorr, 200 V): relative L2 error of the
+    time-averaged density of every species (n_i: all positive ions), of the
+    potential, and of the electron energy distribution (sampled every 4th
+    step) as total-variation distance and relative error of the mean energy.
+    The GPU runs the bench's numerics (FP32 particles, FP64 charge grid,
+    field_mode 2); the oracle runs the same case and draws in FP64 on the
+    host."""
     import hpic
     sys.path.insert(0, os.path.join(REPO, "oracle"))
     import oracle
-    w = WORKLOADS["ar_129x65_50ppc"]
+    w = WORKLOADS[workload]
     opts = dict(field_mode=2, gas_temp_mode=1, move_mode=1, eedf_every=4)
     S = hpic.Setup(make_deck(w), seed=77, **opts)
     c = hpic.Case(setup=S, seed=77, **opts)
@@ -217,6 +225,7 @@ def fp64_check(stream, steps=800):
     d32 = c.grid("AVE_DEN").reshape(c.info.nsp, -1) / n
     p32 = c.grid("AVE_PHI") / n
     h32 = c.grid("EEDF").astype(np.float64)
+    status = c.status()
     c.close()
     t0 = time.perf_counter()
     o = oracle.from_setup(S, 64, field_mode=2)
@@ -229,13 +238,21 @@ def fp64_check(stream, steps=800):
 
     def rel(a, b):
         return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+    names = SPECIES[w.get("gas", "Ar")]
+    pos = [k for k, nm in enumerate(names) if nm.endswith("+")]
     pe, qe = h32 / h32.sum(), h64 / h64.sum()
     ebin = (np.arange(pe.size) + 0.5) * hpic.EEDF_DE
-    return dict(case="ar_129x65_50ppc", steps=steps, rf_periods=steps / 400, tolerance=0.01,
-                rel_l2_ave_n_e=rel(d32[0], d64[0]), rel_l2_ave_n_i=rel(d32[1], d64[1]), rel_l2_ave_phi=rel(p32, p64),
-                eedf_tv=round(0.5 * float(np.abs(pe - qe).sum()), 6),
-                eedf_mean_energy_rel=round(abs(float(pe @ ebin) / float(qe @ ebin) - 1.0), 6),
-                fp64_oracle_s=round(time.perf_counter() - t0, 1))
+    out = dict(case=workload, steps=steps, rf_periods=steps / 400, tolerance=0.01,
+               rel_l2_ave_n_e=rel(d32[0], d64[0]), rel_l2_ave_n_i=rel(d32[pos].sum(0), d64[pos].sum(0)),
+               rel_l2_ave_phi=rel(p32, p64))
+    if len(names) > 2:
+        for k, nm in enumerate(names[1:], 1):
+            if np.linalg.norm(d64[k]) > 0:
+                out[f"rel_l2_ave_n_{nm}"] = rel(d32[k], d64[k])
+    out.update(eedf_tv=round(0.5 * float(np.abs(pe - qe).sum()), 6),
+               eedf_mean_energy_rel=round(abs(float(pe @ ebin) / float(qe @ ebin) - 1.0), 6),
+               device_status=int(status), fp64_oracle_s=round(time.perf_counter() - t0, 1))
+    return out
 
 
 def run_ours(args, rank, world, local, dist):
@@ -351,6 +368,7 @@ def run_ours(args, rank, world, local, dist):
     if rank == 0 and world == 1 and not args.no_fp64_check:
         case.close()
         result["fp64_check"] = fp64_check(stream)
+        result["fp64_check_aro2"] = fp64_check(stream, "aro2_129x65_50ppc")
     return result
 
 
