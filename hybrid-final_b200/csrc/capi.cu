@@ -681,6 +681,32 @@ static hp_status table_of(const Setup &s, const std::vector<float> *prob, const 
             tmpf.push_back((float)s.cond_power_id[k]);
         }
         src = tmpf.data(); nb = tmpf.size() * 4; break;
+    // fluid species (continuity solve)
+    case 41: src = s.fluid_cell_den.data(); nb = s.fluid_cell_den.size() * 4; break;
+    case 42:
+        for (size_t k = 0; k < s.xl_x1.size(); k++) { tmpi.push_back(s.xl_x1[k]); tmpi.push_back(s.xl_x2[k]); tmpi.push_back(s.xl_yy[k]); }
+        src = tmpi.data(); nb = tmpi.size() * 4; break;
+    case 43:
+        for (size_t k = 0; k < s.yl_xx.size(); k++) { tmpi.push_back(s.yl_xx[k]); tmpi.push_back(s.yl_y1[k]); tmpi.push_back(s.yl_y2[k]); }
+        src = tmpi.data(); nb = tmpi.size() * 4; break;
+    case 44:
+        tmpf = s.xl_fg1; tmpf.insert(tmpf.end(), s.xl_fg2.begin(), s.xl_fg2.end());
+        src = tmpf.data(); nb = tmpf.size() * 4; break;
+    case 45:
+        tmpf = s.yl_fg1; tmpf.insert(tmpf.end(), s.yl_fg2.begin(), s.yl_fg2.end());
+        src = tmpf.data(); nb = tmpf.size() * 4; break;
+    case 46: src = s.gax.data(); nb = s.gax.size() * 4; break;
+    case 47: src = s.gbx.data(); nb = s.gbx.size() * 4; break;
+    case 48: src = s.gay.data(); nb = s.gay.size() * 4; break;
+    case 49: src = s.gby.data(); nb = s.gby.size() * 4; break;
+    case 50: src = s.flux_x0.data(); nb = s.flux_x0.size() * 4; break;
+    case 51: src = s.flux_y0.data(); nb = s.flux_y0.size() * 4; break;
+    case 52: src = s.fluid_D.data(); nb = s.fluid_D.size() * 4; break;
+    case 53: // fluid scalars: dtc, N_ave, TimeStep_Conti, nfsp, x lines, y lines
+        tmpf = {s.dtc, (float)s.N_ave, (float)s.DT_CONTI, (float)s.nfsp, (float)s.xl_x1.size(), (float)s.yl_xx.size()};
+        src = tmpf.data(); nb = tmpf.size() * 4; break;
+    case 54: src = s.fluid_rate_f.data(); nb = s.fluid_rate_f.size() * 4; break;
+    case 55: src = s.plasma_region.data(); nb = s.plasma_region.size() * 4; break;
     default: set_error("unknown table id"); return HP_ERR_ARG;
     }
     if (needed) *needed = nb;

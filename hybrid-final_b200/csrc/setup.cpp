@@ -311,7 +311,6 @@ void read_gas(const JVal &root, Setup &s) {
     const JVal &bgo = g.object("Background");
     const JVal &ns = g.object("NeutralSpecies");
     const JVal &cs = g.object("ChargeSpecies");
-    int ftype; float fx0, fx1, fy0, fy1;
     const float me = (float)(5.485799486e-4 * AMU);
     const float mAr = (float)(39.950 * AMU), mArIon = (float)(39.9500 * AMU);
     const float mO2 = (float)(32.0000 * AMU), mO = (float)(16.0000 * AMU);
@@ -322,7 +321,7 @@ void read_gas(const JVal &root, Setup &s) {
         b.Temp = fnum(bgo.object("Argon"), "Temp(eV)");
         b.mass = mAr;
         b.InitDens = (float)(NperTORR * b.Pres / (b.Temp + DBLMIN));
-        read_load(ns, ftype, fx0, fx1, fy0, fy1, false);
+        read_load(ns, s.fluid_loadtype, s.fluid_x_center, s.fluid_x_fall, s.fluid_y_center, s.fluid_y_fall, false);
         read_fluid(ns, "Ar*", s.fg[0], mAr);
         read_load(cs, s.sp[0].loadtype, s.sp[0].x_center, s.sp[0].x_fall, s.sp[0].y_center, s.sp[0].y_fall, true);
         read_species_block(cs, "Electron", s.sp[0], me, qe);
@@ -333,7 +332,7 @@ void read_gas(const JVal &root, Setup &s) {
         b.Temp = fnum(bgo.object("Oxygen"), "Temp(eV)");
         b.mass = mO2;
         b.InitDens = (float)(NperTORR * b.Pres / (b.Temp + DBLMIN));
-        read_load(ns, ftype, fx0, fx1, fy0, fy1, false);
+        read_load(ns, s.fluid_loadtype, s.fluid_x_center, s.fluid_x_fall, s.fluid_y_center, s.fluid_y_fall, false);
         read_fluid(ns, "O2A", s.fg[0], mO2);
         read_fluid(ns, "O2B", s.fg[1], mO2);
         read_fluid(ns, "OP", s.fg[2], mO);
@@ -356,7 +355,7 @@ void read_gas(const JVal &root, Setup &s) {
         o.Pres = s.total_pressure * o.Ratio;
         a.InitDens = (float)(NperTORR * a.Pres / (a.Temp + DBLMIN));
         o.InitDens = (float)(NperTORR * o.Pres / (o.Temp + DBLMIN));
-        read_load(ns, ftype, fx0, fx1, fy0, fy1, false);
+        read_load(ns, s.fluid_loadtype, s.fluid_x_center, s.fluid_x_fall, s.fluid_y_center, s.fluid_y_fall, false);
         read_fluid(ns, "Ar*", s.fg[0], mAr);
         read_fluid(ns, "O2A", s.fg[1], mO2);
         read_fluid(ns, "O2B", s.fg[2], mO2);
@@ -374,7 +373,7 @@ void read_gas(const JVal &root, Setup &s) {
 void read_method(const JVal &root, Setup &s) { // src/start.c:732-747
     const JVal &m = root.object("SimulationMethod");
     s.DT_PIC = ivnzc(m, "TimeStep_PIC");
-    ivnzc(m, "TimeStep_Conti");
+    s.DT_CONTI = ivnzc(m, "TimeStep_Conti");
     s.PCGtol = fvnzc(m, "PCGMarginOfError");
     s.PCGtol2 = s.PCGtol * s.PCGtol;
     ivnzc(m, "HistoryMax");
@@ -384,6 +383,10 @@ void read_method(const JVal &root, Setup &s) { // src/start.c:732-747
     if (s.N_smt < 0) s.N_smt = 0;
     ivnzc(m, "ParticleLimit");
     if (inum(m, "ConstB_Flag")) unsupported("constant magnetic field (ConstB_Flag)");
+    // ContinuitySteadyState (src/start.c:773-786) switches the continuity
+    // solve of each fluid species off once its mean density settles
+    if (m.has("ContinuitySteadyState") && inum(m.object("ContinuitySteadyState"), "Flag"))
+        unsupported("ContinuitySteadyState (the continuity solve runs every step here)");
     // power-driven sources (src/start.c:786-790): the amplitude is revised
     // every Interval RF periods, by at most VoltageUpDownRatio upwards
     const JVal &pd = m.object("PowerDrivenOption");
@@ -935,13 +938,219 @@ void laplace_and_gas(Setup &s, int gas_temp_mode) {
             s.back_vel2[g] = (float)sqrt(T * 1.38e-23 / s.bg[1].mass);
         }
     }
-    // fluid (metastable) densities: held at the deck's value on the nodes of
-    // the plasma region; the continuity solver that evolves them is outside
-    // this library (src/cuda_Fluid.cu)
-    s.fluid_den.assign((size_t)s.nfsp * G, 0.0f);
+}
+
+// ---------------------------------------------------------------- fluid species
+// Ar_meta_omega (src/cuda_Fluid.cu:299-320): the collision integral of
+// metastable Ar.  The reference's loop has no break, so every tabulated point
+// above the argument overwrites the result and the last interval (50..100)
+// decides; kept as written.
+float ar_meta_omega(float value) {
+    static const float tstar[27] = {0.250f, 0.267f, 0.286f, 0.308f, 0.333f, 0.364f, 0.400f, 0.444f, 0.500f,
+                                    0.571f, 0.667f, 0.800f, 1.000f, 1.330f, 2.000f, 2.500f, 2.860f, 3.330f,
+                                    4.000f, 5.000f, 6.670f, 10.00f, 12.50f, 16.67f, 25.00f, 50.00f, 100.0f};
+    static const float omega[27] = {1.8714f, 1.8344f, 1.7962f, 1.7560f, 1.7142f, 1.6702f, 1.6238f, 1.5748f, 1.5228f,
+                                    1.4676f, 1.4090f, 1.3466f, 1.2802f, 1.2096f, 1.1348f, 1.1042f, 1.0888f, 1.0738f,
+                                    1.0592f, 1.0450f, 1.0318f, 1.0198f, 1.0154f, 1.0112f, 1.0072f, 1.0034f, 1.000f};
+    float temp2 = 0.0f; // the reference's DBL_MIN (1e-200) as a float
+    if (value < tstar[0]) temp2 = omega[0];
+    else if (value > tstar[26]) temp2 = omega[26];
+    else
+        for (int i = 1; i < 27; i++)
+            if (value < tstar[i]) {
+                const float temp1 = (value - tstar[i - 1]) / (tstar[i] - tstar[i - 1]);
+                temp2 = omega[i] * temp1 + omega[i - 1] * (1 - temp1);
+            }
+    return temp2;
+}
+
+// Sync_Fluid_GFCtoGFG_forDen (src/cuda_Fluid.cu:321-339): node (i, j) takes
+// cell (i, j)'s density; a cell of the last column or row also writes node
+// (i+1, j+1), as the reference does.
+void fluid_cells_to_nodes(const Setup &s, const std::vector<float> &cell, std::vector<float> &node) {
+    const int G = s.Gsize, C = s.Csize, ncy = s.ncy, ngy = s.ngy;
+    node.assign((size_t)s.nfsp * G, 0.0f);
     for (int f = 0; f < s.nfsp; f++)
-        for (int g = 0; g < G; g++)
-            if (s.dens_region[g]) s.fluid_den[(size_t)f * G + g] = s.fg[f].InitDens;
+        for (int i = 0; i < s.ncx; i++)
+            for (int j = 0; j < ncy; j++) {
+                const float v = cell[(size_t)f * C + i * ncy + j];
+                node[(size_t)f * G + i * ngy + j] = v;
+                if (i == s.ncx - 1 || j == ncy - 1) node[(size_t)f * G + (i + 1) * ngy + j + 1] = v;
+            }
+}
+
+// Fluid_Setting, Set_Con_Region and Set_Con_Boundary (src/Fluid.c:3-224),
+// then Set_Fluid_cuda's diffusion coefficients, Gummel coefficients and
+// initial fluxes (src/cuda_Fluid.cu:3-33,54-95,185-298).
+void fluid_setting(Setup &s) {
+    const int F = s.nfsp, C = s.Csize, ncx = s.ncx, ncy = s.ncy, ngy = s.ngy, ngx = s.ngx;
+    s.dtc = s.dt * (float)s.DT_CONTI; // src/Efield.c:8
+    s.fluid_cell_den.assign((size_t)F * C, 0.0f);
+    for (int f = 0; f < F; f++)
+        for (int i = 0; i < ncx; i++)
+            for (int j = 0; j < ncy; j++) {
+                const int c = i * ncy + j;
+                if (s.plasma_region[c] == 0) continue;
+                const float xx = (float)i * s.dx, yy = (float)j * s.dy;
+                float v = s.fg[f].InitDens;
+                if (s.fluid_loadtype == 1) {
+                    const float ax = (xx - s.fluid_x_center) / s.fluid_x_fall, ay = (yy - s.fluid_y_center) / s.fluid_y_fall;
+                    const float wv = (float)(::exp((double)(-1 * ax * ax)) * ::exp((double)(-1 * ay * ay)));
+                    v = s.fg[f].InitDens * wv;
+                } else if (s.fluid_loadtype == 2) {
+                    const float wv = (float)std::fabs(::cos((double)(xx - s.fluid_x_center) * MPI / 2 / s.fluid_x_fall) *
+                                                      ::cos((double)(yy - s.fluid_y_center) * MPI / 2 / s.fluid_y_fall));
+                    v = s.fg[f].InitDens * wv;
+                }
+                s.fluid_cell_den[(size_t)f * C + c] = v;
+            }
+    fluid_cells_to_nodes(s, s.fluid_cell_den, s.fluid_den);
+    // lines of consecutive plasma cells (PlasmaRegion 1): x lines row by row,
+    // y lines column by column
+    auto plasma = [&](int i, int j) { return s.plasma_region[(size_t)i * ncy + j] == 1; };
+    s.xl_x1.clear(); s.xl_x2.clear(); s.xl_yy.clear(); s.yl_xx.clear(); s.yl_y1.clear(); s.yl_y2.clear();
+    for (int j = 0; j < ncy; j++)
+        for (int i = 0; i < ncx; i++) {
+            if (!plasma(i, j)) continue;
+            if (i == 0 || !plasma(i - 1, j)) { s.xl_x1.push_back(i); s.xl_yy.push_back(j); }
+            if (i == ncx - 1 || !plasma(i + 1, j)) s.xl_x2.push_back(i);
+        }
+    for (int i = 0; i < ncx; i++)
+        for (int j = 0; j < ncy; j++) {
+            if (!plasma(i, j)) continue;
+            if (j == 0 || !plasma(i, j - 1)) { s.yl_xx.push_back(i); s.yl_y1.push_back(j); }
+            if (j == ncy - 1 || !plasma(i, j + 1)) s.yl_y2.push_back(j);
+        }
+    const int nx = (int)s.xl_x1.size(), ny = (int)s.yl_xx.size();
+    // wall factors: Gamma1 ("Quenching"), 0 on a Neumann wall of the domain
+    s.xl_fg1.assign((size_t)F * nx, 0.0f); s.xl_fg2.assign((size_t)F * nx, 0.0f);
+    s.yl_fg1.assign((size_t)F * ny, 0.0f); s.yl_fg2.assign((size_t)F * ny, 0.0f);
+    auto neu = [&](int g) { return s.boundary[g] == BC_NEUMANN; };
+    for (int f = 0; f < F; f++) {
+        const float g1 = s.fg[f].Gamma1;
+        for (int k = 0; k < nx; k++) {
+            const int x1 = s.xl_x1[k], x2 = s.xl_x2[k], yy = s.xl_yy[k];
+            const int a = x1 * ngy + yy, a1 = x1 * ngy + yy + 1, b = (x2 + 1) * ngy + yy, b1 = (x2 + 1) * ngy + yy + 1;
+            s.xl_fg1[(size_t)f * nx + k] = ((neu(a) || neu(a1)) && x1 == 0) ? 0.0f : g1;
+            s.xl_fg2[(size_t)f * nx + k] = ((neu(b) || neu(b1)) && x2 == ncx - 1) ? 0.0f : g1;
+        }
+        for (int k = 0; k < ny; k++) {
+            const int xx = s.yl_xx[k], y1 = s.yl_y1[k], y2 = s.yl_y2[k];
+            const int a = xx * ngy + y1, a1 = (xx + 1) * ngy + y1, b = xx * ngy + y2 + 1, b1 = (xx + 1) * ngy + y2 + 1;
+            s.yl_fg1[(size_t)f * ny + k] = ((neu(a) || neu(a1)) && y1 == 0) ? 0.0f : g1;
+            s.yl_fg2[(size_t)f * ny + k] = ((neu(b) || neu(b1)) && y2 == ncy - 1) ? 0.0f : g1;
+        }
+    }
+    // diffusion coefficients (Cal_D_Argon / Cal_D_Oxygen / Cal_D_ArO2) from
+    // the gas temperature of the cell's four nodes
+    s.fluid_D.assign((size_t)F * C, 0.0f);
+    const float P = s.total_pressure;
+    for (int f = 0; f < F; f++)
+        for (int i = 0; i < ncx; i++)
+            for (int j = 0; j < ncy; j++) {
+                const int g = i * ngy + j;
+                const float *T4 = s.node_temp.data();
+                const float T = (float)(0.25 * (double)(T4[g] + T4[g + 1] + T4[g + ngy] + T4[g + ngy + 1]));
+                double D;
+                if (s.main_gas == GAS_AR) {
+                    const float om = ar_meta_omega(T / 124.0f);
+                    D = 1.997279e-4 * ::sqrt((double)T / 39.948) * (double)T / (double)(P * 11.682724f * om) * 20;
+                } else {
+                    // the float square root of a float argument (the reference
+                    // is C++: sqrt(float) is the float overload); the
+                    // reference's sigma^2 constants are floats
+                    const double s0 = (double)0.08559f, s1 = (double)0.10892f, s2 = (double)0.08650f;
+                    if (s.main_gas == GAS_O2) {
+                        if (f <= 1) D = 2.63e-3 * (double)std::sqrt(T * T * T * 24 / 32 / 32) / (double)P * s2;
+                        else D = 2.63e-3 * (double)std::sqrt(T * T * T * 24 / 16 / 16) / (double)P * s1;
+                    } else {
+                        if (f == 0) D = 2.63e-3 * ::sqrt((double)(T * T * T * 24) / 39.948 / 39.948) / (double)P * s0;
+                        else if (f <= 2) D = 2.63e-3 * (double)std::sqrt(T * T * T * 24 / 32 / 32) / (double)P * s2;
+                        else D = 2.63e-3 * (double)std::sqrt(T * T * T * 24 / 16 / 16) / (double)P * s1;
+                    }
+                }
+                s.fluid_D[(size_t)f * C + i * ncy + j] = (float)D;
+            }
+    // Gummel coefficients (calculate_gummel_coef_x/_y; the x interior face
+    // averages D[i-1] with itself, as the reference writes it)
+    s.gax.assign((size_t)F * ngx * ncy, 0.0f); s.gbx.assign((size_t)F * ngx * ncy, 0.0f);
+    s.gay.assign((size_t)F * ncx * ngy, 0.0f); s.gby.assign((size_t)F * ncx * ngy, 0.0f);
+    for (int f = 0; f < F; f++) {
+        float *ax = &s.gax[(size_t)f * ngx * ncy], *bx = &s.gbx[(size_t)f * ngx * ncy];
+        float *ay = &s.gay[(size_t)f * ncx * ngy], *by = &s.gby[(size_t)f * ncx * ngy];
+        const float *D = &s.fluid_D[(size_t)f * C];
+        const double m = (double)s.fg[f].mass;
+        for (int k = 0; k < nx; k++) {
+            const int x1 = s.xl_x1[k], x2 = s.xl_x2[k], yy = s.xl_yy[k];
+            const double fg1 = s.xl_fg1[(size_t)f * nx + k], fg2 = s.xl_fg2[(size_t)f * nx + k];
+            bx[x1 * ncy + yy] = (float)(-fg1 * (-0.25 * ::sqrt((double)s.node_temp[x1 * ngy + yy] * 1.38e-23 / m)));
+            ax[x1 * ncy + yy] = 0;
+            for (int i = x1 + 1; i <= x2; i++) {
+                ax[i * ncy + yy] = (D[(i - 1) * ncy + yy] + D[(i - 1) * ncy + yy]) / 2 / s.dx;
+                bx[i * ncy + yy] = ax[i * ncy + yy];
+            }
+            ax[(x2 + 1) * ncy + yy] = (float)(fg2 * (0.25 * ::sqrt((double)s.node_temp[x2 * ngy + yy] * 1.38e-23 / m)));
+            bx[(x2 + 1) * ncy + yy] = 0;
+        }
+        for (int k = 0; k < ny; k++) {
+            const int xx = s.yl_xx[k], y1 = s.yl_y1[k], y2 = s.yl_y2[k];
+            const double fg1 = s.yl_fg1[(size_t)f * ny + k], fg2 = s.yl_fg2[(size_t)f * ny + k];
+            by[xx * ngy + y1] = (float)(-fg1 * (-0.25 * ::sqrt((double)s.node_temp[xx * ngy + y1] * 1.38e-23 / m)));
+            ay[xx * ngy + y1] = 0;
+            for (int j = y1 + 1; j <= y2; j++) {
+                ay[xx * ngy + j] = (D[xx * ncy + j - 1] + D[xx * ncy + j]) / 2 / s.dy;
+                by[xx * ngy + j] = ay[xx * ngy + j];
+            }
+            ay[xx * ngy + y2 + 1] = (float)(fg2 * (0.25 * ::sqrt((double)s.node_temp[xx * ngy + y2] * 1.38e-23 / m)));
+            by[xx * ngy + y2 + 1] = 0;
+        }
+    }
+    // tally -> rate factors (Average_Argon/Oxygen/ArO2_MCC_rate): channel
+    // ranges scaled by Denscale / N_ave / dt of their projectile, a few
+    // single channels by Denscale x (1 / N_ave / dt), as the reference groups
+    // the float operations
+    s.fluid_rate_f.assign((size_t)std::max(s.TnRct, 1), 0.0f);
+    auto range = [&](int a, int b, int sp) {
+        const float t = s.sp[sp].Denscale / (float)s.N_ave / s.dt;
+        for (int k = a; k <= b && k < s.TnRct; k++) s.fluid_rate_f[k] = t;
+    };
+    auto single = [&](int k, int sp) {
+        const float t = 1 / (float)s.N_ave / s.dt;
+        if (k < s.TnRct) s.fluid_rate_f[k] = s.sp[sp].Denscale * t;
+    };
+    if (s.main_gas == GAS_AR) {
+        range(0, 6, 0);
+        range(8, 8, 0);
+    } else if (s.main_gas == GAS_O2) {
+        range(0, 40, 0); range(41, 46, 3); range(47, 52, 1); range(53, 57, 2);
+        single(58, 3);
+    } else {
+        range(0, 45, 0); range(46, 51, 4); range(52, 59, 2); range(60, 64, 3); range(65, 67, 1);
+        single(69, 3); single(70, 3); single(79, 1); single(80, 1); single(81, 0);
+    }
+    // initial fluxes (Calculate_Flux_x/_y of Set_Fluid_cuda)
+    s.flux_x0.assign((size_t)F * ngx * ncy, 0.0f);
+    s.flux_y0.assign((size_t)F * ncx * ngy, 0.0f);
+    for (int f = 0; f < F; f++) {
+        const float *ax = &s.gax[(size_t)f * ngx * ncy], *bx = &s.gbx[(size_t)f * ngx * ncy];
+        const float *ay = &s.gay[(size_t)f * ncx * ngy], *by = &s.gby[(size_t)f * ncx * ngy];
+        const float *den = &s.fluid_cell_den[(size_t)f * C];
+        float *fx = &s.flux_x0[(size_t)f * ngx * ncy], *fy = &s.flux_y0[(size_t)f * ncx * ngy];
+        for (int k = 0; k < nx; k++) {
+            const int x1 = s.xl_x1[k], x2 = s.xl_x2[k], yy = s.xl_yy[k];
+            fx[x1 * ncy + yy] = -s.xl_fg1[(size_t)f * nx + k] * bx[x1 * ncy + yy] * den[x1 * ncy + yy];
+            for (int i = x1 + 1; i <= x2; i++)
+                fx[i * ncy + yy] = ax[i * ncy + yy] * den[(i - 1) * ncy + yy] - bx[i * ncy + yy] * den[i * ncy + yy];
+            fx[(x2 + 1) * ncy + yy] = s.xl_fg2[(size_t)f * nx + k] * ax[(x2 + 1) * ncy + yy] * den[x2 * ncy + yy];
+        }
+        for (int k = 0; k < ny; k++) {
+            const int xx = s.yl_xx[k], y1 = s.yl_y1[k], y2 = s.yl_y2[k];
+            fy[xx * ngy + y1] = -s.yl_fg1[(size_t)f * ny + k] * by[xx * ngy + y1] * den[xx * ncy + y1];
+            for (int j = y1 + 1; j <= y2; j++)
+                fy[xx * ngy + j] = ay[xx * ngy + j] * den[xx * ncy + j - 1] - by[xx * ngy + j] * den[xx * ncy + j];
+            fy[xx * ngy + y2 + 1] = s.yl_fg2[(size_t)f * ny + k] * ay[xx * ngy + y2 + 1] * den[xx * ncy + y2];
+        }
+    }
 }
 
 // ---------------------------------------------------------------- species + load
@@ -1226,6 +1435,7 @@ void build_setup(const char *json, size_t len, const BuildOpts &o, Setup &s) {
     gas_setting(s, o);
     null_collision(s);
     laplace_and_gas(s, o.gas_temp_mode);
+    fluid_setting(s);
 }
 
 } // namespace hp

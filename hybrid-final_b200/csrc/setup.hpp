@@ -113,9 +113,29 @@ struct Setup {
     std::vector<float> sigv;        // sigma-v max per target
     int mcc_n = 1;                  // DT_MCCn
     float dt_mcc = 0;
-    std::vector<float> fluid_den;   // [nfsp * Gsize] metastable/radical densities (constant here)
+    std::vector<float> fluid_den;   // [nfsp * Gsize] metastable/radical densities at the nodes (MCC input)
     std::vector<float> vsave;       // Maxwellian speed table (src/Particle.c:176-210)
     int nvel = 0;
+
+    // --- continuity solve of the fluid species (src/Fluid.c:3-256, src/cuda_Fluid.cu:3-349) ---
+    int DT_CONTI = 1;
+    float dtc = 0;                  // dt * TimeStep_Conti (src/Efield.c:8)
+    int fluid_loadtype = 0;         // the neutral species' load (uniform, exponential, cosine)
+    float fluid_x_center = 0, fluid_x_fall = 0, fluid_y_center = 0, fluid_y_fall = 0;
+    std::vector<float> fluid_cell_den;  // [nfsp * Csize] initial density per cell
+    // lines of plasma cells: x lines (x1, x2, yy) and y lines (xx, y1, y2)
+    // with the wall factors fg1, fg2 of each species ([nfsp * lines])
+    std::vector<int> xl_x1, xl_x2, xl_yy, yl_xx, yl_y1, yl_y2;
+    std::vector<float> xl_fg1, xl_fg2, yl_fg1, yl_fg2;
+    std::vector<float> fluid_D;     // [nfsp * Csize] diffusion coefficient
+    // Gummel coefficients: x faces [nfsp][ngx*ncy] at i*ncy + j (i in 0..ncx),
+    // y faces [nfsp][ncx*ngy] at i*ngy + j (j in 0..ncy)
+    std::vector<float> gax, gbx, gay, gby;
+    std::vector<float> flux_x0, flux_y0; // initial fluxes (Set_Fluid_cuda)
+    // per reaction channel: the factor that turns a channel's tally over one
+    // averaging window into a rate (m^-3 s^-1), as Average_*_MCC_rate
+    // (src/cuda_Diagnostic.cu:548-633) scales by the projectile's Denscale
+    std::vector<float> fluid_rate_f;    // [TnRct]
 
     // --- initial particles (src/Particle.c:3-175), cell-sorted ---
     std::vector<int> p_count[MAXSP];                       // [Csize]

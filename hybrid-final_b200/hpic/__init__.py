@@ -33,9 +33,12 @@ TABLE = dict(sidx=0, a_idx=1, boundary=2, face=3, cond_id=4, area=5, back_den1=6
              stencil=9, vsave=10, xsec=11, collf=12, sigv=13, dens_region=14, prob=15, eps_r=16,
              back_den2=17, back_vel2=18, a_val=19, ai=20, aj=21, matm=22, cond_b=23, temp_b=24, ta_val=25,
              species=26, node_temp=27, dep_factor=28, fluid_den=29, scalars=30, sources=31, unk_node=32,
-             fs_info=33, fs_V=34, fs_Vt=35, fs_W=36, fs_Wt=37, fs_inv=38, sig_mode=39, power=40)
+             fs_info=33, fs_V=34, fs_Vt=35, fs_W=36, fs_Wt=37, fs_inv=38, sig_mode=39, power=40,
+             fluid_cell_den=41, fluid_xlines=42, fluid_ylines=43, fluid_xl_fg=44, fluid_yl_fg=45, fluid_gax=46,
+             fluid_gbx=47, fluid_gay=48, fluid_gby=49, fluid_flux_x0=50, fluid_flux_y0=51, fluid_D=52,
+             fluid_scalars=53, fluid_rate_f=54, plasma_region=55)
 TABLE_DTYPE = {0: np.int32, 1: np.int32, 2: np.int32, 3: np.int32, 4: np.int32, 14: np.int32, 20: np.int32,
-               21: np.int32, 32: np.int32, 33: np.int32, 39: np.int32}
+               21: np.int32, 32: np.int32, 33: np.int32, 39: np.int32, 42: np.int32, 43: np.int32, 55: np.int32}
 
 
 class HpicError(RuntimeError):

@@ -21,6 +21,7 @@
 #include <array>
 #include <thread>
 
+#include "hp_fluid.h"
 #include "hp_math.h"
 #include "hp_rng.h"
 #include "hpic.h"
@@ -129,6 +130,156 @@ struct SimBase {
         }
         return script.u[(size_t)(script.start[key] + p++)];
     }
+    // ------------------------------------------------------------ fluid species
+    // The continuity solve of the metastable / radical densities
+    // (Solve_Continuity_eqn, src/cuda_Fluid.cu:34-167) and the diagnostic
+    // cycle that feeds it (Diagnostic_Basic, src/cuda_Diagnostic.cu:268-330):
+    // every n_ave + 1 steps the electron density and the collision tallies
+    // are averaged into sources; from the first such step on the densities
+    // are copied to the nodes (the MCC's input) each step, and from the next
+    // one the continuity solve runs each step.  All in float as the reference.
+    std::vector<float> fden, fsrc, fflx, ffly, fnode, prob_v, f_gam, f_x;
+    std::vector<double> sum_den_e;
+    std::vector<unsigned> fl_base;
+    void fluid_init() {
+        const size_t F = (size_t)c.nfsp, ngx = c.ngx, ncy = c.ncy, ncx = c.ncx, ngy = c.ngy;
+        fden.assign(c.fluid_cell_den, c.fluid_cell_den + F * C);
+        fsrc.assign(F * C, 0.0f);
+        fflx.assign(c.flux_x0, c.flux_x0 + F * ngx * ncy);
+        ffly.assign(c.flux_y0, c.flux_y0 + F * ncx * ngy);
+        fnode.assign(c.fluid_den, c.fluid_den + F * G);
+        prob_v.assign(c.prob, c.prob + 3 * (size_t)C);
+        f_gam.assign(F * C, 0.0f);
+        f_x.assign(F * C, 0.0f);
+        sum_den_e.assign(G, 0.0);
+        fl_base.assign((size_t)(c.mcc_stride > 0 ? c.mcc_stride : 8) * C, 0u);
+    }
+    // tridiag (src/cuda_Fluid.cu:168-184); false where a pivot vanishes
+    static bool tridiag(const float *a, const float *b, const float *cc, const float *d, float *x, float *gam, int n) {
+        float bet;
+        x[0] = d[0] / (bet = b[0]);
+        for (int j = 1; j < n; j++) {
+            gam[j - 1] = cc[j - 1] / bet;
+            bet = b[j] - a[j] * cc[j - 1] / bet;
+            x[j] = (d[j] - a[j] * x[j - 1]) / bet;
+            if (bet == 0) return false;
+        }
+        for (int j = n - 2; j >= 0; j--) x[j] -= gam[j] * x[j + 1];
+        return true;
+    }
+    // Solve_Density_x + Calculate_Flux_x of one species (dir 0), or the y
+    // pair (dir 1), line by line
+    void fluid_sweep(int f, int dir) {
+        const int ngx = c.ngx, ngy = c.ngy, ncx = c.ncx, ncy = c.ncy;
+        const int nl = dir ? c.nyl : c.nxl;
+        const int *L = dir ? c.yl : c.xl;
+        const float *fg = dir ? c.yl_fg : c.xl_fg;
+        const float *A = dir ? c.gay : c.gax, *B = dir ? c.gby : c.gbx;
+        const size_t fo = dir ? (size_t)f * ncx * ngy : (size_t)f * ngx * ncy; // face arrays
+        const float *ga_ = A + fo, *gb_ = B + fo;
+        float *flux = (dir ? ffly.data() : fflx.data()) + fo;
+        const float *other = (dir ? fflx.data() + (size_t)f * ngx * ncy : ffly.data() + (size_t)f * ncx * ngy);
+        float *den = fden.data() + (size_t)f * C;
+        const float *src = fsrc.data() + (size_t)f * C;
+        const float dtc = c.dtc, del_f = dtc / (dir ? c.dy : c.dx), dother = dir ? c.dx : c.dy;
+        std::vector<float> a, b, cc, d, x, gam;
+        for (int k = 0; k < nl; k++) {
+            const int p = L[3 * k], lo = L[3 * k + 1], hi = L[3 * k + 2]; // x: x1, x2, yy; y: xx, y1, y2
+            const int first = dir ? lo : p, last = dir ? hi : lo, fixed = dir ? p : hi;
+            const int num = last - first + 1;
+            a.assign(num, 0); b.assign(num, 0); cc.assign(num, 0); d.assign(num, 0); x.assign(num, 0); gam.assign(num, 0);
+            // face index of position q along the line, cell index of q
+            auto face = [&](int q) { return dir ? fixed * ngy + q : q * ncy + fixed; };
+            auto cell = [&](int q) { return dir ? fixed * ncy + q : q * ncy + fixed; };
+            // the other direction's two faces of cell q: an x sweep reads the y
+            // faces (q, fixed) and (q, fixed + 1), a y sweep the x faces
+            // (fixed, q) and (fixed + 1, q)
+            auto olo = [&](int q) { return dir ? fixed * ncy + q : q * ngy + fixed; };
+            auto ohi = [&](int q) { return dir ? (fixed + 1) * ncy + q : q * ngy + fixed + 1; };
+            for (int i = 0; i < num; i++) {
+                const int q = i + first;
+                a[i] = -ga_[face(q)] * del_f;
+                b[i] = 1 + (ga_[face(q + 1)] + gb_[face(q)]) * del_f;
+                cc[i] = -gb_[face(q + 1)] * del_f;
+                d[i] = den[cell(q)] + src[cell(q)] * dtc - (other[ohi(q)] - other[olo(q)]) * dtc / dother;
+            }
+            if (!tridiag(a.data(), b.data(), cc.data(), d.data(), x.data(), gam.data(), num)) continue;
+            for (int i = 0; i < num; i++) {
+                const int q = i + first;
+                den[cell(q)] = (c.plasma[cell(q)] == 1 && x[i] > 1e9f) ? x[i] : 0.0f;
+            }
+            const float fg1 = fg[(size_t)f * nl + k], fg2 = fg[(size_t)c.nfsp * nl + (size_t)f * nl + k];
+            flux[face(first)] = -fg1 * gb_[face(first)] * den[cell(first)];
+            for (int q = first + 1; q <= last; q++)
+                flux[face(q)] = ga_[face(q)] * den[cell(q - 1)] - gb_[face(q)] * den[cell(q)];
+            flux[face(last + 1)] = fg2 * ga_[face(last + 1)] * den[cell(last)];
+        }
+    }
+    void fluid_sweeps() {
+        for (int f = 0; f < c.nfsp; f++) {
+            fluid_sweep(f, 0);
+            fluid_sweep(f, 1);
+        }
+    }
+    // the diagnostic cycle of step t (1-based): accumulate, or average into
+    // sources; then, once the first average is in, the node copy (and the Ar
+    // collision probability that reads it)
+    void fluid_diag(int64_t t, const double *den_e) {
+        const int N = c.n_ave;
+        const int64_t per = (int64_t)N + 1;
+        const int ph = (int)((t - 1) % per);
+        const int st = c.mcc_stride > 0 ? c.mcc_stride : 8;
+        if (ph < N) {
+            for (int g = 0; g < G; g++) sum_den_e[g] += den_e[g];
+        } else {
+            const float temp = c.denscale0 / (float)N;
+            std::vector<float> R(96), S(5);
+            float nn[5];
+            for (int g = 0; g < G; g++) {
+                const int i = g / c.ngy, j = g - i * c.ngy;
+                const bool has_cell = i < c.ncx && j < c.ncy;
+                const int cell = i * c.ncy + j;
+                const float ave = temp * (float)(sum_den_e[g] + den_e[g]);
+                sum_den_e[g] = 0.0;
+                const float eden = (float)(0.25 * (double)ave);
+                std::fill(R.begin(), R.end(), 0.0f);
+                if (has_cell)
+                    for (int ch = 0; ch < st && ch < c.tnrct; ch++) {
+                        const unsigned now = mcc_count[(size_t)cell * st + ch];
+                        R[ch] = c.rate_f[ch] * (float)(now - fl_base[(size_t)cell * st + ch]);
+                        fl_base[(size_t)cell * st + ch] = now;
+                    }
+                for (int f = 0; f < 5; f++) nn[f] = f < c.nfsp ? fnode[(size_t)f * G + g] : 0.0f;
+                const float bd1 = c.back_den1 ? c.back_den1[g] : 0.0f, bd2 = c.back_den2 ? c.back_den2[g] : 0.0f;
+                hp_fluid_sources(c.gas, R.data(), nn, bd1, bd2, eden, c.rr, S.data());
+                if (has_cell)
+                    for (int f = 0; f < c.nfsp; f++) fsrc[(size_t)f * C + cell] = S[f];
+            }
+        }
+        if (t >= per) fluid_sync();
+    }
+    void fluid_sync() {
+        const int ncy = c.ncy, ngy = c.ngy;
+        for (int f = 0; f < c.nfsp; f++)
+            for (int i = 0; i < c.ncx; i++)
+                for (int j = 0; j < ncy; j++) {
+                    const float v = fden[(size_t)f * C + i * ncy + j];
+                    fnode[(size_t)f * G + i * ngy + j] = v;
+                    if (i == c.ncx - 1 || j == ncy - 1) fnode[(size_t)f * G + (i + 1) * ngy + j + 1] = v;
+                }
+        if (c.gas == 0)
+            for (int cell = 0; cell < C; cell++) {
+                const int i = cell / ncy, j = cell - i * ncy, node = i * ngy + j;
+                const float e = hp_expf(-1 * c.dt_mcc * c.sigv[1] * fnode[node]);
+                prob_v[(size_t)C + cell] = prob_v[cell] + 1.0f - e;
+            }
+    }
+    void fluid(int64_t t, const double *den_e) {
+        if (!c.fluid_on || c.nfsp <= 0) return;
+        if (t >= (int64_t)c.n_ave + 2) fluid_sweeps();
+        fluid_diag(t, den_e);
+    }
+    virtual void fluid_step(int64_t t) = 0;
     virtual void power(int64_t tstep) = 0;
     int64_t ave_count = 0;
     bool walk_bound_hit = false; // a walk that reached its crossing bound
@@ -202,7 +353,9 @@ template <class R> struct Sim : SimBase {
         cond_step.assign((size_t)c.nsp * c.cond_numr, 0u);
         for (int n = 0; n < G; n++)
             if (c.cond_id[n]) cond_list.push_back(n);
+        fluid_init();
     }
+    void fluid_step(int64_t t) override { fluid(t, den.data()); }
 
     // ------------------------------------------------------------ state
     void set_particles(int s, const int *counts, const float *x, const float *y, const float *vx, const float *vy,
@@ -261,6 +414,11 @@ template <class R> struct Sim : SimBase {
         case 8: std::memcpy(out, sig.data(), sig.size() * 8); break;
         case 9: std::memcpy(d, sigma.data(), sigma.size() * 8); break;
         case 10: std::memcpy(f, src_amp.data(), src_amp.size() * 4); break;
+        case 11: std::memcpy(f, fden.data(), fden.size() * 4); break;
+        case 12: std::memcpy(f, fnode.data(), fnode.size() * 4); break;
+        case 13: std::memcpy(f, fsrc.data(), fsrc.size() * 4); break;
+        case 14: std::memcpy(f, fflx.data(), fflx.size() * 4); break;
+        case 15: std::memcpy(f, ffly.data(), ffly.size() * 4); break;
         }
     }
     void set_grid(int which, const void *in) override {
@@ -280,6 +438,11 @@ template <class R> struct Sim : SimBase {
             break;
         case 8: std::memcpy(sig.data(), in, sig.size() * 8); break;
         case 9: std::memcpy(sigma.data(), d, sigma.size() * 8); break;
+        case 11: std::memcpy(fden.data(), f, fden.size() * 4); break;
+        case 12: std::memcpy(fnode.data(), f, fnode.size() * 4); break;
+        case 13: std::memcpy(fsrc.data(), f, fsrc.size() * 4); break;
+        case 14: std::memcpy(fflx.data(), f, fflx.size() * 4); break;
+        case 15: std::memcpy(ffly.data(), f, ffly.size() * 4); break;
         }
     }
 
@@ -1018,8 +1181,8 @@ template <class R> struct Sim : SimBase {
         par_for(C, [&](int cell) {
             const int i = cell / c.ncy, j = cell - i * c.ncy, node = i * c.ngy + j, Gn = G;
             const R bd1 = c.back_den1[node], bd2 = aro2 ? (R)c.back_den2[node] : (R)0;
-            const R F0 = c.fluid_den[node], F1 = c.fluid_den[Gn + node], F2 = c.fluid_den[2 * Gn + node];
-            const R F3 = c.fluid_den[3 * Gn + node], F4 = aro2 ? (R)c.fluid_den[4 * Gn + node] : (R)0;
+            const R F0 = fnode[node], F1 = fnode[Gn + node], F2 = fnode[2 * Gn + node];
+            const R F3 = fnode[3 * Gn + node], F4 = aro2 ? (R)fnode[4 * Gn + node] : (R)0;
             auto xe = [&](R a, R b, R n) { return ox_exp(-1 * a * b * n); };
             auto nq = [&](int s, R sig, R dtx) {
                 R t = -1 * dtx;
@@ -1226,7 +1389,7 @@ template <class R> struct Sim : SimBase {
         std::vector<std::vector<R>> enew(C), inew(C); // created particles: x,y,vx,vy,vz
         par_for(C, [&](int cell) {
             const int i = cell / c.ncy, j = cell - i * c.ncy, node = i * c.ngy + j;
-            const float P1 = c.prob[cell], P2 = c.prob[C + cell], Pion = c.prob[2 * C + cell];
+            const float P1 = prob_v[cell], P2 = prob_v[C + cell], Pion = prob_v[2 * C + cell];
             const R bvel = c.back_vel1[node];
             unsigned cnt_ch[7] = {0, 0, 0, 0, 0, 0, 0};
             const int ni = ion.cnt[cell];
@@ -1996,6 +2159,9 @@ int or_collide_oxy(or_sim *s, int isp, int t, const float *v, float bv1, float b
                    int pair_rl, int *ch, int *keep, float *vout, int *bsp, float *bv, int *kill) {
     return s->impl->collide_oxy(isp, t, v, bv1, bv2, u, nu, pair_rl, ch, keep, vout, bsp, bv, kill);
 }
+void or_fluid_sweeps(or_sim *s, int nsteps) {
+    for (int k = 0; k < nsteps; k++) s->impl->fluid_sweeps();
+}
 void or_field(or_sim *s, int64_t tstep) { s->impl->field(tstep); }
 void or_move(or_sim *s) { s->impl->move(); }
 void or_sort(or_sim *s) { s->impl->sort(); }
@@ -2010,6 +2176,7 @@ void or_run(or_sim *s, int64_t tstep0, int nsteps, int accumulate) {
         s->impl->sort();
         s->impl->mcc(t);
         s->impl->deposit(true);
+        s->impl->fluid_step(t);
         if (accumulate) {
             s->impl->accumulate();
             const int ev = s->impl->c.eedf_every;

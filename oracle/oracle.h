@@ -61,7 +61,7 @@ typedef struct or_case {
     int gas, mcc_stride, mcc_all_species;
     int eedf_every; /* electron energy histogram every k-th step in or_run with accumulation (0 off) */
     float dt_mcc, np2c[5];
-    const float *back_den1, *back_den2, *back_vel2, *fluid_den;
+    const float *back_den1, *back_den2, *back_vel2;
     /* 1-2-1 density smoothing in Deposit (DensitySmoothing passes) */
     int n_smt;
     const int *dens_region; /* [G] */
@@ -75,6 +75,19 @@ typedef struct or_case {
     int cond_src_num[8], cond_power_id[8];
     int pd_intv;
     float pd_ratio;
+    /* fluid species: the continuity solve (src/cuda_Fluid.cu) and its sources
+     * (src/cuda_Diagnostic.cu:548-743); fluid_on 0 holds the densities at
+     * their initial values */
+    int nfsp, fluid_on, n_ave, nxl, nyl, tnrct;
+    float dtc, denscale0;
+    const float *fluid_cell_den;        /* [nfsp*C] initial density per cell */
+    const float *fluid_den;             /* [nfsp*G] initial density per node (MCC input) */
+    const int *xl, *yl;                 /* [3*nxl] x1, x2, yy; [3*nyl] xx, y1, y2 */
+    const float *xl_fg, *yl_fg;         /* [2*nfsp*nxl]: fg1 block, then fg2 block (same for y) */
+    const float *gax, *gbx, *gay, *gby; /* [nfsp*ngx*ncy], [nfsp*ncx*ngy] Gummel coefficients */
+    const float *flux_x0, *flux_y0;     /* initial fluxes, same layouts */
+    const int *plasma;                  /* [C] PlasmaRegion */
+    float rate_f[96], rr[96];           /* rate factor per channel (tally -> m^-3 s^-1), CollF.RR */
 } or_case;
 
 typedef struct or_sim or_sim;
@@ -94,7 +107,9 @@ void or_get_movers(or_sim *s, int isp, int *counts, float *x, float *y, float *v
 /* node fields: which 0 Ex, 1 Ey, 2 phi, 3 phi_pois (float[G]); 4 den (double[nsp*G]);
  * 5 source (double[G]); 6 b (double[G]); 7 x (double[G]);
  * 8 dielectric surface weights (int64[nsp*G], HP_SIGMA_FRAC_BITS fraction bits); 9 Sigma (double[G]);
- * 10 AC amplitudes in use (float[src_num]) */
+ * 10 AC amplitudes in use (float[src_num]); 11 fluid density per cell (float[nfsp*C]); 12 fluid density
+ * per node (float[nfsp*G]); 13 fluid source per cell (float[nfsp*C]); 14 fluid x fluxes
+ * (float[nfsp*ngx*ncy]); 15 fluid y fluxes (float[nfsp*ncx*ngy]) */
 void or_get_grid(or_sim *s, int which, void *out);
 void or_set_grid(or_sim *s, int which, const void *in);
 void or_get_counters(or_sim *s, float *cond_charge, unsigned *mcc_count, int *pcg_iters);
@@ -147,6 +162,9 @@ void or_kinematics(or_sim *s, int kind, const float *in, float *out, int n);
  * when the list ran out. */
 int or_collide_oxy(or_sim *s, int isp, int t, const float *v, float bv1, float bv2, const float *u, int nu,
                    int pair_rl, int *ch, int *keep, float *vout, int *bsp, float *bv, int *kill);
+/* only the continuity solve (src/cuda_Fluid.cu:34-42), nsteps times, with
+ * the fluid sources of grid 13 as they are */
+void or_fluid_sweeps(or_sim *s, int nsteps);
 int or_num_threads(void);
 void or_set_threads(int n);
 

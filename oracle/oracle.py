@@ -42,11 +42,16 @@ class OrCase(C.Structure):
         ("gas", C.c_int), ("mcc_stride", C.c_int), ("mcc_all_species", C.c_int), ("eedf_every", C.c_int),
         ("dt_mcc", C.c_float),
         ("np2c", C.c_float * 5),
-        ("back_den1", _F), ("back_den2", _F), ("back_vel2", _F), ("fluid_den", _F),
+        ("back_den1", _F), ("back_den2", _F), ("back_vel2", _F),
         ("n_smt", C.c_int), ("dens_region", _I),
         ("n_diel", C.c_int), ("sig_mode", _I), ("area", _F),
         ("n_power", C.c_int), ("src_power", C.c_float * 8), ("cond_src_num", C.c_int * 8),
         ("cond_power_id", C.c_int * 8), ("pd_intv", C.c_int), ("pd_ratio", C.c_float),
+        ("nfsp", C.c_int), ("fluid_on", C.c_int), ("n_ave", C.c_int), ("nxl", C.c_int), ("nyl", C.c_int),
+        ("tnrct", C.c_int), ("dtc", C.c_float), ("denscale0", C.c_float),
+        ("fluid_cell_den", _F), ("fluid_den", _F), ("xl", _I), ("yl", _I), ("xl_fg", _F), ("yl_fg", _F),
+        ("gax", _F), ("gbx", _F), ("gay", _F), ("gby", _F), ("flux_x0", _F), ("flux_y0", _F), ("plasma", _I),
+        ("rate_f", C.c_float * 96), ("rr", C.c_float * 96),
     ]
 
 
@@ -94,6 +99,7 @@ def lib():
             "or_kinematics": (None, [P, C.c_int, _F, _F, C.c_int]),
             "or_collide_oxy": (C.c_int, [P, C.c_int, C.c_int, _F, C.c_float, C.c_float, _F, C.c_int, C.c_int, _I,
                                          _I, _F, _I, _F, _I]),
+            "or_fluid_sweeps": (None, [P, C.c_int]),
             "or_num_threads": (C.c_int, []),
             "or_set_threads": (None, [C.c_int]),
         }
@@ -117,7 +123,8 @@ class Oracle:
     """CPU restatement of one case.  `tables` is a callable name -> array
     (hpic.Case.table or hpic.Setup.table); `info` the case info."""
 
-    GRID = dict(EX=0, EY=1, PHI=2, PHI_POIS=3, DEN=4, SOURCE=5, B=6, X=7, SURFACE_CHARGE=8, SIGMA=9, SOURCE_AC=10)
+    GRID = dict(EX=0, EY=1, PHI=2, PHI_POIS=3, DEN=4, SOURCE=5, B=6, X=7, SURFACE_CHARGE=8, SIGMA=9, SOURCE_AC=10,
+                FLUID_CELL_DEN=11, FLUID_DEN=12, FLUID_SOURCE=13, FLUID_FLUX_X=14, FLUID_FLUX_Y=15)
 
     def __init__(self, tables, info, opts, precision=32, pcg_cluster=1, pcg_block=512, field_mode=None,
                  fs_passes=None):
@@ -168,11 +175,29 @@ class Oracle:
         c.dt_mcc = sc[1]
         for s in range(info.nsp):
             c.np2c[s] = spc[s, 0]
+        c.back_den1 = keep("bd1", t("back_den1"), np.float32)
         if info.main_gas != 0:
-            c.back_den1 = keep("bd1", t("back_den1"), np.float32)
             c.back_den2 = keep("bd2", t("back_den2"), np.float32)
             c.back_vel2 = keep("bv2", t("back_vel2"), np.float32)
-            c.fluid_den = keep("fd", t("fluid_den"), np.float32)
+        # fluid species: the continuity solve and its sources
+        fs = t("fluid_scalars")
+        c.dtc, c.n_ave, c.nfsp, c.nxl, c.nyl = fs[0], int(fs[1]), int(fs[3]), int(fs[4]), int(fs[5])
+        c.fluid_on = 0 if getattr(opts, "fluid_fixed", 0) else 1
+        c.tnrct = info.n_reactions
+        c.denscale0 = spc[0, 8]
+        c.fluid_cell_den = keep("fcd", t("fluid_cell_den"), np.float32)
+        c.fluid_den = keep("fd", t("fluid_den"), np.float32)
+        c.xl = keep("xl", t("fluid_xlines"), np.int32)
+        c.yl = keep("yl", t("fluid_ylines"), np.int32)
+        c.xl_fg = keep("xlfg", t("fluid_xl_fg"), np.float32)
+        c.yl_fg = keep("ylfg", t("fluid_yl_fg"), np.float32)
+        for k in ("gax", "gbx", "gay", "gby", "flux_x0", "flux_y0"):
+            setattr(c, k, keep(k, t("fluid_" + k), np.float32))
+        c.plasma = keep("plasma", t("plasma_region"), np.int32)
+        rf = t("fluid_rate_f")
+        for k in range(min(96, rf.size)):
+            c.rate_f[k] = rf[k]
+            c.rr[k] = collf[k, 3]
         c.n_smt = info.n_smt
         c.dens_region = keep("dr", t("dens_region"), np.int32)
         c.n_diel = info.n_dielectric
@@ -279,7 +304,11 @@ class Oracle:
     def grid(self, name):
         G, nsp = self.info.Gsize, self.info.nsp
         w = self.GRID[name]
-        if w <= 3:
+        if w >= 11:
+            nf, info = int(self.c.nfsp), self.info
+            n = {11: nf * info.Csize, 12: nf * G, 13: nf * info.Csize, 14: nf * info.ngx * info.ncy, 15: nf * info.ncx * info.ngy}[w]
+            out = np.zeros(n, np.float32)
+        elif w <= 3:
             out = np.zeros(G, np.float32)
         elif w == 4:
             out = np.zeros(nsp * G, np.float64)
@@ -294,7 +323,7 @@ class Oracle:
 
     def set_grid(self, name, arr):
         w = self.GRID[name]
-        dt = np.float32 if w <= 3 else np.int64 if w == 8 else np.float64
+        dt = np.float32 if (w <= 3 or w >= 11) else np.int64 if w == 8 else np.float64
         a = np.ascontiguousarray(arr, dtype=dt)
         lib().or_set_grid(self.h, w, a.ctypes.data_as(C.c_void_p))
 
@@ -387,6 +416,10 @@ class Oracle:
                                     int(pair_rl), C.byref(ch), C.byref(keep), _fp(vout), _ip(bsp), _fp(bv),
                                     C.byref(kill))
         return ch.value, bool(keep.value), vout, bsp, bv.reshape(2, 3), bool(kill.value), bool(over)
+
+    def fluid_sweeps(self, nsteps):
+        """The continuity solve alone, nsteps times, with the current sources."""
+        lib().or_fluid_sweeps(self.h, nsteps)
 
     def averages(self):
         G, nsp = self.info.Gsize, self.info.nsp

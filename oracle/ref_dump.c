@@ -18,7 +18,12 @@
  * The call order is the reference main()'s (src/main.c:43-49).  The random seed
  * that main() takes from getpid() (src/main.c:43) is a command-line argument here.
  *
- * usage: ref_dump <deck.json> <seed> <outdir>
+ * usage: ref_dump <deck.json> <seed> <outdir> [<temps.bin> [<src.bin> <nsteps>]]
+ *
+ * With temps.bin (float[Gsize], the gas temperature of every node) the
+ * reference's fluid set-up and continuity solve also run (rf_fluid in
+ * ref_fluid.cu); with src.bin (float[nfsp*Csize]) the solve takes nsteps
+ * steps with those sources.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -42,7 +47,7 @@ extern int CondNUM, CondNUMR, SrcNUM, DielNUM;
 extern int *SrcM_ID;
 extern float *SrcDC, *SrcAC, *SrcFREQ, *SrcPHASE, *SrcRPHASE, *Src2piFREQ;
 extern int *Efield_Flag;
-extern int DT_PIC;
+extern int DT_PIC, DT_CONTI, N_ave;
 extern GGA *vec_G;
 extern GCA *vec_C;
 extern int *vec_StructureIndex;
@@ -70,6 +75,18 @@ extern void GasSetting();
 
 static char g_out[512];
 
+/* ref_fluid.cu */
+int rf_fluid(const char *outdir, const float *temps, const float *src, int nsteps);
+
+static float *read_floats(const char *path, size_t n) {
+    FILE *f = fopen(path, "rb");
+    if (!f) { perror(path); exit(2); }
+    float *p = (float *)malloc(n * sizeof(float));
+    if (fread(p, sizeof(float), n, f) != n) { fprintf(stderr, "%s: short file\n", path); exit(2); }
+    fclose(f);
+    return p;
+}
+
 static void wr(const char *name, const void *p, size_t bytes) {
     char path[700];
     snprintf(path, sizeof path, "%s/%s.bin", g_out, name);
@@ -80,7 +97,10 @@ static void wr(const char *name, const void *p, size_t bytes) {
 }
 
 int main(int argc, char **argv) {
-    if (argc != 4) { fprintf(stderr, "usage: %s deck.json seed outdir\n", argv[0]); return 1; }
+    if (argc != 4 && argc != 5 && argc != 7) {
+        fprintf(stderr, "usage: %s deck.json seed outdir [temps.bin [src.bin nsteps]]\n", argv[0]);
+        return 1;
+    }
     strncpy(InputFile, argv[1], 79);
     seed = atol(argv[2]);
     strncpy(g_out, argv[3], sizeof g_out - 1);
@@ -100,6 +120,7 @@ int main(int argc, char **argv) {
     fprintf(m, "dx %.9g\ndy %.9g\nzlength %.9g\nxlength %.9g\nylength %.9g\n", dx, dy, zlength, xlength, ylength);
     fprintf(m, "idx %.9g\nidy %.9g\nhdx %.9g\nhdy %.9g\nidxy %.9g\n", idx, idy, hdx, hdy, idxy);
     fprintf(m, "dt %.9g\ndt_dx %.9g\ndt_dy %.9g\nDT_PIC %d\n", dt, dt_dx, dt_dy, DT_PIC);
+    fprintf(m, "DT_CONTI %d\nN_ave %d\n", DT_CONTI, N_ave);
     fprintf(m, "nsp %d\nnfsp %d\nnBG %d\nMainGas %d\n", nsp, nfsp, nBG, MainGas);
     fprintf(m, "CondNUM %d\nCondNUMR %d\nSrcNUM %d\nDielNUM %d\nA_size %d\n", CondNUM, CondNUMR, SrcNUM, DielNUM, A_size);
     fprintf(m, "TnRct %d\nN_LOGX %d\nidLOGX %.9g\nh_nvel %d\nPCGtol %.9g\n", TnRct, N_LOGX, idLOGX, h_nvel, PCGtol);
@@ -158,6 +179,13 @@ int main(int argc, char **argv) {
         snprintf(nm, sizeof nm, "p%d_vx", s); wr(nm, PtD[s].vx, (size_t)np * sizeof(float));
         snprintf(nm, sizeof nm, "p%d_vy", s); wr(nm, PtD[s].vy, (size_t)np * sizeof(float));
         snprintf(nm, sizeof nm, "p%d_vz", s); wr(nm, PtD[s].vz, (size_t)np * sizeof(float));
+    }
+    if (argc >= 5) {
+        float *temps = read_floats(argv[4], (size_t)Gsize);
+        float *src = argc == 7 ? read_floats(argv[5], (size_t)nfsp * Csize) : NULL;
+        rf_fluid(g_out, temps, src, argc == 7 ? atoi(argv[6]) : 0);
+        free(temps);
+        free(src);
     }
     return 0;
 }

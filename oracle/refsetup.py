@@ -87,7 +87,48 @@ class RefSetup:
             os.mkdir(out)
             subprocess.run([REF_DUMP, deck, str(int(seed)), out], check=True, stdout=subprocess.DEVNULL,
                            stderr=subprocess.DEVNULL)
+            self._deck, self._seed = deck, int(seed)
             self._load(out, seed, field_mode, move_mode, pcg_rtol)
+
+    def _fluid(self, d, temp, m, t):
+        """The fluid species' set-up: the reference's Fluid_Setting, diffusion
+        and Gummel coefficients and initial fluxes (src/Fluid.c:3-224,
+        src/cuda_Fluid.cu:3-95,185-298), which need the gas temperature of every
+        node, so ref_dump runs again with it."""
+        fd = d + "_fluid"
+        os.mkdir(fd)
+        tp = os.path.join(fd, "temps.bin")
+        temp.astype(np.float32).tofile(tp)
+        subprocess.run([REF_DUMP, self._deck, str(self._seed), fd, tp], check=True, stdout=subprocess.DEVNULL,
+                       stderr=subprocess.DEVNULL)
+        ngx, ngy, ncx, ncy, nfsp = m["ngx"], m["ngy"], m["ncx"], m["ncy"], m["nfsp"]
+        G, C = ngx * ngy, ncx * ncy
+        cell = _read(fd, "fl_den0", np.float32)
+        # Sync_Fluid_GFCtoGFG_forDen (src/cuda_Fluid.cu:321-339): node (i, j) of
+        # cell (i, j), and node (i+1, j+1) of the last row and column; nodes
+        # (0, ncy) and (ncx, 0) are written by nothing in the reference (its
+        # memory there is never set) and are 0 here
+        node = np.zeros((max(nfsp, 1), ngx, ngy), np.float32)
+        cg = cell.reshape(max(nfsp, 1), ncx, ncy) if nfsp else np.zeros((1, ncx, ncy), np.float32)
+        node[:, :ncx, :ncy] = cg
+        node[:, ncx, 1:] = cg[:, ncx - 1, :]
+        node[:, 1:, ncy] = cg[:, :, ncy - 1]
+        t["fluid_cell_den"] = cell
+        t["fluid_den"] = node.reshape(-1)[:max(nfsp, 1) * G] if nfsp else np.zeros(G, np.float32)
+        xl, yl = _read(fd, "fl_xlines", np.int32), _read(fd, "fl_ylines", np.int32)
+        t["fluid_xlines"], t["fluid_ylines"] = xl, yl
+        for k in ("xl_fg", "yl_fg", "D", "gax", "gbx", "gay", "gby", "flux_x0", "flux_y0"):
+            t["fluid_" + k] = _read(fd, "fl_" + k, np.float32)
+        dt = np.float32(m["dt"])
+        t["fluid_scalars"] = np.array([dt * np.float32(m["DT_CONTI"]), m["N_ave"], m["DT_CONTI"], nfsp, xl.size // 3,
+                                       yl.size // 3], np.float32)
+        # Argon_Update_Source's rate factors (src/cuda_Diagnostic.cu:634-642):
+        # the electron channels 0-6 and 8 at Denscale / N_ave / dt
+        rf = np.zeros(m["TnRct"], np.float32)
+        f0 = np.float32(np.float32(m["sp0_Denscale"]) / np.float32(m["N_ave"])) / dt
+        rf[0:7] = f0
+        rf[8] = f0
+        t["fluid_rate_f"] = rf
 
     # ------------------------------------------------------------ assembly
     def _load(self, d, seed, field_mode, move_mode, pcg_rtol):
@@ -155,10 +196,9 @@ class RefSetup:
         t["back_den2"] = np.zeros(G, np.float32)
         t["back_vel2"] = np.zeros(G, np.float32)
         nfsp = m["nfsp"]
-        fl = np.zeros((max(nfsp, 1), G), np.float32)
-        for f in range(nfsp):
-            fl[f, dr] = m[f"fg{f}_InitDens"]
-        t["fluid_den"] = fl.ravel()
+        t["plasma_region"] = np.ascontiguousarray(gca["PlasmaRegion"])
+        self._fluid(d, temp, m, t)
+        fl = t["fluid_den"].reshape(max(nfsp, 1), G)
         # DepositBoundary's factors
         face, bnd, cid = gga["Face"], gga["Boundary"], gga["CondID"]
         dep = np.ones(G, np.float32)

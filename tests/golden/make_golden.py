@@ -72,6 +72,44 @@ def dump(name, deck, seed):
                             meta=json.dumps(meta), **arrs)
 
 
+# decks whose fluid set-up and continuity solve are pinned (fluid_<name>.npz)
+FLUID = ["ar_33x17", "ar_block_33x21", "o2_33x17", "aro2_33x17", "ar_33x17_exp", "ar_33x17_cos"]
+FLUID_STEPS = 5
+
+
+def dump_fluid(name, deck, seed):
+    """The reference's fluid set-up (Fluid_Setting, Cal_D_*, the Gummel
+    coefficients, the initial fluxes) and FLUID_STEPS steps of its
+    Solve_Continuity_eqn, through ref_dump's temps/src arguments.  The gas
+    temperature per node is this library's solve of the reference's own
+    temperature system (the reference solves it on the GPU); the sources are
+    a seeded field of the size the collision rates give."""
+    import hpic
+    exe = os.path.join(REPO, "oracle", "_ref", "ref_dump")
+    S = hpic.Setup(deck, seed=seed, gas_temp_mode=0)
+    temps = S.table("node_temp").astype(np.float32)
+    nf, C = int(S.table("fluid_scalars")[3]), S.info.Csize
+    rng = np.random.default_rng(seed)
+    src = (rng.normal(0.0, 1.0, nf * C) * 10 ** rng.uniform(19, 22, nf * C)).astype(np.float32)
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "deck.json")
+        with open(path, "w") as f:
+            json.dump(deck, f)
+        out = os.path.join(tmp, "out")
+        os.makedirs(out)
+        temps.tofile(os.path.join(tmp, "temps.bin"))
+        src.tofile(os.path.join(tmp, "src.bin"))
+        subprocess.run([exe, path, str(seed), out, os.path.join(tmp, "temps.bin"), os.path.join(tmp, "src.bin"),
+                        str(FLUID_STEPS)], check=True, stdout=subprocess.DEVNULL)
+        arrs = {}
+        for fn in os.listdir(out):
+            if fn.startswith("fl_"):
+                dt = np.int32 if fn.endswith("lines.bin") else np.float32
+                arrs[fn[:-4]] = np.fromfile(os.path.join(out, fn), dtype=dt)
+    np.savez_compressed(os.path.join(HERE, f"fluid_{name}.npz"), deck=json.dumps(deck), seed=seed, temps=temps,
+                        src=src, nsteps=FLUID_STEPS, **arrs)
+
+
 if __name__ == "__main__":
     only = set(sys.argv[1:])  # names to (re)generate; all when none are given
     for name, (deck, seed) in DECKS.items():
@@ -79,3 +117,6 @@ if __name__ == "__main__":
             continue
         dump(name, deck, seed)
         print("wrote", name)
+        if name in FLUID:
+            dump_fluid(name, deck, seed)
+            print("wrote fluid", name)

@@ -15,7 +15,9 @@ pytestmark = pytest.mark.skipif(not refsetup.available(), reason="oracle/_ref/re
 
 EXACT = ["sidx", "boundary", "face", "cond_id", "dens_region", "area", "eps_r", "xsec", "collf", "vsave", "stencil",
          "unk_node", "dep_factor", "sigv", "scalars", "sources", "lap", "back_den1", "back_vel1", "fluid_den",
-         "node_temp", "a_val", "ai", "aj", "matm"]
+         "node_temp", "a_val", "ai", "aj", "matm", "plasma_region", "fluid_cell_den", "fluid_xlines", "fluid_ylines",
+         "fluid_xl_fg", "fluid_yl_fg", "fluid_D", "fluid_gax", "fluid_gbx", "fluid_gay", "fluid_gby", "fluid_flux_x0",
+         "fluid_flux_y0", "fluid_scalars", "fluid_rate_f"]
 
 
 def bits(a):
