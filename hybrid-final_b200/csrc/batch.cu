@@ -39,7 +39,8 @@ namespace hpi {
 
 hp_status batch_dev_build(hp_case *const *cases, int n, BatchDev &b) {
     std::vector<DevCase> hd(n);
-    std::vector<int> part(n + 1, 0), cell(n + 1, 0), node(n + 1, 0);
+    std::vector<int> part(n + 1, 0), cell(n + 1, 0), node(n + 1, 0), fl(2 * (n + 1), 0);
+    b.fluid = FluidPlan();
     b.max_g = 0;
     b.any_eedf = false;
     b.max_smt = 0;
@@ -56,7 +57,18 @@ hp_status batch_dev_build(hp_case *const *cases, int n, BatchDev &b) {
         cell[i + 1] = cell[i] + s.Csize;
         node[i + 1] = node[i] + s.Gsize;
         b.max_g = std::max(b.max_g, s.Gsize);
+        const DevCase &h = cases[i]->h;
+        const bool on = h.fluid_on != 0;
+        fl[i + 1] = fl[i] + (on ? h.nfsp * h.nxl : 0);
+        fl[n + 1 + i + 1] = fl[n + 1 + i] + (on ? h.nfsp * h.nyl : 0);
+        if (on) {
+            b.fluid.any = true;
+            b.fluid.len_x = std::max(b.fluid.len_x, s.ncx);
+            b.fluid.len_y = std::max(b.fluid.len_y, s.ncy);
+        }
     }
+    b.fluid.n_x = fl[n];
+    b.fluid.n_y = fl[2 * n + 1];
     b.n = n;
     b.n_part = part[n];
     b.n_cell = cell[n];
@@ -69,6 +81,10 @@ hp_status batch_dev_build(hp_case *const *cases, int n, BatchDev &b) {
     CK(cudaMemcpy(b.d_part, part.data(), sizeof(int) * (size_t)(n + 1), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(b.d_cell, cell.data(), sizeof(int) * (size_t)(n + 1), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(b.d_node, node.data(), sizeof(int) * (size_t)(n + 1), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&b.d_fluid, sizeof(int) * fl.size()));
+    CK(cudaMemcpy(b.d_fluid, fl.data(), sizeof(int) * fl.size(), cudaMemcpyHostToDevice));
+    b.fluid.xl_items = b.d_fluid;
+    b.fluid.yl_items = b.d_fluid + n + 1;
     std::vector<int> lists;
     for (int m = 0; m < 5; m++)
         for (int k = 0; k <= m; k++) {
@@ -112,6 +128,7 @@ void batch_dev_free(BatchDev &b) {
     cudaFree(b.d_cell);
     cudaFree(b.d_node);
     cudaFree(b.d_lists);
+    cudaFree(b.d_fluid);
     fast_plan_free(b.fast);
     b = BatchDev();
 }
@@ -125,6 +142,7 @@ hp_status run_step(const BatchDev &b, const LaunchCfg &lc, int gas, cudaStream_t
     if (gas != GAS_AR) CK(launch_mcc_oxy(b.d_cases, b.d_cell, b.n, b.n_cell, gas, st));
     else CK(launch_mcc_ar(b.d_cases, b.d_cell, b.n, b.n_cell, lc, st));
     CK(launch_deposit(b.d_cases, b.d_part, b.d_node, b.n, b.n_part, b.n_node, lc, st, b.max_smt));
+    if (b.fluid.any) CK(launch_fluid(b.d_cases, b.d_node, b.n, b.n_node, b.fluid, st));
     CK(launch_accumulate(b.d_cases, b.d_node, b.n, b.n_node, st));
     if (b.any_eedf) CK(launch_eedf(b.d_cases, b.d_cell, b.n, b.n_cell, st));
     if (b.power) CK(launch_power(b.d_cases, b.n, st));

@@ -145,6 +145,7 @@ void fill_info(const Setup &s, hp_case_info *out) {
     out->n_sources = s.src_num;
     out->power_driven = s.power_driven() ? 1 : 0;
     out->n_reactions = s.TnRct;
+    out->n_fluid = s.nfsp;
 }
 
 // Collision probability per cell from its lower-left node
@@ -396,14 +397,61 @@ hp_status build_device(hp_case *c) {
     }
     h.mcc_stride = s.main_gas == GAS_AR ? 8 : 72;
     h.mcc_all_species = c->opts.o2_all_species ? 1 : 0;
+    TRY(dupload(c, (float **)&h.back_den1, s.back_den1));
     if (s.main_gas != GAS_AR) {
-        TRY(dupload(c, (float **)&h.back_den1, s.back_den1));
         TRY(dupload(c, (float **)&h.back_den2, s.back_den2));
         TRY(dupload(c, (float **)&h.back_vel2, s.back_vel2));
-        TRY(dupload(c, (float **)&h.fluid_den, s.fluid_den));
     }
+    // fluid species and the state of their averaging window: the electron
+    // density sum, the tallies at the last average and the collision
+    // probabilities (one block, HP_GRID_FLUID_STATE)
     c->prob = cell_probabilities(s);
-    TRY(dupload(c, (float **)&h.prob, c->prob));
+    {
+        const int F = s.nfsp, st = h.mcc_stride;
+        c->fl_state_bytes = (size_t)G * 8 + (size_t)C * st * 4 + (size_t)3 * C * 4;
+        TRY(dalloc(c, &c->fl_state, c->fl_state_bytes));
+        h.fl_sum = (double *)c->fl_state;
+        h.fl_base = (unsigned int *)(c->fl_state + (size_t)G * 8);
+        h.prob = (float *)(c->fl_state + (size_t)G * 8 + (size_t)C * st * 4);
+        CK(cudaMemcpy(h.prob, c->prob.data(), (size_t)3 * C * 4, cudaMemcpyHostToDevice));
+        h.nfsp = F;
+        h.fluid_on = (F > 0 && !c->opts.fluid_fixed) ? 1 : 0;
+        h.n_ave = s.N_ave;
+        h.tnrct = s.TnRct;
+        h.dtc = s.dtc;
+        h.denscale0 = s.sp[0].Denscale;
+        h.nxl = (int)s.xl_x1.size();
+        h.nyl = (int)s.yl_xx.size();
+        for (int k = 0; k < s.TnRct && k < 96; k++) {
+            h.rate_f[k] = s.fluid_rate_f[k];
+            h.rr[k] = s.collf[k].RR;
+        }
+        if (F > 0) {
+            if (h.fluid_on && (fluid_sweep_warps(s.ncx) == 0 || fluid_sweep_warps(s.ncy) == 0))
+                return set_error("grid too wide for the fluid sweep"), HP_ERR_UNSUPPORTED;
+            if (h.fluid_on && s.N_ave < 1) return set_error("AverageIter must be at least 1"), HP_ERR_UNSUPPORTED;
+            std::vector<int> xl, yl;
+            for (int k = 0; k < h.nxl; k++) { xl.push_back(s.xl_x1[k]); xl.push_back(s.xl_x2[k]); xl.push_back(s.xl_yy[k]); }
+            for (int k = 0; k < h.nyl; k++) { yl.push_back(s.yl_xx[k]); yl.push_back(s.yl_y1[k]); yl.push_back(s.yl_y2[k]); }
+            std::vector<float> xfg(s.xl_fg1), yfg(s.yl_fg1);
+            xfg.insert(xfg.end(), s.xl_fg2.begin(), s.xl_fg2.end());
+            yfg.insert(yfg.end(), s.yl_fg2.begin(), s.yl_fg2.end());
+            TRY(dupload(c, &h.fluid_den, s.fluid_den));
+            TRY(dupload(c, &h.fden, s.fluid_cell_den));
+            TRY(dalloc(c, &h.fsrc, (size_t)F * C));
+            TRY(dupload(c, &h.fflx, s.flux_x0));
+            TRY(dupload(c, &h.ffly, s.flux_y0));
+            TRY(dupload(c, (int **)&h.fl_xl, xl));
+            TRY(dupload(c, (int **)&h.fl_yl, yl));
+            TRY(dupload(c, (float **)&h.fl_xfg, xfg));
+            TRY(dupload(c, (float **)&h.fl_yfg, yfg));
+            TRY(dupload(c, (float **)&h.gax, s.gax));
+            TRY(dupload(c, (float **)&h.gbx, s.gbx));
+            TRY(dupload(c, (float **)&h.gay, s.gay));
+            TRY(dupload(c, (float **)&h.gby, s.gby));
+            TRY(dupload(c, (int **)&h.plasma, s.plasma_region));
+        }
+    }
     TRY(dupload(c, (float **)&h.back_vel1, s.back_vel1));
     TRY(dupload(c, (float **)&h.vsave, s.vsave));
     h.nvel = s.nvel;
@@ -454,8 +502,17 @@ hp_status build_device(hp_case *c) {
     TRY(dalloc(c, &c->d_case, 1));
     CK(cudaMemcpy(c->d_case, &h, sizeof(h), cudaMemcpyHostToDevice));
     {
-        std::vector<int> items = {0, s.nsp * C, 0, C, 0, G};
+        // particles, cells, nodes, fluid x lines, fluid y lines
+        const int nx = h.fluid_on ? s.nfsp * h.nxl : 0, ny = h.fluid_on ? s.nfsp * h.nyl : 0;
+        std::vector<int> items = {0, s.nsp * C, 0, C, 0, G, 0, nx, 0, ny};
         TRY(dupload(c, &c->d_items, items));
+        c->fplan_fluid.xl_items = c->d_items + 6;
+        c->fplan_fluid.yl_items = c->d_items + 8;
+        c->fplan_fluid.n_x = nx;
+        c->fplan_fluid.n_y = ny;
+        c->fplan_fluid.len_x = s.ncx;
+        c->fplan_fluid.len_y = s.ncy;
+        c->fplan_fluid.any = h.fluid_on != 0;
     }
     for (int isp = 0; isp < s.nsp; isp++) {
         if (s.load_deferred) TRY(hpi::device_load(c, isp));
@@ -518,6 +575,10 @@ hp_status one_step(hp_case *c, cudaStream_t st) {
     TRY(op_sort(c, st));
     TRY(op_mcc(c, st));
     TRY(op_deposit(c, st, true));
+    if (c->fplan_fluid.any) {
+        e = launch_fluid(c->d_case, c->d_items + 4, 1, c->s.Gsize, c->fplan_fluid, st);
+        if (e != cudaSuccess) return cuda_fail(e, "fluid");
+    }
     e = launch_accumulate(c->d_case, c->d_items + 4, 1, c->s.Gsize, st);
     if (e == cudaSuccess && c->h.eedf_every > 0) e = launch_eedf(c->d_case, c->d_items + 2, 1, c->s.Csize, st);
     if (e == cudaSuccess && c->h.pw) e = launch_power(c->d_case, 1, st);
@@ -1046,6 +1107,12 @@ static hp_status grid_ptr(hp_case *c, hp_grid_field f, void **p, size_t *nb) {
     case HP_GRID_SIGMA: *p = c->h.sigma; *nb = c->h.sigma ? (size_t)G * 8 : 0; break;
     case HP_GRID_SOURCE_AC: *p = c->h.src_amp; *nb = (size_t)c->s.src_num * 4; break;
     case HP_GRID_POWER_STATE: *p = c->h.pw; *nb = c->h.pw ? sizeof(PowerState) : 0; break;
+    case HP_GRID_FLUID_CELL_DEN: *p = c->h.fden; *nb = (size_t)c->s.nfsp * c->s.Csize * 4; break;
+    case HP_GRID_FLUID_DEN: *p = c->h.fluid_den; *nb = (size_t)c->s.nfsp * G * 4; break;
+    case HP_GRID_FLUID_SOURCE: *p = c->h.fsrc; *nb = (size_t)c->s.nfsp * c->s.Csize * 4; break;
+    case HP_GRID_FLUID_FLUX_X: *p = c->h.fflx; *nb = (size_t)c->s.nfsp * c->s.ngx * c->s.ncy * 4; break;
+    case HP_GRID_FLUID_FLUX_Y: *p = c->h.ffly; *nb = (size_t)c->s.nfsp * c->s.ncx * c->s.ngy * 4; break;
+    case HP_GRID_FLUID_STATE: *p = c->fl_state; *nb = c->fl_state_bytes; break;
     default: return set_error("unknown grid field"), HP_ERR_ARG;
     }
     return HP_OK;

@@ -34,7 +34,8 @@ struct hp_case {
     int device = 0;
     hp::DevCase h{};               // host image of the device descriptor
     hp::DevCase *d_case = nullptr; // device descriptor
-    int *d_items = nullptr;        // item_start arrays: [0..1] particles, [2..3] cells, [4..5] nodes
+    int *d_items = nullptr;        // item_start arrays: [0..1] particles, [2..3] cells, [4..5] nodes,
+                                   // [6..7] fluid x lines, [8..9] fluid y lines
     std::vector<void *> allocs;
     std::vector<size_t> alloc_bytes;
     size_t bytes = 0;
@@ -49,7 +50,10 @@ struct hp_case {
     cudaGraphExec_t graph = nullptr;
     int graph_kernels = 0; // kernel nodes in the captured step
     hp_batch *batch = nullptr;
-    std::vector<float> prob; // [3*C]
+    std::vector<float> prob; // [3*C] initial collision probabilities
+    char *fl_state = nullptr;  // fluid averaging state (HP_GRID_FLUID_STATE), also holding h.prob
+    size_t fl_state_bytes = 0;
+    hp::FluidPlan fplan_fluid; // the case's own fluid launch lists (into d_items)
     std::vector<uint32_t> mcc_base; // collision tallies at the last hp_reset_averages (empty: zeros)
 };
 
@@ -74,6 +78,8 @@ struct BatchDev {
     int max_smt = 0; // most density smoothing passes of any case
     bool surface = false; // some case has dielectric blocks
     bool power = false;   // some case has power-driven sources
+    int *d_fluid = nullptr; // fluid line prefixes: x lines [n+1], then y lines [n+1]
+    hp::FluidPlan fluid;
     // PCG groups for every cluster cap 1,2,4,8,16: lists of case indices per
     // cluster size, concatenated in d_lists
     int *d_lists = nullptr;

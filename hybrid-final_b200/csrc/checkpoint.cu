@@ -4,20 +4,21 @@
 // src/cuda_SaveDump.cu:5-106; read back by V000_LoadDUMP, src/load.c:5-120),
 // field for field, so that the reference's loader and its post-processing
 // read it: time, step counters, gas, every particle as (CellID, x, y, vx, vy,
-// vz) with x, y in grid units, fluid arrays, (empty) history, per-node
-// densities, background gas, potentials, fields and their time averages.
-// Quantities this library does not model are written as the reference's
-// neutral values: no continuity solve (Conti_Flag 0, fluid densities the
-// deck's constants, sources and fluxes 0), no history records, MCC rates 0
-// (the exact per-cell tallies are in the extension).  The dielectric surface
-// charge goes out as the reference's float sigma per (species, node).
+// vz) with x, y in grid units, the fluid species (Conti_Flag, densities,
+// sources, fluxes), (empty) history, per-node densities, background gas,
+// potentials, fields and their time averages.  Quantities this library does
+// not model are written as the reference's neutral values: no history
+// records, MCC rates 0 (the exact per-cell tallies are in the extension).
+// The dielectric surface charge goes out as the reference's float sigma per
+// (species, node).
 //
-// An extension block follows ("HPICX002"): everything a resumed run needs to
+// An extension block follows ("HPICX003"): everything a resumed run needs to
 // continue bit for bit -- the step counter that keys the Philox streams, the
 // case seed, the particles as in-cell offsets in the device's cell order,
 // the field solver's warm start, the charge grid and right-hand side, the
-// running sums, tallies and histogram.  hp_case_load reads the V000 part only
-// to check it against the case, then restores the extension.
+// running sums, tallies and histogram, the fluid species and their averaging
+// window.  hp_case_load reads the V000 part only to check it against the
+// case, then restores the extension.
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -61,16 +62,18 @@ struct File {
     }
 };
 
-const char MAGIC[8] = {'H', 'P', 'I', 'C', 'X', '0', '0', '2'};
+const char MAGIC[8] = {'H', 'P', 'I', 'C', 'X', '0', '0', '3'};
 // the extension's format version; the magic's last digits carry the same number
-constexpr uint32_t EXT_VERSION = 2u;
+constexpr uint32_t EXT_VERSION = 3u;
 const char TAIL[8] = {'H', 'P', 'I', 'C', 'E', 'N', 'D', '1'};
 // grid fields carried by the extension, in file order
 const hp_grid_field EXT_GRIDS[] = {HP_GRID_EX,         HP_GRID_EY,          HP_GRID_PHI,     HP_GRID_PHI_POIS,
                                    HP_GRID_DEN,        HP_GRID_SOURCE,      HP_GRID_PCG_X,   HP_GRID_PCG_B,
                                    HP_GRID_AVE_DEN,    HP_GRID_AVE_PHI,     HP_GRID_AVE_SOURCE, HP_GRID_AVE_EX,
                                    HP_GRID_AVE_EY,     HP_GRID_COND_CHARGE, HP_GRID_MCC_COUNT, HP_GRID_EEDF,
-                                   HP_GRID_SURFACE_CHARGE, HP_GRID_SIGMA, HP_GRID_SOURCE_AC, HP_GRID_POWER_STATE};
+                                   HP_GRID_SURFACE_CHARGE, HP_GRID_SIGMA, HP_GRID_SOURCE_AC, HP_GRID_POWER_STATE,
+                                   HP_GRID_FLUID_CELL_DEN, HP_GRID_FLUID_DEN, HP_GRID_FLUID_SOURCE,
+                                   HP_GRID_FLUID_FLUX_X, HP_GRID_FLUID_FLUX_Y, HP_GRID_FLUID_STATE};
 
 template <class T> std::vector<T> fetch(hp_case *c, hp_grid_field f) {
     void *p = nullptr;
@@ -138,19 +141,23 @@ hp_status write_v000(hp_case *c, File &F, int64_t tstep, int64_t ave_count, cons
         }
         F.put(buf.data(), buf.size());
     }
-    // fluid: Conti_Flag, then per fluid species den[ncx][ncy], Source[ncx][ncy],
+    // fluid: Conti_Flag (set from the first average on), then per fluid
+    // species den and Source row by row interleaved ([ncx][ncy] each),
     // flux_x[ngx][ncy], flux_y[ncx][ngy]
-    F.put1<int32_t>(0);
-    for (int f = 0; f < s.nfsp; f++) {
-        std::vector<float> row((size_t)ncy);
-        for (int i = 0; i < s.ncx; i++) {
-            for (int j = 0; j < ncy; j++)
-                row[(size_t)j] = s.fluid_den.empty() ? 0.f : s.fluid_den[(size_t)f * G + (size_t)i * ngy + j];
-            F.put(row.data(), row.size() * 4);
-            F.zeros((size_t)ncy * 4);
+    {
+        const auto fden = fetch<float>(c, HP_GRID_FLUID_CELL_DEN), fsrc = fetch<float>(c, HP_GRID_FLUID_SOURCE);
+        const auto fx = fetch<float>(c, HP_GRID_FLUID_FLUX_X), fy = fetch<float>(c, HP_GRID_FLUID_FLUX_Y);
+        const bool on = c->h.fluid_on && tstep >= (int64_t)c->h.n_ave + 1;
+        F.put1<int32_t>(on ? 1 : 0);
+        const size_t C = (size_t)s.Csize, nfx = (size_t)s.ngx * ncy, nfy = (size_t)s.ncx * ngy;
+        for (int f = 0; f < s.nfsp; f++) {
+            for (int i = 0; i < s.ncx; i++) {
+                F.put(&fden[(size_t)f * C + (size_t)i * ncy], (size_t)ncy * 4);
+                F.put(&fsrc[(size_t)f * C + (size_t)i * ncy], (size_t)ncy * 4);
+            }
+            F.put(&fx[(size_t)f * nfx], nfx * 4);
+            F.put(&fy[(size_t)f * nfy], nfy * 4);
         }
-        F.zeros((size_t)s.ngx * ncy * 4);
-        F.zeros((size_t)s.ncx * ngy * 4);
     }
     // history: hist_count 0, dHIST, no records (every array has hist_count
     // entries), then hist_ave_count 0

@@ -115,10 +115,10 @@ struct DevCase {
     float mofm[96];
     int mcc_stride;                 // counters per cell in mcc_count (8 for Ar, 72 for the oxygen sets)
     int mcc_all_species;            // O2 set: 0 electrons only (the reference's launch), 1 every species
-    const float *prob;              // [3*C]: electron P1, P2; ion P (Ar)
+    float *prob;                    // [3*C]: electron P1, P2; ion P (Ar); P2 follows the Ar* density
     const float *back_vel1;         // [G]
-    const float *back_den1, *back_den2, *back_vel2; // [G] (oxygen sets)
-    const float *fluid_den;         // [nfsp*G] metastable / radical densities (oxygen sets)
+    const float *back_den1, *back_den2, *back_vel2; // [G] (back_den2, back_vel2: oxygen sets)
+    float *fluid_den;               // [nfsp*G] metastable / radical densities at the nodes (the MCC's input)
     const float *vsave;
     int nvel, mcc_n;
     float dt_mcc;                   // electron collision sub-step (DT_MCCn sub-cycles)
@@ -143,6 +143,22 @@ struct DevCase {
     float *fs_a1, *fs_y;            // [ny*nx] products
     const float *fs_V, *fs_Vt, *fs_W, *fs_Wt, *fs_inv;
     double *fs_res;                 // [2]: final ||r||, ||b||
+    // fluid species (metastables, radicals): the continuity solve of
+    // src/cuda_Fluid.cu:34-167 and the source cycle of
+    // src/cuda_Diagnostic.cu:268-330, 548-743.  nfsp 0 or fluid_on 0: the
+    // densities stay at their initial values.
+    int nfsp, fluid_on, n_ave, nxl, nyl, tnrct;
+    float dtc, denscale0;           // continuity step dt x TimeStep_Conti; electron Denscale
+    float *fden, *fsrc;             // [nfsp*C] cell densities and sources (m^-3, m^-3 s^-1)
+    float *fflx, *ffly;             // [nfsp*ngx*ncy] x-face fluxes at i*ncy+j, [nfsp*ncx*ngy] y-face at i*ngy+j
+    const int *fl_xl, *fl_yl;       // [3*nxl] x lines (x1, x2, y); [3*nyl] y lines (x, y1, y2)
+    const float *fl_xfg, *fl_yfg;   // wall factors of every line: [nfsp*lines] fg1, then [nfsp*lines] fg2
+    const float *gax, *gbx;         // [nfsp*ngx*ncy] Gummel coefficients of the x faces
+    const float *gay, *gby;         // [nfsp*ncx*ngy] of the y faces
+    const int *plasma;              // [C] PlasmaRegion
+    double *fl_sum;                 // [G] electron density summed over the averaging window
+    unsigned int *fl_base;          // [C*mcc_stride] collision tallies at the last average
+    float rate_f[96], rr[96];       // tally -> rate factor and CollF.RR per reaction channel
     // solver controls
     int field_mode, pcg_max_iter;
     float pcg_tol2;

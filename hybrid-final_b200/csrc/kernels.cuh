@@ -87,5 +87,19 @@ cudaError_t launch_advance(const DevCase *cases, int ncases, cudaStream_t st);
 cudaError_t launch_eedf(const DevCase *cases, const int *cell_items, int ncases, int n_cell_items, cudaStream_t st);
 cudaError_t launch_accumulate(const DevCase *cases, const int *node_items, int ncases, int n_node_items,
                               cudaStream_t st);
+// fluid species (fluid.cu): the continuity sweeps, one warp per line, and the
+// averaging cycle, one thread per node
+struct FluidPlan {
+    const int *xl_items = nullptr; // device prefix [n+1] of nfsp x lines per case (0 where held fixed)
+    const int *yl_items = nullptr; // the same for the y lines
+    int n_x = 0, n_y = 0;          // total line items
+    int len_x = 0, len_y = 0;      // longest line in cells (ncx, ncy of the widest case)
+    bool any = false;              // some case runs the fluid cycle
+};
+constexpr size_t FLUID_SMEM_MAX = 200 * 1024;
+// warps per CTA of the sweep for lines of up to L cells (0: L too long)
+int fluid_sweep_warps(int L);
+cudaError_t launch_fluid(const DevCase *cases, const int *node_items, int ncases, int n_node_items,
+                         const FluidPlan &fp, cudaStream_t st);
 
 } // namespace hp

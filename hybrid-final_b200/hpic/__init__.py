@@ -25,7 +25,8 @@ STATUS_WALK_BOUND, STATUS_SURFACE_OVERFLOW = 0x10, 0x20
 
 GRID = dict(EX=0, EY=1, PHI=2, PHI_POIS=3, DEN=4, SOURCE=5, PCG_X=6, PCG_B=7, AVE_DEN=8, AVE_PHI=9,
             COND_CHARGE=10, MCC_COUNT=11, EEDF=12, AVE_SOURCE=13, AVE_EX=14, AVE_EY=15,
-            SURFACE_CHARGE=16, SIGMA=17, SOURCE_AC=18, POWER_STATE=19)
+            SURFACE_CHARGE=16, SIGMA=17, SOURCE_AC=18, POWER_STATE=19, FLUID_CELL_DEN=20, FLUID_DEN=21,
+            FLUID_SOURCE=22, FLUID_FLUX_X=23, FLUID_FLUX_Y=24, FLUID_STATE=25)
 SIGMA_FRAC_BITS = 28  # fixed-point fraction bits of SURFACE_CHARGE (particle weights)
 POWER_STATE_BYTES = 8 * 8 * 3 + 4 * 8 * 2 + 8  # PowerState: surf, old, old2 (double[8]); power, count; flags
 EEDF_BINS, EEDF_DE = 200, 0.25  # electron energy histogram: 0.25 eV bins from 0, one overflow bin
@@ -51,7 +52,7 @@ class CaseOpts(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("cap_per_cell", C.c_int), ("field_mode", C.c_int),
                 ("pcg_rtol", C.c_double), ("pcg_max_iter", C.c_int), ("o2_all_species", C.c_int),
                 ("device", C.c_int), ("gas_temp_mode", C.c_int), ("move_mode", C.c_int),
-                ("fs_passes", C.c_int), ("eedf_every", C.c_int), ("gpu_load", C.c_int)]
+                ("fs_passes", C.c_int), ("eedf_every", C.c_int), ("gpu_load", C.c_int), ("fluid_fixed", C.c_int)]
 
 
 class CaseInfo(C.Structure):
@@ -61,7 +62,7 @@ class CaseInfo(C.Structure):
                 ("dx", C.c_double), ("dy", C.c_double), ("tstep", C.c_int64), ("device_bytes", C.c_size_t),
                 ("pcg_cluster", C.c_int), ("pcg_block", C.c_int), ("field_mode", C.c_int), ("mcc_stride", C.c_int),
                 ("n_smt", C.c_int), ("n_dielectric", C.c_int), ("n_sources", C.c_int),
-                ("power_driven", C.c_int), ("n_reactions", C.c_int)]
+                ("power_driven", C.c_int), ("n_reactions", C.c_int), ("n_fluid", C.c_int)]
 
 
 class Tune(C.Structure):
@@ -365,7 +366,7 @@ class Case:
 
     def grid(self, name):
         info = self.info
-        G, nsp = info.Gsize, info.nsp
+        G, nsp, nf = info.Gsize, info.nsp, info.n_fluid
         sizes = dict(EX=(G, np.float32), EY=(G, np.float32), PHI=(G, np.float32), PHI_POIS=(G, np.float32),
                      DEN=(nsp * G, np.float64), SOURCE=(G, np.float64),
                      PCG_X=(G, np.float32 if self.opts.field_mode == 0 else np.float64),
@@ -376,7 +377,11 @@ class Case:
                      SURFACE_CHARGE=(nsp * G if info.n_dielectric else 0, np.int64),
                      SIGMA=(G if (info.n_dielectric or info.power_driven) else 0, np.float64),
                      SOURCE_AC=(info.n_sources, np.float32),
-                     POWER_STATE=(POWER_STATE_BYTES if info.power_driven else 0, np.uint8))
+                     POWER_STATE=(POWER_STATE_BYTES if info.power_driven else 0, np.uint8),
+                     FLUID_CELL_DEN=(nf * info.Csize, np.float32), FLUID_DEN=(nf * G, np.float32),
+                     FLUID_SOURCE=(nf * info.Csize, np.float32), FLUID_FLUX_X=(nf * info.ngx * info.ncy, np.float32),
+                     FLUID_FLUX_Y=(nf * info.ncx * info.ngy, np.float32),
+                     FLUID_STATE=(G * 8 + info.Csize * info.mcc_stride * 4 + 3 * info.Csize * 4, np.uint8))
         n, dt = sizes[name]
         out = np.zeros(n, dtype=dt)
         _check(lib().hp_get_grid(self.h, GRID[name], out.ctypes.data_as(_P), out.nbytes))

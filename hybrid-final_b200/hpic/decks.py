@@ -47,7 +47,7 @@ def ccp_deck(ngx, ngy, xlen, ylen, *, gas="Ar", pressure_torr=0.05, voltage=100.
              freq=13.56e6, steps_per_cycle=400, ppc=50, density=1e15, te_ev=2.0,
              ti_ev=0.026, gas_k=300.0, max_np_factor=4, aro2_ratio=(80, 20),
              ion_density=None, pcg_tol=1e-3, smoothing=0, load_type=0, load_pos=None, ratio=1,
-             power_w=0.0, pd_interval=5.0):
+             power_w=0.0, pd_interval=5.0, average_iter=None):
     """Build one CCP deck.
 
     ppc is the macro-particles per cell per species at `density`; np2c is
@@ -118,7 +118,8 @@ def ccp_deck(ngx, ngy, xlen, ylen, *, gas="Ar", pressure_torr=0.05, voltage=100.
             "TimeStep_PIC": steps_per_cycle, "TimeStep_Conti": 200,
             "FieldTest": {"Laplace_Test_Flag": 0, "Laplace_Field_Solver": 8, "Laplace_Field_Tec_Save": 0},
             "PCGMarginOfError": pcg_tol, "HistoryMax": 1000000, "HistoryDivide": 4,
-            "AverageIter": steps_per_cycle, "DensitySmoothing": smoothing,
+            "AverageIter": steps_per_cycle if average_iter is None else average_iter,
+            "DensitySmoothing": smoothing,
             "ParticleLimit": max_np, "ConstB_Flag": 0,
             "ContinuitySteadyState": {"Flag": 0, "Check": 1, "Margin": 1.0},
             "PowerDrivenOption": {"Interval": pd_interval, "VoltageUpDownRatio": 0.05},

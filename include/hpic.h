@@ -114,6 +114,10 @@ typedef struct hp_case_opts {
                             Park-Miller draws and cell order as the host load; a cos() in the Maxwellian
                             may differ in its last double bit, so rare vx/vy differ by one float ulp);
                             0 = the reference's host load (default) */
+    int fluid_fixed;     /* fluid species (Ar*, the O2 metastables and O atoms): 0 = the reference's
+                            continuity solve, fed every AverageIter + 1 steps by the averaged collision
+                            rates (src/cuda_Fluid.cu:34-167, src/cuda_Diagnostic.cu:268-330); 1 = hold
+                            them at their initial densities */
 } hp_case_opts;
 
 /* Default options. */
@@ -144,6 +148,7 @@ typedef struct hp_case_info {
     int n_sources;         /* Source entries */
     int power_driven;      /* 1 when a conductor has a power-driven source (Power(W) != 0) */
     int n_reactions;       /* TnRct: reaction channels of the gas's collision set */
+    int n_fluid;           /* nfsp: fluid species (1 Ar: Ar*; 4 O2: O2(a), O2(b), O, O(1D); 5 Ar/O2: Ar* first) */
 } hp_case_info;
 hp_status hp_case_get_info(const hp_case *c, hp_case_info *out);
 hp_status hp_setup_get_info(const hp_setup *s, hp_case_info *out);
@@ -248,8 +253,17 @@ typedef enum hp_grid_field {
                                  0 bytes in a case with neither dielectrics nor power-driven sources */
     HP_GRID_SOURCE_AC = 18,   /* float[number of sources] AC amplitudes in use (V): the deck's, as revised by
                                  the power controller of power-driven sources */
-    HP_GRID_POWER_STATE = 19  /* the power controller's state (opaque bytes; 0 bytes without power-driven
+    HP_GRID_POWER_STATE = 19, /* the power controller's state (opaque bytes; 0 bytes without power-driven
                                  sources), carried by checkpoints */
+    /* fluid species, f = 0 .. nfsp-1 (Fluid_sp, src/Fluid.c:3-75); cell (i, j) at i*ncy + j */
+    HP_GRID_FLUID_CELL_DEN = 20, /* float[nfsp*Csize] densities in the cells (GFC.den, m^-3) */
+    HP_GRID_FLUID_DEN = 21,      /* float[nfsp*Gsize] densities at the nodes, the collisions' targets (Fluid_Den) */
+    HP_GRID_FLUID_SOURCE = 22,   /* float[nfsp*Csize] sources of the last average (GFC.Source, m^-3 s^-1) */
+    HP_GRID_FLUID_FLUX_X = 23,   /* float[nfsp*ngx*ncy] x-face fluxes at i*ncy + j (GFC.flux_x) */
+    HP_GRID_FLUID_FLUX_Y = 24,   /* float[nfsp*ncx*ngy] y-face fluxes at i*ngy + j (GFC.flux_y) */
+    HP_GRID_FLUID_STATE = 25     /* the averaging window: electron density sum (double[Gsize]), tallies at
+                                  the last average (uint32[Csize*mcc_stride]) and the collision
+                                  probabilities (float[3*Csize]); carried by checkpoints */
 } hp_grid_field;
 hp_status hp_get_grid(hp_case *c, hp_grid_field f, void *out, size_t bytes);
 hp_status hp_set_grid(hp_case *c, hp_grid_field f, const void *in, size_t bytes);

@@ -2159,6 +2159,20 @@ int or_collide_oxy(or_sim *s, int isp, int t, const float *v, float bv1, float b
                    int pair_rl, int *ch, int *keep, float *vout, int *bsp, float *bv, int *kill) {
     return s->impl->collide_oxy(isp, t, v, bv1, bv2, u, nu, pair_rl, ch, keep, vout, bsp, bv, kill);
 }
+void or_fluid_sources(int gas, int n, int tnrct, int nfsp, float *R, const float *fden, const float *eden,
+                      const float *bd1, const float *bd2, const float *rr, float *S) {
+    std::vector<float> r(96), rrv(96, 0.0f);
+    std::copy(rr, rr + std::min(tnrct, 96), rrv.begin());
+    for (int g = 0; g < n; g++) {
+        std::fill(r.begin(), r.end(), 0.0f);
+        std::copy(R + (size_t)g * tnrct, R + (size_t)g * tnrct + std::min(tnrct, 96), r.begin());
+        float nn[5] = {0, 0, 0, 0, 0}, out[5] = {0, 0, 0, 0, 0};
+        for (int f = 0; f < nfsp && f < 5; f++) nn[f] = fden[(size_t)f * n + g];
+        hp_fluid_sources(gas, r.data(), nn, bd1[g], bd2[g], eden[g], rrv.data(), out);
+        std::copy(r.begin(), r.begin() + std::min(tnrct, 96), R + (size_t)g * tnrct);
+        for (int f = 0; f < nfsp && f < 5; f++) S[(size_t)f * n + g] = out[f];
+    }
+}
 void or_fluid_sweeps(or_sim *s, int nsteps) {
     for (int k = 0; k < nsteps; k++) s->impl->fluid_sweeps();
 }

@@ -165,6 +165,11 @@ int or_collide_oxy(or_sim *s, int isp, int t, const float *v, float bv1, float b
 /* only the continuity solve (src/cuda_Fluid.cu:34-42), nsteps times, with
  * the fluid sources of grid 13 as they are */
 void or_fluid_sweeps(or_sim *s, int nsteps);
+/* hp_fluid_sources at n nodes: R[n*tnrct] rates in (neutral channels filled,
+ * out), fden[nfsp*n], eden[n] (0.25 x the averaged electron density), bd1,
+ * bd2[n], rr[tnrct]; S[nfsp*n] out */
+void or_fluid_sources(int gas, int n, int tnrct, int nfsp, float *R, const float *fden, const float *eden,
+                      const float *bd1, const float *bd2, const float *rr, float *S);
 int or_num_threads(void);
 void or_set_threads(int n);
 

@@ -100,6 +100,7 @@ def lib():
             "or_collide_oxy": (C.c_int, [P, C.c_int, C.c_int, _F, C.c_float, C.c_float, _F, C.c_int, C.c_int, _I,
                                          _I, _F, _I, _F, _I]),
             "or_fluid_sweeps": (None, [P, C.c_int]),
+            "or_fluid_sources": (None, [C.c_int, C.c_int, C.c_int, C.c_int, _F, _F, _F, _F, _F, _F, _F]),
             "or_num_threads": (C.c_int, []),
             "or_set_threads": (None, [C.c_int]),
         }
@@ -428,6 +429,20 @@ class Oracle:
         n = C.c_int64(0)
         lib().or_get_averages(self.h, d.ctypes.data_as(_D), p.ctypes.data_as(_D), C.byref(n))
         return d, p, n.value
+
+
+def fluid_sources(gas, rates, fden, eden, bd1, bd2, rr):
+    """The fluid sources of n nodes (include/hp_fluid.h): rates [n, tnrct],
+    fden [nfsp, n], eden [n], bd1 and bd2 [n], rr [tnrct].  Returns (rates
+    with the neutral channels filled, sources [nfsp, n])."""
+    R = np.array(rates, np.float32, copy=True)
+    n, tnrct = R.shape
+    fden = np.ascontiguousarray(fden, np.float32)
+    nfsp = fden.shape[0]
+    S = np.zeros((nfsp, n), np.float32)
+    f = [np.ascontiguousarray(a, np.float32) for a in (eden, bd1, bd2, rr)]
+    lib().or_fluid_sources(gas, n, tnrct, nfsp, _fp(R), _fp(fden), *[_fp(a) for a in f], _fp(S))
+    return R, S
 
 
 def from_setup(setup, precision=32, field_mode=0, pcg_cluster=1, pcg_block=512):

@@ -69,6 +69,13 @@ __device__ void dev_maxwellv(float *vx_local, float *vy_local, float *vz_local, 
 __device__ void dev_anewvel(float energy, float vel, float *n_vx, float *n_vy, float *n_vz, int e_flag,
                             float massrate, float rand1, float rand2);
 __device__ void dev_newvel_IONSC(float *vx_sc, float *vy_sc, float *vz_sc, float vel, float rand1, float rand2);
+// src/cuda_Diagnostic.cu:634,643,684
+__global__ void Argon_Update_Source(int Gsize, int ngy, int TnRct, float *MCCR, CollF *CollP, GPG *SP, GFG *FG,
+                                    GFG *FG_S, GGA *BG);
+__global__ void Oxygen_Update_Source(int Gsize, int TnRct, float *MCCR, CollF *CollP, GPG *SP, GFG *FG, GFG *FG_S,
+                                     GGA *BG);
+__global__ void ArO2_Update_Source(int Gsize, int ngy, int TnRct, float *MCCR, CollF *CollP, GPG *SP, GFG *FG,
+                                   GFG *FG_S, GGA *BG);
 // src/cuda_mccAr.cu:707, src/cuda_mccO2.cu:978, src/cuda_mccArO2.cu:2461
 __device__ float Argon_CrossSection(int R, float engy, int N_LOGX, float idLOGX, ArCollD *data);
 __device__ float O2_CrossSection(int R, float engy, int N_LOGX, float idLOGX, O2CollD *data);
@@ -917,6 +924,58 @@ int rk_oxy_collide(int gas, int isp, int n, const int *imcc, float idlogx, const
             }
         }
         if (overrun) *overrun = script_overrun();
+    });
+}
+
+
+// The fluid sources of G nodes (Argon_Update_Source, Oxygen_Update_Source,
+// ArO2_Update_Source): rates[G*tnrct] the averaged collision rates in (and
+// the neutral reaction channels the kernel fills, out); ave_e[G] the averaged
+// electron density; fden[nfsp*G]; bd1, bd2[G]; rr[tnrct]; src[nfsp*G] out.
+int rk_fluid_source(int gas, int G, int ngy, int tnrct, int nfsp, float *rates, const float *rr, const float *ave_e,
+                    const float *fden, const float *bd1, const float *bd2, float *src) {
+    return guarded([&] {
+        need(gas >= 0 && gas <= 2 && G > 0, "rk_fluid_source: bad gas or size");
+        // channels and fluid species the kernel indexes
+        need(tnrct >= (gas == 0 ? 10 : gas == 1 ? 67 : 88), "rk_fluid_source: too few channels");
+        need(nfsp >= (gas == 0 ? 1 : gas == 1 ? 4 : 5), "rk_fluid_source: too few fluid species");
+        Arena a;
+        std::vector<CollF> cf((size_t)tnrct);
+        for (int k = 0; k < tnrct; k++) {
+            std::memset(&cf[(size_t)k], 0, sizeof(CollF));
+            cf[(size_t)k].RR = rr[k];
+        }
+        std::vector<GPG> sp((size_t)G);
+        std::vector<GGA> bg((size_t)G);
+        for (int g = 0; g < G; g++) {
+            std::memset(&sp[(size_t)g], 0, sizeof(GPG));
+            std::memset(&bg[(size_t)g], 0, sizeof(GGA));
+            sp[(size_t)g].ave_den = ave_e[g];
+            bg[(size_t)g].BackDen1 = bd1[g];
+            bg[(size_t)g].BackDen2 = bd2[g];
+        }
+        std::vector<GFG> fg((size_t)nfsp * G), fs((size_t)nfsp * G);
+        for (size_t k = 0; k < fg.size(); k++) {
+            std::memset(&fg[k], 0, sizeof(GFG));
+            std::memset(&fs[k], 0, sizeof(GFG));
+            fg[k].n = fden[k];
+        }
+        float *dr = a.put(rates, (size_t)G * tnrct);
+        CollF *dc = a.put(cf);
+        GPG *dsp = a.put(sp);
+        GGA *dbg = a.put(bg);
+        GFG *dfg = a.put(fg);
+        GFG *dfs = a.put(fs);
+        const unsigned nb = blocks(G, 256);
+        if (gas == 0) Argon_Update_Source<<<nb, 256>>>(G, ngy, tnrct, dr, dc, dsp, dfg, dfs, dbg);
+        else if (gas == 1) Oxygen_Update_Source<<<nb, 256>>>(G, tnrct, dr, dc, dsp, dfg, dfs, dbg);
+        else ArO2_Update_Source<<<nb, 256>>>(G, ngy, tnrct, dr, dc, dsp, dfg, dfs, dbg);
+        sync("Update_Source");
+        std::vector<float> hr((size_t)G * tnrct);
+        get(hr, dr);
+        std::memcpy(rates, hr.data(), hr.size() * sizeof(float));
+        get(fs, dfs);
+        for (size_t k = 0; k < fs.size(); k++) src[k] = fs[k].n;
     });
 }
 

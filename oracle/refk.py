@@ -51,6 +51,7 @@ def lib():
             "rk_kinematics": (C.c_int, [C.c_int, _F, _F, C.c_int]),
             "rk_mcc_ar": (C.c_int, [P, _F, _I, C.c_float, _F, _F, _F, _F, _F, _F, _F, _F, _LL, _I,
                                     _F, _F, _F, _F, _F, _F, _LL]),
+            "rk_fluid_source": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _F, _F, _F, _F, _F, _F, _F]),
             "rk_oxy_collide": (C.c_int, [C.c_int, C.c_int, C.c_int, _I, C.c_float, _F, _F, _F, _F, C.c_int, _F,
                                          _F, _I, _F, _F, _F, C.c_int, _I, _F, _F, _LL]),
         }
@@ -276,3 +277,17 @@ def oxy_collide(gas, isp, imcc, idlogx, escale, vsave, table, sigv, collf, v, t,
                                 _f(f32(table)), _f(sg), sg.size, _f(f32(collf)), _f(v), _i(i32(t)), _f(f32(bv1)),
                                 _f(f32(bv2)), _f(u), nu, _i(cnt), _f(vout), _f(mccr), over.ctypes.data_as(_LL)))
     return cnt.reshape(n, nsp), vout.reshape(n, nsp, 4, 3), mccr.reshape(n, tnrct), int(over[0])
+
+
+def fluid_source(gas, ngy, rates, rr, ave_e, fden, bd1, bd2):
+    """The reference's Argon/Oxygen/ArO2_Update_Source on n nodes: rates
+    [n, tnrct] averaged collision rates, ave_e [n] averaged electron density,
+    fden [nfsp, n], bd1 and bd2 [n], rr [tnrct].  Returns (rates with the
+    neutral channels filled, sources [nfsp, n])."""
+    R = np.array(rates, np.float32, copy=True)
+    n, tnrct = R.shape
+    fden = np.ascontiguousarray(fden, np.float32)
+    S = np.zeros(fden.shape, np.float32)
+    _check(lib().rk_fluid_source(gas, n, ngy, tnrct, fden.shape[0], _f(R), _f(f32(rr)), _f(f32(ave_e)), _f(fden),
+                                 _f(f32(bd1)), _f(f32(bd2)), _f(S)))
+    return R, S

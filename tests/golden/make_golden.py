@@ -7,7 +7,7 @@ tests/golden/setup_<name>.npz together with the deck text and seed.  Needs
 the reference tree, so it runs only where that exists; the .npz files are
 committed and the tests read only them.
 
-usage: python tests/golden/make_golden.py [deck names]
+usage: python tests/golden/make_golden.py [--fluid] [deck names]
 """
 import json
 import os
@@ -77,6 +77,33 @@ FLUID = ["ar_33x17", "ar_block_33x21", "o2_33x17", "aro2_33x17", "ar_33x17_exp",
 FLUID_STEPS = 5
 
 
+# initial fluid densities of the pinned decks (the deck builder leaves them 0)
+FLUID_DENSITY = {"Ar*": 1e16, "O2A": 1e17, "O2B": 1e16, "OP": 1e18, "OD": 1e15}
+
+
+def with_fluid_density(deck):
+    d = json.loads(json.dumps(deck))
+
+    def walk(o):
+        if isinstance(o, dict):
+            for k, v in o.items():
+                if k in FLUID_DENSITY and isinstance(v, dict) and "Density" in v:
+                    v["Density"] = FLUID_DENSITY[k]
+                else:
+                    walk(v)
+        elif isinstance(o, list):
+            for v in o:
+                walk(v)
+
+    walk(d)
+    # the exponential and cosine decks load the fluid species the same way
+    gas = d["GasSpecies"]
+    if gas["ChargeSpecies"]["Loadtype"] in (1, 2):
+        gas["NeutralSpecies"]["Loadtype"] = gas["ChargeSpecies"]["Loadtype"]
+        gas["NeutralSpecies"]["LoadPosition(m)"] = dict(gas["ChargeSpecies"]["LoadPosition(m)"])
+    return d
+
+
 def dump_fluid(name, deck, seed):
     """The reference's fluid set-up (Fluid_Setting, Cal_D_*, the Gummel
     coefficients, the initial fluxes) and FLUID_STEPS steps of its
@@ -86,6 +113,7 @@ def dump_fluid(name, deck, seed):
     a seeded field of the size the collision rates give."""
     import hpic
     exe = os.path.join(REPO, "oracle", "_ref", "ref_dump")
+    deck = with_fluid_density(deck)
     S = hpic.Setup(deck, seed=seed, gas_temp_mode=0)
     temps = S.table("node_temp").astype(np.float32)
     nf, C = int(S.table("fluid_scalars")[3]), S.info.Csize
@@ -112,11 +140,14 @@ def dump_fluid(name, deck, seed):
 
 if __name__ == "__main__":
     only = set(sys.argv[1:])  # names to (re)generate; all when none are given
+    fluid_only = "--fluid" in only  # the fluid fixtures alone
+    only.discard("--fluid")
     for name, (deck, seed) in DECKS.items():
         if only and name not in only:
             continue
-        dump(name, deck, seed)
-        print("wrote", name)
+        if not fluid_only:
+            dump(name, deck, seed)
+            print("wrote", name)
         if name in FLUID:
             dump_fluid(name, deck, seed)
             print("wrote fluid", name)

@@ -2,7 +2,8 @@
 
 `make -C oracle ref_kernels` compiles the reference's src/cuda_Move.cu,
 cuda_Sortboundary.cu, cuda_Deposit.cu, cuda_Field.cu, cuda_mcc.cu,
-cuda_mccAr.cu, cuda_mccO2.cu and cuda_mccArO2.cu as they are, for sm_100a
+cuda_mccAr.cu, cuda_mccO2.cu, cuda_mccArO2.cu, cuda_Diagnostic.cu and
+cuda_Fluid.cu as they are, for sm_100a
 with the reference's own flags (-use_fast_math -rdc=true), into
 oracle/_ref/libref_kernels.so; oracle/refk.py runs its kernels on states these
 tests build from the oracle's.  The product kernels are compared with the
@@ -30,6 +31,9 @@ reference's code, which pins the restatement:
   reference's curand_uniform calls are routed to the lists by
   oracle/ref_shim.h), so every collision is compared one for one; the two
   draws passed to one kinematics call are taken left to right on both sides;
+* Argon_Update_Source, Oxygen_Update_Source and ArO2_Update_Source
+  (src/cuda_Diagnostic.cu:634-743) vs the oracle's fluid sources
+  (include/hp_fluid.h) on the same averaged rates and densities;
 * the Ar/O2 and O2 species handlers (src/cuda_mccArO2.cu:51-1129,
   src/cuda_mccO2.cu:2-866) vs the oracle's ladders, one collision per
   (species, target, energy, draws): this is what checks the channel tables.
@@ -488,3 +492,33 @@ def test_oxygen_ladders_match_reference(gas_name, gas):
     print(f"{gas_name}: {compared} collisions compared, {skipped} skipped (running sum undefined in the "
           f"reference), largest |dv|/|v_in| {worst:.1e}, channels hit {sorted(hit)}")
     assert len(hit) >= 0.5 * tnrct, f"{gas_name}: only {len(hit)} of {tnrct} channels exercised"
+
+
+# ------------------------------------------------------------ fluid sources
+@pytest.mark.parametrize("gas", ["Ar", "O2", "ArO2"])
+def test_fluid_sources(gas):
+    """The sources of the fluid species from averaged collision rates, node
+    densities and the background gas: every channel the sources sum is given
+    a rate of its own size, so a term added to the wrong species, with the
+    wrong sign or factor, or read from the wrong channel shows.  The
+    reference's kernels multiply and add in float as the restatement; its
+    -use_fast_math contraction only meets the 2 x R terms, which are exact."""
+    S = hpic.Setup(ccp_deck(17, 9, 0.005, 0.0025, gas=gas, ppc=4), seed=3)
+    info = S.info
+    g = {"Ar": 0, "O2": 1, "ArO2": 2}[gas]
+    n, tnrct, nf = 4096, info.n_reactions, info.n_fluid
+    rng = np.random.default_rng(11 + g)
+    rr = S.table("collf").reshape(-1, 4)[:, 3].astype(np.float32)
+    rates = (10 ** rng.uniform(18, 23, (n, tnrct)) * (rng.uniform(size=(n, tnrct)) > 0.1)).astype(np.float32)
+    ave_e = (10 ** rng.uniform(13, 17, n)).astype(np.float32)
+    fden = (10 ** rng.uniform(12, 19, (nf, n))).astype(np.float32)
+    bd1 = np.full(n, S.table("back_den1").max(), np.float32) * rng.uniform(0.5, 1.5, n).astype(np.float32)
+    bd2 = (bd1 * np.float32(0.25)).astype(np.float32) if g == 2 else np.zeros(n, np.float32)
+    R_ref, S_ref = refk.fluid_source(g, info.ngy, rates, rr, ave_e, fden, bd1, bd2)
+    eden = (0.25 * ave_e.astype(np.float64)).astype(np.float32)
+    R_or, S_or = oracle.fluid_sources(g, rates, fden, eden, bd1, bd2, rr)
+    assert np.array_equal(R_ref.view(np.uint32), R_or.view(np.uint32)), "neutral reaction rates"
+    scale = np.maximum(np.abs(S_ref), 1.0)
+    err = float(np.max(np.abs(S_ref.astype(np.float64) - S_or) / scale))
+    print(f"{gas}: {nf} fluid species x {n} nodes, largest relative difference {err:.1e}")
+    assert np.array_equal(S_ref.view(np.uint32), S_or.view(np.uint32)), f"sources differ (largest {err:.1e})"
