@@ -630,6 +630,7 @@ void hp_setup_destroy(hp_setup *s) { delete s; }
 hp_status hp_setup_get_info(const hp_setup *s, hp_case_info *out) {
     if (!s || !out) return HP_ERR_ARG;
     fill_info(s->s, out);
+    out->device_bytes = hpi::estimate_device_bytes(s->s, s->opts); // what a case built from it will hold
     return HP_OK;
 }
 

@@ -138,7 +138,7 @@ typedef struct hp_case_info {
     int mcc_subcycles;     /* DT_MCCn (src/cuda_mcc.cu:258-266) */
     double dt, dx, dy;
     int64_t tstep;         /* steps taken */
-    size_t device_bytes;   /* device memory held by the case */
+    size_t device_bytes;   /* device memory held by the case (of a set-up: the estimate the server admits by) */
     int pcg_cluster;       /* CTAs per case in the field-solve cluster */
     int pcg_block;         /* threads per CTA in the field solve */
     int field_mode;        /* solver in use: 2 falls back to 1 when the operator is not separable */
@@ -383,6 +383,20 @@ typedef struct hp_result {
  * are copied when the pointers are non-NULL.  *got = 0 when none is ready. */
 hp_status hp_server_take_result(hp_server *s, hp_result *r, double *ave_den, size_t den_cap,
                                 double *ave_phi, size_t phi_cap, int *got);
+
+/* ------------------------------------------------------------- several GPUs
+ * Cases -> devices for the batched and served forms on the GPUs of one node
+ * (no counterpart in the reference, which runs one case on one GPU).  Cases
+ * have no exchange step, so they shard by case: each device runs its share
+ * as a batch and the host gathers the results.  Longest-first greedy: cases
+ * in decreasing weight (ties: lower index) go to the device with the least
+ * weight so far among those whose remaining budget holds the case's bytes
+ * (ties: lower device).  weight: work per step (particles); bytes: device
+ * footprint (hp_case_info.device_bytes of the set-up); budget: bytes per
+ * device, NULL for none.  device_of[k] = -1 and HP_ERR_CAPACITY for a case
+ * that fits nowhere (the others are still placed).  Host only: needs no GPU. */
+hp_status hp_partition_cases(const double *weight, const size_t *bytes, int ncases, int ndevices,
+                             const size_t *budget, int *device_of);
 
 #ifdef __cplusplus
 }
