@@ -166,6 +166,61 @@ def move_traffic(workload):
     return None
 
 
+def kernel_traffic(kernel, workload):
+    """dram bytes per launch of a kernel from its committed ncu summary, if any."""
+    path = os.path.join(REPO, "profiles", f"{kernel}_{workload}.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("dram_bytes_per_launch:"):
+            return float(line.split(":")[1].split()[0])
+    return None
+
+
+def kernel_rooflines(case, stream, peak, peak_kind, workload, steps=3):
+    """Per-kernel device times of op-by-op steps (hp_profile_step: CUDA events
+    around every launch on the launching stream) and the HBM rooflines of
+    the kernels with an algorithmic byte count:
+      k_move           32 B per particle + 8 B per slot change
+      k_sort_push      41 B per mover (5 floats read and written, the code read)
+      k_deposit_cells  8 B per particle (x, y) + 32 B per (species, cell) corner sums
+      k_pcg            40 B per unknown per inner iteration (x, r, p, Ap, the
+                       stencil diagonal), field modes 0 and 1
+    Returns (kernels, rooflines)."""
+    info = case.info
+    nsp = info.nsp
+    parts = sum(case.particles_count(s) for s in range(nsp))
+    ch0 = case.slot_changes()
+    stats = case.profile(steps, stream)
+    changes = (case.slot_changes() - ch0) / steps
+    movers = sum(case.movers_count(s) for s in range(nsp))  # those of the last step
+    total = sum(ms for _, _, ms in stats)
+    kernels = [dict(name=n, launches_per_step=l / steps, ms_per_step=ms / steps, share=ms / total)
+               for n, l, ms in sorted(stats, key=lambda t: -t[2])]
+    bytes_per_launch = {
+        "k_move": 32.0 * parts + 8.0 * changes,
+        "k_sort_push": 41.0 * movers,
+        "k_deposit_cells": 8.0 * parts + 32.0 * nsp * info.Csize,
+    }
+    inner, outer = case.pcg_iters()
+    if inner > 0:
+        bytes_per_launch["k_pcg"] = 40.0 * info.n_unknowns * inner
+    rooflines = []
+    for n, l, ms in stats:
+        if n not in bytes_per_launch or l == 0:
+            continue
+        t = ms / l * 1e-3
+        ach = bytes_per_launch[n] / t / 1e9
+        r = dict(kernel=n, bound="hbm", achieved=ach, peak=peak, unit="GB/s", frac=ach / peak, peak_source=peak_kind,
+                 algorithmic_bytes_per_launch=bytes_per_launch[n], us_per_launch=t * 1e6,
+                 traffic=kernel_traffic(n, workload))
+        if n == "k_pcg":
+            r.update(inner_iterations=inner, outer_passes=outer, us_per_iteration=t * 1e6 / max(inner, 1),
+                     unknowns=info.n_unknowns)
+        rooflines.append(r)
+    return kernels, rooflines
+
+
 def peaks():
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -344,6 +399,7 @@ def run_ours(args, rank, world, local, dist):
     torch.cuda.synchronize()
     e2e_ms = allreduce(dist, f0.elapsed_time(f1), "max")
     e2e_pushes = allreduce(dist, case.pushes() - pe0, "sum")
+    kernels, rooflines = kernel_rooflines(case, stream, peak, peak_kind, args.workload)
 
     result = dict(
         metric=METRIC, value=pushes_all / (ms_max * 1e-3), unit=UNIT, n_gpus=world, steps=args.steps,
@@ -360,6 +416,8 @@ def run_ours(args, rank, world, local, dist):
         roofline=dict(bound="hbm", kernel="k_move", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
                       peak_source=peak_kind, traffic=traffic, algorithmic_bytes_per_launch=move_bytes),
         op_ms=op_ms,
+        kernels=kernels,
+        rooflines=rooflines,
         gpu_launches=case.step_kernels() * args.steps,
         clocks=clk,
     )

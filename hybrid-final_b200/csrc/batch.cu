@@ -46,12 +46,14 @@ hp_status batch_dev_build(hp_case *const *cases, int n, BatchDev &b) {
     b.max_smt = 0;
     b.surface = false;
     b.power = false;
+    b.circuit = false;
     for (int i = 0; i < n; i++) {
         hd[i] = cases[i]->h;
         b.any_eedf |= cases[i]->h.eedf_every > 0;
         b.max_smt = std::max(b.max_smt, cases[i]->s.N_smt);
         b.surface = b.surface || cases[i]->s.diel_num > 0;
-        b.power = b.power || cases[i]->s.power_driven();
+        b.power = b.power || cases[i]->s.power_driven() || cases[i]->s.external;
+        b.circuit = b.circuit || cases[i]->s.external;
         const Setup &s = cases[i]->s;
         part[i + 1] = part[i] + s.nsp * s.Csize;
         cell[i + 1] = cell[i] + s.Csize;
@@ -136,7 +138,7 @@ void batch_dev_free(BatchDev &b) {
 hp_status run_step(const BatchDev &b, const LaunchCfg &lc, int gas, cudaStream_t st) {
     CK(launch_advance(b.d_cases, b.n, st));
     const std::vector<PcgGroup> g = b.groups(lc.pcg_cluster_max, lc.pcg_block);
-    CK(launch_field(b.d_cases, b.d_node, b.n, b.n_node, g.data(), (int)g.size(), &b.fast.plan, st));
+    CK(launch_field(b.d_cases, b.d_node, b.n, b.n_node, g.data(), (int)g.size(), &b.fast.plan, st, b.circuit));
     CK(launch_move(b.d_cases, b.d_part, b.n, b.n_part, lc, st));
     CK(launch_sort(b.d_cases, b.d_part, b.n, b.n_part, lc, st, b.surface));
     if (gas != GAS_AR) CK(launch_mcc_oxy(b.d_cases, b.d_cell, b.n, b.n_cell, gas, st));

@@ -9,6 +9,7 @@
 #include <vector>
 
 #include "capi_internal.hpp"
+#include "prof.cuh"
 
 using namespace hp;
 
@@ -146,6 +147,7 @@ void fill_info(const Setup &s, hp_case_info *out) {
     out->power_driven = s.power_driven() ? 1 : 0;
     out->n_reactions = s.TnRct;
     out->n_fluid = s.nfsp;
+    out->circuit = s.external ? 1 : 0;
 }
 
 // Collision probability per cell from its lower-left node
@@ -305,6 +307,8 @@ hp_status build_device(hp_case *c) {
         if ((long long)C >= (1LL << 24)) return set_error("dielectric decks hold at most 2^24 cells"), HP_ERR_ARG;
     }
     if (c->opts.move_mode != 0 && c->opts.move_mode != 1) return set_error("move_mode must be 0 or 1"), HP_ERR_ARG;
+    if (c->opts.circuit_mode != 0 && c->opts.circuit_mode != 1)
+        return set_error("circuit_mode must be 0 or 1"), HP_ERR_ARG;
     for (int isp = 0; isp < s.nsp; isp++) {
         // a far mover's key holds its rank r < cap/2 in 18 bits
         if (s.cap[isp] > (1 << 19)) return set_error("cap_per_cell above 2^19"), HP_ERR_ARG;
@@ -364,7 +368,8 @@ hp_status build_device(hp_case *c) {
     }
     for (int k = 0; k < s.cond_numr; k++) h.efield_flag[k] = s.efield_flag[k];
     TRY(dupload(c, (float **)&h.src_amp, std::vector<float>(s.src_ac.begin(), s.src_ac.end())));
-    if (s.power_driven()) {
+    // the power controller's surface charge and absorbed counts also feed the external circuit
+    if (s.power_driven() || s.external) {
         for (int k = 0; k < s.src_num; k++) h.src_power[k] = s.src_power[k];
         for (int k = 0; k < s.cond_numr; k++) {
             h.cond_src_num[k] = s.cond_src_num[k];
@@ -377,11 +382,20 @@ hp_status build_device(hp_case *c) {
         std::vector<int> cn;
         for (int n = 0; n < G; n++)
             if (s.cond_id[n]) cn.push_back(n | ((s.cond_id[n] - 1) << 24));
-        if (G >= (1 << 24)) return set_error("power-driven decks hold at most 2^24 nodes"), HP_ERR_ARG;
+        if (G >= (1 << 24)) return set_error("power-driven and circuit decks hold at most 2^24 nodes"), HP_ERR_ARG;
         h.n_cond_nodes = (int)cn.size();
         TRY(dupload(c, (int **)&h.cond_nodes, cn));
     }
-    if (s.power_driven() || s.diel_num > 0) {
+    if (s.external) { // src/cuda_Field.cu:43-103
+        TRY(dalloc(c, &h.cs, 1));
+        h.circuit_mode = c->opts.circuit_mode;
+        const int nc = s.cond_numr;
+        for (int i = 0; i < nc; i++) {
+            for (int q = 0; q < 5; q++) h.cc_a[i * 5 + q] = s.cc_a[(size_t)i * 5 + q];
+            for (int j = 0; j < nc; j++) h.lap_sig[j * HP_CIRCUIT_MAX + i] = s.lap_sig[(size_t)j * nc + i];
+        }
+    }
+    if (s.power_driven() || s.diel_num > 0 || s.external) {
         TRY(dupload(c, (float **)&h.area, s.area));
         TRY(dalloc(c, &h.sigma, (size_t)G));
     }
@@ -535,7 +549,7 @@ hp_status op_field(hp_case *c, cudaStream_t st) {
     PcgGroup g{c->pcg_cluster, c->lc.pcg_block, c->d_list0, 1};
     const bool fast = c->h.field_mode == 2;
     cudaError_t e = launch_field(c->d_case, c->d_items + 4, 1, c->s.Gsize, &g, fast ? 0 : 1,
-                                 fast ? &c->fplan.plan : nullptr, st);
+                                 fast ? &c->fplan.plan : nullptr, st, c->h.cs != nullptr);
     return e == cudaSuccess ? HP_OK : cuda_fail(e, "field");
 }
 hp_status op_move(hp_case *c, cudaStream_t st) {
@@ -769,6 +783,10 @@ static hp_status table_of(const Setup &s, const std::vector<float> *prob, const 
         src = tmpf.data(); nb = tmpf.size() * 4; break;
     case 54: src = s.fluid_rate_f.data(); nb = s.fluid_rate_f.size() * 4; break;
     case 55: src = s.plasma_region.data(); nb = s.plasma_region.size() * 4; break;
+    case 56: // external circuit: CC_a per conductor, then Lap_SIG_Sol by basis
+        tmpf = s.cc_a;
+        tmpf.insert(tmpf.end(), s.lap_sig.begin(), s.lap_sig.end());
+        src = tmpf.data(); nb = tmpf.size() * 4; break;
     default: set_error("unknown table id"); return HP_ERR_ARG;
     }
     if (needed) *needed = nb;
@@ -976,6 +994,35 @@ hp_status hp_step(hp_case *c, int nsteps, void *stream) {
     return HP_OK;
 }
 
+hp_status hp_profile_step(hp_case *c, int nsteps, void *stream, hp_kernel_stat *out, int cap, int *n) {
+    if (!c || nsteps < 1 || !n || cap < 0 || (cap > 0 && !out)) return HP_ERR_ARG;
+    if (c->batch) return set_error("case belongs to a batch"), HP_ERR_ARG;
+    CK(cudaSetDevice(c->device));
+    cudaStream_t st = as_stream(stream);
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    CK(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return set_error("hp_profile_step cannot run inside a stream capture"), HP_ERR_ARG;
+    std::vector<std::string> names;
+    std::vector<int> launches;
+    std::vector<double> ms;
+    prof::begin();
+    hp_status s1 = HP_OK;
+    for (int k = 0; k < nsteps && s1 == HP_OK; k++) s1 = one_step(c, st);
+    prof::mark_slow(st, nullptr); // closes the last kernel
+    const bool ok = prof::end(names, launches, ms);
+    c->last_stream = st;
+    if (s1 != HP_OK) return s1;
+    if (!ok) return cuda_fail(cudaGetLastError(), "profile events");
+    *n = (int)names.size();
+    for (int k = 0; k < (int)names.size() && k < cap; k++) {
+        std::memset(out[k].name, 0, sizeof out[k].name);
+        std::strncpy(out[k].name, names[k].c_str(), sizeof out[k].name - 1);
+        out[k].launches = launches[k];
+        out[k].ms = ms[k];
+    }
+    return HP_OK;
+}
+
 hp_status hp_case_set_tune(hp_case *c, const hp_tune *t) {
     if (!c || !t) return HP_ERR_ARG;
     if (c->batch) return set_error("case belongs to a batch: tune the batch"), HP_ERR_ARG;
@@ -1114,6 +1161,7 @@ static hp_status grid_ptr(hp_case *c, hp_grid_field f, void **p, size_t *nb) {
     case HP_GRID_FLUID_FLUX_X: *p = c->h.fflx; *nb = (size_t)c->s.nfsp * c->s.ngx * c->s.ncy * 4; break;
     case HP_GRID_FLUID_FLUX_Y: *p = c->h.ffly; *nb = (size_t)c->s.nfsp * c->s.ncx * c->s.ngy * 4; break;
     case HP_GRID_FLUID_STATE: *p = c->fl_state; *nb = c->fl_state_bytes; break;
+    case HP_GRID_CIRCUIT: *p = c->h.cs; *nb = c->h.cs ? sizeof(CircuitState) : 0; break;
     default: return set_error("unknown grid field"), HP_ERR_ARG;
     }
     return HP_OK;

@@ -77,7 +77,8 @@ struct BatchDev {
     bool any_eedf = false;
     int max_smt = 0; // most density smoothing passes of any case
     bool surface = false; // some case has dielectric blocks
-    bool power = false;   // some case has power-driven sources
+    bool power = false;   // some case has power-driven sources or an external circuit
+    bool circuit = false; // some case has an external circuit
     int *d_fluid = nullptr; // fluid line prefixes: x lines [n+1], then y lines [n+1]
     hp::FluidPlan fluid;
     // PCG groups for every cluster cap 1,2,4,8,16: lists of case indices per

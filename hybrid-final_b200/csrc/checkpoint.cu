@@ -62,9 +62,9 @@ struct File {
     }
 };
 
-const char MAGIC[8] = {'H', 'P', 'I', 'C', 'X', '0', '0', '3'};
+const char MAGIC[8] = {'H', 'P', 'I', 'C', 'X', '0', '0', '4'};
 // the extension's format version; the magic's last digits carry the same number
-constexpr uint32_t EXT_VERSION = 3u;
+constexpr uint32_t EXT_VERSION = 4u;
 const char TAIL[8] = {'H', 'P', 'I', 'C', 'E', 'N', 'D', '1'};
 // grid fields carried by the extension, in file order
 const hp_grid_field EXT_GRIDS[] = {HP_GRID_EX,         HP_GRID_EY,          HP_GRID_PHI,     HP_GRID_PHI_POIS,
@@ -73,7 +73,8 @@ const hp_grid_field EXT_GRIDS[] = {HP_GRID_EX,         HP_GRID_EY,          HP_G
                                    HP_GRID_AVE_EY,     HP_GRID_COND_CHARGE, HP_GRID_MCC_COUNT, HP_GRID_EEDF,
                                    HP_GRID_SURFACE_CHARGE, HP_GRID_SIGMA, HP_GRID_SOURCE_AC, HP_GRID_POWER_STATE,
                                    HP_GRID_FLUID_CELL_DEN, HP_GRID_FLUID_DEN, HP_GRID_FLUID_SOURCE,
-                                   HP_GRID_FLUID_FLUX_X, HP_GRID_FLUID_FLUX_Y, HP_GRID_FLUID_STATE};
+                                   HP_GRID_FLUID_FLUX_X, HP_GRID_FLUID_FLUX_Y, HP_GRID_FLUID_STATE,
+                                   HP_GRID_CIRCUIT};
 
 template <class T> std::vector<T> fetch(hp_case *c, hp_grid_field f) {
     void *p = nullptr;

@@ -24,6 +24,7 @@
 #define HP_FAR_BUCKET 128
 
 #include "hpic.h" // HP_EEDF_BINS, HP_EEDF_DE
+#include "hp_circuit.h"
 
 namespace hp {
 
@@ -52,6 +53,16 @@ struct PowerState {
     int pad;
 };
 static_assert(sizeof(PowerState) == 8 * DMAXCOND * 3 + 4 * DMAXCOND * 2 + 8, "PowerState layout (the Python binding sizes it)");
+
+// The external circuit (src/cuda_Field.cu:43-103) per case: the circuit
+// charge history, the absorbed charge of the last step, and the conductor
+// potentials and Poisson-part surface charges of the last solve.
+struct CircuitState {
+    float q[4 * HP_CIRCUIT_MAX]; // q(t-1), q(t-2), q(t-3), q(t-4) per conductor
+    float qconv[HP_CIRCUIT_MAX]; // -sum_s q_density_s x particles absorbed in the last step
+    float phi[HP_CIRCUIT_MAX];   // conductor potentials (phi_cond)
+    float pois[HP_CIRCUIT_MAX];  // Pois_SIG_Sol
+};
 
 struct DevCase {
     // geometry
@@ -106,6 +117,11 @@ struct DevCase {
     float src_power[DMAXSRC];
     int pd_intv;
     float pd_ratio;
+    // external circuit (null cs without one)
+    CircuitState *cs;
+    int circuit_mode;                                   // hp_case_opts.circuit_mode
+    float cc_a[HP_CIRCUIT_MAX * 5];                     // coefficients per conductor (src/Efield.c:70-78)
+    float lap_sig[HP_CIRCUIT_MAX * HP_CIRCUIT_MAX];     // [j * HP_CIRCUIT_MAX + i]: conductor i in Laplace basis j
     // collisions
     const float *xsec;              // [n_logx * xw]
     int n_logx, xw;

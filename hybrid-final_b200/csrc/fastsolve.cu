@@ -12,6 +12,7 @@
 #include <cstdint>
 
 #include "kernels.cuh"
+#include "prof.cuh"
 
 namespace hp {
 namespace {
@@ -226,18 +227,22 @@ inline unsigned nblocks(long long threads, int per) { return (unsigned)((threads
 cudaError_t launch_fast_field(const DevCase *cases, const FastPlan &fp, cudaStream_t st) {
     if (fp.n <= 0) return cudaSuccess;
     for (int pass = 0; pass < fp.passes; pass++) {
+        prof::mark(st, "k_fs_resid");
         k_fs_resid<<<nblocks(fp.items, 256), 256, 0, st>>>(cases, fp.list, fp.item_start, fp.n, fp.items);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
         for (int s = 0; s < 4; s++) {
+            prof::mark(st, "k_gemm");
             k_gemm<<<(unsigned)fp.ntiles[s], GTHREADS, 0, st>>>(fp.probs[s], fp.n);
             e = cudaGetLastError();
             if (e != cudaSuccess) return e;
         }
     }
+    prof::mark(st, "k_fs_final");
     k_fs_final<<<dim3((unsigned)fp.final_chunks, (unsigned)fp.n), 256, 0, st>>>(cases, fp.list);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    prof::mark(st, "k_fs_norm");
     k_fs_norm<<<(unsigned)fp.n, 32, 0, st>>>(cases, fp.list);
     return cudaGetLastError();
 }

@@ -30,6 +30,7 @@
 #include "hp_fluid.h"
 #include "hp_math.h"
 #include "kernels.cuh"
+#include "prof.cuh"
 
 namespace hp {
 namespace {
@@ -199,15 +200,18 @@ cudaError_t launch_fluid(const DevCase *cases, const int *node_items, int ncases
         const size_t smem = (size_t)w * 16 * (size_t)L;
         if (dir == 0) {
             if (smem > 48 * 1024) cudaFuncSetAttribute(k_fluid_sweep<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            prof::mark(st, "k_fluid_sweep_x");
             k_fluid_sweep<0><<<blocks_for(items, w), 32 * w, smem, st>>>(cases, fp.xl_items, ncases, items, L);
         } else {
             if (smem > 48 * 1024) cudaFuncSetAttribute(k_fluid_sweep<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            prof::mark(st, "k_fluid_sweep_y");
             k_fluid_sweep<1><<<blocks_for(items, w), 32 * w, smem, st>>>(cases, fp.yl_items, ncases, items, L);
         }
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
     if (fp.n_x > 0 || fp.n_y > 0 || fp.any) {
+        prof::mark(st, "k_fluid_diag");
         k_fluid_diag<<<blocks_for(n_node_items, 256), 256, 0, st>>>(cases, node_items, ncases, n_node_items);
         return cudaGetLastError();
     }

@@ -19,6 +19,7 @@
 #include "hp_math.h"
 #include "hp_rng.h"
 #include "kernels.cuh"
+#include "prof.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -248,7 +249,10 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // the domain.
 // The particle loads are asynchronous copies into a ring of R chunk slots per
 // warp in shared memory, so that R - 1 chunks of every warp are in flight
-// without holding registers.
+// without holding registers.  vz is copied with the other arrays and written
+// back only where the slot changes: a per-particle load of it where needed
+// measured 4 % slower on the 257x129 case (148 vs 142 us) than the extra
+// 4 bytes per particle.
 constexpr int MOVE_RING = 4;
 
 template <int R>
@@ -272,24 +276,22 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
     // loads: issue them together (slots 0..31 of a cell are always inside the
     // pool, cap >= 32; lanes past the count are ignored)
     const int n = sp.cnt[c];
-    const int prev_m = sp.nmov[c]; // movers of the last step
     const float ex_ws = d.Ex[node], ex_wn = d.Ex[node + 1], ex_es = d.Ex[node + d.ngy], ex_en = d.Ex[node + d.ngy + 1];
     const float ey_ws = d.Ey[node], ey_wn = d.Ey[node + 1], ey_es = d.Ey[node + d.ngy], ey_en = d.Ey[node + d.ngy + 1];
     // chunk q of the cell (all 32 slots: k0 + 32 <= cap, as cap is a multiple
     // of 32 and k0 < n <= cap) goes to ring slot q % R as 16-byte copies: lanes
     // 0-7 x, 8-15 y, 16-23 vx, 24-31 vy, then lanes 0-7 vz; one commit group
-    // per chunk (possibly empty).  vz only when asked: a particle that keeps
-    // its slot keeps its vz.
+    // per chunk (possibly empty)
     const float *arr4 = lane < 8 ? sp.x : lane < 16 ? sp.y : lane < 24 ? sp.vx : sp.vy;
-    auto issue = [&](int k0, int lim, bool with_vz) {
+    auto issue = [&](int k0, int lim) {
         float *sl = ring + ((k0 >> 5) % R) * 160;
         if (k0 < lim) {
             cp_async16(sl + 4 * lane, arr4 + base + k0 + 4 * (lane & 7));
-            if (with_vz && lane < 8) cp_async16(sl + 128 + 4 * lane, sp.vz + base + k0 + 4 * lane);
+            if (lane < 8) cp_async16(sl + 128 + 4 * lane, sp.vz + base + k0 + 4 * lane);
         }
         cp_async_commit();
     };
-    issue(0, 32, true); // slots 0..31 of a cell are always inside the pool (cap >= 32)
+    issue(0, 32); // slots 0..31 of a cell are always inside the pool (cap >= 32)
     // an interior cell whose 3x3 neighbourhood is all plasma (ghost code 0):
     // a particle that ends in a neighbour after one wrap needs no walk
     const int g3 = lane < 9 ? d.sidx[(i + lane / 3) * (d.ncy + 2) + (j + lane % 3)] : 0;
@@ -310,11 +312,8 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
         cp_async_wait_all();
         return;
     }
-    // a cell that had movers last step will most likely shift its particles
-    // again: copy vz ahead too; otherwise only the shifted ones read it
-    const bool eager_vz = prev_m > 0;
 #pragma unroll
-    for (int q = 1; q < R - 1; q++) issue(q * 32, n, eager_vz);
+    for (int q = 1; q < R - 1; q++) issue(q * 32, n);
     const float As = sp.Ascale, dtdx = d.dt_dx, dtdy = d.dt_dy;
     const unsigned lt = lanemask_lt();
     int m = 0, shifted = 0;
@@ -326,13 +325,12 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
     for (int k0 = 0; k0 < n; k0 += 32) {
         const int k = k0 + lane;
         const bool act = k < n;
-        issue(k0 + (R - 1) * 32, n, eager_vz);
+        issue(k0 + (R - 1) * 32, n);
         cp_async_wait<R - 1>();
         __syncwarp(); // the chunk was copied by eight lanes per array
         const float *sl = ring + ((k0 >> 5) % R) * 160;
         float lx = sl[lane], ly = sl[32 + lane], vx = sl[64 + lane], vy = sl[96 + lane];
-        const bool have_vz = k0 == 0 || eager_vz;
-        float vz = have_vz ? sl[128 + lane] : 0.f;
+        const float vz = sl[128 + lane];
         // bilinear weights once, then fused multiply-adds (one rounding each)
         const float wx = 1 - lx, wy = 1 - ly;
         const float w00 = wx * wy, w01 = wx * ly, w10 = lx * wy, w11 = lx * ly;
@@ -385,7 +383,6 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
         const unsigned bout = __ballot_sync(FULL, out);
         const int before = m + __popc(bout & lt);
         const bool moved = act && (out || before != 0); // its slot changes
-        if (moved && !have_vz) vz = sp.vz[base + k];
         shifted += __popc(__ballot_sync(FULL, moved));
         __syncwarp(); // every lane's loads of this chunk precede the in-place stores
         if (act) {
@@ -1632,7 +1629,9 @@ __global__ void __launch_bounds__(256) k_potential(const DevCase *__restrict__ c
     const int n = t - item_start[ci];
     const double time = (double)(*d.tstep) * (double)d.dt;
     float tot = 0.0f;
-    for (int k = 0; k < d.cond_numr; k++) tot += cond_voltage(d, k, time) * d.lap[(size_t)k * d.G + n];
+    // with an external circuit the conductors sit at the circuit's potentials
+    for (int k = 0; k < d.cond_numr; k++)
+        tot += (d.cs ? d.cs->phi[k] : cond_voltage(d, k, time)) * d.lap[(size_t)k * d.G + n];
     tot += 1 * d.phi_p[n];
     d.phi[n] = tot;
 }
@@ -1662,6 +1661,23 @@ __device__ float cond_sigma(const DevCase &d, int n, int x, int y, int eT, int e
     default: return 0.0f;
     }
     (void)x; (void)y;
+}
+
+// Cond_Sigma at node n, with the index arithmetic of VtoEfield
+__device__ float cond_sigma_at(const DevCase &d, int n) {
+    const int ngx = d.ngx, ngy = d.ngy;
+    const int x = n / ngy, y = n - x * ngy;
+    const int pL = x ? n - ngy : n, pR = (x == ngx - 1) ? n : n + ngy;
+    const int pD = y ? n - 1 : n, pU = (y == ngy - 1) ? n : n + 1;
+    int eT = x * (ngy - 1) + y;
+    int eL = x ? eT - ngy + 1 : eT;
+    int eD = y ? eT - 1 : eT;
+    const int eX = eL + eD - eT;
+    const int xo = (x == ngx - 1) ? ngy - 1 : 0, yo = (y == ngy - 1) ? 1 : 0;
+    eT -= (xo + yo);
+    eL -= yo;
+    eD -= xo;
+    return cond_sigma(d, n, x, y, eT, eL, eD, eX, pL, pR, pD, pU);
 }
 
 // VtoEfield (src/cuda_Field.cu:698-846): E = -grad phi at nodes with the
@@ -1831,12 +1847,14 @@ __global__ void __launch_bounds__(PW_T) k_power(DevCase *cases, int ncases) {
         P.old2[i] = P.old[i];
         P.old[i] = P.surf[i];
         P.surf[i] = part[0][i];
-        float cond_current = 0.0f;
+        float cond_current = 0.0f, q_conv = 0.0f;
         for (int s = 0; s < d.nsp; s++) {
             unsigned int &cnt = d.cond_step[s * nc + i];
             cond_current += d.sp[s].q_density * (float)cnt / d.dt;
+            q_conv -= d.sp[s].q_density * (float)cnt; // the circuit's convective charge (src/cuda_Field.cu:61-64)
             cnt = 0;
         }
+        if (d.cs) d.cs->qconv[i] = q_conv;
         const float dis_current = (float)(0.5 * (3.0 * P.surf[i] - 4.0 * P.old[i] + P.old2[i]) / (double)d.dt);
         const float current = dis_current - cond_current;
         if (d.cond_src_num[i] != 1) continue; // voltage driven, or the reference's (empty) dual-power branch
@@ -1855,6 +1873,53 @@ __global__ void __launch_bounds__(PW_T) k_power(DevCase *cases, int ncases) {
         P.power[i] = 0.0f;
         P.power_init++;
     }
+    (void)ncases;
+}
+
+// Efield_cuda's circuit (src/cuda_Field.cu:43-81), once per step after the
+// Poisson solve, one block per case (cases without a circuit return): the
+// surface charge of this step's Poisson part, Sigma (Cond_Sigma on phi_p,
+// den of the last Deposit) x Area over the conductor nodes, summed as
+// k_power sums the surface charge (FP64, a strided share per thread, then a
+// fixed tree; rounded to float, where the reference adds floats with
+// atomics), then the circuit solve of hp_circuit.h on one thread with the
+// last step's surface charge and absorbed charge.  k_potential then puts the
+// conductors at the circuit's potentials.
+__global__ void __launch_bounds__(PW_T) k_circuit(DevCase *cases, int ncases) {
+    const DevCase &d = cases[blockIdx.x];
+    if (!d.cs) return;
+    __shared__ double part[PW_T][HP_CIRCUIT_MAX];
+    const int t = threadIdx.x, nc = d.cond_numr;
+    double acc[HP_CIRCUIT_MAX];
+#pragma unroll
+    for (int k = 0; k < HP_CIRCUIT_MAX; k++) acc[k] = 0.0;
+    for (int q = t; q < d.n_cond_nodes; q += PW_T) {
+        const int v = d.cond_nodes[q], n = v & 0xFFFFFF, k = v >> 24;
+        const int b = d.boundary[n], f = d.face[n];
+        const double sg = ((b == 3 || b == 1) && f != 8) ? (double)cond_sigma_at(d, n) : 0.0;
+        const double a = sg * (double)d.area[n];
+#pragma unroll
+        for (int kk = 0; kk < HP_CIRCUIT_MAX; kk++)
+            if (kk == k) acc[kk] += a;
+    }
+#pragma unroll
+    for (int k = 0; k < HP_CIRCUIT_MAX; k++) part[t][k] = acc[k];
+    __syncthreads();
+    for (int h = PW_T / 2; h > 0; h >>= 1) {
+        if (t < h)
+            for (int k = 0; k < nc; k++) part[t][k] += part[t + h][k];
+        __syncthreads();
+    }
+    if (t != 0) return;
+    CircuitState &C = *d.cs;
+    const double time = (double)(*d.tstep) * (double)d.dt;
+    float vt[HP_CIRCUIT_MAX], surf[HP_CIRCUIT_MAX], pois[HP_CIRCUIT_MAX];
+    for (int i = 0; i < nc; i++) {
+        vt[i] = cond_voltage(d, i, time);
+        surf[i] = (float)d.pw->surf[i];
+        pois[i] = (float)part[0][i];
+    }
+    hp_circuit_step(nc, d.cc_a, d.lap_sig, vt, C.qconv, surf, pois, C.q, C.phi, C.pois, d.circuit_mode);
     (void)ncases;
 }
 
@@ -1951,6 +2016,7 @@ cudaError_t launch_move(const DevCase *cases, const int *item_start, int ncases,
     if (items <= 0) return cudaSuccess;
     const int tpb = 32 * std::min(std::max(lc.warps_per_block, 1), 16);
     const unsigned nb = blocks_for((long long)items * 32, tpb);
+    prof::mark(st, "k_move");
     if (lc.move_unroll == 2) k_move_u<2><<<nb, tpb, 0, st>>>(cases, item_start, ncases, items);
     else if (lc.move_unroll == 4) k_move_u<4><<<nb, tpb, 0, st>>>(cases, item_start, ncases, items);
     else
@@ -1961,6 +2027,7 @@ cudaError_t launch_move(const DevCase *cases, const int *item_start, int ncases,
 
 cudaError_t launch_power(DevCase *cases, int ncases, cudaStream_t st) {
     if (ncases <= 0) return cudaSuccess;
+    prof::mark(st, "k_power");
     k_power<<<ncases, PW_T, 0, st>>>(cases, ncases);
     return cudaGetLastError();
 }
@@ -1969,6 +2036,7 @@ cudaError_t launch_sort(const DevCase *cases, const int *item_start, int ncases,
                         cudaStream_t st, bool surface) {
     if (items <= 0) return cudaSuccess;
     if (surface) {
+        prof::mark(st, "k_surface");
         k_surface<<<ncases, 256, 0, st>>>(cases, ncases);
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -1976,10 +2044,12 @@ cudaError_t launch_sort(const DevCase *cases, const int *item_start, int ncases,
     // at least 8 warps per block: the push gains from them even where Move
     // and Deposit prefer smaller blocks
     const int tpb = 32 * std::min(std::max(lc.warps_per_block, 8), SORT_MAXW);
+    prof::mark(st, "k_sort_push");
     k_sort_push<<<blocks_for((long long)(items + SORT_G - 1) / SORT_G * 32, tpb), tpb, 0, st>>>(cases, item_start,
                                                                                                ncases, items);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    prof::mark(st, "k_sort_count");
     k_sort_count<<<blocks_for((long long)(items + 31) / 32 * 32, tpb), tpb, 0, st>>>(cases, item_start, ncases,
                                                                                      items);
     return cudaGetLastError();
@@ -1990,6 +2060,7 @@ cudaError_t launch_mcc_ar(const DevCase *cases, const int *item_start, int ncase
     if (items <= 0) return cudaSuccess;
     const int g = lc.mcc_cells;
     const long long threads = (long long)((items + g - 1) / g) * 32;
+    prof::mark(st, "k_mcc_ar");
     if (g == 1) k_mcc_ar<1><<<blocks_for(threads, MCC_TPB), MCC_TPB, 0, st>>>(cases, item_start, ncases, items);
     else if (g == 2) k_mcc_ar<2><<<blocks_for(threads, MCC_TPB), MCC_TPB, 0, st>>>(cases, item_start, ncases, items);
     else if (g == 8) k_mcc_ar<8><<<blocks_for(threads, MCC_TPB), MCC_TPB, 0, st>>>(cases, item_start, ncases, items);
@@ -2001,17 +2072,24 @@ cudaError_t launch_mcc_ar(const DevCase *cases, const int *item_start, int ncase
 cudaError_t launch_deposit(const DevCase *cases, const int *cell_items, const int *node_items, int ncases,
                            int n_cell_items, int n_node_items, const LaunchCfg &lc, cudaStream_t st, int max_smt) {
     const int tpb = 32 * std::min(std::max(lc.warps_per_block, 1), 16);
-    if (n_cell_items > 0)
+    if (n_cell_items > 0) {
+        prof::mark(st, "k_deposit_cells");
         k_deposit_cells<<<blocks_for((long long)(n_cell_items + DEP_G - 1) / DEP_G * 32, tpb), tpb, 0, st>>>(cases, cell_items, ncases,
                                                                                         n_cell_items);
+    }
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    if (n_node_items > 0)
+    if (n_node_items > 0) {
+        prof::mark(st, "k_deposit_nodes");
         k_deposit_nodes<<<blocks_for(n_node_items, 256), 256, 0, st>>>(cases, node_items, ncases, n_node_items);
+    }
     if (max_smt > 0 && n_node_items > 0) {
         for (int p = 0; p < max_smt; p++)
-            for (int yy = 0; yy < 2; yy++)
+            for (int yy = 0; yy < 2; yy++) {
+                prof::mark(st, "k_smooth");
                 k_smooth<<<blocks_for(n_node_items, 256), 256, 0, st>>>(cases, node_items, ncases, n_node_items, p, yy);
+            }
+        prof::mark(st, "k_source");
         k_source<<<blocks_for(n_node_items, 256), 256, 0, st>>>(cases, node_items, ncases, n_node_items);
     }
     return cudaGetLastError();
@@ -2025,7 +2103,7 @@ int pcg_cluster_for_nodes(int G) {
 }
 
 cudaError_t launch_field(const DevCase *cases, const int *node_items, int ncases, int n_node_items,
-                         const PcgGroup *groups, int ngroups, const FastPlan *fast, cudaStream_t st) {
+                         const PcgGroup *groups, int ngroups, const FastPlan *fast, cudaStream_t st, bool circuit) {
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(k_pcg, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
@@ -2046,6 +2124,7 @@ cudaError_t launch_field(const DevCase *cases, const int *node_items, int ncases
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
         cfg.numAttrs = 1;
+        prof::mark(st, "k_pcg");
         cudaError_t e = cudaLaunchKernelEx(&cfg, k_pcg, cases, pg.list, pg.n);
         if (e != cudaSuccess) return e;
     }
@@ -2053,9 +2132,17 @@ cudaError_t launch_field(const DevCase *cases, const int *node_items, int ncases
         cudaError_t ef = launch_fast_field(cases, *fast, st);
         if (ef != cudaSuccess) return ef;
     }
+    if (circuit) {
+        prof::mark(st, "k_circuit");
+        k_circuit<<<ncases, PW_T, 0, st>>>(const_cast<DevCase *>(cases), ncases);
+        cudaError_t ec = cudaGetLastError();
+        if (ec != cudaSuccess) return ec;
+    }
+    prof::mark(st, "k_potential");
     k_potential<<<blocks_for(n_node_items, 256), 256, 0, st>>>(cases, node_items, ncases, n_node_items);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    prof::mark(st, "k_efield");
     k_efield<<<blocks_for(n_node_items, 256), 256, 0, st>>>(cases, node_items, ncases, n_node_items);
     return cudaGetLastError();
 }
@@ -2066,12 +2153,14 @@ cudaError_t launch_scatter(const DevSpecies &sp, int C, const int *start, const 
 }
 
 cudaError_t launch_advance(const DevCase *cases, int ncases, cudaStream_t st) {
+    prof::mark(st, "k_advance");
     k_advance<<<blocks_for(ncases, 128), 128, 0, st>>>(cases, ncases);
     return cudaGetLastError();
 }
 
 cudaError_t launch_eedf(const DevCase *cases, const int *cell_items, int ncases, int n_cell_items, cudaStream_t st) {
     if (n_cell_items <= 0) return cudaSuccess;
+    prof::mark(st, "k_eedf");
     k_eedf<<<blocks_for((long long)n_cell_items * 32, 256), 256, 0, st>>>(cases, cell_items, ncases, n_cell_items);
     return cudaGetLastError();
 }
@@ -2079,6 +2168,7 @@ cudaError_t launch_eedf(const DevCase *cases, const int *cell_items, int ncases,
 cudaError_t launch_accumulate(const DevCase *cases, const int *node_items, int ncases, int n_node_items,
                               cudaStream_t st) {
     if (n_node_items <= 0) return cudaSuccess;
+    prof::mark(st, "k_accumulate");
     k_accumulate<<<blocks_for(n_node_items, 256), 256, 0, st>>>(cases, node_items, ncases, n_node_items);
     return cudaGetLastError();
 }

@@ -74,7 +74,8 @@ constexpr int FS_CHUNK = 1024;
 constexpr int FS_TILE = 32; // GEMM output tile edge
 cudaError_t launch_fast_field(const DevCase *cases, const FastPlan &fp, cudaStream_t st);
 cudaError_t launch_field(const DevCase *cases, const int *node_items, int ncases, int n_node_items,
-                         const PcgGroup *groups, int ngroups, const FastPlan *fast, cudaStream_t st);
+                         const PcgGroup *groups, int ngroups, const FastPlan *fast, cudaStream_t st,
+                         bool circuit = false);
 // CTAs per case for a grid of G nodes
 int pcg_cluster_for_nodes(int G);
 // CSR particles (5 arrays of start[C] floats back to back: x, y, vx, vy, vz)

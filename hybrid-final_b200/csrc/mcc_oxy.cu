@@ -35,6 +35,7 @@
 
 #include "devutil.cuh"
 #include "kernels.cuh"
+#include "prof.cuh"
 
 namespace hp {
 namespace {
@@ -775,6 +776,7 @@ cudaError_t launch_mcc_oxy(const DevCase *cases, const int *item_start, int ncas
     if (items <= 0) return cudaSuccess;
     constexpr int G = OXY_G;
     const unsigned nb = (unsigned)(((items + G - 1) / G * 32LL + OXY_TPB - 1) / OXY_TPB);
+    prof::mark(st, "k_mcc_oxy");
     if (gas == 2) k_mcc_oxy<2, G><<<nb, OXY_TPB, 0, st>>>(cases, item_start, ncases, items);
     else if (gas == 1) k_mcc_oxy<1, G><<<nb, OXY_TPB, 0, st>>>(cases, item_start, ncases, items);
     else return cudaErrorNotSupported;

@@ -8,6 +8,7 @@
 // Arithmetic keeps the reference's float/double mix so that tables compare
 // bit-exactly with the reference's own set-up code (tests/test_setup.py).
 #include "setup.hpp"
+#include "hp_circuit.h"
 #include "json.hpp"
 
 #include <algorithm>
@@ -210,9 +211,14 @@ void read_geometry(const JVal &root, Setup &s, std::vector<int> &bx0, std::vecto
         s.cond_x0.push_back(x0); s.cond_x1.push_back(x1); s.cond_y0.push_back(y0); s.cond_y1.push_back(y1);
         s.cond_temp.push_back(fnum(c, "Temp"));
         float R = fnum(c, "R(Ohm)"), L = fnum(c, "L(H)"), C = fnum(c, "C(F)");
+        s.cond_R.push_back(R);
+        s.cond_L.push_back(L);
+        s.cond_C.push_back(C);
         if (!(L < 1e-30f && R < 1e-30f && C >= 1)) external = 1; // src/start.c:173-177
     }
-    if (external) unsupported("external circuit (R/L/C on a conductor) is outside this library's step path");
+    s.external = external != 0;
+    if (s.external && s.cond_numr > HP_CIRCUIT_MAX)
+        unsupported("external circuit with more than " + std::to_string(HP_CIRCUIT_MAX) + " conductors");
     const auto &src = geo.array("Source");
     s.src_num = (int)src.size();
     s.max_freq = 0.0f;
@@ -887,6 +893,75 @@ std::vector<double> setup_solve(const Setup &s, const std::vector<float> &vals, 
     return x;
 }
 
+// External circuit, Source_setting's coefficients (src/Efield.c:70-78): per
+// conductor id (the last ConductorSpec line of an M_ID sets them), in the
+// reference's mixed precision -- the terms with a double literal in double,
+// the integer-literal ones in float, 1/C in float.
+void circuit_coefficients(Setup &s) {
+    s.cc_a.assign((size_t)s.cond_numr * 5, 0.0f);
+    const double dtd = (double)s.dt;
+    for (size_t i = 0; i < s.cond_mid.size(); i++) {
+        const float L = s.cond_L[i], R = s.cond_R[i], C = s.cond_C[i], dt = s.dt;
+        float *a = &s.cc_a[(size_t)(s.cond_mid[i] - 1) * 5];
+        a[0] = (float)(2.25 * (double)L / dtd / dtd + 1.5 * (double)R / dtd + (double)(1 / C));
+        a[1] = -6 * L / dt / dt - 2 * R / dt;
+        a[2] = (float)(5.5 * (double)L / dtd / dtd + .5 * (double)R / dtd);
+        a[3] = -2 * L / dt / dt;
+        a[4] = (float)(.25 * (double)L / dtd / dtd);
+    }
+}
+
+// The charge each conductor carries in each Laplace basis (PCG_SOLVER_Laplace,
+// src/cuda_Field.cu:207-216): Cond_Sigma_Lap (src/cuda_Field.cu:448-499) at
+// the conductor and Dirichlet face nodes, times the node Area, summed per
+// CondID in node order in float.  lap_sig[k * cond_numr + i]: basis k,
+// conductor i.
+void circuit_laplace_charges(Setup &s) {
+    const int ngx = s.ngx, ngy = s.ngy, G = s.Gsize, nc = s.cond_numr;
+    std::vector<float> eps((size_t)s.Csize);
+    for (int k = 0; k < s.Csize; k++) eps[k] = (float)(EPS0 * s.eps_r[k]);
+    s.lap_sig.assign((size_t)nc * nc, 0.0f);
+    const double dx = (double)s.dx, dy = (double)s.dy;
+    for (int k = 0; k < nc; k++) {
+        const float *P = &s.lap_basis[(size_t)k * G];
+        for (int n = 0; n < G; n++) {
+            if (!s.cond_id[n]) continue;
+            const int b = s.boundary[n], f = s.face[n];
+            float sig = 0.0f; // the reference clears the buffer before the kernel
+            if ((b == 3 || b == 1) && f != 8) {
+                const int x = n / ngy, y = n - x * ngy;
+                int eT = x * (ngy - 1) + y;
+                int eL = x ? eT - ngy + 1 : eT;
+                int eD = y ? eT - 1 : eT;
+                const int eX = eL + eD - eT;
+                const int xo = (x == ngx - 1) ? ngy - 1 : 0, yo = (y == ngy - 1) ? 1 : 0;
+                eT -= xo + yo;
+                eL -= yo;
+                eD -= xo;
+                const int pL = x ? n - ngy : n, pR = (x == ngx - 1) ? n : n + ngy;
+                const int pD = y ? n - 1 : n, pU = (y == ngy - 1) ? n : n + 1;
+                auto up = [&] { return 0.5 * (double)(eps[eT] + eps[eL]) * (double)(P[n] - P[pU]) / dy; };
+                auto down = [&] { return 0.5 * (double)(eps[eD] + eps[eX]) * (double)(P[n] - P[pD]) / dy; };
+                auto left = [&] { return 0.5 * (double)(eps[eL] + eps[eX]) * (double)(P[n] - P[pL]) / dx; };
+                auto right = [&] { return 0.5 * (double)(eps[eT] + eps[eD]) * (double)(P[n] - P[pR]) / dx; };
+                switch (f) {
+                case 2: sig = (float)up(); break;
+                case 3: sig = (float)down(); break;
+                case 0: sig = (float)left(); break;
+                case 1: sig = (float)right(); break;
+                case 4: sig = (float)(up() + left()); break;
+                case 5: sig = (float)(up() + right()); break;
+                case 6: sig = (float)(down() + left()); break;
+                case 7: sig = (float)(down() + right()); break;
+                default: break;
+                }
+            }
+            float &acc = s.lap_sig[(size_t)k * nc + (s.cond_id[n] - 1)];
+            acc += sig * s.area[n];
+        }
+    }
+}
+
 void laplace_and_gas(Setup &s, int gas_temp_mode) {
     const int N = s.n_unknowns, G = s.Gsize;
     // Laplace basis: conductor k at 1 V, the others at 0 V (src/cuda_Field.cu:192-219)
@@ -1431,10 +1506,12 @@ void build_setup(const char *json, size_t len, const BuildOpts &o, Setup &s) {
                 if (s.cond_src_num[i] == 0) s.cond_power_id[i] = j;
                 s.cond_src_num[i]++;
             }
+    if (s.external) circuit_coefficients(s);
     field_matrix(s);
     gas_setting(s, o);
     null_collision(s);
     laplace_and_gas(s, o.gas_temp_mode);
+    if (s.external) circuit_laplace_charges(s);
     fluid_setting(s);
 }
 

@@ -65,6 +65,10 @@ struct Setup {
     int cond_num = 0, cond_numr = 0;
     std::vector<int> cond_mid, cond_x0, cond_x1, cond_y0, cond_y1;
     std::vector<float> cond_temp;
+    std::vector<float> cond_R, cond_L, cond_C;     // per ConductorSpec line
+    bool external = false;                         // an R/L/C circuit on some conductor (External_Flag)
+    std::vector<float> cc_a;                       // [cond_numr*5] circuit coefficients (src/Efield.c:70-78)
+    std::vector<float> lap_sig;                    // [cond_numr*cond_numr] charge on conductor i of Laplace basis k at k*n+i
     int src_num = 0;
     std::vector<int> src_mid;
     std::vector<float> src_dc, src_ac, src_freq, src_2pifreq, src_rphase;

@@ -23,10 +23,12 @@ HP_OK, HP_ERR_ARG, HP_ERR_DECK, HP_ERR_CUDA, HP_ERR_OOM, HP_ERR_UNSUPPORTED, HP_
 STATUS_CELL_OVERFLOW, STATUS_NONFINITE, STATUS_PCG_NOCONV, STATUS_WAIT_TIMEOUT = 1, 2, 4, 8
 STATUS_WALK_BOUND, STATUS_SURFACE_OVERFLOW = 0x10, 0x20
 
+# conductors an external circuit may have (HP_CIRCUIT_MAX, include/hp_circuit.h)
+CIRCUIT_MAX = 4
 GRID = dict(EX=0, EY=1, PHI=2, PHI_POIS=3, DEN=4, SOURCE=5, PCG_X=6, PCG_B=7, AVE_DEN=8, AVE_PHI=9,
             COND_CHARGE=10, MCC_COUNT=11, EEDF=12, AVE_SOURCE=13, AVE_EX=14, AVE_EY=15,
             SURFACE_CHARGE=16, SIGMA=17, SOURCE_AC=18, POWER_STATE=19, FLUID_CELL_DEN=20, FLUID_DEN=21,
-            FLUID_SOURCE=22, FLUID_FLUX_X=23, FLUID_FLUX_Y=24, FLUID_STATE=25)
+            FLUID_SOURCE=22, FLUID_FLUX_X=23, FLUID_FLUX_Y=24, FLUID_STATE=25, CIRCUIT=26)
 SIGMA_FRAC_BITS = 28  # fixed-point fraction bits of SURFACE_CHARGE (particle weights)
 POWER_STATE_BYTES = 8 * 8 * 3 + 4 * 8 * 2 + 8  # PowerState: surf, old, old2 (double[8]); power, count; flags
 EEDF_BINS, EEDF_DE = 200, 0.25  # electron energy histogram: 0.25 eV bins from 0, one overflow bin
@@ -37,7 +39,7 @@ TABLE = dict(sidx=0, a_idx=1, boundary=2, face=3, cond_id=4, area=5, back_den1=6
              fs_info=33, fs_V=34, fs_Vt=35, fs_W=36, fs_Wt=37, fs_inv=38, sig_mode=39, power=40,
              fluid_cell_den=41, fluid_xlines=42, fluid_ylines=43, fluid_xl_fg=44, fluid_yl_fg=45, fluid_gax=46,
              fluid_gbx=47, fluid_gay=48, fluid_gby=49, fluid_flux_x0=50, fluid_flux_y0=51, fluid_D=52,
-             fluid_scalars=53, fluid_rate_f=54, plasma_region=55)
+             fluid_scalars=53, fluid_rate_f=54, plasma_region=55, circuit=56)
 TABLE_DTYPE = {0: np.int32, 1: np.int32, 2: np.int32, 3: np.int32, 4: np.int32, 14: np.int32, 20: np.int32,
                21: np.int32, 32: np.int32, 33: np.int32, 39: np.int32, 42: np.int32, 43: np.int32, 55: np.int32}
 
@@ -52,7 +54,8 @@ class CaseOpts(C.Structure):
     _fields_ = [("seed", C.c_uint64), ("cap_per_cell", C.c_int), ("field_mode", C.c_int),
                 ("pcg_rtol", C.c_double), ("pcg_max_iter", C.c_int), ("o2_all_species", C.c_int),
                 ("device", C.c_int), ("gas_temp_mode", C.c_int), ("move_mode", C.c_int),
-                ("fs_passes", C.c_int), ("eedf_every", C.c_int), ("gpu_load", C.c_int), ("fluid_fixed", C.c_int)]
+                ("fs_passes", C.c_int), ("eedf_every", C.c_int), ("gpu_load", C.c_int), ("fluid_fixed", C.c_int),
+                ("circuit_mode", C.c_int)]
 
 
 class CaseInfo(C.Structure):
@@ -62,7 +65,7 @@ class CaseInfo(C.Structure):
                 ("dx", C.c_double), ("dy", C.c_double), ("tstep", C.c_int64), ("device_bytes", C.c_size_t),
                 ("pcg_cluster", C.c_int), ("pcg_block", C.c_int), ("field_mode", C.c_int), ("mcc_stride", C.c_int),
                 ("n_smt", C.c_int), ("n_dielectric", C.c_int), ("n_sources", C.c_int),
-                ("power_driven", C.c_int), ("n_reactions", C.c_int), ("n_fluid", C.c_int)]
+                ("power_driven", C.c_int), ("n_reactions", C.c_int), ("n_fluid", C.c_int), ("circuit", C.c_int)]
 
 
 class Tune(C.Structure):
@@ -71,6 +74,10 @@ class Tune(C.Structure):
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class KernelStat(C.Structure):
+    _fields_ = [("name", C.c_char * 32), ("launches", C.c_int), ("ms", C.c_double)]
 
 
 class ServerOpts(C.Structure):
@@ -115,6 +122,7 @@ _SIGS = {
     "hp_case_set_tune": (C.c_int, [_P, _P]),
     "hp_case_get_tune": (C.c_int, [_P, _P]),
     "hp_batch_step_kernels": (C.c_int, [_P, C.POINTER(C.c_int)]),
+    "hp_profile_step": (C.c_int, [_P, C.c_int, _P, C.POINTER(KernelStat), C.c_int, C.POINTER(C.c_int)]),
     "hp_Deposit_noalloc": (C.c_int, [_P, _P, _P]),
     "hp_get_particles": (C.c_int, [_P, C.c_int, _I, _F, _F, _F, _F, _F, C.c_size_t, C.POINTER(C.c_size_t)]),
     "hp_set_particles": (C.c_int, [_P, C.c_int, _I, _F, _F, _F, _F, _F]),
@@ -381,7 +389,8 @@ class Case:
                      FLUID_CELL_DEN=(nf * info.Csize, np.float32), FLUID_DEN=(nf * G, np.float32),
                      FLUID_SOURCE=(nf * info.Csize, np.float32), FLUID_FLUX_X=(nf * info.ngx * info.ncy, np.float32),
                      FLUID_FLUX_Y=(nf * info.ncx * info.ngy, np.float32),
-                     FLUID_STATE=(G * 8 + info.Csize * info.mcc_stride * 4 + 3 * info.Csize * 4, np.uint8))
+                     FLUID_STATE=(G * 8 + info.Csize * info.mcc_stride * 4 + 3 * info.Csize * 4, np.uint8),
+                     CIRCUIT=(7 * CIRCUIT_MAX if info.circuit else 0, np.float32))
         n, dt = sizes[name]
         out = np.zeros(n, dtype=dt)
         _check(lib().hp_get_grid(self.h, GRID[name], out.ctypes.data_as(_P), out.nbytes))
@@ -417,6 +426,21 @@ class Case:
 
     def n_particles(self):
         return [int(self.particles_count(s)) for s in range(self.info.nsp)]
+
+    def movers_count(self, isp):
+        """Movers parked in the cells by the last Move (their number only)."""
+        n = C.c_size_t(0)
+        _check(lib().hp_get_movers(self.h, isp, None, None, None, None, None, None, None, 0, C.byref(n)))
+        return n.value
+
+    def profile(self, n=1, stream=None):
+        """Per-kernel device times of n op-by-op steps (hp_profile_step):
+        [(name, launches, ms)] in the order the kernels first ran."""
+        cap = 64
+        out = (KernelStat * cap)()
+        k = C.c_int(0)
+        _check(lib().hp_profile_step(self.h, int(n), stream, out, cap, C.byref(k)))
+        return [(out[i].name.decode(), out[i].launches, out[i].ms) for i in range(min(k.value, cap))]
 
     def particles_count(self, isp):
         n = C.c_size_t(0)

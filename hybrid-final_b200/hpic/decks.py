@@ -47,12 +47,15 @@ def ccp_deck(ngx, ngy, xlen, ylen, *, gas="Ar", pressure_torr=0.05, voltage=100.
              freq=13.56e6, steps_per_cycle=400, ppc=50, density=1e15, te_ev=2.0,
              ti_ev=0.026, gas_k=300.0, max_np_factor=4, aro2_ratio=(80, 20),
              ion_density=None, pcg_tol=1e-3, smoothing=0, load_type=0, load_pos=None, ratio=1,
-             power_w=0.0, pd_interval=5.0, average_iter=None):
+             power_w=0.0, pd_interval=5.0, average_iter=None, circuit=None):
     """Build one CCP deck.
 
     ppc is the macro-particles per cell per species at `density`; np2c is
     chosen so that the reference loader's integer n_per_cell
-    (src/Particle.c:10) comes out at exactly ppc.
+    (src/Particle.c:10) comes out at exactly ppc.  circuit = (R, L, C)
+    puts that series R-L-C between the powered electrode and its source
+    (the reference's external circuit); None keeps R = L = 0, C = 1 F on
+    both electrodes, which the reference reads as no circuit.
     """
     dx = xlen / (ngx - 1)
     dy = ylen / (ngy - 1)
@@ -67,9 +70,10 @@ def ccp_deck(ngx, ngy, xlen, ylen, *, gas="Ar", pressure_torr=0.05, voltage=100.
         {"X0": 0, "X1": ngx - 1, "Y0": 0, "Y1": 0, "B.C": 3, "Temp": gas_k},
         {"X0": 0, "X1": ngx - 1, "Y0": ngy - 1, "Y1": ngy - 1, "B.C": 3, "Temp": gas_k},
     ]
+    r_, l_, c_ = circuit if circuit is not None else (0.0, 0.0, 1.0)
     cond = [
         {"M_ID": 1, "X0": 0, "X1": ngx - 1, "Y0": 0, "Y1": 0, "Temp": gas_k,
-         "R(Ohm)": 0.0, "L(H)": 0.0, "C(F)": 1.0},
+         "R(Ohm)": float(r_), "L(H)": float(l_), "C(F)": float(c_)},
         {"M_ID": 2, "X0": 0, "X1": ngx - 1, "Y0": ngy - 1, "Y1": ngy - 1, "Temp": gas_k,
          "R(Ohm)": 0.0, "L(H)": 0.0, "C(F)": 1.0},
     ]
@@ -147,18 +151,23 @@ def ccp_deck(ngx, ngy, xlen, ylen, *, gas="Ar", pressure_torr=0.05, voltage=100.
     return deck
 
 
-def block_deck():
+def block_deck(circuits=None, ppc=8, voltage=100.0, max_np_factor=4):
     """A 33 x 21 CCP with thick block electrodes (node rows 0-2 and 18-20)
     and a floating block conductor inside (nodes 12-18 x 8-11): exercises the
     conductor-face classification and the >= 100 StructureIndex codes, so
-    particles are absorbed on (and counted for) conductors."""
-    d = ccp_deck(33, 21, 0.01, 0.00625, ppc=8)
+    particles are absorbed on (and counted for) conductors.  circuits: an
+    (R, L, C) per conductor (M_ID 1, 2, 3), the reference's external circuit;
+    None is R = L = 0, C = 1 F everywhere (no circuit)."""
+    d = ccp_deck(33, 21, 0.01, 0.00625, ppc=ppc, voltage=voltage, max_np_factor=max_np_factor)
     geo = d["Geometry"]
+    rlc = circuits or [(0.0, 0.0, 1.0)] * 3
     geo["ConductorSpec"] = [
-        {"M_ID": 1, "X0": 0, "X1": 32, "Y0": 0, "Y1": 2, "Temp": 300.0, "R(Ohm)": 0.0, "L(H)": 0.0, "C(F)": 1.0},
-        {"M_ID": 2, "X0": 0, "X1": 32, "Y0": 18, "Y1": 20, "Temp": 300.0, "R(Ohm)": 0.0, "L(H)": 0.0, "C(F)": 1.0},
-        {"M_ID": 3, "X0": 12, "X1": 18, "Y0": 8, "Y1": 11, "Temp": 350.0, "R(Ohm)": 0.0, "L(H)": 0.0, "C(F)": 1.0},
+        {"M_ID": 1, "X0": 0, "X1": 32, "Y0": 0, "Y1": 2, "Temp": 300.0},
+        {"M_ID": 2, "X0": 0, "X1": 32, "Y0": 18, "Y1": 20, "Temp": 300.0},
+        {"M_ID": 3, "X0": 12, "X1": 18, "Y0": 8, "Y1": 11, "Temp": 350.0},
     ]
+    for c, (r_, l_, c_) in zip(geo["ConductorSpec"], rlc):
+        c.update({"R(Ohm)": float(r_), "L(H)": float(l_), "C(F)": float(c_)})
     geo["BoundaryCondition"] = [
         {"X0": 0, "X1": 0, "Y0": 0, "Y1": 20, "B.C": 2, "Temp": 300.0},
         {"X0": 32, "X1": 32, "Y0": 0, "Y1": 20, "B.C": 2, "Temp": 300.0},

@@ -118,6 +118,13 @@ typedef struct hp_case_opts {
                             continuity solve, fed every AverageIter + 1 steps by the averaged collision
                             rates (src/cuda_Fluid.cu:34-167, src/cuda_Diagnostic.cu:268-330); 1 = hold
                             them at their initial densities */
+    int circuit_mode;    /* external circuit (R/L/C on a conductor): 0 = the reference's update
+                            (src/cuda_Field.cu:49-80), which divides V - K_t (a voltage minus a charge)
+                            by cc0, advances every conductor's circuit charge with the history term K_t
+                            of the last conductor and carries only the Poisson part of a conductor's
+                            charge from step to step; 1 = a charge balance: V / cc0 - K_t, each
+                            conductor's own K_t, and its whole charge (Laplace and Poisson parts)
+                            carried, changed only by the circuit and the absorbed particles */
 } hp_case_opts;
 
 /* Default options. */
@@ -149,6 +156,7 @@ typedef struct hp_case_info {
     int power_driven;      /* 1 when a conductor has a power-driven source (Power(W) != 0) */
     int n_reactions;       /* TnRct: reaction channels of the gas's collision set */
     int n_fluid;           /* nfsp: fluid species (1 Ar: Ar*; 4 O2: O2(a), O2(b), O, O(1D); 5 Ar/O2: Ar* first) */
+    int circuit;           /* 1 when a conductor has an R/L/C external circuit (the reference's External_Flag) */
 } hp_case_info;
 hp_status hp_case_get_info(const hp_case *c, hp_case_info *out);
 hp_status hp_setup_get_info(const hp_setup *s, hp_case_info *out);
@@ -261,9 +269,13 @@ typedef enum hp_grid_field {
     HP_GRID_FLUID_SOURCE = 22,   /* float[nfsp*Csize] sources of the last average (GFC.Source, m^-3 s^-1) */
     HP_GRID_FLUID_FLUX_X = 23,   /* float[nfsp*ngx*ncy] x-face fluxes at i*ncy + j (GFC.flux_x) */
     HP_GRID_FLUID_FLUX_Y = 24,   /* float[nfsp*ncx*ngy] y-face fluxes at i*ngy + j (GFC.flux_y) */
-    HP_GRID_FLUID_STATE = 25     /* the averaging window: electron density sum (double[Gsize]), tallies at
+    HP_GRID_FLUID_STATE = 25,    /* the averaging window: electron density sum (double[Gsize]), tallies at
                                   the last average (uint32[Csize*mcc_stride]) and the collision
                                   probabilities (float[3*Csize]); carried by checkpoints */
+    HP_GRID_CIRCUIT = 26         /* external circuit (0 bytes without one), float[28] (HP_CIRCUIT_MAX = 4): the
+                                  circuit charge q(t-1..t-4) per conductor (4 rows of HP_CIRCUIT_MAX), the
+                                  absorbed charge of the last step, the conductor potentials and the
+                                  Poisson-part surface charges of the last solve (src/cuda_Field.cu:43-103) */
 } hp_grid_field;
 hp_status hp_get_grid(hp_case *c, hp_grid_field f, void *out, size_t bytes);
 hp_status hp_set_grid(hp_case *c, hp_grid_field f, const void *in, size_t bytes);
@@ -304,6 +316,21 @@ hp_status hp_case_pushes(hp_case *c, int64_t *pushes);
  * (32 B per particle + 8 B per slot change).  No reference counterpart. */
 hp_status hp_case_slot_changes(hp_case *c, int64_t *changes);
 
+/* Per-kernel device times of nsteps steps run operator by operator on
+ * `stream` (not the captured graph of hp_step): every kernel launch is
+ * bracketed by CUDA events, and the entries sum each kernel's launches and
+ * milliseconds, in the order the kernels first ran.  *n = the number of
+ * kernels; at most cap entries are written.  Not inside a stream capture;
+ * one profile at a time per process.  The measurement tool behind the bench's
+ * per-kernel rooflines (the reference times whole operators with events,
+ * src/cuda_main.cu:112-236). */
+typedef struct hp_kernel_stat {
+    char name[32];
+    int launches;
+    double ms;
+} hp_kernel_stat;
+hp_status hp_profile_step(hp_case *c, int nsteps, void *stream, hp_kernel_stat *out, int cap, int *n);
+
 /* Case tables (constant over a run), for checkers and tools.  `what`:
  * 0 StructureIndex int[(ncx+2)(ncy+2)], 1 A_idx int[Gsize], 2 node Boundary int[Gsize],
  * 3 node Face int[Gsize], 4 node CondID int[Gsize], 5 node Area float[Gsize],
@@ -316,7 +343,11 @@ hp_status hp_case_slot_changes(hp_case *c, int64_t *changes);
  * domain edge: Sigma doubled, 3 conductor: surface charge cleared),
  * 40 power-driven sources float[2 + nsrc + 2*CondNUMR]: steps between
  * revisions, VoltageUpDownRatio, target power per source, then per conductor
- * its number of power-driven sources and the first one's index. */
+ * its number of power-driven sources and the first one's index,
+ * 56 external circuit float[5*CondNUMR + CondNUMR^2] (empty without one): the
+ * coefficients CC_a per conductor (src/Efield.c:70-78), then the charge on
+ * conductor i of the Laplace basis of conductor k at k*CondNUMR + i
+ * (Lap_SIG_Sol, src/cuda_Field.cu:207-216). */
 hp_status hp_get_table(hp_case *c, int what, void *out, size_t bytes, size_t *bytes_needed);
 hp_status hp_setup_get_table(const hp_setup *s, int what, void *out, size_t bytes, size_t *bytes_needed);
 

@@ -22,6 +22,7 @@
 #include <thread>
 
 #include "hp_fluid.h"
+#include "hp_circuit.h"
 #include "hp_math.h"
 #include "hp_rng.h"
 #include "hpic.h"
@@ -102,6 +103,11 @@ struct SimBase {
         int power_init;
     } pw{};
     std::vector<int> cond_list; // nodes with a CondID, in node order
+    // external circuit: charge history, absorbed charge of the last step,
+    // conductor potentials and Poisson-part surface charges of the last solve
+    struct {
+        float q[4 * HP_CIRCUIT_MAX], qconv[HP_CIRCUIT_MAX], phi[HP_CIRCUIT_MAX], pois[HP_CIRCUIT_MAX];
+    } circ{};
     // Scripted uniforms, for pinning against the reference's own MCC code:
     // when on, every MCC draw (null-collision tests included) is taken in
     // order from a per-key list instead of Philox; key = cell, or species *
@@ -419,6 +425,7 @@ template <class R> struct Sim : SimBase {
         case 13: std::memcpy(f, fsrc.data(), fsrc.size() * 4); break;
         case 14: std::memcpy(f, fflx.data(), fflx.size() * 4); break;
         case 15: std::memcpy(f, ffly.data(), ffly.size() * 4); break;
+        case 16: std::memcpy(f, &circ, sizeof circ); break;
         }
     }
     void set_grid(int which, const void *in) override {
@@ -443,6 +450,7 @@ template <class R> struct Sim : SimBase {
         case 13: std::memcpy(fsrc.data(), f, fsrc.size() * 4); break;
         case 14: std::memcpy(fflx.data(), f, fflx.size() * 4); break;
         case 15: std::memcpy(ffly.data(), f, ffly.size() * 4); break;
+        case 16: std::memcpy(&circ, f, sizeof circ); break;
         }
     }
 
@@ -651,7 +659,7 @@ template <class R> struct Sim : SimBase {
                             code = 15;
                             if (cond >= 0 && cond < c.cond_numr) {
                                 cond_charge[(size_t)s * c.cond_numr + cond] += 1.0f;
-                                if (c.n_power > 0) cond_step[(size_t)s * c.cond_numr + cond]++;
+                                if (c.n_power > 0 || c.external) cond_step[(size_t)s * c.cond_numr + cond]++;
                             } else if (cond <= -2 && c.n_diel > 0) hits.push_back({s, fi, fj, -2 - cond, lx, ly, mvX, mvY});
                             if (r == 2) walk_bound_hit = true;
                         } else {
@@ -1901,6 +1909,7 @@ template <class R> struct Sim : SimBase {
                                              (double)src_amp[q] * std::sin((double)c.src_2pif[q] * time + (double)c.src_rphase[q])));
             vk[k] = v;
         }
+        if (c.external) circuit(vk);
         for (int n = 0; n < G; n++) {
             R tot = 0;
             for (int k = 0; k < c.cond_numr; k++) tot += vk[k] * (R)c.lap[(size_t)k * G + n];
@@ -1929,7 +1938,7 @@ template <class R> struct Sim : SimBase {
             R ex, ey;
             bool write = true;
             // Cond_Sigma's Sigma at conductor and Dirichlet face nodes (the power controller's input)
-            if ((c.n_power > 0 || c.n_diel > 0) && (b == 3 || b == 1) && f != 8)
+            if ((c.n_power > 0 || c.n_diel > 0 || c.external) && (b == 3 || b == 1) && f != 8)
                 sigma[n] = (double)cond_sigma(n, eT, eL, eD, eX, pL, pR, pD, pU);
             if (f == 0) {
                 if (b == 3 || b == 2 || b == 1) {
@@ -2006,11 +2015,52 @@ template <class R> struct Sim : SimBase {
         }
     }
 
+    // Efield_cuda's circuit (src/cuda_Field.cu:43-81) as the kernel computes
+    // it: the surface charge of this step's Poisson part per conductor
+    // (Cond_Sigma on phi_p x Area, FP64, list entry q added to partial q % 256,
+    // the partials reduced by halving, rounded to float), then the circuit
+    // solve of hp_circuit.h; vk becomes the conductors' potentials.
+    template <class V> void circuit(V &vk) {
+        const int nc = c.cond_numr, ngx = c.ngx, ngy = c.ngy;
+        std::vector<double> part((size_t)256 * 8, 0.0);
+        for (size_t q = 0; q < cond_list.size(); q++) {
+            const int n = cond_list[q];
+            const int b = c.boundary[n], f = c.face[n];
+            double sg = 0.0;
+            if ((b == 3 || b == 1) && f != 8) {
+                const int x = n / ngy, y = n - x * ngy;
+                const int pL = x ? n - ngy : n, pR = (x == ngx - 1) ? n : n + ngy;
+                const int pD = y ? n - 1 : n, pU = (y == ngy - 1) ? n : n + 1;
+                int eT = x * (ngy - 1) + y;
+                int eL = x ? eT - ngy + 1 : eT;
+                int eD = y ? eT - 1 : eT;
+                const int eX = eL + eD - eT;
+                const int xo = (x == ngx - 1) ? ngy - 1 : 0, yo = (y == ngy - 1) ? 1 : 0;
+                eT -= (xo + yo);
+                eL -= yo;
+                eD -= xo;
+                sg = (double)(float)cond_sigma(n, eT, eL, eD, eX, pL, pR, pD, pU);
+            }
+            part[(q % 256) * 8 + (c.cond_id[n] - 1)] += sg * (double)c.area[n];
+        }
+        for (int h = 128; h > 0; h >>= 1)
+            for (int t = 0; t < h; t++)
+                for (int k = 0; k < nc; k++) part[(size_t)t * 8 + k] += part[(size_t)(t + h) * 8 + k];
+        float vt[HP_CIRCUIT_MAX], surf[HP_CIRCUIT_MAX], pois[HP_CIRCUIT_MAX];
+        for (int i = 0; i < nc; i++) {
+            vt[i] = (float)vk[i];
+            surf[i] = (float)pw.surf[i];
+            pois[i] = (float)part[i];
+        }
+        hp_circuit_step(nc, c.cc_a, c.lap_sig, vt, circ.qconv, surf, pois, circ.q, circ.phi, circ.pois, c.circuit_mode);
+        for (int i = 0; i < nc; i++) vk[i] = circ.phi[i];
+    }
+
     // The reference's power controller (src/cuda_Diagnostic.cu:365-420) as
     // the kernel computes it: surface charge per conductor in FP64, list entry
     // q added to partial q % 256, the 256 partials reduced by halving.
     void power(int64_t tstep) override {
-        if (c.n_power <= 0) return;
+        if (c.n_power <= 0 && !c.external) return;
         const int nc = c.cond_numr;
         std::vector<double> part((size_t)256 * 8, 0.0);
         for (size_t q = 0; q < cond_list.size(); q++) {
@@ -2025,12 +2075,14 @@ template <class R> struct Sim : SimBase {
             pw.old2[i] = pw.old[i];
             pw.old[i] = pw.surf[i];
             pw.surf[i] = part[i];
-            float cond_current = 0.0f;
+            float cond_current = 0.0f, q_conv = 0.0f;
             for (int s = 0; s < c.nsp; s++) {
                 unsigned &cnt = cond_step[(size_t)s * nc + i];
                 cond_current += c.q_density[s] * (float)cnt / c.dt;
+                q_conv -= c.q_density[s] * (float)cnt; // the circuit's convective charge
                 cnt = 0;
             }
+            if (c.external) circ.qconv[i] = q_conv;
             const float dis_current = (float)(0.5 * (3.0 * pw.surf[i] - 4.0 * pw.old[i] + pw.old2[i]) / (double)c.dt);
             const float current = dis_current - cond_current;
             if (c.cond_src_num[i] != 1) continue;
@@ -2213,6 +2265,13 @@ void or_get_averages(or_sim *s, double *ave_den, double *ave_phi, int64_t *count
     if (count) *count = b->ave_count;
 }
 int or_num_threads(void) { return nthreads(); }
+// the circuit arithmetic of hp_circuit.h, for checking it against the
+// reference's own cofactor and a transcription of Efield_cuda
+void or_circuit_inverse(float *m, int n) { hp_ci_inverse(m, n); }
+void or_circuit_step(int nc, const float *cc, const float *lap, const float *vt, const float *qconv,
+                     const float *surf, const float *pois_new, float *q, float *phi, float *pois, int mode) {
+    hp_circuit_step(nc, cc, lap, vt, qconv, surf, pois_new, q, phi, pois, mode);
+}
 void or_set_threads(int n) { g_threads = n; }
 
 } // extern "C"

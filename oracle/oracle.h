@@ -88,6 +88,11 @@ typedef struct or_case {
     const float *flux_x0, *flux_y0;     /* initial fluxes, same layouts */
     const int *plasma;                  /* [C] PlasmaRegion */
     float rate_f[96], rr[96];           /* rate factor per channel (tally -> m^-3 s^-1), CollF.RR */
+    /* external circuit (src/cuda_Field.cu:43-103): present when external != 0 */
+    int external;
+    float cc_a[20];    /* [4*5] coefficients per conductor */
+    float lap_sig[16]; /* [j*4 + i] charge on conductor i of the Laplace basis of conductor j */
+    int circuit_mode;   /* hp_case_opts.circuit_mode */
 } or_case;
 
 typedef struct or_sim or_sim;
@@ -111,6 +116,10 @@ void or_get_movers(or_sim *s, int isp, int *counts, float *x, float *y, float *v
  * per node (float[nfsp*G]); 13 fluid source per cell (float[nfsp*C]); 14 fluid x fluxes
  * (float[nfsp*ngx*ncy]); 15 fluid y fluxes (float[nfsp*ncx*ngy]) */
 void or_get_grid(or_sim *s, int which, void *out);
+/* hp_circuit.h: the reference's cofactor inverse (m: n x n, row stride 4) and one circuit step */
+void or_circuit_inverse(float *m, int n);
+void or_circuit_step(int nc, const float *cc, const float *lap, const float *vt, const float *qconv,
+                     const float *surf, const float *pois_new, float *q, float *phi, float *pois, int mode);
 void or_set_grid(or_sim *s, int which, const void *in);
 void or_get_counters(or_sim *s, float *cond_charge, unsigned *mcc_count, int *pcg_iters);
 /* 1 once a move_mode 1 walk reached its crossing bound (the particle was absorbed) */

@@ -52,6 +52,7 @@ class OrCase(C.Structure):
         ("fluid_cell_den", _F), ("fluid_den", _F), ("xl", _I), ("yl", _I), ("xl_fg", _F), ("yl_fg", _F),
         ("gax", _F), ("gbx", _F), ("gay", _F), ("gby", _F), ("flux_x0", _F), ("flux_y0", _F), ("plasma", _I),
         ("rate_f", C.c_float * 96), ("rr", C.c_float * 96),
+        ("external", C.c_int), ("cc_a", C.c_float * 20), ("lap_sig", C.c_float * 16), ("circuit_mode", C.c_int),
     ]
 
 
@@ -125,7 +126,7 @@ class Oracle:
     (hpic.Case.table or hpic.Setup.table); `info` the case info."""
 
     GRID = dict(EX=0, EY=1, PHI=2, PHI_POIS=3, DEN=4, SOURCE=5, B=6, X=7, SURFACE_CHARGE=8, SIGMA=9, SOURCE_AC=10,
-                FLUID_CELL_DEN=11, FLUID_DEN=12, FLUID_SOURCE=13, FLUID_FLUX_X=14, FLUID_FLUX_Y=15)
+                FLUID_CELL_DEN=11, FLUID_DEN=12, FLUID_SOURCE=13, FLUID_FLUX_X=14, FLUID_FLUX_Y=15, CIRCUIT=16)
 
     def __init__(self, tables, info, opts, precision=32, pcg_cluster=1, pcg_block=512, field_mode=None,
                  fs_passes=None):
@@ -204,6 +205,16 @@ class Oracle:
         c.n_diel = info.n_dielectric
         c.sig_mode = keep("sgm", t("sig_mode"), np.int32)
         c.area = keep("area", t("area"), np.float32)
+        c.external = getattr(info, "circuit", 0)
+        c.circuit_mode = getattr(opts, "circuit_mode", 0)
+        if c.external:  # CC_a per conductor, then the Laplace bases' conductor charges
+            tc = t("circuit")
+            nc = info.cond_numr
+            for i in range(nc):
+                for q in range(5):
+                    c.cc_a[i * 5 + q] = tc[i * 5 + q]
+                for j in range(nc):
+                    c.lap_sig[j * 4 + i] = tc[5 * nc + j * nc + i]
         c.n_power = info.power_driven
         pw = t("power")
         c.pd_intv, c.pd_ratio = int(pw[0]), pw[1]
@@ -305,7 +316,9 @@ class Oracle:
     def grid(self, name):
         G, nsp = self.info.Gsize, self.info.nsp
         w = self.GRID[name]
-        if w >= 11:
+        if w == 16:
+            out = np.zeros(28, np.float32)
+        elif w >= 11:
             nf, info = int(self.c.nfsp), self.info
             n = {11: nf * info.Csize, 12: nf * G, 13: nf * info.Csize, 14: nf * info.ngx * info.ncy, 15: nf * info.ncx * info.ngy}[w]
             out = np.zeros(n, np.float32)

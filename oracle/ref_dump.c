@@ -47,6 +47,8 @@ extern int CondNUM, CondNUMR, SrcNUM, DielNUM;
 extern int *SrcM_ID;
 extern float *SrcDC, *SrcAC, *SrcFREQ, *SrcPHASE, *SrcRPHASE, *Src2piFREQ;
 extern int *Efield_Flag;
+extern int External_Flag;
+extern float **CC_a;
 extern int DT_PIC, DT_CONTI, N_ave;
 extern GGA *vec_G;
 extern GCA *vec_C;
@@ -142,6 +144,12 @@ int main(int argc, char **argv) {
     for (int k = 0; k < CondNUMR; k++) fprintf(m, "efield_flag%d %d\n", k, Efield_Flag[k]);
     fclose(m);
 
+    if (External_Flag) { /* external circuit coefficients (src/Efield.c:70-78), CondNUMR rows of 5 */
+        float *a = (float *)malloc((size_t)CondNUMR * 5 * sizeof(float));
+        for (int k = 0; k < CondNUMR; k++) memcpy(a + (size_t)k * 5, CC_a[k], 5 * sizeof(float));
+        wr("cc_a", a, (size_t)CondNUMR * 5 * sizeof(float));
+        free(a);
+    }
     wr("gga", vec_G, (size_t)Gsize * sizeof(GGA));
     wr("gca", vec_C, (size_t)Csize * sizeof(GCA));
     wr("sidx", vec_StructureIndex, (size_t)(ncx + 2) * (ncy + 2) * sizeof(int));

@@ -31,6 +31,9 @@ DECKS = {
     "ar_17x9": (ccp_deck(17, 9, 0.005, 0.0025, ppc=10), 12345),
     "ar_33x17": (ccp_deck(33, 17, 0.01, 0.005, ppc=20, pressure_torr=0.1, voltage=200.0), 777),
     "ar_block_33x21": (block_deck(), 4242),
+    # an R-L-C on the driven electrode and a capacitor on the floating block (src/Efield.c:70-78)
+    "ar_circuit_33x21": (block_deck(circuits=[(50.0, 1e-6, 1e-9), (0.0, 0.0, 1.0), (2.0, 0.0, 1e-12)], ppc=16,
+                                    voltage=200.0), 4444),
     "ar_diel_33x21": (dielectric_deck(), 4343),
     "aro2_33x17": (ccp_deck(33, 17, 0.01, 0.005, gas="ArO2", ppc=12, pressure_torr=0.1, voltage=200.0, te_ev=3.0,
                             ion_density={"Ar+": 1e15, "O2+": 2e14, "O+": 0.0, "O-": 2e14}), 515),

@@ -172,11 +172,10 @@ def test_deck_errors():
     with pytest.raises(hpic.HpicError) as e:
         hpic.Setup(bad)
     assert e.value.status == hpic.HP_ERR_DECK
-    bad = json.loads(json.dumps(deck))
-    bad["Geometry"]["ConductorSpec"][0]["R(Ohm)"] = 50.0
-    with pytest.raises(hpic.HpicError) as e:
-        hpic.Setup(bad)
-    assert e.value.status == hpic.HP_ERR_UNSUPPORTED
+    # an R/L/C on a conductor is the external circuit (tests/test_circuit.py)
+    ok = json.loads(json.dumps(deck))
+    ok["Geometry"]["ConductorSpec"][0]["R(Ohm)"] = 50.0
+    assert hpic.Setup(ok).info.circuit == 1
     bad = json.loads(json.dumps(deck))
     bad["SimulationMethod"]["PCGMarginOfError"] = 0
     with pytest.raises(hpic.HpicError) as e:

@@ -18,11 +18,12 @@ from hpic.decks import ccp_deck  # noqa: E402
 
 
 def _decks():
-    return [ccp_deck(33, 17, 0.01, 0.005, ppc=8, voltage=150.0),
-            ccp_deck(65, 33, 0.02, 0.01, ppc=12, voltage=100.0),
-            ccp_deck(33, 17, 0.01, 0.005, ppc=16, voltage=200.0, gas="ArO2", pressure_torr=0.1),
-            ccp_deck(17, 9, 0.005, 0.0025, ppc=20, voltage=80.0),
-            ccp_deck(65, 33, 0.02, 0.01, ppc=6, voltage=250.0)]
+    # slots for 8x the load per cell: no cell reaches the half-full (ReArg) status
+    return [ccp_deck(33, 17, 0.01, 0.005, ppc=8, voltage=150.0, max_np_factor=8),
+            ccp_deck(65, 33, 0.02, 0.01, ppc=12, voltage=100.0, max_np_factor=8),
+            ccp_deck(33, 17, 0.01, 0.005, ppc=16, voltage=200.0, gas="ArO2", pressure_torr=0.1, max_np_factor=8),
+            ccp_deck(17, 9, 0.005, 0.0025, ppc=20, voltage=80.0, max_np_factor=8),
+            ccp_deck(65, 33, 0.02, 0.01, ppc=6, voltage=250.0, max_np_factor=8)]
 
 
 def test_longest_first_placement():
@@ -127,7 +128,8 @@ def test_sharded_run_equals_each_case_alone():
         c = hpic.Case(deck=deck, seed=seed)
         c.step(12)
         r = res[k]
-        assert r["status"] == 0 and r["steps"] == 12 and r["pushes"] == c.pushes()
+        assert r["status"] == c.status() == 0
+        assert r["steps"] == 12 and r["pushes"] == c.pushes()
         assert np.array_equal(r["ave_phi"].view(np.uint64), c.grid("AVE_PHI").view(np.uint64))
         assert np.array_equal(r["ave_den"].reshape(-1).view(np.uint64), c.grid("AVE_DEN").view(np.uint64))
         c.close()
