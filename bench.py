@@ -157,22 +157,17 @@ def replica_throughput(dist, units, ms, device="cuda"):
 
 def move_traffic(workload):
     """dram bytes per k_move launch from the committed ncu summary, if any."""
-    path = os.path.join(REPO, "profiles", f"k_move_{workload}.md")
-    if not os.path.exists(path):
-        return None
-    for line in open(path):
-        if line.startswith("dram_bytes_per_launch_full_case:"):
-            return float(line.split(":")[1].split()[0])
-    return None
+    return kernel_traffic("k_move", workload)
 
 
 def kernel_traffic(kernel, workload):
-    """dram bytes per launch of a kernel from its committed ncu summary, if any."""
-    path = os.path.join(REPO, "profiles", f"{kernel}_{workload}.md")
+    """dram bytes per launch of a kernel (read + write) from the committed ncu
+    summary of the workload (profiles/dram_per_kernel_<workload>.md), if any."""
+    path = os.path.join(REPO, "profiles", f"dram_per_kernel_{workload}.md")
     if not os.path.exists(path):
         return None
     for line in open(path):
-        if line.startswith("dram_bytes_per_launch:"):
+        if line.startswith(f"dram_bytes_per_launch {kernel}:"):
             return float(line.split(":")[1].split()[0])
     return None
 
@@ -184,7 +179,7 @@ def kernel_rooflines(case, stream, peak, peak_kind, workload, steps=3):
       k_move           32 B per particle + 8 B per slot change
       k_sort_push      41 B per mover (5 floats read and written, the code read)
       k_deposit_cells  8 B per particle (x, y) + 32 B per (species, cell) corner sums
-      k_pcg            40 B per unknown per inner iteration (x, r, p, Ap, the
+      k_pcg(_grid)     40 B per unknown per inner iteration (x, r, p, Ap, the
                        stencil diagonal), field modes 0 and 1
     Returns (kernels, rooflines)."""
     info = case.info
@@ -203,8 +198,8 @@ def kernel_rooflines(case, stream, peak, peak_kind, workload, steps=3):
         "k_deposit_cells": 8.0 * parts + 32.0 * nsp * info.Csize,
     }
     inner, outer = case.pcg_iters()
-    if inner > 0:
-        bytes_per_launch["k_pcg"] = 40.0 * info.n_unknowns * inner
+    if inner > 0:  # the cluster solve (k_pcg) or the whole-GPU cooperative one (k_pcg_grid)
+        bytes_per_launch["k_pcg"] = bytes_per_launch["k_pcg_grid"] = 40.0 * info.n_unknowns * inner
     rooflines = []
     for n, l, ms in stats:
         if n not in bytes_per_launch or l == 0:
@@ -214,7 +209,7 @@ def kernel_rooflines(case, stream, peak, peak_kind, workload, steps=3):
         r = dict(kernel=n, bound="hbm", achieved=ach, peak=peak, unit="GB/s", frac=ach / peak, peak_source=peak_kind,
                  algorithmic_bytes_per_launch=bytes_per_launch[n], us_per_launch=t * 1e6,
                  traffic=kernel_traffic(n, workload))
-        if n == "k_pcg":
+        if n.startswith("k_pcg"):
             r.update(inner_iterations=inner, outer_passes=outer, us_per_iteration=t * 1e6 / max(inner, 1),
                      unknowns=info.n_unknowns)
         rooflines.append(r)

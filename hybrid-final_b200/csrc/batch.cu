@@ -93,10 +93,17 @@ hp_status batch_dev_build(hp_case *const *cases, int n, BatchDev &b) {
             b.list_off[m][k] = (int)lists.size();
             for (int i = 0; i < n; i++) {
                 if (cases[i]->h.field_mode == 2) continue; // separable inner solve, not PCG
+                if (cases[i]->pcg_cluster > 16) continue;  // whole-GPU solve, launched on its own
                 int cs = std::min(pcg_cluster_for_nodes(cases[i]->s.Gsize), 1 << m);
                 if (cs == (1 << k)) lists.push_back(i);
             }
             b.list_n[m][k] = (int)lists.size() - b.list_off[m][k];
+        }
+    b.grid_cases.clear();
+    for (int i = 0; i < n; i++)
+        if (cases[i]->h.field_mode != 2 && cases[i]->pcg_cluster > 16) {
+            b.grid_cases.push_back({(int)lists.size(), cases[i]->pcg_cluster});
+            lists.push_back(i);
         }
     {
         std::vector<int> fidx;
@@ -121,6 +128,7 @@ std::vector<PcgGroup> BatchDev::groups(int cluster_max, int block) const {
     std::vector<PcgGroup> g;
     for (int k = 0; k <= m; k++)
         if (list_n[m][k] > 0) g.push_back(PcgGroup{1 << k, block, d_lists + list_off[m][k], list_n[m][k]});
+    for (const auto &gc : grid_cases) g.push_back(PcgGroup{gc.second, block, d_lists + gc.first, 1});
     return g;
 }
 

@@ -512,6 +512,10 @@ hp_status build_device(hp_case *c) {
     h.pcg_max_iter = c->opts.pcg_max_iter > 0 ? c->opts.pcg_max_iter : 100000;
     h.pcg_tol2 = s.PCGtol2;
     h.pcg_rtol = c->opts.pcg_rtol > 0 ? c->opts.pcg_rtol : 1e-8;
+    // a PCG case too large for a 16-CTA cluster solves over the whole GPU
+    // (cooperative launch); its CTA totals need 2 x 2 doubles per CTA
+    const int grid_ctas = h.field_mode != 2 ? pcg_grid_ctas(G, c->lc.pcg_block) : 0;
+    if (grid_ctas > 0) TRY(dalloc(c, &h.pcg_part, 4 * (size_t)((G + 1023) / 1024)));
     TRY(dalloc(c, &c->d_list0, 1));
     TRY(dalloc(c, &c->d_case, 1));
     CK(cudaMemcpy(c->d_case, &h, sizeof(h), cudaMemcpyHostToDevice));
@@ -534,7 +538,7 @@ hp_status build_device(hp_case *c) {
             TRY(upload_particles(c, isp, s.p_count[isp].data(), s.p_x[isp].data(), s.p_y[isp].data(),
                                  s.p_vx[isp].data(), s.p_vy[isp].data(), s.p_vz[isp].data()));
     }
-    c->pcg_cluster = pcg_cluster_for_nodes(G);
+    c->pcg_cluster = grid_ctas > 0 ? grid_ctas : pcg_cluster_for_nodes(G);
     if (h.field_mode == 2) {
         hp_case *one[1] = {c};
         TRY(hpi::fast_plan_build(one, std::vector<int>{0}, c->fplan));
@@ -1032,7 +1036,10 @@ hp_status hp_case_set_tune(hp_case *c, const hp_tune *t) {
     c->lc.pcg_cluster_max = t->pcg_cluster_max;
     c->lc.move_unroll = t->move_unroll;
     c->lc.mcc_cells = t->mcc_cells_per_warp;
-    c->pcg_cluster = std::min(pcg_cluster_for_nodes(c->s.Gsize), t->pcg_cluster_max);
+    {
+        const int gp = c->h.pcg_part ? pcg_grid_ctas(c->s.Gsize, t->pcg_block) : 0;
+        c->pcg_cluster = gp > 0 ? gp : std::min(pcg_cluster_for_nodes(c->s.Gsize), t->pcg_cluster_max);
+    }
     if (c->graph) {
         cudaGraphExecDestroy(c->graph);
         c->graph = nullptr;

@@ -85,6 +85,7 @@ struct BatchDev {
     // cluster size, concatenated in d_lists
     int *d_lists = nullptr;
     int list_off[5][5] = {}, list_n[5][5] = {};
+    std::vector<std::pair<int, int>> grid_cases; // whole-GPU PCG cases: (offset in the lists, CTAs)
     std::vector<hp::PcgGroup> groups(int cluster_max, int block) const;
     FastPlanDev fast;
 };

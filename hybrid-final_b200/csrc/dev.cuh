@@ -97,6 +97,7 @@ struct DevCase {
     float *pf_x, *pf_r, *pf_p, *pf_ap; // [G] FP32 PCG vectors
     double *x64, *b64;              // [G] FP64 solution and right-hand side
     double *dots;                   // scratch for cluster reductions [64]
+    double *pcg_part;               // [2 x 2 x CTAs] CTA totals of the cooperative grid solve (null: cluster)
     double *den;                    // [nsp*G]
     double *source;                 // [G]
     double4 *cw[DMAXSP];            // [C] per-cell corner weight sums

@@ -1390,10 +1390,14 @@ __device__ __forceinline__ double spmv_d(const float *__restrict__ st, int G, in
     return out;
 }
 
+// CTAs of the whole-GPU solve, at most
+constexpr int PCG_GRID_MAX = 512;
+
 struct ClusterRed {
     double *warp_part; // [32] in shared memory
     double *slot;      // [4]  in shared memory, read by the whole cluster
     double *bcast;     // [4]
+    double *grid_part; // [2 * PCG_GRID_MAX] in shared memory (whole-GPU solve)
 };
 
 // Sum of v over the cluster.  Deterministic for a fixed launch shape: warp
@@ -1415,13 +1419,21 @@ __device__ double cluster_sum2(cg::cluster_group &cl, double v0, double v1, cons
         sh.slot[2 * parity + 1] = b;
     }
     cl.sync();
+    // the CTA totals are read in parallel (lane r reads rank r) and added in
+    // rank order by one thread, so the remote reads do not queue one behind
+    // another
+    const unsigned ncta = cl.num_blocks();
+    if (threadIdx.x < ncta) {
+        const double *rem = cl.map_shared_rank(sh.slot, threadIdx.x);
+        sh.warp_part[threadIdx.x] = rem[2 * parity];
+        sh.warp_part[16 + threadIdx.x] = rem[2 * parity + 1];
+    }
+    __syncwarp();
     if (threadIdx.x == 0) {
         double a = 0.0, b = 0.0;
-        const unsigned ncta = cl.num_blocks();
         for (unsigned r = 0; r < ncta; r++) {
-            const double *rem = cl.map_shared_rank(sh.slot, r);
-            a += rem[2 * parity];
-            b += rem[2 * parity + 1];
+            a += sh.warp_part[r];
+            b += sh.warp_part[16 + r];
         }
         sh.bcast[0] = a;
         sh.bcast[1] = b;
@@ -1433,19 +1445,69 @@ __device__ double cluster_sum2(cg::cluster_group &cl, double v0, double v1, cons
     return r;
 }
 
-// PCG_float (src/cuda_Field.cu:942-1072) as one launch per case cluster.
+// The same sum over all CTAs of a cooperative grid: the CTA totals go to
+// global memory (two buffers by parity, as the cluster slots), a grid
+// barrier, and every CTA adds them in rank order -- the same tree as
+// cluster_sum2 for the same number of CTAs.
+__device__ double grid_sum2(cg::grid_group &gr, double v0, double v1, const ClusterRed &sh, int parity,
+                            double *out1, double *part, int ncta, int rank) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    v0 = warp_sum_d(v0);
+    v1 = warp_sum_d(v1);
+    if (lane == 0) {
+        sh.warp_part[wid] = v0;
+        sh.warp_part[16 + wid] = v1;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < nw; k++) { a += sh.warp_part[k]; b += sh.warp_part[16 + k]; }
+        part[2 * ((size_t)parity * ncta + rank)] = a;
+        part[2 * ((size_t)parity * ncta + rank) + 1] = b;
+    }
+    gr.sync();
+    // the CTA totals are loaded in parallel into shared memory, then added in
+    // rank order by one thread
+    for (int r = threadIdx.x; r < ncta; r += blockDim.x) {
+        sh.grid_part[r] = __ldcg(&part[2 * ((size_t)parity * ncta + r)]);
+        sh.grid_part[PCG_GRID_MAX + r] = __ldcg(&part[2 * ((size_t)parity * ncta + r) + 1]);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int r = 0; r < ncta; r++) {
+            a += sh.grid_part[r];
+            b += sh.grid_part[PCG_GRID_MAX + r];
+        }
+        sh.bcast[0] = a;
+        sh.bcast[1] = b;
+    }
+    __syncthreads();
+    if (out1) *out1 = sh.bcast[1];
+    const double r = sh.bcast[0];
+    __syncthreads();
+    return r;
+}
+
+// PCG_float (src/cuda_Field.cu:942-1072) as one launch per case cluster, or
+// (GRID) as one cooperative launch over the whole GPU for a case too large for
+// a 16-CTA cluster: the same algorithm, node partition and reduction tree
+// for its number of CTAs, with grid barriers for cluster barriers.  Every
+// CTA takes the same branches (the sums are identical on all of them), so
+// every CTA reaches every barrier.
 // field_mode 0 keeps the reference's rule: FP32 Jacobi-PCG on the assembled
 // operator from the previous solution, until r'z <= PCGtol^2 (absolute).
 // field_mode 1: FP64 residual b - A x on the FP64 solution, an FP32 PCG
 // inner solve of the symmetrised system D^-1 A e = D^-1 r (D = 2 on each
 // Neumann edge the reference doubles), x += e, until ||r|| <= rtol ||b||.
 // Dot products are accumulated in FP64 in both modes.
+template <bool GRID>
 __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, const int *__restrict__ list,
                                              int nlist) {
     cg::cluster_group cl = cg::this_cluster();
-    const int CS = (int)cl.num_blocks();
-    const int rank = (int)cl.block_rank();
-    const int li = (int)blockIdx.x / CS;
+    const int CS = GRID ? (int)gridDim.x : (int)cl.num_blocks();
+    const int rank = GRID ? (int)blockIdx.x : (int)cl.block_rank();
+    const int li = GRID ? 0 : (int)blockIdx.x / CS;
     if (li >= nlist) return;
     const DevCase &d = cases[list[li]];
     const int G = d.G, ngy = d.ngy, ngx = d.ngx;
@@ -1455,7 +1517,18 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
     __shared__ double s_warp[32];
     __shared__ double s_slot[4];
     __shared__ double s_bcast[4];
-    const ClusterRed sh{s_warp, s_slot, s_bcast};
+    __shared__ double s_grid[GRID ? 2 * PCG_GRID_MAX : 1];
+    const ClusterRed sh{s_warp, s_slot, s_bcast, s_grid};
+    cg::grid_group gr = cg::this_grid();
+    // one barrier and one sum over the case's CTAs, in the launch's scope
+    auto bar = [&]() {
+        if (GRID) gr.sync();
+        else cl.sync();
+    };
+    auto sum2 = [&](double v0, double v1, int par, double *out1) {
+        return GRID ? grid_sum2(gr, v0, v1, sh, par, out1, d.pcg_part, CS, rank)
+                    : cluster_sum2(cl, v0, v1, sh, par, out1);
+    };
     int parity = 0;
     float *__restrict__ x = d.pf_x;
     float *__restrict__ r = d.pf_r;
@@ -1477,7 +1550,7 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
             p[n] = z;
             part += (double)(rr * z);
         }
-        double rz = cluster_sum2(cl, part, 0.0, sh, parity, nullptr);
+        double rz = sum2(part, 0.0, parity, nullptr);
         parity ^= 1;
         // a non-finite right-hand side or warm start: the reference's loop
         // test (r'z > tol^2) is false for NaN and leaves x as it was
@@ -1492,7 +1565,7 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
                 ap[n] = a;
                 part += (double)(p[n] * a);
             }
-            const double pap = cluster_sum2(cl, part, 0.0, sh, parity, nullptr);
+            const double pap = sum2(part, 0.0, parity, nullptr);
             parity ^= 1;
             const float alpha = (pap != 0.0) ? (float)rz / (float)pap : 0.0f;
             part = 0.0;
@@ -1504,7 +1577,7 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
                 r[n] = rr;
                 part += (double)(rr * ((1 / cc) * rr));
             }
-            const double rznew = cluster_sum2(cl, part, 0.0, sh, parity, nullptr);
+            const double rznew = sum2(part, 0.0, parity, nullptr);
             parity ^= 1;
             if (!(rznew == rznew) || isinf(rznew)) { bad = true; break; }
             const float beta = (rz != 0.0) ? (float)rznew / (float)rz : 0.0f;
@@ -1515,7 +1588,7 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
             }
             rz = rznew;
             iter++;
-            cl.sync();
+            bar();
         }
         iters = iter;
         for (int n = lo + threadIdx.x; n < hi; n += T) d.phi_p[n] = d.st[2 * G + n] != 0.0f ? x[n] : 0.0f;
@@ -1527,7 +1600,7 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
         const double *b64 = d.b64;
         double bb = 0.0;
         for (int n = lo + threadIdx.x; n < hi; n += T) bb += b64[n] * b64[n];
-        bb = cluster_sum2(cl, bb, 0.0, sh, parity, nullptr);
+        bb = sum2(bb, 0.0, parity, nullptr);
         parity ^= 1;
         const double target = d.pcg_rtol * d.pcg_rtol * bb;
         const double inner_rel2 = 1e-10; // inner solve: 1e-5 reduction of the preconditioned residual norm
@@ -1545,7 +1618,7 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
                 p[n] = z;
                 rz += (double)(rs * z);
             }
-            rr = cluster_sum2(cl, rr, rz, sh, parity, &rz);
+            rr = sum2(rr, rz, parity, &rz);
             parity ^= 1;
             if (!(rr == rr) || isinf(rr)) { bad = true; break; }
             if (rr <= target || bb == 0.0) break;
@@ -1560,7 +1633,7 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
                     ap[n] = a;
                     part += (double)(p[n] * a);
                 }
-                const double pap = cluster_sum2(cl, part, 0.0, sh, parity, nullptr);
+                const double pap = sum2(part, 0.0, parity, nullptr);
                 parity ^= 1;
                 const float alpha = (pap != 0.0) ? (float)(rz / pap) : 0.0f;
                 part = 0.0;
@@ -1572,7 +1645,7 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
                     r[n] = rs;
                     part += (double)(rs * ((1 / cc) * rs));
                 }
-                const double rznew = cluster_sum2(cl, part, 0.0, sh, parity, nullptr);
+                const double rznew = sum2(part, 0.0, parity, nullptr);
                 parity ^= 1;
                 if (!(rznew == rznew) || isinf(rznew)) { bad = true; break; }
                 const float beta = (rz != 0.0) ? (float)(rznew / rz) : 0.0f;
@@ -1583,13 +1656,13 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
                 }
                 rz = rznew;
                 iter++;
-                cl.sync();
+                bar();
             }
             iters += iter;
             if (bad) break;
             for (int n = lo + threadIdx.x; n < hi; n += T)
                 if (st[2 * G + n] != 0.0f) x64[n] += (double)x[n];
-            cl.sync();
+            bar();
         }
         if (outer >= 12 && rank == 0 && threadIdx.x == 0) atomicOr(d.status, ST_NOCONV);
         for (int n = lo + threadIdx.x; n < hi; n += T) d.phi_p[n] = st[2 * G + n] != 0.0f ? (float)x64[n] : 0.0f;
@@ -1600,7 +1673,7 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
         if (bad) atomicOr(d.status, ST_NONFINITE);
     }
     // no CTA may leave while another can still read its shared memory
-    cl.sync();
+    bar();
 }
 
 // Efield_cuda_Basic potential assembly (src/cuda_Field.cu:9-34):
@@ -2095,6 +2168,21 @@ cudaError_t launch_deposit(const DevCase *cases, const int *cell_items, const in
     return cudaGetLastError();
 }
 
+// CTAs of the cooperative grid solve for a case of G nodes: about 1024 nodes
+// (two per thread) per CTA, at most what the device keeps resident at once;
+// 0 where a cluster of at most 16 CTAs covers the case at 8 nodes per thread
+int pcg_grid_ctas(int G, int block) {
+    if ((long long)G <= 16LL * 512 * 8) return 0;
+    int dev = 0, sms = 0, per_sm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pcg<true>, block, 0) != cudaSuccess)
+        return 0;
+    const int want = (G + 1023) / 1024;
+    const int most = std::min(sms * per_sm, PCG_GRID_MAX);
+    return most > 16 ? std::min(want, most) : 0;
+}
+
 int pcg_cluster_for_nodes(int G) {
     // about 8 nodes per thread at 512 threads per CTA, up to a 16-CTA cluster
     int cs = 1;
@@ -2106,12 +2194,30 @@ cudaError_t launch_field(const DevCase *cases, const int *node_items, int ncases
                          const PcgGroup *groups, int ngroups, const FastPlan *fast, cudaStream_t st, bool circuit) {
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(k_pcg, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+        cudaFuncSetAttribute(k_pcg<false>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
         attr_set = true;
     }
     for (int g = 0; g < ngroups; g++) {
         const PcgGroup &pg = groups[g];
         if (pg.n <= 0) continue;
+        if (pg.cluster > 16) { // one cooperative launch per case over pg.cluster CTAs
+            for (int k = 0; k < pg.n; k++) {
+                cudaLaunchConfig_t cfg = {};
+                cfg.gridDim = dim3((unsigned)pg.cluster, 1, 1);
+                cfg.blockDim = dim3((unsigned)pg.block, 1, 1);
+                cfg.dynamicSmemBytes = 0;
+                cfg.stream = st;
+                cudaLaunchAttribute attr[1];
+                attr[0].id = cudaLaunchAttributeCooperative;
+                attr[0].val.cooperative = 1;
+                cfg.attrs = attr;
+                cfg.numAttrs = 1;
+                prof::mark(st, "k_pcg_grid");
+                cudaError_t e = cudaLaunchKernelEx(&cfg, k_pcg<true>, cases, pg.list + k, 1);
+                if (e != cudaSuccess) return e;
+            }
+            continue;
+        }
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3((unsigned)(pg.n * pg.cluster), 1, 1);
         cfg.blockDim = dim3((unsigned)pg.block, 1, 1);
@@ -2125,7 +2231,7 @@ cudaError_t launch_field(const DevCase *cases, const int *node_items, int ncases
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         prof::mark(st, "k_pcg");
-        cudaError_t e = cudaLaunchKernelEx(&cfg, k_pcg, cases, pg.list, pg.n);
+        cudaError_t e = cudaLaunchKernelEx(&cfg, k_pcg<false>, cases, pg.list, pg.n);
         if (e != cudaSuccess) return e;
     }
     if (fast && fast->n > 0) {

@@ -44,7 +44,7 @@ cudaError_t launch_deposit(const DevCase *cases, const int *cell_items, const in
 // cluster shape), and each case's cluster size depends only on its own grid,
 // so a case gets the same reduction order alone and inside any batch.
 struct PcgGroup {
-    int cluster;      // CTAs per case
+    int cluster;      // CTAs per case (above 16: one cooperative launch per case over the grid)
     int block;        // threads per CTA
     const int *list;  // device array of case indices
     int n;
@@ -78,6 +78,8 @@ cudaError_t launch_field(const DevCase *cases, const int *node_items, int ncases
                          bool circuit = false);
 // CTAs per case for a grid of G nodes
 int pcg_cluster_for_nodes(int G);
+// CTAs of the whole-GPU cooperative PCG for a case of G nodes (0: a cluster suffices)
+int pcg_grid_ctas(int G, int block);
 // CSR particles (5 arrays of start[C] floats back to back: x, y, vx, vy, vz)
 // into the cell-blocked slots of one species; sets cnt and clears nmov
 cudaError_t launch_scatter(const DevSpecies &sp, int C, const int *start, const float *src, cudaStream_t st);

@@ -83,13 +83,15 @@ def test_ar_513x257_200ppc_3_steps():
     check_state(case, o, "513x257, 3 steps")
 
 
-@pytest.mark.parametrize("field_mode", [1, 2])
+@pytest.mark.parametrize("field_mode", [0, 1, 2])
 def test_ar_513x257_field(field_mode):
-    """The field solve of the 513x257 case on its initial charge: the cluster
-    PCG with FP64 refinement (mode 1) and the separable solver (mode 2)."""
+    """The field solve of the 513x257 case on its initial charge: the
+    whole-GPU cooperative PCG (131k nodes, above one 16-CTA cluster) with the
+    reference's rule (mode 0) and with FP64 refinement (mode 1), and the
+    separable solver (mode 2)."""
     case, o = pair("ar_513x257_200ppc", field_mode=field_mode, move_mode=1)
-    if field_mode == 1:
-        assert case.info.pcg_cluster > 1
+    if field_mode in (0, 1):
+        assert case.info.pcg_cluster == (513 * 257 + 1023) // 1024  # one CTA per 1024 nodes
     case.set_tstep(1)
     case.Field()
     o.Field(1)
@@ -105,3 +107,29 @@ def test_aro2_257x129_100ppc_5_steps():
     case.step(5)
     o.run(0, 5, accumulate=True)
     check_state(case, o, "Ar/O2 257x129, 5 steps")
+
+
+@pytest.mark.parametrize("field_mode", [0, 1])
+def test_whole_gpu_pcg_through_the_step_graph(field_mode):
+    """A 321x225 case (72k nodes) solves with the cooperative whole-GPU PCG
+    (71 CTAs) inside the captured step graph, three steps, and in a batch
+    next to a cluster-solved case: bit for bit with the oracle."""
+    from hpic.decks import ccp_deck
+    deck = ccp_deck(321, 225, 0.1, 0.07, ppc=4, voltage=150.0, max_np_factor=16)
+    kw = dict(seed=77, gas_temp_mode=1, field_mode=field_mode, move_mode=1)
+    S = hpic.Setup(deck, **kw)
+    case = hpic.Case(setup=S, **kw)
+    assert case.info.pcg_cluster == (321 * 225 + 1023) // 1024
+    o = oracle.Oracle(S.table, S.info, case.opts, 32, pcg_cluster=case.info.pcg_cluster,
+                      pcg_block=case.info.pcg_block)
+    for s in range(S.info.nsp):
+        counts, arrs = S.particles(s, layout=0)
+        o.set_particles(s, counts, *arrs)
+    o.DepositBasic()
+    small = hpic.Case(deck=ccp_deck(65, 33, 0.02, 0.01, ppc=8), seed=5, field_mode=field_mode)
+    batch = hpic.Batch([small, case])
+    batch.step(3)
+    batch.close()
+    o.run(0, 3)
+    check_state(case, o, "321x225 grid PCG, 3 steps")
+    assert case.pcg_iters()[0] == o.counters()[2][0]
