@@ -80,6 +80,32 @@ class KernelStat(C.Structure):
     _fields_ = [("name", C.c_char * 32), ("launches", C.c_int), ("ms", C.c_double)]
 
 
+class Gcp(C.Structure):  # the reference's GCP record (inc/def.h)
+    _fields_ = [("CellID", C.c_int), ("x", C.c_float), ("y", C.c_float), ("vx", C.c_float), ("vy", C.c_float),
+                ("vz", C.c_float)]
+
+
+class Gpg(C.Structure):  # the reference's GPG record
+    _fields_ = [("PtNumInCell", C.c_int), ("PtNumMoveInterCell", C.c_int), ("MaxPtNumInCell", C.c_int),
+                ("PtNumMCCInCell", C.c_int), ("PtNullMCCInCell", C.c_int), ("den", C.c_float),
+                ("smt_den", C.c_float), ("sum_den", C.c_float), ("ave_den", C.c_float), ("sigma", C.c_float)]
+
+
+class Gga(C.Structure):  # the reference's GGA record
+    _fields_ = [("Boundary", C.c_int), ("CondID", C.c_int), ("Face", C.c_int), ("DensRegion", C.c_int)] + \
+        [(k, C.c_float) for k in ("Area", "Temp", "BackDen1", "BackVel1", "BackDen2", "BackVel2", "Lap_Pot",
+                                   "Pois_Pot", "Ex", "Ey")]
+
+
+GCP_DTYPE = np.dtype([("CellID", "i4"), ("x", "f4"), ("y", "f4"), ("vx", "f4"), ("vy", "f4"), ("vz", "f4")])
+GPG_DTYPE = np.dtype([("PtNumInCell", "i4"), ("PtNumMoveInterCell", "i4"), ("MaxPtNumInCell", "i4"),
+                      ("PtNumMCCInCell", "i4"), ("PtNullMCCInCell", "i4"), ("den", "f4"), ("smt_den", "f4"),
+                      ("sum_den", "f4"), ("ave_den", "f4"), ("sigma", "f4")])
+GGA_DTYPE = np.dtype([("Boundary", "i4"), ("CondID", "i4"), ("Face", "i4"), ("DensRegion", "i4")] +
+                     [(k, "f4") for k in ("Area", "Temp", "BackDen1", "BackVel1", "BackDen2", "BackVel2", "Lap_Pot",
+                                          "Pois_Pot", "Ex", "Ey")])
+
+
 class ServerOpts(C.Structure):
     _fields_ = [("mem_budget_bytes", C.c_size_t), ("max_slots", C.c_int), ("steps_per_launch", C.c_int),
                 ("case_opts", CaseOpts)]
@@ -123,6 +149,9 @@ _SIGS = {
     "hp_case_get_tune": (C.c_int, [_P, _P]),
     "hp_batch_step_kernels": (C.c_int, [_P, C.POINTER(C.c_int)]),
     "hp_profile_step": (C.c_int, [_P, C.c_int, _P, C.POINTER(KernelStat), C.c_int, C.POINTER(C.c_int)]),
+    "hp_export_gcp": (C.c_int, [_P, C.c_int, C.c_int, _P, _P]),
+    "hp_import_gcp": (C.c_int, [_P, C.c_int, C.c_int, _P, _P]),
+    "hp_export_gga": (C.c_int, [_P, _P]),
     "hp_Deposit_noalloc": (C.c_int, [_P, _P, _P]),
     "hp_get_particles": (C.c_int, [_P, C.c_int, _I, _F, _F, _F, _F, _F, C.c_size_t, C.POINTER(C.c_size_t)]),
     "hp_set_particles": (C.c_int, [_P, C.c_int, _I, _F, _F, _F, _F, _F]),
@@ -432,6 +461,25 @@ class Case:
         n = C.c_size_t(0)
         _check(lib().hp_get_movers(self.h, isp, None, None, None, None, None, None, None, 0, C.byref(n)))
         return n.value
+
+    def export_gcp(self, isp, mpnc):
+        """Species isp in the reference's layout: (GCP records [mpnc*Gsize],
+        GPG records [Gsize]) as numpy structured arrays."""
+        G = self.info.Gsize
+        gcp = np.zeros(mpnc * G, GCP_DTYPE)
+        gpg = np.zeros(G, GPG_DTYPE)
+        _check(lib().hp_export_gcp(self.h, isp, mpnc, gcp.ctypes.data_as(_P), gpg.ctypes.data_as(_P)))
+        return gcp, gpg
+
+    def import_gcp(self, isp, mpnc, gcp, gpg):
+        gcp = np.ascontiguousarray(gcp, GCP_DTYPE)
+        gpg = np.ascontiguousarray(gpg, GPG_DTYPE)
+        _check(lib().hp_import_gcp(self.h, isp, mpnc, gcp.ctypes.data_as(_P), gpg.ctypes.data_as(_P)))
+
+    def export_gga(self):
+        gga = np.zeros(self.info.Gsize, GGA_DTYPE)
+        _check(lib().hp_export_gga(self.h, gga.ctypes.data_as(_P)))
+        return gga
 
     def profile(self, n=1, stream=None):
         """Per-kernel device times of n op-by-op steps (hp_profile_step):

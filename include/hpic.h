@@ -316,6 +316,37 @@ hp_status hp_case_pushes(hp_case *c, int64_t *pushes);
  * (32 B per particle + 8 B per slot change).  No reference counterpart. */
 hp_status hp_case_slot_changes(hp_case *c, int64_t *changes);
 
+/* The reference's own device structs (inc/def.h), field for field: a host
+ * that keeps the reference's GCP / GPG / GGA arrays exchanges a case's state
+ * through them.  Particle k of the cell whose lower-left node is
+ * ID = i*ngy + j sits at gcp[ID + k*Gsize] (k < mpnc, the reference's MPNC;
+ * src/cuda_Move.cu:195) with gpg[ID].PtNumInCell of them; x, y are offsets in
+ * the cell.  hp_export_gcp writes a species' particles (every record of the
+ * Gsize*mpnc block: unused slots zero, CellID the node ID), and with gpg
+ * non-NULL its Gsize GPG records: PtNumInCell, MaxPtNumInCell = mpnc, den (the
+ * charge grid's boundary-scaled count), ave_den (the average since
+ * hp_reset_averages) and sigma (the dielectric surface charge in particle
+ * weights); the collision counters are 0.  HP_ERR_CAPACITY when a cell holds
+ * more than mpnc.  hp_import_gcp replaces a species' particles by those of a
+ * GCP block and its GPG counts (as hp_set_particles).  hp_export_gga fills
+ * Gsize GGA records from the case's tables and fields (Lap_Pot is
+ * TotPotential - Pois_Pot). */
+typedef struct hp_gcp {
+    int CellID;
+    float x, y, vx, vy, vz;
+} hp_gcp;
+typedef struct hp_gpg {
+    int PtNumInCell, PtNumMoveInterCell, MaxPtNumInCell, PtNumMCCInCell, PtNullMCCInCell;
+    float den, smt_den, sum_den, ave_den, sigma;
+} hp_gpg;
+typedef struct hp_gga {
+    int Boundary, CondID, Face, DensRegion;
+    float Area, Temp, BackDen1, BackVel1, BackDen2, BackVel2, Lap_Pot, Pois_Pot, Ex, Ey;
+} hp_gga;
+hp_status hp_export_gcp(hp_case *c, int isp, int mpnc, hp_gcp *gcp, hp_gpg *gpg);
+hp_status hp_import_gcp(hp_case *c, int isp, int mpnc, const hp_gcp *gcp, const hp_gpg *gpg);
+hp_status hp_export_gga(hp_case *c, hp_gga *gga);
+
 /* Per-kernel device times of nsteps steps run operator by operator on
  * `stream` (not the captured graph of hp_step): every kernel launch is
  * bracketed by CUDA events, and the entries sum each kernel's launches and

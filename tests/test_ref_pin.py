@@ -271,6 +271,43 @@ def test_pcg_matches_reference():
     assert rel_err(x1, xo, xs) <= 1e-2
 
 
+@pytest.mark.parametrize("ngx,ngy,xl,yl", [(129, 65, 0.04, 0.02), (513, 257, 0.16, 0.08)])
+def test_pcg_solve_time_against_the_reference_kernel(ngx, ngy, xl, yl):
+    """The first Poisson solve of a CCP deck (warm start 0, the reference's
+    absolute r'z rule, field mode 0): this library's PCG (one cluster, or the
+    whole-GPU cooperative solve above 65,536 nodes) against the reference's
+    PCG_float launched as PCG_SOLVER launches it, on the same right-hand
+    side, both timed with CUDA events.  This library's solve must take less
+    time; both per-iteration times are printed."""
+    deck = ccp_deck(ngx, ngy, xl, yl, ppc=4, max_np_factor=8)
+    S, o = oracle_for(deck, 5)
+    o.DepositBasic()
+    b_node = o.grid("B")
+    idx = S.table("a_idx")
+    unk = np.nonzero(idx)[0]
+    n = int(idx.max())
+    b = np.zeros(n, np.float32)
+    b[idx[unk] - 1] = b_node[unk]
+    ai, aj, val, m = S.table("ai"), S.table("aj"), S.table("a_val"), S.table("matm")
+    tol2 = float(o.c.pcg_tol2)
+    refk.pcg(ai, aj, val, m, b, np.zeros(n, np.float32), tol2)  # warm-up (module load, first launch)
+    _, it_ref, ms_ref = refk.pcg(ai, aj, val, m, b, np.zeros(n, np.float32), tol2)
+    case = hpic.Case(setup=S, seed=5, field_mode=0, move_mode=0)
+    case.set_tstep(1)
+    case.Field()  # warm-up of the launch path (the solve starts from 0 again below)
+    case.set_grid("PCG_X", np.zeros(case.info.Gsize, np.float32))
+    case.set_tstep(0)
+    # one profiled step: its Field phase solves the same system from 0 (the
+    # Poisson part holds the conductors at 0 V, whatever the step's voltage)
+    stats = {name: ms for name, _, ms in case.profile(1)}
+    it_ours = case.pcg_iters()[0]
+    ms_ours = stats.get("k_pcg", stats.get("k_pcg_grid"))
+    print(f"{ngx}x{ngy}: PCG_float (reference launch) {it_ref} it {ms_ref:.3f} ms = {1e3 * ms_ref / max(it_ref, 1):.2f} "
+          f"us/it; this library ({'grid' if 'k_pcg_grid' in stats else 'cluster'} {case.info.pcg_cluster} CTAs) "
+          f"{it_ours} it {ms_ours:.3f} ms = {1e3 * ms_ours / max(it_ours, 1):.2f} us/it")
+    assert ms_ours < ms_ref
+
+
 # ------------------------------------------------------------ cross sections, kinematics
 @pytest.mark.parametrize("gas_name,gas", [("Ar", 0), ("O2", 1), ("ArO2", 2)])
 def test_cross_sections_match_reference(gas_name, gas):
