@@ -347,6 +347,9 @@ hp_status build_device(hp_case *c) {
     TRY(dalloc(c, &h.pf_x, G));
     TRY(dalloc(c, &h.pf_r, G));
     TRY(dalloc(c, &h.pf_p, G));
+    TRY(dalloc(c, &h.pf_p2, G));
+    // one halo of 2 x ngy directions per CTA, for up to 16 cluster CTAs or one per 1024 nodes
+    TRY(dalloc(c, &h.pcg_halo, (size_t)2 * s.ngy * std::max(16, (G + 1023) / 1024)));
     TRY(dalloc(c, &h.pf_ap, G));
     TRY(dalloc(c, &h.x64, G));
     TRY(dalloc(c, &h.b64, G));

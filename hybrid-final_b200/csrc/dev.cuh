@@ -95,6 +95,8 @@ struct DevCase {
     const float *st_sym;            // [5*G] row-scaled symmetric stencil (refinement mode)
     const float *row_scale;         // [G] 1/d_i used to symmetrise (refinement mode)
     float *pf_x, *pf_r, *pf_p, *pf_ap; // [G] FP32 PCG vectors
+    float *pf_p2;                   // [G] the second search-direction buffer (directions alternate)
+    float *pcg_halo;                // [2 x ngy x CTAs] each CTA's copy of the directions of its neighbours' nodes
     double *x64, *b64;              // [G] FP64 solution and right-hand side
     double *dots;                   // scratch for cluster reductions [64]
     double *pcg_part;               // [2 x 2 x CTAs] CTA totals of the cooperative grid solve (null: cluster)

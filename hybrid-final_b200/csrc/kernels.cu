@@ -1532,13 +1532,68 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
     int parity = 0;
     float *__restrict__ x = d.pf_x;
     float *__restrict__ r = d.pf_r;
-    float *__restrict__ p = d.pf_p;
     float *__restrict__ ap = d.pf_ap;
+    // The search direction p alternates between two buffers, and each CTA
+    // keeps its own copy of the p values of the other CTAs' unknowns its
+    // product reads (the nodes [lo - ngy, lo) and [hi, hi + ngy): its halo),
+    // computed from the same operands as their owners compute them.  An
+    // iteration then needs no barrier after the direction update: the two
+    // sums' barriers are the only ones.
+    float *const pbuf0 = d.pf_p, *const pbuf1 = d.pf_p2;
+    auto pbuf = [&](int k) { return k ? pbuf1 : pbuf0; };
+    float *__restrict__ halo = d.pcg_halo + (size_t)rank * 2 * ngy;
+    auto hnode = [&](int q) { return q < ngy ? lo - ngy + q : hi + (q - ngy); };
+    auto owned = [&](int m) { return m >= lo && m < hi; };
+    // p at node m of the current direction: own nodes from the buffer, the others from the halo
+    auto pv = [&](const float *pc, int m) { return owned(m) ? pc[m] : halo[m < lo ? m - (lo - ngy) : ngy + (m - hi)]; };
+    // the 5-point product at own node n on the current direction (CSR order W, S, C, N, E)
+    auto spmv_h = [&](const float *__restrict__ stc, const float *pc, int n) {
+        float out = 0.0f;
+        const float cw = stc[n], cs = stc[G + n], cc = stc[2 * G + n], cn = stc[3 * G + n], ce = stc[4 * G + n];
+        if (cw != 0.0f) out += cw * pv(pc, n - ngy);
+        if (cs != 0.0f) out += cs * pv(pc, n - 1);
+        out += cc * pc[n];
+        if (cn != 0.0f) out += cn * pv(pc, n + 1);
+        if (ce != 0.0f) out += ce * pv(pc, n + ngy);
+        return out;
+    };
+    // the halo of p_0 = D^-1 r_0 (the owners' residuals are visible after the sum's barrier)
+    auto halo_first = [&](const float *__restrict__ stc) {
+        for (int q = threadIdx.x; q < 2 * ngy; q += T) {
+            const int h = hnode(q);
+            float v = 0.0f;
+            if (h >= 0 && h < G) {
+                const float cc = stc[2 * G + h];
+                if (cc != 0.0f) v = (1 / cc) * r[h];
+            }
+            halo[q] = v;
+        }
+        __syncthreads();
+    };
+    // own p_{k+1} = beta p_k + D^-1 r_{k+1} into the other buffer, and the halo likewise
+    auto next_dir = [&](const float *__restrict__ stc, const float *pc, float *pn, float beta) {
+        for (int n = lo + threadIdx.x; n < hi; n += T) {
+            const float cc = stc[2 * G + n];
+            if (cc == 0.0f) continue;
+            pn[n] = beta * pc[n] + (1 / cc) * r[n];
+        }
+        for (int q = threadIdx.x; q < 2 * ngy; q += T) {
+            const int h = hnode(q);
+            float v = 0.0f;
+            if (h >= 0 && h < G) {
+                const float cc = stc[2 * G + h];
+                if (cc != 0.0f) v = beta * pc[h] + (1 / cc) * r[h];
+            }
+            halo[q] = v;
+        }
+        __syncthreads();
+    };
     const int maxit = d.pcg_max_iter;
     int iters = 0, outer = 0;
     bool bad = false;
     if (d.field_mode == 0) {
-        const float *st = d.st;
+        const float *__restrict__ st = d.st;
+        float *p0 = pbuf(0);
         double part = 0.0;
         for (int n = lo + threadIdx.x; n < hi; n += T) {
             const float cc = st[2 * G + n];
@@ -1547,23 +1602,25 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
             const float rr = -1.0f * ax + (float)d.b64[n];
             r[n] = rr;
             const float z = (1 / cc) * rr;
-            p[n] = z;
+            p0[n] = z;
             part += (double)(rr * z);
         }
         double rz = sum2(part, 0.0, parity, nullptr);
         parity ^= 1;
+        halo_first(st);
         // a non-finite right-hand side or warm start: the reference's loop
         // test (r'z > tol^2) is false for NaN and leaves x as it was
         if (!(rz == rz) || isinf(rz)) bad = true;
-        int iter = 1;
+        int iter = 1, pb = 0;
         while (rz > (double)d.pcg_tol2 && iter <= maxit) {
+            const float *pc = pbuf(pb);
             part = 0.0;
             for (int n = lo + threadIdx.x; n < hi; n += T) {
                 const float cc = st[2 * G + n];
                 if (cc == 0.0f) continue;
-                const float a = spmv_f(st, G, ngy, n, 0, 0, ngx, p);
+                const float a = spmv_h(st, pc, n);
                 ap[n] = a;
-                part += (double)(p[n] * a);
+                part += (double)(pc[n] * a);
             }
             const double pap = sum2(part, 0.0, parity, nullptr);
             parity ^= 1;
@@ -1572,7 +1629,7 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
             for (int n = lo + threadIdx.x; n < hi; n += T) {
                 const float cc = st[2 * G + n];
                 if (cc == 0.0f) continue;
-                x[n] = alpha * p[n] + x[n];
+                x[n] = alpha * pc[n] + x[n];
                 const float rr = -alpha * ap[n] + r[n];
                 r[n] = rr;
                 part += (double)(rr * ((1 / cc) * rr));
@@ -1581,23 +1638,19 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
             parity ^= 1;
             if (!(rznew == rznew) || isinf(rznew)) { bad = true; break; }
             const float beta = (rz != 0.0) ? (float)rznew / (float)rz : 0.0f;
-            for (int n = lo + threadIdx.x; n < hi; n += T) {
-                const float cc = st[2 * G + n];
-                if (cc == 0.0f) continue;
-                p[n] = beta * p[n] + (1 / cc) * r[n];
-            }
+            next_dir(st, pc, pbuf(pb ^ 1), beta);
+            pb ^= 1;
             rz = rznew;
             iter++;
-            bar();
         }
         iters = iter;
         for (int n = lo + threadIdx.x; n < hi; n += T) d.phi_p[n] = d.st[2 * G + n] != 0.0f ? x[n] : 0.0f;
         if (iter > maxit && rank == 0 && threadIdx.x == 0) atomicOr(d.status, ST_NOCONV);
     } else {
-        const float *st = d.st;
-        const float *ss = d.st_sym;
-        double *x64 = d.x64;
-        const double *b64 = d.b64;
+        const float *__restrict__ st = d.st;
+        const float *__restrict__ ss = d.st_sym;
+        double *__restrict__ x64 = d.x64;
+        const double *__restrict__ b64 = d.b64;
         double bb = 0.0;
         for (int n = lo + threadIdx.x; n < hi; n += T) bb += b64[n] * b64[n];
         bb = sum2(bb, 0.0, parity, nullptr);
@@ -1605,6 +1658,7 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
         const double target = d.pcg_rtol * d.pcg_rtol * bb;
         const double inner_rel2 = 1e-10; // inner solve: 1e-5 reduction of the preconditioned residual norm
         for (outer = 0; outer < 12; outer++) {
+            float *p0 = pbuf(0);
             double rr = 0.0, rz = 0.0;
             for (int n = lo + threadIdx.x; n < hi; n += T) {
                 const float cc = st[2 * G + n];
@@ -1615,23 +1669,25 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
                 r[n] = rs;
                 x[n] = 0.0f;
                 const float z = (1 / ss[2 * G + n]) * rs;
-                p[n] = z;
+                p0[n] = z;
                 rz += (double)(rs * z);
             }
             rr = sum2(rr, rz, parity, &rz);
             parity ^= 1;
             if (!(rr == rr) || isinf(rr)) { bad = true; break; }
             if (rr <= target || bb == 0.0) break;
+            halo_first(ss);
             const double rz0 = rz;
-            int iter = 0;
+            int iter = 0, pb = 0;
             while (rz > inner_rel2 * rz0 && iter < maxit) {
+                const float *pc = pbuf(pb);
                 double part = 0.0;
                 for (int n = lo + threadIdx.x; n < hi; n += T) {
                     const float cc = ss[2 * G + n];
                     if (cc == 0.0f) continue;
-                    const float a = spmv_f(ss, G, ngy, n, 0, 0, ngx, p);
+                    const float a = spmv_h(ss, pc, n);
                     ap[n] = a;
-                    part += (double)(p[n] * a);
+                    part += (double)(pc[n] * a);
                 }
                 const double pap = sum2(part, 0.0, parity, nullptr);
                 parity ^= 1;
@@ -1640,7 +1696,7 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
                 for (int n = lo + threadIdx.x; n < hi; n += T) {
                     const float cc = ss[2 * G + n];
                     if (cc == 0.0f) continue;
-                    x[n] = alpha * p[n] + x[n];
+                    x[n] = alpha * pc[n] + x[n];
                     const float rs = -alpha * ap[n] + r[n];
                     r[n] = rs;
                     part += (double)(rs * ((1 / cc) * rs));
@@ -1649,14 +1705,10 @@ __global__ void __launch_bounds__(512) k_pcg(const DevCase *__restrict__ cases, 
                 parity ^= 1;
                 if (!(rznew == rznew) || isinf(rznew)) { bad = true; break; }
                 const float beta = (rz != 0.0) ? (float)(rznew / rz) : 0.0f;
-                for (int n = lo + threadIdx.x; n < hi; n += T) {
-                    const float cc = ss[2 * G + n];
-                    if (cc == 0.0f) continue;
-                    p[n] = beta * p[n] + (1 / cc) * r[n];
-                }
+                next_dir(ss, pc, pbuf(pb ^ 1), beta);
+                pb ^= 1;
                 rz = rznew;
                 iter++;
-                bar();
             }
             iters += iter;
             if (bad) break;
