@@ -602,10 +602,12 @@ def run_served(args):
     status_nonzero = sum(1 for r, _, _ in results if r.error == 0 and r.status)
     status_bits = {f"0x{b:x}": int(sum(1 for r, _, _ in results if r.error == 0 and r.status & b))
                    for b in (1, 2, 4, 8, 16, 32)}
-    # the same stream, one case at a time on the plain path (set-up included)
+    # the same stream, one case at a time on the plain path (set-up included);
+    # --plain-requests bounds it to the stream's first requests
+    n_plain = len(reqs) if args.plain_requests <= 0 else min(args.plain_requests, len(reqs))
     t_start = time.perf_counter()
     plain_lat, plain_pushes = [], 0
-    for t_arr, deck, nsteps, seed, _ in reqs:
+    for t_arr, deck, nsteps, seed, _ in reqs[:n_plain]:
         now = time.perf_counter() - t_start
         if now < t_arr:
             time.sleep(t_arr - now)
@@ -630,7 +632,7 @@ def run_served(args):
                 device_status_nonzero=status_nonzero, device_status_bits=status_bits, wall_s=t_end,
                 plain=dict(value=plain_pushes / plain_end, latency_s=dict(p50=pct(plain_lat, 50),
                                                                           p99=pct(plain_lat, 99)),
-                           wall_s=plain_end, served_over_plain=value / (plain_pushes / plain_end)))
+                           requests=n_plain, wall_s=plain_end, served_over_plain=value / (plain_pushes / plain_end)))
 
 
 def main():
@@ -651,6 +653,8 @@ def main():
     ap.add_argument("--requests", type=int, default=64)
     ap.add_argument("--rate", type=float, default=4.0)
     ap.add_argument("--steps-scale", type=float, default=0.1, help="served: steps per RF period / 400")
+    ap.add_argument("--plain-requests", type=int, default=0,
+                    help="served: the plain arm runs the stream's first N requests (0: all)")
     ap.add_argument("--slots", type=int, default=64)
     ap.add_argument("--steps-per-launch", type=int, default=40)
     ap.add_argument("--budget-gb", type=float, default=150.0)
