@@ -259,7 +259,9 @@ template <int R>
 __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
                                                    const int *__restrict__ item_start, int ncases, int items) {
     extern __shared__ float move_ring_s[];
+    __shared__ int dc_s[16][12]; // at most 16 warps per block (512 threads)
     float *ring = move_ring_s + (threadIdx.x >> 5) * (R * 5 * 32);
+    int *dc = dc_s[threadIdx.x >> 5];
     const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
     const int lane = threadIdx.x & 31;
     if (warp >= items) return;
@@ -317,8 +319,9 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
     const float As = sp.Ascale, dtdx = d.dt_dx, dtdy = d.dt_dy;
     const unsigned lt = lanemask_lt();
     int m = 0, shifted = 0;
-    // per-lane mover counts per destination code, three 21-bit fields per word
-    unsigned long long pk0 = 0, pk1 = 0, pk2 = 0;
+    // movers per destination code, counted in shared memory
+    if (lane < 9) dc[lane] = 0;
+    __syncwarp();
     // R - 1 chunks in flight while one is pushed (stores only go to slots at
     // or below the current chunk, or to the top region at or above
     // cap - n >= n, so no slot still to be copied is touched)
@@ -344,15 +347,13 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
         int code = 4, fi = i, fj = j;
         bool near = false;
         if (out && open3) { // the walk's first crossing with ghost code 0: a wrap, no flip
-            const float wy = ly >= 1 ? ly - 1.0f : ly < 0 ? ly + 1.0f : ly;
-            const float wx = lx >= 1 ? lx - 1.0f : lx < 0 ? lx + 1.0f : lx;
+            // (lx - (float)di is lx - 1, lx + 1 or lx, exactly the walk's wrap)
+            const int dj = (int)(ly >= 1) - (int)(ly < 0), di = (int)(lx >= 1) - (int)(lx < 0);
+            const float wy = ly - (float)dj, wx = lx - (float)di;
             if (!(wy >= 1 || wy < 0 || wx >= 1 || wx < 0)) {
-                const int dj = ly >= 1 ? 1 : ly < 0 ? -1 : 0, di = lx >= 1 ? 1 : lx < 0 ? -1 : 0;
                 lx = wx;
                 ly = wy;
-                fi = i + di;
-                fj = j + dj;
-                code = (di + 1) * 3 + (dj + 1);
+                code = 3 * di + dj + 4;
                 near = true;
             }
         }
@@ -373,13 +374,7 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
                 code = (ddi >= -1 && ddi <= 1 && ddj >= -1 && ddj <= 1) ? (ddi + 1) * 3 + (ddj + 1) : CODE_FAR;
             }
         }
-        if (out && code < 9) {
-            const int q3 = code / 3;
-            const unsigned long long one = 1ull << (21 * (code - 3 * q3));
-            if (q3 == 0) pk0 += one;
-            else if (q3 == 1) pk1 += one;
-            else pk2 += one;
-        }
+        if (out && code < 9) atomicAdd(&dc[code], 1);
         const unsigned bout = __ballot_sync(FULL, out);
         const int before = m + __popc(bout & lt);
         const bool moved = act && (out || before != 0); // its slot changes
@@ -410,14 +405,8 @@ __global__ void __launch_bounds__(512) k_move(const DevCase *__restrict__ cases,
         sp.nmov[c] = m;
         atomicAdd(&d.pushes[32 + (warp & 31)], (unsigned long long)shifted);
     }
-    int mine = 0;
-#pragma unroll
-    for (int D = 0; D < 9; D++) {
-        const unsigned long long wv = D < 3 ? pk0 : D < 6 ? pk1 : pk2;
-        const unsigned t = __reduce_add_sync(FULL, (unsigned)((wv >> (21 * (D % 3))) & 0x1FFFFFull));
-        if (lane == D) mine = (int)t;
-    }
-    if (lane < 9) sp.dcount[(size_t)c * 9 + lane] = mine;
+    __syncwarp();
+    if (lane < 9) sp.dcount[(size_t)c * 9 + lane] = dc[lane];
 }
 
 // The same push with U chunks of 32 particles loaded per iteration before
@@ -575,47 +564,65 @@ __global__ void __launch_bounds__(512) k_move_u(const DevCase *__restrict__ case
 //   k_sort_count (lane per destination cell) new count, then the far movers.
 constexpr int SORT_MAXW = 16; // warps per block, at most
 
-// Memory-level parallelism: every read a source warp needs (its first
-// SORT_PRE chunks of 32 movers, the nine destinations' counts and the 81
-// pair counts) is issued before the first result is used, so a warp waits
-// for one round trip instead of one per dependent step.
+// Memory-level parallelism: a source warp's movers arrive through a ring of
+// SORT_PRE chunk slots in shared memory, filled by asynchronous 16-byte copies
+// of the cell's top slots (no registers held while they are in flight); the
+// first chunk is requested before the mover count is known (the top 32 slots
+// exist in every cell), the next ones with the destinations' counts, so a
+// warp waits for about one round trip after its count.
 #ifndef SORT_PRE
 #define SORT_PRE 4
 #endif
+constexpr int SORT_SLOT = 5 * 32 + 8; // floats per ring slot: x, y, vx, vy, vz, then 32 code bytes
+#ifndef SORT_MINB
+#define SORT_MINB 2 // resident blocks per SM the register budget is set for
+#endif
 
-struct MoverRegs {
-    float x, y, vx, vy, vz;
-    int code;
-};
-
-__device__ __forceinline__ MoverRegs load_mover(const DevSpecies &sp, size_t base, int cap, int r, int m) {
-    MoverRegs v;
-    v.code = -1;
-    v.x = v.y = v.vx = v.vy = v.vz = 0.f;
-    if (r < m) {
-        const size_t q = base + (size_t)(cap - 1 - r);
-        v.code = (int)sp.code[q];
-        v.x = sp.x[q];
-        v.y = sp.y[q];
-        v.vx = sp.vx[q];
-        v.vy = sp.vy[q];
-        v.vz = sp.vz[q];
-    }
-    return v;
-}
-
-// the movers of one source cell (m > 0) of species s
-__device__ __forceinline__ void sort_push_cell(const DevCase &d, int s, int c, int m, int *s_off, int *s_lim,
-                                               int lane) {
+// One warp per (species, source cell): its movers (the r-th at slot cap-1-r)
+// go to their destinations' free slots in (source, rank) order.
+__global__ void __launch_bounds__(SORT_MAXW * 32, SORT_MINB) k_sort_push(const DevCase *__restrict__ cases,
+                                                           const int *__restrict__ item_start, int ncases, int items) {
+    extern __shared__ float sort_ring_s[];
+    __shared__ int s_off[SORT_MAXW][9], s_lim[SORT_MAXW][9];
+    const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+    if (warp >= items) return;
+    float *ring = sort_ring_s + wl * (SORT_PRE * SORT_SLOT);
+    const int ci = find_case(item_start, ncases, warp);
+    const DevCase &d = cases[ci];
+    const int w = warp - item_start[ci];
+    const int s = w / d.C, c = w - s * d.C;
     const DevSpecies &sp = d.sp[s];
     const int cap = sp.cap, ncy = d.ncy;
-    const int i = c / ncy, j = c - i * ncy;
     const size_t base = (size_t)c * cap;
-    // issue every read first: the movers ...
-    MoverRegs mv[SORT_PRE];
+    // chunk h (movers 32h .. 32h+31) is the 32 slots cap-32-32h .. cap-1-32h,
+    // all inside the cell as m <= cap/2 and cap is a multiple of 32; mover
+    // 32h + l is element 31 - l of each array in ring slot h % SORT_PRE.
+    // Lanes 0-7 copy x, 8-15 y, 16-23 vx, 24-31 vy, then lanes 0-7 vz and
+    // lanes 8-9 the codes; one commit group per chunk (possibly empty).  Slots
+    // of the chunk below the movers belong to the cell's free region, which
+    // other warps may be filling: those values are copied but never used
+    const float *arr4 = lane < 8 ? sp.x : lane < 16 ? sp.y : lane < 24 ? sp.vx : sp.vy;
+    auto issue = [&](int h, bool any) {
+        if (any) {
+            float *sl = ring + (h % SORT_PRE) * SORT_SLOT;
+            const size_t o = base + (size_t)(cap - 32 - 32 * h);
+            cp_async16(sl + 4 * lane, arr4 + o + 4 * (lane & 7));
+            if (lane < 8) cp_async16(sl + 128 + 4 * lane, sp.vz + o + 4 * lane);
+            else if (lane < 10) cp_async16(sl + 160 + 4 * (lane - 8), (const float *)(sp.code + o) + 4 * (lane - 8));
+        }
+        cp_async_commit();
+    };
+    issue(0, true);
+    const int m = sp.nmov[c];
+    if (m == 0) {
+        cp_async_wait_all();
+        return;
+    }
 #pragma unroll
-    for (int h = 0; h < SORT_PRE; h++) mv[h] = load_mover(sp, base, cap, h * 32 + lane, m);
-    // ... destination D = code (di+1)*3 + (dj+1): its stayers and slot limit ...
+    for (int h = 1; h < SORT_PRE; h++) issue(h, 32 * h < m);
+    const int i = c / ncy, j = c - i * ncy;
+    // destination D = code (di+1)*3 + (dj+1): its stayers and slot limit ...
     int off9 = 0, lim9 = 0;
     if (lane < 9) {
         const int Di = i + lane / 3 - 1, Dj = j + lane % 3 - 1;
@@ -641,89 +648,55 @@ __device__ __forceinline__ void sort_push_cell(const DevCase &d, int s, int c, i
                 pv[t] = sp.dcount[(size_t)S * 9 + (8 - Ss)];
         }
     }
+    int *so = s_off[wl], *sm = s_lim[wl];
     if (lane < 9) {
-        s_off[lane] = off9;
-        s_lim[lane] = lim9;
+        so[lane] = off9;
+        sm[lane] = lim9;
     }
     __syncwarp();
 #pragma unroll
     for (int t = 0; t < 3; t++)
-        if (pv[t]) atomicAdd(&s_off[(lane + 32 * t) / 9], pv[t]);
+        if (pv[t]) atomicAdd(&so[(lane + 32 * t) / 9], pv[t]);
     __syncwarp();
     const unsigned lt = lanemask_lt();
-    int run[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     bool overflow = false;
-    auto place = [&](const MoverRegs &v) {
-        int rank = 0;
+    for (int h = 0; 32 * h < m; h++) {
+        cp_async_wait<SORT_PRE - 1>();
+        __syncwarp(); // the chunk was copied by other lanes
+        const float *sl = ring + (h % SORT_PRE) * SORT_SLOT;
+        const int code = 32 * h + lane < m ? (int)((const int8_t *)(sl + 160))[31 - lane] : -1;
+        const float x = sl[31 - lane], y = sl[63 - lane], vx = sl[95 - lane], vy = sl[127 - lane],
+                    vz = sl[159 - lane];
+        __syncwarp(); // every lane has read the slot before it is refilled
+        issue(h + SORT_PRE, 32 * (h + SORT_PRE) < m);
+        // rank among this chunk's movers to the same destination; so[D] then
+        // advances by the chunk's movers to D
+        int rank = 0, nD = 0;
 #pragma unroll
         for (int D = 0; D < 9; D++) {
-            const unsigned b = __ballot_sync(FULL, v.code == D);
-            if (v.code == D) rank = run[D] + __popc(b & lt);
-            run[D] += __popc(b);
+            const unsigned bD = __ballot_sync(FULL, code == D);
+            if (code == D) rank = __popc(bD & lt);
+            if (lane == D) nD = __popc(bD);
         }
-        if (v.code >= 0 && v.code < 9) {
-            const int slot = s_off[v.code] + rank;
-            if (slot < s_lim[v.code]) {
-                const size_t dst = (size_t)(c + (v.code / 3 - 1) * ncy + (v.code % 3 - 1)) * cap + (size_t)slot;
-                sp.x[dst] = v.x;
-                sp.y[dst] = v.y;
-                sp.vx[dst] = v.vx;
-                sp.vy[dst] = v.vy;
-                sp.vz[dst] = v.vz;
+        const int slot = code >= 0 && code < 9 ? so[code] + rank : 0;
+        __syncwarp();
+        if (lane < 9) so[lane] += nD;
+        __syncwarp();
+        if (code >= 0 && code < 9) {
+            if (slot < sm[code]) {
+                const size_t dst = (size_t)(c + (code / 3 - 1) * ncy + (code % 3 - 1)) * cap + (size_t)slot;
+                sp.x[dst] = x;
+                sp.y[dst] = y;
+                sp.vx[dst] = vx;
+                sp.vy[dst] = vy;
+                sp.vz[dst] = vz;
             } else {
                 overflow = true;
             }
         }
-    };
-#pragma unroll
-    for (int h = 0; h < SORT_PRE; h++)
-        if (h * 32 < m) place(mv[h]);
-    for (int r0 = SORT_PRE * 32; r0 < m; r0 += SORT_PRE * 32) {
-#pragma unroll
-        for (int h = 0; h < SORT_PRE; h++) mv[h] = load_mover(sp, base, cap, r0 + h * 32 + lane, m);
-#pragma unroll
-        for (int h = 0; h < SORT_PRE; h++)
-            if (r0 + h * 32 < m) place(mv[h]);
     }
+    cp_async_wait_all();
     if (__any_sync(FULL, overflow) && lane == 0) atomicOr(d.status, ST_OVERFLOW);
-    __syncwarp(); // s_off / s_lim are reused by the warp's next cell
-}
-
-// SORT_G consecutive (species, cell) items per warp: one lane per item reads
-// its mover count, then the warp places the movers of the items that have
-// any, one cell after the other.  One item per warp is fastest on B200 (the
-// cells' dependent load chains then overlap across warps instead of running
-// one after the other inside a warp); larger groups only save the idle ion
-// warps.
-#ifndef SORT_G
-#define SORT_G 1
-#endif
-#ifndef SORT_MINB
-#define SORT_MINB 2 // resident blocks per SM the register budget is set for
-#endif
-__global__ void __launch_bounds__(SORT_MAXW * 32, SORT_MINB) k_sort_push(const DevCase *__restrict__ cases,
-                                                           const int *__restrict__ item_start, int ncases, int items) {
-    __shared__ int s_off[SORT_MAXW][9], s_lim[SORT_MAXW][9];
-    const int warp = (int)((blockIdx.x * (unsigned)blockDim.x + threadIdx.x) >> 5);
-    const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
-    const int first = warp * SORT_G;
-    if (first >= items) return;
-    int ci = 0, m = 0;
-    if (lane < SORT_G && first + lane < items) {
-        ci = find_case(item_start, ncases, first + lane);
-        const DevCase &d = cases[ci];
-        const int w = first + lane - item_start[ci];
-        const int s = w / d.C, c = w - s * d.C;
-        m = d.sp[s].nmov[c];
-    }
-    for (unsigned todo = __ballot_sync(FULL, m > 0); todo; todo &= todo - 1) {
-        const int src = __ffs(todo) - 1;
-        const int fci = __shfl_sync(FULL, ci, src), fm = __shfl_sync(FULL, m, src);
-        const DevCase &d = cases[fci];
-        const int w = first + src - item_start[fci];
-        const int s = w / d.C, c = w - s * d.C;
-        sort_push_cell(d, s, c, fm, s_off[wl], s_lim[wl], lane);
-    }
 }
 
 // One lane per destination cell (32 cells per warp): the new count is its
@@ -2170,8 +2143,8 @@ cudaError_t launch_sort(const DevCase *cases, const int *item_start, int ncases,
     // and Deposit prefer smaller blocks
     const int tpb = 32 * std::min(std::max(lc.warps_per_block, 8), SORT_MAXW);
     prof::mark(st, "k_sort_push");
-    k_sort_push<<<blocks_for((long long)(items + SORT_G - 1) / SORT_G * 32, tpb), tpb, 0, st>>>(cases, item_start,
-                                                                                               ncases, items);
+    k_sort_push<<<blocks_for((long long)items * 32, tpb), tpb, (size_t)(tpb / 32) * SORT_PRE * SORT_SLOT * sizeof(float),
+                  st>>>(cases, item_start, ncases, items);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     prof::mark(st, "k_sort_count");
