@@ -87,6 +87,7 @@ hp_status batch_dev_build(hp_case *const *cases, int n, BatchDev &b) {
     CK(cudaMemcpy(b.d_fluid, fl.data(), sizeof(int) * fl.size(), cudaMemcpyHostToDevice));
     b.fluid.xl_items = b.d_fluid;
     b.fluid.yl_items = b.d_fluid + n + 1;
+    if (b.fluid.n_x + b.fluid.n_y > 0) CK(fluid_fork_create(b.fluid_fork));
     std::vector<int> lists;
     for (int m = 0; m < 5; m++)
         for (int k = 0; k <= m; k++) {
@@ -140,11 +141,13 @@ void batch_dev_free(BatchDev &b) {
     cudaFree(b.d_lists);
     cudaFree(b.d_fluid);
     fast_plan_free(b.fast);
+    fluid_fork_destroy(b.fluid_fork);
     b = BatchDev();
 }
 
 hp_status run_step(const BatchDev &b, const LaunchCfg &lc, int gas, cudaStream_t st) {
     CK(launch_advance(b.d_cases, b.n, st));
+    if (b.fluid.any) CK(fluid_begin(b.d_cases, b.n, b.fluid, b.fluid_fork, st));
     const std::vector<PcgGroup> g = b.groups(lc.pcg_cluster_max, lc.pcg_block);
     CK(launch_field(b.d_cases, b.d_node, b.n, b.n_node, g.data(), (int)g.size(), &b.fast.plan, st, b.circuit));
     CK(launch_move(b.d_cases, b.d_part, b.n, b.n_part, lc, st));
@@ -152,7 +155,7 @@ hp_status run_step(const BatchDev &b, const LaunchCfg &lc, int gas, cudaStream_t
     if (gas != GAS_AR) CK(launch_mcc_oxy(b.d_cases, b.d_cell, b.n, b.n_cell, gas, st));
     else CK(launch_mcc_ar(b.d_cases, b.d_cell, b.n, b.n_cell, lc, st));
     CK(launch_deposit(b.d_cases, b.d_part, b.d_node, b.n, b.n_part, b.n_node, lc, st, b.max_smt));
-    if (b.fluid.any) CK(launch_fluid(b.d_cases, b.d_node, b.n, b.n_node, b.fluid, st));
+    if (b.fluid.any) CK(fluid_end(b.d_cases, b.d_node, b.n, b.n_node, b.fluid, b.fluid_fork, st));
     CK(launch_accumulate(b.d_cases, b.d_node, b.n, b.n_node, st));
     if (b.any_eedf) CK(launch_eedf(b.d_cases, b.d_cell, b.n, b.n_cell, st));
     if (b.power) CK(launch_power(b.d_cases, b.n, st));

@@ -591,13 +591,17 @@ hp_status op_deposit(hp_case *c, cudaStream_t st, bool smooth) {
 hp_status one_step(hp_case *c, cudaStream_t st) {
     cudaError_t e = launch_advance(c->d_case, 1, st);
     if (e != cudaSuccess) return cuda_fail(e, "advance");
+    if (c->fplan_fluid.any) {
+        e = fluid_begin(c->d_case, 1, c->fplan_fluid, c->fl_fork, st);
+        if (e != cudaSuccess) return cuda_fail(e, "fluid");
+    }
     TRY(op_field(c, st));
     TRY(op_move(c, st));
     TRY(op_sort(c, st));
     TRY(op_mcc(c, st));
     TRY(op_deposit(c, st, true));
     if (c->fplan_fluid.any) {
-        e = launch_fluid(c->d_case, c->d_items + 4, 1, c->s.Gsize, c->fplan_fluid, st);
+        e = fluid_end(c->d_case, c->d_items + 4, 1, c->s.Gsize, c->fplan_fluid, c->fl_fork, st);
         if (e != cudaSuccess) return cuda_fail(e, "fluid");
     }
     e = launch_accumulate(c->d_case, c->d_items + 4, 1, c->s.Gsize, st);
@@ -839,6 +843,10 @@ static hp_status case_from(Setup s, const hp_case_opts *opts, hp_case **out) {
         cudaError_t e = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) st = cuda_fail(e, "cudaStreamCreate");
     }
+    if (st == HP_OK && c->fplan_fluid.n_x + c->fplan_fluid.n_y > 0) {
+        cudaError_t e = fluid_fork_create(c->fl_fork);
+        if (e != cudaSuccess) st = cuda_fail(e, "fluid side stream");
+    }
     if (st == HP_OK) st = op_deposit(c, c->own_stream, false); // Deposit_Basic before the loop (src/cuda_main.cu:28)
     if (st == HP_OK) {
         cudaError_t e = cudaStreamSynchronize(c->own_stream);
@@ -920,6 +928,7 @@ hp_status hp_case_destroy(hp_case *c) {
         cudaStreamSynchronize(c->own_stream);
         cudaStreamDestroy(c->own_stream);
     }
+    fluid_fork_destroy(c->fl_fork);
     cudaDeviceSynchronize();
     for (void *p : c->allocs) cudaFree(p);
     hpi::fast_plan_free(c->fplan);

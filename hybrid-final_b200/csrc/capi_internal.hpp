@@ -54,6 +54,7 @@ struct hp_case {
     char *fl_state = nullptr;  // fluid averaging state (HP_GRID_FLUID_STATE), also holding h.prob
     size_t fl_state_bytes = 0;
     hp::FluidPlan fplan_fluid; // the case's own fluid launch lists (into d_items)
+    hp::FluidFork fl_fork;     // side stream of the fluid sweeps (fluid cases)
     std::vector<uint32_t> mcc_base; // collision tallies at the last hp_reset_averages (empty: zeros)
 };
 
@@ -81,6 +82,7 @@ struct BatchDev {
     bool circuit = false; // some case has an external circuit
     int *d_fluid = nullptr; // fluid line prefixes: x lines [n+1], then y lines [n+1]
     hp::FluidPlan fluid;
+    hp::FluidFork fluid_fork; // side stream of the fluid sweeps (batches with fluid cases)
     // PCG groups for every cluster cap 1,2,4,8,16: lists of case indices per
     // cluster size, concatenated in d_lists
     int *d_lists = nullptr;

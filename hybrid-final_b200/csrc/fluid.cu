@@ -85,22 +85,59 @@ __global__ void __launch_bounds__(128) k_fluid_sweep(const DevCase *__restrict__
     __syncwarp();
     int ok = 1;
     if (lane == 0) { // tridiag, src/cuda_Fluid.cu:168-184
-        float bet;
-        D[0] = D[0] / (bet = B[0]);
+        // The recurrences carry their last values in registers and the next
+        // cell's coefficients are loaded one cell ahead, so the loop's chain
+        // is the arithmetic alone (a shared-memory load per step otherwise:
+        // the compiler cannot tell the four diagonals apart).  The float
+        // operations and their order are the reference's.
+        float bet = B[0];
+        float dprev = D[0] / bet;
+        D[0] = dprev;
+        float c1 = Cc[0], a = 0.f, b = 0.f, dj = 0.f, cn = 0.f;
+        if (num > 1) {
+            a = A[1];
+            b = B[1];
+            dj = D[1];
+            cn = Cc[1];
+        }
         for (int j = 1; j < num; j++) {
-            const float c1 = Cc[j - 1];
+            float an = 0.f, bn = 0.f, dn = 0.f, cnn = 0.f;
+            if (j + 1 < num) {
+                an = A[j + 1];
+                bn = B[j + 1];
+                dn = D[j + 1];
+                cnn = Cc[j + 1];
+            }
             const float gam = c1 / bet;
-            const float nb = B[j] - A[j] * c1 / bet;
-            D[j] = (D[j] - A[j] * D[j - 1]) / nb;
+            const float nb = b - a * c1 / bet;
+            dprev = (dj - a * dprev) / nb;
+            D[j] = dprev;
             Cc[j - 1] = gam;
             bet = nb;
             if (bet == 0) {
                 ok = 0;
                 break;
             }
+            c1 = cn;
+            a = an;
+            b = bn;
+            dj = dn;
+            cn = cnn;
         }
-        if (ok)
-            for (int j = num - 2; j >= 0; j--) D[j] -= Cc[j] * D[j + 1];
+        if (ok && num > 1) {
+            float xn = dprev, dk = D[num - 2], ck = Cc[num - 2];
+            for (int j = num - 2; j >= 0; j--) {
+                float dk1 = 0.f, ck1 = 0.f;
+                if (j > 0) {
+                    dk1 = D[j - 1];
+                    ck1 = Cc[j - 1];
+                }
+                xn = dk - ck * xn;
+                D[j] = xn;
+                dk = dk1;
+                ck = ck1;
+            }
+        }
     }
     ok = __shfl_sync(FULL, ok, 0);
     __syncwarp();
@@ -190,8 +227,8 @@ int fluid_sweep_warps(int L) {
     return per_warp > FLUID_SMEM_MAX ? 0 : w;
 }
 
-cudaError_t launch_fluid(const DevCase *cases, const int *node_items, int ncases, int n_node_items,
-                         const FluidPlan &fp, cudaStream_t st) {
+namespace {
+cudaError_t launch_fluid_sweeps(const DevCase *cases, int ncases, const FluidPlan &fp, cudaStream_t st) {
     for (int dir = 0; dir < 2; dir++) {
         const int items = dir ? fp.n_y : fp.n_x, L = dir ? fp.len_y : fp.len_x;
         if (items <= 0) continue;
@@ -210,12 +247,62 @@ cudaError_t launch_fluid(const DevCase *cases, const int *node_items, int ncases
         cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
+    return cudaSuccess;
+}
+
+cudaError_t launch_fluid_diag(const DevCase *cases, const int *node_items, int ncases, int n_node_items,
+                              const FluidPlan &fp, cudaStream_t st) {
     if (fp.n_x > 0 || fp.n_y > 0 || fp.any) {
         prof::mark(st, "k_fluid_diag");
         k_fluid_diag<<<blocks_for(n_node_items, 256), 256, 0, st>>>(cases, node_items, ncases, n_node_items);
         return cudaGetLastError();
     }
     return cudaSuccess;
+}
+
+bool forked(const FluidPlan &fp, const FluidFork &f) { return f.side && !prof::g_on && (fp.n_x > 0 || fp.n_y > 0); }
+} // namespace
+
+cudaError_t launch_fluid(const DevCase *cases, const int *node_items, int ncases, int n_node_items,
+                         const FluidPlan &fp, cudaStream_t st) {
+    cudaError_t e = launch_fluid_sweeps(cases, ncases, fp, st);
+    if (e != cudaSuccess) return e;
+    return launch_fluid_diag(cases, node_items, ncases, n_node_items, fp, st);
+}
+
+cudaError_t fluid_fork_create(FluidFork &f) {
+    cudaError_t e = cudaStreamCreateWithFlags(&f.side, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f.fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&f.join, cudaEventDisableTiming);
+    if (e != cudaSuccess) fluid_fork_destroy(f);
+    return e;
+}
+
+void fluid_fork_destroy(FluidFork &f) {
+    if (f.side) {
+        cudaStreamSynchronize(f.side);
+        cudaStreamDestroy(f.side);
+    }
+    if (f.fork) cudaEventDestroy(f.fork);
+    if (f.join) cudaEventDestroy(f.join);
+    f = FluidFork();
+}
+
+cudaError_t fluid_begin(const DevCase *cases, int ncases, const FluidPlan &fp, const FluidFork &f, cudaStream_t st) {
+    if (!forked(fp, f)) return cudaSuccess;
+    cudaError_t e = cudaEventRecord(f.fork, st);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(f.side, f.fork, 0);
+    if (e == cudaSuccess) e = launch_fluid_sweeps(cases, ncases, fp, f.side);
+    if (e == cudaSuccess) e = cudaEventRecord(f.join, f.side);
+    return e;
+}
+
+cudaError_t fluid_end(const DevCase *cases, const int *node_items, int ncases, int n_node_items, const FluidPlan &fp,
+                      const FluidFork &f, cudaStream_t st) {
+    if (!forked(fp, f)) return launch_fluid(cases, node_items, ncases, n_node_items, fp, st);
+    cudaError_t e = cudaStreamWaitEvent(st, f.join, 0);
+    if (e != cudaSuccess) return e;
+    return launch_fluid_diag(cases, node_items, ncases, n_node_items, fp, st);
 }
 
 } // namespace hp

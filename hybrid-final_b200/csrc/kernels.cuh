@@ -104,5 +104,22 @@ constexpr size_t FLUID_SMEM_MAX = 200 * 1024;
 int fluid_sweep_warps(int L);
 cudaError_t launch_fluid(const DevCase *cases, const int *node_items, int ncases, int n_node_items,
                          const FluidPlan &fp, cudaStream_t st);
+// The same split around the step's particle phases: the sweeps read only the
+// fluid arrays (densities, fluxes, the sources of the last averaging cycle)
+// and the step counter, and nothing between k_advance and the averaging cycle
+// touches those arrays, so fluid_begin (right after k_advance) runs the
+// sweeps on a side stream forked from st, concurrently with Field ... Deposit,
+// and fluid_end (before the accumulation) joins it back and runs the
+// averaging cycle.  Without a side stream, or while a per-kernel profile is
+// recorded, fluid_begin does nothing and fluid_end runs launch_fluid.
+struct FluidFork {
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork = nullptr, join = nullptr;
+};
+cudaError_t fluid_fork_create(FluidFork &f);
+void fluid_fork_destroy(FluidFork &f);
+cudaError_t fluid_begin(const DevCase *cases, int ncases, const FluidPlan &fp, const FluidFork &f, cudaStream_t st);
+cudaError_t fluid_end(const DevCase *cases, const int *node_items, int ncases, int n_node_items, const FluidPlan &fp,
+                      const FluidFork &f, cudaStream_t st);
 
 } // namespace hp
