@@ -171,6 +171,7 @@ constexpr int CODE_FAR = 14, CODE_ABSORBED = 15;
 // far movers a destination cell accepts per step (per species)
 constexpr int FAR_B = HP_FAR_BUCKET;
 constexpr int FAR_W = FAR_B / 32; // bucket keys per lane when a warp sorts a bucket
+constexpr int FAR_LANE = 8;       // buckets up to this size are finished by one lane
 static_assert(FAR_B % 32 == 0, "far buckets hold whole warps of keys");
 
 // Where a particle that left cell (i, j) ends.  Each crossing wraps the
@@ -730,7 +731,47 @@ __global__ void __launch_bounds__(SORT_MAXW * 32) k_sort_count(const DevCase *__
         nf = d.far_in[(size_t)s * d.C + c];
     }
     bool overflow = false;
-    for (unsigned fm = __ballot_sync(FULL, nf > 0); fm; fm &= fm - 1) {
+    // a bucket of at most FAR_LANE keys is finished by its own lane: keys
+    // sorted in registers by a fixed 19-comparator network (padding keys ~0
+    // sort last), then its movers copied in that order; the lanes' buckets
+    // proceed together instead of one after the other
+    if (nf > 0 && nf <= FAR_LANE) {
+        const DevCase &d = cases[ci];
+        const DevSpecies &sp = d.sp[s];
+        const int cap = sp.cap;
+        const size_t b = (size_t)s * d.C + c;
+        unsigned long long k8[FAR_LANE];
+#pragma unroll
+        for (int t = 0; t < FAR_LANE; t++) k8[t] = t < nf ? d.far_key[b * FAR_B + t] : ~0ull;
+        d.far_in[b] = 0;
+        constexpr int NET[19][2] = {{0, 2}, {1, 3}, {4, 6}, {5, 7}, {0, 4}, {1, 5}, {2, 6}, {3, 7}, {0, 1}, {2, 3},
+                                    {4, 5}, {6, 7}, {2, 4}, {3, 5}, {1, 4}, {3, 6}, {1, 2}, {3, 4}, {5, 6}};
+#pragma unroll
+        for (int e = 0; e < 19; e++) {
+            const unsigned long long lo = k8[NET[e][0]], hi = k8[NET[e][1]];
+            k8[NET[e][0]] = lo < hi ? lo : hi;
+            k8[NET[e][1]] = lo < hi ? hi : lo;
+        }
+#pragma unroll
+        for (int t = 0; t < FAR_LANE; t++) {
+            if (t >= nf) break;
+            const int slot = out + t;
+            if (slot < limit) {
+                const int sc = (int)(k8[t] >> 18), r = (int)(k8[t] & 0x3FFFF);
+                const size_t q = (size_t)sc * cap + (size_t)(cap - 1 - r);
+                const size_t dst = (size_t)c * cap + (size_t)slot;
+                sp.x[dst] = sp.x[q];
+                sp.y[dst] = sp.y[q];
+                sp.vx[dst] = sp.vx[q];
+                sp.vy[dst] = sp.vy[q];
+                sp.vz[dst] = sp.vz[q];
+            } else {
+                overflow = true;
+            }
+        }
+        out += nf;
+    }
+    for (unsigned fm = __ballot_sync(FULL, nf > FAR_LANE); fm; fm &= fm - 1) {
         const int src = __ffs(fm) - 1;
         const int fci = __shfl_sync(FULL, ci, src), fs = __shfl_sync(FULL, s, src), fc = __shfl_sync(FULL, c, src);
         const int fout = __shfl_sync(FULL, out, src), flimit = __shfl_sync(FULL, limit, src);
