@@ -207,7 +207,9 @@ hp_status hp_Deposit(hp_case *c, void *stream);
 hp_status hp_Deposit_noalloc(hp_case *c, double *den_out, void *stream);
 /* n steps of the main loop body (src/cuda_main.cu:114-183 without the
  * diagnostics and dump calls), fused where results allow; replayed from a
- * CUDA graph after the first call on a stream. */
+ * CUDA graph after the first call on a stream.  A case with fluid species
+ * runs each step's continuity sweeps on a stream of its own, forked from and
+ * joined back into `stream` within the step. */
 hp_status hp_step(hp_case *c, int nsteps, void *stream);
 /* Kernels launched by one hp_step (the kernel nodes of its captured graph;
  * 0 before the first hp_step).  No reference counterpart: launch accounting
