@@ -670,18 +670,15 @@ __global__ void __launch_bounds__(SORT_MAXW * 32, SORT_MINB) k_sort_push(const D
                     vz = sl[159 - lane];
         __syncwarp(); // every lane has read the slot before it is refilled
         issue(h + SORT_PRE, 32 * (h + SORT_PRE) < m);
-        // rank among this chunk's movers to the same destination; so[D] then
-        // advances by the chunk's movers to D
-        int rank = 0, nD = 0;
-#pragma unroll
-        for (int D = 0; D < 9; D++) {
-            const unsigned bD = __ballot_sync(FULL, code == D);
-            if (code == D) rank = __popc(bD & lt);
-            if (lane == D) nD = __popc(bD);
-        }
-        const int slot = code >= 0 && code < 9 ? so[code] + rank : 0;
+        // rank among this chunk's movers to the same destination (the lanes
+        // holding the same code); so[D] then advances by their number, added
+        // by the group's highest lane
+        const unsigned grp = __match_any_sync(FULL, code);
+        const int rank = __popc(grp & lt);
+        const bool near = code >= 0 && code < 9;
+        const int slot = near ? so[code] + rank : 0;
         __syncwarp();
-        if (lane < 9) so[lane] += nD;
+        if (near && (grp >> lane) == 1u) so[code] += __popc(grp);
         __syncwarp();
         if (code >= 0 && code < 9) {
             if (slot < sm[code]) {
