@@ -14,7 +14,7 @@ struct LaunchCfg {
     int pcg_block = 512;       // PCG: threads per CTA
     int pcg_cluster_max = 16;  // PCG: upper bound on CTAs per case
     int move_unroll = 1;       // Move: chunks of 32 loaded per iteration (1: k_move, one-chunk prefetch)
-    int mcc_cells = 8;         // MCC (Ar): consecutive cells per warp, sharing collision batches (1, 2, 4, 8, 16)
+    int mcc_cells = 16;        // MCC (Ar): consecutive cells per warp, sharing collision batches (1, 2, 4, 8, 16)
 };
 
 // Move: gather + push + single-cell exit test (src/cuda_Move.cu:181-270)
