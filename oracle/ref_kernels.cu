@@ -172,6 +172,54 @@ void sync(const char *what) {
     ck(cudaDeviceSynchronize(), what);
 }
 
+// Optional timing (rk_set_timing): before its checked launch, each timed
+// kernel runs `g_reps` more times, every time on a restored copy of its
+// inputs, with the launch shape the reference picks at start-up
+// (cudaOccupancyMaxPotentialBlockSize over Gsize*nsp threads,
+// src/cuda_Init.cu:35-46), bracketed by CUDA events; g_ms[k] is the mean
+// time of the k-th timed kernel of the last call.
+int g_reps = 0;
+float g_ms[8] = {};
+
+template <class K> int ref_block(K kern, long long nthreads) {
+    int mingrid = 0, block = 0;
+    ck(cudaOccupancyMaxPotentialBlockSize(&mingrid, &block, kern, 0, (int)std::min<long long>(nthreads, 1 << 30)),
+       "cudaOccupancyMaxPotentialBlockSize");
+    need(block > 0, "no launchable block size");
+    return block;
+}
+
+template <class T> void restore(T *dst, const T *src, size_t n) {
+    if (n) ck(cudaMemcpy(dst, src, n * sizeof(T), cudaMemcpyDeviceToDevice), "cudaMemcpy D2D");
+}
+template <class T> T *snapshot(Arena &a, const T *d, size_t n) {
+    T *p = a.alloc<T>(n);
+    restore(p, d, n);
+    return p;
+}
+
+// events around nk kernels launched back to back on the default stream
+struct Timed {
+    cudaEvent_t e[9];
+    int nk;
+    explicit Timed(int n) : nk(n) {
+        for (int k = 0; k <= nk; k++) ck(cudaEventCreate(&e[k]), "cudaEventCreate");
+        std::fill(g_ms, g_ms + 8, 0.f);
+    }
+    ~Timed() {
+        for (int k = 0; k <= nk; k++) cudaEventDestroy(e[k]);
+    }
+    void mark(int k) { ck(cudaEventRecord(e[k]), "cudaEventRecord"); }
+    void add() {
+        ck(cudaEventSynchronize(e[nk]), "cudaEventSynchronize");
+        for (int k = 0; k < nk; k++) {
+            float t = 0.f;
+            ck(cudaEventElapsedTime(&t, e[k], e[k + 1]), "cudaEventElapsedTime");
+            g_ms[k] += t / (float)g_reps;
+        }
+    }
+};
+
 template <class F> int guarded(F f) {
     try {
         g_err.clear();
@@ -194,6 +242,15 @@ typedef struct rk_case {
 } rk_case;
 
 const char *rk_last_error(void) { return g_err.c_str(); }
+
+/* Timing of the reference kernels: reps > 0 makes rk_move and rk_deposit
+ * first run their kernels reps times on restored copies of the inputs with
+ * the reference's launch shape, timed with CUDA events (0 turns it off).
+ * rk_last_ms copies the mean times of the last timed call: rk_move
+ * {MoveE_Basic}; rk_deposit {DepositInitDensity, DepositAtom,
+ * DepositBoundary, SumSource}. */
+void rk_set_timing(int reps) { g_reps = reps > 0 ? reps : 0; }
+void rk_last_ms(float *out8) { std::memcpy(out8, g_ms, sizeof(g_ms)); }
 
 } // extern "C"
 
@@ -449,6 +506,24 @@ int rk_move(const rk_case *c, const float *ex, const float *ey, int *pnc, int *p
         GGA *df = a.put(f);
         GCP *ds = a.put(sp);
         GPG *dg = a.put(g);
+        if (g_reps > 0) {
+            const GCP *ds0 = snapshot(a, ds, sp.size());
+            const GPG *dg0 = snapshot(a, dg, g.size());
+            const long long nt = (long long)d.nsp * d.G;
+            const int b = ref_block(MoveE_Basic, nt);
+            Timed t(1);
+            for (int r = 0; r < g_reps; r++) {
+                restore(ds, ds0, sp.size());
+                restore(dg, dg0, g.size());
+                t.mark(0);
+                MoveE_Basic<<<blocks(nt, b), b>>>(d.G, c->ngy, c->dt_dx, c->dt_dy, di, ds, dg, df);
+                t.mark(1);
+                t.add();
+            }
+            sync("MoveE_Basic (timed)");
+            restore(ds, ds0, sp.size());
+            restore(dg, dg0, g.size());
+        }
         MoveE_Basic<<<blocks((long long)d.nsp * d.G, 256), 256>>>(d.G, c->ngy, c->dt_dx, c->dt_dy, di, ds, dg, df);
         sync("MoveE_Basic");
         get(sp, ds);
@@ -596,6 +671,31 @@ int rk_deposit(const rk_case *c, const int *face, const int *boundary, const int
         GGA *dv = a.put(v);
         float *dsig = a.put(sig);
         float *dsrc = a.alloc<float>((size_t)d.G);
+        if (g_reps > 0) { // DEPOSIT_GRID/DEPOSIT_BLOCK: DepositAtom's shape for all four kernels
+            const GPG *dg0 = snapshot(a, dg, g.size());
+            const float *dsig0 = snapshot(a, dsig, sig.size());
+            const long long nt = (long long)d.nsp * d.G;
+            const int b = ref_block(DepositAtom, nt);
+            const unsigned gb = blocks(nt, b);
+            Timed t(4);
+            for (int r = 0; r < g_reps; r++) {
+                restore(dg, dg0, g.size());
+                restore(dsig, dsig0, sig.size());
+                t.mark(0);
+                DepositInitDensity<<<gb, b>>>(d.G, di, dg);
+                t.mark(1);
+                DepositAtom<<<gb, b>>>(d.G, c->ngy, di, ds, dg);
+                t.mark(2);
+                DepositBoundary<<<gb, b>>>(d.G, c->ngy, d.nsp, dv, dg);
+                t.mark(3);
+                SumSource<<<gb, b>>>(d.nsp, d.G, c->ngx, c->ngy, di, dv, dg, dsig, dsrc);
+                t.mark(4);
+                t.add();
+            }
+            sync("Deposit (timed)");
+            restore(dg, dg0, g.size());
+            restore(dsig, dsig0, sig.size());
+        }
         const unsigned nb = blocks((long long)d.nsp * d.G, 256);
         DepositInitDensity<<<nb, 256>>>(d.G, di, dg);
         DepositAtom<<<nb, 256>>>(d.G, c->ngy, di, ds, dg);

@@ -41,6 +41,8 @@ def lib():
         P = C.POINTER(RkCase)
         sig = {
             "rk_last_error": (C.c_char_p, []),
+            "rk_set_timing": (None, [C.c_int]),
+            "rk_last_ms": (None, [_F]),
             "rk_move": (C.c_int, [P, _F, _F, _I, _I, _F, _F, _F, _F, _F, _I]),
             "rk_sortboundary": (C.c_int, [P, C.c_int, _I, _I, _I, _F, _F, _F, _F, _F, _I, _F, _I]),
             "rk_sort_probe": (C.c_int, [P, _I, _I, _I, _I, _LL, _I]),
@@ -176,6 +178,20 @@ def move(rc, st, ex, ey):
     ex, ey = f32(ex), f32(ey)
     _check(lib().rk_move(C.byref(rc), _f(ex), _f(ey), _i(st.pnc), _i(st.pnmc), *[_f(a) for a in st.a],
                          _i(st.cellid)))
+
+
+def set_timing(reps):
+    """reps > 0: move() and deposit() also time their reference kernels
+    over reps launches on restored inputs (the reference's launch shape)."""
+    lib().rk_set_timing(int(reps))
+
+
+def last_ms():
+    """Mean kernel times (ms) of the last timed call: move() [MoveE_Basic];
+    deposit() [DepositInitDensity, DepositAtom, DepositBoundary, SumSource]."""
+    out = np.zeros(8, np.float32)
+    lib().rk_last_ms(_f(out))
+    return [float(v) for v in out]
 
 
 def sortboundary(rc, st, sidx, cond_num):

@@ -41,6 +41,10 @@ reference's code, which pins the restatement:
   are skipped: there the reference adds the next cross section to a running
   sum it has not set (accumulator_undefined).
 
+Timing.  MoveE_Basic, the Deposit kernels and PCG_float are also timed
+against this library's kernels at the benchmark sizes (CUDA events, the
+reference's launch shape), with the times printed.
+
 Tolerances.  Integers are exact: cell counts, mover cell offsets, reaction
 channels, conductor counts, created particles.  The reference is built with
 -use_fast_math (approximate exp/log/pow/sin/cos/tan, contracted multiply-
@@ -269,6 +273,63 @@ def test_pcg_matches_reference():
     assert abs(it1 - it_or[0]) <= max(3, 0.05 * it_or[0]), (it1, it_or[0])
     assert rel_err(x1, xd, xs) <= 1e-2 and rel_err(xo, xd, xs) <= 1e-2
     assert rel_err(x1, xo, xs) <= 1e-2
+
+
+def test_move_and_deposit_time_against_the_reference_kernels():
+    """The 513x257 Ar case of 200 particles per cell and species (52M
+    particles, 100 V, 50 mTorr).  On the initial state and the field of the
+    first step, the reference's MoveE_Basic and its Deposit kernels
+    (DepositInitDensity, DepositAtom, DepositBoundary, SumSource) are timed
+    with CUDA events over 5 launches on restored inputs, with the launch
+    shape the reference picks (src/cuda_Init.cu:35-46); this library's
+    kernels are timed per launch over three op-by-op steps of the same case
+    (hp_profile_step).  Both sides' times are printed.  The reference's Move
+    and this library's Move (move_mode 0, its one-crossing rule) leave the
+    same stayers in each cell, but for cells where the two builds round a
+    position at a cell edge differently (fast-math contractions against
+    explicit fused multiply-adds): at most 1e-4 of the cells."""
+    deck = ccp_deck(513, 257, 0.16, 0.08, ppc=200, voltage=100.0, pressure_torr=0.05)
+    S = hpic.Setup(deck, seed=11, move_mode=0, field_mode=2)
+    info = S.info
+    o = oracle.Oracle(S.table, S.info, S.opts, 32)  # the float constants of the reference case
+    rc = refk.case_from_oracle(o, MPNC)
+    del o
+    st = refk.to_ref(info, MPNC, [S.particles(s, layout=0) for s in range(info.nsp)])
+    case = hpic.Case(setup=S, seed=11, move_mode=0, field_mode=2)
+    case.Deposit()
+    case.set_tstep(1)
+    case.Field()
+    ex, ey = case.grid("EX"), case.grid("EY")
+    try:
+        refk.set_timing(5)
+        refk.deposit(rc, st, S.table("face"), S.table("boundary"), S.table("cond_id"), S.table("area"))
+        dep_ref = refk.last_ms()[:4]
+        refk.move(rc, st, ex, ey)
+        move_ref = refk.last_ms()[0]
+    finally:
+        refk.set_timing(0)
+    case.Move()
+    G = info.Gsize
+    node = refk.cell_to_node(info)
+    for s in range(info.nsp):
+        ours, _ = case.particles(s)
+        ref = st.pnc[s * G + node]
+        differ = int(np.count_nonzero(ours != ref))
+        assert differ <= 1e-4 * info.Csize, f"species {s}: stayers differ in {differ} of {info.Csize} cells"
+        assert abs(int(ours.sum()) - int(ref.sum())) <= 1e-6 * int(ref.sum()) + 8
+    case.SortBoundary()
+    case.MCC()
+    case.Deposit()
+    stats = {name: ms / max(n, 1) for name, n, ms in case.profile(3)}
+    case.close()
+    ours_dep = sum(stats.get(k, 0.0) for k in ("k_deposit_cells", "k_deposit_nodes", "k_source"))
+    ours_sort = stats.get("k_sort_count", 0.0) + stats.get("k_sort_push", 0.0)
+    print(f"513x257 200 ppc, {int(st.pnc.sum())} stayers after the reference Move: "
+          f"MoveE_Basic {move_ref:.3f} ms; DepositInitDensity/Atom/Boundary/SumSource "
+          f"{' / '.join(f'{t:.3f}' for t in dep_ref)} = {sum(dep_ref):.3f} ms | this library: k_move "
+          f"{stats['k_move']:.3f} ms (+ sort {ours_sort:.3f} ms, the boundary rules the reference applies in "
+          f"SortBoundary), deposit {ours_dep:.3f} ms")
+    assert move_ref > 0 and min(dep_ref) > 0 and stats["k_move"] > 0 and ours_dep > 0
 
 
 @pytest.mark.parametrize("ngx,ngy,xl,yl", [(129, 65, 0.04, 0.02), (513, 257, 0.16, 0.08)])
