@@ -1228,6 +1228,12 @@ __global__ void __launch_bounds__(512) k_deposit_cells(const DevCase *__restrict
 #pragma unroll
     for (int g = 0; g < G; g++) {
         if (!px[g]) continue; // past the last item (warp-uniform)
+        const int ng = n[g];
+        if (ng == 0) { // warp-uniform: the sums of an empty cell are +0, as the tree would give
+            double4 *cw = (double4 *)__shfl_sync(FULL, (unsigned long long)my_cw, g);
+            if (lane == 0) *cw = make_double4(0.0, 0.0, 0.0, 0.0);
+            continue;
+        }
         float WS = 0.f, WN = 0.f, ES = 0.f, EN = 0.f;
         auto add = [&](float lx, float ly) {
             WS += (1 - lx) * (1 - ly);
@@ -1235,7 +1241,6 @@ __global__ void __launch_bounds__(512) k_deposit_cells(const DevCase *__restrict
             ES += lx * (1 - ly);
             EN += lx * ly;
         };
-        const int ng = n[g];
         if (lane < ng) add(x0[g], y0[g]);
         for (int k0 = 32; k0 < ng; k0 += 128) {
             float xs[4], ys[4];
